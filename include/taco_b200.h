@@ -1,0 +1,164 @@
+/*
+ * taco_b200.h -- C-ABI of the B200 TCL4 engine (libtaco_b200.so).
+ *
+ * Plain pointers and sizes only.  Complex numbers are interleaved (re, im) pairs,
+ * layout-compatible with std::complex<double> / cuDoubleComplex (taco_c128) and
+ * std::complex<float> (taco_c64).  Matrices are column-major, as Eigen's defaults in
+ * the reference.  Every entry point returns a taco_status; on failure the message is
+ * available from taco_last_error() (thread-local).  The status codes correspond to the
+ * exception types the reference throws:
+ *   TACO_ERR_INVALID_ARGUMENT  std::invalid_argument
+ *   TACO_ERR_OUT_OF_RANGE      std::out_of_range   (time index >= Nt)
+ *   TACO_ERR_RUNTIME           std::runtime_error  (pair_to_freq contains -1, ...)
+ *   TACO_ERR_OVERFLOW          std::overflow_error (sizes)
+ *   TACO_ERR_CUDA              std::runtime_error raised by cuda_check
+ *
+ * Calls are synchronous (they return after the results are in the output buffers),
+ * use one CUDA stream per host thread and device unless a stream is passed, and keep
+ * a grow-only device workspace per host thread and device, like the reference's
+ * thread-local fused workspace (cpp/src/backend/cuda/tcl4_fused_cuda.cu:676-685).
+ */
+#ifndef TACO_B200_H
+#define TACO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TACO_B200_VERSION "0.1.0"
+
+typedef struct { double re, im; } taco_c128;
+typedef struct { float re, im; } taco_c64;
+
+typedef enum {
+    TACO_OK = 0,
+    TACO_ERR_INVALID_ARGUMENT = 1,
+    TACO_ERR_OUT_OF_RANGE = 2,
+    TACO_ERR_RUNTIME = 3,
+    TACO_ERR_OVERFLOW = 4,
+    TACO_ERR_CUDA = 5,
+    TACO_ERR_TIMEOUT = 6,
+    TACO_ERR_NO_DEVICE = 7
+} taco_status;
+
+/* FCRMethod (cpp/include/taco/tcl4_kernels.hpp:11-14).  The device path implements
+ * Convolution only, like the reference's fused CUDA path
+ * (cpp/src/backend/cuda/tcl4_fused_cuda.cu:1107-1109). */
+enum { TACO_FCR_CONVOLUTION = 0, TACO_FCR_DIRECT = 1 };
+
+/* TACO_PREC_FP64: the plain FP64 path (complex128 results).
+ * TACO_PREC_FP32: FFT convolutions and the L4 contraction in FP32 (complex64 L4),
+ *                 FP64 phases, FP64 prefix-integral carries. */
+enum { TACO_PREC_FP64 = 0, TACO_PREC_FP32 = 1 };
+
+/* flags */
+enum {
+    TACO_IN_DEVICE = 1,          /* gamma (and RK4 inputs) are device pointers */
+    TACO_OUT_DEVICE = 2,         /* outputs are device pointers */
+    TACO_CAUSAL_TRUNCATION = 4   /* FFT length from max(tidx)+1 instead of Nt (same results) */
+};
+
+/* What the device path reads from taco::sys::System (cpp/include/taco/system.hpp:201-226)
+ * and the Tcl4Map (cpp/include/taco/tcl4.hpp:13-26). */
+typedef struct {
+    int N;                       /* system dimension (eig.dim) */
+    int nf;                      /* number of Bohr-frequency buckets */
+    int num_ops;                 /* number of coupling operators */
+    const double* omegas;        /* [nf] bucket frequencies, ascending */
+    const int* mirror;           /* [nf] bucket of -omega (NULL: computed as build_map does) */
+    const int* pair_to_freq;     /* [N*N] column-major bucket index of pair (a, b) */
+    const taco_c128* ops;        /* [num_ops][N*N] column-major coupling operators, eigenbasis */
+    double tol;                  /* bucket tolerance used for the mirror search (<= 0: 1e-9) */
+} taco_system_view;
+
+/* One instance of the batched build. */
+typedef struct {
+    taco_system_view sys;
+    const taco_c128* gamma;      /* [Nt x nf] column-major: gamma[t + Nt*b] */
+    size_t Nt;
+    double dt;
+    const uint32_t* tidx;        /* host array of requested time indices (NULL/T=0: all Nt) */
+    size_t T;
+    void* L4_out;                /* [T][N^2 x N^2]: taco_c128 (FP64) or taco_c64 (FP32) */
+} taco_tcl4_instance;
+
+const char* taco_version(void);
+const char* taco_last_error(void);
+int taco_device_count(int* count);
+int taco_set_device(int gpu_id);
+
+/* set_fcr_fft_pad_factor / get_fcr_fft_pad_factor (cpp/include/taco/tcl4_kernels.hpp:16-19):
+ * Nfft = next_pow2(max(2n-1, factor*n)); 0 keeps the default. */
+void taco_set_fcr_fft_pad_factor(size_t factor);
+size_t taco_get_fcr_fft_pad_factor(void);
+
+/* compute_triple_kernels(system, gamma_series, dt, nmax, method, exec{Cuda})
+ * (cpp/include/taco/tcl4.hpp:37-42, backend cpp/src/backend/cuda/tcl4_kernels_cuda.cu:41-291).
+ * F, C, R: [nf^3][Nt] complex128, series of triple (i,j,k) at index (i*nf + j)*nf + k
+ * (TripleKernelSeries F[i][j][k](t), cpp/include/taco/tcl4.hpp:30-34). */
+int taco_compute_triple_kernels(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
+                                int method, taco_c128* F, taco_c128* C, taco_c128* R, int flags,
+                                void* stream);
+
+/* build_TCL4_generator_cuda_fused_batch(system, gamma_series, dt, time_indices, method, exec,
+ * cuda_fcr_ms) (cpp/include/taco/backend/cuda/tcl4_fused_cuda.hpp:25-41).  tidx == NULL or
+ * T == 0 means all time indices [0, Nt).  L4_out: [T][N^2 x N^2] column-major, complex128
+ * for TACO_PREC_FP64 and complex64 for TACO_PREC_FP32.  fcr_ms (nullable) receives the
+ * device time of the F/C/R stage. */
+int taco_tcl4_build_batch(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
+                          const uint32_t* tidx, size_t T, int method, int precision, void* L4_out,
+                          int flags, void* stream, double* fcr_ms);
+
+/* build_TCL4_generator_cuda_fused(system, gamma_series, dt, time_index, method, exec)
+ * (cpp/include/taco/backend/cuda/tcl4_fused_cuda.hpp:16-21). */
+int taco_tcl4_build(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
+                    size_t time_index, int method, taco_c128* L4_out, int flags, void* stream);
+
+/* build_correction_series_cuda_fused (cpp/include/taco/backend/cuda/tcl4_fused_cuda.hpp:44-48):
+ * L4 at every t in [0, Nt). */
+int taco_tcl4_correction_series(const taco_system_view* sys, const taco_c128* gamma, size_t Nt,
+                                double dt, int method, taco_c128* L4_out, int flags, void* stream);
+
+/* Batching form (no counterpart in the reference): many instances of possibly different
+ * (N, nf, Nt, T) in one call; instances sharing an FFT length share every launch. */
+int taco_tcl4_build_instances(const taco_tcl4_instance* inst, size_t count, int method, int precision,
+                              int flags, void* stream);
+
+/* propagate_rk4_dense_serial/_omp(L_series[, L_half_series], r, t0, dt, on_sample, sample_every)
+ * (cpp/include/taco/rk4_dense.hpp:85-100, 114-129) on the device.
+ * L_series: [steps+1][D x D]; L_half: [steps][D x D] or NULL (midpoints by averaging);
+ * L_add: [steps+1][D x D] or NULL, added to L_series (e.g. L2 + L4);
+ * l_is_fp32: the three series are complex64 instead of complex128;
+ * r: [D] complex128 in/out; samples (nullable): r every sample_every steps plus the final
+ * state, [n][D]; obs (nullable, [D]) and obs_out ([n]): <O> = sum_l obs_l r_l at each sample.
+ * n = ceil(steps / sample_every) + 1.  All pointers follow TACO_IN_DEVICE. */
+int taco_rk4_propagate(const void* L_series, const void* L_half, const void* L_add, int l_is_fp32,
+                       size_t steps, int D, double dt, taco_c128* r, size_t sample_every,
+                       taco_c128* samples, const taco_c128* obs, taco_c128* obs_out, int flags,
+                       void* stream);
+
+/* The time-independent linear map L4_e(t) = sum_k coef_k * v_{src_k}(t) (v conjugated when
+ * bit 31 of src_k is set) of the MIKX -> GW -> L4 chain (cpp/src/tcl/tcl4_mikx.cpp:87-177,
+ * cpp/src/tcl/tcl4_assemble.cpp:53-230).  Sources: F (s < nf^3), C, R of triple s mod nf^3.
+ * rowptr: [N^4 + 1]; src/coef: capacity `cap`; nnz receives the number of terms (when it
+ * exceeds cap only nnz is written). */
+int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t* src, taco_c128* coef,
+                         size_t cap, size_t* nnz);
+
+/* Kernel accounting (tracing).  taco_kernel_launches: kernels this library launched since
+ * the process started.  With profiling on, every launch is bracketed by CUDA events and its
+ * device time is summed per kernel name (CUDA-event stage timing, as the reference's
+ * TACO_CUDA_FCR_PROFILE / TACO_CUDA_GW_PROFILE switches).  taco_profile_get returns entry
+ * `index` (name valid until the next reset) and writes the number of entries to *count. */
+int taco_kernel_launches(uint64_t* launches);
+int taco_profile_enable(int on);
+int taco_profile_reset(void);
+int taco_profile_get(size_t index, const char** name, uint64_t* launches, double* total_ms, size_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

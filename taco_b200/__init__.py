@@ -1,0 +1,324 @@
+"""taco_b200 -- B200-native TCL4 generator engine.
+
+Python mirror of the reference's C++ entry points for the L4(t) path, calling the
+CUDA library through its C-ABI (include/taco_b200.h):
+
+=================================  =====================================================
+this module                        reference (cpp/include/taco/...)
+=================================  =====================================================
+System                             sys::System::build (system.hpp:201-226) + build_map
+compute_triple_kernels             tcl4::compute_triple_kernels (tcl4.hpp:37-42), Exec{Cuda}
+build_TCL4_generator               build_TCL4_generator_cuda_fused (backend/cuda/tcl4_fused_cuda.hpp:16-21)
+build_TCL4_generator_batch         build_TCL4_generator_cuda_fused_batch (tcl4_fused_cuda.hpp:25-41)
+build_correction_series            build_correction_series_cuda_fused (tcl4_fused_cuda.hpp:44-48)
+propagate_rk4_dense                tcl::propagate_rk4_dense_* (rk4_dense.hpp:85-129), on the device
+set_fcr_fft_pad_factor             tcl4::set_fcr_fft_pad_factor (tcl4_kernels.hpp:16-19)
+=================================  =====================================================
+
+Arrays: numpy arrays are host buffers (copied in and out inside the call); torch CUDA
+tensors are device buffers (the call reads and writes them in place).  Gamma is
+[nf, Nt] (row b = bucket b; the reference's column-major Nt x nf matrix).  L4 results
+are returned as [T, N^2, N^2] arrays indexed [t, row, col].  Errors raise the
+exception type the reference throws (ValueError for std::invalid_argument, IndexError
+for std::out_of_range, OverflowError, RuntimeError).  There is no CPU fallback: every
+call needs the CUDA library and a GPU.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import _capi
+from ._capi import (TacoError, TacoInvalidArgument, TacoOutOfRange, TacoOverflow,  # noqa: F401
+                    TACO_PREC_FP32, TACO_PREC_FP64)
+from .inputs import System, bcf_fft, gamma_trapz, spin_boson_system  # noqa: F401
+
+__all__ = [
+    "System", "bcf_fft", "gamma_trapz", "spin_boson_system", "compute_triple_kernels",
+    "build_TCL4_generator", "build_TCL4_generator_batch", "build_correction_series", "build_instances",
+    "propagate_rk4_dense", "l4_coefficients", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
+    "version", "device_count", "kernel_launches", "profile",
+]
+
+
+def version() -> str:
+    return _capi.lib().taco_version().decode()
+
+
+def device_count() -> int:
+    n = ct.c_int(0)
+    _capi.check(_capi.lib().taco_device_count(ct.byref(n)))
+    return n.value
+
+
+def kernel_launches() -> int:
+    """Kernels launched by the library since the process started."""
+    n = ct.c_uint64(0)
+    _capi.check(_capi.lib().taco_kernel_launches(ct.byref(n)))
+    return int(n.value)
+
+
+class profile:
+    """Context manager: per-kernel device time (CUDA events around each launch).
+
+    >>> with taco_b200.profile() as p: ...
+    >>> p.entries  # {name: (launches, total_ms)}
+    """
+
+    def __enter__(self):
+        L = _capi.lib()
+        _capi.check(L.taco_profile_reset())
+        _capi.check(L.taco_profile_enable(1))
+        self.entries = {}
+        return self
+
+    def __exit__(self, *exc):
+        L = _capi.lib()
+        _capi.check(L.taco_profile_enable(0))
+        count = ct.c_size_t(0)
+        _capi.check(L.taco_profile_get(0, None, None, None, ct.byref(count)))
+        for k in range(count.value):
+            name = ct.c_char_p()
+            n = ct.c_uint64(0)
+            ms = ct.c_double(0.0)
+            _capi.check(L.taco_profile_get(k, ct.byref(name), ct.byref(n), ct.byref(ms), None))
+            self.entries[name.value.decode()] = (int(n.value), float(ms.value))
+        return False
+
+
+def set_fcr_fft_pad_factor(factor: int) -> None:
+    _capi.lib().taco_set_fcr_fft_pad_factor(int(factor))
+
+
+def get_fcr_fft_pad_factor() -> int:
+    return int(_capi.lib().taco_get_fcr_fft_pad_factor())
+
+
+# ----------------------------------------------------------------- helpers --
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if _is_torch(x):
+        return ct.c_void_p(x.data_ptr())
+    return x.ctypes.data_as(ct.c_void_p)
+
+
+def _stream_ptr(x):
+    if x is not None and _is_torch(x) and x.is_cuda:
+        return ct.c_void_p(_torch().cuda.current_stream(x.device).cuda_stream)
+    return None
+
+
+def _c128_host(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def _prep_gamma(gamma):
+    """-> (array, on_device).  Device tensors must be contiguous complex128 [nf, Nt]."""
+    if _is_torch(gamma):
+        torch = _torch()
+        if gamma.is_cuda:
+            if gamma.dtype != torch.complex128:
+                gamma = gamma.to(torch.complex128)
+            return gamma.contiguous(), True
+        gamma = gamma.numpy()
+    return _c128_host(gamma), False
+
+
+class _View:
+    """Keeps the numpy buffers of a taco_system_view alive."""
+
+    def __init__(self, system: System):
+        self.omegas = np.ascontiguousarray(system.omegas, np.float64)
+        self.mirror = np.ascontiguousarray(system.mirror, np.int32)
+        self.p2f = np.ascontiguousarray(np.asarray(system.pair_to_freq).T, np.int32)  # column-major
+        ops = system.A_eig
+        self.ops = (np.ascontiguousarray(np.stack([np.asarray(A, np.complex128).T for A in ops]))
+                    if len(ops) else np.zeros((0,), np.complex128))
+        self.view = _capi.SystemView(int(system.N), int(system.nf), len(ops), _ptr(self.omegas).value,
+                                     _ptr(self.mirror).value, _ptr(self.p2f).value,
+                                     _ptr(self.ops).value if len(ops) else None, float(system.tol))
+
+
+def _out_array(like_device, shape, dtype, device=None):
+    if like_device:
+        torch = _torch()
+        td = torch.complex128 if dtype == np.complex128 else torch.complex64
+        return torch.empty(shape, dtype=td, device=device)
+    return np.empty(shape, dtype=dtype)
+
+
+def _l4_view(buf, N2):
+    """[T, N^2*N^2] column-major matrices -> [T, N^2, N^2] indexed [t, row, col]."""
+    T = buf.shape[0]
+    if _is_torch(buf):
+        return buf.view(T, N2, N2).transpose(1, 2)
+    return buf.reshape(T, N2, N2).transpose(0, 2, 1)
+
+
+# --------------------------------------------------------------- entry points --
+def compute_triple_kernels(system: System, gamma, dt: float, nmax: int = 2, method: int = 0):
+    """F, C, R series of every frequency triple: arrays [nf, nf, nf, Nt] (complex128).
+
+    ``nmax`` is accepted and ignored, as in the reference (tcl4.cpp:117).
+    """
+    del nmax
+    g, dev = _prep_gamma(gamma)
+    nf, Nt = g.shape
+    v = _View(system)
+    shape = (nf, nf, nf, Nt)
+    outs = [_out_array(dev, shape, np.complex128, g.device if dev else None) for _ in range(3)]
+    flags = (_capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE) if dev else 0
+    _capi.check(_capi.lib().taco_compute_triple_kernels(ct.byref(v.view), _ptr(g), Nt, float(dt), int(method),
+                                                        _ptr(outs[0]), _ptr(outs[1]), _ptr(outs[2]), flags,
+                                                        _stream_ptr(g)))
+    return tuple(outs)
+
+
+def build_TCL4_generator_batch(system: System, gamma, dt: float, time_indices=None, method: int = 0,
+                               precision: str = "fp64", causal_truncation: bool = False, out=None,
+                               return_fcr_ms: bool = False):
+    """L4 at each requested time index (all of [0, Nt) when ``time_indices`` is None/empty).
+
+    precision "fp64": complex128 (the plain path); "fp32": FP32 FFT convolutions and
+    contraction, FP64 phases and carries, complex64 results.
+    """
+    g, dev = _prep_gamma(gamma)
+    nf, Nt = g.shape
+    prec = {"fp64": _capi.TACO_PREC_FP64, "fp32": _capi.TACO_PREC_FP32}[precision]
+    tid = None if time_indices is None else np.ascontiguousarray(time_indices, dtype=np.uint32)
+    if tid is not None and tid.size == 0:
+        tid = None
+    T = Nt if tid is None else tid.size
+    N2 = int(system.N) ** 2
+    dtype = np.complex128 if prec == _capi.TACO_PREC_FP64 else np.complex64
+    if out is None:
+        out = _out_array(dev, (T, N2 * N2), dtype, g.device if dev else None)
+    flags = (_capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE) if dev else 0
+    if causal_truncation:
+        flags |= _capi.TACO_CAUSAL_TRUNCATION
+    v = _View(system)
+    ms = ct.c_double(0.0)
+    _capi.check(_capi.lib().taco_tcl4_build_batch(ct.byref(v.view), _ptr(g), Nt, float(dt), _ptr(tid),
+                                                  0 if tid is None else tid.size, int(method), prec, _ptr(out),
+                                                  flags, _stream_ptr(g), ct.byref(ms)))
+    res = _l4_view(out, N2)
+    return (res, ms.value) if return_fcr_ms else res
+
+
+def build_TCL4_generator(system: System, gamma, dt: float, time_index: int, method: int = 0):
+    """L4 at one time index: [N^2, N^2] complex128."""
+    g, dev = _prep_gamma(gamma)
+    Nt = g.shape[1]
+    if time_index < 0 or time_index >= Nt:
+        raise TacoOutOfRange(_capi.TACO_ERR_OUT_OF_RANGE, "build_TCL4_generator: time_index out of range")
+    return build_TCL4_generator_batch(system, g, dt, [time_index], method)[0]
+
+
+def build_correction_series(system: System, gamma, dt: float, method: int = 0):
+    return build_TCL4_generator_batch(system, gamma, dt, None, method)
+
+
+def build_instances(instances, precision: str = "fp64", method: int = 0, outs=None):
+    """Batching form: ``instances`` is a list of (system, gamma, dt, tidx); gammas all host
+    (numpy) or all device (torch CUDA).  Returns one [T, N^2, N^2] result per instance."""
+    prec = {"fp64": _capi.TACO_PREC_FP64, "fp32": _capi.TACO_PREC_FP32}[precision]
+    dtype = np.complex128 if prec == _capi.TACO_PREC_FP64 else np.complex64
+    arr = (_capi.Instance * len(instances))()
+    keep = []
+    results = []
+    dev = None
+    for k, (system, gamma, dt, tidx) in enumerate(instances):
+        g, d = _prep_gamma(gamma)
+        if dev is None:
+            dev = d
+        elif dev != d:
+            raise ValueError("build_instances: mix of host and device gamma")
+        nf, Nt = g.shape
+        tid = None if tidx is None or len(tidx) == 0 else np.ascontiguousarray(tidx, np.uint32)
+        T = Nt if tid is None else tid.size
+        N2 = int(system.N) ** 2
+        o = outs[k] if outs is not None else _out_array(d, (T, N2 * N2), dtype, g.device if d else None)
+        v = _View(system)
+        keep += [g, tid, o, v]
+        arr[k].sys = v.view
+        arr[k].gamma = _ptr(g).value
+        arr[k].Nt = Nt
+        arr[k].dt = float(dt)
+        arr[k].tidx = _ptr(tid).value if tid is not None else None
+        arr[k].T = 0 if tid is None else tid.size
+        arr[k].L4_out = _ptr(o).value
+        results.append(_l4_view(o, N2))
+    flags = (_capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE) if dev else 0
+    _capi.check(_capi.lib().taco_tcl4_build_instances(arr, len(instances), int(method), prec, flags,
+                                                      _stream_ptr(keep[0]) if keep else None))
+    return results
+
+
+def propagate_rk4_dense(L_series, r0, dt: float, L_half=None, L_add=None, sample_every: int = 0, obs=None):
+    """RK4 for r' = L(t) r on the device (rk4_dense.cpp:246-321).
+
+    L_series: [steps+1, D, D] (indexed [step, row, col]); L_half: [steps, D, D] or None
+    (midpoints by averaging); L_add: [steps+1, D, D] or None (added to L_series).
+    Returns (r_final, samples or None, obs_values or None); samples every
+    ``sample_every`` steps plus the final state.
+    """
+    dev = _is_torch(L_series) and L_series.is_cuda
+
+    def prep_series(x):
+        if x is None:
+            return None
+        if dev:
+            return x.transpose(-1, -2).contiguous()  # column-major matrices
+        a = np.asarray(x)
+        dtype = np.complex64 if a.dtype == np.complex64 else np.complex128
+        return np.ascontiguousarray(np.swapaxes(a, -1, -2), dtype=dtype)
+
+    Ls = prep_series(L_series)
+    Lh = prep_series(L_half)
+    La = prep_series(L_add)
+    is32 = (str(Ls.dtype).endswith("complex64"))
+    for x in (Lh, La):
+        if x is not None and str(x.dtype).endswith("complex64") != is32:
+            raise ValueError("propagate_rk4_dense: all generator series must share one dtype")
+    steps = Ls.shape[0] - 1
+    D = Ls.shape[-1]
+    if dev:
+        torch = _torch()
+        r = r0.to(torch.complex128).clone().contiguous()
+        o = obs.to(torch.complex128).contiguous() if obs is not None else None
+    else:
+        r = _c128_host(r0).copy()
+        o = _c128_host(obs) if obs is not None else None
+    ns = 0 if sample_every <= 0 else (steps + sample_every - 1) // sample_every + 1
+    samples = _out_array(dev, (ns, D), np.complex128, Ls.device if dev else None) if sample_every > 0 else None
+    obs_out = _out_array(dev, (ns,), np.complex128, Ls.device if dev else None) if (sample_every > 0 and obs is not None) else None
+    flags = _capi.TACO_IN_DEVICE if dev else 0
+    _capi.check(_capi.lib().taco_rk4_propagate(_ptr(Ls), _ptr(Lh), _ptr(La), 1 if is32 else 0, steps, D, float(dt),
+                                               _ptr(r), sample_every if sample_every > 0 else 0, _ptr(samples),
+                                               _ptr(o), _ptr(obs_out), flags, _stream_ptr(Ls) if dev else None))
+    return r, samples, obs_out
+
+
+def l4_coefficients(system: System):
+    """(rowptr [N^4+1], src [nnz], coef [nnz]) of the linear map F/C/R(t) -> L4(t)."""
+    v = _View(system)
+    N4 = int(system.N) ** 4
+    rowptr = np.zeros(N4 + 1, np.int32)
+    nnz = ct.c_size_t(0)
+    _capi.check(_capi.lib().taco_l4_coefficients(ct.byref(v.view), _ptr(rowptr), None, None, 0, ct.byref(nnz)))
+    src = np.zeros(max(1, nnz.value), np.uint32)
+    coef = np.zeros(max(1, nnz.value), np.complex128)
+    _capi.check(_capi.lib().taco_l4_coefficients(ct.byref(v.view), _ptr(rowptr), _ptr(src), _ptr(coef),
+                                                 nnz.value, ct.byref(nnz)))
+    return rowptr, src[: nnz.value], coef[: nnz.value]

@@ -1,0 +1,113 @@
+"""ctypes binding of libtaco_b200.so (the C-ABI declared in include/taco_b200.h)."""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libtaco_b200.so")
+
+TACO_OK = 0
+TACO_ERR_INVALID_ARGUMENT = 1
+TACO_ERR_OUT_OF_RANGE = 2
+TACO_ERR_RUNTIME = 3
+TACO_ERR_OVERFLOW = 4
+TACO_ERR_CUDA = 5
+TACO_ERR_TIMEOUT = 6
+TACO_ERR_NO_DEVICE = 7
+
+TACO_FCR_CONVOLUTION = 0
+TACO_FCR_DIRECT = 1
+TACO_PREC_FP64 = 0
+TACO_PREC_FP32 = 1
+TACO_IN_DEVICE = 1
+TACO_OUT_DEVICE = 2
+TACO_CAUSAL_TRUNCATION = 4
+
+# every symbol the header declares
+EXPORTED = [
+    "taco_version", "taco_last_error", "taco_device_count", "taco_set_device",
+    "taco_set_fcr_fft_pad_factor", "taco_get_fcr_fft_pad_factor", "taco_compute_triple_kernels",
+    "taco_tcl4_build_batch", "taco_tcl4_build", "taco_tcl4_correction_series",
+    "taco_tcl4_build_instances", "taco_rk4_propagate", "taco_l4_coefficients",
+    "taco_kernel_launches", "taco_profile_enable", "taco_profile_reset", "taco_profile_get",
+]
+
+
+class SystemView(ct.Structure):
+    _fields_ = [("N", ct.c_int), ("nf", ct.c_int), ("num_ops", ct.c_int),
+                ("omegas", ct.c_void_p), ("mirror", ct.c_void_p), ("pair_to_freq", ct.c_void_p),
+                ("ops", ct.c_void_p), ("tol", ct.c_double)]
+
+
+class Instance(ct.Structure):
+    _fields_ = [("sys", SystemView), ("gamma", ct.c_void_p), ("Nt", ct.c_size_t), ("dt", ct.c_double),
+                ("tidx", ct.c_void_p), ("T", ct.c_size_t), ("L4_out", ct.c_void_p)]
+
+
+class TacoError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class TacoInvalidArgument(TacoError, ValueError):
+    pass
+
+
+class TacoOutOfRange(TacoError, IndexError):
+    pass
+
+
+class TacoOverflow(TacoError, OverflowError):
+    pass
+
+
+_ERRS = {TACO_ERR_INVALID_ARGUMENT: TacoInvalidArgument, TACO_ERR_OUT_OF_RANGE: TacoOutOfRange,
+         TACO_ERR_OVERFLOW: TacoOverflow}
+
+_lib = None
+
+
+def lib():
+    """Load libtaco_b200.so; raises if it was not built (there is no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m taco_b200.build` (nvcc, sm_100a)")
+        L = ct.CDLL(LIB_PATH)
+        L.taco_version.restype = ct.c_char_p
+        L.taco_last_error.restype = ct.c_char_p
+        L.taco_get_fcr_fft_pad_factor.restype = ct.c_size_t
+        L.taco_set_fcr_fft_pad_factor.argtypes = [ct.c_size_t]
+        L.taco_device_count.argtypes = [ct.POINTER(ct.c_int)]
+        L.taco_set_device.argtypes = [ct.c_int]
+        L.taco_compute_triple_kernels.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t, ct.c_double,
+                                                  ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int,
+                                                  ct.c_void_p]
+        L.taco_tcl4_build_batch.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t, ct.c_double,
+                                            ct.c_void_p, ct.c_size_t, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int,
+                                            ct.c_void_p, ct.POINTER(ct.c_double)]
+        L.taco_tcl4_build.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t, ct.c_double, ct.c_size_t,
+                                      ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.taco_tcl4_correction_series.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t, ct.c_double,
+                                                  ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.taco_tcl4_build_instances.argtypes = [ct.POINTER(Instance), ct.c_size_t, ct.c_int, ct.c_int, ct.c_int,
+                                                ct.c_void_p]
+        L.taco_rk4_propagate.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_size_t, ct.c_int,
+                                         ct.c_double, ct.c_void_p, ct.c_size_t, ct.c_void_p, ct.c_void_p,
+                                         ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.taco_l4_coefficients.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                           ct.c_size_t, ct.POINTER(ct.c_size_t)]
+        L.taco_kernel_launches.argtypes = [ct.POINTER(ct.c_uint64)]
+        L.taco_profile_enable.argtypes = [ct.c_int]
+        L.taco_profile_get.argtypes = [ct.c_size_t, ct.POINTER(ct.c_char_p), ct.POINTER(ct.c_uint64),
+                                       ct.POINTER(ct.c_double), ct.POINTER(ct.c_size_t)]
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != TACO_OK:
+        msg = lib().taco_last_error().decode(errors="replace")
+        raise _ERRS.get(rc, TacoError)(rc, msg)

@@ -1,0 +1,317 @@
+// capi.cpp -- extern "C" entry points of libtaco_b200.so (see include/taco_b200.h).
+#include "taco_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+#include "gw_coef.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<std::size_t> g_pad_factor{0};
+
+template <class Fn>
+int guarded(Fn&& fn) {
+    try {
+        fn();
+        return TACO_OK;
+    } catch (const taco::Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return TACO_ERR_RUNTIME;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return TACO_ERR_RUNTIME;
+    }
+}
+
+void require_device() {
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        throw taco::Error(taco::kNoDevice, std::string("no CUDA device: ") + cudaGetErrorString(e));
+}
+
+taco::SystemDesc to_desc(const taco_system_view* v, bool need_ops = true) {
+    if (!v) throw taco::Error(taco::kInvalidArgument, "system view is null");
+    taco::SystemDesc s;
+    s.N = v->N;
+    s.nf = v->nf;
+    s.num_ops = v->num_ops;
+    if (s.N <= 0) throw taco::Error(taco::kInvalidArgument, "system: N must be > 0");
+    if (s.nf <= 0) throw taco::Error(taco::kInvalidArgument, "system: nf must be > 0");
+    if (!v->omegas || !v->pair_to_freq) throw taco::Error(taco::kInvalidArgument, "system: null metadata");
+    s.omegas.assign(v->omegas, v->omegas + s.nf);
+    s.p2f.assign(v->pair_to_freq, v->pair_to_freq + static_cast<std::size_t>(s.N) * s.N);
+    if (v->mirror) {
+        s.mirror.assign(v->mirror, v->mirror + s.nf);
+    } else {
+        taco::build_mirror(s.omegas, v->tol > 0 ? v->tol : 1e-9, s.mirror, nullptr);
+    }
+    if (need_ops) {
+        if (s.num_ops <= 0) throw taco::Error(taco::kInvalidArgument, "coupling_ops must be non-empty");
+        if (!v->ops) throw taco::Error(taco::kInvalidArgument, "coupling_ops is null");
+        const double2* o = reinterpret_cast<const double2*>(v->ops);
+        s.ops.assign(o, o + static_cast<std::size_t>(s.num_ops) * s.N * s.N);
+    } else if (s.num_ops > 0 && v->ops) {
+        const double2* o = reinterpret_cast<const double2*>(v->ops);
+        s.ops.assign(o, o + static_cast<std::size_t>(s.num_ops) * s.N * s.N);
+    } else {
+        s.num_ops = 0;
+    }
+    return s;
+}
+
+void check_method(int method) {
+    if (method != TACO_FCR_CONVOLUTION)
+        throw taco::Error(taco::kInvalidArgument, "only FCRMethod::Convolution is supported on the device path");
+}
+
+taco::BuildOptions options(int precision, int flags, double* fcr_ms) {
+    if (precision != TACO_PREC_FP64 && precision != TACO_PREC_FP32)
+        throw taco::Error(taco::kInvalidArgument, "precision must be TACO_PREC_FP64 or TACO_PREC_FP32");
+    taco::BuildOptions o;
+    o.fp32 = (precision == TACO_PREC_FP32);
+    o.causal_truncation = (flags & TACO_CAUSAL_TRUNCATION) != 0;
+    o.pad_factor = g_pad_factor.load();
+    o.fcr_ms = fcr_ms;
+    return o;
+}
+
+void fill_tidx(taco::Tcl4Instance& in, const uint32_t* tidx, std::size_t T) {
+    if (tidx == nullptr || T == 0) {
+        in.tidx.resize(in.Nt);
+        for (std::size_t t = 0; t < in.Nt; ++t) in.tidx[t] = static_cast<uint32_t>(t);
+    } else {
+        in.tidx.assign(tidx, tidx + T);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* taco_version(void) { return TACO_B200_VERSION; }
+
+const char* taco_last_error(void) { return g_last_error.c_str(); }
+
+int taco_device_count(int* count) {
+    return guarded([&] {
+        int n = 0;
+        const cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess) n = 0;
+        if (count) *count = n;
+    });
+}
+
+int taco_set_device(int gpu_id) {
+    return guarded([&] {
+        require_device();
+        taco::cuda_check(cudaSetDevice(gpu_id), "cudaSetDevice");
+    });
+}
+
+void taco_set_fcr_fft_pad_factor(size_t factor) { g_pad_factor.store(factor); }
+size_t taco_get_fcr_fft_pad_factor(void) { return g_pad_factor.load(); }
+
+int taco_compute_triple_kernels(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
+                                int method, taco_c128* F, taco_c128* C, taco_c128* R, int flags, void* stream) {
+    return guarded([&] {
+        check_method(method);
+        require_device();
+        taco::SystemDesc s = to_desc(sys, false);
+        taco::BuildOptions o = options(TACO_PREC_FP64, 0, nullptr);
+        taco::triple_kernels(s, reinterpret_cast<const double2*>(gamma), (flags & TACO_IN_DEVICE) != 0, Nt, dt,
+                             reinterpret_cast<double2*>(F), reinterpret_cast<double2*>(C),
+                             reinterpret_cast<double2*>(R), (flags & TACO_OUT_DEVICE) != 0, o,
+                             static_cast<cudaStream_t>(stream));
+    });
+}
+
+int taco_tcl4_build_batch(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
+                          const uint32_t* tidx, size_t T, int method, int precision, void* L4_out, int flags,
+                          void* stream, double* fcr_ms) {
+    return guarded([&] {
+        check_method(method);
+        require_device();
+        std::vector<taco::Tcl4Instance> insts(1);
+        taco::Tcl4Instance& in = insts[0];
+        in.sys = to_desc(sys);
+        in.gamma = reinterpret_cast<const double2*>(gamma);
+        in.gamma_on_device = (flags & TACO_IN_DEVICE) != 0;
+        in.Nt = Nt;
+        in.dt = dt;
+        if (Nt == 0) throw taco::Error(taco::kInvalidArgument, "empty gamma_series");
+        fill_tidx(in, tidx, T);
+        in.out = L4_out;
+        in.out_on_device = (flags & TACO_OUT_DEVICE) != 0;
+        taco::tcl4_build(insts, options(precision, flags, fcr_ms), static_cast<cudaStream_t>(stream));
+    });
+}
+
+int taco_tcl4_build(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt, size_t time_index,
+                    int method, taco_c128* L4_out, int flags, void* stream) {
+    if (time_index >= Nt) {
+        g_last_error = "build_TCL4_generator: time_index out of range";
+        return TACO_ERR_OUT_OF_RANGE;
+    }
+    const uint32_t t = static_cast<uint32_t>(time_index);
+    return taco_tcl4_build_batch(sys, gamma, Nt, dt, &t, 1, method, TACO_PREC_FP64, L4_out, flags, stream, nullptr);
+}
+
+int taco_tcl4_correction_series(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
+                                int method, taco_c128* L4_out, int flags, void* stream) {
+    return taco_tcl4_build_batch(sys, gamma, Nt, dt, nullptr, 0, method, TACO_PREC_FP64, L4_out, flags, stream,
+                                 nullptr);
+}
+
+int taco_tcl4_build_instances(const taco_tcl4_instance* inst, size_t count, int method, int precision, int flags,
+                              void* stream) {
+    return guarded([&] {
+        check_method(method);
+        require_device();
+        if (count > 0 && !inst) throw taco::Error(taco::kInvalidArgument, "instances is null");
+        std::vector<taco::Tcl4Instance> insts(count);
+        for (std::size_t k = 0; k < count; ++k) {
+            taco::Tcl4Instance& in = insts[k];
+            in.sys = to_desc(&inst[k].sys);
+            in.gamma = reinterpret_cast<const double2*>(inst[k].gamma);
+            in.gamma_on_device = (flags & TACO_IN_DEVICE) != 0;
+            in.Nt = inst[k].Nt;
+            in.dt = inst[k].dt;
+            if (in.Nt == 0) throw taco::Error(taco::kInvalidArgument, "empty gamma_series");
+            fill_tidx(in, inst[k].tidx, inst[k].T);
+            in.out = inst[k].L4_out;
+            in.out_on_device = (flags & TACO_OUT_DEVICE) != 0;
+        }
+        taco::tcl4_build(insts, options(precision, flags, nullptr), static_cast<cudaStream_t>(stream));
+    });
+}
+
+int taco_rk4_propagate(const void* L_series, const void* L_half, const void* L_add, int l_is_fp32, size_t steps,
+                       int D, double dt, taco_c128* r, size_t sample_every, taco_c128* samples,
+                       const taco_c128* obs, taco_c128* obs_out, int flags, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (D <= 0) throw taco::Error(taco::kInvalidArgument, "rk4: dimension must be > 0");
+        if (!(dt > 0.0)) throw taco::Error(taco::kInvalidArgument, "propagate_rk4_dense: dt must be > 0");
+        if (steps < 1)
+            throw taco::Error(taco::kInvalidArgument,
+                              "propagate_rk4_dense: L_series must have at least 2 matrices (endpoints)");
+        if ((samples || obs_out) && sample_every == 0)
+            throw taco::Error(taco::kInvalidArgument, "propagate_rk4_dense: sample_every must be > 0");
+        if (!L_series || !r) throw taco::Error(taco::kInvalidArgument, "rk4: null pointer");
+        const bool dev = (flags & TACO_IN_DEVICE) != 0;
+        const std::size_t esz = l_is_fp32 ? sizeof(float2) : sizeof(double2);
+        const std::size_t DD = static_cast<std::size_t>(D) * D;
+        const std::size_t ns = taco::rk4_num_samples(steps, sample_every);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        taco::Rk4Request q;
+        q.fp32_storage = l_is_fp32 != 0;
+        q.steps = steps;
+        q.D = D;
+        q.dt = dt;
+        q.sample_every = (samples || obs_out) ? sample_every : 0;
+        if (dev) {
+            q.L = L_series;
+            q.L_half = L_half;
+            q.L_add = L_add;
+            q.r = reinterpret_cast<double2*>(r);
+            q.samples = reinterpret_cast<double2*>(samples);
+            q.obs = reinterpret_cast<const double2*>(obs);
+            q.obs_out = reinterpret_cast<double2*>(obs_out);
+            taco::rk4_propagate_device({q}, st);
+            return;
+        }
+        // host buffers: stage through device memory owned by this call
+        std::vector<void*> allocs;
+        auto dalloc = [&](std::size_t bytes) {
+            void* p = nullptr;
+            taco::cuda_check(cudaMalloc(&p, bytes), "cudaMalloc(rk4)");
+            allocs.push_back(p);
+            return p;
+        };
+        try {
+            auto up = [&](const void* h, std::size_t bytes) -> void* {
+                if (!h) return nullptr;
+                void* d = dalloc(bytes);
+                taco::cuda_check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(rk4 in)");
+                return d;
+            };
+            q.L = up(L_series, (steps + 1) * DD * esz);
+            q.L_half = up(L_half, steps * DD * esz);
+            q.L_add = up(L_add, (steps + 1) * DD * esz);
+            q.r = static_cast<double2*>(up(r, D * sizeof(double2)));
+            q.obs = static_cast<const double2*>(up(obs, D * sizeof(double2)));
+            if (samples) q.samples = static_cast<double2*>(dalloc(ns * D * sizeof(double2)));
+            if (obs_out) q.obs_out = static_cast<double2*>(dalloc(ns * sizeof(double2)));
+            taco::rk4_propagate_device({q}, st);
+            taco::cuda_check(cudaMemcpyAsync(r, q.r, D * sizeof(double2), cudaMemcpyDeviceToHost, st), "rk4 out");
+            if (samples)
+                taco::cuda_check(cudaMemcpyAsync(samples, q.samples, ns * D * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                                 "rk4 samples");
+            if (obs_out)
+                taco::cuda_check(cudaMemcpyAsync(obs_out, q.obs_out, ns * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                                 "rk4 obs");
+            taco::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(rk4)");
+        } catch (...) {
+            cudaStreamSynchronize(st);
+            for (void* p : allocs) cudaFree(p);
+            throw;
+        }
+        for (void* p : allocs) cudaFree(p);
+    });
+}
+
+int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t* src, taco_c128* coef, size_t cap,
+                         size_t* nnz) {
+    return guarded([&] {
+        taco::SystemDesc s = to_desc(sys);
+        for (int v : s.p2f)
+            if (v < 0 || v >= s.nf) throw taco::Error(taco::kRuntime, "pair_to_freq contains -1 or an invalid bucket");
+        taco::CoefTable t;
+        taco::build_coef_table(s.N, s.nf, s.p2f.data(), s.ops.data(), s.num_ops, t);
+        if (nnz) *nnz = t.src.size();
+        if (rowptr) std::memcpy(rowptr, t.rowptr.data(), t.rowptr.size() * sizeof(int32_t));
+        if (t.src.size() <= cap) {
+            if (src) std::memcpy(src, t.src.data(), t.src.size() * sizeof(uint32_t));
+            if (coef) std::memcpy(coef, t.coef.data(), t.coef.size() * sizeof(taco_c128));
+        }
+    });
+}
+
+int taco_kernel_launches(uint64_t* launches) {
+    return guarded([&] {
+        if (launches) *launches = taco::kernel_launches();
+    });
+}
+
+int taco_profile_enable(int on) {
+    return guarded([&] { taco::profile_enable(on != 0); });
+}
+
+int taco_profile_reset(void) {
+    return guarded([&] { taco::profile_reset(); });
+}
+
+int taco_profile_get(size_t index, const char** name, uint64_t* launches, double* total_ms, size_t* count) {
+    return guarded([&] {
+        const auto e = taco::profile_entries();
+        if (count) *count = e.size();
+        if (index < e.size()) {
+            if (name) *name = e[index].name;
+            if (launches) *launches = e[index].launches;
+            if (total_ms) *total_ms = e[index].total_ms;
+        }
+    });
+}
+
+}  // extern "C"

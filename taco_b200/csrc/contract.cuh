@@ -1,0 +1,58 @@
+// contract.cuh -- fused MIKX -> GW -> (T + T^H) -> L4 contraction for all requested times.
+//
+// Each L4 entry e is a sparse linear form in the F/C/R values at one time (see
+// gw_coef.hpp).  A CTA takes a tile of OT output times; thread (e, o) walks the CSR
+// row of e, gathers v_s at the time of output o (source-major layout v[s][u]: lanes
+// with consecutive outputs read consecutive addresses) and accumulates in the working
+// type.  Results are staged in shared memory and written as whole L4 matrices
+// (column-major, output-major: out[o][e]).
+#pragma once
+
+#include "common.cuh"
+
+namespace taco {
+
+struct ContractJob {
+    const int32_t* rowptr;  // [E + 1]
+    const uint32_t* src;    // [nnz] source | conj << 31
+    const void* coef;       // [nnz] working complex type
+    const void* v;          // [3 nf^3][U] working complex type
+    const uint32_t* out_u;  // [T] unique-time position of each output
+    void* out;              // [T][E] working complex type
+    uint32_t T, U, E;
+};
+
+template <class R>
+__global__ void k_contract(const ContractJob* __restrict__ jobs, int OT) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* res = reinterpret_cast<C*>(smem_raw);  // [OT][E]
+    const ContractJob job = jobs[blockIdx.y];
+    const uint32_t o0 = blockIdx.x * OT;
+    if (o0 >= job.T) return;
+    const uint32_t ot = min(static_cast<uint32_t>(OT), job.T - o0);
+    const C* coef = static_cast<const C*>(job.coef);
+    const C* v = static_cast<const C*>(job.v);
+    const uint32_t work = job.E * OT;
+    for (uint32_t idx = threadIdx.x; idx < work; idx += blockDim.x) {
+        const uint32_t ol = idx % OT, e = idx / OT;
+        if (ol >= ot) continue;
+        const uint32_t u = __ldg(&job.out_u[o0 + ol]);
+        C acc = C{0, 0};
+        const int32_t b = __ldg(&job.rowptr[e]), end = __ldg(&job.rowptr[e + 1]);
+        for (int32_t k = b; k < end; ++k) {
+            const uint32_t sk = __ldg(&job.src[k]);
+            const C w = coef[k];
+            C x = v[static_cast<size_t>(sk & 0x7fffffffu) * job.U + u];
+            if (sk & 0x80000000u) x.y = -x.y;
+            acc = cadd(acc, cmul(w, x));
+        }
+        res[ol * job.E + e] = acc;
+    }
+    __syncthreads();
+    C* out = static_cast<C*>(job.out) + static_cast<size_t>(o0) * job.E;
+    const uint32_t total = ot * job.E;
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) out[idx] = res[idx];
+}
+
+}  // namespace taco

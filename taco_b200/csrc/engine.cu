@@ -1,0 +1,860 @@
+// engine.cu -- host orchestration of the TCL4 device path.
+//
+// Per call: validate, derive per-instance metadata (requested-time maps, FFT length,
+// merged GW coefficient table), group instances with equal FFT length, and run
+//   spectra (2 nf per instance) -> per-triple B1/B2/B3 chain in chunks -> scans and
+//   F/C/R assembly -> fused MIKX/GW/L4 contraction,
+// all on one stream.  Device memory comes from a per-thread, per-device arena that
+// grows on demand and is reused across calls (like the reference's thread-local fused
+// workspace, cpp/src/backend/cuda/tcl4_fused_cuda.cu:676-685).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <mutex>
+#include <string>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <unordered_map>
+
+#include "contract.cuh"
+#include "fcr_kernels.cuh"
+#include "gw_coef.hpp"
+#include "rk4.cuh"
+
+namespace taco {
+
+namespace {
+
+std::atomic<uint64_t> g_launches{0};
+std::atomic<bool> g_profile{false};
+
+constexpr int kColTile = 4096;  // elements per column-pass tile
+constexpr int kRowTile = 2048;  // elements per row-pass tile (two tiles in shared memory)
+
+std::size_t align_up(std::size_t x, std::size_t a) { return (x + a - 1) / a * a; }
+
+struct DeviceBuffer {
+    void* p = nullptr;
+    std::size_t cap = 0;
+    void ensure(std::size_t bytes) {
+        if (bytes <= cap) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const std::size_t want = align_up(bytes + bytes / 8, std::size_t(1) << 20);
+        cuda_check(cudaMalloc(&p, want), "cudaMalloc(workspace)");
+        cap = want;
+    }
+    ~DeviceBuffer() {
+        if (p) cudaFree(p);
+    }
+};
+
+struct PinnedBuffer {
+    void* p = nullptr;
+    std::size_t cap = 0;
+    void ensure(std::size_t bytes) {
+        if (bytes <= cap) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const std::size_t want = align_up(bytes + bytes / 8, std::size_t(1) << 16);
+        cuda_check(cudaMallocHost(&p, want), "cudaMallocHost(staging)");
+        cap = want;
+    }
+    ~PinnedBuffer() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+// Bump layout over one buffer: first a measuring pass (base == nullptr), then the real one.
+struct Layout {
+    char* base = nullptr;
+    std::size_t off = 0;
+    template <class T>
+    T* take(std::size_t count) {
+        off = align_up(off, 256);
+        T* r = reinterpret_cast<T*>(base ? base + off : nullptr);
+        off += count * sizeof(T);
+        return r;
+    }
+};
+
+struct PlanTables {
+    DeviceBuffer buf;
+    int L = 0, L1 = 0, L2 = 0, s = 0;
+};
+
+struct Workspace {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer arena;
+    PinnedBuffer staging;
+    std::map<std::pair<int, int>, std::unique_ptr<PlanTables>> plans;  // (L, fp32)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~Workspace() {
+        plans.clear();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+Workspace& workspace() {
+    thread_local std::unordered_map<int, std::unique_ptr<Workspace>> tl;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    auto& w = tl[dev];
+    if (!w) {
+        w = std::make_unique<Workspace>();
+        w->device = dev;
+        cuda_check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreate(&w->ev0), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&w->ev1), "cudaEventCreate");
+    }
+    return *w;
+}
+
+template <class C>
+__global__ void k_fill_twiddle(C* out, uint32_t count, double denom) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= count) return;
+    double s, c;
+    sincospi(-2.0 * static_cast<double>(m) / denom, &s, &c);
+    out[m] = from_d2<C>(make_double2(c, s));
+}
+
+template <class R>
+FftPlan<cplx_t<R>> get_plan(Workspace& ws, int L, cudaStream_t st) {
+    using C = cplx_t<R>;
+    const bool fp32 = std::is_same<R, float>::value;
+    auto& slot = ws.plans[{L, fp32 ? 1 : 0}];
+    if (!slot) {
+        auto pt = std::make_unique<PlanTables>();
+        pt->L = L;
+        pt->L2 = (L + 1) / 2;
+        pt->L1 = L - pt->L2;
+        pt->s = (L + 1) / 2;
+        const std::size_t N = std::size_t(1) << L, N1 = std::size_t(1) << pt->L1, N2 = std::size_t(1) << pt->L2;
+        const std::size_t nc = N >> pt->s, nfine = std::size_t(1) << pt->s;
+        pt->buf.ensure((N1 + N2 + nc + nfine) * sizeof(C) + 4 * 256);
+        Layout lay{static_cast<char*>(pt->buf.p)};
+        C* tw1 = lay.take<C>(N1);
+        C* tw2 = lay.take<C>(N2);
+        C* twc = lay.take<C>(nc);
+        C* twf = lay.take<C>(nfine);
+        auto fill = [&](C* p, std::size_t count, double denom) {
+            k_fill_twiddle<C><<<static_cast<unsigned>((count + 255) / 256), 256, 0, st>>>(p, static_cast<uint32_t>(count), denom);
+            cuda_check(cudaGetLastError(), "k_fill_twiddle");
+            g_launches.fetch_add(1);
+        };
+        fill(tw1, N1, static_cast<double>(N1));
+        fill(tw2, N2, static_cast<double>(N2));
+        fill(twc, nc, static_cast<double>(nc));
+        fill(twf, nfine, static_cast<double>(N));
+        slot = std::move(pt);
+    }
+    const PlanTables& pt = *slot;
+    const std::size_t N = std::size_t(1) << L, N1 = std::size_t(1) << pt.L1, N2 = std::size_t(1) << pt.L2;
+    Layout lay{static_cast<char*>(pt.buf.p)};
+    FftPlan<C> p;
+    p.L = L;
+    p.L1 = pt.L1;
+    p.L2 = pt.L2;
+    p.s = pt.s;
+    p.tw1 = lay.take<C>(N1);
+    p.tw2 = lay.take<C>(N2);
+    p.twc = lay.take<C>(N >> pt.s);
+    p.twf = lay.take<C>(std::size_t(1) << pt.s);
+    return p;
+}
+
+template <class K>
+void set_smem(K kernel, std::size_t bytes) {
+    if (bytes > 48 * 1024)
+        cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
+                   "cudaFuncSetAttribute(smem)");
+}
+
+struct Geometry {
+    int col_cols, col_threads, row_rows, row_threads;
+    std::size_t col_smem, row_smem;
+    unsigned col_grid, row_grid;
+};
+
+template <class C>
+Geometry geometry(const FftPlan<C>& p) {
+    Geometry g;
+    const int N1 = 1 << p.L1, N2 = 1 << p.L2;
+    g.col_cols = std::max(1, std::min(N2, kColTile / N1));
+    g.col_threads = N1 * g.col_cols / 8;
+    g.col_smem = static_cast<std::size_t>(N1) * g.col_cols * sizeof(C);
+    g.col_grid = static_cast<unsigned>(N2 / g.col_cols);
+    g.row_rows = std::max(1, std::min(N1, kRowTile / N2));
+    g.row_threads = N2 * g.row_rows / 8;
+    g.row_smem = 2 * static_cast<std::size_t>(N2) * g.row_rows * sizeof(C);
+    g.row_grid = static_cast<unsigned>(N1 / g.row_rows);
+    return g;
+}
+
+struct ProfStore {
+    std::mutex mu;
+    std::map<std::string, std::pair<uint64_t, double>> acc;
+    std::vector<std::string> order;
+};
+ProfStore& prof_store() {
+    static ProfStore s;
+    return s;
+}
+
+// Event pairs recorded around launches of one call; resolved after the final sync.
+struct ProfRecorder {
+    struct Rec {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    cudaStream_t st = nullptr;
+    const char* pending = nullptr;
+    cudaEvent_t pend_a = nullptr;
+    void before(const char* name) {
+        if (!g_profile.load()) return;
+        cuda_check(cudaEventCreate(&pend_a), "cudaEventCreate(prof)");
+        cuda_check(cudaEventRecord(pend_a, st), "cudaEventRecord(prof)");
+        pending = name;
+    }
+    void after() {
+        if (!pending) return;
+        cudaEvent_t b;
+        cuda_check(cudaEventCreate(&b), "cudaEventCreate(prof)");
+        cuda_check(cudaEventRecord(b, st), "cudaEventRecord(prof)");
+        recs.push_back({pending, pend_a, b});
+        pending = nullptr;
+    }
+    void resolve() {
+        if (recs.empty()) return;
+        ProfStore& ps = prof_store();
+        std::lock_guard<std::mutex> lk(ps.mu);
+        for (auto& r : recs) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            auto it = ps.acc.find(r.name);
+            if (it == ps.acc.end()) {
+                ps.order.push_back(r.name);
+                it = ps.acc.emplace(r.name, std::make_pair(uint64_t(0), 0.0)).first;
+            }
+            it->second.first += 1;
+            it->second.second += ms;
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        recs.clear();
+    }
+    ~ProfRecorder() {
+        for (auto& r : recs) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+    }
+};
+
+void check_launch(const char* what, ProfRecorder* pr = nullptr) {
+    cuda_check(cudaGetLastError(), what);
+    g_launches.fetch_add(1);
+    if (pr) pr->after();
+}
+
+// --------------------------------------------------------------- metadata --
+struct InstMeta {
+    std::size_t T = 0, U = 0, t_count = 0, n_in = 0;
+    int L = 0;
+    std::vector<int> tmap;          // [t_count]
+    std::vector<uint32_t> out_u;    // [T]
+    CoefTable coef;
+};
+
+void derive_meta(const Tcl4Instance& in, const BuildOptions& opt, InstMeta& m, bool want_coef) {
+    m.T = in.tidx.size();
+    uint32_t tmax = 0;
+    for (uint32_t t : in.tidx) tmax = std::max(tmax, t);
+    m.t_count = static_cast<std::size_t>(tmax) + 1;
+    std::vector<uint32_t> uniq(in.tidx);
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    m.U = uniq.size();
+    m.tmap.assign(m.t_count, -1);
+    for (std::size_t u = 0; u < uniq.size(); ++u) m.tmap[uniq[u]] = static_cast<int>(u);
+    m.out_u.resize(m.T);
+    for (std::size_t o = 0; o < m.T; ++o) m.out_u[o] = static_cast<uint32_t>(m.tmap[in.tidx[o]]);
+    m.n_in = opt.causal_truncation ? m.t_count : in.Nt;
+    std::size_t target = 2 * m.n_in - 1;
+    if (opt.pad_factor > 0) target = std::max(target, opt.pad_factor * m.n_in);
+    std::size_t nfft = std::max<std::size_t>(8, next_pow2(target));
+    if (nfft > (std::size_t(1) << 22)) throw Error(kOverflow, "FFT length above 2^22 is not supported");
+    m.L = ilog2(nfft);
+    if (want_coef)
+        build_coef_table(in.sys.N, in.sys.nf, in.sys.p2f.data(), in.sys.ops.data(), in.sys.num_ops, m.coef);
+}
+
+struct TripleRef {
+    int inst;
+    int tri;  // (i*nf + j)*nf + k
+};
+
+// Core of one group (equal FFT length).  `fcr_only` writes F/C/R series (FP64) straight
+// into caller buffers instead of running the contraction.
+template <class R>
+void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas, const BuildOptions& opt,
+               cudaStream_t st, Workspace& ws, double2* const* fcr_out, bool fcr_out_dev) {
+    using C = cplx_t<R>;
+    const int L = metas[0]->L;
+    const FftPlan<C> plan = get_plan<R>(ws, L, st);
+    const Geometry g = geometry(plan);
+    const std::size_t Nfft = std::size_t(1) << L;
+    const std::size_t ni = insts.size();
+    const bool fcr_only = (fcr_out != nullptr);
+
+    // triples running the FFT chain / scans (all nf^3 of every instance)
+    std::vector<TripleRef> tris;
+    for (std::size_t a = 0; a < ni; ++a) {
+        const int nf3 = insts[a]->sys.nf * insts[a]->sys.nf * insts[a]->sys.nf;
+        for (int t = 0; t < nf3; ++t) tris.push_back({static_cast<int>(a), t});
+    }
+    const std::size_t ntri = tris.size();
+    const std::size_t per_tri_scratch = 2 * Nfft * sizeof(C);
+    std::size_t Q = std::max<std::size_t>(1, opt.scratch_budget / per_tri_scratch);
+    Q = std::min<std::size_t>({Q, ntri, 65535});
+    const std::size_t nchunks = (ntri + Q - 1) / Q;
+
+    // ---- device layout ----
+    struct Ptrs {
+        std::vector<const double2*> gamma;
+        std::vector<C*> spec;
+        std::vector<C*> conv;     // per instance: [nf^3][2][t_count]
+        std::vector<C*> v;        // per instance: [3 nf^3][U]
+        std::vector<int*> tmap;
+        std::vector<uint32_t*> out_u;
+        std::vector<int32_t*> rowptr;
+        std::vector<uint32_t*> src;
+        std::vector<C*> coef;
+        std::vector<C*> out;
+        C* scratch = nullptr;
+        ColJob* colj = nullptr;
+        RowJob* rowj = nullptr;
+        InvJob* invj = nullptr;
+        ScanJob* scanj = nullptr;
+        ContractJob* conj = nullptr;
+    } P;
+    const std::size_t n_spec_jobs = [&] {
+        std::size_t s = 0;
+        for (auto* in : insts) s += 2 * in->sys.nf;
+        return s;
+    }();
+    const std::size_t n_col_jobs = n_spec_jobs + ntri;
+    const std::size_t n_row_jobs = n_spec_jobs + ntri;
+    auto layout = [&](Layout& lay) {
+        P.gamma.assign(ni, nullptr);
+        P.spec.assign(ni, nullptr);
+        P.conv.assign(ni, nullptr);
+        P.v.assign(ni, nullptr);
+        P.tmap.assign(ni, nullptr);
+        P.out_u.assign(ni, nullptr);
+        P.rowptr.assign(ni, nullptr);
+        P.src.assign(ni, nullptr);
+        P.coef.assign(ni, nullptr);
+        P.out.assign(ni, nullptr);
+        for (std::size_t a = 0; a < ni; ++a) {
+            const Tcl4Instance& in = *insts[a];
+            const InstMeta& m = *metas[a];
+            const std::size_t nf = in.sys.nf, nf3 = nf * nf * nf;
+            if (!in.gamma_on_device) P.gamma[a] = lay.take<double2>(nf * in.Nt);
+            P.spec[a] = lay.take<C>(2 * nf * Nfft);
+            P.conv[a] = lay.take<C>(nf3 * 2 * m.t_count);
+            P.tmap[a] = lay.take<int>(m.t_count);
+            if (!fcr_only) {
+                P.v[a] = lay.take<C>(3 * nf3 * m.U);
+                P.out_u[a] = lay.take<uint32_t>(m.T);
+                P.rowptr[a] = lay.take<int32_t>(m.coef.rowptr.size());
+                P.src[a] = lay.take<uint32_t>(std::max<std::size_t>(1, m.coef.src.size()));
+                P.coef[a] = lay.take<C>(std::max<std::size_t>(1, m.coef.coef.size()));
+                if (!in.out_on_device) {
+                    const std::size_t E = static_cast<std::size_t>(in.sys.N) * in.sys.N * in.sys.N * in.sys.N;
+                    P.out[a] = lay.take<C>(m.T * E);
+                }
+            } else if (!fcr_out_dev) {
+                P.v[a] = lay.take<C>(3 * nf3 * m.U);
+            }
+        }
+        P.scratch = lay.take<C>(Q * 2 * Nfft);
+        P.colj = lay.take<ColJob>(n_col_jobs);
+        P.rowj = lay.take<RowJob>(n_row_jobs);
+        P.invj = lay.take<InvJob>(2 * ntri);
+        P.scanj = lay.take<ScanJob>(ntri);
+        P.conj = lay.take<ContractJob>(ni);
+    };
+    Layout meas;
+    layout(meas);
+    ws.arena.ensure(meas.off);
+    Layout lay{static_cast<char*>(ws.arena.p)};
+    layout(lay);
+    for (std::size_t a = 0; a < ni; ++a)
+        if (insts[a]->gamma_on_device) P.gamma[a] = insts[a]->gamma;
+
+    // ---- host staging of small metadata (one pinned buffer, one copy per array) ----
+    std::vector<ColJob> colj(n_col_jobs);
+    std::vector<RowJob> rowj(n_row_jobs);
+    std::vector<InvJob> invj(2 * ntri);
+    std::vector<ScanJob> scanj(ntri);
+    std::vector<ContractJob> conj(ni);
+    std::size_t cj = 0;
+    for (std::size_t a = 0; a < ni; ++a) {
+        const Tcl4Instance& in = *insts[a];
+        const InstMeta& m = *metas[a];
+        const int nf = in.sys.nf;
+        for (int half = 0; half < 2; ++half)
+            for (int b = 0; b < nf; ++b) {
+                ColJob& c = colj[cj];
+                c.g = P.gamma[a] + static_cast<std::size_t>(b) * in.Nt;
+                c.omega = 0.0;
+                c.dt = in.dt;
+                c.has_phase = 0;
+                c.conj = half;
+                c.n_in = static_cast<uint32_t>(m.n_in);
+                c.out = P.spec[a] + (static_cast<std::size_t>(half) * nf + b) * Nfft;
+                rowj[cj] = RowJob{c.out, nullptr, nullptr, nullptr};
+                ++cj;
+            }
+    }
+    for (std::size_t q = 0; q < ntri; ++q) {
+        const int a = tris[q].inst, tri = tris[q].tri;
+        const Tcl4Instance& in = *insts[a];
+        const InstMeta& m = *metas[a];
+        const int nf = in.sys.nf;
+        const int i = tri / (nf * nf), j = (tri / nf) % nf, k = tri % nf;
+        const int jm = in.sys.mirror[j] >= 0 ? in.sys.mirror[j] : j;
+        const double w = in.sys.omegas[i] + in.sys.omegas[j] + in.sys.omegas[k];
+        const std::size_t slot = q % Q;
+        C* z = P.scratch + slot * 2 * Nfft;
+        C* wcb = z + Nfft;
+        ColJob& c = colj[n_spec_jobs + q];
+        c.g = P.gamma[a] + static_cast<std::size_t>(i) * in.Nt;
+        c.omega = w;
+        c.dt = in.dt;
+        c.has_phase = 1;
+        c.conj = 0;
+        c.n_in = static_cast<uint32_t>(m.n_in);
+        c.out = z;
+        rowj[n_spec_jobs + q] = RowJob{z, wcb, P.spec[a] + static_cast<std::size_t>(jm) * Nfft,
+                                       P.spec[a] + static_cast<std::size_t>(nf + j) * Nfft};
+        C* cf = P.conv[a] + static_cast<std::size_t>(tri) * 2 * m.t_count;
+        C* cc = cf + m.t_count;
+        const double scale = in.dt / static_cast<double>(Nfft);
+        invj[2 * q] = InvJob{z, cf, static_cast<uint32_t>(m.t_count), scale};
+        invj[2 * q + 1] = InvJob{wcb, cc, static_cast<uint32_t>(m.t_count), scale};
+        ScanJob& s = scanj[q];
+        s.gi = P.gamma[a] + static_cast<std::size_t>(i) * in.Nt;
+        s.gj = P.gamma[a] + static_cast<std::size_t>(j) * in.Nt;
+        s.gmj = P.gamma[a] + static_cast<std::size_t>(jm) * in.Nt;
+        s.omega = w;
+        s.dt = in.dt;
+        s.t_count = static_cast<uint32_t>(m.t_count);
+        s.conv_f = cf;
+        s.conv_c = cc;
+        s.tmap = P.tmap[a];
+        const std::size_t nf3 = static_cast<std::size_t>(nf) * nf * nf;
+        if (fcr_only && fcr_out_dev) {
+            s.vf = fcr_out[0] + static_cast<std::size_t>(tri) * m.U;
+            s.vc = fcr_out[1] + static_cast<std::size_t>(tri) * m.U;
+            s.vr = fcr_out[2] + static_cast<std::size_t>(tri) * m.U;
+        } else {
+            s.vf = P.v[a] + static_cast<std::size_t>(tri) * m.U;
+            s.vc = P.v[a] + (nf3 + tri) * m.U;
+            s.vr = P.v[a] + (2 * nf3 + tri) * m.U;
+        }
+    }
+    if (!fcr_only) {
+        for (std::size_t a = 0; a < ni; ++a) {
+            const Tcl4Instance& in = *insts[a];
+            const InstMeta& m = *metas[a];
+            ContractJob& c = conj[a];
+            c.rowptr = P.rowptr[a];
+            c.src = P.src[a];
+            c.coef = P.coef[a];
+            c.v = P.v[a];
+            c.out_u = P.out_u[a];
+            c.out = in.out_on_device ? in.out : P.out[a];
+            c.T = static_cast<uint32_t>(m.T);
+            c.U = static_cast<uint32_t>(m.U);
+            c.E = static_cast<uint32_t>(in.sys.N * in.sys.N * in.sys.N * in.sys.N);
+        }
+    }
+    // pack everything small into the pinned staging buffer
+    struct Copy {
+        void* dst;
+        std::size_t off, bytes;
+    };
+    std::vector<Copy> copies;
+    std::size_t soff = 0;
+    auto stage_size = [&](std::size_t bytes) {
+        soff = align_up(soff, 64);
+        const std::size_t o = soff;
+        soff += bytes;
+        return o;
+    };
+    auto plan_copy = [&](void* dst, std::size_t bytes) {
+        if (bytes) copies.push_back({dst, stage_size(bytes), bytes});
+    };
+    plan_copy(P.colj, colj.size() * sizeof(ColJob));
+    plan_copy(P.rowj, rowj.size() * sizeof(RowJob));
+    plan_copy(P.invj, invj.size() * sizeof(InvJob));
+    plan_copy(P.scanj, scanj.size() * sizeof(ScanJob));
+    if (!fcr_only) plan_copy(P.conj, conj.size() * sizeof(ContractJob));
+    for (std::size_t a = 0; a < ni; ++a) {
+        const InstMeta& m = *metas[a];
+        plan_copy(P.tmap[a], m.tmap.size() * sizeof(int));
+        if (!fcr_only) {
+            plan_copy(P.out_u[a], m.out_u.size() * sizeof(uint32_t));
+            plan_copy(P.rowptr[a], m.coef.rowptr.size() * sizeof(int32_t));
+            plan_copy(P.src[a], m.coef.src.size() * sizeof(uint32_t));
+            plan_copy(P.coef[a], m.coef.coef.size() * sizeof(C));
+        }
+    }
+    ws.staging.ensure(soff);
+    char* sb = static_cast<char*>(ws.staging.p);
+    {
+        std::size_t k = 0;
+        auto put = [&](const void* src, std::size_t bytes) {
+            if (!bytes) return;
+            std::memcpy(sb + copies[k].off, src, bytes);
+            ++k;
+        };
+        put(colj.data(), colj.size() * sizeof(ColJob));
+        put(rowj.data(), rowj.size() * sizeof(RowJob));
+        put(invj.data(), invj.size() * sizeof(InvJob));
+        put(scanj.data(), scanj.size() * sizeof(ScanJob));
+        if (!fcr_only) put(conj.data(), conj.size() * sizeof(ContractJob));
+        for (std::size_t a = 0; a < ni; ++a) {
+            const InstMeta& m = *metas[a];
+            put(m.tmap.data(), m.tmap.size() * sizeof(int));
+            if (!fcr_only) {
+                put(m.out_u.data(), m.out_u.size() * sizeof(uint32_t));
+                put(m.coef.rowptr.data(), m.coef.rowptr.size() * sizeof(int32_t));
+                put(m.coef.src.data(), m.coef.src.size() * sizeof(uint32_t));
+                if (std::is_same<R, double>::value) {
+                    put(m.coef.coef.data(), m.coef.coef.size() * sizeof(C));
+                } else {
+                    std::vector<float2> cf(m.coef.coef.size());
+                    for (std::size_t e = 0; e < cf.size(); ++e) cf[e] = to_f2(m.coef.coef[e]);
+                    put(cf.data(), cf.size() * sizeof(float2));
+                }
+            }
+        }
+    }
+    for (const Copy& c : copies)
+        cuda_check(cudaMemcpyAsync(c.dst, sb + c.off, c.bytes, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(meta)");
+    for (std::size_t a = 0; a < ni; ++a)
+        if (!insts[a]->gamma_on_device)
+            cuda_check(cudaMemcpyAsync(const_cast<double2*>(P.gamma[a]), insts[a]->gamma,
+                                       insts[a]->sys.nf * insts[a]->Nt * sizeof(double2), cudaMemcpyHostToDevice, st),
+                       "cudaMemcpyAsync(gamma)");
+
+    // ---- launches ----
+    set_smem(k_fwd_col<R>, g.col_smem);
+    set_smem(k_inv_col<R>, g.col_smem);
+    set_smem(k_row<R>, g.row_smem);
+    ProfRecorder pr;
+    pr.st = st;
+    const bool f32 = std::is_same<R, float>::value;
+    if (opt.fcr_ms) cuda_check(cudaEventRecord(ws.ev0, st), "cudaEventRecord");
+    pr.before(f32 ? "spectra_col_f32" : "spectra_col_f64");
+    k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(n_spec_jobs)), g.col_threads, g.col_smem, st>>>(
+        P.colj, plan, g.col_cols);
+    check_launch("k_fwd_col(spectra)", &pr);
+    pr.before(f32 ? "spectra_row_f32" : "spectra_row_f64");
+    k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
+        P.rowj, plan, g.row_rows);
+    check_launch("k_row(spectra)", &pr);
+    for (std::size_t ch = 0; ch < nchunks; ++ch) {
+        const std::size_t q0 = ch * Q, nq = std::min(Q, ntri - q0);
+        pr.before(f32 ? "fwd_col_f32" : "fwd_col_f64");
+        k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(nq)), g.col_threads, g.col_smem, st>>>(
+            P.colj + n_spec_jobs + q0, plan, g.col_cols);
+        check_launch("k_fwd_col", &pr);
+        pr.before(f32 ? "row_conv_f32" : "row_conv_f64");
+        k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
+            P.rowj + n_spec_jobs + q0, plan, g.row_rows);
+        check_launch("k_row", &pr);
+        pr.before(f32 ? "inv_col_f32" : "inv_col_f64");
+        k_inv_col<R><<<dim3(g.col_grid, static_cast<unsigned>(2 * nq)), g.col_threads, g.col_smem, st>>>(
+            P.invj + 2 * q0, plan, g.col_cols);
+        check_launch("k_inv_col", &pr);
+    }
+    pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
+    k_scan_assemble<R><<<static_cast<unsigned>(ntri), SCAN_THREADS, 0, st>>>(P.scanj);
+    check_launch("k_scan_assemble", &pr);
+    if (opt.fcr_ms) cuda_check(cudaEventRecord(ws.ev1, st), "cudaEventRecord");
+    if (!fcr_only) {
+        int maxE = 0;
+        for (auto* in : insts) maxE = std::max(maxE, in->sys.N * in->sys.N * in->sys.N * in->sys.N);
+        const int OT = std::max(1, std::min(128, static_cast<int>((48 * 1024) / (maxE * sizeof(C)))));
+        std::size_t maxT = 0;
+        for (auto* m : metas) maxT = std::max(maxT, m->T);
+        const std::size_t smem = static_cast<std::size_t>(OT) * maxE * sizeof(C);
+        set_smem(k_contract<R>, smem);
+        const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
+        pr.before(f32 ? "contract_f32" : "contract_f64");
+        k_contract<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, smem, st>>>(P.conj, OT);
+        check_launch("k_contract", &pr);
+        for (std::size_t a = 0; a < ni; ++a) {
+            if (insts[a]->out_on_device) continue;
+            const std::size_t E = static_cast<std::size_t>(insts[a]->sys.N) * insts[a]->sys.N * insts[a]->sys.N * insts[a]->sys.N;
+            cuda_check(cudaMemcpyAsync(insts[a]->out, P.out[a], metas[a]->T * E * sizeof(C), cudaMemcpyDeviceToHost, st),
+                       "cudaMemcpyAsync(L4 out)");
+        }
+    } else if (!fcr_out_dev) {
+        const Tcl4Instance& in = *insts[0];
+        const std::size_t nf3 = static_cast<std::size_t>(in.sys.nf) * in.sys.nf * in.sys.nf;
+        const std::size_t U = metas[0]->U;
+        for (int kind = 0; kind < 3; ++kind)
+            cuda_check(cudaMemcpyAsync(fcr_out[kind], P.v[0] + kind * nf3 * U, nf3 * U * sizeof(C),
+                                       cudaMemcpyDeviceToHost, st),
+                       "cudaMemcpyAsync(F/C/R out)");
+    }
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    pr.resolve();
+    if (opt.fcr_ms) {
+        float ms = 0.f;
+        cuda_check(cudaEventElapsedTime(&ms, ws.ev0, ws.ev1), "cudaEventElapsedTime");
+        *opt.fcr_ms += ms;
+    }
+}
+
+void validate_system(const SystemDesc& s) {
+    if (s.N <= 0) throw Error(kInvalidArgument, "system: N must be > 0");
+    if (s.nf <= 0) throw Error(kInvalidArgument, "system: nf must be > 0");
+    if (s.num_ops <= 0) throw Error(kInvalidArgument, "coupling_ops must be non-empty");
+    if (static_cast<int>(s.omegas.size()) != s.nf || static_cast<int>(s.mirror.size()) != s.nf)
+        throw Error(kInvalidArgument, "system: frequency metadata has wrong size");
+    if (static_cast<int>(s.p2f.size()) != s.N * s.N) throw Error(kInvalidArgument, "system: pair_to_freq has wrong shape");
+    for (int v : s.p2f) {
+        if (v < 0) throw Error(kRuntime, "pair_to_freq contains -1 (missing frequency buckets)");
+        if (v >= s.nf) throw Error(kInvalidArgument, "pair_to_freq entry out of range");
+    }
+    for (int v : s.mirror)
+        if (v < 0 || v >= s.nf) throw Error(kInvalidArgument, "mirror entry out of range");
+    if (static_cast<std::size_t>(s.num_ops) * s.N * s.N != s.ops.size())
+        throw Error(kInvalidArgument, "coupling operator has wrong shape");
+    const double nf3 = static_cast<double>(s.nf) * s.nf * s.nf;
+    if (3.0 * nf3 >= 2147483647.0) throw Error(kOverflow, "nf too large");
+}
+
+}  // namespace
+
+cudaStream_t default_stream() { return workspace().stream; }
+
+uint64_t kernel_launches() { return g_launches.load(); }
+void profile_enable(bool on) { g_profile.store(on); }
+void profile_reset() {
+    ProfStore& ps = prof_store();
+    std::lock_guard<std::mutex> lk(ps.mu);
+    ps.acc.clear();
+    ps.order.clear();
+}
+std::vector<ProfileEntry> profile_entries() {
+    ProfStore& ps = prof_store();
+    std::lock_guard<std::mutex> lk(ps.mu);
+    std::vector<ProfileEntry> out;
+    for (const auto& n : ps.order) {
+        const auto& v = ps.acc.at(n);
+        out.push_back({n.c_str(), v.first, v.second});
+    }
+    return out;
+}
+
+void build_mirror(const std::vector<double>& omegas, double tol, std::vector<int>& mirror, int* zero_index) {
+    const double t = std::max(1e-12, tol);
+    const int nf = static_cast<int>(omegas.size());
+    mirror.assign(nf, -1);
+    int zero = -1;
+    for (int b = 0; b < nf; ++b) {
+        const double w = omegas[b];
+        int best = -1;
+        if (std::abs(w) <= t) {
+            best = b;
+            if (zero < 0) zero = b;
+        } else {
+            double ba = std::numeric_limits<double>::infinity();
+            for (int bp = 0; bp < nf; ++bp) {
+                const double d = std::abs(omegas[bp] - (-w));
+                if (d < ba) {
+                    ba = d;
+                    best = bp;
+                }
+            }
+        }
+        mirror[b] = best;
+    }
+    if (zero < 0) {
+        double ba = std::numeric_limits<double>::infinity();
+        for (int b = 0; b < nf; ++b)
+            if (std::abs(omegas[b]) < ba) {
+                ba = std::abs(omegas[b]);
+                zero = b;
+            }
+        if (zero < 0) zero = 0;
+    }
+    if (zero_index) *zero_index = zero;
+}
+
+void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream) {
+    Workspace& ws = workspace();
+    cudaStream_t st = stream ? stream : ws.stream;
+    if (opt.fcr_ms) *opt.fcr_ms = 0.0;
+    std::vector<InstMeta> metas(insts.size());
+    for (std::size_t a = 0; a < insts.size(); ++a) {
+        Tcl4Instance& in = insts[a];
+        validate_system(in.sys);
+        if (in.Nt == 0) throw Error(kInvalidArgument, "empty gamma_series");
+        if (in.Nt >= (std::size_t(1) << 31)) throw Error(kOverflow, "Nt too large");
+        if (!(in.dt > 0.0)) throw Error(kInvalidArgument, "dt must be > 0");
+        if (!in.gamma) throw Error(kInvalidArgument, "gamma is null");
+        if (in.tidx.empty()) continue;
+        if (!in.out) throw Error(kInvalidArgument, "output pointer is null");
+        for (uint32_t t : in.tidx)
+            if (t >= in.Nt) throw Error(kOutOfRange, "time_index out of range");
+        derive_meta(in, opt, metas[a], true);
+    }
+    // group by FFT length
+    std::map<int, std::vector<std::size_t>> groups;
+    for (std::size_t a = 0; a < insts.size(); ++a)
+        if (!insts[a].tidx.empty()) groups[metas[a].L].push_back(a);
+    for (auto& kv : groups) {
+        std::vector<Tcl4Instance*> gi;
+        std::vector<InstMeta*> gm;
+        for (std::size_t a : kv.second) {
+            gi.push_back(&insts[a]);
+            gm.push_back(&metas[a]);
+        }
+        if (opt.fp32) run_group<float>(gi, gm, opt, st, ws, nullptr, false);
+        else run_group<double>(gi, gm, opt, st, ws, nullptr, false);
+    }
+}
+
+void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_device, std::size_t Nt, double dt,
+                    double2* F, double2* Cc, double2* R, bool out_on_device, const BuildOptions& opt,
+                    cudaStream_t stream) {
+    Workspace& ws = workspace();
+    cudaStream_t st = stream ? stream : ws.stream;
+    SystemDesc s = sys;
+    if (s.num_ops <= 0) {  // F/C/R do not depend on the coupling operators
+        s.num_ops = 1;
+        s.ops.assign(static_cast<std::size_t>(s.N) * s.N, make_double2(0.0, 0.0));
+    }
+    validate_system(s);
+    if (Nt == 0) throw Error(kInvalidArgument, "empty gamma_series");
+    if (Nt >= (std::size_t(1) << 31)) throw Error(kOverflow, "Nt too large");
+    if (!(dt > 0.0)) throw Error(kInvalidArgument, "dt must be > 0");
+    if (!gamma || !F || !Cc || !R) throw Error(kInvalidArgument, "null pointer");
+    Tcl4Instance in;
+    in.sys = s;
+    in.gamma = gamma;
+    in.gamma_on_device = gamma_on_device;
+    in.Nt = Nt;
+    in.dt = dt;
+    in.tidx.resize(Nt);
+    for (std::size_t t = 0; t < Nt; ++t) in.tidx[t] = static_cast<uint32_t>(t);
+    BuildOptions o = opt;
+    o.fp32 = false;
+    o.causal_truncation = false;
+    InstMeta m;
+    derive_meta(in, o, m, false);
+    std::vector<Tcl4Instance*> gi{&in};
+    std::vector<InstMeta*> gm{&m};
+    double2* outs[3] = {F, Cc, R};
+    if (opt.fcr_ms) *opt.fcr_ms = 0.0;
+    run_group<double>(gi, gm, o, st, ws, outs, out_on_device);
+}
+
+std::size_t rk4_num_samples(std::size_t steps, std::size_t sample_every) {
+    if (sample_every == 0) return 0;
+    return (steps + sample_every - 1) / sample_every + 1;
+}
+
+void rk4_propagate_device(const std::vector<Rk4Request>& reqs, cudaStream_t stream) {
+    if (reqs.empty()) return;
+    Workspace& ws = workspace();
+    cudaStream_t st = stream ? stream : ws.stream;
+    // group by (D, storage)
+    std::map<std::pair<int, int>, std::vector<std::size_t>> groups;
+    for (std::size_t k = 0; k < reqs.size(); ++k) {
+        const Rk4Request& r = reqs[k];
+        if (r.D <= 0) throw Error(kInvalidArgument, "rk4: dimension must be > 0");
+        if (!(r.dt > 0.0)) throw Error(kInvalidArgument, "rk4: dt must be > 0");
+        if (r.steps < 1) throw Error(kInvalidArgument, "rk4: L_series must have at least 2 matrices (endpoints)");
+        if (!r.L || !r.r) throw Error(kInvalidArgument, "rk4: null pointer");
+        if (r.obs_out && !r.obs) throw Error(kInvalidArgument, "rk4: obs_out needs obs");
+        if ((r.samples || r.obs_out) && r.sample_every == 0)
+            throw Error(kInvalidArgument, "rk4: sample_every must be > 0");
+        groups[{r.D, r.fp32_storage ? 1 : 0}].push_back(k);
+    }
+    std::vector<Rk4Job> jobs(reqs.size());
+    for (std::size_t k = 0; k < reqs.size(); ++k) {
+        const Rk4Request& r = reqs[k];
+        jobs[k] = Rk4Job{r.L, r.L_half, r.L_add, r.steps, r.dt, r.r, r.sample_every, r.samples, r.obs, r.obs_out};
+    }
+    // reorder jobs group-contiguously and upload once
+    std::vector<Rk4Job> ordered;
+    std::vector<std::pair<std::size_t, std::size_t>> ranges;
+    for (auto& kv : groups) {
+        ranges.push_back({ordered.size(), kv.second.size()});
+        for (std::size_t k : kv.second) ordered.push_back(jobs[k]);
+    }
+    ws.arena.ensure(ordered.size() * sizeof(Rk4Job) + 256);
+    ws.staging.ensure(ordered.size() * sizeof(Rk4Job));
+    std::memcpy(ws.staging.p, ordered.data(), ordered.size() * sizeof(Rk4Job));
+    Rk4Job* dj = static_cast<Rk4Job*>(ws.arena.p);
+    cuda_check(cudaMemcpyAsync(dj, ws.staging.p, ordered.size() * sizeof(Rk4Job), cudaMemcpyHostToDevice, st),
+               "cudaMemcpyAsync(rk4 jobs)");
+    std::size_t gi = 0;
+    ProfRecorder pr;
+    pr.st = st;
+    for (auto& kv : groups) {
+        const int D = kv.first.first;
+        pr.before(D <= 16 ? "rk4_warp" : "rk4_cta");
+        const bool f32 = kv.first.second != 0;
+        const auto rg = ranges[gi++];
+        Rk4Job* base = dj + rg.first;
+        const int n = static_cast<int>(rg.second);
+        if (D <= 16) {
+            const int warps_per_block = 4;
+            const unsigned grid = static_cast<unsigned>((n + warps_per_block - 1) / warps_per_block);
+            if (D <= 4) {
+                if (f32) k_rk4_warp<float2, 4><<<grid, 32 * warps_per_block, 0, st>>>(base, n, D);
+                else k_rk4_warp<double2, 4><<<grid, 32 * warps_per_block, 0, st>>>(base, n, D);
+            } else {
+                if (f32) k_rk4_warp<float2, 16><<<grid, 32 * warps_per_block, 0, st>>>(base, n, D);
+                else k_rk4_warp<double2, 16><<<grid, 32 * warps_per_block, 0, st>>>(base, n, D);
+            }
+            check_launch("k_rk4_warp", &pr);
+        } else {
+            const std::size_t smem = 6 * static_cast<std::size_t>(D) * sizeof(double2);
+            const int threads = std::min(256, ((D + 31) / 32) * 32);
+            if (f32) {
+                set_smem(k_rk4_cta<float2>, smem);
+                k_rk4_cta<float2><<<static_cast<unsigned>(n), threads, smem, st>>>(base, D);
+            } else {
+                set_smem(k_rk4_cta<double2>, smem);
+                k_rk4_cta<double2><<<static_cast<unsigned>(n), threads, smem, st>>>(base, D);
+            }
+            check_launch("k_rk4_cta", &pr);
+        }
+    }
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(rk4)");
+    pr.resolve();
+}
+
+}  // namespace taco

@@ -1,0 +1,88 @@
+// engine.hpp -- host orchestration of the TCL4 device path (no torch types).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+namespace taco {
+
+struct SystemDesc {
+    int N = 0, nf = 0, num_ops = 0;
+    std::vector<double> omegas;
+    std::vector<int> mirror;
+    std::vector<int> p2f;       // column-major N x N
+    std::vector<double2> ops;   // num_ops x (N x N) column-major
+};
+
+struct Tcl4Instance {
+    SystemDesc sys;
+    const double2* gamma = nullptr;  // [nf][Nt] (column-major Nt x nf)
+    bool gamma_on_device = false;
+    std::size_t Nt = 0;
+    double dt = 0.0;
+    std::vector<uint32_t> tidx;      // explicit list of requested time indices
+    void* out = nullptr;             // [T][N^2 x N^2] complex (FP64: double2, FP32: float2)
+    bool out_on_device = false;
+};
+
+struct BuildOptions {
+    bool fp32 = false;
+    bool causal_truncation = false;  // FFT length from max(tidx)+1 instead of Nt
+    std::size_t pad_factor = 0;      // Nfft = next_pow2(max(2 n - 1, pad * n))
+    std::size_t scratch_budget = std::size_t(1) << 30;
+    double* fcr_ms = nullptr;        // device time of the F/C/R stage
+};
+
+// Full L4 builds (build_TCL4_generator_cuda_fused[_batch]) for a set of instances.
+void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream);
+
+// compute_triple_kernels: full F/C/R series [nf^3][Nt] (FP64) for one instance.
+void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_device, std::size_t Nt,
+                    double dt, double2* F, double2* Cc, double2* R, bool out_on_device,
+                    const BuildOptions& opt, cudaStream_t stream);
+
+struct Rk4Request {
+    const void* L = nullptr;       // [steps+1][D x D]
+    const void* L_half = nullptr;  // [steps][D x D] or nullptr
+    const void* L_add = nullptr;   // [steps+1][D x D] or nullptr
+    bool fp32_storage = false;     // L, L_half, L_add are complex64 when true
+    std::size_t steps = 0;
+    int D = 0;
+    double dt = 0.0;
+    double2* r = nullptr;          // [D]
+    std::size_t sample_every = 0;
+    double2* samples = nullptr;    // [n_samples][D]
+    const double2* obs = nullptr;  // [D]
+    double2* obs_out = nullptr;    // [n_samples]
+};
+
+// RK4 propagation; all pointers are device pointers.  Requests with equal D and storage
+// type run in one launch.
+void rk4_propagate_device(const std::vector<Rk4Request>& reqs, cudaStream_t stream);
+
+std::size_t rk4_num_samples(std::size_t steps, std::size_t sample_every);
+
+// Mirror map of cpp/src/tcl/tcl4.cpp:40-101.
+void build_mirror(const std::vector<double>& omegas, double tol, std::vector<int>& mirror, int* zero_index);
+
+// Per-host-thread CUDA stream of the current device (created on first use).
+cudaStream_t default_stream();
+
+// Kernel accounting: every launch increments a process-wide counter; when profiling is
+// on, each launch is bracketed by CUDA events and its device time is accumulated per
+// kernel name after the call's final synchronisation.
+uint64_t kernel_launches();
+void profile_enable(bool on);
+void profile_reset();
+struct ProfileEntry {
+    const char* name;
+    uint64_t launches;
+    double total_ms;
+};
+std::vector<ProfileEntry> profile_entries();
+
+}  // namespace taco

@@ -1,0 +1,131 @@
+// fft.cuh -- shared-memory Stockham FFT engine for power-of-two lengths.
+//
+// A tile in shared memory holds `nfft` independent transforms of length n; element
+// i of transform f lives at s[f*fs + i*es].  Every thread owns 8 elements per stage
+// (blockDim.x == nfft*n/8), so each radix-2^r stage reads 8 values into registers,
+// twiddles them, runs 8/2^r small DFTs and writes them back (Stockham autosort:
+// natural order in, natural order out; in place with a barrier between the read and
+// the write phase).  The twiddle table tw[m] = exp(-2*pi*i*m/n), m in [0, n), is read
+// through the read-only path; inverse transforms conjugate it and are unnormalised.
+#pragma once
+
+#include "common.cuh"
+
+namespace taco {
+
+template <class C, bool INV>
+__device__ __forceinline__ C mul_w(C a, C w) {
+    return INV ? cmulc(a, w) : cmul(a, w);  // INV: a * conj(w)
+}
+
+// multiply by -i (forward) or +i (inverse)
+template <class C, bool INV>
+__device__ __forceinline__ C rot90(C a) {
+    return INV ? C{-a.y, a.x} : C{a.y, -a.x};
+}
+
+template <class C, bool INV>
+__device__ __forceinline__ void dft2(C& a, C& b) {
+    const C t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+template <class C, bool INV>
+__device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3) {
+    const C a = cadd(x0, x2), b = csub(x0, x2);
+    const C c = cadd(x1, x3), d = rot90<C, INV>(csub(x1, x3));
+    x0 = cadd(a, c);
+    x2 = csub(a, c);
+    x1 = cadd(b, d);
+    x3 = csub(b, d);
+}
+
+template <class C, bool INV>
+__device__ __forceinline__ void dft8(C* x) {
+    using R = decltype(x[0].x);
+    const R h = static_cast<R>(0.70710678118654752440084436210484903928);
+    C e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6];
+    C o0 = x[1], o1 = x[3], o2 = x[5], o3 = x[7];
+    dft4<C, INV>(e0, e1, e2, e3);
+    dft4<C, INV>(o0, o1, o2, o3);
+    // twiddles w8^k, k = 0..3 (w8 = exp(-+ 2 pi i / 8))
+    const C t1 = INV ? C{h * (o1.x - o1.y), h * (o1.x + o1.y)} : C{h * (o1.x + o1.y), h * (o1.y - o1.x)};
+    const C t2 = rot90<C, INV>(o2);
+    const C t3 = INV ? C{-h * (o3.x + o3.y), h * (o3.x - o3.y)} : C{h * (o3.y - o3.x), -h * (o3.x + o3.y)};
+    x[0] = cadd(e0, o0);
+    x[4] = csub(e0, o0);
+    x[1] = cadd(e1, t1);
+    x[5] = csub(e1, t1);
+    x[2] = cadd(e2, t2);
+    x[6] = csub(e2, t2);
+    x[3] = cadd(e3, t3);
+    x[7] = csub(e3, t3);
+}
+
+// One Stockham stage of radix 2^LR on a shared-memory tile.
+template <class C, int LR, bool INV>
+__device__ __forceinline__ void stockham_stage(C* s, int log2n, int p, int fs, int es,
+                                               const C* __restrict__ tw) {
+    constexpr int RAD = 1 << LR;
+    constexpr int ITEMS = 8 / RAD;
+    const int n = 1 << log2n;
+    const int lq = log2n - LR;  // log2(n / RAD): items per transform
+    const int q_mask = (1 << lq) - 1;
+    C x[8];
+    int base[ITEMS], jout[ITEMS];
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+        const int g = threadIdx.x * ITEMS + q;
+        const int f = g >> lq;
+        const int i = g & q_mask;
+        const int k = i & (p - 1);
+        base[q] = f * fs;
+        jout[q] = ((i - k) << LR) + k;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) x[q * RAD + r] = s[base[q] + (i + (r << lq)) * es];
+        if (p > 1) {
+            // w_{p*RAD}^{r*k} = tw[r * k * n / (p * RAD)]
+            const int stride = (n / (p * RAD)) * k;
+#pragma unroll
+            for (int r = 1; r < RAD; ++r) x[q * RAD + r] = mul_w<C, INV>(x[q * RAD + r], __ldg(&tw[r * stride]));
+        }
+        if (RAD == 8) dft8<C, INV>(&x[q * RAD]);
+        else if (RAD == 4) dft4<C, INV>(x[q * RAD], x[q * RAD + 1], x[q * RAD + 2], x[q * RAD + 3]);
+        else dft2<C, INV>(x[q * RAD], x[q * RAD + 1]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) s[base[q] + (jout[q] + r * p) * es] = x[q * RAD + r];
+    }
+    __syncthreads();
+}
+
+// Full transform of every length-n sequence in the tile.  Requires
+// blockDim.x * 8 == (number of transforms) * n and n >= 2.  The tile must be
+// visible to all threads (a __syncthreads() after filling it) on entry; it is
+// complete and visible on exit.
+template <class C, bool INV>
+__device__ void tile_fft(C* s, int log2n, int fs, int es, const C* __restrict__ tw) {
+    int p = 1;
+    int rem = log2n;
+    // radix-4 first when log2n % 3 == 2, radix-2 first when log2n % 3 == 1, then radix-8
+    if (rem % 3 == 2) {
+        stockham_stage<C, 2, INV>(s, log2n, p, fs, es, tw);
+        p <<= 2;
+        rem -= 2;
+    } else if (rem % 3 == 1) {
+        stockham_stage<C, 1, INV>(s, log2n, p, fs, es, tw);
+        p <<= 1;
+        rem -= 1;
+    }
+    while (rem > 0) {
+        stockham_stage<C, 3, INV>(s, log2n, p, fs, es, tw);
+        p <<= 3;
+        rem -= 3;
+    }
+}
+
+}  // namespace taco

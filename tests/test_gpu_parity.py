@@ -1,0 +1,169 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle and the golden vectors.
+
+Tolerances (relative Frobenius unless stated):
+  plain FP64 path   L4 <= 1e-10, F/C/R <= 1e-10 of max |series|
+  FP32 form         L4 <= 1e-6
+  RK4 (FP64 state)  <= 1e-10 against the oracle; analytic cases <= 1e-6
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import taco_b200 as tb
+from cases import oracle_l4, random_case, relerr, spin_boson_case
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def torch_dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def test_synthetic_gamma_triple_kernels_and_l4():
+    g = np.load(os.path.join(GOLD, "synthetic_gamma.npz"))
+    s = tb.System.from_arrays(int(g["N"]), g["omegas"], g["p2f"], list(g["ops"]), mirror=g["mirror"])
+    dt = float(g["dt"])
+    F, C, R = tb.compute_triple_kernels(s, g["gamma"], dt)
+    nf = int(g["nf"])
+    for a, b in ((F, g["F"]), (C, g["C"]), (R, g["R"])):
+        a = a.reshape(nf ** 3, -1)
+        assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b)))
+    L4 = tb.build_correction_series(s, g["gamma"], dt)
+    assert relerr(L4, g["L4_all"]) <= 1e-10
+    L4s = tb.build_TCL4_generator_batch(s, g["gamma"], dt, g["tids"])
+    assert relerr(L4s, g["L4_all"][g["tids"]]) <= 1e-10
+    one = tb.build_TCL4_generator(s, g["gamma"], dt, 8)
+    assert relerr(one, g["L4_all"][8]) <= 1e-10
+
+
+def test_spin_boson_golden_end_to_end():
+    g = np.load(os.path.join(GOLD, "spin_boson_small.npz"))
+    s = tb.System.from_arrays(int(g["N"]), g["omegas"], g["p2f"], list(g["ops"]), mirror=g["mirror"])
+    dt = float(g["dt"])
+    steps = int(g["steps"])
+    L4 = tb.build_TCL4_generator_batch(s, g["gamma"], dt, np.arange(steps + 1))
+    assert relerr(L4, g["L4"]) <= 1e-10
+    L = g["L2"] + np.asarray(L4)
+    r, _, _ = tb.propagate_rk4_dense(L, g["r0"], dt)
+    assert relerr(r, g["r_final"]) <= 1e-10
+    r2, _, _ = tb.propagate_rk4_dense(torch_dev(g["L2"]), torch_dev(g["r0"]), dt, L_add=torch_dev(np.asarray(L4)))
+    assert relerr(r2.cpu().numpy(), g["r_final"]) <= 1e-10
+
+
+@pytest.mark.parametrize("device_io", [False, True])
+def test_config1_shape_fp64_vs_oracle(device_io):
+    """d=2 spin boson, alpha=0.05, wc=10, beta=1, dt=0.005, on a 4001-sample grid, tidx 0..1000."""
+    osys, s, G = spin_boson_case(4000, 0.005)
+    tidx = np.arange(1001)
+    ref = oracle_l4(osys, G, 0.005, tidx)
+    if device_io:
+        out = tb.build_TCL4_generator_batch(s, torch_dev(G), 0.005, tidx).cpu().numpy()
+    else:
+        out = tb.build_TCL4_generator_batch(s, G, 0.005, tidx)
+    assert relerr(out, ref) <= 1e-10
+
+
+def test_fp32_form_error_bound():
+    osys, s, G = spin_boson_case(4000, 0.005)
+    tidx = np.arange(0, 4001, 3)
+    ref = oracle_l4(osys, G, 0.005, tidx)
+    out = tb.build_TCL4_generator_batch(s, G, 0.005, tidx, precision="fp32")
+    assert out.dtype == np.complex64
+    assert relerr(out, ref) <= 1e-6
+
+
+def test_triple_kernels_match_oracle_full_series():
+    osys, s, G = spin_boson_case(3000, 0.005)
+    F, C, R = tb.compute_triple_kernels(s, G, 0.005)
+    Fo, Co, Ro = oracle.fcr_series(G, osys.omegas, osys.mirror, 0.005)
+    nf = osys.nf
+    for a, b in ((F, Fo), (C, Co), (R, Ro)):
+        assert relerr(a.reshape(nf ** 3, -1), b) <= 1e-10
+
+
+@pytest.mark.parametrize("d,nops,Nt", [(3, 1, 700), (4, 2, 300)])
+def test_random_systems_vs_oracle(d, nops, Nt):
+    osys, s, G = random_case(d, nops, Nt, 0.01, seed=d)
+    tidx = np.array([0, 1, Nt // 3, Nt // 2, Nt - 1, 5, 5])
+    ref = oracle_l4(osys, G, 0.01, tidx)
+    out = tb.build_TCL4_generator_batch(s, G, 0.01, tidx)
+    assert relerr(out, ref) <= 1e-10
+    out32 = tb.build_TCL4_generator_batch(s, G, 0.01, tidx, precision="fp32")
+    assert relerr(out32, ref) <= 1e-6
+
+
+def test_pad_factor_and_causal_truncation_keep_results():
+    osys, s, G = spin_boson_case(2000, 0.005)
+    tidx = np.arange(0, 300)
+    base = tb.build_TCL4_generator_batch(s, G, 0.005, tidx)
+    tb.set_fcr_fft_pad_factor(8)
+    try:
+        padded = tb.build_TCL4_generator_batch(s, G, 0.005, tidx)
+    finally:
+        tb.set_fcr_fft_pad_factor(0)
+    trunc = tb.build_TCL4_generator_batch(s, G, 0.005, tidx, causal_truncation=True)
+    assert relerr(padded, base) <= 1e-12 and relerr(trunc, base) <= 1e-12
+
+
+def test_batched_instances_match_single_calls():
+    cases = [spin_boson_case(1500, 0.005, eps=e, delta=dl, alpha=a) for e, dl, a in
+             ((1.0, 1.0, 0.05), (0.7, 1.3, 0.1), (1.5, 0.6, 0.02))]
+    cases.append(random_case(3, 1, 900, 0.01, seed=7))
+    inst = []
+    for k, (osys, s, G) in enumerate(cases):
+        dtk = 0.01 if k == 3 else 0.005
+        inst.append((s, G, dtk, np.arange(0, G.shape[1], 7 + k)))
+    outs = tb.build_instances(inst)
+    for (s, G, dtk, tidx), (osys, _, _), out in zip(inst, cases, outs):
+        ref = oracle_l4(osys, G, dtk, tidx)
+        assert relerr(out, ref) <= 1e-10
+    outs32 = tb.build_instances(inst, precision="fp32")
+    for (s, G, dtk, tidx), (osys, _, _), out in zip(inst, cases, outs32):
+        assert relerr(out, oracle_l4(osys, G, dtk, tidx)) <= 1e-6
+
+
+def test_errors_follow_reference_exceptions():
+    osys, s, G = spin_boson_case(100, 0.005)
+    with pytest.raises(IndexError):
+        tb.build_TCL4_generator_batch(s, G, 0.005, [0, 101])
+    with pytest.raises(ValueError):
+        tb.build_TCL4_generator_batch(s, G, -1.0, [0])
+    bad = tb.System.from_arrays(s.N, s.omegas, s.pair_to_freq, [], mirror=s.mirror)
+    with pytest.raises(ValueError):
+        tb.build_TCL4_generator_batch(bad, G, 0.005, [0])
+
+
+def test_rk4_analytic_cases_on_device():
+    """tests/rk4_dense_tests.cpp:43-101 (constant L via a constant series; L = t I with midpoints)."""
+    import scipy.linalg
+    L = np.zeros((4, 4), np.complex128)
+    L[0, 0], L[1, 1], L[2, 2], L[3, 3] = 0.10 - 0.03j, -0.07 + 0.05j, 0.02, -0.04 - 0.02j
+    L[0, 2], L[2, 0], L[1, 3] = 0.03 + 0.01j, -0.02 + 0.02j, 0.01 - 0.04j
+    r0 = np.array([1.0, 0.5 - 0.2j, -0.7 + 0.1j, 0.1 + 0.3j])
+    steps = 500
+    r, _, _ = tb.propagate_rk4_dense(np.repeat(L[None], steps + 1, 0), r0, 0.0025)
+    assert relerr(r, scipy.linalg.expm(1.25 * L) @ r0) <= 1e-6
+    D, steps, dt = 3, 100, 0.01
+    Ls = np.stack([i * dt * np.eye(D, dtype=np.complex128) for i in range(steps + 1)])
+    Lh = np.stack([(i + 0.5) * dt * np.eye(D, dtype=np.complex128) for i in range(steps)])
+    r0 = np.array([0.3 + 0.1j, -0.2 + 0.4j, 0.9 - 0.3j])
+    r, _, _ = tb.propagate_rk4_dense(Ls, r0, dt, L_half=Lh)
+    assert relerr(r, np.exp(0.5) * r0) <= 1e-6
+
+
+@pytest.mark.parametrize("D", [4, 9, 36])
+def test_rk4_vs_oracle_with_samples(D):
+    rng = np.random.default_rng(D)
+    steps = 257
+    Ls = 0.1 * (rng.standard_normal((steps + 1, D, D)) + 1j * rng.standard_normal((steps + 1, D, D)))
+    r0 = rng.standard_normal(D) + 1j * rng.standard_normal(D)
+    obs = rng.standard_normal(D) + 1j * rng.standard_normal(D)
+    r_ref, s_ref = oracle.rk4_propagate(Ls, r0, 0.01, sample_every=16)
+    r, samples, ov = tb.propagate_rk4_dense(Ls, r0, 0.01, sample_every=16, obs=obs)
+    assert relerr(r, r_ref) <= 1e-12
+    assert samples.shape == s_ref.shape and relerr(samples, s_ref) <= 1e-12
+    assert relerr(ov, s_ref @ obs) <= 1e-12
