@@ -54,40 +54,6 @@ def parse():
     return p.parse_args()
 
 
-def draw_params(rng, B):
-    return [dict(eps=rng.uniform(0.5, 2.0), delta=rng.uniform(0.5, 2.0),
-                 alpha=math.exp(rng.uniform(math.log(0.01), math.log(0.2))),
-                 wc=rng.uniform(1.0, 20.0), beta=math.exp(rng.uniform(math.log(0.2), math.log(5.0))))
-            for _ in range(B)]
-
-
-def make_gamma_device(torch, sysm, prm, N, dt, device):
-    """C(t) (correlation_fft.hpp:153-214) and trapezoid Gamma (gamma.hpp:166-213) with torch."""
-    Nt = N + 1
-    nfft = 1 << (2 * Nt - 1).bit_length()
-    dw = 2 * math.pi / (dt * nfft)
-    wny = math.pi / dt
-    a, wc, beta = prm["alpha"], prm["wc"], prm["beta"]
-    k = torch.arange(1, nfft // 2, dtype=torch.float64, device=device)
-    w = dw * k
-    J = a * w * torch.exp(-w / wc)
-    r = math.exp(-beta * dw)
-    kms = torch.exp(-beta * dw * k)
-    sp = (math.pi / 2) * J / (1.0 - kms)
-    S = torch.zeros(nfft, dtype=torch.complex128, device=device)
-    S[1:nfft // 2] = sp.to(torch.complex128)
-    S[nfft // 2 + 1:] = torch.flip(sp * kms, [0]).to(torch.complex128)
-    S[0] = 0.5 * (math.pi / 2) * (a * dw * math.exp(-dw / wc)) * (1 + r) / (1 - r)
-    S[nfft // 2] = 0.25 * math.pi * (a * wny * math.exp(-wny / wc)) * (1 + 2 / math.expm1(beta * wny))
-    C = torch.fft.fft(S)[:Nt] * (dw / math.pi)
-    t = torch.arange(Nt, dtype=torch.float64, device=device) * dt
-    G = torch.zeros((sysm.nf, Nt), dtype=torch.complex128, device=device)
-    for b, om in enumerate(sysm.omegas):
-        y = torch.exp(1j * om * t) * C
-        G[b, 1:] = torch.cumsum(0.5 * dt * (y[:-1] + y[1:]), 0)
-    return G
-
-
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -185,6 +151,7 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return
     import oracle
+    from taco_b200.workloads import draw_params
     threads = oracle.max_threads()
     rng = np.random.default_rng(args.seed)
     prm = draw_params(rng, 1)[0]
@@ -217,6 +184,20 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def timed(torch, fn, reps, warmup=1):
+    """Average device ms of fn() over reps calls (CUDA events on the current stream)."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -228,6 +209,7 @@ def main():
 
     import torch
     import taco_b200 as tb
+    from taco_b200.workloads import spin_boson_batch
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
@@ -237,24 +219,6 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
-
-    B = args.instances
-    rng = np.random.default_rng(args.seed + 1000 * rank)
-    params = draw_params(rng, B)
-    systems, gammas = [], []
-    for prm in params:
-        s = tb.System(0.5 * prm["eps"] * SZ + 0.5 * prm["delta"] * SX, [SZ])
-        systems.append(s)
-        gammas.append(make_gamma_device(torch, s, prm, args.N, args.dt, device))
-    T = args.tmax + 1
-    tidx = np.arange(T, dtype=np.uint32)
-    N2 = 4
-    outs32 = [torch.empty((T, N2 * N2), dtype=torch.complex64, device=device) for _ in range(B)]
-    inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
-    torch.cuda.synchronize()
-
-    def step32():
-        tb.build_instances(inst, precision="fp32", outs=outs32)
 
     def barrier():
         if dist is not None:
@@ -267,8 +231,20 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    B = args.instances
+    params, systems, gammas = spin_boson_batch(torch, B, args.N, args.dt, seed=args.seed + 1000 * rank,
+                                               device=device)
+    T = args.tmax + 1
+    tidx = np.arange(T, dtype=np.uint32)
+    N2 = 4
+    outs32 = [torch.empty((T, N2 * N2), dtype=torch.complex64, device=device) for _ in range(B)]
+    inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
+    torch.cuda.synchronize()
+
+    # ---- headline: the batching form, prepared once and replayed as one CUDA graph ----
+    plan32 = tb.Tcl4Plan(inst, precision="fp32", outs=outs32)
     for _ in range(args.warmup):
-        step32()
+        plan32.run()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -278,7 +254,7 @@ def main():
     with ClockSampler(local) as clk:
         ev0.record()
         for _ in range(args.steps):
-            step32()
+            plan32.run()
         ev1.record()
         torch.cuda.synchronize()
     launches = tb.kernel_launches() - launches0
@@ -287,36 +263,37 @@ def main():
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
     value = world * B * T / (ms / 1e3)
 
-    # per-kernel device time of one more step (CUDA events around each launch)
+    # per-kernel device time of one more step (the same launches, not graph-captured)
     with tb.profile() as prof:
-        step32()
-    # plain FP64 path: one instance per call
+        tb.build_instances(inst, precision="fp32", outs=outs32)
+    direct32_ms = max_over_ranks(timed(torch, lambda: tb.build_instances(inst, precision="fp32", outs=outs32), 2))
+
+    # ---- plain FP64 path: one instance per call (replayed plan, and the direct call) ----
     P = min(args.plain_instances, B)
     outs64 = [torch.empty((T, N2 * N2), dtype=torch.complex128, device=device) for _ in range(P)]
-    for k in range(P):
-        tb.build_TCL4_generator_batch(systems[k], gammas[k], args.dt, tidx, precision="fp64", out=outs64[k])
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for k in range(P):
-        tb.build_TCL4_generator_batch(systems[k], gammas[k], args.dt, tidx, precision="fp64", out=outs64[k])
-    e1.record()
-    torch.cuda.synchronize()
-    ms64 = max_over_ranks(e0.elapsed_time(e1) / P)
+    plans64 = [tb.Tcl4Plan([inst[k]], precision="fp64", outs=[outs64[k]]) for k in range(P)]
+    ms64 = max_over_ranks(timed(torch, lambda: [p.run() for p in plans64], 3) / P)
+    ms64_direct = max_over_ranks(timed(torch, lambda: [tb.build_TCL4_generator_batch(
+        systems[k], gammas[k], args.dt, tidx, precision="fp64", out=outs64[k]) for k in range(P)], 2) / P)
     plain_value = T / (ms64 / 1e3)
     err32 = max(float(torch.linalg.vector_norm(outs32[k].to(torch.complex128) - outs64[k])
                       / torch.linalg.vector_norm(outs64[k])) for k in range(P))
-    causal_ms = None
-    for _ in range(2):
-        e0.record()
-        tb.build_TCL4_generator_batch(systems[0], gammas[0], args.dt, tidx, precision="fp64",
-                                      causal_truncation=True, out=outs64[0])
-        e1.record()
-        torch.cuda.synchronize()
-        causal_ms = e0.elapsed_time(e1)
 
-    # end to end through the C-ABI with pinned host buffers (H2D of Gamma, D2H of L4 inside)
+    # ---- the same work with the reference's FFT length (2^19 from Nt), labelled separately ----
+    Bf = min(B, 64)
+    outs32f = [torch.empty((T, N2 * N2), dtype=torch.complex64, device=device) for _ in range(Bf)]
+    plan32f = tb.Tcl4Plan(inst[:Bf], precision="fp32", outs=outs32f, full_length=True)
+    ms_full = max_over_ranks(timed(torch, plan32f.run, 2))
+    plan64f = tb.Tcl4Plan([inst[0]], precision="fp64", outs=[outs64[0]], full_length=True)
+    ms64_full = max_over_ranks(timed(torch, plan64f.run, 3))
+    torch.cuda.synchronize()
+    full_err = float(torch.linalg.vector_norm(outs32f[0].to(torch.complex128) - outs64[0])
+                     / torch.linalg.vector_norm(outs64[0]))
+    for p in plans64:
+        p.run()  # restore the truncated-path result in outs64 for the parity checks below
+    torch.cuda.synchronize()
+
+    # ---- end to end through the C-ABI with pinned host buffers (H2D of Gamma, D2H of L4) ----
     host_g = [g.cpu().pin_memory() for g in gammas]
     host_out = [torch.empty((T, N2 * N2), dtype=torch.complex64).pin_memory() for _ in range(B)]
     inst_h = [(s, hg.numpy(), args.dt, tidx) for s, hg in zip(systems, host_g)]
@@ -327,71 +304,88 @@ def main():
     for _ in range(args.e2e_steps):
         tb.build_instances(inst_h, precision="fp32", outs=outs_h)
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.e2e_steps)
-    h2d = sum(g.numel() * 16 for g in gammas)
+    h2d = sum(g.shape[0] * T * 16 for g in gammas)  # the consumed samples t <= tmax of every bucket
     d2h = B * T * N2 * N2 * 8
     e2e_value = world * B * T / (e2e_ms / 1e3)
     err_e2e = float(np.abs(outs_h[0] - outs32[0].cpu().numpy()).max())
 
-    # roofline of the dominant kernel
+    # ---- roofline of the dominant kernel ----
     peaks, peak_kind = measured_peaks()
-    nfft = 1 << (2 * (args.N + 1) - 1).bit_length()
-    shape = (args.N + 1, nfft, T, T, 3)
+    nfft = 1 << (2 * T - 2).bit_length()  # next_pow2(2 (tmax+1) - 1)
+    shape = (T, nfft, T, T, 3)
     units_total = {"triple": B * 27, "spectrum": B * 6}
-    dom = max(prof.entries.items(), key=lambda kv: kv[1][1]) if prof.entries else None
-    roofline = None
+    tot_all = sum(v[1] for v in prof.entries.values()) or 1.0
     kernels = {}
     for name, (n, tot) in prof.entries.items():
         per_unit, unit = kernel_model_bytes(name, shape)
-        ent = {"launches": n, "total_ms": round(tot, 4), "share": round(tot / sum(v[1] for v in prof.entries.values()), 4)}
+        ent = {"launches": n, "total_ms": round(tot, 4), "share": round(tot / tot_all, 4)}
         if per_unit:
             ent["gbs"] = round(per_unit * units_total[unit] / (tot / 1e3) / 1e9, 1)
         kernels[name] = ent
-    if dom is not None:
-        name, (n, tot) = dom
+    roofline = None
+    ranked = sorted(prof.entries.items(), key=lambda kv: -kv[1][1])
+    for name, (n, tot) in ranked:
         per_unit, unit = kernel_model_bytes(name, shape)
-        if per_unit:
-            per_launch = per_unit * units_total[unit] / n
-            avg_s = tot / n / 1e3
-            achieved = per_launch / avg_s / 1e9
-            tr = ncu_traffic().get(name.rsplit("_", 1)[0] + "_" + name.rsplit("_", 1)[1])
-            roofline = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1),
-                        "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
-                        "peak_source": peak_kind,
-                        "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": round(tot / n, 4),
-                        "traffic": (tr * units_total[unit] / n) if tr else None}
+        if not per_unit:
+            continue
+        per_launch = per_unit * units_total[unit] / n
+        achieved = per_launch / (tot / n / 1e3) / 1e9
+        tr = ncu_traffic().get(name)
+        roofline = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
+                    "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_kind,
+                    "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": round(tot / n, 4),
+                    "share_of_step": round(tot / tot_all, 4),
+                    "traffic": (tr * units_total[unit] / n) if tr else None}
+        break
 
     cpu = None
-    fp64_vs_oracle = None
+    fp64_parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
         s0 = systems[0]
         G0 = gammas[0].cpu().numpy()
+        p2f = np.ascontiguousarray(s0.pair_to_freq.T, np.int32)
+        ops = np.ascontiguousarray(np.stack([A.T for A in s0.A_eig]))
         t0 = time.perf_counter()
-        L4o = oracle.tcl4_build_batch(s0.N, s0.nf, s0.omegas, s0.mirror,
-                                      np.ascontiguousarray(s0.pair_to_freq.T, np.int32),
-                                      np.ascontiguousarray(np.stack([A.T for A in s0.A_eig])), G0, args.dt, tidx=tidx)
+        L4o = oracle.tcl4_build_batch(s0.N, s0.nf, s0.omegas, s0.mirror, p2f, ops, G0, args.dt, tidx=tidx)
         sec = time.perf_counter() - t0
         cpu = {"value": T / sec, "unit": "builds/s", "cores": oracle.max_threads(), "kind": "port",
-               "sample": f"1 instance ({T} L4 builds, all 27 triples, FFT 2^19) of the {B}-instance step"}
+               "sample": f"1 instance ({T} L4 builds, all 27 triples, FFT 2^19 as the reference) of the "
+                         f"{B}-instance step"}
+        # exact reference at t <= tmax: the Direct method on the causally truncated series
+        L4d = oracle.tcl4_build_batch(s0.N, s0.nf, s0.omegas, s0.mirror, p2f, ops, np.ascontiguousarray(G0[:, :T]),
+                                      args.dt, tidx=tidx, method=oracle.FCR_DIRECT)
         g64 = outs64[0].view(T, N2, N2).transpose(1, 2).cpu().numpy()
-        fp64_vs_oracle = float(np.linalg.norm(g64 - L4o) / np.linalg.norm(L4o))
+        g32 = outs32[0].view(T, N2, N2).transpose(1, 2).cpu().numpy()
+
+        def re(a, b):
+            return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+        fp64_parity = {"vs_oracle_convolution": re(g64, L4o), "vs_oracle_direct": re(g64, L4d),
+                       "oracle_convolution_vs_direct": re(L4o, L4d), "fp32_vs_oracle_direct": re(g32, L4d)}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{B} spin-boson instances per GPU (d=2, nf=3), N={args.N} (Nt={args.N + 1}, "
-                                   f"FFT 2^{nfft.bit_length() - 1}), dt={args.dt}, tidx 0..{args.tmax}, "
-                                   "batched FP32 form",
+            "config": {"workload": f"{B} spin-boson instances per GPU (d=2, nf=3), N={args.N} (Nt={args.N + 1}), "
+                                   f"dt={args.dt}, tidx 0..{args.tmax}, batched FP32 form, one CUDA-graph replay "
+                                   f"per step, FFT length 2^{nfft.bit_length() - 1} from max(tidx)+1",
                        "instances_per_gpu": B, "builds_per_instance": T,
-                       "l2": "inputs larger than L2 (Gamma 9.6 MB x instances, spectra 24 MB per instance)",
+                       "l2": "inputs larger than L2 (Gamma 9.6 MB x instances; L4 outputs 1.3 MB x instances)",
                        "parallelism": f"instance-sharded x{world}"},
             "plain_fp64": {"value": plain_value, "unit": "builds/s", "ms_per_instance": ms64,
-                           "instances": P, "causal_truncation_ms_per_instance": causal_ms},
+                           "ms_per_instance_direct_call": ms64_direct, "instances": P},
             "speedup_vs_plain_fp64": value / (world * plain_value),
             "fp32_rel_err_vs_fp64": err32,
-            "fp64_rel_err_vs_oracle": fp64_vs_oracle,
+            "fp64_parity": fp64_parity,
+            "direct_call_ms_per_step": direct32_ms,
+            "full_length_fft": {"note": "FFT length 2^19 from Nt as the reference; same results",
+                                "value": world * Bf * T / (ms_full / 1e3), "instances": Bf, "ms_per_step": ms_full,
+                                "plain_fp64_value": T / (ms64_full / 1e3),
+                                "speedup_vs_plain_fp64": (Bf * T / (ms_full / 1e3)) / (T / (ms64_full / 1e3)),
+                                "fp32_rel_err_vs_fp64": full_err},
             "e2e": {"value": e2e_value, "unit": "builds/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms, "max_abs_diff_vs_device_run": err_e2e},
             "roofline": roofline, "kernels": kernels,
@@ -400,6 +394,8 @@ def main():
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
+    for p in [plan32, plan32f, plan64f, *plans64]:
+        p.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -58,7 +58,8 @@ enum { TACO_PREC_FP64 = 0, TACO_PREC_FP32 = 1 };
 enum {
     TACO_IN_DEVICE = 1,          /* gamma (and RK4 inputs) are device pointers */
     TACO_OUT_DEVICE = 2,         /* outputs are device pointers */
-    TACO_CAUSAL_TRUNCATION = 4   /* FFT length from max(tidx)+1 instead of Nt (same results) */
+    TACO_CAUSAL_TRUNCATION = 4,  /* (default) FFT length from max(tidx)+1: F/C/R(t) depend on gamma[0..t] only */
+    TACO_FULL_LENGTH_FFT = 8     /* FFT length from Nt, as the reference (same results, more work) */
 };
 
 /* What the device path reads from taco::sys::System (cpp/include/taco/system.hpp:201-226)
@@ -127,6 +128,18 @@ int taco_tcl4_correction_series(const taco_system_view* sys, const taco_c128* ga
 int taco_tcl4_build_instances(const taco_tcl4_instance* inst, size_t count, int method, int precision,
                               int flags, void* stream);
 
+/* Plans (no counterpart in the reference, whose fused path caches one CUDA graph per
+ * shape, cpp/src/backend/cuda/tcl4_fused_cuda.cu:164-191): validate and prepare a batched
+ * build once -- metadata and job tables resident on the device, the whole launch sequence
+ * captured in a CUDA graph -- and replay it.  Inputs and outputs must be device pointers
+ * (TACO_IN_DEVICE | TACO_OUT_DEVICE); they are bound at creation.  taco_tcl4_plan_execute
+ * is asynchronous on `stream`. */
+typedef struct taco_tcl4_plan taco_tcl4_plan;
+int taco_tcl4_plan_create(const taco_tcl4_instance* inst, size_t count, int method, int precision, int flags,
+                          taco_tcl4_plan** plan);
+int taco_tcl4_plan_execute(taco_tcl4_plan* plan, void* stream);
+int taco_tcl4_plan_destroy(taco_tcl4_plan* plan);
+
 /* propagate_rk4_dense_serial/_omp(L_series[, L_half_series], r, t0, dt, on_sample, sample_every)
  * (cpp/include/taco/rk4_dense.hpp:85-100, 114-129) on the device.
  * L_series: [steps+1][D x D]; L_half: [steps][D x D] or NULL (midpoints by averaging);
@@ -147,6 +160,16 @@ int taco_rk4_propagate(const void* L_series, const void* L_half, const void* L_a
  * exceeds cap only nnz is written). */
 int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t* src, taco_c128* coef,
                          size_t cap, size_t* nnz);
+
+/* Launch schedule of the F/C/R passes for FFT length 2^log2_nfft and a precision, as chosen
+ * by the autotuner (taco_b200/autotune.py): column / row tile sizes in elements (powers of
+ * two in [8, 8192]), bytes of Z/W scratch per chunk of triples (sized to stay in L2), and
+ * the largest number of output rows for which the inverse column pass is a pruned direct
+ * DFT.  Unset lengths use the defaults (4096, 2048, 48 MiB, 16). */
+int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows);
+int taco_get_tuning(int log2_nfft, int precision, int* col_tile, int* row_tile, size_t* chunk_bytes,
+                    int* inv_dft_rows);
+int taco_clear_tuning(void);
 
 /* Kernel accounting (tracing).  taco_kernel_launches: kernels this library launched since
  * the process started.  With profiling on, every launch is bracketed by CUDA events and its

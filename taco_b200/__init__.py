@@ -33,11 +33,15 @@ from . import _capi
 from ._capi import (TacoError, TacoInvalidArgument, TacoOutOfRange, TacoOverflow,  # noqa: F401
                     TACO_PREC_FP32, TACO_PREC_FP64)
 from .inputs import System, bcf_fft, gamma_trapz, spin_boson_system  # noqa: F401
+from . import autotune as _autotune
+
+# persisted launch schedules measured by the autotuner (taco_b200/tuning.json)
+_autotune.load()
 
 __all__ = [
     "System", "bcf_fft", "gamma_trapz", "spin_boson_system", "compute_triple_kernels",
     "build_TCL4_generator", "build_TCL4_generator_batch", "build_correction_series", "build_instances",
-    "propagate_rk4_dense", "l4_coefficients", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
+    "propagate_rk4_dense", "l4_coefficients", "Tcl4Plan", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
     "version", "device_count", "kernel_launches", "profile",
 ]
 
@@ -186,12 +190,14 @@ def compute_triple_kernels(system: System, gamma, dt: float, nmax: int = 2, meth
 
 
 def build_TCL4_generator_batch(system: System, gamma, dt: float, time_indices=None, method: int = 0,
-                               precision: str = "fp64", causal_truncation: bool = False, out=None,
+                               precision: str = "fp64", full_length: bool = False, out=None,
                                return_fcr_ms: bool = False):
     """L4 at each requested time index (all of [0, Nt) when ``time_indices`` is None/empty).
 
     precision "fp64": complex128 (the plain path); "fp32": FP32 FFT convolutions and
-    contraction, FP64 phases and carries, complex64 results.
+    contraction, FP64 phases and carries, complex64 results.  The FFT length follows
+    max(time_indices)+1 (F/C/R(t) depend on gamma[0..t] only); ``full_length`` sizes it
+    from Nt as the reference does (same results, more work).
     """
     g, dev = _prep_gamma(gamma)
     nf, Nt = g.shape
@@ -205,8 +211,8 @@ def build_TCL4_generator_batch(system: System, gamma, dt: float, time_indices=No
     if out is None:
         out = _out_array(dev, (T, N2 * N2), dtype, g.device if dev else None)
     flags = (_capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE) if dev else 0
-    if causal_truncation:
-        flags |= _capi.TACO_CAUSAL_TRUNCATION
+    if full_length:
+        flags |= _capi.TACO_FULL_LENGTH_FFT
     v = _View(system)
     ms = ct.c_double(0.0)
     _capi.check(_capi.lib().taco_tcl4_build_batch(ct.byref(v.view), _ptr(g), Nt, float(dt), _ptr(tid),
@@ -229,10 +235,7 @@ def build_correction_series(system: System, gamma, dt: float, method: int = 0):
     return build_TCL4_generator_batch(system, gamma, dt, None, method)
 
 
-def build_instances(instances, precision: str = "fp64", method: int = 0, outs=None):
-    """Batching form: ``instances`` is a list of (system, gamma, dt, tidx); gammas all host
-    (numpy) or all device (torch CUDA).  Returns one [T, N^2, N^2] result per instance."""
-    prec = {"fp64": _capi.TACO_PREC_FP64, "fp32": _capi.TACO_PREC_FP32}[precision]
+def _instance_array(instances, prec, outs):
     dtype = np.complex128 if prec == _capi.TACO_PREC_FP64 else np.complex64
     arr = (_capi.Instance * len(instances))()
     keep = []
@@ -243,7 +246,7 @@ def build_instances(instances, precision: str = "fp64", method: int = 0, outs=No
         if dev is None:
             dev = d
         elif dev != d:
-            raise ValueError("build_instances: mix of host and device gamma")
+            raise ValueError("mix of host and device gamma")
         nf, Nt = g.shape
         tid = None if tidx is None or len(tidx) == 0 else np.ascontiguousarray(tidx, np.uint32)
         T = Nt if tid is None else tid.size
@@ -259,7 +262,55 @@ def build_instances(instances, precision: str = "fp64", method: int = 0, outs=No
         arr[k].T = 0 if tid is None else tid.size
         arr[k].L4_out = _ptr(o).value
         results.append(_l4_view(o, N2))
+    return arr, keep, results, bool(dev)
+
+
+class Tcl4Plan:
+    """A batched build prepared once and replayed as one CUDA graph (device tensors only).
+
+    >>> plan = Tcl4Plan([(system, gamma_cuda, dt, tidx), ...], precision="fp32")
+    >>> plan.run()          # asynchronous on the current torch stream
+    >>> plan.results[k]     # [T, N^2, N^2] views of the output buffers
+    """
+
+    def __init__(self, instances, precision: str = "fp32", method: int = 0, outs=None, full_length: bool = False):
+        prec = {"fp64": _capi.TACO_PREC_FP64, "fp32": _capi.TACO_PREC_FP32}[precision]
+        arr, self._keep, self.results, dev = _instance_array(instances, prec, outs)
+        if not dev:
+            raise ValueError("Tcl4Plan needs CUDA tensors for gamma")
+        flags = _capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE
+        if full_length:
+            flags |= _capi.TACO_FULL_LENGTH_FFT
+        self._h = ct.c_void_p()
+        _capi.check(_capi.lib().taco_tcl4_plan_create(arr, len(instances), int(method), prec, flags,
+                                                      ct.byref(self._h)))
+        self._stream_of = self._keep[0]
+
+    def run(self, stream=None):
+        s = _stream_ptr(self._stream_of) if stream is None else ct.c_void_p(stream)
+        _capi.check(_capi.lib().taco_tcl4_plan_execute(self._h, s))
+        return self.results
+
+    def close(self):
+        if self._h and self._h.value:
+            _capi.check(_capi.lib().taco_tcl4_plan_destroy(self._h))
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def build_instances(instances, precision: str = "fp64", method: int = 0, outs=None, full_length: bool = False):
+    """Batching form: ``instances`` is a list of (system, gamma, dt, tidx); gammas all host
+    (numpy) or all device (torch CUDA).  Returns one [T, N^2, N^2] result per instance."""
+    prec = {"fp64": _capi.TACO_PREC_FP64, "fp32": _capi.TACO_PREC_FP32}[precision]
+    arr, keep, results, dev = _instance_array(instances, prec, outs)
     flags = (_capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE) if dev else 0
+    if full_length:
+        flags |= _capi.TACO_FULL_LENGTH_FFT
     _capi.check(_capi.lib().taco_tcl4_build_instances(arr, len(instances), int(method), prec, flags,
                                                       _stream_ptr(keep[0]) if keep else None))
     return results

@@ -23,6 +23,7 @@ TACO_PREC_FP32 = 1
 TACO_IN_DEVICE = 1
 TACO_OUT_DEVICE = 2
 TACO_CAUSAL_TRUNCATION = 4
+TACO_FULL_LENGTH_FFT = 8
 
 # every symbol the header declares
 EXPORTED = [
@@ -31,6 +32,8 @@ EXPORTED = [
     "taco_tcl4_build_batch", "taco_tcl4_build", "taco_tcl4_correction_series",
     "taco_tcl4_build_instances", "taco_rk4_propagate", "taco_l4_coefficients",
     "taco_kernel_launches", "taco_profile_enable", "taco_profile_reset", "taco_profile_get",
+    "taco_set_tuning", "taco_get_tuning", "taco_clear_tuning",
+    "taco_tcl4_plan_create", "taco_tcl4_plan_execute", "taco_tcl4_plan_destroy",
 ]
 
 
@@ -103,6 +106,13 @@ def lib():
         L.taco_profile_enable.argtypes = [ct.c_int]
         L.taco_profile_get.argtypes = [ct.c_size_t, ct.POINTER(ct.c_char_p), ct.POINTER(ct.c_uint64),
                                        ct.POINTER(ct.c_double), ct.POINTER(ct.c_size_t)]
+        L.taco_set_tuning.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_size_t, ct.c_int]
+        L.taco_get_tuning.argtypes = [ct.c_int, ct.c_int, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
+                                      ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_int)]
+        L.taco_tcl4_plan_create.argtypes = [ct.POINTER(Instance), ct.c_size_t, ct.c_int, ct.c_int, ct.c_int,
+                                            ct.POINTER(ct.c_void_p)]
+        L.taco_tcl4_plan_execute.argtypes = [ct.c_void_p, ct.c_void_p]
+        L.taco_tcl4_plan_destroy.argtypes = [ct.c_void_p]
         _lib = L
     return _lib
 

@@ -80,7 +80,7 @@ taco::BuildOptions options(int precision, int flags, double* fcr_ms) {
         throw taco::Error(taco::kInvalidArgument, "precision must be TACO_PREC_FP64 or TACO_PREC_FP32");
     taco::BuildOptions o;
     o.fp32 = (precision == TACO_PREC_FP32);
-    o.causal_truncation = (flags & TACO_CAUSAL_TRUNCATION) != 0;
+    o.causal_truncation = (flags & TACO_FULL_LENGTH_FFT) == 0;
     o.pad_factor = g_pad_factor.load();
     o.fcr_ms = fcr_ms;
     return o;
@@ -93,6 +93,24 @@ void fill_tidx(taco::Tcl4Instance& in, const uint32_t* tidx, std::size_t T) {
     } else {
         in.tidx.assign(tidx, tidx + T);
     }
+}
+
+std::vector<taco::Tcl4Instance> to_instances(const taco_tcl4_instance* inst, size_t count, int flags) {
+    if (count > 0 && !inst) throw taco::Error(taco::kInvalidArgument, "instances is null");
+    std::vector<taco::Tcl4Instance> insts(count);
+    for (std::size_t k = 0; k < count; ++k) {
+        taco::Tcl4Instance& in = insts[k];
+        in.sys = to_desc(&inst[k].sys);
+        in.gamma = reinterpret_cast<const double2*>(inst[k].gamma);
+        in.gamma_on_device = (flags & TACO_IN_DEVICE) != 0;
+        in.Nt = inst[k].Nt;
+        in.dt = inst[k].dt;
+        if (in.Nt == 0) throw taco::Error(taco::kInvalidArgument, "empty gamma_series");
+        fill_tidx(in, inst[k].tidx, inst[k].T);
+        in.out = inst[k].L4_out;
+        in.out_on_device = (flags & TACO_OUT_DEVICE) != 0;
+    }
+    return insts;
 }
 
 }  // namespace
@@ -178,21 +196,40 @@ int taco_tcl4_build_instances(const taco_tcl4_instance* inst, size_t count, int 
     return guarded([&] {
         check_method(method);
         require_device();
-        if (count > 0 && !inst) throw taco::Error(taco::kInvalidArgument, "instances is null");
-        std::vector<taco::Tcl4Instance> insts(count);
-        for (std::size_t k = 0; k < count; ++k) {
-            taco::Tcl4Instance& in = insts[k];
-            in.sys = to_desc(&inst[k].sys);
-            in.gamma = reinterpret_cast<const double2*>(inst[k].gamma);
-            in.gamma_on_device = (flags & TACO_IN_DEVICE) != 0;
-            in.Nt = inst[k].Nt;
-            in.dt = inst[k].dt;
-            if (in.Nt == 0) throw taco::Error(taco::kInvalidArgument, "empty gamma_series");
-            fill_tidx(in, inst[k].tidx, inst[k].T);
-            in.out = inst[k].L4_out;
-            in.out_on_device = (flags & TACO_OUT_DEVICE) != 0;
-        }
+        std::vector<taco::Tcl4Instance> insts = to_instances(inst, count, flags);
         taco::tcl4_build(insts, options(precision, flags, nullptr), static_cast<cudaStream_t>(stream));
+    });
+}
+
+struct taco_tcl4_plan {
+    taco::Tcl4Plan* p;
+};
+
+int taco_tcl4_plan_create(const taco_tcl4_instance* inst, size_t count, int method, int precision, int flags,
+                          taco_tcl4_plan** plan) {
+    return guarded([&] {
+        if (!plan) throw taco::Error(taco::kInvalidArgument, "plan is null");
+        *plan = nullptr;
+        check_method(method);
+        require_device();
+        std::vector<taco::Tcl4Instance> insts = to_instances(inst, count, flags);
+        taco::Tcl4Plan* p = taco::plan_create(insts, options(precision, flags, nullptr));
+        *plan = new taco_tcl4_plan{p};
+    });
+}
+
+int taco_tcl4_plan_execute(taco_tcl4_plan* plan, void* stream) {
+    return guarded([&] {
+        if (!plan) throw taco::Error(taco::kInvalidArgument, "plan is null");
+        taco::plan_execute(plan->p, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int taco_tcl4_plan_destroy(taco_tcl4_plan* plan) {
+    return guarded([&] {
+        if (!plan) return;
+        taco::plan_destroy(plan->p);
+        delete plan;
     });
 }
 
@@ -286,6 +323,33 @@ int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t*
             if (coef) std::memcpy(coef, t.coef.data(), t.coef.size() * sizeof(taco_c128));
         }
     });
+}
+
+int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows) {
+    return guarded([&] {
+        if (log2_nfft < 3 || log2_nfft > 22) throw taco::Error(taco::kInvalidArgument, "tuning: log2_nfft out of range");
+        taco::Tuning t;
+        t.col_tile = col_tile;
+        t.row_tile = row_tile;
+        t.chunk_bytes = chunk_bytes;
+        t.inv_dft_rows = inv_dft_rows;
+        taco::set_tuning(log2_nfft, precision == TACO_PREC_FP32, t);
+    });
+}
+
+int taco_get_tuning(int log2_nfft, int precision, int* col_tile, int* row_tile, size_t* chunk_bytes,
+                    int* inv_dft_rows) {
+    return guarded([&] {
+        const taco::Tuning t = taco::get_tuning(log2_nfft, precision == TACO_PREC_FP32);
+        if (col_tile) *col_tile = t.col_tile;
+        if (row_tile) *row_tile = t.row_tile;
+        if (chunk_bytes) *chunk_bytes = t.chunk_bytes;
+        if (inv_dft_rows) *inv_dft_rows = t.inv_dft_rows;
+    });
+}
+
+int taco_clear_tuning(void) {
+    return guarded([&] { taco::clear_tuning(); });
 }
 
 int taco_kernel_launches(uint64_t* launches) {

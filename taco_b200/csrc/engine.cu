@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <functional>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -32,8 +33,15 @@ namespace {
 std::atomic<uint64_t> g_launches{0};
 std::atomic<bool> g_profile{false};
 
-constexpr int kColTile = 4096;  // elements per column-pass tile
-constexpr int kRowTile = 2048;  // elements per row-pass tile (two tiles in shared memory)
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, Tuning> g_tune;  // (L, fp32) -> schedule set by the autotuner
+
+Tuning tuning_for(int L, bool fp32) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find({L, fp32 ? 1 : 0});
+    if (it != g_tune.end()) return it->second;
+    return Tuning{};
+}
 
 std::size_t align_up(std::size_t x, std::size_t a) { return (x + a - 1) / a * a; }
 
@@ -181,23 +189,27 @@ void set_smem(K kernel, std::size_t bytes) {
 }
 
 struct Geometry {
-    int col_cols, col_threads, row_rows, row_threads;
+    int log2c, col_threads, log2r, row_threads;
     std::size_t col_smem, row_smem;
     unsigned col_grid, row_grid;
 };
 
+// Tile shapes: column tiles of col_tile elements (N1 rows x 2^log2c columns), row tiles
+// of row_tile elements (2^log2r rows of N2), both padded in shared memory.
 template <class C>
-Geometry geometry(const FftPlan<C>& p) {
+Geometry geometry(const FftPlan<C>& p, int col_tile, int row_tile) {
     Geometry g;
     const int N1 = 1 << p.L1, N2 = 1 << p.L2;
-    g.col_cols = std::max(1, std::min(N2, kColTile / N1));
-    g.col_threads = N1 * g.col_cols / 8;
-    g.col_smem = static_cast<std::size_t>(N1) * g.col_cols * sizeof(C);
-    g.col_grid = static_cast<unsigned>(N2 / g.col_cols);
-    g.row_rows = std::max(1, std::min(N1, kRowTile / N2));
-    g.row_threads = N2 * g.row_rows / 8;
-    g.row_smem = 2 * static_cast<std::size_t>(N2) * g.row_rows * sizeof(C);
-    g.row_grid = static_cast<unsigned>(N1 / g.row_rows);
+    const int cc = std::max(1, std::min(N2, col_tile / N1));
+    g.log2c = ilog2(static_cast<std::size_t>(cc));
+    g.col_threads = (N1 << g.log2c) / 8;
+    g.col_smem = static_cast<std::size_t>(padded_size<C>(N1 << g.log2c)) * sizeof(C);
+    g.col_grid = static_cast<unsigned>(N2 >> g.log2c);
+    const int rr = std::max(1, std::min(N1, row_tile / N2));
+    g.log2r = ilog2(static_cast<std::size_t>(rr));
+    g.row_threads = (N2 << g.log2r) / 8;
+    g.row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << g.log2r)) * sizeof(C);
+    g.row_grid = static_cast<unsigned>(N1 >> g.log2r);
     return g;
 }
 
@@ -222,7 +234,7 @@ struct ProfRecorder {
     const char* pending = nullptr;
     cudaEvent_t pend_a = nullptr;
     void before(const char* name) {
-        if (!g_profile.load()) return;
+        if (!g_profile.load() || st == nullptr) return;
         cuda_check(cudaEventCreate(&pend_a), "cudaEventCreate(prof)");
         cuda_check(cudaEventRecord(pend_a, st), "cudaEventRecord(prof)");
         pending = name;
@@ -305,15 +317,22 @@ struct TripleRef {
     int tri;  // (i*nf + j)*nf + k
 };
 
-// Core of one group (equal FFT length).  `fcr_only` writes F/C/R series (FP64) straight
-// into caller buffers instead of running the contraction.
+// One group (instances with equal FFT length): lays out `mem`, stages the small
+// metadata and the host inputs (stream-ordered on `st`), and returns the closure that
+// enqueues the group's kernels (and the D2H copies of host outputs) on a stream.
+// `fcr_out` (non-null) writes the F/C/R series (FP64) into caller buffers instead of
+// running the contraction.
+using Enqueue = std::function<void(cudaStream_t, ProfRecorder*, cudaEvent_t, cudaEvent_t)>;
+
 template <class R>
-void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas, const BuildOptions& opt,
-               cudaStream_t st, Workspace& ws, double2* const* fcr_out, bool fcr_out_dev) {
+Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas, const BuildOptions& opt,
+                      cudaStream_t st, Workspace& ws, DeviceBuffer& mem, double2* const* fcr_out,
+                      bool fcr_out_dev) {
     using C = cplx_t<R>;
     const int L = metas[0]->L;
     const FftPlan<C> plan = get_plan<R>(ws, L, st);
-    const Geometry g = geometry(plan);
+    const Tuning tune = tuning_for(L, std::is_same<R, float>::value);
+    const Geometry g = geometry(plan, tune.col_tile, tune.row_tile);
     const std::size_t Nfft = std::size_t(1) << L;
     const std::size_t ni = insts.size();
     const bool fcr_only = (fcr_out != nullptr);
@@ -325,10 +344,17 @@ void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas,
         for (int t = 0; t < nf3; ++t) tris.push_back({static_cast<int>(a), t});
     }
     const std::size_t ntri = tris.size();
+    // chunk of triples whose Z / W intermediates are meant to stay in L2 between passes
     const std::size_t per_tri_scratch = 2 * Nfft * sizeof(C);
-    std::size_t Q = std::max<std::size_t>(1, opt.scratch_budget / per_tri_scratch);
+    std::size_t Q = std::max<std::size_t>(1, tune.chunk_bytes / per_tri_scratch);
     Q = std::min<std::size_t>({Q, ntri, 65535});
     const std::size_t nchunks = (ntri + Q - 1) / Q;
+    // inverse column pass: pruned direct DFT when only a few output rows are needed
+    std::size_t max_tcount = 0;
+    for (auto* m : metas) max_tcount = std::max(max_tcount, m->t_count);
+    const int N2 = 1 << plan.L2;
+    const int inv_rows = static_cast<int>((max_tcount + N2 - 1) / N2);
+    const bool inv_dft = inv_rows <= std::min(tune.inv_dft_rows, INV_DFT_MAXR);
 
     // ---- device layout ----
     struct Ptrs {
@@ -371,7 +397,7 @@ void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas,
             const Tcl4Instance& in = *insts[a];
             const InstMeta& m = *metas[a];
             const std::size_t nf = in.sys.nf, nf3 = nf * nf * nf;
-            if (!in.gamma_on_device) P.gamma[a] = lay.take<double2>(nf * in.Nt);
+            if (!in.gamma_on_device) P.gamma[a] = lay.take<double2>(nf * m.n_in);
             P.spec[a] = lay.take<C>(2 * nf * Nfft);
             P.conv[a] = lay.take<C>(nf3 * 2 * m.t_count);
             P.tmap[a] = lay.take<int>(m.t_count);
@@ -398,11 +424,15 @@ void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas,
     };
     Layout meas;
     layout(meas);
-    ws.arena.ensure(meas.off);
-    Layout lay{static_cast<char*>(ws.arena.p)};
+    mem.ensure(meas.off);
+    Layout lay{static_cast<char*>(mem.p)};
     layout(lay);
-    for (std::size_t a = 0; a < ni; ++a)
+    // column stride of gamma on the device: Nt for caller buffers, n_in for staged host input
+    std::vector<std::size_t> gs(ni);
+    for (std::size_t a = 0; a < ni; ++a) {
         if (insts[a]->gamma_on_device) P.gamma[a] = insts[a]->gamma;
+        gs[a] = insts[a]->gamma_on_device ? insts[a]->Nt : metas[a]->n_in;
+    }
 
     // ---- host staging of small metadata (one pinned buffer, one copy per array) ----
     std::vector<ColJob> colj(n_col_jobs);
@@ -418,7 +448,7 @@ void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas,
         for (int half = 0; half < 2; ++half)
             for (int b = 0; b < nf; ++b) {
                 ColJob& c = colj[cj];
-                c.g = P.gamma[a] + static_cast<std::size_t>(b) * in.Nt;
+                c.g = P.gamma[a] + static_cast<std::size_t>(b) * gs[a];
                 c.omega = 0.0;
                 c.dt = in.dt;
                 c.has_phase = 0;
@@ -441,7 +471,7 @@ void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas,
         C* z = P.scratch + slot * 2 * Nfft;
         C* wcb = z + Nfft;
         ColJob& c = colj[n_spec_jobs + q];
-        c.g = P.gamma[a] + static_cast<std::size_t>(i) * in.Nt;
+        c.g = P.gamma[a] + static_cast<std::size_t>(i) * gs[a];
         c.omega = w;
         c.dt = in.dt;
         c.has_phase = 1;
@@ -456,11 +486,12 @@ void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas,
         invj[2 * q] = InvJob{z, cf, static_cast<uint32_t>(m.t_count), scale};
         invj[2 * q + 1] = InvJob{wcb, cc, static_cast<uint32_t>(m.t_count), scale};
         ScanJob& s = scanj[q];
-        s.gi = P.gamma[a] + static_cast<std::size_t>(i) * in.Nt;
-        s.gj = P.gamma[a] + static_cast<std::size_t>(j) * in.Nt;
-        s.gmj = P.gamma[a] + static_cast<std::size_t>(jm) * in.Nt;
+        s.gi = P.gamma[a] + static_cast<std::size_t>(i) * gs[a];
+        s.gj = P.gamma[a] + static_cast<std::size_t>(j) * gs[a];
+        s.gmj = P.gamma[a] + static_cast<std::size_t>(jm) * gs[a];
         s.omega = w;
         s.dt = in.dt;
+        s.n_in = static_cast<uint32_t>(m.n_in);
         s.t_count = static_cast<uint32_t>(m.t_count);
         s.conv_f = cf;
         s.conv_c = cc;
@@ -556,74 +587,106 @@ void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas,
     }
     for (const Copy& c : copies)
         cuda_check(cudaMemcpyAsync(c.dst, sb + c.off, c.bytes, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(meta)");
+    // host gamma: only the n_in leading samples of each bucket are consumed
     for (std::size_t a = 0; a < ni; ++a)
         if (!insts[a]->gamma_on_device)
-            cuda_check(cudaMemcpyAsync(const_cast<double2*>(P.gamma[a]), insts[a]->gamma,
-                                       insts[a]->sys.nf * insts[a]->Nt * sizeof(double2), cudaMemcpyHostToDevice, st),
-                       "cudaMemcpyAsync(gamma)");
+            cuda_check(cudaMemcpy2DAsync(const_cast<double2*>(P.gamma[a]), gs[a] * sizeof(double2), insts[a]->gamma,
+                                         insts[a]->Nt * sizeof(double2), metas[a]->n_in * sizeof(double2),
+                                         insts[a]->sys.nf, cudaMemcpyHostToDevice, st),
+                       "cudaMemcpy2DAsync(gamma)");
+
+    // the pinned staging buffer is reused by the next call: wait for the copies
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(meta)");
 
     // ---- launches ----
     set_smem(k_fwd_col<R>, g.col_smem);
     set_smem(k_inv_col<R>, g.col_smem);
     set_smem(k_row<R>, g.row_smem);
-    ProfRecorder pr;
-    pr.st = st;
-    const bool f32 = std::is_same<R, float>::value;
-    if (opt.fcr_ms) cuda_check(cudaEventRecord(ws.ev0, st), "cudaEventRecord");
-    pr.before(f32 ? "spectra_col_f32" : "spectra_col_f64");
-    k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(n_spec_jobs)), g.col_threads, g.col_smem, st>>>(
-        P.colj, plan, g.col_cols);
-    check_launch("k_fwd_col(spectra)", &pr);
-    pr.before(f32 ? "spectra_row_f32" : "spectra_row_f64");
-    k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
-        P.rowj, plan, g.row_rows);
-    check_launch("k_row(spectra)", &pr);
-    for (std::size_t ch = 0; ch < nchunks; ++ch) {
-        const std::size_t q0 = ch * Q, nq = std::min(Q, ntri - q0);
-        pr.before(f32 ? "fwd_col_f32" : "fwd_col_f64");
-        k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(nq)), g.col_threads, g.col_smem, st>>>(
-            P.colj + n_spec_jobs + q0, plan, g.col_cols);
-        check_launch("k_fwd_col", &pr);
-        pr.before(f32 ? "row_conv_f32" : "row_conv_f64");
-        k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
-            P.rowj + n_spec_jobs + q0, plan, g.row_rows);
-        check_launch("k_row", &pr);
-        pr.before(f32 ? "inv_col_f32" : "inv_col_f64");
-        k_inv_col<R><<<dim3(g.col_grid, static_cast<unsigned>(2 * nq)), g.col_threads, g.col_smem, st>>>(
-            P.invj + 2 * q0, plan, g.col_cols);
-        check_launch("k_inv_col", &pr);
-    }
-    pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
-    k_scan_assemble<R><<<static_cast<unsigned>(ntri), SCAN_THREADS, 0, st>>>(P.scanj);
-    check_launch("k_scan_assemble", &pr);
-    if (opt.fcr_ms) cuda_check(cudaEventRecord(ws.ev1, st), "cudaEventRecord");
+    int maxE = 0;
+    for (auto* in : insts) maxE = std::max(maxE, in->sys.N * in->sys.N * in->sys.N * in->sys.N);
+    const int OT = std::max(1, std::min(128, static_cast<int>((48 * 1024) / (maxE * sizeof(C)))));
+    std::size_t maxT = 0;
+    for (auto* m : metas) maxT = std::max(maxT, m->T);
+    const std::size_t csmem = static_cast<std::size_t>(OT) * maxE * sizeof(C);
+    set_smem(k_contract<R>, csmem);
+    struct D2H {
+        void* dst;
+        const void* src;
+        std::size_t bytes;
+    };
+    std::vector<D2H> d2h;
     if (!fcr_only) {
-        int maxE = 0;
-        for (auto* in : insts) maxE = std::max(maxE, in->sys.N * in->sys.N * in->sys.N * in->sys.N);
-        const int OT = std::max(1, std::min(128, static_cast<int>((48 * 1024) / (maxE * sizeof(C)))));
-        std::size_t maxT = 0;
-        for (auto* m : metas) maxT = std::max(maxT, m->T);
-        const std::size_t smem = static_cast<std::size_t>(OT) * maxE * sizeof(C);
-        set_smem(k_contract<R>, smem);
-        const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
-        pr.before(f32 ? "contract_f32" : "contract_f64");
-        k_contract<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, smem, st>>>(P.conj, OT);
-        check_launch("k_contract", &pr);
         for (std::size_t a = 0; a < ni; ++a) {
             if (insts[a]->out_on_device) continue;
-            const std::size_t E = static_cast<std::size_t>(insts[a]->sys.N) * insts[a]->sys.N * insts[a]->sys.N * insts[a]->sys.N;
-            cuda_check(cudaMemcpyAsync(insts[a]->out, P.out[a], metas[a]->T * E * sizeof(C), cudaMemcpyDeviceToHost, st),
-                       "cudaMemcpyAsync(L4 out)");
+            const std::size_t E = static_cast<std::size_t>(insts[a]->sys.N) * insts[a]->sys.N * insts[a]->sys.N *
+                                  insts[a]->sys.N;
+            d2h.push_back({insts[a]->out, P.out[a], metas[a]->T * E * sizeof(C)});
         }
     } else if (!fcr_out_dev) {
         const Tcl4Instance& in = *insts[0];
         const std::size_t nf3 = static_cast<std::size_t>(in.sys.nf) * in.sys.nf * in.sys.nf;
         const std::size_t U = metas[0]->U;
         for (int kind = 0; kind < 3; ++kind)
-            cuda_check(cudaMemcpyAsync(fcr_out[kind], P.v[0] + kind * nf3 * U, nf3 * U * sizeof(C),
-                                       cudaMemcpyDeviceToHost, st),
-                       "cudaMemcpyAsync(F/C/R out)");
+            d2h.push_back({fcr_out[kind], P.v[0] + kind * nf3 * U, nf3 * U * sizeof(C)});
     }
+    const std::size_t n_scan = ntri;
+    return [=](cudaStream_t st, ProfRecorder* prp, cudaEvent_t ev0, cudaEvent_t ev1) {
+    ProfRecorder dummy;
+    ProfRecorder& pr = prp ? *prp : dummy;
+    const bool f32 = std::is_same<R, float>::value;
+    if (ev0) cuda_check(cudaEventRecord(ev0, st), "cudaEventRecord");
+    pr.before(f32 ? "spectra_col_f32" : "spectra_col_f64");
+    k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(n_spec_jobs)), g.col_threads, g.col_smem, st>>>(
+        P.colj, plan, g.log2c);
+    check_launch("k_fwd_col(spectra)", &pr);
+    pr.before(f32 ? "spectra_row_f32" : "spectra_row_f64");
+    k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
+        P.rowj, plan, g.log2r);
+    check_launch("k_row(spectra)", &pr);
+    const unsigned dft_grid = static_cast<unsigned>((N2 + INV_DFT_THREADS - 1) / INV_DFT_THREADS);
+    for (std::size_t ch = 0; ch < nchunks; ++ch) {
+        const std::size_t q0 = ch * Q, nq = std::min(Q, ntri - q0);
+        pr.before(f32 ? "fwd_col_f32" : "fwd_col_f64");
+        k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(nq)), g.col_threads, g.col_smem, st>>>(
+            P.colj + n_spec_jobs + q0, plan, g.log2c);
+        check_launch("k_fwd_col", &pr);
+        pr.before(f32 ? "row_conv_f32" : "row_conv_f64");
+        k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
+            P.rowj + n_spec_jobs + q0, plan, g.log2r);
+        check_launch("k_row", &pr);
+        pr.before(f32 ? "inv_col_f32" : "inv_col_f64");
+        if (inv_dft) {
+            k_inv_col_dft<R><<<dim3(dft_grid, static_cast<unsigned>(2 * nq)), INV_DFT_THREADS, 0, st>>>(
+                P.invj + 2 * q0, plan, inv_rows);
+            check_launch("k_inv_col_dft", &pr);
+        } else {
+            k_inv_col<R><<<dim3(g.col_grid, static_cast<unsigned>(2 * nq)), g.col_threads, g.col_smem, st>>>(
+                P.invj + 2 * q0, plan, g.log2c);
+            check_launch("k_inv_col", &pr);
+        }
+    }
+    pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
+    k_scan_assemble<R><<<static_cast<unsigned>(n_scan), SCAN_THREADS, 0, st>>>(P.scanj);
+    check_launch("k_scan_assemble", &pr);
+    if (ev1) cuda_check(cudaEventRecord(ev1, st), "cudaEventRecord");
+    if (!fcr_only) {
+        pr.before(f32 ? "contract_f32" : "contract_f64");
+        const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
+        k_contract<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(P.conj, OT);
+        check_launch("k_contract", &pr);
+    }
+    for (const D2H& c : d2h)
+        cuda_check(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(out)");
+    };
+}
+
+template <class R>
+void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas, const BuildOptions& opt,
+               cudaStream_t st, Workspace& ws, double2* const* fcr_out, bool fcr_out_dev) {
+    Enqueue enq = prepare_group<R>(insts, metas, opt, st, ws, ws.arena, fcr_out, fcr_out_dev);
+    ProfRecorder pr;
+    pr.st = st;
+    enq(st, &pr, opt.fcr_ms ? ws.ev0 : nullptr, opt.fcr_ms ? ws.ev1 : nullptr);
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     pr.resolve();
     if (opt.fcr_ms) {
@@ -655,6 +718,21 @@ void validate_system(const SystemDesc& s) {
 }  // namespace
 
 cudaStream_t default_stream() { return workspace().stream; }
+
+void set_tuning(int L, bool fp32, const Tuning& t) {
+    if (t.col_tile < 8 || t.row_tile < 8 || (t.col_tile & (t.col_tile - 1)) || (t.row_tile & (t.row_tile - 1)) ||
+        t.col_tile > 8192 || t.row_tile > 8192 || t.chunk_bytes == 0)
+        throw Error(kInvalidArgument, "tuning: tiles must be powers of two in [8, 8192] and chunk_bytes > 0");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{L, fp32 ? 1 : 0}] = t;
+}
+
+Tuning get_tuning(int L, bool fp32) { return tuning_for(L, fp32); }
+
+void clear_tuning() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+}
 
 uint64_t kernel_launches() { return g_launches.load(); }
 void profile_enable(bool on) { g_profile.store(on); }
@@ -710,24 +788,16 @@ void build_mirror(const std::vector<double>& omegas, double tol, std::vector<int
     if (zero_index) *zero_index = zero;
 }
 
+namespace {
+void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, std::vector<InstMeta>& metas);
+}
+
 void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream) {
     Workspace& ws = workspace();
     cudaStream_t st = stream ? stream : ws.stream;
     if (opt.fcr_ms) *opt.fcr_ms = 0.0;
-    std::vector<InstMeta> metas(insts.size());
-    for (std::size_t a = 0; a < insts.size(); ++a) {
-        Tcl4Instance& in = insts[a];
-        validate_system(in.sys);
-        if (in.Nt == 0) throw Error(kInvalidArgument, "empty gamma_series");
-        if (in.Nt >= (std::size_t(1) << 31)) throw Error(kOverflow, "Nt too large");
-        if (!(in.dt > 0.0)) throw Error(kInvalidArgument, "dt must be > 0");
-        if (!in.gamma) throw Error(kInvalidArgument, "gamma is null");
-        if (in.tidx.empty()) continue;
-        if (!in.out) throw Error(kInvalidArgument, "output pointer is null");
-        for (uint32_t t : in.tidx)
-            if (t >= in.Nt) throw Error(kOutOfRange, "time_index out of range");
-        derive_meta(in, opt, metas[a], true);
-    }
+    std::vector<InstMeta> metas;
+    validate_and_derive(insts, opt, metas);
     // group by FFT length
     std::map<int, std::vector<std::size_t>> groups;
     for (std::size_t a = 0; a < insts.size(); ++a)
@@ -778,6 +848,96 @@ void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_d
     if (opt.fcr_ms) *opt.fcr_ms = 0.0;
     run_group<double>(gi, gm, o, st, ws, outs, out_on_device);
 }
+
+struct Tcl4Plan {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<std::unique_ptr<DeviceBuffer>> mems;
+    std::vector<Enqueue> enqs;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;
+    ~Tcl4Plan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, std::vector<InstMeta>& metas) {
+    metas.resize(insts.size());
+    for (std::size_t a = 0; a < insts.size(); ++a) {
+        Tcl4Instance& in = insts[a];
+        validate_system(in.sys);
+        if (in.Nt == 0) throw Error(kInvalidArgument, "empty gamma_series");
+        if (in.Nt >= (std::size_t(1) << 31)) throw Error(kOverflow, "Nt too large");
+        if (!(in.dt > 0.0)) throw Error(kInvalidArgument, "dt must be > 0");
+        if (!in.gamma) throw Error(kInvalidArgument, "gamma is null");
+        if (in.tidx.empty()) continue;
+        if (!in.out) throw Error(kInvalidArgument, "output pointer is null");
+        for (uint32_t t : in.tidx)
+            if (t >= in.Nt) throw Error(kOutOfRange, "time_index out of range");
+        derive_meta(in, opt, metas[a], true);
+    }
+}
+}  // namespace
+
+Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt) {
+    for (const auto& in : insts)
+        if (!in.gamma_on_device || !in.out_on_device)
+            throw Error(kInvalidArgument, "plans take device inputs and outputs (TACO_IN_DEVICE | TACO_OUT_DEVICE)");
+    std::vector<InstMeta> metas;
+    validate_and_derive(insts, opt, metas);
+    auto plan = std::make_unique<Tcl4Plan>();
+    cuda_check(cudaGetDevice(&plan->device), "cudaGetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate(plan)");
+    Workspace& ws = workspace();
+    std::map<int, std::vector<std::size_t>> groups;
+    for (std::size_t a = 0; a < insts.size(); ++a)
+        if (!insts[a].tidx.empty()) groups[metas[a].L].push_back(a);
+    for (auto& kv : groups) {
+        std::vector<Tcl4Instance*> gi;
+        std::vector<InstMeta*> gm;
+        for (std::size_t a : kv.second) {
+            gi.push_back(&insts[a]);
+            gm.push_back(&metas[a]);
+        }
+        plan->mems.push_back(std::make_unique<DeviceBuffer>());
+        if (opt.fp32)
+            plan->enqs.push_back(prepare_group<float>(gi, gm, opt, plan->stream, ws, *plan->mems.back(), nullptr, false));
+        else
+            plan->enqs.push_back(prepare_group<double>(gi, gm, opt, plan->stream, ws, *plan->mems.back(), nullptr, false));
+    }
+    const uint64_t k0 = g_launches.load();
+    cuda_check(cudaStreamBeginCapture(plan->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+        for (auto& e : plan->enqs) e(plan->stream, nullptr, nullptr, nullptr);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(plan->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    cuda_check(cudaStreamEndCapture(plan->stream, &plan->graph), "cudaStreamEndCapture");
+    plan->kernels = g_launches.load() - k0;
+    g_launches.fetch_sub(plan->kernels);  // captured, not launched
+    cuda_check(cudaGraphInstantiate(&plan->exec, plan->graph, 0), "cudaGraphInstantiate");
+    return plan.release();
+}
+
+void plan_execute(Tcl4Plan* plan, cudaStream_t stream) {
+    if (!plan) throw Error(kInvalidArgument, "plan is null");
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev != plan->device) throw Error(kInvalidArgument, "plan belongs to another device");
+    cuda_check(cudaGraphLaunch(plan->exec, stream ? stream : workspace().stream), "cudaGraphLaunch");
+    g_launches.fetch_add(plan->kernels);
+}
+
+void plan_destroy(Tcl4Plan* plan) { delete plan; }
+
+uint64_t plan_kernels(const Tcl4Plan* plan) { return plan ? plan->kernels : 0; }
 
 std::size_t rk4_num_samples(std::size_t steps, std::size_t sample_every) {
     if (sample_every == 0) return 0;

@@ -29,16 +29,34 @@ struct Tcl4Instance {
     bool out_on_device = false;
 };
 
+// Launch schedule of the F/C/R passes for one FFT length and precision.
+struct Tuning {
+    int col_tile = 4096;                        // elements per column-pass tile
+    int row_tile = 2048;                        // elements per row-pass tile
+    std::size_t chunk_bytes = std::size_t(48) << 20;  // Z/W scratch per chunk of triples
+    int inv_dft_rows = 16;                      // pruned inverse column DFT up to this many rows
+};
+void set_tuning(int L, bool fp32, const Tuning& t);
+Tuning get_tuning(int L, bool fp32);
+void clear_tuning();
+
 struct BuildOptions {
     bool fp32 = false;
     bool causal_truncation = false;  // FFT length from max(tidx)+1 instead of Nt
     std::size_t pad_factor = 0;      // Nfft = next_pow2(max(2 n - 1, pad * n))
-    std::size_t scratch_budget = std::size_t(1) << 30;
     double* fcr_ms = nullptr;        // device time of the F/C/R stage
 };
 
 // Full L4 builds (build_TCL4_generator_cuda_fused[_batch]) for a set of instances.
 void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream);
+
+// Prepared batched build: metadata resident on the device, launch sequence captured in a
+// CUDA graph; execute replays it (stream-ordered, no host work).
+struct Tcl4Plan;
+Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt);
+void plan_execute(Tcl4Plan* plan, cudaStream_t stream);
+void plan_destroy(Tcl4Plan* plan);
+uint64_t plan_kernels(const Tcl4Plan* plan);
 
 // compute_triple_kernels: full F/C/R series [nf^3][Nt] (FP64) for one instance.
 void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_device, std::size_t Nt,

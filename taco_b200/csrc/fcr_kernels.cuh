@@ -1,21 +1,32 @@
 // fcr_kernels.cuh -- device kernels of the F/C/R stage.
 //
-// The causal convolutions of the F and C kernels are computed with a four-step FFT of
-// length Nfft = N1*N2 (both powers of two, at most 2048):
-//   B1  column pass: x[t] generated on the fly (gamma column, optional phase
-//       exp(-i w t dt), optional conjugate; zero for t >= n_in), N1-point FFTs down the
-//       columns, inter-step twiddle w_N^(n2*k1), stored as Z[k1*N2 + n2];
+// F and C (cpp/src/tcl/tcl4_kernels.cpp:105-152) are
+//   F[t] = g1[t] e_t P_F(t) - dt sum_{m<=t} g1[t-m] e_{t-m} g2[m],   e_t = exp(-i w t dt),
+// a prefix integral minus a causal convolution that nearly cancel (term ratios above
+// 100 occur).  The kernels evaluate the algebraically identical form with both series
+// shifted by their last sample (c1 = g1[n_in-1], c2 = g2[n_in-1], d = g - c):
+//   F[t] = d1[t] e_t P_F(t) - dt sum_m d1[t-m] e_{t-m} d2[m] - c2 S(t),
+//   S(t) = dt sum_{k<=t} d1[k] e_k,
+// which leaves only the transient in the FFT operands: the FFT round-off, proportional
+// to the operand norms, drops by about three orders of magnitude (what makes the FP32
+// form meet 1e-6), and the FP64 path gains accuracy as well.
+//
+// The convolutions use a four-step FFT of length Nfft = N1*N2 (powers of two <= 2048):
+//   B1  column pass: x[t] generated on the fly (gamma column minus its last sample,
+//       optional conjugate, optional phase exp(-i w t dt); zero for t >= n_in),
+//       N1-point FFTs down the columns, inter-step twiddle w_N^(n2*k1), stored as
+//       Z[k1*N2 + n2];
 //   B2  row pass: N2-point FFT of each row -> spectrum row in the permuted order
 //       S[k1*N2 + k2]; multiplied by the hoisted spectra of the two partner series
-//       (F: gamma[:, mirror j]; C: conj gamma[:, j]), both products transformed back
-//       along the row and twiddled by w_N^(-n2*k1) (the spectrum of x never leaves
+//       (F: d of gamma[:, mirror j]; C: conj d of gamma[:, j]), both products transformed
+//       back along the row and twiddled by w_N^(-n2*k1) (the spectrum of x never leaves
 //       shared memory);
 //   B3  inverse column pass: N1-point inverse FFTs down the columns, scaled by dt/Nfft,
 //       only samples t <= t_max written.
-// The spectra of gamma[:, b] and conj(gamma[:, b]) are produced once per instance by
-// B1 + a plain forward row pass.
-// The scan kernel forms the three prefix integrals per triple (P_F, P_R1, P_R2;
-// P_C = conj(P_R1)) with FP64 carries and assembles F, C, R at the requested times.
+// The spectra of d_b and conj(d_b) are produced once per instance by B1 + a plain
+// forward row pass.  The scan kernel forms the prefix integrals per triple (P_F, P_R1,
+// P_R2, S; P_C = conj(P_R1)) with FP64 carries and assembles F, C, R at the requested
+// times.
 #pragma once
 
 #include "common.cuh"
@@ -40,7 +51,7 @@ __device__ __forceinline__ C inter_twiddle(const FftPlan<C>& p, uint32_t a) {
 }
 
 struct ColJob {
-    const double2* g;  // gamma column, n_in valid samples
+    const double2* g;  // gamma column, n_in valid samples; g[n_in-1] is subtracted
     double omega;      // phase exp(-i omega t dt) applied when has_phase
     double dt;
     int has_phase;
@@ -69,6 +80,7 @@ struct ScanJob {
     const double2* gmj;
     double omega;
     double dt;
+    uint32_t n_in;     // samples used by the convolution operands (shift = g[n_in-1])
     uint32_t t_count;  // t_max + 1
     const void* conv_f;
     const void* conv_c;
@@ -86,68 +98,75 @@ __device__ __forceinline__ double2 phase_minus(double omega, double dt, uint32_t
 }
 
 // ---------------------------------------------------------------- B1 -------
+// Column tile: 2^log2c columns n2_0 .. n2_0 + 2^log2c - 1, all N1 rows; element
+// (column c, row n1) at pad(n1 * 2^log2c + c).
 template <class R>
-__global__ void k_fwd_col(const ColJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int C_cols) {
+__global__ void k_fwd_col(const ColJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2c) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     const ColJob job = jobs[blockIdx.y];
-    const int N1 = 1 << plan.L1, N2 = 1 << plan.L2;
-    const int n2_0 = blockIdx.x * C_cols;
-    const int elems = N1 * C_cols;
+    const int N2 = 1 << plan.L2;
+    const int ccols = 1 << log2c;
+    const int n2_0 = blockIdx.x << log2c;
+    const int elems = ccols << plan.L1;
+    const double2 shift = __ldg(&job.g[job.n_in - 1]);
     for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
-        const int n1 = idx / C_cols, c = idx - n1 * C_cols;
+        const int n1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
         double2 v = make_double2(0.0, 0.0);
         if (t < job.n_in) {
-            v = __ldg(&job.g[t]);
+            v = csub(__ldg(&job.g[t]), shift);
             if (job.conj) v.y = -v.y;
             if (job.has_phase) v = cmul(v, phase_minus(job.omega, job.dt, t));
         }
-        s[idx] = from_d2<C>(v);
+        s[pad_idx<C>(idx)] = from_d2<C>(v);
     }
     __syncthreads();
-    tile_fft<C, false>(s, plan.L1, 1, C_cols, plan.tw1);
+    tile_fft<C, false, true>(s, plan.L1, log2c, 1, ccols, plan.tw1);
     C* out = static_cast<C*>(job.out);
     for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
-        const int k1 = idx / C_cols, c = idx - k1 * C_cols;
+        const int k1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t n2 = n2_0 + c;
-        out[static_cast<size_t>(k1) * N2 + n2] = cmul(s[idx], inter_twiddle(plan, n2 * static_cast<uint32_t>(k1)));
+        out[static_cast<size_t>(k1) * N2 + n2] =
+            cmul(s[pad_idx<C>(idx)], inter_twiddle(plan, n2 * static_cast<uint32_t>(k1)));
     }
 }
 
 // ---------------------------------------------------------------- B2 -------
+// Row tile: 2^log2r rows of N2 elements, element (row r, i) at pad(r * N2 + i).
 // Forward row FFT; with spec_f set: two spectral products, inverse row FFTs and the
-// inverse inter-step twiddle.  Shared memory: two tiles of rows*N2 elements.
+// inverse inter-step twiddle.  Shared memory: two padded tiles.
 template <class R>
-__global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int rows) {
+__global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2r) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N2 = 1 << plan.L2;
-    const int elems = rows * N2;
+    const int elems = N2 << log2r;
     C* a = reinterpret_cast<C*>(smem_raw);
-    C* p = a + elems;
+    C* p = a + padded_size<C>(elems);
     const RowJob job = jobs[blockIdx.y];
     const size_t off = static_cast<size_t>(blockIdx.x) * elems;
     C* data = static_cast<C*>(job.data) + off;
-    for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) a[idx] = data[idx];
+    for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) a[pad_idx<C>(idx)] = data[idx];
     __syncthreads();
-    tile_fft<C, false>(a, plan.L2, N2, 1, plan.tw2);
+    tile_fft<C, false, false>(a, plan.L2, log2r, N2, 1, plan.tw2);
     if (job.spec_f == nullptr) {
-        for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) data[idx] = a[idx];
+        for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) data[idx] = a[pad_idx<C>(idx)];
         return;
     }
-    const int k1_0 = blockIdx.x * rows;
+    const int k1_0 = blockIdx.x << log2r;
     for (int which = 0; which < 2; ++which) {
         const C* spec = static_cast<const C*>(which == 0 ? job.spec_f : job.spec_c) + off;
-        for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) p[idx] = cmul(a[idx], spec[idx]);
+        for (int idx = threadIdx.x; idx < elems; idx += blockDim.x)
+            p[pad_idx<C>(idx)] = cmul(a[pad_idx<C>(idx)], spec[idx]);
         __syncthreads();
-        tile_fft<C, true>(p, plan.L2, N2, 1, plan.tw2);
+        tile_fft<C, true, false>(p, plan.L2, log2r, N2, 1, plan.tw2);
         C* dst = (which == 0 ? data : static_cast<C*>(job.wc) + off);
         for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
             const int r = idx >> plan.L2, n2 = idx & (N2 - 1);
             const uint32_t k1 = static_cast<uint32_t>(k1_0 + r);
-            dst[idx] = cmulc(p[idx], inter_twiddle(plan, static_cast<uint32_t>(n2) * k1));
+            dst[idx] = cmulc(p[pad_idx<C>(idx)], inter_twiddle(plan, static_cast<uint32_t>(n2) * k1));
         }
         __syncthreads();
     }
@@ -155,83 +174,128 @@ __global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, 
 
 // ---------------------------------------------------------------- B3 -------
 template <class R>
-__global__ void k_inv_col(const InvJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int C_cols) {
+__global__ void k_inv_col(const InvJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2c) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     const InvJob job = jobs[blockIdx.y];
-    const int N1 = 1 << plan.L1, N2 = 1 << plan.L2;
-    const int n2_0 = blockIdx.x * C_cols;
-    const int elems = N1 * C_cols;
+    const int N2 = 1 << plan.L2;
+    const int ccols = 1 << log2c;
+    const int n2_0 = blockIdx.x << log2c;
+    const int elems = ccols << plan.L1;
     const C* w = static_cast<const C*>(job.w);
     for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
-        const int k1 = idx / C_cols, c = idx - k1 * C_cols;
-        s[idx] = w[static_cast<size_t>(k1) * N2 + n2_0 + c];
+        const int k1 = idx >> log2c, c = idx & (ccols - 1);
+        s[pad_idx<C>(idx)] = w[static_cast<size_t>(k1) * N2 + n2_0 + c];
     }
     __syncthreads();
-    tile_fft<C, true>(s, plan.L1, 1, C_cols, plan.tw1);
+    tile_fft<C, true, true>(s, plan.L1, log2c, 1, ccols, plan.tw1);
     C* out = static_cast<C*>(job.out);
     const R scale = static_cast<R>(job.scale);
     for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
-        const int n1 = idx / C_cols, c = idx - n1 * C_cols;
+        const int n1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
-        if (t < job.t_count) out[t] = cscale(s[idx], scale);
+        if (t < job.t_count) out[t] = cscale(s[pad_idx<C>(idx)], scale);
+    }
+}
+
+// Pruned inverse column pass for t_count <= MAXR * N2: only rows n1 < nrows of the
+// output are needed, so each thread owns one column and evaluates those rows as a
+// direct inverse DFT over k1 (one streaming read of W, no shared-memory stages).
+constexpr int INV_DFT_MAXR = 16;
+constexpr int INV_DFT_THREADS = 128;
+
+template <class R>
+__global__ void __launch_bounds__(INV_DFT_THREADS) k_inv_col_dft(const InvJob* __restrict__ jobs,
+                                                                  FftPlan<cplx_t<R>> plan, int nrows) {
+    using C = cplx_t<R>;
+    const InvJob job = jobs[blockIdx.y];
+    const int N1 = 1 << plan.L1, N2 = 1 << plan.L2;
+    const int n2 = blockIdx.x * INV_DFT_THREADS + threadIdx.x;
+    if (n2 >= N2) return;
+    const C* w = static_cast<const C*>(job.w) + n2;
+    C acc[INV_DFT_MAXR];
+#pragma unroll
+    for (int r = 0; r < INV_DFT_MAXR; ++r) acc[r] = C{0, 0};
+    const int mask = N1 - 1;
+#pragma unroll 4
+    for (int k1 = 0; k1 < N1; ++k1) {
+        const C x = w[static_cast<size_t>(k1) * N2];
+#pragma unroll
+        for (int r = 0; r < INV_DFT_MAXR; ++r) {
+            if (r < nrows) acc[r] = cadd(acc[r], cmulc(x, __ldg(&plan.tw1[(r * k1) & mask])));
+        }
+    }
+    C* out = static_cast<C*>(job.out);
+    const R scale = static_cast<R>(job.scale);
+#pragma unroll
+    for (int r = 0; r < INV_DFT_MAXR; ++r) {
+        const uint32_t t = static_cast<uint32_t>(r) * N2 + n2;
+        if (r < nrows && t < job.t_count) out[t] = cscale(acc[r], scale);
     }
 }
 
 // ---------------------------------------------------------------- scans ----
-__device__ __forceinline__ void add6(double* a, const double* b) {
-#pragma unroll
-    for (int q = 0; q < 6; ++q) a[q] += b[q];
-}
-
-// One CTA per triple; SCAN_ITEMS consecutive samples per thread; FP64 carries.
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_W = 8;  // four complex prefix sums
 
+// One CTA per triple; SCAN_ITEMS consecutive samples per thread; FP64 sums and carries.
+// Prefixes: P_F = sum g_mj e^{+iwt}, P_R1 = sum g_j e^{-iwt}, P_R2 = sum g_i g_j e^{-iwt},
+// S = sum (g_i - c_i) e^{-iwt} (all times dt).
 template <class R>
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_assemble(const ScanJob* __restrict__ jobs) {
     using C = cplx_t<R>;
-    __shared__ double warp_tot[SCAN_THREADS / 32][6];
-    __shared__ double carry_sh[6];
+    __shared__ double warp_tot[SCAN_THREADS / 32][SCAN_W];
+    __shared__ double carry_sh[SCAN_W];
     const ScanJob job = jobs[blockIdx.x];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double carry[6] = {0, 0, 0, 0, 0, 0};
+    double carry[SCAN_W];
+#pragma unroll
+    for (int k = 0; k < SCAN_W; ++k) carry[k] = 0.0;
     const C* cf = static_cast<const C*>(job.conv_f);
     const C* cc = static_cast<const C*>(job.conv_c);
     C* vf = static_cast<C*>(job.vf);
     C* vc = static_cast<C*>(job.vc);
     C* vr = static_cast<C*>(job.vr);
+    const double2 ci = __ldg(&job.gi[job.n_in - 1]);
+    const double2 cmj = __ldg(&job.gmj[job.n_in - 1]);
+    const double2 cj = __ldg(&job.gj[job.n_in - 1]);
     const uint32_t tile = SCAN_THREADS * SCAN_ITEMS;
     for (uint32_t t0 = 0; t0 < job.t_count; t0 += tile) {
-        // integrands: y0 = g_mj e^{+iwt}, y1 = g_j e^{-iwt}, y2 = g_i g_j e^{-iwt}
-        double y[SCAN_ITEMS][6];
-        double run[6] = {0, 0, 0, 0, 0, 0};
+        double y[SCAN_ITEMS][SCAN_W];
+        double run[SCAN_W];
+#pragma unroll
+        for (int k = 0; k < SCAN_W; ++k) run[k] = 0.0;
         const uint32_t tb = t0 + threadIdx.x * SCAN_ITEMS;
 #pragma unroll
         for (int q = 0; q < SCAN_ITEMS; ++q) {
             const uint32_t t = tb + q;
-            double v[6] = {0, 0, 0, 0, 0, 0};
+            double v[SCAN_W];
+#pragma unroll
+            for (int k = 0; k < SCAN_W; ++k) v[k] = 0.0;
             if (t < job.t_count) {
                 const double2 pm = phase_minus(job.omega, job.dt, t);
                 const double2 gmj = __ldg(&job.gmj[t]);
                 const double2 gj = __ldg(&job.gj[t]);
                 const double2 gi = __ldg(&job.gi[t]);
-                const double2 a = cmulc(gmj, pm);  // g_mj * e^{+iwt}
+                const double2 a = cmulc(gmj, pm);  // g_mj e^{+iwt}
                 const double2 b = cmul(gj, pm);
                 const double2 c = cmul(cmul(gi, gj), pm);
-                v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y;
+                const double2 d = cmul(csub(gi, ci), pm);
+                v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+                v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
             }
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
+            for (int k = 0; k < SCAN_W; ++k) {
                 run[k] += v[k];
                 y[q][k] = run[k];
             }
         }
         // exclusive scan of the per-thread totals across the block
-        double incl[6];
+        double incl[SCAN_W];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
+        for (int k = 0; k < SCAN_W; ++k) {
             double x = run[k];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -242,12 +306,12 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_assemble(const ScanJob* _
         }
         if (lane == 31) {
 #pragma unroll
-            for (int k = 0; k < 6; ++k) warp_tot[warp][k] = incl[k];
+            for (int k = 0; k < SCAN_W; ++k) warp_tot[warp][k] = incl[k];
         }
         __syncthreads();
-        double pre[6];
+        double pre[SCAN_W];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
+        for (int k = 0; k < SCAN_W; ++k) {
             double excl = __shfl_up_sync(0xffffffffu, incl[k], 1);
             if (lane == 0) excl = 0.0;
             double w = 0.0;
@@ -260,22 +324,24 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_assemble(const ScanJob* _
             if (t >= job.t_count) break;
             const int u = __ldg(&job.tmap[t]);
             if (u < 0) continue;
-            const double2 PF = make_double2((pre[0] + y[q][0]) * job.dt, (pre[1] + y[q][1]) * job.dt);
-            const double2 PR1 = make_double2((pre[2] + y[q][2]) * job.dt, (pre[3] + y[q][3]) * job.dt);
-            const double2 PR2 = make_double2((pre[4] + y[q][4]) * job.dt, (pre[5] + y[q][5]) * job.dt);
+            const double dt = job.dt;
+            const double2 PF = make_double2((pre[0] + y[q][0]) * dt, (pre[1] + y[q][1]) * dt);
+            const double2 PR1 = make_double2((pre[2] + y[q][2]) * dt, (pre[3] + y[q][3]) * dt);
+            const double2 PR2 = make_double2((pre[4] + y[q][4]) * dt, (pre[5] + y[q][5]) * dt);
+            const double2 S = make_double2((pre[6] + y[q][6]) * dt, (pre[7] + y[q][7]) * dt);
             const double2 pm = phase_minus(job.omega, job.dt, t);
             const double2 gi = __ldg(&job.gi[t]);
-            const double2 gip = cmul(gi, pm);
-            const double2 convf = to_d2(cf[t]);
-            const double2 convc = to_d2(cc[t]);
-            vf[u] = from_d2<C>(csub(cmul(gip, PF), convf));
-            vc[u] = from_d2<C>(csub(cmulc(gip, PR1), convc));  // P_C = conj(P_R1)
+            const double2 dip = cmul(csub(gi, ci), pm);
+            const double2 convf = cadd(to_d2(cf[t]), cmul(cmj, S));
+            const double2 convc = cadd(to_d2(cc[t]), cmulc(S, cj));  // conj(c_j) S
+            vf[u] = from_d2<C>(csub(cmul(dip, PF), convf));
+            vc[u] = from_d2<C>(csub(cmulc(dip, PR1), convc));  // P_C = conj(P_R1)
             vr[u] = from_d2<C>(csub(cmul(gi, PR1), PR2));
         }
         __syncthreads();
         if (threadIdx.x == 0) {
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
+            for (int k = 0; k < SCAN_W; ++k) {
                 double w = 0.0;
                 for (int q = 0; q < SCAN_THREADS / 32; ++q) w += warp_tot[q][k];
                 carry_sh[k] = carry[k] + w;
@@ -283,7 +349,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_assemble(const ScanJob* _
         }
         __syncthreads();
 #pragma unroll
-        for (int k = 0; k < 6; ++k) carry[k] = carry_sh[k];
+        for (int k = 0; k < SCAN_W; ++k) carry[k] = carry_sh[k];
         __syncthreads();
     }
 }

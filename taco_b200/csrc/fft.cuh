@@ -1,17 +1,33 @@
 // fft.cuh -- shared-memory Stockham FFT engine for power-of-two lengths.
 //
-// A tile in shared memory holds `nfft` independent transforms of length n; element
-// i of transform f lives at s[f*fs + i*es].  Every thread owns 8 elements per stage
+// A tile in shared memory holds `nfft` independent transforms of length n.  Element i
+// of transform f lives at pad(f*fs + i*es), where pad(x) = x + (x >> PAD) inserts one
+// spare slot every 2^PAD elements (128 bytes) so that the strided Stockham writes of
+// the first stages do not pile onto one bank.  Every thread owns 8 elements per stage
 // (blockDim.x == nfft*n/8), so each radix-2^r stage reads 8 values into registers,
-// twiddles them, runs 8/2^r small DFTs and writes them back (Stockham autosort:
-// natural order in, natural order out; in place with a barrier between the read and
-// the write phase).  The twiddle table tw[m] = exp(-2*pi*i*m/n), m in [0, n), is read
-// through the read-only path; inverse transforms conjugate it and are unnormalised.
+// twiddles them, runs 8/2^r small DFTs and writes them back (Stockham autosort: natural
+// order in, natural order out; in place with a barrier between the read and the write
+// phase).  F_FAST selects the thread -> (transform, element) mapping: transforms
+// fastest for column tiles (fs == 1: consecutive threads touch consecutive addresses),
+// elements fastest for row tiles (es == 1).  The twiddle table tw[m] =
+// exp(-2*pi*i*m/n), m in [0, n), is read through the read-only path; inverse transforms
+// conjugate it and are unnormalised.
 #pragma once
 
 #include "common.cuh"
 
 namespace taco {
+
+// one pad slot per 128 bytes: every 8 complex doubles or 16 complex floats
+template <class C> struct PadShift;
+template <> struct PadShift<double2> { static constexpr int value = 3; };
+template <> struct PadShift<float2> { static constexpr int value = 4; };
+
+template <class C>
+__host__ __device__ __forceinline__ int pad_idx(int x) { return x + (x >> PadShift<C>::value); }
+
+template <class C>
+__host__ __device__ __forceinline__ int padded_size(int n) { return n + (n >> PadShift<C>::value) + 1; }
 
 template <class C, bool INV>
 __device__ __forceinline__ C mul_w(C a, C w) {
@@ -64,26 +80,31 @@ __device__ __forceinline__ void dft8(C* x) {
 }
 
 // One Stockham stage of radix 2^LR on a shared-memory tile.
-template <class C, int LR, bool INV>
-__device__ __forceinline__ void stockham_stage(C* s, int log2n, int p, int fs, int es,
+template <class C, int LR, bool INV, bool F_FAST>
+__device__ __forceinline__ void stockham_stage(C* s, int log2n, int log2nfft, int p, int fs, int es,
                                                const C* __restrict__ tw) {
     constexpr int RAD = 1 << LR;
     constexpr int ITEMS = 8 / RAD;
     const int n = 1 << log2n;
     const int lq = log2n - LR;  // log2(n / RAD): items per transform
-    const int q_mask = (1 << lq) - 1;
     C x[8];
     int base[ITEMS], jout[ITEMS];
 #pragma unroll
     for (int q = 0; q < ITEMS; ++q) {
         const int g = threadIdx.x * ITEMS + q;
-        const int f = g >> lq;
-        const int i = g & q_mask;
+        int f, i;
+        if (F_FAST) {
+            f = g & ((1 << log2nfft) - 1);
+            i = g >> log2nfft;
+        } else {
+            f = g >> lq;
+            i = g & ((1 << lq) - 1);
+        }
         const int k = i & (p - 1);
         base[q] = f * fs;
         jout[q] = ((i - k) << LR) + k;
 #pragma unroll
-        for (int r = 0; r < RAD; ++r) x[q * RAD + r] = s[base[q] + (i + (r << lq)) * es];
+        for (int r = 0; r < RAD; ++r) x[q * RAD + r] = s[pad_idx<C>(base[q] + (i + (r << lq)) * es)];
         if (p > 1) {
             // w_{p*RAD}^{r*k} = tw[r * k * n / (p * RAD)]
             const int stride = (n / (p * RAD)) * k;
@@ -98,31 +119,31 @@ __device__ __forceinline__ void stockham_stage(C* s, int log2n, int p, int fs, i
 #pragma unroll
     for (int q = 0; q < ITEMS; ++q) {
 #pragma unroll
-        for (int r = 0; r < RAD; ++r) s[base[q] + (jout[q] + r * p) * es] = x[q * RAD + r];
+        for (int r = 0; r < RAD; ++r) s[pad_idx<C>(base[q] + (jout[q] + r * p) * es)] = x[q * RAD + r];
     }
     __syncthreads();
 }
 
-// Full transform of every length-n sequence in the tile.  Requires
-// blockDim.x * 8 == (number of transforms) * n and n >= 2.  The tile must be
-// visible to all threads (a __syncthreads() after filling it) on entry; it is
-// complete and visible on exit.
-template <class C, bool INV>
-__device__ void tile_fft(C* s, int log2n, int fs, int es, const C* __restrict__ tw) {
+// Full transform of every length-n sequence in the tile (2^log2nfft sequences).
+// Requires blockDim.x * 8 == 2^log2nfft * n and n >= 2.  The tile must be visible to all
+// threads (a __syncthreads() after filling it) on entry; it is complete and visible on
+// exit.
+template <class C, bool INV, bool F_FAST>
+__device__ void tile_fft(C* s, int log2n, int log2nfft, int fs, int es, const C* __restrict__ tw) {
     int p = 1;
     int rem = log2n;
     // radix-4 first when log2n % 3 == 2, radix-2 first when log2n % 3 == 1, then radix-8
     if (rem % 3 == 2) {
-        stockham_stage<C, 2, INV>(s, log2n, p, fs, es, tw);
+        stockham_stage<C, 2, INV, F_FAST>(s, log2n, log2nfft, p, fs, es, tw);
         p <<= 2;
         rem -= 2;
     } else if (rem % 3 == 1) {
-        stockham_stage<C, 1, INV>(s, log2n, p, fs, es, tw);
+        stockham_stage<C, 1, INV, F_FAST>(s, log2n, log2nfft, p, fs, es, tw);
         p <<= 1;
         rem -= 1;
     }
     while (rem > 0) {
-        stockham_stage<C, 3, INV>(s, log2n, p, fs, es, tw);
+        stockham_stage<C, 3, INV, F_FAST>(s, log2n, log2nfft, p, fs, es, tw);
         p <<= 3;
         rem -= 3;
     }

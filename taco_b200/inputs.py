@@ -131,7 +131,8 @@ def bcf_fft(N: int, dt: float, J, beta: float):
         S[k] = sp
         S[nfft - k] = sp * kms
         S[0] = 0.5 * (np.pi / 2) * J(np.array([dw]))[0] * (1 + r) / (1 - r)
-        S[nfft // 2] = 0.25 * np.pi * J(np.array([wny]))[0] * (1 + 2 / np.expm1(beta * wny))
+        x = beta * wny  # coth(x/2) = 1 + 2/(e^x - 1); the term vanishes once e^x overflows
+        S[nfft // 2] = 0.25 * np.pi * J(np.array([wny]))[0] * (1 + (2 / np.expm1(x) if x < 700 else 0.0))
     C = np.fft.fft(S) * (dw / np.pi)
     return np.arange(Nt) * dt, C[:Nt]
 

@@ -96,7 +96,7 @@ def test_random_systems_vs_oracle(d, nops, Nt):
     assert relerr(out32, ref) <= 1e-6
 
 
-def test_pad_factor_and_causal_truncation_keep_results():
+def test_pad_factor_and_full_length_keep_results():
     osys, s, G = spin_boson_case(2000, 0.005)
     tidx = np.arange(0, 300)
     base = tb.build_TCL4_generator_batch(s, G, 0.005, tidx)
@@ -105,8 +105,35 @@ def test_pad_factor_and_causal_truncation_keep_results():
         padded = tb.build_TCL4_generator_batch(s, G, 0.005, tidx)
     finally:
         tb.set_fcr_fft_pad_factor(0)
-    trunc = tb.build_TCL4_generator_batch(s, G, 0.005, tidx, causal_truncation=True)
-    assert relerr(padded, base) <= 1e-12 and relerr(trunc, base) <= 1e-12
+    full = tb.build_TCL4_generator_batch(s, G, 0.005, tidx, full_length=True)
+    assert relerr(padded, base) <= 1e-12 and relerr(full, base) <= 1e-12
+    full32 = tb.build_TCL4_generator_batch(s, G, 0.005, tidx, precision="fp32", full_length=True)
+    ref = oracle_l4(osys, G, 0.005, tidx)
+    assert relerr(full, ref) <= 1e-10 and relerr(full32, ref) <= 1e-6
+
+
+def test_plan_replay_matches_direct_call():
+    import torch
+    cases = [spin_boson_case(1200, 0.005, eps=e) for e in (0.8, 1.0, 1.7)]
+    inst = [(s, torch_dev(G), 0.005, np.arange(0, 1201, 2)) for _, s, G in cases]
+    direct = [x.cpu().numpy() for x in tb.build_instances(inst, precision="fp32")]
+    plan = tb.Tcl4Plan(inst, precision="fp32")
+    n0 = tb.kernel_launches()
+    for _ in range(3):
+        res = plan.run()
+    torch.cuda.synchronize()
+    assert tb.kernel_launches() > n0
+    for a, b in zip(res, direct):
+        assert np.array_equal(a.cpu().numpy(), b)
+    plan64 = tb.Tcl4Plan(inst, precision="fp64")
+    res64 = plan64.run()
+    torch.cuda.synchronize()
+    for (osys, _, G), r in zip(cases, res64):
+        assert relerr(r.cpu().numpy(), oracle_l4(osys, G, 0.005, np.arange(0, 1201, 2))) <= 1e-10
+    plan.close()
+    plan64.close()
+    with pytest.raises(ValueError):
+        tb.Tcl4Plan([(s, G, 0.005, None) for _, s, G in cases])
 
 
 def test_batched_instances_match_single_calls():
