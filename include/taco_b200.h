@@ -133,7 +133,8 @@ int taco_tcl4_build_instances(const taco_tcl4_instance* inst, size_t count, int 
  * build once -- metadata and job tables resident on the device, the whole launch sequence
  * captured in a CUDA graph -- and replay it.  Inputs and outputs must be device pointers
  * (TACO_IN_DEVICE | TACO_OUT_DEVICE); they are bound at creation.  taco_tcl4_plan_execute
- * is asynchronous on `stream`. */
+ * is asynchronous on exactly `stream` (NULL is the legacy default stream, not the library's
+ * per-thread stream), so the caller orders it with its own work and synchronises. */
 typedef struct taco_tcl4_plan taco_tcl4_plan;
 int taco_tcl4_plan_create(const taco_tcl4_instance* inst, size_t count, int method, int precision, int flags,
                           taco_tcl4_plan** plan);

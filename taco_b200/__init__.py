@@ -287,8 +287,10 @@ class Tcl4Plan:
         self._stream_of = self._keep[0]
 
     def run(self, stream=None):
-        s = _stream_ptr(self._stream_of) if stream is None else ct.c_void_p(stream)
-        _capi.check(_capi.lib().taco_tcl4_plan_execute(self._h, s))
+        """Replay on `stream` (a raw cudaStream_t handle) or torch's current stream."""
+        if stream is None:
+            stream = _torch().cuda.current_stream(self._stream_of.device).cuda_stream
+        _capi.check(_capi.lib().taco_tcl4_plan_execute(self._h, ct.c_void_p(stream)))
         return self.results
 
     def close(self):

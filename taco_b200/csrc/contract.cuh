@@ -55,4 +55,53 @@ __global__ void k_contract(const ContractJob* __restrict__ jobs, int OT) {
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) out[idx] = res[idx];
 }
 
+// Shared-memory variant: the CTA stages v[s][u(o)] for its OT outputs and the CSR table,
+// then every thread evaluates (entry, output) pairs from shared memory.  Used when the
+// F/C/R tile fits (small systems: S = 3 nf^3 sources).
+template <class R>
+__global__ void k_contract_smem(const ContractJob* __restrict__ jobs, int OT, int S, int nnz_cap) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const ContractJob job = jobs[blockIdx.y];
+    const uint32_t o0 = blockIdx.x * OT;
+    if (o0 >= job.T) return;
+    const uint32_t ot = min(static_cast<uint32_t>(OT), job.T - o0);
+    C* vs = reinterpret_cast<C*>(smem_raw);           // [S][OT]
+    C* res = vs + static_cast<size_t>(S) * OT;         // [OT][E]
+    C* cf = res + static_cast<size_t>(OT) * job.E;     // [nnz]
+    uint32_t* sr = reinterpret_cast<uint32_t*>(cf + nnz_cap);
+    int32_t* rp = reinterpret_cast<int32_t*>(sr + nnz_cap);
+    const int32_t nnz = __ldg(&job.rowptr[job.E]);
+    const C* coef = static_cast<const C*>(job.coef);
+    for (int32_t k = threadIdx.x; k < nnz; k += blockDim.x) {
+        cf[k] = coef[k];
+        sr[k] = __ldg(&job.src[k]);
+    }
+    for (uint32_t e = threadIdx.x; e <= job.E; e += blockDim.x) rp[e] = __ldg(&job.rowptr[e]);
+    const C* v = static_cast<const C*>(job.v);
+    const uint32_t nv = static_cast<uint32_t>(S) * OT;
+    for (uint32_t idx = threadIdx.x; idx < nv; idx += blockDim.x) {
+        const uint32_t sidx = idx / OT, ol = idx - sidx * OT;
+        vs[idx] = ol < ot ? v[static_cast<size_t>(sidx) * job.U + __ldg(&job.out_u[o0 + ol])] : C{0, 0};
+    }
+    __syncthreads();
+    const uint32_t work = job.E * OT;
+    for (uint32_t idx = threadIdx.x; idx < work; idx += blockDim.x) {
+        const uint32_t ol = idx % OT, e = idx / OT;
+        C acc = C{0, 0};
+        const int32_t b = rp[e], end = rp[e + 1];
+        for (int32_t k = b; k < end; ++k) {
+            const uint32_t sk = sr[k];
+            C x = vs[(sk & 0x7fffffffu) * OT + ol];
+            if (sk & 0x80000000u) x.y = -x.y;
+            acc = cadd(acc, cmul(cf[k], x));
+        }
+        res[ol * job.E + e] = acc;
+    }
+    __syncthreads();
+    C* out = static_cast<C*>(job.out) + static_cast<size_t>(o0) * job.E;
+    const uint32_t total = ot * job.E;
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) out[idx] = res[idx];
+}
+
 }  // namespace taco

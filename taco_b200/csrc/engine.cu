@@ -602,13 +602,30 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     set_smem(k_fwd_col<R>, g.col_smem);
     set_smem(k_inv_col<R>, g.col_smem);
     set_smem(k_row<R>, g.row_smem);
-    int maxE = 0;
-    for (auto* in : insts) maxE = std::max(maxE, in->sys.N * in->sys.N * in->sys.N * in->sys.N);
-    const int OT = std::max(1, std::min(128, static_cast<int>((48 * 1024) / (maxE * sizeof(C)))));
+    int maxE = 0, maxS = 0;
+    std::size_t maxNnz = 1;
+    for (auto* in : insts) {
+        maxE = std::max(maxE, in->sys.N * in->sys.N * in->sys.N * in->sys.N);
+        maxS = std::max(maxS, 3 * in->sys.nf * in->sys.nf * in->sys.nf);
+    }
+    for (auto* m : metas) maxNnz = std::max(maxNnz, m->coef.src.size());
     std::size_t maxT = 0;
     for (auto* m : metas) maxT = std::max(maxT, m->T);
-    const std::size_t csmem = static_cast<std::size_t>(OT) * maxE * sizeof(C);
-    set_smem(k_contract<R>, csmem);
+    // shared-memory contraction when the F/C/R tile of >= 16 outputs and the CSR table fit
+    const std::size_t smem_budget = 100 * 1024;
+    const std::size_t csr_bytes = maxNnz * (sizeof(C) + 4) + (maxE + 1) * 4 + 64;
+    int OTs = 128;
+    auto smem_need = [&](int ot) {
+        return (static_cast<std::size_t>(maxS) + maxE) * ot * sizeof(C) + csr_bytes;
+    };
+    while (OTs > 16 && smem_need(OTs) > smem_budget) OTs /= 2;
+    const bool contract_smem = smem_need(OTs) <= smem_budget;
+    const int OT = contract_smem ? OTs
+                                 : std::max(1, std::min(128, static_cast<int>((48 * 1024) / (maxE * sizeof(C)))));
+    const std::size_t csmem = contract_smem ? smem_need(OT) : static_cast<std::size_t>(OT) * maxE * sizeof(C);
+    if (contract_smem) set_smem(k_contract_smem<R>, csmem);
+    else set_smem(k_contract<R>, csmem);
+    const int nnz_cap = static_cast<int>(maxNnz);
     struct D2H {
         void* dst;
         const void* src;
@@ -672,7 +689,10 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     if (!fcr_only) {
         pr.before(f32 ? "contract_f32" : "contract_f64");
         const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
-        k_contract<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(P.conj, OT);
+        if (contract_smem)
+            k_contract_smem<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(P.conj, OT, maxS, nnz_cap);
+        else
+            k_contract<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(P.conj, OT);
         check_launch("k_contract", &pr);
     }
     for (const D2H& c : d2h)
@@ -931,7 +951,8 @@ void plan_execute(Tcl4Plan* plan, cudaStream_t stream) {
     int dev = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev != plan->device) throw Error(kInvalidArgument, "plan belongs to another device");
-    cuda_check(cudaGraphLaunch(plan->exec, stream ? stream : workspace().stream), "cudaGraphLaunch");
+    // asynchronous on exactly the caller's stream (0 is the legacy default stream)
+    cuda_check(cudaGraphLaunch(plan->exec, stream), "cudaGraphLaunch");
     g_launches.fetch_add(plan->kernels);
 }
 

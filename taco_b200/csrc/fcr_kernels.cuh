@@ -111,21 +111,32 @@ __global__ void k_fwd_col(const ColJob* __restrict__ jobs, FftPlan<cplx_t<R>> pl
     const int n2_0 = blockIdx.x << log2c;
     const int elems = ccols << plan.L1;
     const double2 shift = __ldg(&job.g[job.n_in - 1]);
-    for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+    // elems == 8 * blockDim.x: issue the 8 loads of a thread before using any of them
+    double2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int idx = threadIdx.x + q * blockDim.x;
         const int n1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
-        double2 v = make_double2(0.0, 0.0);
-        if (t < job.n_in) {
-            v = csub(__ldg(&job.g[t]), shift);
-            if (job.conj) v.y = -v.y;
-            if (job.has_phase) v = cmul(v, phase_minus(job.omega, job.dt, t));
-        }
-        s[pad_idx<C>(idx)] = from_d2<C>(v);
+        v[q] = t < job.n_in ? __ldg(&job.g[t]) : shift;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int idx = threadIdx.x + q * blockDim.x;
+        const int n1 = idx >> log2c, c = idx & (ccols - 1);
+        const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
+        double2 x = csub(v[q], shift);  // zero beyond n_in
+        if (job.conj) x.y = -x.y;
+        if (job.has_phase && t < job.n_in) x = cmul(x, phase_minus(job.omega, job.dt, t));
+        s[pad_idx<C>(idx)] = from_d2<C>(x);
     }
     __syncthreads();
     tile_fft<C, false, true>(s, plan.L1, log2c, 1, ccols, plan.tw1);
     C* out = static_cast<C*>(job.out);
-    for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+    (void)elems;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int idx = threadIdx.x + q * blockDim.x;
         const int k1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t n2 = n2_0 + c;
         out[static_cast<size_t>(k1) * N2 + n2] =
@@ -148,22 +159,47 @@ __global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, 
     const RowJob job = jobs[blockIdx.y];
     const size_t off = static_cast<size_t>(blockIdx.x) * elems;
     C* data = static_cast<C*>(job.data) + off;
-    for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) a[pad_idx<C>(idx)] = data[idx];
+    // elems == 8 * blockDim.x: 8 loads per thread in flight at once
+    C x[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) x[q] = data[threadIdx.x + q * blockDim.x];
+    const bool conv = job.spec_f != nullptr;
+    // the partner spectra arrive while the forward transform runs
+    C sf[8], sc[8];
+    if (conv) {
+        const C* spf = static_cast<const C*>(job.spec_f) + off;
+        const C* spc = static_cast<const C*>(job.spec_c) + off;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            sf[q] = __ldg(&spf[threadIdx.x + q * blockDim.x]);
+            sc[q] = __ldg(&spc[threadIdx.x + q * blockDim.x]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[pad_idx<C>(threadIdx.x + q * blockDim.x)] = x[q];
     __syncthreads();
     tile_fft<C, false, false>(a, plan.L2, log2r, N2, 1, plan.tw2);
-    if (job.spec_f == nullptr) {
-        for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) data[idx] = a[pad_idx<C>(idx)];
+    if (!conv) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = threadIdx.x + q * blockDim.x;
+            data[idx] = a[pad_idx<C>(idx)];
+        }
         return;
     }
     const int k1_0 = blockIdx.x << log2r;
     for (int which = 0; which < 2; ++which) {
-        const C* spec = static_cast<const C*>(which == 0 ? job.spec_f : job.spec_c) + off;
-        for (int idx = threadIdx.x; idx < elems; idx += blockDim.x)
-            p[pad_idx<C>(idx)] = cmul(a[pad_idx<C>(idx)], spec[idx]);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = threadIdx.x + q * blockDim.x;
+            p[pad_idx<C>(idx)] = cmul(a[pad_idx<C>(idx)], which == 0 ? sf[q] : sc[q]);
+        }
         __syncthreads();
         tile_fft<C, true, false>(p, plan.L2, log2r, N2, 1, plan.tw2);
         C* dst = (which == 0 ? data : static_cast<C*>(job.wc) + off);
-        for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = threadIdx.x + q * blockDim.x;
             const int r = idx >> plan.L2, n2 = idx & (N2 - 1);
             const uint32_t k1 = static_cast<uint32_t>(k1_0 + r);
             dst[idx] = cmulc(p[pad_idx<C>(idx)], inter_twiddle(plan, static_cast<uint32_t>(n2) * k1));
@@ -184,15 +220,23 @@ __global__ void k_inv_col(const InvJob* __restrict__ jobs, FftPlan<cplx_t<R>> pl
     const int n2_0 = blockIdx.x << log2c;
     const int elems = ccols << plan.L1;
     const C* w = static_cast<const C*>(job.w);
-    for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+    (void)elems;
+    C x[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int idx = threadIdx.x + q * blockDim.x;
         const int k1 = idx >> log2c, c = idx & (ccols - 1);
-        s[pad_idx<C>(idx)] = w[static_cast<size_t>(k1) * N2 + n2_0 + c];
+        x[q] = w[static_cast<size_t>(k1) * N2 + n2_0 + c];
     }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s[pad_idx<C>(threadIdx.x + q * blockDim.x)] = x[q];
     __syncthreads();
     tile_fft<C, true, true>(s, plan.L1, log2c, 1, ccols, plan.tw1);
     C* out = static_cast<C*>(job.out);
     const R scale = static_cast<R>(job.scale);
-    for (int idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int idx = threadIdx.x + q * blockDim.x;
         const int n1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
         if (t < job.t_count) out[t] = cscale(s[pad_idx<C>(idx)], scale);
@@ -240,19 +284,32 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_W = 8;  // four complex prefix sums
 
-// One CTA per triple; SCAN_ITEMS consecutive samples per thread; FP64 sums and carries.
-// Prefixes: P_F = sum g_mj e^{+iwt}, P_R1 = sum g_j e^{-iwt}, P_R2 = sum g_i g_j e^{-iwt},
-// S = sum (g_i - c_i) e^{-iwt} (all times dt).
+// The four integrands at sample t (times dt later):
+// P_F <- g_mj e^{+iwt}, P_R1 <- g_j e^{-iwt}, P_R2 <- g_i g_j e^{-iwt}, S <- (g_i - c_i) e^{-iwt}.
+__device__ __forceinline__ void scan_integrands(const ScanJob& job, uint32_t t, double2 ci, double2 pm,
+                                                double2 gi, double* v) {
+    const double2 gmj = __ldg(&job.gmj[t]);
+    const double2 gj = __ldg(&job.gj[t]);
+    const double2 a = cmulc(gmj, pm);
+    const double2 b = cmul(gj, pm);
+    const double2 c = cmul(cmul(gi, gj), pm);
+    const double2 d = cmul(csub(gi, ci), pm);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
+}
+
+// One CTA per triple, SCAN_ITEMS consecutive samples per thread, FP64 sums and carries.
+// Pass 1 of a tile sums each thread's samples; after the block scan, pass 2 recomputes
+// the integrands (cheaper than keeping them live: it doubles the occupancy) and
+// assembles F, C, R at the requested times.
 template <class R>
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_assemble(const ScanJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_assemble(const ScanJob* __restrict__ jobs) {
     using C = cplx_t<R>;
     __shared__ double warp_tot[SCAN_THREADS / 32][SCAN_W];
-    __shared__ double carry_sh[SCAN_W];
+    __shared__ double carry[SCAN_W];
     const ScanJob job = jobs[blockIdx.x];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double carry[SCAN_W];
-#pragma unroll
-    for (int k = 0; k < SCAN_W; ++k) carry[k] = 0.0;
+    if (threadIdx.x < SCAN_W) carry[threadIdx.x] = 0.0;
     const C* cf = static_cast<const C*>(job.conv_f);
     const C* cc = static_cast<const C*>(job.conv_c);
     C* vf = static_cast<C*>(job.vf);
@@ -261,39 +318,26 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_assemble(const ScanJob* _
     const double2 ci = __ldg(&job.gi[job.n_in - 1]);
     const double2 cmj = __ldg(&job.gmj[job.n_in - 1]);
     const double2 cj = __ldg(&job.gj[job.n_in - 1]);
+    const double dt = job.dt;
     const uint32_t tile = SCAN_THREADS * SCAN_ITEMS;
+    __syncthreads();
     for (uint32_t t0 = 0; t0 < job.t_count; t0 += tile) {
-        double y[SCAN_ITEMS][SCAN_W];
+        const uint32_t tb = t0 + threadIdx.x * SCAN_ITEMS;
         double run[SCAN_W];
 #pragma unroll
         for (int k = 0; k < SCAN_W; ++k) run[k] = 0.0;
-        const uint32_t tb = t0 + threadIdx.x * SCAN_ITEMS;
 #pragma unroll
         for (int q = 0; q < SCAN_ITEMS; ++q) {
             const uint32_t t = tb + q;
-            double v[SCAN_W];
-#pragma unroll
-            for (int k = 0; k < SCAN_W; ++k) v[k] = 0.0;
             if (t < job.t_count) {
-                const double2 pm = phase_minus(job.omega, job.dt, t);
-                const double2 gmj = __ldg(&job.gmj[t]);
-                const double2 gj = __ldg(&job.gj[t]);
-                const double2 gi = __ldg(&job.gi[t]);
-                const double2 a = cmulc(gmj, pm);  // g_mj e^{+iwt}
-                const double2 b = cmul(gj, pm);
-                const double2 c = cmul(cmul(gi, gj), pm);
-                const double2 d = cmul(csub(gi, ci), pm);
-                v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-                v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
-            }
+                double v[SCAN_W];
+                scan_integrands(job, t, ci, phase_minus(job.omega, dt, t), __ldg(&job.gi[t]), v);
 #pragma unroll
-            for (int k = 0; k < SCAN_W; ++k) {
-                run[k] += v[k];
-                y[q][k] = run[k];
+                for (int k = 0; k < SCAN_W; ++k) run[k] += v[k];
             }
         }
-        // exclusive scan of the per-thread totals across the block
-        double incl[SCAN_W];
+        // block-exclusive prefix of the per-thread sums
+        double pre[SCAN_W];
 #pragma unroll
         for (int k = 0; k < SCAN_W; ++k) {
             double x = run[k];
@@ -302,35 +346,33 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_assemble(const ScanJob* _
                 const double nb = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= o) x += nb;
             }
-            incl[k] = x;
-        }
-        if (lane == 31) {
-#pragma unroll
-            for (int k = 0; k < SCAN_W; ++k) warp_tot[warp][k] = incl[k];
+            if (lane == 31) warp_tot[warp][k] = x;
+            double excl = __shfl_up_sync(0xffffffffu, x, 1);
+            pre[k] = lane == 0 ? 0.0 : excl;
         }
         __syncthreads();
-        double pre[SCAN_W];
 #pragma unroll
         for (int k = 0; k < SCAN_W; ++k) {
-            double excl = __shfl_up_sync(0xffffffffu, incl[k], 1);
-            if (lane == 0) excl = 0.0;
             double w = 0.0;
             for (int q = 0; q < warp; ++q) w += warp_tot[q][k];
-            pre[k] = carry[k] + (w + excl);
+            pre[k] = carry[k] + (w + pre[k]);
         }
 #pragma unroll
         for (int q = 0; q < SCAN_ITEMS; ++q) {
             const uint32_t t = tb + q;
             if (t >= job.t_count) break;
+            const double2 pm = phase_minus(job.omega, dt, t);
+            const double2 gi = __ldg(&job.gi[t]);
+            double v[SCAN_W];
+            scan_integrands(job, t, ci, pm, gi, v);
+#pragma unroll
+            for (int k = 0; k < SCAN_W; ++k) pre[k] += v[k];
             const int u = __ldg(&job.tmap[t]);
             if (u < 0) continue;
-            const double dt = job.dt;
-            const double2 PF = make_double2((pre[0] + y[q][0]) * dt, (pre[1] + y[q][1]) * dt);
-            const double2 PR1 = make_double2((pre[2] + y[q][2]) * dt, (pre[3] + y[q][3]) * dt);
-            const double2 PR2 = make_double2((pre[4] + y[q][4]) * dt, (pre[5] + y[q][5]) * dt);
-            const double2 S = make_double2((pre[6] + y[q][6]) * dt, (pre[7] + y[q][7]) * dt);
-            const double2 pm = phase_minus(job.omega, job.dt, t);
-            const double2 gi = __ldg(&job.gi[t]);
+            const double2 PF = make_double2(pre[0] * dt, pre[1] * dt);
+            const double2 PR1 = make_double2(pre[2] * dt, pre[3] * dt);
+            const double2 PR2 = make_double2(pre[4] * dt, pre[5] * dt);
+            const double2 S = make_double2(pre[6] * dt, pre[7] * dt);
             const double2 dip = cmul(csub(gi, ci), pm);
             const double2 convf = cadd(to_d2(cf[t]), cmul(cmj, S));
             const double2 convc = cadd(to_d2(cc[t]), cmulc(S, cj));  // conj(c_j) S
@@ -339,17 +381,11 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_assemble(const ScanJob* _
             vr[u] = from_d2<C>(csub(cmul(gi, PR1), PR2));
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < SCAN_W; ++k) {
-                double w = 0.0;
-                for (int q = 0; q < SCAN_THREADS / 32; ++q) w += warp_tot[q][k];
-                carry_sh[k] = carry[k] + w;
-            }
+        if (threadIdx.x < SCAN_W) {
+            double w = 0.0;
+            for (int q = 0; q < SCAN_THREADS / 32; ++q) w += warp_tot[q][threadIdx.x];
+            carry[threadIdx.x] += w;
         }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < SCAN_W; ++k) carry[k] = carry_sh[k];
         __syncthreads();
     }
 }

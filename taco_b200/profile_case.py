@@ -1,0 +1,45 @@
+"""Small, self-contained workload for profiler captures (ncu) of the TCL4 kernels.
+
+Builds `--instances` C2-shaped spin-boson instances (N=200000, dt=5e-4, tidx 0..tmax)
+on the device and runs the batched build `--reps` times through the direct API (no CUDA
+graph, so every kernel is a separate launch a profiler can select).
+
+    python -m taco_b200.profile_case --instances 8 --precision fp32 --reps 2
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+import numpy as np
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--instances", type=int, default=8)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--N", type=int, default=200000)
+    ap.add_argument("--dt", type=float, default=5e-4)
+    ap.add_argument("--tmax", type=int, default=10000)
+    ap.add_argument("--full-length", action="store_true")
+    args = ap.parse_args()
+
+    import torch
+
+    import taco_b200 as tb
+    from taco_b200.workloads import spin_boson_batch
+
+    _, systems, gammas = spin_boson_batch(torch, args.instances, args.N, args.dt, seed=7)
+    tidx = np.arange(args.tmax + 1, dtype=np.uint32)
+    inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
+    torch.cuda.synchronize()
+    for _ in range(args.reps):
+        t0 = time.perf_counter()
+        tb.build_instances(inst, precision=args.precision, full_length=args.full_length)
+        torch.cuda.synchronize()
+        print(f"build {args.instances} x {tidx.size} ({args.precision}): {(time.perf_counter() - t0) * 1e3:.2f} ms")
+
+
+if __name__ == "__main__":
+    main()
