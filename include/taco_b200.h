@@ -141,6 +141,25 @@ int taco_tcl4_plan_create(const taco_tcl4_instance* inst, size_t count, int meth
 int taco_tcl4_plan_execute(taco_tcl4_plan* plan, void* stream);
 int taco_tcl4_plan_destroy(taco_tcl4_plan* plan);
 
+/* No counterpart in the reference.  The L4 build of one instance (the job of
+ * taco_tcl4_build_batch with TACO_IN_DEVICE | TACO_OUT_DEVICE) for callers that cannot
+ * allocate device memory while they run: code inside a framework whose caching allocator
+ * already holds the GPU's memory, latency-critical loops where cudaMalloc/cudaFree would
+ * synchronise the device, plugin hosts that forbid allocation after start-up.  It calls no
+ * cudaMalloc, cudaFree or other allocating routine: all scratch comes from one fixed device
+ * array of TACO_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until the
+ * process exits.  gamma ([Nt x nf] column-major) and L4_out ([T][N^2 x N^2]: complex128 for
+ * TACO_PREC_FP64, complex64 for TACO_PREC_FP32) are device pointers; tidx is a host array
+ * (NULL/T = 0: all Nt).  The FFT length follows max(tidx)+1.  A request whose scratch would
+ * exceed the fixed size fails with TACO_ERR_OVERFLOW and a message stating the need.  The
+ * first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current: make it before any stream capture.  All calls share the array, so
+ * calls that overlap on the GPU (other threads or streams) race; the call synchronises
+ * `stream` (NULL: the legacy default stream) before returning. */
+#define TACO_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int taco_tcl4_build_batch_noalloc(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
+                                  const uint32_t* tidx, size_t T, int precision, void* L4_out, void* stream);
+
 /* propagate_rk4_dense_serial/_omp(L_series[, L_half_series], r, t0, dt, on_sample, sample_every)
  * (cpp/include/taco/rk4_dense.hpp:85-100, 114-129) on the device.
  * L_series: [steps+1][D x D]; L_half: [steps][D x D] or NULL (midpoints by averaging);

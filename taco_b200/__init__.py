@@ -33,10 +33,7 @@ from . import _capi
 from ._capi import (TacoError, TacoInvalidArgument, TacoOutOfRange, TacoOverflow,  # noqa: F401
                     TACO_PREC_FP32, TACO_PREC_FP64)
 from .inputs import System, bcf_fft, gamma_trapz, spin_boson_system  # noqa: F401
-from . import autotune as _autotune
-
-# persisted launch schedules measured by the autotuner (taco_b200/tuning.json)
-_autotune.load()
+from . import autotune as _autotune  # noqa: F401  (schedules load with the library)
 
 __all__ = [
     "System", "bcf_fft", "gamma_trapz", "spin_boson_system", "compute_triple_kernels",

@@ -24,6 +24,7 @@ TACO_IN_DEVICE = 1
 TACO_OUT_DEVICE = 2
 TACO_CAUSAL_TRUNCATION = 4
 TACO_FULL_LENGTH_FFT = 8
+TACO_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
 # every symbol the header declares
 EXPORTED = [
@@ -34,6 +35,7 @@ EXPORTED = [
     "taco_kernel_launches", "taco_profile_enable", "taco_profile_reset", "taco_profile_get",
     "taco_set_tuning", "taco_get_tuning", "taco_clear_tuning",
     "taco_tcl4_plan_create", "taco_tcl4_plan_execute", "taco_tcl4_plan_destroy",
+    "taco_tcl4_build_batch_noalloc",
 ]
 
 
@@ -113,8 +115,29 @@ def lib():
                                             ct.POINTER(ct.c_void_p)]
         L.taco_tcl4_plan_execute.argtypes = [ct.c_void_p, ct.c_void_p]
         L.taco_tcl4_plan_destroy.argtypes = [ct.c_void_p]
+        L.taco_tcl4_build_batch_noalloc.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t,
+                                                    ct.c_double, ct.c_void_p, ct.c_size_t, ct.c_int, ct.c_void_p,
+                                                    ct.c_void_p]
         _lib = L
+        _apply_tuning_table(L)
     return _lib
+
+
+def _apply_tuning_table(L):
+    """Apply the persisted launch schedules measured by the autotuner (taco_b200/tuning.json)."""
+    import json
+
+    path = os.path.join(_PKG, "tuning.json")
+    if not os.path.exists(path):
+        return
+    with open(path) as f:
+        table = json.load(f)
+    for key, sch in table.items():
+        if key.startswith("_"):
+            continue
+        L2, prec = key.split(":")
+        L.taco_set_tuning(int(L2), TACO_PREC_FP32 if prec == "fp32" else TACO_PREC_FP64, int(sch["col_tile"]),
+                          int(sch["row_tile"]), int(sch["chunk_bytes"]), int(sch["inv_dft_rows"]))
 
 
 def check(rc: int) -> None:

@@ -233,6 +233,25 @@ int taco_tcl4_plan_destroy(taco_tcl4_plan* plan) {
     });
 }
 
+int taco_tcl4_build_batch_noalloc(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
+                                  const uint32_t* tidx, size_t T, int precision, void* L4_out, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (precision != TACO_PREC_FP64 && precision != TACO_PREC_FP32)
+            throw taco::Error(taco::kInvalidArgument, "precision must be TACO_PREC_FP64 or TACO_PREC_FP32");
+        taco::SystemDesc s = to_desc(sys);
+        std::vector<uint32_t> t;
+        if (tidx == nullptr || T == 0) {
+            t.resize(Nt);
+            for (std::size_t k = 0; k < Nt; ++k) t[k] = static_cast<uint32_t>(k);
+        } else {
+            t.assign(tidx, tidx + T);
+        }
+        taco::noalloc_tcl4_build(s, reinterpret_cast<const double2*>(gamma), Nt, dt, t, precision == TACO_PREC_FP32,
+                                 g_pad_factor.load(), L4_out, static_cast<cudaStream_t>(stream));
+    });
+}
+
 int taco_rk4_propagate(const void* L_series, const void* L_half, const void* L_add, int l_is_fp32, size_t steps,
                        int D, double dt, taco_c128* r, size_t sample_every, taco_c128* samples,
                        const taco_c128* obs, taco_c128* obs_out, int flags, void* stream) {

@@ -58,6 +58,12 @@ void plan_execute(Tcl4Plan* plan, cudaStream_t stream);
 void plan_destroy(Tcl4Plan* plan);
 uint64_t plan_kernels(const Tcl4Plan* plan);
 
+// L4 build of one instance with every scratch buffer in a fixed file-scope device array
+// (noalloc.cu); gamma and out are device pointers.
+void noalloc_tcl4_build(const SystemDesc& sys, const double2* gamma, std::size_t Nt, double dt,
+                        const std::vector<uint32_t>& tidx, bool fp32, std::size_t pad_factor, void* out,
+                        cudaStream_t stream);
+
 // compute_triple_kernels: full F/C/R series [nf^3][Nt] (FP64) for one instance.
 void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_device, std::size_t Nt,
                     double dt, double2* F, double2* Cc, double2* R, bool out_on_device,
