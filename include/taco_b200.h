@@ -189,6 +189,10 @@ int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t*
 int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows);
 int taco_get_tuning(int log2_nfft, int precision, int* col_tile, int* row_tile, size_t* chunk_bytes,
                     int* inv_dft_rows);
+/* Points per CTA of the thread-block-cluster convolution path for FFT length 2^log2_nfft:
+ * -1 automatic (2^13 FP32 / 2^12 FP64 points per CTA, at most 8 CTAs per cluster), 0 the
+ * multi-pass four-step path, 3..13 a fixed 2^log2_points (clamped to the precision's maximum). */
+int taco_set_cluster_points(int log2_nfft, int precision, int log2_points);
 int taco_clear_tuning(void);
 
 /* Kernel accounting (tracing).  taco_kernel_launches: kernels this library launched since

@@ -33,7 +33,7 @@ EXPORTED = [
     "taco_tcl4_build_batch", "taco_tcl4_build", "taco_tcl4_correction_series",
     "taco_tcl4_build_instances", "taco_rk4_propagate", "taco_l4_coefficients",
     "taco_kernel_launches", "taco_profile_enable", "taco_profile_reset", "taco_profile_get",
-    "taco_set_tuning", "taco_get_tuning", "taco_clear_tuning",
+    "taco_set_tuning", "taco_get_tuning", "taco_clear_tuning", "taco_set_cluster_points",
     "taco_tcl4_plan_create", "taco_tcl4_plan_execute", "taco_tcl4_plan_destroy",
     "taco_tcl4_build_batch_noalloc",
 ]
@@ -111,6 +111,7 @@ def lib():
         L.taco_set_tuning.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_size_t, ct.c_int]
         L.taco_get_tuning.argtypes = [ct.c_int, ct.c_int, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
                                       ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_int)]
+        L.taco_set_cluster_points.argtypes = [ct.c_int, ct.c_int, ct.c_int]
         L.taco_tcl4_plan_create.argtypes = [ct.POINTER(Instance), ct.c_size_t, ct.c_int, ct.c_int, ct.c_int,
                                             ct.POINTER(ct.c_void_p)]
         L.taco_tcl4_plan_execute.argtypes = [ct.c_void_p, ct.c_void_p]
@@ -136,8 +137,11 @@ def _apply_tuning_table(L):
         if key.startswith("_"):
             continue
         L2, prec = key.split(":")
-        L.taco_set_tuning(int(L2), TACO_PREC_FP32 if prec == "fp32" else TACO_PREC_FP64, int(sch["col_tile"]),
-                          int(sch["row_tile"]), int(sch["chunk_bytes"]), int(sch["inv_dft_rows"]))
+        pr = TACO_PREC_FP32 if prec == "fp32" else TACO_PREC_FP64
+        L.taco_set_tuning(int(L2), pr, int(sch["col_tile"]), int(sch["row_tile"]), int(sch["chunk_bytes"]),
+                          int(sch["inv_dft_rows"]))
+        if "cluster_lm" in sch:
+            L.taco_set_cluster_points(int(L2), pr, int(sch["cluster_lm"]))
 
 
 def check(rc: int) -> None:

@@ -104,4 +104,61 @@ __global__ void k_contract_smem(const ContractJob* __restrict__ jobs, int OT, in
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) out[idx] = res[idx];
 }
 
+// Output-per-thread variant: thread o evaluates every L4 entry at output time o, walking
+// the CSR rows with warp-uniform (broadcast) coefficient loads while the lanes gather
+// consecutive times of the same source (coalesced, L1-resident after the first touch).
+// GW is assembled as T + T^H, so GW(c, r) = conj(GW(r, c)) exactly and
+// L4[(n,m),(i,j)] = conj(L4[(m,n),(j,i)]): only entries with e <= partner(e) are summed,
+// the others are their partners' conjugates.  Results are staged in shared memory
+// ([threads][E + 1]) and written as whole matrices.
+constexpr int CONTRACT_ROW_THREADS = 128;
+
+__device__ __forceinline__ uint32_t l4_partner(uint32_t e, int N) {
+    const uint32_t N2 = static_cast<uint32_t>(N) * N;
+    const uint32_t row = e % N2, col = e / N2;
+    const uint32_t n = row % N, m = row / N, i = col % N, j = col / N;
+    return (m + N * n) + N2 * (j + N * i);
+}
+
+template <class R>
+__global__ void __launch_bounds__(CONTRACT_ROW_THREADS) k_contract_rows(const ContractJob* __restrict__ jobs, int N) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* res = reinterpret_cast<C*>(smem_raw);  // [threads][E + 1]
+    const ContractJob job = jobs[blockIdx.y];
+    const uint32_t o0 = blockIdx.x * CONTRACT_ROW_THREADS;
+    if (o0 >= job.T) return;
+    const uint32_t ot = min(static_cast<uint32_t>(CONTRACT_ROW_THREADS), job.T - o0);
+    const uint32_t E = job.E, ld = E + 1;
+    const uint32_t o = o0 + threadIdx.x;
+    const C* coef = static_cast<const C*>(job.coef);
+    const C* v = static_cast<const C*>(job.v);
+    if (threadIdx.x < ot) {
+        const uint32_t u = __ldg(&job.out_u[o]);
+        for (uint32_t e = 0; e < E; ++e) {
+            if (l4_partner(e, N) < e) continue;
+            C acc = C{0, 0};
+            const int32_t b = __ldg(&job.rowptr[e]), end = __ldg(&job.rowptr[e + 1]);
+            for (int32_t k = b; k < end; ++k) {
+                const uint32_t sk = __ldg(&job.src[k]);
+                C x = v[static_cast<size_t>(sk & 0x7fffffffu) * job.U + u];
+                if (sk & 0x80000000u) x.y = -x.y;
+                acc = cadd(acc, cmul(coef[k], x));
+            }
+            res[threadIdx.x * ld + e] = acc;
+        }
+        for (uint32_t e = 0; e < E; ++e) {
+            const uint32_t p = l4_partner(e, N);
+            if (p < e) res[threadIdx.x * ld + e] = cconj(res[threadIdx.x * ld + p]);
+        }
+    }
+    __syncthreads();
+    C* out = static_cast<C*>(job.out) + static_cast<size_t>(o0) * E;
+    const uint32_t total = ot * E;
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const uint32_t ol = idx / E, e = idx - ol * E;
+        out[idx] = res[ol * ld + e];
+    }
+}
+
 }  // namespace taco

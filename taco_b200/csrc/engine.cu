@@ -21,6 +21,7 @@
 #include <memory>
 #include <unordered_map>
 
+#include "cluster_conv.cuh"
 #include "contract.cuh"
 #include "fcr_kernels.cuh"
 #include "gw_coef.hpp"
@@ -179,6 +180,87 @@ FftPlan<cplx_t<R>> get_plan(Workspace& ws, int L, cudaStream_t st) {
     p.twc = lay.take<C>(N >> pt.s);
     p.twf = lay.take<C>(std::size_t(1) << pt.s);
     return p;
+}
+
+// Tables of the cluster path: M-point twiddles and the N-point coarse/fine tables.
+template <class R>
+ClusterPlan<cplx_t<R>> get_cluster_plan(Workspace& ws, int L, int LM, cudaStream_t st) {
+    using C = cplx_t<R>;
+    const bool fp32 = std::is_same<R, float>::value;
+    auto& slot = ws.plans[{L + 64 * (LM + 1), fp32 ? 1 : 0}];
+    const int s = (L + 1) / 2;
+    const std::size_t N = std::size_t(1) << L, M = std::size_t(1) << LM;
+    const std::size_t nc = N >> s, nfine = std::size_t(1) << s;
+    if (!slot) {
+        auto pt = std::make_unique<PlanTables>();
+        pt->buf.ensure((M + nc + nfine) * sizeof(C) + 3 * 256);
+        Layout lay{static_cast<char*>(pt->buf.p)};
+        C* twM = lay.take<C>(M);
+        C* twc = lay.take<C>(nc);
+        C* twf = lay.take<C>(nfine);
+        auto fill = [&](C* p, std::size_t count, double denom) {
+            k_fill_twiddle<C><<<static_cast<unsigned>((count + 255) / 256), 256, 0, st>>>(p, static_cast<uint32_t>(count), denom);
+            cuda_check(cudaGetLastError(), "k_fill_twiddle");
+            g_launches.fetch_add(1);
+        };
+        fill(twM, M, static_cast<double>(M));
+        fill(twc, nc, static_cast<double>(nc));
+        fill(twf, nfine, static_cast<double>(N));
+        slot = std::move(pt);
+    }
+    Layout lay{static_cast<char*>(slot->buf.p)};
+    ClusterPlan<C> p;
+    p.LN = L;
+    p.LM = LM;
+    p.s = s;
+    p.twM = lay.take<C>(M);
+    p.twc = lay.take<C>(nc);
+    p.twf = lay.take<C>(nfine);
+    return p;
+}
+
+template <class R, int KLOG>
+void launch_cluster_k(const ClusterJob* jobs, std::size_t njobs, const ClusterPlan<cplx_t<R>>& plan, std::size_t smem,
+                      cudaStream_t st) {
+    cuda_check(cudaFuncSetAttribute(k_conv_cluster<R, KLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)),
+               "cudaFuncSetAttribute(cluster smem)");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(njobs << KLOG), 1, 1);
+    cfg.blockDim = dim3(static_cast<unsigned>((1u << plan.LM) / 8), 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1u << KLOG;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cuda_check(cudaLaunchKernelEx(&cfg, k_conv_cluster<R, KLOG>, jobs, plan), "cudaLaunchKernelEx(k_conv_cluster)");
+}
+
+template <class R>
+void launch_cluster(const ClusterJob* jobs, std::size_t njobs, const ClusterPlan<cplx_t<R>>& plan, cudaStream_t st) {
+    using C = cplx_t<R>;
+    const std::size_t smem = 2 * static_cast<std::size_t>(padded_size<C>(1 << plan.LM)) * sizeof(C);
+    switch (plan.LN - plan.LM) {
+        case 0: launch_cluster_k<R, 0>(jobs, njobs, plan, smem, st); break;
+        case 1: launch_cluster_k<R, 1>(jobs, njobs, plan, smem, st); break;
+        case 2: launch_cluster_k<R, 2>(jobs, njobs, plan, smem, st); break;
+        case 3: launch_cluster_k<R, 3>(jobs, njobs, plan, smem, st); break;
+        default: throw Error(kInvalidArgument, "cluster path: at most 8 CTAs per cluster");
+    }
+}
+
+// Points per CTA of the cluster path for FFT length 2^L, or -1 when the multi-pass path runs.
+int cluster_lm_for(int L, bool fp32, const Tuning& t) {
+    const int lm_max = fp32 ? 13 : 12;  // 1024 / 512 threads, two padded tiles in shared memory
+    if (t.cluster_lm == 0) return -1;
+    int lm = t.cluster_lm > 0 ? std::min(t.cluster_lm, lm_max) : std::min(L, lm_max);
+    lm = std::min(lm, L);
+    if (lm < 3 || L - lm > 3) return -1;
+    return lm;
 }
 
 template <class K>
@@ -345,6 +427,10 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     }
     const std::size_t ntri = tris.size();
     // chunk of triples whose Z / W intermediates are meant to stay in L2 between passes
+    const int clm = cluster_lm_for(L, std::is_same<R, float>::value, tune);
+    const bool use_cluster = clm > 0;
+    ClusterPlan<C> cplan{};
+    if (use_cluster) cplan = get_cluster_plan<R>(ws, L, clm, st);
     const std::size_t per_tri_scratch = 2 * Nfft * sizeof(C);
     std::size_t Q = std::max<std::size_t>(1, tune.chunk_bytes / per_tri_scratch);
     Q = std::min<std::size_t>({Q, ntri, 65535});
@@ -355,6 +441,7 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     const int N2 = 1 << plan.L2;
     const int inv_rows = static_cast<int>((max_tcount + N2 - 1) / N2);
     const bool inv_dft = inv_rows <= std::min(tune.inv_dft_rows, INV_DFT_MAXR);
+    const int max_chunks = static_cast<int>((max_tcount + SCAN_CHUNK - 1) / SCAN_CHUNK);
 
     // ---- device layout ----
     struct Ptrs {
@@ -369,6 +456,8 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
         std::vector<C*> coef;
         std::vector<C*> out;
         C* scratch = nullptr;
+        double* partial = nullptr;
+        ClusterJob* clj = nullptr;
         ColJob* colj = nullptr;
         RowJob* rowj = nullptr;
         InvJob* invj = nullptr;
@@ -415,7 +504,9 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
                 P.v[a] = lay.take<C>(3 * nf3 * m.U);
             }
         }
-        P.scratch = lay.take<C>(Q * 2 * Nfft);
+        P.scratch = lay.take<C>(use_cluster ? 1 : Q * 2 * Nfft);
+        P.partial = lay.take<double>(ntri * max_chunks * SCAN_W);
+        P.clj = lay.take<ClusterJob>(n_spec_jobs + ntri);
         P.colj = lay.take<ColJob>(n_col_jobs);
         P.rowj = lay.take<RowJob>(n_row_jobs);
         P.invj = lay.take<InvJob>(2 * ntri);
@@ -507,6 +598,18 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
             s.vr = P.v[a] + (2 * nf3 + tri) * m.U;
         }
     }
+    // the same jobs for the cluster path (spectra in its [K][M] order)
+    std::vector<ClusterJob> clj(n_spec_jobs + ntri);
+    for (std::size_t k = 0; k < n_spec_jobs; ++k) {
+        const ColJob& c = colj[k];
+        clj[k] = ClusterJob{c.g, 0.0, c.dt, 0, c.conj, c.n_in, 0u, 0.0, nullptr, nullptr, c.out, nullptr};
+    }
+    for (std::size_t q = 0; q < ntri; ++q) {
+        const ColJob& c = colj[n_spec_jobs + q];
+        const RowJob& r = rowj[n_spec_jobs + q];
+        clj[n_spec_jobs + q] = ClusterJob{c.g, c.omega, c.dt, 1, 0, c.n_in, invj[2 * q].t_count, invj[2 * q].scale,
+                                          r.spec_f, r.spec_c, invj[2 * q].out, invj[2 * q + 1].out};
+    }
     if (!fcr_only) {
         for (std::size_t a = 0; a < ni; ++a) {
             const Tcl4Instance& in = *insts[a];
@@ -543,6 +646,7 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     plan_copy(P.rowj, rowj.size() * sizeof(RowJob));
     plan_copy(P.invj, invj.size() * sizeof(InvJob));
     plan_copy(P.scanj, scanj.size() * sizeof(ScanJob));
+    plan_copy(P.clj, clj.size() * sizeof(ClusterJob));
     if (!fcr_only) plan_copy(P.conj, conj.size() * sizeof(ContractJob));
     for (std::size_t a = 0; a < ni; ++a) {
         const InstMeta& m = *metas[a];
@@ -567,6 +671,7 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
         put(rowj.data(), rowj.size() * sizeof(RowJob));
         put(invj.data(), invj.size() * sizeof(InvJob));
         put(scanj.data(), scanj.size() * sizeof(ScanJob));
+        put(clj.data(), clj.size() * sizeof(ClusterJob));
         if (!fcr_only) put(conj.data(), conj.size() * sizeof(ContractJob));
         for (std::size_t a = 0; a < ni; ++a) {
             const InstMeta& m = *metas[a];
@@ -611,7 +716,17 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     for (auto* m : metas) maxNnz = std::max(maxNnz, m->coef.src.size());
     std::size_t maxT = 0;
     for (auto* m : metas) maxT = std::max(maxT, m->T);
-    // shared-memory contraction when the F/C/R tile of >= 16 outputs and the CSR table fit
+    // contraction: one thread per output time while a [threads][E+1] result tile fits in
+    // shared memory (d <= 3); the shared-memory-tile kernels otherwise
+    const std::size_t rows_smem = static_cast<std::size_t>(CONTRACT_ROW_THREADS) * (maxE + 1) * sizeof(C);
+    const bool contract_rows = rows_smem <= 100 * 1024;
+    int maxN = 0;
+    for (auto* in : insts) maxN = std::max(maxN, in->sys.N);
+    const bool same_N = [&] {
+        for (auto* in : insts)
+            if (in->sys.N != maxN) return false;
+        return true;
+    }();
     const std::size_t smem_budget = 100 * 1024;
     const std::size_t csr_bytes = maxNnz * (sizeof(C) + 4) + (maxE + 1) * 4 + 64;
     int OTs = 128;
@@ -619,11 +734,15 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
         return (static_cast<std::size_t>(maxS) + maxE) * ot * sizeof(C) + csr_bytes;
     };
     while (OTs > 16 && smem_need(OTs) > smem_budget) OTs /= 2;
-    const bool contract_smem = smem_need(OTs) <= smem_budget;
-    const int OT = contract_smem ? OTs
-                                 : std::max(1, std::min(128, static_cast<int>((48 * 1024) / (maxE * sizeof(C)))));
-    const std::size_t csmem = contract_smem ? smem_need(OT) : static_cast<std::size_t>(OT) * maxE * sizeof(C);
-    if (contract_smem) set_smem(k_contract_smem<R>, csmem);
+    const bool use_rows = contract_rows && same_N;
+    const bool contract_smem = !use_rows && smem_need(OTs) <= smem_budget;
+    const int OT = use_rows ? CONTRACT_ROW_THREADS
+                            : contract_smem ? OTs
+                                            : std::max(1, std::min(128, static_cast<int>((48 * 1024) / (maxE * sizeof(C)))));
+    const std::size_t csmem = use_rows ? rows_smem
+                                       : contract_smem ? smem_need(OT) : static_cast<std::size_t>(OT) * maxE * sizeof(C);
+    if (use_rows) set_smem(k_contract_rows<R>, csmem);
+    else if (contract_smem) set_smem(k_contract_smem<R>, csmem);
     else set_smem(k_contract<R>, csmem);
     const int nnz_cap = static_cast<int>(maxNnz);
     struct D2H {
@@ -652,44 +771,60 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     ProfRecorder& pr = prp ? *prp : dummy;
     const bool f32 = std::is_same<R, float>::value;
     if (ev0) cuda_check(cudaEventRecord(ev0, st), "cudaEventRecord");
-    pr.before(f32 ? "spectra_col_f32" : "spectra_col_f64");
-    k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(n_spec_jobs)), g.col_threads, g.col_smem, st>>>(
-        P.colj, plan, g.log2c);
-    check_launch("k_fwd_col(spectra)", &pr);
-    pr.before(f32 ? "spectra_row_f32" : "spectra_row_f64");
-    k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
-        P.rowj, plan, g.log2r);
-    check_launch("k_row(spectra)", &pr);
-    const unsigned dft_grid = static_cast<unsigned>((N2 + INV_DFT_THREADS - 1) / INV_DFT_THREADS);
-    for (std::size_t ch = 0; ch < nchunks; ++ch) {
-        const std::size_t q0 = ch * Q, nq = std::min(Q, ntri - q0);
-        pr.before(f32 ? "fwd_col_f32" : "fwd_col_f64");
-        k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(nq)), g.col_threads, g.col_smem, st>>>(
-            P.colj + n_spec_jobs + q0, plan, g.log2c);
-        check_launch("k_fwd_col", &pr);
-        pr.before(f32 ? "row_conv_f32" : "row_conv_f64");
-        k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
-            P.rowj + n_spec_jobs + q0, plan, g.log2r);
-        check_launch("k_row", &pr);
-        pr.before(f32 ? "inv_col_f32" : "inv_col_f64");
-        if (inv_dft) {
-            k_inv_col_dft<R><<<dim3(dft_grid, static_cast<unsigned>(2 * nq)), INV_DFT_THREADS, 0, st>>>(
-                P.invj + 2 * q0, plan, inv_rows);
-            check_launch("k_inv_col_dft", &pr);
-        } else {
-            k_inv_col<R><<<dim3(g.col_grid, static_cast<unsigned>(2 * nq)), g.col_threads, g.col_smem, st>>>(
-                P.invj + 2 * q0, plan, g.log2c);
-            check_launch("k_inv_col", &pr);
+    if (use_cluster) {
+        pr.before(f32 ? "spectra_cluster_f32" : "spectra_cluster_f64");
+        launch_cluster<R>(P.clj, n_spec_jobs, cplan, st);
+        check_launch("k_conv_cluster(spectra)", &pr);
+        pr.before(f32 ? "conv_cluster_f32" : "conv_cluster_f64");
+        launch_cluster<R>(P.clj + n_spec_jobs, ntri, cplan, st);
+        check_launch("k_conv_cluster", &pr);
+    } else {
+        pr.before(f32 ? "spectra_col_f32" : "spectra_col_f64");
+        k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(n_spec_jobs)), g.col_threads, g.col_smem, st>>>(
+            P.colj, plan, g.log2c);
+        check_launch("k_fwd_col(spectra)", &pr);
+        pr.before(f32 ? "spectra_row_f32" : "spectra_row_f64");
+        k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
+            P.rowj, plan, g.log2r);
+        check_launch("k_row(spectra)", &pr);
+        const unsigned dft_grid = static_cast<unsigned>((N2 + INV_DFT_THREADS - 1) / INV_DFT_THREADS);
+        for (std::size_t ch = 0; ch < nchunks; ++ch) {
+            const std::size_t q0 = ch * Q, nq = std::min(Q, ntri - q0);
+            pr.before(f32 ? "fwd_col_f32" : "fwd_col_f64");
+            k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(nq)), g.col_threads, g.col_smem, st>>>(
+                P.colj + n_spec_jobs + q0, plan, g.log2c);
+            check_launch("k_fwd_col", &pr);
+            pr.before(f32 ? "row_conv_f32" : "row_conv_f64");
+            k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
+                P.rowj + n_spec_jobs + q0, plan, g.log2r);
+            check_launch("k_row", &pr);
+            pr.before(f32 ? "inv_col_f32" : "inv_col_f64");
+            if (inv_dft) {
+                k_inv_col_dft<R><<<dim3(dft_grid, static_cast<unsigned>(2 * nq)), INV_DFT_THREADS, 0, st>>>(
+                    P.invj + 2 * q0, plan, inv_rows);
+                check_launch("k_inv_col_dft", &pr);
+            } else {
+                k_inv_col<R><<<dim3(g.col_grid, static_cast<unsigned>(2 * nq)), g.col_threads, g.col_smem, st>>>(
+                    P.invj + 2 * q0, plan, g.log2c);
+                check_launch("k_inv_col", &pr);
+            }
         }
     }
+    pr.before(f32 ? "scan_reduce_f32" : "scan_reduce_f64");
+    k_scan_reduce<R><<<dim3(static_cast<unsigned>(max_chunks), static_cast<unsigned>(n_scan)), SCAN_THREADS, 0, st>>>(
+        P.scanj, P.partial, max_chunks);
+    check_launch("k_scan_reduce", &pr);
     pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
-    k_scan_assemble<R><<<static_cast<unsigned>(n_scan), SCAN_THREADS, 0, st>>>(P.scanj);
-    check_launch("k_scan_assemble", &pr);
+    k_scan_chunks<R><<<dim3(static_cast<unsigned>(max_chunks), static_cast<unsigned>(n_scan)), SCAN_THREADS, 0, st>>>(
+        P.scanj, P.partial, max_chunks);
+    check_launch("k_scan_chunks", &pr);
     if (ev1) cuda_check(cudaEventRecord(ev1, st), "cudaEventRecord");
     if (!fcr_only) {
         pr.before(f32 ? "contract_f32" : "contract_f64");
         const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
-        if (contract_smem)
+        if (use_rows)
+            k_contract_rows<R><<<dim3(gx, static_cast<unsigned>(ni)), CONTRACT_ROW_THREADS, csmem, st>>>(P.conj, maxN);
+        else if (contract_smem)
             k_contract_smem<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(P.conj, OT, maxS, nnz_cap);
         else
             k_contract<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(P.conj, OT);

@@ -35,6 +35,7 @@ struct Tuning {
     int row_tile = 2048;                        // elements per row-pass tile
     std::size_t chunk_bytes = std::size_t(48) << 20;  // Z/W scratch per chunk of triples
     int inv_dft_rows = 16;                      // pruned inverse column DFT up to this many rows
+    int cluster_lm = 0;  // log2 points per CTA of the cluster path (0: multi-pass path, -1: automatic)
 };
 void set_tuning(int L, bool fp32, const Tuning& t);
 Tuning get_tuning(int L, bool fp32);

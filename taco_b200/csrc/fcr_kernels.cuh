@@ -390,4 +390,138 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_assemble(const ScanJob
     }
 }
 
+// ------------------------------------------------------- chunked scans ----
+// Reduce-then-scan over chunks of SCAN_THREADS*SCAN_ITEMS samples, so that one triple's
+// time axis spreads over many CTAs: k_scan_reduce writes the FP64 integrand sums of each
+// chunk; k_scan_chunks adds the sums of the preceding chunks of its triple (its carry),
+// rescans its chunk and assembles F, C, R.  No CTA waits on another.
+constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ void block_sum8(double* v, double (*warp_tot)[SCAN_W]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < SCAN_W; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) warp_tot[warp][k] = x;
+    }
+    __syncthreads();
+}
+
+template <class R>  // R unused: a template keeps the header-defined kernel out of every TU's link
+__global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_reduce(const ScanJob* __restrict__ jobs,
+                                                                  double* __restrict__ partial, int max_chunks) {
+    __shared__ double warp_tot[SCAN_THREADS / 32][SCAN_W];
+    const ScanJob job = jobs[blockIdx.y];
+    const uint32_t t0 = blockIdx.x * SCAN_CHUNK;
+    if (t0 >= job.t_count) return;
+    const double2 ci = __ldg(&job.gi[job.n_in - 1]);
+    double run[SCAN_W];
+#pragma unroll
+    for (int k = 0; k < SCAN_W; ++k) run[k] = 0.0;
+    const uint32_t tb = t0 + threadIdx.x * SCAN_ITEMS;
+#pragma unroll
+    for (int q = 0; q < SCAN_ITEMS; ++q) {
+        const uint32_t t = tb + q;
+        if (t < job.t_count) {
+            double v[SCAN_W];
+            scan_integrands(job, t, ci, phase_minus(job.omega, job.dt, t), __ldg(&job.gi[t]), v);
+#pragma unroll
+            for (int k = 0; k < SCAN_W; ++k) run[k] += v[k];
+        }
+    }
+    block_sum8(run, warp_tot);
+    if (threadIdx.x < SCAN_W) {
+        double w = 0.0;
+        for (int q = 0; q < SCAN_THREADS / 32; ++q) w += warp_tot[q][threadIdx.x];
+        partial[(static_cast<size_t>(blockIdx.y) * max_chunks + blockIdx.x) * SCAN_W + threadIdx.x] = w;
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_chunks(const ScanJob* __restrict__ jobs,
+                                                                  const double* __restrict__ partial,
+                                                                  int max_chunks) {
+    using C = cplx_t<R>;
+    __shared__ double warp_tot[SCAN_THREADS / 32][SCAN_W];
+    __shared__ double carry[SCAN_W];
+    const ScanJob job = jobs[blockIdx.y];
+    const uint32_t t0 = blockIdx.x * SCAN_CHUNK;
+    if (t0 >= job.t_count) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x < SCAN_W) {
+        double w = 0.0;
+        const double* pp = partial + static_cast<size_t>(blockIdx.y) * max_chunks * SCAN_W + threadIdx.x;
+        for (uint32_t c = 0; c < blockIdx.x; ++c) w += pp[c * SCAN_W];
+        carry[threadIdx.x] = w;
+    }
+    const C* cf = static_cast<const C*>(job.conv_f);
+    const C* cc = static_cast<const C*>(job.conv_c);
+    C* vf = static_cast<C*>(job.vf);
+    C* vc = static_cast<C*>(job.vc);
+    C* vr = static_cast<C*>(job.vr);
+    const double2 ci = __ldg(&job.gi[job.n_in - 1]);
+    const double2 cmj = __ldg(&job.gmj[job.n_in - 1]);
+    const double2 cj = __ldg(&job.gj[job.n_in - 1]);
+    const double dt = job.dt;
+    const uint32_t tb = t0 + threadIdx.x * SCAN_ITEMS;
+    double run[SCAN_W];
+#pragma unroll
+    for (int k = 0; k < SCAN_W; ++k) run[k] = 0.0;
+#pragma unroll
+    for (int q = 0; q < SCAN_ITEMS; ++q) {
+        const uint32_t t = tb + q;
+        if (t < job.t_count) {
+            double v[SCAN_W];
+            scan_integrands(job, t, ci, phase_minus(job.omega, dt, t), __ldg(&job.gi[t]), v);
+#pragma unroll
+            for (int k = 0; k < SCAN_W; ++k) run[k] += v[k];
+        }
+    }
+    double pre[SCAN_W];
+#pragma unroll
+    for (int k = 0; k < SCAN_W; ++k) {
+        double x = run[k];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double nb = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += nb;
+        }
+        if (lane == 31) warp_tot[warp][k] = x;
+        const double excl = __shfl_up_sync(0xffffffffu, x, 1);
+        pre[k] = lane == 0 ? 0.0 : excl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < SCAN_W; ++k) {
+        double w = 0.0;
+        for (int q = 0; q < warp; ++q) w += warp_tot[q][k];
+        pre[k] = carry[k] + (w + pre[k]);
+    }
+#pragma unroll
+    for (int q = 0; q < SCAN_ITEMS; ++q) {
+        const uint32_t t = tb + q;
+        if (t >= job.t_count) break;
+        const double2 pm = phase_minus(job.omega, dt, t);
+        const double2 gi = __ldg(&job.gi[t]);
+        double v[SCAN_W];
+        scan_integrands(job, t, ci, pm, gi, v);
+#pragma unroll
+        for (int k = 0; k < SCAN_W; ++k) pre[k] += v[k];
+        const int u = __ldg(&job.tmap[t]);
+        if (u < 0) continue;
+        const double2 PF = make_double2(pre[0] * dt, pre[1] * dt);
+        const double2 PR1 = make_double2(pre[2] * dt, pre[3] * dt);
+        const double2 PR2 = make_double2(pre[4] * dt, pre[5] * dt);
+        const double2 S = make_double2(pre[6] * dt, pre[7] * dt);
+        const double2 dip = cmul(csub(gi, ci), pm);
+        const double2 convf = cadd(to_d2(cf[t]), cmul(cmj, S));
+        const double2 convc = cadd(to_d2(cc[t]), cmulc(S, cj));
+        vf[u] = from_d2<C>(csub(cmul(dip, PF), convf));
+        vc[u] = from_d2<C>(csub(cmulc(dip, PR1), convc));
+        vr[u] = from_d2<C>(csub(cmul(gi, PR1), PR2));
+    }
+}
+
 }  // namespace taco
