@@ -173,6 +173,28 @@ int taco_rk4_propagate(const void* L_series, const void* L_half, const void* L_a
                        taco_c128* samples, const taco_c128* obs, taco_c128* obs_out, int flags,
                        void* stream);
 
+/* The TCL2 generator L2(t) = -i[diag(eps) + H_LS(t), .] + D2(t) at the requested times
+ * (build_tcl2_components(...).total(), cpp/src/tcl/generator.cpp:164-177, with the
+ * spin-boson example's kernel fill, examples/TCL4_spin_boson_example.cpp:303-315).
+ * eps: [N] eigenvalues (host).  L2_out: [T][N^2 x N^2] complex128. */
+int taco_tcl2_generator_series(const taco_system_view* sys, const double* eps, const taco_c128* gamma, size_t Nt,
+                               const uint32_t* tidx, size_t T, taco_c128* L2_out, int flags, void* stream);
+
+/* gamma::compute_trapz_prefix_multi_matrix (cpp/include/taco/gamma.hpp:166-213) on the
+ * device: G [M][N] (the reference's column-major N x M) from C [N]; omegas: host [M]. */
+int taco_gamma_trapz(const taco_c128* C, size_t N, double dt, const double* omegas, size_t M, taco_c128* G,
+                     int flags, void* stream);
+
+/* The example's propagation (examples/TCL4_spin_boson_example.cpp:317-394) on the device:
+ * L(t_k) = L0 (order 0), L2(t_k) (order 2) or L2(t_k) + L4(t_k) (order 4) for k = 0..steps,
+ * RK4 with midpoints by averaging, rho(0) = rho0 ([N^2] vec, eigenbasis), FP64 state.
+ * obs (nullable, [N^2]) gives <O>(t) = sum_l obs_l r_l every sample_every steps plus the
+ * final step (obs_out: ceil(steps/sample_every)+1 values); rho_out (nullable): final state.
+ * precision applies to the L4 build (FP32: complex64 L4 added to the FP64 L2). */
+int taco_propagate_tcl(const taco_system_view* sys, const double* eps, const taco_c128* gamma, size_t Nt, double dt,
+                       size_t steps, int order, int precision, const taco_c128* rho0, const taco_c128* obs,
+                       size_t sample_every, taco_c128* obs_out, taco_c128* rho_out, int flags, void* stream);
+
 /* The time-independent linear map L4_e(t) = sum_k coef_k * v_{src_k}(t) (v conjugated when
  * bit 31 of src_k is set) of the MIKX -> GW -> L4 chain (cpp/src/tcl/tcl4_mikx.cpp:87-177,
  * cpp/src/tcl/tcl4_assemble.cpp:53-230).  Sources: F (s < nf^3), C, R of triple s mod nf^3.

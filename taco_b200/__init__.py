@@ -39,7 +39,8 @@ __all__ = [
     "System", "bcf_fft", "gamma_trapz", "spin_boson_system", "compute_triple_kernels",
     "build_TCL4_generator", "build_TCL4_generator_batch", "build_correction_series", "build_instances",
     "propagate_rk4_dense", "l4_coefficients", "Tcl4Plan", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
-    "version", "device_count", "kernel_launches", "profile",
+    "version", "device_count", "kernel_launches", "profile", "tcl2_generator_series", "gamma_trapz_device",
+    "propagate_tcl",
 ]
 
 
@@ -358,6 +359,69 @@ def propagate_rk4_dense(L_series, r0, dt: float, L_half=None, L_add=None, sample
                                                _ptr(r), sample_every if sample_every > 0 else 0, _ptr(samples),
                                                _ptr(o), _ptr(obs_out), flags, _stream_ptr(Ls) if dev else None))
     return r, samples, obs_out
+
+
+def tcl2_generator_series(system: System, gamma, time_indices=None):
+    """L2(t) (TCL2 total(), generator.cpp:164-177) at the requested times: [T, N^2, N^2]."""
+    if getattr(system, "eps", None) is None:
+        raise ValueError("tcl2_generator_series needs the system eigenvalues (System.eps)")
+    g, dev = _prep_gamma(gamma)
+    nf, Nt = g.shape
+    tid = None if time_indices is None else np.ascontiguousarray(time_indices, np.uint32)
+    T = Nt if tid is None or tid.size == 0 else tid.size
+    N2 = int(system.N) ** 2
+    out = _out_array(dev, (T, N2 * N2), np.complex128, g.device if dev else None)
+    eps = np.ascontiguousarray(system.eps, np.float64)
+    v = _View(system)
+    flags = (_capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE) if dev else 0
+    _capi.check(_capi.lib().taco_tcl2_generator_series(ct.byref(v.view), _ptr(eps), _ptr(g), Nt, _ptr(tid),
+                                                       0 if tid is None else tid.size, _ptr(out), flags,
+                                                       _stream_ptr(g)))
+    return _l4_view(out, N2)
+
+
+def gamma_trapz_device(C, dt: float, omegas):
+    """Gamma_b(t_k) by the trapezoid rule on the device (gamma.hpp:166-213): [nb, N]."""
+    dev = _is_torch(C) and C.is_cuda
+    if dev:
+        torch = _torch()
+        c = C.to(torch.complex128).contiguous()
+    else:
+        c = _c128_host(C)
+    om = np.ascontiguousarray(omegas, np.float64)
+    out = _out_array(dev, (om.size, c.shape[0]), np.complex128, c.device if dev else None)
+    flags = (_capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE) if dev else 0
+    _capi.check(_capi.lib().taco_gamma_trapz(_ptr(c), c.shape[0], float(dt), _ptr(om), om.size, _ptr(out), flags,
+                                             _stream_ptr(c)))
+    return out
+
+
+def propagate_tcl(system: System, gamma, dt: float, steps: int, rho0, obs=None, order: int = 4,
+                  sample_every: int = 1, precision: str = "fp64"):
+    """RK4 propagation of vec(rho) under L = L2 + L4 (order 4), L2 (order 2) or L0 (order 0)
+    on the device (examples/TCL4_spin_boson_example.cpp:317-394).  rho0: [N^2] eigenbasis
+    vec; obs: [N^2] weights with <O> = sum_l obs_l r_l.  Returns (obs_values or None, rho_final)."""
+    g, dev = _prep_gamma(gamma)
+    nf, Nt = g.shape
+    D = int(system.N) ** 2
+    eps = np.ascontiguousarray(system.eps, np.float64)
+    prec = {"fp64": _capi.TACO_PREC_FP64, "fp32": _capi.TACO_PREC_FP32}[precision]
+    if dev:
+        torch = _torch()
+        r0 = torch.as_tensor(rho0, dtype=torch.complex128, device=g.device).contiguous()
+        o = torch.as_tensor(obs, dtype=torch.complex128, device=g.device).contiguous() if obs is not None else None
+    else:
+        r0 = _c128_host(rho0)
+        o = _c128_host(obs) if obs is not None else None
+    ns = (steps + sample_every - 1) // sample_every + 1
+    obs_out = _out_array(dev, (ns,), np.complex128, g.device if dev else None) if obs is not None else None
+    rho_out = _out_array(dev, (D,), np.complex128, g.device if dev else None)
+    v = _View(system)
+    flags = (_capi.TACO_IN_DEVICE | _capi.TACO_OUT_DEVICE) if dev else 0
+    _capi.check(_capi.lib().taco_propagate_tcl(ct.byref(v.view), _ptr(eps), _ptr(g), Nt, float(dt), int(steps),
+                                               int(order), prec, _ptr(r0), _ptr(o), int(sample_every), _ptr(obs_out),
+                                               _ptr(rho_out), flags, _stream_ptr(g)))
+    return obs_out, rho_out
 
 
 def l4_coefficients(system: System):

@@ -35,7 +35,7 @@ EXPORTED = [
     "taco_kernel_launches", "taco_profile_enable", "taco_profile_reset", "taco_profile_get",
     "taco_set_tuning", "taco_get_tuning", "taco_clear_tuning", "taco_set_cluster_points",
     "taco_tcl4_plan_create", "taco_tcl4_plan_execute", "taco_tcl4_plan_destroy",
-    "taco_tcl4_build_batch_noalloc",
+    "taco_tcl4_build_batch_noalloc", "taco_tcl2_generator_series", "taco_gamma_trapz", "taco_propagate_tcl",
 ]
 
 
@@ -116,6 +116,13 @@ def lib():
                                             ct.POINTER(ct.c_void_p)]
         L.taco_tcl4_plan_execute.argtypes = [ct.c_void_p, ct.c_void_p]
         L.taco_tcl4_plan_destroy.argtypes = [ct.c_void_p]
+        L.taco_tcl2_generator_series.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_void_p, ct.c_size_t,
+                                                 ct.c_void_p, ct.c_size_t, ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.taco_gamma_trapz.argtypes = [ct.c_void_p, ct.c_size_t, ct.c_double, ct.c_void_p, ct.c_size_t, ct.c_void_p,
+                                       ct.c_int, ct.c_void_p]
+        L.taco_propagate_tcl.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_void_p, ct.c_size_t, ct.c_double,
+                                         ct.c_size_t, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_size_t,
+                                         ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]
         L.taco_tcl4_build_batch_noalloc.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t,
                                                     ct.c_double, ct.c_void_p, ct.c_size_t, ct.c_int, ct.c_void_p,
                                                     ct.c_void_p]

@@ -20,10 +20,11 @@ DEFAULT_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning
 
 
 def set_schedule(log2_nfft: int, precision: str, col_tile: int, row_tile: int, chunk_bytes: int,
-                 inv_dft_rows: int) -> None:
+                 inv_dft_rows: int, cluster_lm: int = 0) -> None:
     prec = _capi.TACO_PREC_FP32 if precision == "fp32" else _capi.TACO_PREC_FP64
     _capi.check(_capi.lib().taco_set_tuning(int(log2_nfft), prec, int(col_tile), int(row_tile), int(chunk_bytes),
                                             int(inv_dft_rows)))
+    _capi.check(_capi.lib().taco_set_cluster_points(int(log2_nfft), prec, int(cluster_lm)))
 
 
 def get_schedule(log2_nfft: int, precision: str) -> dict:
@@ -45,7 +46,8 @@ def load(path: str = DEFAULT_TABLE) -> int:
         if key.startswith("_"):
             continue
         L, prec = key.split(":")
-        set_schedule(int(L), prec, sch["col_tile"], sch["row_tile"], sch["chunk_bytes"], sch["inv_dft_rows"])
+        set_schedule(int(L), prec, sch["col_tile"], sch["row_tile"], sch["chunk_bytes"], sch["inv_dft_rows"],
+                     sch.get("cluster_lm", 0))
         n += 1
     return n
 
@@ -85,7 +87,35 @@ def tune(run, log2_nfft: int, precision: str, cands=None, reps: int = 3, warmup:
         if log:
             log(f"{precision} 2^{log2_nfft} {sch} -> {ms:.3f} ms")
     results.sort(key=lambda x: x[0])
-    best = results[0][1]
+    best = dict(results[0][1])
+    # phase 2: the thread-block-cluster path (points per CTA), with the best multi-pass tiles
+    lm_max = 13 if precision == "fp32" else 12
+    for lm in (11, 12, 13):
+        if lm > lm_max or log2_nfft - lm > 3 or lm > log2_nfft:
+            continue
+        sch = dict(best, cluster_lm=lm)
+        try:
+            set_schedule(log2_nfft, precision, **sch)
+            for _ in range(warmup):
+                run()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                run()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+        except _capi.TacoError as exc:
+            ms = float("inf")
+            if log:
+                log(f"schedule {sch} failed: {exc}")
+        results.append((ms, sch))
+        if log:
+            log(f"{precision} 2^{log2_nfft} {sch} -> {ms:.3f} ms")
+    results.sort(key=lambda x: x[0])
+    best = dict(results[0][1])
+    best.setdefault("cluster_lm", 0)
     set_schedule(log2_nfft, precision, **best)
     return best, results
 

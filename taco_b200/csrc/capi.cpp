@@ -327,6 +327,165 @@ int taco_rk4_propagate(const void* L_series, const void* L_half, const void* L_a
     });
 }
 
+namespace {
+// device staging for host buffers of the convenience paths
+struct DevAllocs {
+    std::vector<void*> ptrs;
+    void* take(std::size_t bytes) {
+        void* p = nullptr;
+        taco::cuda_check(cudaMalloc(&p, bytes ? bytes : 16), "cudaMalloc(staging)");
+        ptrs.push_back(p);
+        return p;
+    }
+    ~DevAllocs() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+}  // namespace
+
+int taco_tcl2_generator_series(const taco_system_view* sys, const double* eps, const taco_c128* gamma, size_t Nt,
+                               const uint32_t* tidx, size_t T, taco_c128* L2_out, int flags, void* stream) {
+    return guarded([&] {
+        require_device();
+        taco::SystemDesc s = to_desc(sys);
+        if (!eps || !gamma || !L2_out) throw taco::Error(taco::kInvalidArgument, "tcl2 series: null pointer");
+        if (Nt == 0) throw taco::Error(taco::kInvalidArgument, "empty gamma_series");
+        std::vector<uint32_t> t;
+        if (!tidx || T == 0) {
+            t.resize(Nt);
+            for (std::size_t k = 0; k < Nt; ++k) t[k] = static_cast<uint32_t>(k);
+        } else {
+            t.assign(tidx, tidx + T);
+        }
+        for (uint32_t k : t)
+            if (k >= Nt) throw taco::Error(taco::kOutOfRange, "time_index out of range");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        const std::size_t E = static_cast<std::size_t>(s.N) * s.N * s.N * s.N;
+        DevAllocs da;
+        const double2* g = reinterpret_cast<const double2*>(gamma);
+        if (!(flags & TACO_IN_DEVICE)) {
+            void* dg = da.take(s.nf * Nt * sizeof(double2));
+            taco::cuda_check(cudaMemcpyAsync(dg, gamma, s.nf * Nt * sizeof(double2), cudaMemcpyHostToDevice, st), "gamma");
+            g = static_cast<const double2*>(dg);
+        }
+        double2* out = reinterpret_cast<double2*>(L2_out);
+        if (!(flags & TACO_OUT_DEVICE)) out = static_cast<double2*>(da.take(t.size() * E * sizeof(double2)));
+        taco::tcl2_series_device(s, eps, g, Nt, t, out, st);
+        if (!(flags & TACO_OUT_DEVICE)) {
+            taco::cuda_check(cudaMemcpyAsync(L2_out, out, t.size() * E * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                             "L2 out");
+            taco::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        }
+    });
+}
+
+int taco_gamma_trapz(const taco_c128* C, size_t N, double dt, const double* omegas, size_t M, taco_c128* G, int flags,
+                     void* stream) {
+    return guarded([&] {
+        require_device();
+        if (!C || !G || (M > 0 && !omegas)) throw taco::Error(taco::kInvalidArgument, "gamma_trapz: null pointer");
+        if (N == 0 || M == 0 || !(dt > 0.0)) throw taco::Error(taco::kInvalidArgument, "gamma_trapz: empty input");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        DevAllocs da;
+        const double2* c = reinterpret_cast<const double2*>(C);
+        if (!(flags & TACO_IN_DEVICE)) {
+            void* dc = da.take(N * sizeof(double2));
+            taco::cuda_check(cudaMemcpyAsync(dc, C, N * sizeof(double2), cudaMemcpyHostToDevice, st), "C");
+            c = static_cast<const double2*>(dc);
+        }
+        double2* g = reinterpret_cast<double2*>(G);
+        if (!(flags & TACO_OUT_DEVICE)) g = static_cast<double2*>(da.take(M * N * sizeof(double2)));
+        taco::gamma_trapz_device(c, N, dt, std::vector<double>(omegas, omegas + M), g, st);
+        if (!(flags & TACO_OUT_DEVICE)) {
+            taco::cuda_check(cudaMemcpyAsync(G, g, M * N * sizeof(double2), cudaMemcpyDeviceToHost, st), "G out");
+            taco::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        }
+    });
+}
+
+int taco_propagate_tcl(const taco_system_view* sys, const double* eps, const taco_c128* gamma, size_t Nt, double dt,
+                       size_t steps, int order, int precision, const taco_c128* rho0, const taco_c128* obs,
+                       size_t sample_every, taco_c128* obs_out, taco_c128* rho_out, int flags, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (order != 0 && order != 2 && order != 4) throw taco::Error(taco::kInvalidArgument, "order must be 0, 2, or 4");
+        if (steps < 1) throw taco::Error(taco::kInvalidArgument, "propagate: steps must be >= 1");
+        if (steps >= Nt) throw taco::Error(taco::kOutOfRange, "propagate: steps must be < Nt");
+        if (!eps || !gamma || !rho0) throw taco::Error(taco::kInvalidArgument, "propagate: null pointer");
+        if (obs_out && !obs) throw taco::Error(taco::kInvalidArgument, "propagate: obs_out needs obs");
+        if (obs_out && sample_every == 0) throw taco::Error(taco::kInvalidArgument, "sample_every must be > 0");
+        taco::SystemDesc s = to_desc(sys);
+        const int D = s.N * s.N;
+        const std::size_t E = static_cast<std::size_t>(D) * D, ns = taco::rk4_num_samples(steps, sample_every);
+        const bool dev_in = (flags & TACO_IN_DEVICE) != 0, dev_out = (flags & TACO_OUT_DEVICE) != 0;
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        DevAllocs da;
+        const double2* g = reinterpret_cast<const double2*>(gamma);
+        if (!dev_in) {
+            void* dg = da.take(s.nf * Nt * sizeof(double2));
+            taco::cuda_check(cudaMemcpyAsync(dg, gamma, s.nf * Nt * sizeof(double2), cudaMemcpyHostToDevice, st), "gamma");
+            g = static_cast<const double2*>(dg);
+        }
+        std::vector<uint32_t> t(steps + 1);
+        for (std::size_t k = 0; k <= steps; ++k) t[k] = static_cast<uint32_t>(k);
+        // L2 (or L0 alone for order 0: L2 with gamma = 0 is the unitary part)
+        double2* L2 = static_cast<double2*>(da.take((steps + 1) * E * sizeof(double2)));
+        if (order == 0) {
+            double2* zero = static_cast<double2*>(da.take(s.nf * Nt * sizeof(double2)));
+            taco::cuda_check(cudaMemsetAsync(zero, 0, s.nf * Nt * sizeof(double2), st), "cudaMemsetAsync");
+            taco::tcl2_series_device(s, eps, zero, Nt, t, L2, st);
+        } else {
+            taco::tcl2_series_device(s, eps, g, Nt, t, L2, st);
+        }
+        const bool fp32 = precision == TACO_PREC_FP32;
+        void* L4 = nullptr;
+        if (order == 4) {
+            L4 = da.take((steps + 1) * E * (fp32 ? sizeof(float2) : sizeof(double2)));
+            std::vector<taco::Tcl4Instance> insts(1);
+            insts[0].sys = s;
+            insts[0].gamma = g;
+            insts[0].gamma_on_device = true;
+            insts[0].Nt = Nt;
+            insts[0].dt = dt;
+            insts[0].tidx = t;
+            insts[0].out = L4;
+            insts[0].out_on_device = true;
+            taco::tcl4_build(insts, options(precision, 0, nullptr), st);
+        }
+        double2* r = static_cast<double2*>(da.take(D * sizeof(double2)));
+        taco::cuda_check(cudaMemcpyAsync(r, rho0, D * sizeof(double2), dev_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st), "rho0");
+        const double2* o = nullptr;
+        if (obs) {
+            void* d_o = da.take(D * sizeof(double2));
+            taco::cuda_check(cudaMemcpyAsync(d_o, obs, D * sizeof(double2), dev_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st), "obs");
+            o = static_cast<const double2*>(d_o);
+        }
+        double2* oo = obs_out ? static_cast<double2*>(da.take(ns * sizeof(double2))) : nullptr;
+        if (order == 4 && fp32) {
+            // the RK4 kernel reads one storage type: widen the complex64 L4 into the FP64 L2
+            taco::add_c64_into_c128(static_cast<const float2*>(L4), L2, (steps + 1) * E, st);
+            L4 = nullptr;
+        }
+        taco::Rk4Request q;
+        q.L = L2;
+        q.L_add = L4;
+        q.fp32_storage = false;
+        q.steps = steps;
+        q.D = D;
+        q.dt = dt;
+        q.r = r;
+        q.sample_every = obs_out ? sample_every : 0;
+        q.obs = o;
+        q.obs_out = oo;
+        taco::rk4_propagate_device({q}, st);
+        if (obs_out)
+            taco::cuda_check(cudaMemcpyAsync(obs_out, oo, ns * sizeof(double2), dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st), "obs out");
+        if (rho_out)
+            taco::cuda_check(cudaMemcpyAsync(rho_out, r, D * sizeof(double2), dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st), "rho out");
+        taco::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(propagate)");
+    });
+}
+
 int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t* src, taco_c128* coef, size_t cap,
                          size_t* nnz) {
     return guarded([&] {

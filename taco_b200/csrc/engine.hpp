@@ -65,6 +65,16 @@ void noalloc_tcl4_build(const SystemDesc& sys, const double2* gamma, std::size_t
                         const std::vector<uint32_t>& tidx, bool fp32, std::size_t pad_factor, void* out,
                         cudaStream_t stream);
 
+// TCL2 generator at the requested times (tcl2.cu); gamma and out are device pointers.
+void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2* gamma, std::size_t Nt,
+                        const std::vector<uint32_t>& tidx, double2* out, cudaStream_t st);
+// Trapezoid Gamma(w_b, t_k) for all buckets: C [N] and G [nb][N] are device pointers.
+void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::vector<double>& omegas, double2* G,
+                        cudaStream_t st);
+
+// dst[k] += src[k] (complex64 into complex128), n entries, device pointers.
+void add_c64_into_c128(const float2* src, double2* dst, std::size_t n, cudaStream_t st);
+
 // compute_triple_kernels: full F/C/R series [nf^3][Nt] (FP64) for one instance.
 void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_device, std::size_t Nt,
                     double dt, double2* F, double2* Cc, double2* R, bool out_on_device,

@@ -1,0 +1,288 @@
+// tcl2.cu -- second-order generator series L2(t) and the trapezoid Gamma(w, t) on the device.
+//
+// L2(t) is the TCL2 generator total() of cpp/src/tcl/generator.cpp:164-177 with the
+// spin-boson example's kernel fill (examples/TCL4_spin_boson_example.cpp:303-315:
+// Gamma_b(alpha, alpha) = Gamma_b(t) for every channel, zero across channels):
+//   L2(t) = -i[diag(eps) + H_LS(t), .] + sum_{b,alpha} gamma_b(t) [conj(A_ab) (x) A_ab
+//           - 1/2 I (x) A_ab^+ A_ab - 1/2 (A_ab^+ A_ab)^T (x) I],
+//   H_LS(t) = hermitize(sum_{b,alpha} S_b(t) A_ab^+ A_ab),  gamma_b = 2 Re Gamma_b, S_b = Im Gamma_b,
+// with A_ab the entries of the eigenbasis coupling operator alpha on the pairs of bucket b
+// (system.hpp:163-182).  It is affine in (gamma_b, S_b):
+//   L2(t) = L0 + sum_b gamma_b(t) D_b + sum_b S_b(t) U_b,
+// so the host forms L0, D_b, U_b once (N^2 x N^2 each) and one kernel writes L2 at every
+// requested time.  Terms the reference skips (zero gamma, zero S, zero A_ab^+ A_ab) add
+// exact zeros here.
+//
+// gamma_trapz: Gamma_b(t_k) = sum_{m<k} dt/2 (phi_m C_m + phi_{m+1} C_{m+1}),
+// phi_m = exp(i w_b m dt) (cpp/include/taco/gamma.hpp:166-213), as a reduce-then-scan over
+// chunks of 1024 samples with FP64 sums (phases from sincos rather than the reference's
+// running product, which drifts by O(k eps)).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <complex>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.hpp"
+
+namespace taco {
+
+namespace {
+
+using cd = std::complex<double>;
+
+// --------------------------------------------------------------- TCL2 series
+__global__ void k_tcl2_series(const double2* __restrict__ gamma, std::size_t Nt, int nf, const uint32_t* __restrict__ tidx,
+                              uint32_t T, const double2* __restrict__ L0, const double2* __restrict__ Db,
+                              const double2* __restrict__ Ub, uint32_t E, double2* __restrict__ out) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t o = blockIdx.y;
+    if (e >= E || o >= T) return;
+    const uint32_t t = tidx[o];
+    double2 acc = L0[e];
+    for (int b = 0; b < nf; ++b) {
+        const double2 g = gamma[static_cast<std::size_t>(b) * Nt + t];
+        const double gam = 2.0 * g.x, S = g.y;
+        const double2 d = Db[static_cast<std::size_t>(b) * E + e];
+        const double2 u = Ub[static_cast<std::size_t>(b) * E + e];
+        acc.x += gam * d.x + S * u.x;
+        acc.y += gam * d.y + S * u.y;
+    }
+    out[static_cast<std::size_t>(o) * E + e] = acc;
+}
+
+// kron(A, B) entry (r1 n + r2, c1 n + c2) = A(r1, c1) B(r2, c2); column-major N^2 x N^2.
+void kron_add(std::vector<cd>& L, int n, const std::vector<cd>& A, const std::vector<cd>& B, cd s) {
+    const std::size_t D = static_cast<std::size_t>(n) * n;
+    for (int r1 = 0; r1 < n; ++r1)
+        for (int c1 = 0; c1 < n; ++c1) {
+            const cd a = A[r1 + n * c1];
+            if (a == cd(0.0, 0.0)) continue;
+            for (int r2 = 0; r2 < n; ++r2)
+                for (int c2 = 0; c2 < n; ++c2)
+                    L[(static_cast<std::size_t>(r1) * n + r2) + D * (static_cast<std::size_t>(c1) * n + c2)] +=
+                        s * a * B[r2 + n * c2];
+        }
+}
+
+// -i (kron(I, H) - kron(H^T, I)) (generator.cpp:81-90)
+void unitary_add(std::vector<cd>& L, int n, const std::vector<cd>& H, cd s) {
+    std::vector<cd> I(static_cast<std::size_t>(n) * n, cd(0.0, 0.0)), HT(I.size());
+    for (int i = 0; i < n; ++i) I[i + n * i] = 1.0;
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) HT[r + n * c] = H[c + n * r];
+    kron_add(L, n, I, H, s * cd(0.0, -1.0));
+    kron_add(L, n, HT, I, s * cd(0.0, 1.0));
+}
+
+// ------------------------------------------------------------- Gamma (trapz)
+constexpr int GT_THREADS = 256;
+constexpr int GT_ITEMS = 4;
+constexpr int GT_CHUNK = GT_THREADS * GT_ITEMS;
+
+// trapezoid increment of step k (k >= 1): dt/2 (phi_{k-1} C_{k-1} + phi_k C_k)
+__device__ __forceinline__ double2 trapz_inc(const double2* C, double w, double dt, std::size_t k) {
+    double s0, c0, s1, c1;
+    sincos(w * (static_cast<double>(k - 1) * dt), &s0, &c0);
+    sincos(w * (static_cast<double>(k) * dt), &s1, &c1);
+    const double2 a = cmul(make_double2(c0, s0), C[k - 1]);
+    const double2 b = cmul(make_double2(c1, s1), C[k]);
+    return make_double2(0.5 * dt * (a.x + b.x), 0.5 * dt * (a.y + b.y));
+}
+
+__global__ void k_gamma_reduce(const double2* __restrict__ C, std::size_t N, double dt,
+                               const double* __restrict__ omegas, double2* __restrict__ partial, int nchunks) {
+    __shared__ double2 wsum[GT_THREADS / 32];
+    const int b = blockIdx.y;
+    const std::size_t k0 = static_cast<std::size_t>(blockIdx.x) * GT_CHUNK + threadIdx.x * GT_ITEMS;
+    const double w = omegas[b];
+    double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int q = 0; q < GT_ITEMS; ++q) {
+        const std::size_t k = k0 + q;
+        if (k >= 1 && k < N) s = cadd(s, trapz_inc(C, w, dt, k));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+    }
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int q = 0; q < GT_THREADS / 32; ++q) t = cadd(t, wsum[q]);
+        partial[static_cast<std::size_t>(b) * nchunks + blockIdx.x] = t;
+    }
+}
+
+__global__ void k_gamma_scan(const double2* __restrict__ C, std::size_t N, double dt, const double* __restrict__ omegas,
+                             const double2* __restrict__ partial, int nchunks, double2* __restrict__ G) {
+    __shared__ double2 wsum[GT_THREADS / 32];
+    __shared__ double2 carry;
+    const int b = blockIdx.y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int c = 0; c < static_cast<int>(blockIdx.x); ++c) t = cadd(t, partial[static_cast<std::size_t>(b) * nchunks + c]);
+        carry = t;
+    }
+    const std::size_t k0 = static_cast<std::size_t>(blockIdx.x) * GT_CHUNK + threadIdx.x * GT_ITEMS;
+    const double w = omegas[b];
+    double2 v[GT_ITEMS];
+    double2 run = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int q = 0; q < GT_ITEMS; ++q) {
+        const std::size_t k = k0 + q;
+        v[q] = (k >= 1 && k < N) ? trapz_inc(C, w, dt, k) : make_double2(0.0, 0.0);
+        run = cadd(run, v[q]);
+    }
+    double2 x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double nx = __shfl_up_sync(0xffffffffu, x.x, o);
+        const double ny = __shfl_up_sync(0xffffffffu, x.y, o);
+        if (lane >= o) {
+            x.x += nx;
+            x.y += ny;
+        }
+    }
+    if (lane == 31) wsum[warp] = x;
+    double2 excl = make_double2(__shfl_up_sync(0xffffffffu, x.x, 1), __shfl_up_sync(0xffffffffu, x.y, 1));
+    if (lane == 0) excl = make_double2(0.0, 0.0);
+    __syncthreads();
+    double2 pre = carry;
+    for (int q = 0; q < warp; ++q) pre = cadd(pre, wsum[q]);
+    pre = cadd(pre, excl);
+    double2* Gb = G + static_cast<std::size_t>(b) * N;
+#pragma unroll
+    for (int q = 0; q < GT_ITEMS; ++q) {
+        const std::size_t k = k0 + q;
+        pre = cadd(pre, v[q]);
+        if (k < N) Gb[k] = pre;  // G(0) = 0: the k = 0 increment is zero
+    }
+}
+
+__global__ void k_add_c64(const float2* __restrict__ src, double2* __restrict__ dst, std::size_t n) {
+    for (std::size_t k = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<std::size_t>(gridDim.x) * blockDim.x)
+        dst[k] = cadd(dst[k], to_d2(src[k]));
+}
+
+}  // namespace
+
+void add_c64_into_c128(const float2* src, double2* dst, std::size_t n, cudaStream_t st) {
+    const unsigned grid = static_cast<unsigned>(std::min<std::size_t>((n + 255) / 256, 148 * 16));
+    k_add_c64<<<grid, 256, 0, st>>>(src, dst, n);
+    cuda_check(cudaGetLastError(), "k_add_c64");
+}
+
+void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2* gamma, std::size_t Nt,
+                        const std::vector<uint32_t>& tidx, double2* out, cudaStream_t st) {
+    const int n = sys.N, nf = sys.nf;
+    const std::size_t D = static_cast<std::size_t>(n) * n, E = D * D;
+    std::vector<cd> L0(E, cd(0.0, 0.0)), Db(nf * E, cd(0.0, 0.0)), Ub(nf * E, cd(0.0, 0.0));
+    std::vector<cd> Hd(D, cd(0.0, 0.0)), I(D, cd(0.0, 0.0));
+    for (int i = 0; i < n; ++i) {
+        Hd[i + n * i] = eps[i];
+        I[i + n * i] = 1.0;
+    }
+    unitary_add(L0, n, Hd, 1.0);
+    const cd* ops = reinterpret_cast<const cd*>(sys.ops.data());
+    for (int b = 0; b < nf; ++b) {
+        std::vector<cd> D_b(E, cd(0.0, 0.0)), AdA_sum(D, cd(0.0, 0.0));
+        for (int al = 0; al < sys.num_ops; ++al) {
+            std::vector<cd> Aw(D, cd(0.0, 0.0));
+            double nrm = 0.0;
+            for (std::size_t k = 0; k < D; ++k)
+                if (sys.p2f[k] == b) {
+                    Aw[k] = ops[static_cast<std::size_t>(al) * D + k];
+                    nrm += std::norm(Aw[k]);
+                }
+            if (nrm == 0.0) continue;
+            std::vector<cd> AdA(D, cd(0.0, 0.0)), Ac(D), AdAT(D);
+            for (int r = 0; r < n; ++r)
+                for (int c = 0; c < n; ++c) {
+                    cd acc(0.0, 0.0);
+                    for (int k = 0; k < n; ++k) acc += std::conj(Aw[k + n * r]) * Aw[k + n * c];
+                    AdA[r + n * c] = acc;
+                }
+            double an = 0.0;
+            for (auto& x : AdA) an += std::norm(x);
+            if (an == 0.0) continue;
+            for (int r = 0; r < n; ++r)
+                for (int c = 0; c < n; ++c) {
+                    Ac[r + n * c] = std::conj(Aw[r + n * c]);
+                    AdAT[r + n * c] = AdA[c + n * r];
+                }
+            kron_add(D_b, n, Ac, Aw, 1.0);
+            kron_add(D_b, n, I, AdA, -0.5);
+            kron_add(D_b, n, AdAT, I, -0.5);
+            for (std::size_t k = 0; k < D; ++k) AdA_sum[k] += AdA[k];
+        }
+        std::vector<cd> Hh(D);  // hermitize (ops.hpp:234)
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < n; ++c) Hh[r + n * c] = 0.5 * (AdA_sum[r + n * c] + std::conj(AdA_sum[c + n * r]));
+        std::vector<cd> U_b(E, cd(0.0, 0.0));
+        unitary_add(U_b, n, Hh, 1.0);
+        std::copy(D_b.begin(), D_b.end(), Db.begin() + static_cast<std::ptrdiff_t>(b * E));
+        std::copy(U_b.begin(), U_b.end(), Ub.begin() + static_cast<std::ptrdiff_t>(b * E));
+    }
+    // device staging of the (small) maps: allocated for the call, released after it
+    const std::size_t bytes = (E + 2 * nf * E) * sizeof(double2) + tidx.size() * sizeof(uint32_t);
+    void* d = nullptr;
+    cuda_check(cudaMalloc(&d, bytes), "cudaMalloc(tcl2 maps)");
+    try {
+        double2* dL0 = static_cast<double2*>(d);
+        double2* dD = dL0 + E;
+        double2* dU = dD + nf * E;
+        uint32_t* dt = reinterpret_cast<uint32_t*>(dU + nf * E);
+        cuda_check(cudaMemcpyAsync(dL0, L0.data(), E * sizeof(double2), cudaMemcpyHostToDevice, st), "tcl2 L0");
+        cuda_check(cudaMemcpyAsync(dD, Db.data(), nf * E * sizeof(double2), cudaMemcpyHostToDevice, st), "tcl2 D");
+        cuda_check(cudaMemcpyAsync(dU, Ub.data(), nf * E * sizeof(double2), cudaMemcpyHostToDevice, st), "tcl2 U");
+        cuda_check(cudaMemcpyAsync(dt, tidx.data(), tidx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st), "tcl2 t");
+        const unsigned gx = static_cast<unsigned>((E + 127) / 128);
+        for (std::size_t o0 = 0; o0 < tidx.size(); o0 += 65535) {
+            const unsigned gy = static_cast<unsigned>(std::min<std::size_t>(65535, tidx.size() - o0));
+            k_tcl2_series<<<dim3(gx, gy), 128, 0, st>>>(gamma, Nt, nf, dt + o0, gy, dL0, dD, dU,
+                                                         static_cast<uint32_t>(E), out + o0 * E);
+            cuda_check(cudaGetLastError(), "k_tcl2_series");
+        }
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl2)");
+    } catch (...) {
+        cudaStreamSynchronize(st);
+        cudaFree(d);
+        throw;
+    }
+    cudaFree(d);
+}
+
+void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::vector<double>& omegas, double2* G,
+                        cudaStream_t st) {
+    const int nb = static_cast<int>(omegas.size());
+    const int nchunks = static_cast<int>((N + GT_CHUNK - 1) / GT_CHUNK);
+    if (nb > 65535) throw Error(kInvalidArgument, "gamma_trapz: too many frequencies");
+    void* d = nullptr;
+    const std::size_t bytes = nb * sizeof(double) + static_cast<std::size_t>(nb) * nchunks * sizeof(double2) + 256;
+    cuda_check(cudaMalloc(&d, bytes), "cudaMalloc(gamma_trapz)");
+    try {
+        double* dom = static_cast<double*>(d);
+        double2* part = reinterpret_cast<double2*>(static_cast<char*>(d) + ((nb * sizeof(double) + 255) / 256) * 256);
+        cuda_check(cudaMemcpyAsync(dom, omegas.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st), "omegas");
+        k_gamma_reduce<<<dim3(static_cast<unsigned>(nchunks), static_cast<unsigned>(nb)), GT_THREADS, 0, st>>>(
+            C, N, dt, dom, part, nchunks);
+        cuda_check(cudaGetLastError(), "k_gamma_reduce");
+        k_gamma_scan<<<dim3(static_cast<unsigned>(nchunks), static_cast<unsigned>(nb)), GT_THREADS, 0, st>>>(
+            C, N, dt, dom, part, nchunks, G);
+        cuda_check(cudaGetLastError(), "k_gamma_scan");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(gamma)");
+    } catch (...) {
+        cudaStreamSynchronize(st);
+        cudaFree(d);
+        throw;
+    }
+    cudaFree(d);
+}
+
+}  // namespace taco
