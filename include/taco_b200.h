@@ -195,6 +195,21 @@ int taco_propagate_tcl(const taco_system_view* sys, const double* eps, const tac
                        size_t steps, int order, int precision, const taco_c128* rho0, const taco_c128* obs,
                        size_t sample_every, taco_c128* obs_out, taco_c128* rho_out, int flags, void* stream);
 
+/* The unfused stages, batched over T times (leading dimension), for callers of the
+ * reference's stage-by-stage API.  All array arguments follow TACO_IN_DEVICE / TACO_OUT_DEVICE.
+ * build_mikx_cuda / build_mikx_cuda_batch (cpp/include/taco/backend/cuda/tcl4_mikx_cuda.hpp:56-79):
+ *   F, C, R: [T][nf^3] at (i*nf + j)*nf + k; pair_to_freq [N*N] column-major;
+ *   M, I, K: [T][N^2 x N^2] column-major (row (j,k) = j + N k); X: [T][N^6] flat6 order. */
+int taco_build_mikx(const taco_c128* F, const taco_c128* C, const taco_c128* R, const int* pair_to_freq, int N,
+                    int nf, size_t T, taco_c128* M, taco_c128* I, taco_c128* K, taco_c128* X, int flags, void* stream);
+/* assemble_liouvillian_cuda (cpp/include/taco/backend/cuda/tcl4_assemble_cuda.hpp:18-44): GW [T][N^2 x N^2]
+ * (row (n,i), col (m,j)); symmetrize = 0 gives the raw T (assemble_liouvillian_cuda_device_raw). */
+int taco_assemble_liouvillian(const taco_c128* M, const taco_c128* I, const taco_c128* K, const taco_c128* X,
+                              const taco_c128* ops, int N, int num_ops, size_t T, int symmetrize, taco_c128* GW,
+                              int flags, void* stream);
+/* gw_to_liouvillian (cpp/include/taco/tcl4_assemble.hpp:18-21): L4(n + N m, i + N j) = GW(n + N i, m + N j). */
+int taco_gw_to_liouvillian(const taco_c128* GW, int N, size_t T, taco_c128* L4, int flags, void* stream);
+
 /* The time-independent linear map L4_e(t) = sum_k coef_k * v_{src_k}(t) (v conjugated when
  * bit 31 of src_k is set) of the MIKX -> GW -> L4 chain (cpp/src/tcl/tcl4_mikx.cpp:87-177,
  * cpp/src/tcl/tcl4_assemble.cpp:53-230).  Sources: F (s < nf^3), C, R of triple s mod nf^3.

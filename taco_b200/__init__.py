@@ -40,7 +40,7 @@ __all__ = [
     "build_TCL4_generator", "build_TCL4_generator_batch", "build_correction_series", "build_instances",
     "propagate_rk4_dense", "l4_coefficients", "Tcl4Plan", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
     "version", "device_count", "kernel_launches", "profile", "tcl2_generator_series", "gamma_trapz_device",
-    "propagate_tcl",
+    "propagate_tcl", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
 ]
 
 
@@ -422,6 +422,48 @@ def propagate_tcl(system: System, gamma, dt: float, steps: int, rho0, obs=None, 
                                                int(order), prec, _ptr(r0), _ptr(o), int(sample_every), _ptr(obs_out),
                                                _ptr(rho_out), flags, _stream_ptr(g)))
     return obs_out, rho_out
+
+
+def build_mikx(F, C, R, pair_to_freq, N):
+    """M, I, K ([T, N^2, N^2] indexed [t, row, col]) and X ([T, N^6] flat6) from F, C, R
+    ([T, nf^3] at (i*nf + j)*nf + k) on the device (build_mikx_cuda_batch)."""
+    F, C, R = (_c128_host(np.atleast_2d(x)) for x in (F, C, R))
+    T, nf3 = F.shape
+    nf = round(nf3 ** (1 / 3))
+    p2f = np.ascontiguousarray(np.asarray(pair_to_freq).T, np.int32)
+    N2 = N * N
+    M = np.empty((T, N2 * N2), np.complex128)
+    I = np.empty_like(M)
+    K = np.empty_like(M)
+    X = np.empty((T, N2 ** 3), np.complex128)
+    _capi.check(_capi.lib().taco_build_mikx(_ptr(F), _ptr(C), _ptr(R), _ptr(p2f), N, nf, T, _ptr(M), _ptr(I),
+                                            _ptr(K), _ptr(X), 0, None))
+    return _l4_view(M, N2), _l4_view(I, N2), _l4_view(K, N2), X
+
+
+def assemble_liouvillian(M, I, K, X, coupling_ops, symmetrize: bool = True):
+    """GW ([T, N^2, N^2]) by the NAKZWAN sums on the device (assemble_liouvillian_cuda)."""
+    M, I, K = (np.asarray(x) for x in (M, I, K))
+    T, N2 = M.shape[0], M.shape[1]
+    N = round(N2 ** 0.5)
+    cm = [_c128_host(np.swapaxes(x, -1, -2)) for x in (M, I, K)]  # column-major storage
+    Xc = _c128_host(X)
+    ops = _c128_host(np.stack([np.asarray(A, np.complex128).T for A in coupling_ops]))
+    GW = np.empty((T, N2 * N2), np.complex128)
+    _capi.check(_capi.lib().taco_assemble_liouvillian(_ptr(cm[0]), _ptr(cm[1]), _ptr(cm[2]), _ptr(Xc), _ptr(ops), N,
+                                                      len(coupling_ops), T, 1 if symmetrize else 0, _ptr(GW), 0, None))
+    return _l4_view(GW, N2)
+
+
+def gw_to_liouvillian(GW):
+    """L4 ([T, N^2, N^2]) from GW ([T, N^2, N^2]), L4(n+Nm, i+Nj) = GW(n+Ni, m+Nj)."""
+    GW = np.asarray(GW)
+    T, N2 = GW.shape[0], GW.shape[1]
+    N = round(N2 ** 0.5)
+    g = _c128_host(np.swapaxes(GW, -1, -2))
+    L4 = np.empty((T, N2 * N2), np.complex128)
+    _capi.check(_capi.lib().taco_gw_to_liouvillian(_ptr(g), N, T, _ptr(L4), 0, None))
+    return _l4_view(L4, N2)
 
 
 def l4_coefficients(system: System):

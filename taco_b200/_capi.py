@@ -36,6 +36,7 @@ EXPORTED = [
     "taco_set_tuning", "taco_get_tuning", "taco_clear_tuning", "taco_set_cluster_points",
     "taco_tcl4_plan_create", "taco_tcl4_plan_execute", "taco_tcl4_plan_destroy",
     "taco_tcl4_build_batch_noalloc", "taco_tcl2_generator_series", "taco_gamma_trapz", "taco_propagate_tcl",
+    "taco_build_mikx", "taco_assemble_liouvillian", "taco_gw_to_liouvillian",
 ]
 
 
@@ -123,6 +124,13 @@ def lib():
         L.taco_propagate_tcl.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_void_p, ct.c_size_t, ct.c_double,
                                          ct.c_size_t, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_size_t,
                                          ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.taco_build_mikx.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_int,
+                                      ct.c_size_t, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int,
+                                      ct.c_void_p]
+        L.taco_assemble_liouvillian.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                                ct.c_int, ct.c_int, ct.c_size_t, ct.c_int, ct.c_void_p, ct.c_int,
+                                                ct.c_void_p]
+        L.taco_gw_to_liouvillian.argtypes = [ct.c_void_p, ct.c_int, ct.c_size_t, ct.c_void_p, ct.c_int, ct.c_void_p]
         L.taco_tcl4_build_batch_noalloc.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t,
                                                     ct.c_double, ct.c_void_p, ct.c_size_t, ct.c_int, ct.c_void_p,
                                                     ct.c_void_p]

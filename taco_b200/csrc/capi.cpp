@@ -486,6 +486,96 @@ int taco_propagate_tcl(const taco_system_view* sys, const double* eps, const tac
     });
 }
 
+namespace {
+// Device view of a caller array: the pointer itself (device flag) or a staged copy.
+const void* dev_in(DevAllocs& da, const void* p, std::size_t bytes, bool on_device, cudaStream_t st) {
+    if (on_device || p == nullptr) return p;
+    void* d = da.take(bytes);
+    taco::cuda_check(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(stage in)");
+    return d;
+}
+}  // namespace
+
+int taco_build_mikx(const taco_c128* F, const taco_c128* C, const taco_c128* R, const int* pair_to_freq, int N,
+                    int nf, size_t T, taco_c128* M, taco_c128* I, taco_c128* K, taco_c128* X, int flags, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (N <= 0) throw taco::Error(taco::kInvalidArgument, "build_mikx: N must be > 0");
+        if (nf <= 0 || T == 0) throw taco::Error(taco::kInvalidArgument, "build_mikx: empty input");
+        if (!F || !C || !R || !pair_to_freq || !M || !I || !K || !X)
+            throw taco::Error(taco::kInvalidArgument, "build_mikx: null pointer");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        const bool din = (flags & TACO_IN_DEVICE) != 0, dout = (flags & TACO_OUT_DEVICE) != 0;
+        const std::size_t NN = static_cast<std::size_t>(N) * N;
+        std::vector<int> p2f(NN);
+        taco::cuda_check(cudaMemcpy(p2f.data(), pair_to_freq, NN * sizeof(int), din ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost),
+                         "pair_to_freq");
+        for (int v : p2f) {
+            if (v < 0) throw taco::Error(taco::kRuntime, "tcl4::build_mikx: pair_to_freq contains -1 for a required pair");
+            if (v >= nf) throw taco::Error(taco::kInvalidArgument, "build_mikx: pair_to_freq entry out of range");
+        }
+        const std::size_t nf3 = static_cast<std::size_t>(nf) * nf * nf, N4 = NN * NN, N6 = N4 * NN;
+        DevAllocs da;
+        auto f = static_cast<const double2*>(dev_in(da, F, T * nf3 * 16, din, st));
+        auto c = static_cast<const double2*>(dev_in(da, C, T * nf3 * 16, din, st));
+        auto r = static_cast<const double2*>(dev_in(da, R, T * nf3 * 16, din, st));
+        auto pf = static_cast<const int*>(dev_in(da, p2f.data(), NN * sizeof(int), false, st));
+        double2* outs[4];
+        taco_c128* host[4] = {M, I, K, X};
+        const std::size_t sz[4] = {T * N4, T * N4, T * N4, T * N6};
+        for (int k = 0; k < 4; ++k)
+            outs[k] = dout ? reinterpret_cast<double2*>(host[k]) : static_cast<double2*>(da.take(sz[k] * 16));
+        taco::mikx_device(f, c, r, pf, N, nf, T, outs[0], outs[1], outs[2], outs[3], st);
+        if (!dout)
+            for (int k = 0; k < 4; ++k)
+                taco::cuda_check(cudaMemcpyAsync(host[k], outs[k], sz[k] * 16, cudaMemcpyDeviceToHost, st), "mikx out");
+        taco::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(mikx)");
+    });
+}
+
+int taco_assemble_liouvillian(const taco_c128* M, const taco_c128* I, const taco_c128* K, const taco_c128* X,
+                              const taco_c128* ops, int N, int num_ops, size_t T, int symmetrize, taco_c128* GW,
+                              int flags, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (N <= 0) throw taco::Error(taco::kInvalidArgument, "assemble_liouvillian: tensors.N must be > 0");
+        if (num_ops <= 0) throw taco::Error(taco::kInvalidArgument, "assemble_liouvillian: coupling_ops must be non-empty");
+        if (!M || !I || !K || !X || !ops || !GW || T == 0)
+            throw taco::Error(taco::kInvalidArgument, "assemble_liouvillian: null or empty input");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        const bool din = (flags & TACO_IN_DEVICE) != 0, dout = (flags & TACO_OUT_DEVICE) != 0;
+        const std::size_t NN = static_cast<std::size_t>(N) * N, N4 = NN * NN, N6 = N4 * NN;
+        DevAllocs da;
+        auto m = static_cast<const double2*>(dev_in(da, M, T * N4 * 16, din, st));
+        auto i = static_cast<const double2*>(dev_in(da, I, T * N4 * 16, din, st));
+        auto k = static_cast<const double2*>(dev_in(da, K, T * N4 * 16, din, st));
+        auto x = static_cast<const double2*>(dev_in(da, X, T * N6 * 16, din, st));
+        auto o = static_cast<const double2*>(dev_in(da, ops, num_ops * NN * 16, din, st));
+        double2* gw = dout ? reinterpret_cast<double2*>(GW) : static_cast<double2*>(da.take(T * N4 * 16));
+        double2* tmp = symmetrize ? static_cast<double2*>(da.take(T * N4 * 16)) : nullptr;
+        taco::gw_device(m, i, k, x, o, N, num_ops, T, symmetrize != 0, gw, tmp, st);
+        if (!dout) taco::cuda_check(cudaMemcpyAsync(GW, gw, T * N4 * 16, cudaMemcpyDeviceToHost, st), "GW out");
+        taco::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(assemble)");
+    });
+}
+
+int taco_gw_to_liouvillian(const taco_c128* GW, int N, size_t T, taco_c128* L4, int flags, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (N <= 0) throw taco::Error(taco::kInvalidArgument, "gw_to_liouvillian: N must be > 0");
+        if (!GW || !L4 || T == 0) throw taco::Error(taco::kInvalidArgument, "gw_to_liouvillian: null or empty input");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        const bool din = (flags & TACO_IN_DEVICE) != 0, dout = (flags & TACO_OUT_DEVICE) != 0;
+        const std::size_t N4 = static_cast<std::size_t>(N) * N * N * N;
+        DevAllocs da;
+        auto g = static_cast<const double2*>(dev_in(da, GW, T * N4 * 16, din, st));
+        double2* l = dout ? reinterpret_cast<double2*>(L4) : static_cast<double2*>(da.take(T * N4 * 16));
+        taco::gw_to_l4_device(g, N, T, l, st);
+        if (!dout) taco::cuda_check(cudaMemcpyAsync(L4, l, T * N4 * 16, cudaMemcpyDeviceToHost, st), "L4 out");
+        taco::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(gw_to_l4)");
+    });
+}
+
 int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t* src, taco_c128* coef, size_t cap,
                          size_t* nnz) {
     return guarded([&] {

@@ -72,6 +72,13 @@ void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2*
 void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::vector<double>& omegas, double2* G,
                         cudaStream_t st);
 
+// The unfused stages (mikx_gw.cu), batched over T times; all pointers are device pointers.
+void mikx_device(const double2* F, const double2* C, const double2* R, const int* p2f_dev, int N, int nf, std::size_t T,
+                 double2* M, double2* I, double2* K, double2* X, cudaStream_t st);
+void gw_device(const double2* M, const double2* I, const double2* K, const double2* X, const double2* ops_dev, int N,
+               int num_ops, std::size_t T, bool symmetrize, double2* GW, double2* tmp, cudaStream_t st);
+void gw_to_l4_device(const double2* GW, int N, std::size_t T, double2* L4, cudaStream_t st);
+
 // dst[k] += src[k] (complex64 into complex128), n entries, device pointers.
 void add_c64_into_c128(const float2* src, double2* dst, std::size_t n, cudaStream_t st);
 
