@@ -242,6 +242,95 @@ int taco_profile_enable(int on);
 int taco_profile_reset(void);
 int taco_profile_get(size_t index, const char** name, uint64_t* launches, double* total_ms, size_t* count);
 
+/* ---------------------------------------------------------------------------------------
+ * Bath correlation function on the device: bcf_fft_fun (cpp/include/taco/correlation_fft.hpp:153-214)
+ * for J(w) = alpha w e^{-w/omega_c} (+ 2 lambda gamma w / (w^2 + gamma^2) when model = 1), and
+ * its derivatives in alpha, omega_c, beta (which = 1, 2, 3; the Drude-Lorentz terms are held
+ * fixed).  out[k] = C(k dt) (or its derivative) for k < n_out <= N + 1; host arrays unless
+ * TACO_OUT_DEVICE.  Requests are batched into one pair of launches per FFT length. */
+typedef struct {
+    int model;
+    int which;
+    double alpha, omega_c, lambda, gamma, beta;
+    size_t N;
+    double dt;
+    taco_c128* out;
+    size_t n_out;
+} taco_bcf_request;
+int taco_bcf_fft(const taco_bcf_request* reqs, size_t n, int flags, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Differentiation.  Real losses; every gradient G(z) = dloss/dRe z + i dloss/dIm z.
+ * All arrays are device pointers except where marked host.  No reference counterpart: the
+ * reference has no derivatives.
+ *
+ * RK4 with checkpoints (the endpoint overload of propagate_rk4_dense, rk4_dense.hpp:85-129,
+ * Lh = (L_i + L_{i+1}) / 2): taco_rk4_forward_checkpointed writes <O> samples, the final state
+ * and the state every checkpoint_every steps; taco_rk4_adjoint recomputes each segment from its
+ * checkpoint and returns G(L) for every endpoint, G(rho0) and G(obs).  D = N^2 <= 16. */
+typedef struct {
+    const taco_c128* L;            /* [steps+1][D x D] column-major */
+    const taco_c128* L_add;        /* nullable, added to L (its gradient is L_bar) */
+    size_t steps;
+    int D;
+    double dt;
+    const taco_c128* r0;           /* [D] */
+    const taco_c128* obs;          /* [D]: <O> = sum_l obs_l r_l (nullable without samples) */
+    size_t sample_every;           /* samples at steps 0, s, 2s, ... < steps, and after the last */
+    taco_c128* ckpt;               /* [ceil(steps / checkpoint_every)][D] */
+    taco_c128* obs_out;            /* forward: samples of <O> (nullable) */
+    taco_c128* r_out;              /* forward: final state (nullable) */
+    const taco_c128* obs_bar;      /* adjoint: G(<O>) per sample (nullable) */
+    const taco_c128* r_final_bar;  /* adjoint: G(final state) (nullable) */
+    taco_c128* L_bar;              /* adjoint out: [steps+1][D x D] */
+    taco_c128* r0_bar;             /* adjoint out: [D] (nullable) */
+    taco_c128* obs_vec_bar;        /* adjoint out: [D] (nullable) */
+} taco_rk4_grad_job;
+int taco_rk4_forward_checkpointed(const taco_rk4_grad_job* jobs, size_t n, size_t checkpoint_every, void* stream);
+int taco_rk4_adjoint(const taco_rk4_grad_job* jobs, size_t n, size_t checkpoint_every, void* stream);
+
+/* Adjoint of L4(t), t = 0..T-1 (build_TCL4_generator_cuda_fused_batch with all times), through
+ * GW/MIKX (tcl4_assemble.cpp:53-230, tcl4_mikx.cpp:87-177) and the F/C/R kernels
+ * (tcl4_kernels.cpp:105-281): accumulates G(gamma) ([nf][T], gamma[b*T + t]), dloss/domega_b
+ * (host [nf]) and, when the forward F/C/R series ([nf^3][T] each) are given, G(ops) (host
+ * [num_ops][N*N]).  nf <= 27. */
+typedef struct {
+    const taco_system_view* sys;
+    const taco_c128* gamma;
+    size_t T;
+    double dt;
+    const taco_c128* L_bar;        /* [T][N^2 x N^2] */
+    const taco_c128* F;            /* nullable */
+    const taco_c128* C;
+    const taco_c128* R;
+    taco_c128* gamma_bar;          /* accumulated */
+    double* omega_bar;             /* host, accumulated (nullable) */
+    taco_c128* ops_bar;            /* host, accumulated (nullable) */
+} taco_tcl4_adjoint_job;
+int taco_tcl4_adjoint(const taco_tcl4_adjoint_job* jobs, size_t n, void* stream);
+
+/* Adjoint of the TCL2 generator series (generator.cpp:42-177, the example's kernel fill):
+ * accumulates G(gamma), and (host) G(ops) and dloss/deps. */
+typedef struct {
+    const taco_system_view* sys;
+    const double* eps;             /* host [N] eigenvalues */
+    const taco_c128* gamma;        /* [nf][T] */
+    size_t T;
+    const taco_c128* L_bar;        /* [T][N^2 x N^2] */
+    taco_c128* gamma_bar;          /* accumulated */
+    taco_c128* ops_bar;            /* host, accumulated (nullable) */
+    double* eps_bar;               /* host [N], accumulated (nullable) */
+} taco_tcl2_adjoint_job;
+int taco_tcl2_adjoint(const taco_tcl2_adjoint_job* jobs, size_t n, void* stream);
+
+/* out[k] = sum_i Re(conj(a_k[i]) b_k[i]) for device vectors (host out). */
+typedef struct {
+    const taco_c128* a;
+    const taco_c128* b;
+    size_t n;
+} taco_inner_job;
+int taco_inner_re(const taco_inner_job* jobs, size_t n, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

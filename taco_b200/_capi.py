@@ -37,6 +37,8 @@ EXPORTED = [
     "taco_tcl4_plan_create", "taco_tcl4_plan_execute", "taco_tcl4_plan_destroy",
     "taco_tcl4_build_batch_noalloc", "taco_tcl2_generator_series", "taco_gamma_trapz", "taco_propagate_tcl",
     "taco_build_mikx", "taco_assemble_liouvillian", "taco_gw_to_liouvillian",
+    "taco_bcf_fft", "taco_rk4_forward_checkpointed", "taco_rk4_adjoint", "taco_tcl4_adjoint",
+    "taco_tcl2_adjoint", "taco_inner_re",
 ]
 
 
@@ -71,6 +73,37 @@ class TacoOverflow(TacoError, OverflowError):
 
 _ERRS = {TACO_ERR_INVALID_ARGUMENT: TacoInvalidArgument, TACO_ERR_OUT_OF_RANGE: TacoOutOfRange,
          TACO_ERR_OVERFLOW: TacoOverflow}
+
+
+class BcfRequest(ct.Structure):
+    _fields_ = [("model", ct.c_int), ("which", ct.c_int), ("alpha", ct.c_double), ("omega_c", ct.c_double),
+                ("lam", ct.c_double), ("gam", ct.c_double), ("beta", ct.c_double), ("N", ct.c_size_t),
+                ("dt", ct.c_double), ("out", ct.c_void_p), ("n_out", ct.c_size_t)]
+
+
+class Rk4GradJob(ct.Structure):
+    _fields_ = [("L", ct.c_void_p), ("L_add", ct.c_void_p), ("steps", ct.c_size_t), ("D", ct.c_int),
+                ("dt", ct.c_double), ("r0", ct.c_void_p), ("obs", ct.c_void_p), ("sample_every", ct.c_size_t),
+                ("ckpt", ct.c_void_p), ("obs_out", ct.c_void_p), ("r_out", ct.c_void_p), ("obs_bar", ct.c_void_p),
+                ("r_final_bar", ct.c_void_p), ("L_bar", ct.c_void_p), ("r0_bar", ct.c_void_p),
+                ("obs_vec_bar", ct.c_void_p)]
+
+
+class Tcl4AdjointJob(ct.Structure):
+    _fields_ = [("sys", ct.POINTER(SystemView)), ("gamma", ct.c_void_p), ("T", ct.c_size_t), ("dt", ct.c_double),
+                ("L_bar", ct.c_void_p), ("F", ct.c_void_p), ("C", ct.c_void_p), ("R", ct.c_void_p),
+                ("gamma_bar", ct.c_void_p), ("omega_bar", ct.c_void_p), ("ops_bar", ct.c_void_p)]
+
+
+class Tcl2AdjointJob(ct.Structure):
+    _fields_ = [("sys", ct.POINTER(SystemView)), ("eps", ct.c_void_p), ("gamma", ct.c_void_p), ("T", ct.c_size_t),
+                ("L_bar", ct.c_void_p), ("gamma_bar", ct.c_void_p), ("ops_bar", ct.c_void_p),
+                ("eps_bar", ct.c_void_p)]
+
+
+class InnerJob(ct.Structure):
+    _fields_ = [("a", ct.c_void_p), ("b", ct.c_void_p), ("n", ct.c_size_t)]
+
 
 _lib = None
 
@@ -131,6 +164,12 @@ def lib():
                                                 ct.c_int, ct.c_int, ct.c_size_t, ct.c_int, ct.c_void_p, ct.c_int,
                                                 ct.c_void_p]
         L.taco_gw_to_liouvillian.argtypes = [ct.c_void_p, ct.c_int, ct.c_size_t, ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.taco_bcf_fft.argtypes = [ct.POINTER(BcfRequest), ct.c_size_t, ct.c_int, ct.c_void_p]
+        L.taco_rk4_forward_checkpointed.argtypes = [ct.POINTER(Rk4GradJob), ct.c_size_t, ct.c_size_t, ct.c_void_p]
+        L.taco_rk4_adjoint.argtypes = [ct.POINTER(Rk4GradJob), ct.c_size_t, ct.c_size_t, ct.c_void_p]
+        L.taco_tcl4_adjoint.argtypes = [ct.POINTER(Tcl4AdjointJob), ct.c_size_t, ct.c_void_p]
+        L.taco_tcl2_adjoint.argtypes = [ct.POINTER(Tcl2AdjointJob), ct.c_size_t, ct.c_void_p]
+        L.taco_inner_re.argtypes = [ct.POINTER(InnerJob), ct.c_size_t, ct.c_void_p, ct.c_void_p]
         L.taco_tcl4_build_batch_noalloc.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t,
                                                     ct.c_double, ct.c_void_p, ct.c_size_t, ct.c_int, ct.c_void_p,
                                                     ct.c_void_p]

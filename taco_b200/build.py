@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("TACO_NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = os.environ.get("TACO_HOST_CXX", "g++")
 
-LIB_SOURCES = ["engine.cu", "noalloc.cu", "tcl2.cu", "mikx_gw.cu", "capi.cpp", "gw_coef.cpp"]
+LIB_SOURCES = ["engine.cu", "noalloc.cu", "tcl2.cu", "mikx_gw.cu", "bcf.cu", "adjoint.cu", "capi.cpp", "gw_coef.cpp"]
 
 
 def _native_ext() -> str:

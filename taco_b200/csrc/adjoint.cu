@@ -1,0 +1,1098 @@
+// adjoint.cu -- reverse-mode derivatives of the propagated TCL4 path:
+//   RK4 (checkpointed) -> L(t) = L2(t) + L4(t) -> sources F/C/R(t) -> Gamma(t), Bohr frequencies.
+//
+// Convention: for a real loss l and a complex quantity z, G(z) = dl/dRe z + i dl/dIm z.
+// Then y = a z gives G(z) += conj(a) G(y), y = a conj(z) gives G(z) += a conj(G(y)),
+// y = M x gives G(x) += M^H G(y) and G(M) += G(y) x^H.
+//
+// RK4 (cpp/src/core/rk4_dense.cpp:133-160, endpoint overload with Lh = (L_i + L_{i+1})/2):
+//   k1 = L0 u1, u1 = r;  k2 = Lh u2, u2 = r + dt/2 k1;  k3 = Lh u3, u3 = r + dt/2 k2;
+//   k4 = L1 u4, u4 = r + dt k3;  r' = r + dt/6 (k1 + 2 k2 + 2 k3 + k4).
+// The forward sweep stores r every `every` steps (every ~ sqrt(steps)); the reverse sweep
+// recomputes one segment of states from its checkpoint into shared memory and walks it
+// backwards, so memory is O(sqrt(steps) D) instead of O(steps D).
+//
+// F/C/R (cpp/src/tcl/tcl4_kernels.cpp:105-281, direct forms): with P[k] = e^{-i w k dt},
+// Q = conj(P), w = w_i + w_j + w_k, g1 = Gamma_i and
+//   F[k] = dt sum_{m<=k} g2[m] P[k-m] (g1[k] - g1[k-m]),  g2 = Gamma_{mirror(j)}
+//   C[k] = same with g2 = conj(Gamma_j)
+//   R[k] = dt sum_{m<=k} g2[m] P[m] (g1[k] - g1[m]),      g2 = Gamma_j.
+// Their adjoints split into prefix/suffix scans (O(T), k_fcr_adj_scan) and three
+// correlations per F/C series, c[m] = sum_{k>=m} a[k-m] Fb[k] with a in {conj(g2),
+// conj(P g1), (k-m) conj(P g1)} (O(T^2), k_fcr_adj_corr):
+//   G(g1)[n] = conj(dt P[n] A0[n]) Fb[n] - dt Q[n] c1[n],        A0[n] = sum_{m<=n} g2[m] Q[m]
+//   G(g2)[m] = dt P[m] sum_{k>=m} Q[k] conj(g1[k]) Fb[k] - dt c2[m]
+//   dl/dw   = Re[-i dt^2 sum_k conj(Fb[k]) g1[k] P[k] (k A0[k] - A1[k]) + i dt^2 sum_m g2[m] conj(c3[m])],
+//             A1[n] = sum_{m<=n} m g2[m] Q[m]
+// and for R, with B0[k] = sum_{m<=k} g2[m] P[m], SR0[m] = sum_{k>=m} conj(g1[k]) Rb[k],
+// SR1[m] = sum_{k>=m} Rb[k]:
+//   G(g1)[k] = dt conj(B0[k]) Rb[k] - dt conj(g2[k] P[k]) SR1[k]
+//   G(g2)[m] = dt Q[m] SR0[m] - dt conj(g1[m] P[m]) SR1[m]
+//   dl/dw    = Re sum_m (-i m dt^2) g2[m] P[m] (conj(SR0[m]) - g1[m] conj(SR1[m])).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.hpp"
+#include "gw_coef.hpp"
+
+namespace taco {
+
+namespace {
+
+// ------------------------------------------------------------------ scratch --
+struct GradScratch {
+    void* p = nullptr;
+    std::size_t cap = 0;
+    char* ensure(std::size_t bytes) {
+        if (bytes > cap) {
+            if (p) cudaFree(p);
+            p = nullptr;
+            cap = 0;
+            cuda_check(cudaMalloc(&p, bytes), "cudaMalloc(adjoint scratch)");
+            cap = bytes;
+        }
+        return static_cast<char*>(p);
+    }
+    ~GradScratch() {
+        if (p) cudaFree(p);
+    }
+};
+
+GradScratch& grad_scratch() {
+    thread_local std::map<int, GradScratch> per_dev;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    return per_dev[dev];
+}
+
+std::size_t up256(std::size_t x) { return (x + 255) / 256 * 256; }
+
+struct Carve {
+    char* base;
+    std::size_t off = 0;
+    template <class T>
+    T* take(std::size_t n) {
+        off = up256(off);
+        T* r = reinterpret_cast<T*>(base ? base + off : nullptr);
+        off += n * sizeof(T);
+        return r;
+    }
+};
+
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+__device__ __forceinline__ double2 shfl_up2(double2 v, int d) {
+    return make_double2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+
+__device__ __forceinline__ double2 warp_sum2(double2 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+}
+
+__device__ __forceinline__ double2 cfma2(double2 a, double2 b, double2 c) {  // c + a b
+    return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+
+// ---------------------------------------------------------------------- RK4 --
+struct Rk4GJob {
+    const double2* L;
+    const double2* L_add;
+    uint64_t steps;
+    int D;
+    double dt;
+    const double2* r0;
+    const double2* obs;
+    uint64_t sample_every;
+    double2* ckpt;
+    double2* obs_out;
+    double2* r_out;
+    const double2* obs_bar;
+    const double2* r_final_bar;
+    double2* L_bar;
+    double2* r0_bar;
+    double2* obs_vec_bar;
+};
+
+// entry (r, c) of L + L_add at endpoint t
+__device__ __forceinline__ double2 gen_at(const Rk4GJob& j, uint64_t t, int r, int c) {
+    const size_t e = static_cast<size_t>(t) * j.D * j.D + r + static_cast<size_t>(c) * j.D;
+    double2 v = j.L[e];
+    if (j.L_add) v = cadd(v, j.L_add[e]);
+    return v;
+}
+
+template <int DMAX>
+__device__ __forceinline__ void load_row(const Rk4GJob& j, uint64_t t, int row, double2* out) {
+#pragma unroll
+    for (int c = 0; c < DMAX; ++c) out[c] = c < j.D ? gen_at(j, t, row, c) : make_double2(0.0, 0.0);
+}
+
+template <int DMAX>
+__device__ __forceinline__ void load_col(const Rk4GJob& j, uint64_t t, int col, double2* out) {
+#pragma unroll
+    for (int r = 0; r < DMAX; ++r) out[r] = r < j.D ? gen_at(j, t, r, col) : make_double2(0.0, 0.0);
+}
+
+// (M x)_lane with lane owning row `lane` of M
+template <int DMAX>
+__device__ __forceinline__ double2 mv_row(const double2* row, double2 x, int D) {
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < DMAX; ++c)
+        if (c < D) acc = cfma2(row[c], shfl2(x, c), acc);
+    return acc;
+}
+
+// (M^H g)_lane with lane owning column `lane` of M
+template <int DMAX>
+__device__ __forceinline__ double2 mhv_col(const double2* col, double2 g, int D) {
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < DMAX; ++r)
+        if (r < D) acc = cfma2(cconj(col[r]), shfl2(g, r), acc);
+    return acc;
+}
+
+template <int DMAX>
+__device__ __forceinline__ double2 rk4_step(double2 r, const double2* l0, const double2* l1, double dt, int D) {
+    double2 lh[DMAX];
+#pragma unroll
+    for (int c = 0; c < DMAX; ++c) lh[c] = make_double2(0.5 * (l0[c].x + l1[c].x), 0.5 * (l0[c].y + l1[c].y));
+    const double2 k1 = mv_row<DMAX>(l0, r, D);
+    const double2 k2 = mv_row<DMAX>(lh, cadd(r, cscale(k1, 0.5 * dt)), D);
+    const double2 k3 = mv_row<DMAX>(lh, cadd(r, cscale(k2, 0.5 * dt)), D);
+    const double2 k4 = mv_row<DMAX>(l1, cadd(r, cscale(k3, dt)), D);
+    const double2 s = cadd(cadd(k1, cscale(k2, 2.0)), cadd(cscale(k3, 2.0), k4));
+    return cadd(r, cscale(s, dt / 6.0));
+}
+
+__device__ __forceinline__ uint64_t n_samples(uint64_t steps, uint64_t se) { return se ? (steps + se - 1) / se + 1 : 0; }
+
+// Forward sweep: one warp per job, lane l < D owns component l of r.
+template <int DMAX>
+__global__ void __launch_bounds__(128) k_rk4g_fwd(const Rk4GJob* __restrict__ jobs, int njobs, uint64_t every) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= njobs) return;
+    const Rk4GJob j = jobs[w];
+    const int D = j.D;
+    const int row = lane < D ? lane : 0;
+    double2 l0[DMAX], l1[DMAX];
+    load_row<DMAX>(j, 0, row, l0);
+    load_row<DMAX>(j, 1, row, l1);
+    double2 r = lane < D ? j.r0[lane] : make_double2(0.0, 0.0);
+    const uint64_t se = j.sample_every;
+    auto sample = [&](uint64_t s) {
+        if (!j.obs_out) return;
+        const double2 v = warp_sum2(lane < D ? cmul(j.obs[lane], r) : make_double2(0.0, 0.0));
+        if (lane == 0) j.obs_out[s] = v;
+    };
+    for (uint64_t i = 0; i < j.steps; ++i) {
+        if (j.ckpt && (i % every) == 0 && lane < D) j.ckpt[(i / every) * D + lane] = r;
+        if (se && (i % se) == 0) sample(i / se);
+        r = rk4_step<DMAX>(r, l0, l1, j.dt, D);
+#pragma unroll
+        for (int c = 0; c < DMAX; ++c) l0[c] = l1[c];
+        if (i + 2 <= j.steps) load_row<DMAX>(j, i + 2, row, l1);
+    }
+    if (se) sample(n_samples(j.steps, se) - 1);
+    if (j.r_out && lane < D) j.r_out[lane] = r;
+}
+
+// Reverse sweep: one warp per block and job; shared memory holds one segment of states.
+template <int DMAX>
+__global__ void __launch_bounds__(32) k_rk4g_adj(const Rk4GJob* __restrict__ jobs, uint64_t every) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* seg = reinterpret_cast<double2*>(smem_raw);  // [every][DMAX]
+    const Rk4GJob j = jobs[blockIdx.x];
+    const int lane = threadIdx.x;
+    const int D = j.D;
+    const int me = lane < D ? lane : 0;
+    const bool own = lane < D;
+    const uint64_t steps = j.steps, se = j.sample_every;
+    const uint64_t nck = (steps + every - 1) / every;
+    const uint64_t nsamp = n_samples(steps, se);
+    const double dt = j.dt;
+    const size_t DD = static_cast<size_t>(D) * D;
+    const double2 ob_l = (j.obs && own) ? j.obs[lane] : make_double2(0.0, 0.0);
+    double2 g = (j.r_final_bar && own) ? j.r_final_bar[lane] : make_double2(0.0, 0.0);
+    double2 ovb = make_double2(0.0, 0.0);
+    double2 pend[DMAX];
+#pragma unroll
+    for (int c = 0; c < DMAX; ++c) pend[c] = make_double2(0.0, 0.0);
+    for (uint64_t sg = nck; sg-- > 0;) {
+        const uint64_t s0 = sg * every, s1 = min(s0 + every, steps);
+        // recompute the segment's states from its checkpoint
+        double2 r = own ? j.ckpt[sg * D + lane] : make_double2(0.0, 0.0);
+        {
+            double2 l0[DMAX], l1[DMAX];
+            load_row<DMAX>(j, s0, me, l0);
+            load_row<DMAX>(j, s0 + 1, me, l1);
+            for (uint64_t i = s0; i < s1; ++i) {
+                if (own) seg[(i - s0) * DMAX + lane] = r;
+                r = rk4_step<DMAX>(r, l0, l1, dt, D);
+#pragma unroll
+                for (int c = 0; c < DMAX; ++c) l0[c] = l1[c];
+                if (i + 2 <= s1) load_row<DMAX>(j, i + 2, me, l1);
+            }
+        }
+        if (sg == nck - 1 && se && j.obs_bar) {  // the final sample, taken at r_steps
+            const double2 o = j.obs_bar[nsamp - 1];
+            g = cadd(g, cmulc(o, ob_l));   // conj(obs_l) o
+            ovb = cadd(ovb, cmulc(o, r));  // conj(r_l) o
+        }
+        __syncwarp();
+        double2 r0w[DMAX], r1w[DMAX], c0[DMAX], c1[DMAX];  // rows / columns of L(t_n), L(t_{n+1})
+        load_row<DMAX>(j, s1, me, r1w);
+        load_col<DMAX>(j, s1, me, c1);
+        for (uint64_t n = s1; n-- > s0;) {
+            load_row<DMAX>(j, n, me, r0w);
+            load_col<DMAX>(j, n, me, c0);
+            const double2 rn = own ? seg[(n - s0) * DMAX + lane] : make_double2(0.0, 0.0);
+            double2 rh[DMAX], ch[DMAX];
+#pragma unroll
+            for (int c = 0; c < DMAX; ++c) {
+                rh[c] = make_double2(0.5 * (r0w[c].x + r1w[c].x), 0.5 * (r0w[c].y + r1w[c].y));
+                ch[c] = make_double2(0.5 * (c0[c].x + c1[c].x), 0.5 * (c0[c].y + c1[c].y));
+            }
+            const double2 u1 = rn;
+            const double2 k1 = mv_row<DMAX>(r0w, u1, D);
+            const double2 u2 = cadd(rn, cscale(k1, 0.5 * dt));
+            const double2 k2 = mv_row<DMAX>(rh, u2, D);
+            const double2 u3 = cadd(rn, cscale(k2, 0.5 * dt));
+            const double2 k3 = mv_row<DMAX>(rh, u3, D);
+            const double2 u4 = cadd(rn, cscale(k3, dt));
+            double2 gk1 = cscale(g, dt / 6.0), gk2 = cscale(g, dt / 3.0), gk3 = cscale(g, dt / 3.0);
+            const double2 gk4 = cscale(g, dt / 6.0);
+            double2 gr = g;
+            const double2 gu4 = mhv_col<DMAX>(c1, gk4, D);
+            gr = cadd(gr, gu4);
+            gk3 = cadd(gk3, cscale(gu4, dt));
+            const double2 gu3 = mhv_col<DMAX>(ch, gk3, D);
+            gr = cadd(gr, gu3);
+            gk2 = cadd(gk2, cscale(gu3, 0.5 * dt));
+            const double2 gu2 = mhv_col<DMAX>(ch, gk2, D);
+            gr = cadd(gr, gu2);
+            gk1 = cadd(gk1, cscale(gu2, 0.5 * dt));
+            const double2 gu1 = mhv_col<DMAX>(c0, gk1, D);
+            gr = cadd(gr, gu1);
+            // row `lane` of G(L(t_n)) and G(L(t_{n+1})) from this step
+            double2* Lb1 = j.L_bar + static_cast<size_t>(n + 1) * DD;
+#pragma unroll
+            for (int c = 0; c < DMAX; ++c) {
+                if (c < D) {
+                    const double2 x1 = shfl2(u1, c), x2 = shfl2(u2, c), x3 = shfl2(u3, c), x4 = shfl2(u4, c);
+                    const double2 h = cscale(cadd(cmulc(gk2, x2), cmulc(gk3, x3)), 0.5);
+                    const double2 gl0 = cadd(cmulc(gk1, x1), h);
+                    const double2 gl1 = cadd(cmulc(gk4, x4), h);
+                    if (own) Lb1[lane + static_cast<size_t>(c) * D] = cadd(pend[c], gl1);
+                    pend[c] = gl0;
+                }
+            }
+            if (se && j.obs_bar && (n % se) == 0) {
+                const double2 o = j.obs_bar[n / se];
+                gr = cadd(gr, cmulc(o, ob_l));
+                ovb = cadd(ovb, cmulc(o, rn));
+            }
+            g = own ? gr : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int c = 0; c < DMAX; ++c) {
+                r1w[c] = r0w[c];
+                c1[c] = c0[c];
+            }
+        }
+        __syncwarp();
+    }
+    if (own) {
+#pragma unroll
+        for (int c = 0; c < DMAX; ++c)
+            if (c < D) j.L_bar[lane + static_cast<size_t>(c) * D] = pend[c];
+        if (j.r0_bar) j.r0_bar[lane] = g;
+        if (j.obs_vec_bar) j.obs_vec_bar[lane] = ovb;
+    }
+}
+
+// ---------------------------------------------------- L4 -> sources (CSC) --
+// src_bar[s][t] = sum over entries (e, w, cj) of column s: cj ? w conj(Lb[t][e]) : conj(w) Lb[t][e]
+__global__ void k_src_adj(const double2* __restrict__ Lb, uint32_t T, uint32_t E, const int32_t* __restrict__ colptr,
+                          const uint32_t* __restrict__ rows, const double2* __restrict__ coef,
+                          double2* __restrict__ src_bar) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = blockIdx.y;
+    if (t >= T) return;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int32_t q = colptr[s]; q < colptr[s + 1]; ++q) {
+        const uint32_t e = rows[q] & 0x7fffffffu;
+        const double2 lb = Lb[static_cast<size_t>(t) * E + e];
+        const double2 w = coef[q];
+        acc = (rows[q] >> 31) ? cadd(acc, cmulc(w, lb)) : cadd(acc, cmulc(lb, w));
+    }
+    src_bar[static_cast<size_t>(s) * T + t] = acc;
+}
+
+// Z[q] = sum_t conj(Lb[t][e_q]) v~_q(t), one warp per CSR entry.
+__global__ void k_coef_z(const double2* __restrict__ Lb, uint32_t T, uint32_t E, const uint32_t* __restrict__ entry_row,
+                         const uint32_t* __restrict__ keys, uint32_t nnz, const double2* __restrict__ F,
+                         const double2* __restrict__ Cc, const double2* __restrict__ R, uint32_t nf3,
+                         double2* __restrict__ Z) {
+    const uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (q >= nnz) return;
+    const uint32_t e = entry_row[q], key = keys[q];
+    const uint32_t s = key & 0x7fffffffu;
+    const bool cj = (key >> 31) != 0;
+    const uint32_t kind = s / nf3, tri = s % nf3;
+    const double2* v = (kind == 0 ? F : (kind == 1 ? Cc : R)) + static_cast<size_t>(tri) * T;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint32_t t = lane; t < T; t += 32) {
+        double2 x = v[t];
+        if (cj) x = cconj(x);
+        acc = cadd(acc, cmulc(x, Lb[static_cast<size_t>(t) * E + e]));
+    }
+    acc = warp_sum2(acc);
+    if (lane == 0) Z[q] = acc;
+}
+
+// ---------------------------------------------------------- F/C/R adjoint --
+struct FcrAdjJob {
+    const double2* gamma;  // [nf][T]
+    const double2* Fb;     // [nf^3][T]
+    const double2* Cb;
+    const double2* Rb;
+    const double* omegas;  // [nf] (device)
+    const int* mirror;     // [nf] (device)
+    const uint8_t* fc_used;  // [nf^3]
+    double2* G1;   // [nf^3][T] partials: d/d g1
+    double2* G2F;  // d/d g2 of F (Gamma_{mirror j})
+    double2* G2C;  // d/d g2 of C (conj(Gamma_j))
+    double2* G2R;  // d/d g2 of R (Gamma_j)
+    double2* A2;   // [nf^3][T] conj(P g1)
+    double* wpart;  // [nf^3][1 + ntiles]
+    int ntiles;
+};
+
+constexpr int SC_THREADS = 256;
+constexpr int SC_ITEMS = 4;
+constexpr int SC_CHUNK = SC_THREADS * SC_ITEMS;
+
+// Exclusive block scan of NV complex values per thread; returns the block totals.
+template <int NV>
+__device__ __forceinline__ void block_xscan(double2 (&x)[NV], double2 (&tot)[NV], double2* sm /* [NV][33] */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double2 inc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        inc[v] = x[v];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double2 y = shfl_up2(inc[v], o);
+            if (lane >= o) inc[v] = cadd(inc[v], y);
+        }
+        if (lane == 31) sm[v * 33 + warp] = inc[v];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            double2 a = lane < nw ? sm[v * 33 + lane] : make_double2(0.0, 0.0);
+            double2 ai = a;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double2 y = shfl_up2(ai, o);
+                if (lane >= o) ai = cadd(ai, y);
+            }
+            if (lane < nw) sm[v * 33 + lane] = csub(ai, a);  // exclusive warp offsets
+            if (lane == 31) sm[v * 33 + 32] = ai;            // block total
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        x[v] = cadd(sm[v * 33 + warp], csub(inc[v], x[v]));
+        tot[v] = sm[v * 33 + 32];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sm) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sm[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += sm[w];
+    __syncthreads();
+    return t;
+}
+
+__device__ __forceinline__ double2 phase_m(double w, double dt, uint32_t k) {  // e^{-i w k dt}
+    double s, c;
+    sincos(w * (static_cast<double>(k) * dt), &s, &c);
+    return make_double2(c, -s);
+}
+
+// -i x (multiplication by -i)
+__device__ __forceinline__ double2 mul_mi(double2 x) { return make_double2(x.y, -x.x); }
+
+// One CTA per (triple, job): the O(T) parts of the F, C, R adjoints.
+__global__ void __launch_bounds__(SC_THREADS) k_fcr_adj_scan(const FcrAdjJob* __restrict__ jobs, int nf, uint32_t T,
+                                                             double dt) {
+    __shared__ double2 sm[5 * 33];
+    __shared__ double red[SC_THREADS / 32];
+    const FcrAdjJob jb = jobs[blockIdx.y];
+    const uint32_t q = blockIdx.x;
+    const int nf2 = nf * nf;
+    const int i = static_cast<int>(q / nf2), jj = static_cast<int>((q / nf) % nf), kk = static_cast<int>(q % nf);
+    const double w = jb.omegas[i] + jb.omegas[jj] + jb.omegas[kk];
+    const double2* g1 = jb.gamma + static_cast<size_t>(i) * T;
+    const double2* g2F = jb.gamma + static_cast<size_t>(jb.mirror[jj]) * T;
+    const double2* gj = jb.gamma + static_cast<size_t>(jj) * T;  // C uses conj(gj), R uses gj
+    const size_t qo = static_cast<size_t>(q) * T;
+    const double2* Fb = jb.Fb + qo;
+    const double2* Cb = jb.Cb + qo;
+    const double2* Rb = jb.Rb + qo;
+    const double dt2 = dt * dt;
+    double wacc = 0.0;
+    // prefix pass: A0F, A1F, A0C, A1C, B0
+    double2 carry[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) carry[v] = make_double2(0.0, 0.0);
+    for (uint32_t c0 = 0; c0 < T; c0 += SC_CHUNK) {
+        double2 x[SC_ITEMS][5];
+        double2 tsum[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) tsum[v] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int it = 0; it < SC_ITEMS; ++it) {
+            const uint32_t t = c0 + threadIdx.x * SC_ITEMS + it;
+            if (t < T) {
+                const double2 P = phase_m(w, dt, t), Q = cconj(P);
+                const double2 a = cmul(g2F[t], Q);
+                const double2 b = cmul(cconj(gj[t]), Q);
+                x[it][0] = a;
+                x[it][1] = cscale(a, static_cast<double>(t));
+                x[it][2] = b;
+                x[it][3] = cscale(b, static_cast<double>(t));
+                x[it][4] = cmul(gj[t], P);
+            } else {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) x[it][v] = make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int v = 0; v < 5; ++v) tsum[v] = cadd(tsum[v], x[it][v]);
+        }
+        double2 tot[5];
+        block_xscan<5>(tsum, tot, sm);
+        double2 run[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) run[v] = cadd(carry[v], tsum[v]);
+#pragma unroll
+        for (int it = 0; it < SC_ITEMS; ++it) {
+            const uint32_t t = c0 + threadIdx.x * SC_ITEMS + it;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) run[v] = cadd(run[v], x[it][v]);
+            if (t < T) {
+                const double2 P = phase_m(w, dt, t);
+                const double2 g1t = g1[t];
+                const double2 fb = Fb[t], cb = Cb[t], rb = Rb[t];
+                const double tt = static_cast<double>(t);
+                // F: G(g1) += conj(dt P A0) Fb ; dl/dw += Re[-i dt^2 conj(Fb) g1 P (t A0 - A1)]
+                const double2 SF = cscale(cmul(P, run[0]), dt);
+                const double2 SC = cscale(cmul(P, run[2]), dt);
+                double2 G1 = cadd(cmulc(fb, SF), cmulc(cb, SC));
+                G1 = cadd(G1, cscale(cmulc(rb, run[4]), dt));
+                const double2 TF = cmul(P, csub(cscale(run[0], tt), run[1]));
+                const double2 TC = cmul(P, csub(cscale(run[2], tt), run[3]));
+                wacc += dt2 * (mul_mi(cmul(cmulc(g1t, fb), TF)).x + mul_mi(cmul(cmulc(g1t, cb), TC)).x);
+                jb.G1[qo + t] = G1;
+                jb.A2[qo + t] = cconj(cmul(P, g1t));
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) carry[v] = cadd(carry[v], tot[v]);
+    }
+    __syncthreads();
+    // suffix pass over u = T - 1 - t: SufF, SufC, SR0, SR1
+    double2 carry2[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) carry2[v] = make_double2(0.0, 0.0);
+    for (uint32_t c0 = 0; c0 < T; c0 += SC_CHUNK) {
+        double2 x[SC_ITEMS][4];
+        double2 tsum[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) tsum[v] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int it = 0; it < SC_ITEMS; ++it) {
+            const uint32_t u = c0 + threadIdx.x * SC_ITEMS + it;
+            if (u < T) {
+                const uint32_t t = T - 1 - u;
+                const double2 Q = cconj(phase_m(w, dt, t));
+                const double2 cg1 = cconj(g1[t]);
+                const double2 qg = cmul(Q, cg1);
+                x[it][0] = cmul(qg, Fb[t]);
+                x[it][1] = cmul(qg, Cb[t]);
+                x[it][2] = cmul(cg1, Rb[t]);
+                x[it][3] = Rb[t];
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) x[it][v] = make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) tsum[v] = cadd(tsum[v], x[it][v]);
+        }
+        double2 tot[4];
+        block_xscan<4>(tsum, tot, sm);
+        double2 run[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) run[v] = cadd(carry2[v], tsum[v]);
+#pragma unroll
+        for (int it = 0; it < SC_ITEMS; ++it) {
+            const uint32_t u = c0 + threadIdx.x * SC_ITEMS + it;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) run[v] = cadd(run[v], x[it][v]);
+            if (u < T) {
+                const uint32_t t = T - 1 - u;
+                const double2 P = phase_m(w, dt, t), Q = cconj(P);
+                const double2 g1t = g1[t], g2r = gj[t];
+                jb.G2F[qo + t] = cscale(cmul(P, run[0]), dt);
+                jb.G2C[qo + t] = cscale(cmul(P, run[1]), dt);
+                const double2 g2P = cmul(g2r, P), g1P = cmul(g1t, P);
+                jb.G1[qo + t] = csub(jb.G1[qo + t], cscale(cmul(cconj(g2P), run[3]), dt));
+                jb.G2R[qo + t] = cscale(csub(cmul(Q, run[2]), cmul(cconj(g1P), run[3])), dt);
+                const double2 br = csub(cconj(run[2]), cmul(g1t, cconj(run[3])));
+                wacc += static_cast<double>(t) * dt2 * mul_mi(cmul(g2P, br)).x;
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) carry2[v] = cadd(carry2[v], tot[v]);
+    }
+    const double ws = block_sum(wacc, red);
+    if (threadIdx.x == 0) jb.wpart[static_cast<size_t>(q) * (1 + jb.ntiles)] = ws;
+}
+
+constexpr int CR_TM = 128;  // outputs per CTA (one per thread)
+constexpr int CR_TK = 256;  // k per shared-memory tile
+
+// Correlations c1, c2, c3 of the F and C adjoints: one CTA per (m tile, triple, job).
+__global__ void __launch_bounds__(CR_TM) k_fcr_adj_corr(const FcrAdjJob* __restrict__ jobs, int nf, uint32_t T,
+                                                        double dt) {
+    __shared__ double2 fb_s[CR_TK], cb_s[CR_TK];
+    __shared__ double2 a1f_s[CR_TM + CR_TK], a1c_s[CR_TM + CR_TK], a2_s[CR_TM + CR_TK];
+    __shared__ double red[CR_TM / 32];
+    const FcrAdjJob jb = jobs[blockIdx.z];
+    const uint32_t q = blockIdx.y;
+    if (!jb.fc_used[q]) return;
+    const int nf2 = nf * nf;
+    const int i = static_cast<int>(q / nf2), jj = static_cast<int>((q / nf) % nf), kk = static_cast<int>(q % nf);
+    const double w = jb.omegas[i] + jb.omegas[jj] + jb.omegas[kk];
+    const double2* g2F = jb.gamma + static_cast<size_t>(jb.mirror[jj]) * T;
+    const double2* gj = jb.gamma + static_cast<size_t>(jj) * T;
+    const size_t qo = static_cast<size_t>(q) * T;
+    const double2* Fb = jb.Fb + qo;
+    const double2* Cb = jb.Cb + qo;
+    const double2* A2 = jb.A2 + qo;
+    const uint32_t m0 = blockIdx.x * CR_TM;
+    const uint32_t m = m0 + threadIdx.x;
+    double2 c1f = make_double2(0.0, 0.0), c1c = c1f, c2f = c1f, c2c = c1f, c3f = c1f, c3c = c1f;
+    for (uint32_t k0 = m0; k0 < T; k0 += CR_TK) {
+        // j = k - m ranges over [k0 - m0 - (TM - 1), k0 - m0 + TK - 1]; stage j >= 0
+        const int64_t jbase = static_cast<int64_t>(k0) - m0 - (CR_TM - 1);
+        __syncthreads();
+        for (int x = threadIdx.x; x < CR_TK; x += CR_TM) {
+            const uint32_t k = k0 + x;
+            fb_s[x] = k < T ? Fb[k] : make_double2(0.0, 0.0);
+            cb_s[x] = k < T ? Cb[k] : make_double2(0.0, 0.0);
+        }
+        for (int x = threadIdx.x; x < CR_TM + CR_TK - 1; x += CR_TM) {
+            const int64_t jv = jbase + x;
+            if (jv >= 0 && jv < static_cast<int64_t>(T)) {
+                a1f_s[x] = cconj(g2F[jv]);
+                a1c_s[x] = gj[jv];  // conj(conj(Gamma_j))
+                a2_s[x] = A2[jv];
+            } else {
+                a1f_s[x] = make_double2(0.0, 0.0);
+                a1c_s[x] = a1f_s[x];
+                a2_s[x] = a1f_s[x];
+            }
+        }
+        __syncthreads();
+        if (m < T) {
+            const uint32_t kbeg = max(k0, m), kend = min(k0 + CR_TK, T);
+            for (uint32_t k = kbeg; k < kend; ++k) {
+                const int xs = static_cast<int>(static_cast<int64_t>(k) - m - jbase);
+                const double2 fb = fb_s[k - k0], cb = cb_s[k - k0];
+                const double2 a2 = a2_s[xs];
+                c1f = cfma2(a1f_s[xs], fb, c1f);
+                c1c = cfma2(a1c_s[xs], cb, c1c);
+                const double2 tf = cmul(a2, fb), tc = cmul(a2, cb);
+                const double jd = static_cast<double>(k - m);
+                c2f = cadd(c2f, tf);
+                c2c = cadd(c2c, tc);
+                c3f = make_double2(fma(jd, tf.x, c3f.x), fma(jd, tf.y, c3f.y));
+                c3c = make_double2(fma(jd, tc.x, c3c.x), fma(jd, tc.y, c3c.y));
+            }
+        }
+    }
+    double wv = 0.0;
+    if (m < T) {
+        const double2 Q = cconj(phase_m(w, dt, m));
+        jb.G1[qo + m] = csub(jb.G1[qo + m], cscale(cmul(Q, cadd(c1f, c1c)), dt));
+        jb.G2F[qo + m] = csub(jb.G2F[qo + m], cscale(c2f, dt));
+        jb.G2C[qo + m] = csub(jb.G2C[qo + m], cscale(c2c, dt));
+        // Re[i dt^2 (g2F conj(c3F) + g2C conj(c3C))], g2C = conj(Gamma_j)
+        const double2 s = cadd(cmulc(g2F[m], c3f), cconj(cmul(gj[m], c3c)));
+        wv = -dt * dt * s.y;
+    }
+    const double ws = block_sum(wv, red);
+    if (threadIdx.x == 0) jb.wpart[static_cast<size_t>(q) * (1 + jb.ntiles) + 1 + blockIdx.x] = ws;
+}
+
+// Gamma_bar[b][t] += the partials of every triple that reads column b.
+__global__ void k_fcr_adj_reduce(const FcrAdjJob* __restrict__ jobs, int nf, uint32_t T, double2* const* gbar) {
+    const FcrAdjJob jb = jobs[blockIdx.z];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    if (t >= T) return;
+    const int nf2 = nf * nf;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int x = 0; x < nf2; ++x) {  // g1 = Gamma_i with i = b
+        acc = cadd(acc, jb.G1[(static_cast<size_t>(b) * nf2 + x) * T + t]);
+    }
+    for (int i = 0; i < nf; ++i)
+        for (int jj = 0; jj < nf; ++jj) {
+            const bool mir = jb.mirror[jj] == b, dir = jj == b;
+            if (!mir && !dir) continue;
+            for (int kk = 0; kk < nf; ++kk) {
+                const size_t o = (static_cast<size_t>(i) * nf2 + jj * nf + kk) * T + t;
+                if (mir) acc = cadd(acc, jb.G2F[o]);
+                if (dir) acc = cadd(acc, cadd(cconj(jb.G2C[o]), jb.G2R[o]));
+            }
+        }
+    double2* out = gbar[blockIdx.z] + static_cast<size_t>(b) * T + t;
+    *out = cadd(*out, acc);
+}
+
+// ------------------------------------------------------------ TCL2 adjoint --
+// G(Gamma_b(t)) += 2 Re sum_e conj(Lb_e) D_b,e + i Re sum_e conj(Lb_e) U_b,e
+__global__ void k_tcl2_adj_gamma(const double2* __restrict__ Lb, uint32_t T, uint32_t E, int nf,
+                                 const double2* __restrict__ Db, const double2* __restrict__ Ub,
+                                 double2* __restrict__ gbar) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const double2* l = Lb + static_cast<size_t>(t) * E;
+    for (int b = 0; b < nf; ++b) {
+        double sd = 0.0, su = 0.0;
+        for (uint32_t e = 0; e < E; ++e) {
+            const double2 x = l[e];
+            const double2 d = Db[static_cast<size_t>(b) * E + e], u = Ub[static_cast<size_t>(b) * E + e];
+            sd += x.x * d.x + x.y * d.y;  // Re(conj(x) d)
+            su += x.x * u.x + x.y * u.y;
+        }
+        double2* o = gbar + static_cast<size_t>(b) * T + t;
+        *o = cadd(*o, make_double2(2.0 * sd, su));
+    }
+}
+
+// Per entry e: GL0 = sum_t Lb, GD_b = sum_t 2 Re Gamma_b(t) Lb, GU_b = sum_t Im Gamma_b(t) Lb.
+__global__ void k_tcl2_adj_maps(const double2* __restrict__ Lb, uint32_t T, uint32_t E, int nf,
+                                const double2* __restrict__ gamma, double2* __restrict__ out /* [(1+2nf)][E] */) {
+    __shared__ double2 sm[8][32];
+    const uint32_t e = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int v = 0; v < 1 + 2 * nf; ++v) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (uint32_t t = threadIdx.x; t < T; t += blockDim.x) {
+            const double2 x = Lb[static_cast<size_t>(t) * E + e];
+            double s = 1.0;
+            if (v > 0) {
+                const int b = (v - 1) >> 1;
+                const double2 g = gamma[static_cast<size_t>(b) * T + t];
+                s = ((v - 1) & 1) ? g.y : 2.0 * g.x;
+            }
+            acc = cadd(acc, cscale(x, s));
+        }
+        acc = warp_sum2(acc);
+        if (lane == 0) sm[warp][v & 31] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double2 t2 = make_double2(0.0, 0.0);
+            for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t2 = cadd(t2, sm[w][v & 31]);
+            out[static_cast<size_t>(v) * E + e] = t2;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------- inner products --
+struct InnerJob {
+    const double2* a;
+    const double2* b;
+    uint64_t n;
+};
+
+__global__ void k_inner_re(const InnerJob* __restrict__ jobs, double* __restrict__ out) {
+    __shared__ double red[8];
+    const InnerJob jb = jobs[blockIdx.x];
+    double acc = 0.0;
+    for (uint64_t k = threadIdx.x; k < jb.n; k += blockDim.x) {
+        const double2 x = jb.a[k], y = jb.b[k];
+        acc += x.x * y.x + x.y * y.y;
+    }
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+template <class T>
+T* upload(Carve& cv, const std::vector<T>& v, cudaStream_t st, const char* what) {
+    T* d = cv.take<T>(v.size());
+    if (!v.empty()) cuda_check(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st), what);
+    return d;
+}
+
+}  // namespace
+
+// ============================================================== host side ==
+std::size_t rk4_num_checkpoints(std::size_t steps, std::size_t every) {
+    return every ? (steps + every - 1) / every : 0;
+}
+
+namespace {
+
+void validate_rk4g(const std::vector<Rk4GradJob>& jobs, std::size_t every, bool adjoint) {
+    if (every == 0) throw Error(kInvalidArgument, "rk4 gradient: checkpoint_every must be > 0");
+    for (const auto& j : jobs) {
+        if (j.D <= 0 || j.D > 16) throw Error(kInvalidArgument, "rk4 gradient: D = N^2 must be in [1, 16]");
+        if (!(j.dt > 0.0)) throw Error(kInvalidArgument, "rk4 gradient: dt must be > 0");
+        if (j.steps < 1) throw Error(kInvalidArgument, "rk4 gradient: at least one step");
+        if (!j.L || !j.r0) throw Error(kInvalidArgument, "rk4 gradient: null L or r0");
+        if (!j.ckpt) throw Error(kInvalidArgument, "rk4 gradient: null checkpoint buffer");
+        if ((j.obs_out || j.obs_bar) && (!j.obs || j.sample_every == 0))
+            throw Error(kInvalidArgument, "rk4 gradient: samples need obs and sample_every > 0");
+        if (adjoint && !j.L_bar) throw Error(kInvalidArgument, "rk4 adjoint: null L_bar");
+    }
+    if (every * 16 * sizeof(double2) > 160 * 1024) throw Error(kInvalidArgument, "rk4 adjoint: checkpoint_every too large");
+}
+
+std::vector<Rk4GJob> to_gjobs(const std::vector<Rk4GradJob>& jobs) {
+    std::vector<Rk4GJob> out(jobs.size());
+    for (std::size_t k = 0; k < jobs.size(); ++k) {
+        const auto& j = jobs[k];
+        out[k] = Rk4GJob{j.L,     j.L_add,   j.steps,  j.D,           j.dt,        j.r0,  j.obs,    j.sample_every,
+                         j.ckpt,  j.obs_out, j.r_out,  j.obs_bar,     j.r_final_bar, j.L_bar, j.r0_bar, j.obs_vec_bar};
+    }
+    return out;
+}
+
+}  // namespace
+
+void rk4_forward_checkpointed(const std::vector<Rk4GradJob>& jobs, std::size_t every, cudaStream_t st) {
+    if (jobs.empty()) return;
+    validate_rk4g(jobs, every, false);
+    std::vector<Rk4GJob> gj = to_gjobs(jobs);
+    Carve probe{nullptr};
+    probe.take<Rk4GJob>(gj.size());
+    Carve cv{grad_scratch().ensure(probe.off + 256)};
+    Rk4GJob* dj = upload(cv, gj, st, "rk4g jobs");
+    int dmax = 0;
+    for (const auto& j : jobs) dmax = std::max(dmax, j.D);
+    const int n = static_cast<int>(jobs.size());
+    const unsigned grid = static_cast<unsigned>((n + 3) / 4);
+    if (dmax <= 4) k_rk4g_fwd<4><<<grid, 128, 0, st>>>(dj, n, every);
+    else k_rk4g_fwd<16><<<grid, 128, 0, st>>>(dj, n, every);
+    launched("k_rk4g_fwd");
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(rk4 forward)");
+}
+
+void rk4_adjoint(const std::vector<Rk4GradJob>& jobs, std::size_t every, cudaStream_t st) {
+    if (jobs.empty()) return;
+    validate_rk4g(jobs, every, true);
+    std::vector<Rk4GJob> gj = to_gjobs(jobs);
+    Carve probe{nullptr};
+    probe.take<Rk4GJob>(gj.size());
+    Carve cv{grad_scratch().ensure(probe.off + 256)};
+    Rk4GJob* dj = upload(cv, gj, st, "rk4g jobs");
+    int dmax = 0;
+    for (const auto& j : jobs) dmax = std::max(dmax, j.D);
+    const unsigned n = static_cast<unsigned>(jobs.size());
+    if (dmax <= 4) {
+        const std::size_t smem = every * 4 * sizeof(double2);
+        cuda_check(cudaFuncSetAttribute(k_rk4g_adj<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                   "cudaFuncSetAttribute(k_rk4g_adj)");
+        k_rk4g_adj<4><<<n, 32, smem, st>>>(dj, every);
+    } else {
+        const std::size_t smem = every * 16 * sizeof(double2);
+        cuda_check(cudaFuncSetAttribute(k_rk4g_adj<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                   "cudaFuncSetAttribute(k_rk4g_adj)");
+        k_rk4g_adj<16><<<n, 32, smem, st>>>(dj, every);
+    }
+    launched("k_rk4g_adj");
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(rk4 adjoint)");
+}
+
+void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
+    if (jobs.empty()) return;
+    // group by (nf, T): one launch per kernel and group
+    std::map<std::pair<int, std::size_t>, std::vector<std::size_t>> groups;
+    for (std::size_t k = 0; k < jobs.size(); ++k) {
+        const auto& j = jobs[k];
+        if (!j.sys || j.T == 0 || !j.gamma || !j.L_bar || !j.gamma_bar)
+            throw Error(kInvalidArgument, "tcl4 adjoint: null or empty input");
+        if (!(j.dt > 0.0)) throw Error(kInvalidArgument, "tcl4 adjoint: dt must be > 0");
+        if (j.T > 0x7fffffffu) throw Error(kOverflow, "tcl4 adjoint: T too large");
+        if (j.sys->nf > 27) throw Error(kInvalidArgument, "tcl4 adjoint: at most 27 Bohr frequencies");
+        groups[{j.sys->nf, j.T}].push_back(k);
+    }
+    for (auto& g : groups)
+        for (std::size_t k : g.second)
+            if (jobs[k].dt != jobs[g.second[0]].dt)
+                throw Error(kInvalidArgument, "tcl4 adjoint: jobs with equal (nf, T) must share dt");
+    for (auto& g : groups) {
+        const int nf = g.first.first;
+        const std::size_t T = g.first.second;
+        const std::size_t nf3 = static_cast<std::size_t>(nf) * nf * nf;
+        const auto& idx = g.second;
+        const int ntiles = static_cast<int>((T + CR_TM - 1) / CR_TM);
+        // per job: coefficient tables (structural), CSC transpose, device metadata
+        struct Host {
+            CoefTable tab;
+            std::vector<int32_t> colptr;
+            std::vector<uint32_t> rows;  // e | conj << 31
+            std::vector<double2> ccoef;
+            std::vector<uint32_t> entry_row;
+        };
+        std::vector<Host> hs(idx.size());
+        std::size_t bytes = 0;
+        {
+            Carve probe{nullptr};
+            for (std::size_t a = 0; a < idx.size(); ++a) {
+                const auto& j = jobs[idx[a]];
+                const SystemDesc& s = *j.sys;
+                Host& h = hs[a];
+                build_coef_table(s.N, s.nf, s.p2f.data(), s.ops.data(), s.num_ops, h.tab, true);
+                const std::size_t E = static_cast<std::size_t>(s.N) * s.N * s.N * s.N;
+                const std::size_t nnz = h.tab.src.size();
+                h.colptr.assign(3 * nf3 + 1, 0);
+                for (std::size_t q = 0; q < nnz; ++q) h.colptr[(h.tab.src[q] & 0x7fffffffu) + 1]++;
+                for (std::size_t s2 = 0; s2 < 3 * nf3; ++s2) h.colptr[s2 + 1] += h.colptr[s2];
+                h.rows.resize(nnz);
+                h.ccoef.resize(nnz);
+                h.entry_row.resize(nnz);
+                std::vector<int32_t> fill(h.colptr.begin(), h.colptr.end() - 1);
+                for (std::size_t e = 0; e < E; ++e)
+                    for (int32_t q = h.tab.rowptr[e]; q < h.tab.rowptr[e + 1]; ++q) {
+                        const uint32_t key = h.tab.src[q];
+                        const int32_t dst = fill[key & 0x7fffffffu]++;
+                        h.rows[dst] = static_cast<uint32_t>(e) | (key & 0x80000000u);
+                        h.ccoef[dst] = h.tab.coef[q];
+                        h.entry_row[q] = static_cast<uint32_t>(e);
+                    }
+                probe.take<int32_t>(h.colptr.size());
+                probe.take<uint32_t>(nnz);
+                probe.take<double2>(nnz);
+                probe.take<uint32_t>(nnz);
+                probe.take<uint32_t>(nnz);
+                probe.take<double2>(nnz);             // Z
+                probe.take<double2>(3 * nf3 * T);     // src_bar
+                probe.take<double2>(5 * nf3 * T);     // G1, G2F, G2C, G2R, A2
+                probe.take<double>(nf3 * (1 + ntiles));
+                probe.take<double>(nf);
+                probe.take<int>(nf);
+                probe.take<uint8_t>(nf3);
+            }
+            probe.take<FcrAdjJob>(idx.size());
+            probe.take<double2*>(idx.size());
+            bytes = probe.off + 256;
+        }
+        Carve cv{grad_scratch().ensure(bytes)};
+        std::vector<FcrAdjJob> fj(idx.size());
+        std::vector<double2*> gbar(idx.size());
+        struct Dev {
+            int32_t* colptr;
+            uint32_t* rows;
+            double2* ccoef;
+            uint32_t* erow;
+            uint32_t* keys;
+            double2* Z;
+            double2* src_bar;
+            double* wpart;
+        };
+        std::vector<Dev> dv(idx.size());
+        for (std::size_t a = 0; a < idx.size(); ++a) {
+            const auto& j = jobs[idx[a]];
+            const SystemDesc& s = *j.sys;
+            Host& h = hs[a];
+            Dev& d = dv[a];
+            const std::size_t nnz = h.tab.src.size();
+            d.colptr = upload(cv, h.colptr, st, "adj colptr");
+            d.rows = upload(cv, h.rows, st, "adj rows");
+            d.ccoef = upload(cv, h.ccoef, st, "adj coef");
+            d.erow = upload(cv, h.entry_row, st, "adj entry rows");
+            d.keys = upload(cv, h.tab.src, st, "adj keys");
+            d.Z = cv.take<double2>(nnz);
+            d.src_bar = cv.take<double2>(3 * nf3 * T);
+            double2* parts = cv.take<double2>(5 * nf3 * T);
+            d.wpart = cv.take<double>(nf3 * (1 + ntiles));
+            double* dom = upload(cv, s.omegas, st, "adj omegas");
+            int* dmir = upload(cv, s.mirror, st, "adj mirror");
+            std::vector<uint8_t> used(nf3);
+            for (std::size_t q = 0; q < nf3; ++q) used[q] = h.tab.triple_fc_used[q];
+            uint8_t* dused = upload(cv, used, st, "adj used");
+            FcrAdjJob& f = fj[a];
+            f.gamma = j.gamma;
+            f.Fb = d.src_bar;
+            f.Cb = d.src_bar + nf3 * T;
+            f.Rb = d.src_bar + 2 * nf3 * T;
+            f.omegas = dom;
+            f.mirror = dmir;
+            f.fc_used = dused;
+            f.G1 = parts;
+            f.G2F = parts + nf3 * T;
+            f.G2C = parts + 2 * nf3 * T;
+            f.G2R = parts + 3 * nf3 * T;
+            f.A2 = parts + 4 * nf3 * T;
+            f.wpart = d.wpart;
+            f.ntiles = ntiles;
+            gbar[a] = j.gamma_bar;
+        }
+        FcrAdjJob* dfj = upload(cv, fj, st, "adj jobs");
+        double2** dgbar = upload(cv, gbar, st, "adj gbar");
+        // 1. sources and the coupling-operator aggregation
+        for (std::size_t a = 0; a < idx.size(); ++a) {
+            const auto& j = jobs[idx[a]];
+            const std::size_t E = static_cast<std::size_t>(j.sys->N) * j.sys->N * j.sys->N * j.sys->N;
+            k_src_adj<<<dim3(static_cast<unsigned>((T + 127) / 128), static_cast<unsigned>(3 * nf3)), 128, 0, st>>>(
+                j.L_bar, static_cast<uint32_t>(T), static_cast<uint32_t>(E), dv[a].colptr, dv[a].rows, dv[a].ccoef,
+                dv[a].src_bar);
+            launched("k_src_adj");
+            const std::size_t nnz = hs[a].tab.src.size();
+            if (j.ops_bar && j.F && j.C && j.R && nnz) {
+                k_coef_z<<<static_cast<unsigned>((nnz + 7) / 8), 256, 0, st>>>(
+                    j.L_bar, static_cast<uint32_t>(T), static_cast<uint32_t>(E), dv[a].erow, dv[a].keys,
+                    static_cast<uint32_t>(nnz), j.F, j.C, j.R, static_cast<uint32_t>(nf3), dv[a].Z);
+                launched("k_coef_z");
+            }
+        }
+        // 2. F/C/R adjoint for every triple of every job
+        const unsigned nj = static_cast<unsigned>(idx.size());
+        for (std::size_t a = 0; a < idx.size(); ++a)
+            cuda_check(cudaMemsetAsync(dv[a].wpart, 0, nf3 * (1 + ntiles) * sizeof(double), st), "adj wpart zero");
+        k_fcr_adj_scan<<<dim3(static_cast<unsigned>(nf3), nj), SC_THREADS, 0, st>>>(dfj, nf, static_cast<uint32_t>(T),
+                                                                                    jobs[idx[0]].dt);
+        launched("k_fcr_adj_scan");
+        k_fcr_adj_corr<<<dim3(static_cast<unsigned>(ntiles), static_cast<unsigned>(nf3), nj), CR_TM, 0, st>>>(
+            dfj, nf, static_cast<uint32_t>(T), jobs[idx[0]].dt);
+        launched("k_fcr_adj_corr");
+        k_fcr_adj_reduce<<<dim3(static_cast<unsigned>((T + 127) / 128), static_cast<unsigned>(nf), nj), 128, 0, st>>>(
+            dfj, nf, static_cast<uint32_t>(T), dgbar);
+        launched("k_fcr_adj_reduce");
+        // 3. host: Bohr-frequency and coupling-operator gradients
+        std::vector<double> wpart(nf3 * (1 + ntiles));
+        std::vector<double2> Z;
+        for (std::size_t a = 0; a < idx.size(); ++a) {
+            const auto& j = jobs[idx[a]];
+            const SystemDesc& s = *j.sys;
+            cuda_check(cudaMemcpyAsync(wpart.data(), dv[a].wpart, wpart.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
+                       "adj wpart");
+            const std::size_t nnz = hs[a].tab.src.size();
+            const bool want_ops = j.ops_bar && j.F && j.C && j.R && nnz;
+            if (want_ops) {
+                Z.resize(nnz);
+                cuda_check(cudaMemcpyAsync(Z.data(), dv[a].Z, nnz * sizeof(double2), cudaMemcpyDeviceToHost, st), "adj Z");
+            }
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl4 adjoint)");
+            if (j.omega_bar) {
+                for (std::size_t q = 0; q < nf3; ++q) {
+                    double wq = 0.0;
+                    for (int x = 0; x <= ntiles; ++x) wq += wpart[q * (1 + ntiles) + x];
+                    const int i = static_cast<int>(q / (nf * nf)), jj = static_cast<int>((q / nf) % nf),
+                              kk = static_cast<int>(q % nf);
+                    j.omega_bar[i] += wq;
+                    j.omega_bar[jj] += wq;
+                    j.omega_bar[kk] += wq;
+                }
+            }
+            if (want_ops) coef_table_ops_grad(s.N, s.nf, s.p2f.data(), s.ops.data(), s.num_ops, hs[a].tab, Z.data(), j.ops_bar);
+        }
+    }
+}
+
+void tcl2_adjoint(const std::vector<Tcl2AdjointJob>& jobs, cudaStream_t st) {
+    for (const auto& j : jobs) {
+        if (!j.sys || !j.eps || !j.gamma || !j.L_bar || !j.gamma_bar || j.T == 0)
+            throw Error(kInvalidArgument, "tcl2 adjoint: null or empty input");
+        const SystemDesc& s = *j.sys;
+        const int nf = s.nf;
+        const std::size_t E = static_cast<std::size_t>(s.N) * s.N * s.N * s.N;
+        std::vector<double2> L0, Db, Ub;
+        tcl2_maps(s, j.eps, L0, Db, Ub);
+        Carve probe{nullptr};
+        probe.take<double2>(Db.size());
+        probe.take<double2>(Ub.size());
+        probe.take<double2>((1 + 2 * nf) * E);
+        Carve cv{grad_scratch().ensure(probe.off + 256)};
+        double2* dD = upload(cv, Db, st, "tcl2 adj D");
+        double2* dU = upload(cv, Ub, st, "tcl2 adj U");
+        double2* maps = cv.take<double2>((1 + 2 * nf) * E);
+        k_tcl2_adj_gamma<<<static_cast<unsigned>((j.T + 127) / 128), 128, 0, st>>>(
+            j.L_bar, static_cast<uint32_t>(j.T), static_cast<uint32_t>(E), nf, dD, dU, j.gamma_bar);
+        launched("k_tcl2_adj_gamma");
+        if (j.ops_bar || j.eps_bar) {
+            k_tcl2_adj_maps<<<static_cast<unsigned>(E), 256, 0, st>>>(j.L_bar, static_cast<uint32_t>(j.T),
+                                                                       static_cast<uint32_t>(E), nf, j.gamma, maps);
+            launched("k_tcl2_adj_maps");
+            std::vector<double2> h((1 + 2 * nf) * E);
+            cuda_check(cudaMemcpyAsync(h.data(), maps, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, st), "tcl2 adj maps");
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl2 adjoint)");
+            std::vector<double2> GL0(h.begin(), h.begin() + E), GD(nf * E), GU(nf * E);
+            for (int b = 0; b < nf; ++b)
+                for (std::size_t e = 0; e < E; ++e) {
+                    GD[b * E + e] = h[(1 + 2 * b) * E + e];
+                    GU[b * E + e] = h[(2 + 2 * b) * E + e];
+                }
+            tcl2_maps_grad(s, j.eps, GL0, GD, GU, j.ops_bar, j.eps_bar);
+        } else {
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl2 adjoint)");
+        }
+    }
+}
+
+void inner_re_device(const std::vector<InnerRequest>& reqs, double* out, cudaStream_t st) {
+    if (reqs.empty()) return;
+    std::vector<InnerJob> js(reqs.size());
+    for (std::size_t k = 0; k < reqs.size(); ++k) {
+        if (!reqs[k].a || !reqs[k].b) throw Error(kInvalidArgument, "inner: null pointer");
+        js[k] = InnerJob{reqs[k].a, reqs[k].b, reqs[k].n};
+    }
+    Carve probe{nullptr};
+    probe.take<InnerJob>(js.size());
+    probe.take<double>(js.size());
+    Carve cv{grad_scratch().ensure(probe.off + 256)};
+    InnerJob* dj = upload(cv, js, st, "inner jobs");
+    double* dout = cv.take<double>(js.size());
+    for (std::size_t k0 = 0; k0 < js.size(); k0 += 65535) {
+        const unsigned n = static_cast<unsigned>(std::min<std::size_t>(65535, js.size() - k0));
+        k_inner_re<<<n, 256, 0, st>>>(dj + k0, dout + k0);
+        launched("k_inner_re");
+    }
+    cuda_check(cudaMemcpyAsync(out, dout, js.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "inner out");
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(inner)");
+}
+
+}  // namespace taco

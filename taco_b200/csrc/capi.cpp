@@ -576,6 +576,150 @@ int taco_gw_to_liouvillian(const taco_c128* GW, int N, size_t T, taco_c128* L4, 
     });
 }
 
+int taco_bcf_fft(const taco_bcf_request* reqs, size_t n, int flags, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (!reqs && n) throw taco::Error(taco::kInvalidArgument, "bcf: null requests");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        const bool dout = (flags & TACO_OUT_DEVICE) != 0;
+        std::vector<taco::BcfRequest> rs(n);
+        DevAllocs da;
+        for (size_t k = 0; k < n; ++k) {
+            const taco_bcf_request& q = reqs[k];
+            taco::BcfRequest& r = rs[k];
+            r.model = q.model;
+            r.which = q.which;
+            r.alpha = q.alpha;
+            r.omega_c = q.omega_c;
+            r.lambda = q.lambda;
+            r.gamma = q.gamma;
+            r.beta = q.beta;
+            r.N = q.N;
+            r.dt = q.dt;
+            r.n_out = q.n_out;
+            if (!q.out) throw taco::Error(taco::kInvalidArgument, "bcf: null output");
+            r.out = dout ? reinterpret_cast<double2*>(q.out) : static_cast<double2*>(da.take(q.n_out * sizeof(double2)));
+        }
+        taco::bcf_device(rs, st);
+        if (!dout)
+            for (size_t k = 0; k < n; ++k)
+                taco::cuda_check(cudaMemcpyAsync(reqs[k].out, rs[k].out, reqs[k].n_out * sizeof(double2),
+                                                 cudaMemcpyDeviceToHost, st),
+                                 "bcf out");
+        taco::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(bcf)");
+    });
+}
+
+namespace {
+std::vector<taco::Rk4GradJob> to_rk4g(const taco_rk4_grad_job* jobs, size_t n) {
+    if (!jobs && n) throw taco::Error(taco::kInvalidArgument, "rk4 gradient: null jobs");
+    std::vector<taco::Rk4GradJob> out(n);
+    auto d2 = [](const taco_c128* p) { return reinterpret_cast<const double2*>(p); };
+    auto m2 = [](taco_c128* p) { return reinterpret_cast<double2*>(p); };
+    for (size_t k = 0; k < n; ++k) {
+        const taco_rk4_grad_job& j = jobs[k];
+        taco::Rk4GradJob& o = out[k];
+        o.L = d2(j.L);
+        o.L_add = d2(j.L_add);
+        o.steps = j.steps;
+        o.D = j.D;
+        o.dt = j.dt;
+        o.r0 = d2(j.r0);
+        o.obs = d2(j.obs);
+        o.sample_every = j.sample_every;
+        o.ckpt = m2(j.ckpt);
+        o.obs_out = m2(j.obs_out);
+        o.r_out = m2(j.r_out);
+        o.obs_bar = d2(j.obs_bar);
+        o.r_final_bar = d2(j.r_final_bar);
+        o.L_bar = m2(j.L_bar);
+        o.r0_bar = m2(j.r0_bar);
+        o.obs_vec_bar = m2(j.obs_vec_bar);
+    }
+    return out;
+}
+}  // namespace
+
+int taco_rk4_forward_checkpointed(const taco_rk4_grad_job* jobs, size_t n, size_t checkpoint_every, void* stream) {
+    return guarded([&] {
+        require_device();
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        taco::rk4_forward_checkpointed(to_rk4g(jobs, n), checkpoint_every, st);
+    });
+}
+
+int taco_rk4_adjoint(const taco_rk4_grad_job* jobs, size_t n, size_t checkpoint_every, void* stream) {
+    return guarded([&] {
+        require_device();
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        taco::rk4_adjoint(to_rk4g(jobs, n), checkpoint_every, st);
+    });
+}
+
+int taco_tcl4_adjoint(const taco_tcl4_adjoint_job* jobs, size_t n, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (!jobs && n) throw taco::Error(taco::kInvalidArgument, "tcl4 adjoint: null jobs");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        std::vector<taco::SystemDesc> sys(n);
+        std::vector<taco::Tcl4AdjointJob> js(n);
+        for (size_t k = 0; k < n; ++k) {
+            const taco_tcl4_adjoint_job& j = jobs[k];
+            sys[k] = to_desc(j.sys);
+            taco::Tcl4AdjointJob& o = js[k];
+            o.sys = &sys[k];
+            o.gamma = reinterpret_cast<const double2*>(j.gamma);
+            o.T = j.T;
+            o.dt = j.dt;
+            o.L_bar = reinterpret_cast<const double2*>(j.L_bar);
+            o.F = reinterpret_cast<const double2*>(j.F);
+            o.C = reinterpret_cast<const double2*>(j.C);
+            o.R = reinterpret_cast<const double2*>(j.R);
+            o.gamma_bar = reinterpret_cast<double2*>(j.gamma_bar);
+            o.omega_bar = j.omega_bar;
+            o.ops_bar = reinterpret_cast<double2*>(j.ops_bar);
+        }
+        taco::tcl4_adjoint(js, st);
+    });
+}
+
+int taco_tcl2_adjoint(const taco_tcl2_adjoint_job* jobs, size_t n, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (!jobs && n) throw taco::Error(taco::kInvalidArgument, "tcl2 adjoint: null jobs");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        std::vector<taco::SystemDesc> sys(n);
+        std::vector<taco::Tcl2AdjointJob> js(n);
+        for (size_t k = 0; k < n; ++k) {
+            const taco_tcl2_adjoint_job& j = jobs[k];
+            sys[k] = to_desc(j.sys);
+            taco::Tcl2AdjointJob& o = js[k];
+            o.sys = &sys[k];
+            o.eps = j.eps;
+            o.gamma = reinterpret_cast<const double2*>(j.gamma);
+            o.T = j.T;
+            o.L_bar = reinterpret_cast<const double2*>(j.L_bar);
+            o.gamma_bar = reinterpret_cast<double2*>(j.gamma_bar);
+            o.ops_bar = reinterpret_cast<double2*>(j.ops_bar);
+            o.eps_bar = j.eps_bar;
+        }
+        taco::tcl2_adjoint(js, st);
+    });
+}
+
+int taco_inner_re(const taco_inner_job* jobs, size_t n, double* out, void* stream) {
+    return guarded([&] {
+        require_device();
+        if ((!jobs || !out) && n) throw taco::Error(taco::kInvalidArgument, "inner: null pointer");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        std::vector<taco::InnerRequest> rs(n);
+        for (size_t k = 0; k < n; ++k)
+            rs[k] = taco::InnerRequest{reinterpret_cast<const double2*>(jobs[k].a),
+                                       reinterpret_cast<const double2*>(jobs[k].b), jobs[k].n};
+        taco::inner_re_device(rs, out, st);
+    });
+}
+
 int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t* src, taco_c128* coef, size_t cap,
                          size_t* nnz) {
     return guarded([&] {

@@ -890,6 +890,7 @@ void clear_tuning() {
 }
 
 uint64_t kernel_launches() { return g_launches.load(); }
+void count_launches(uint64_t n) { g_launches.fetch_add(n); }
 void profile_enable(bool on) { g_profile.store(on); }
 void profile_reset() {
     ProfStore& ps = prof_store();

@@ -108,6 +108,86 @@ void rk4_propagate_device(const std::vector<Rk4Request>& reqs, cudaStream_t stre
 
 std::size_t rk4_num_samples(std::size_t steps, std::size_t sample_every);
 
+// ----------------------------------------------------------------- bath ---
+// bcf_fft_fun (correlation_fft.hpp:153-214) on the device (bcf.cu); out is a device pointer.
+struct BcfRequest {
+    int model = 0;   // 0: Ohmic, 1: Ohmic + Drude-Lorentz
+    int which = 0;   // 0: C(t); 1: dC/dalpha; 2: dC/domega_c; 3: dC/dbeta
+    double alpha = 0.0, omega_c = 1.0, lambda = 0.0, gamma = 1.0, beta = 1.0;
+    std::size_t N = 0;  // grid: N + 1 samples
+    double dt = 0.0;
+    double2* out = nullptr;
+    std::size_t n_out = 0;
+};
+std::size_t bcf_nfft(std::size_t N);
+void bcf_device(const std::vector<BcfRequest>& reqs, cudaStream_t st);
+
+// ------------------------------------------------------------- adjoints ---
+// (adjoint.cu) Real losses; G(z) = dloss/dRe z + i dloss/dIm z.  Device pointers unless noted.
+struct Rk4GradJob {
+    const double2* L = nullptr;      // [steps+1][D x D] column-major
+    const double2* L_add = nullptr;  // optional, added to L (its gradient equals L_bar)
+    std::size_t steps = 0;
+    int D = 0;
+    double dt = 0.0;
+    const double2* r0 = nullptr;     // [D]
+    const double2* obs = nullptr;    // [D]: <O> = sum_l obs_l r_l
+    std::size_t sample_every = 0;
+    double2* ckpt = nullptr;         // [rk4_num_checkpoints(steps, every)][D]
+    double2* obs_out = nullptr;      // forward: [rk4_num_samples] samples of <O>
+    double2* r_out = nullptr;        // forward: final state
+    const double2* obs_bar = nullptr;      // adjoint: G(<O>) per sample
+    const double2* r_final_bar = nullptr;  // adjoint: G(final state), optional
+    double2* L_bar = nullptr;        // adjoint out: [steps+1][D x D]
+    double2* r0_bar = nullptr;       // adjoint out: [D]
+    double2* obs_vec_bar = nullptr;  // adjoint out: [D]
+};
+std::size_t rk4_num_checkpoints(std::size_t steps, std::size_t every);
+void rk4_forward_checkpointed(const std::vector<Rk4GradJob>& jobs, std::size_t every, cudaStream_t st);
+void rk4_adjoint(const std::vector<Rk4GradJob>& jobs, std::size_t every, cudaStream_t st);
+
+// L4 adjoint through the MIKX/GW map and the F/C/R kernels of one instance.
+struct Tcl4AdjointJob {
+    const SystemDesc* sys = nullptr;
+    const double2* gamma = nullptr;   // [nf][T]
+    std::size_t T = 0;
+    double dt = 0.0;
+    const double2* L_bar = nullptr;   // [T][N^4]
+    const double2* F = nullptr;       // [nf^3][T] forward sources (needed for ops_bar)
+    const double2* C = nullptr;
+    const double2* R = nullptr;
+    double2* gamma_bar = nullptr;     // [nf][T], accumulated
+    double* omega_bar = nullptr;      // host [nf], accumulated (nullable)
+    double2* ops_bar = nullptr;       // host [num_ops][N x N], accumulated (nullable)
+};
+void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st);
+
+// TCL2 adjoint: L2(t) = L0 + sum_b 2 Re Gamma_b(t) D_b + Im Gamma_b(t) U_b.
+struct Tcl2AdjointJob {
+    const SystemDesc* sys = nullptr;
+    const double* eps = nullptr;      // host [N]
+    const double2* gamma = nullptr;   // [nf][T]
+    std::size_t T = 0;
+    const double2* L_bar = nullptr;   // [T][N^4]
+    double2* gamma_bar = nullptr;     // [nf][T], accumulated
+    double2* ops_bar = nullptr;       // host, accumulated (nullable)
+    double* eps_bar = nullptr;        // host [N], accumulated (nullable)
+};
+void tcl2_adjoint(const std::vector<Tcl2AdjointJob>& jobs, cudaStream_t st);
+// Host maps of the TCL2 generator (tcl2.cu) and the reverse of their construction.
+void tcl2_maps(const SystemDesc& s, const double* eps, std::vector<double2>& L0, std::vector<double2>& Db,
+               std::vector<double2>& Ub);
+void tcl2_maps_grad(const SystemDesc& s, const double* eps, const std::vector<double2>& GL0,
+                    const std::vector<double2>& GD, const std::vector<double2>& GU, double2* ops_bar, double* eps_bar);
+
+struct InnerRequest {
+    const double2* a = nullptr;
+    const double2* b = nullptr;
+    std::size_t n = 0;
+};
+// out[k] = sum_i Re(conj(a_i) b_i) (host out)
+void inner_re_device(const std::vector<InnerRequest>& reqs, double* out, cudaStream_t st);
+
 // Mirror map of cpp/src/tcl/tcl4.cpp:40-101.
 void build_mirror(const std::vector<double>& omegas, double tol, std::vector<int>& mirror, int* zero_index);
 
@@ -118,6 +198,13 @@ cudaStream_t default_stream();
 // on, each launch is bracketed by CUDA events and its device time is accumulated per
 // kernel name after the call's final synchronisation.
 uint64_t kernel_launches();
+// Adds n to the process-wide launch counter (kernels launched outside engine.cu).
+void count_launches(uint64_t n);
+// Checks the launch just issued and counts it.
+inline void launched(const char* what) {
+    cuda_check(cudaGetLastError(), what);
+    count_launches(1);
+}
 void profile_enable(bool on);
 void profile_reset();
 struct ProfileEntry {

@@ -31,6 +31,16 @@ struct CoefTable {
 };
 
 // ops: num_ops matrices, column-major N x N (eigenbasis); p2f column-major N x N.
-void build_coef_table(int N, int nf, const int* p2f, const double2* ops, int num_ops, CoefTable& out);
+// structural: keep every (entry, source) pair the sums reach, zero coefficients included
+// (the sparsity pattern of the map for all operator values, as the gradient needs).
+void build_coef_table(int N, int nf, const int* p2f, const double2* ops, int num_ops, CoefTable& out,
+                      bool structural = false);
+
+// Gradient of a real loss with respect to the coupling operators through the table's
+// coefficients (table built with structural = true).  Z[q] = sum_t conj(G(L4_e(t))) v~_q(t) for CSR entry q of row e (v~ the
+// source value, conjugated for conjugated entries); ops_bar (num_ops x N x N) is
+// accumulated with G(a) = dloss/dRe a + i dloss/dIm a for every operator entry a.
+void coef_table_ops_grad(int N, int nf, const int* p2f, const double2* ops, int num_ops, const CoefTable& table,
+                         const double2* Z, double2* ops_bar);
 
 }  // namespace taco

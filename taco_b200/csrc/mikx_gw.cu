@@ -153,7 +153,7 @@ void mikx_device(const double2* F, const double2* C, const double2* R, const int
         const std::size_t nf3 = static_cast<std::size_t>(nf) * nf * nf, N4 = static_cast<std::size_t>(N) * N * N * N;
         k_mikx<<<dim3(grid_for(N6), nt), 256, 0, st>>>(F + t0 * nf3, C + t0 * nf3, R + t0 * nf3, p2f_dev, N, nf,
                                                        M + t0 * N4, I + t0 * N4, K + t0 * N4, X + t0 * N6);
-        cuda_check(cudaGetLastError(), "k_mikx");
+        launched("k_mikx");
     }
 }
 
@@ -165,10 +165,10 @@ void gw_device(const double2* M, const double2* I, const double2* K, const doubl
         double2* dst = symmetrize ? tmp + t0 * N4 : GW + t0 * N4;
         k_gw_raw<<<dim3(static_cast<unsigned>((N4 + 127) / 128), nt), 128, 0, st>>>(M + t0 * N4, I + t0 * N4, K + t0 * N4,
                                                                                    X + t0 * N6, ops_dev, N, num_ops, dst);
-        cuda_check(cudaGetLastError(), "k_gw_raw");
+        launched("k_gw_raw");
         if (symmetrize) {
             k_gw_sym<<<dim3(static_cast<unsigned>((N4 + 255) / 256), nt), 256, 0, st>>>(dst, N, GW + t0 * N4);
-            cuda_check(cudaGetLastError(), "k_gw_sym");
+            launched("k_gw_sym");
         }
     }
 }
@@ -178,7 +178,7 @@ void gw_to_l4_device(const double2* GW, int N, std::size_t T, double2* L4, cudaS
     for (std::size_t t0 = 0; t0 < T; t0 += 65535) {
         const unsigned nt = static_cast<unsigned>(std::min<std::size_t>(65535, T - t0));
         k_gw_to_l4<<<dim3(static_cast<unsigned>((N4 + 255) / 256), nt), 256, 0, st>>>(GW + t0 * N4, N, L4 + t0 * N4);
-        cuda_check(cudaGetLastError(), "k_gw_to_l4");
+        launched("k_gw_to_l4");
     }
 }
 

@@ -175,11 +175,70 @@ __global__ void k_add_c64(const float2* __restrict__ src, double2* __restrict__ 
 void add_c64_into_c128(const float2* src, double2* dst, std::size_t n, cudaStream_t st) {
     const unsigned grid = static_cast<unsigned>(std::min<std::size_t>((n + 255) / 256, 148 * 16));
     k_add_c64<<<grid, 256, 0, st>>>(src, dst, n);
-    cuda_check(cudaGetLastError(), "k_add_c64");
+    launched("k_add_c64");
 }
 
-void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2* gamma, std::size_t Nt,
-                        const std::vector<uint32_t>& tidx, double2* out, cudaStream_t st) {
+namespace {
+
+// reverse of kron_add(L, n, A, B, s): G(A) and G(B) from G(L) (either may be null)
+void kron_add_grad(const std::vector<cd>& GL, int n, const std::vector<cd>& A, const std::vector<cd>& B, cd s,
+                   std::vector<cd>* GA, std::vector<cd>* GB) {
+    const std::size_t D = static_cast<std::size_t>(n) * n;
+    const cd sc = std::conj(s);
+    for (int r1 = 0; r1 < n; ++r1)
+        for (int c1 = 0; c1 < n; ++c1)
+            for (int r2 = 0; r2 < n; ++r2)
+                for (int c2 = 0; c2 < n; ++c2) {
+                    const cd g = GL[(static_cast<std::size_t>(r1) * n + r2) + D * (static_cast<std::size_t>(c1) * n + c2)];
+                    if (GA) (*GA)[r1 + n * c1] += sc * std::conj(B[r2 + n * c2]) * g;
+                    if (GB) (*GB)[r2 + n * c2] += sc * std::conj(A[r1 + n * c1]) * g;
+                }
+}
+
+// G(H) of unitary_add(L, n, H, 1) = -i kron(I, H) + i kron(H^T, I)
+std::vector<cd> unitary_grad(const std::vector<cd>& GL, int n, const std::vector<cd>& H) {
+    std::vector<cd> I(static_cast<std::size_t>(n) * n, cd(0.0, 0.0)), HT(I.size()), GH(I.size(), cd(0.0, 0.0)),
+        GHT(I.size(), cd(0.0, 0.0));
+    for (int i = 0; i < n; ++i) I[i + n * i] = 1.0;
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) HT[r + n * c] = H[c + n * r];
+    kron_add_grad(GL, n, I, H, cd(0.0, -1.0), nullptr, &GH);
+    kron_add_grad(GL, n, HT, I, cd(0.0, 1.0), &GHT, nullptr);
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) GH[c + n * r] += GHT[r + n * c];
+    return GH;
+}
+
+// Coupling operator alpha restricted to the pairs of bucket b, its A^+ A, and whether the
+// reference includes the term (non-zero A_ab and non-zero A^+ A).
+bool bucket_op(const SystemDesc& s, int b, int al, std::vector<cd>& Aw, std::vector<cd>& AdA) {
+    const int n = s.N;
+    const std::size_t D = static_cast<std::size_t>(n) * n;
+    const cd* ops = reinterpret_cast<const cd*>(s.ops.data());
+    Aw.assign(D, cd(0.0, 0.0));
+    AdA.assign(D, cd(0.0, 0.0));
+    double nrm = 0.0;
+    for (std::size_t k = 0; k < D; ++k)
+        if (s.p2f[k] == b) {
+            Aw[k] = ops[static_cast<std::size_t>(al) * D + k];
+            nrm += std::norm(Aw[k]);
+        }
+    if (nrm == 0.0) return false;
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) {
+            cd acc(0.0, 0.0);
+            for (int k = 0; k < n; ++k) acc += std::conj(Aw[k + n * r]) * Aw[k + n * c];
+            AdA[r + n * c] = acc;
+        }
+    double an = 0.0;
+    for (auto& x : AdA) an += std::norm(x);
+    return an != 0.0;
+}
+
+}  // namespace
+
+void tcl2_maps(const SystemDesc& sys, const double* eps, std::vector<double2>& L0out, std::vector<double2>& Dbout,
+               std::vector<double2>& Ubout) {
     const int n = sys.N, nf = sys.nf;
     const std::size_t D = static_cast<std::size_t>(n) * n, E = D * D;
     std::vector<cd> L0(E, cd(0.0, 0.0)), Db(nf * E, cd(0.0, 0.0)), Ub(nf * E, cd(0.0, 0.0));
@@ -189,28 +248,12 @@ void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2*
         I[i + n * i] = 1.0;
     }
     unitary_add(L0, n, Hd, 1.0);
-    const cd* ops = reinterpret_cast<const cd*>(sys.ops.data());
     for (int b = 0; b < nf; ++b) {
         std::vector<cd> D_b(E, cd(0.0, 0.0)), AdA_sum(D, cd(0.0, 0.0));
         for (int al = 0; al < sys.num_ops; ++al) {
-            std::vector<cd> Aw(D, cd(0.0, 0.0));
-            double nrm = 0.0;
-            for (std::size_t k = 0; k < D; ++k)
-                if (sys.p2f[k] == b) {
-                    Aw[k] = ops[static_cast<std::size_t>(al) * D + k];
-                    nrm += std::norm(Aw[k]);
-                }
-            if (nrm == 0.0) continue;
-            std::vector<cd> AdA(D, cd(0.0, 0.0)), Ac(D), AdAT(D);
-            for (int r = 0; r < n; ++r)
-                for (int c = 0; c < n; ++c) {
-                    cd acc(0.0, 0.0);
-                    for (int k = 0; k < n; ++k) acc += std::conj(Aw[k + n * r]) * Aw[k + n * c];
-                    AdA[r + n * c] = acc;
-                }
-            double an = 0.0;
-            for (auto& x : AdA) an += std::norm(x);
-            if (an == 0.0) continue;
+            std::vector<cd> Aw, AdA;
+            if (!bucket_op(sys, b, al, Aw, AdA)) continue;
+            std::vector<cd> Ac(D), AdAT(D);
             for (int r = 0; r < n; ++r)
                 for (int c = 0; c < n; ++c) {
                     Ac[r + n * c] = std::conj(Aw[r + n * c]);
@@ -229,6 +272,90 @@ void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2*
         std::copy(D_b.begin(), D_b.end(), Db.begin() + static_cast<std::ptrdiff_t>(b * E));
         std::copy(U_b.begin(), U_b.end(), Ub.begin() + static_cast<std::ptrdiff_t>(b * E));
     }
+    auto out = [](const std::vector<cd>& v, std::vector<double2>& o) {
+        o.resize(v.size());
+        for (std::size_t k = 0; k < v.size(); ++k) o[k] = make_double2(v[k].real(), v[k].imag());
+    };
+    out(L0, L0out);
+    out(Db, Dbout);
+    out(Ub, Ubout);
+}
+
+void tcl2_maps_grad(const SystemDesc& sys, const double* eps, const std::vector<double2>& GL0v,
+                    const std::vector<double2>& GDv, const std::vector<double2>& GUv, double2* ops_bar, double* eps_bar) {
+    const int n = sys.N, nf = sys.nf;
+    const std::size_t D = static_cast<std::size_t>(n) * n, E = D * D;
+    auto in = [](const double2* p, std::size_t cnt) {
+        std::vector<cd> v(cnt);
+        for (std::size_t k = 0; k < cnt; ++k) v[k] = cd(p[k].x, p[k].y);
+        return v;
+    };
+    if (eps_bar) {
+        std::vector<cd> Hd(D, cd(0.0, 0.0));
+        for (int i = 0; i < n; ++i) Hd[i + n * i] = eps[i];
+        const std::vector<cd> GH = unitary_grad(in(GL0v.data(), E), n, Hd);
+        for (int i = 0; i < n; ++i) eps_bar[i] += GH[i + n * i].real();
+    }
+    if (!ops_bar) return;
+    cd* G = reinterpret_cast<cd*>(ops_bar);
+    std::vector<cd> I(D, cd(0.0, 0.0));
+    for (int i = 0; i < n; ++i) I[i + n * i] = 1.0;
+    for (int b = 0; b < nf; ++b) {
+        const std::vector<cd> GD = in(GDv.data() + b * E, E), GU = in(GUv.data() + b * E, E);
+        // U_b = unitary(Hh), Hh = (S + S^H) / 2, S = sum_alpha A^+ A over the included terms
+        std::vector<cd> S(D, cd(0.0, 0.0));
+        std::vector<std::vector<cd>> Aws, AdAs;
+        std::vector<int> als;
+        for (int al = 0; al < sys.num_ops; ++al) {
+            std::vector<cd> Aw, AdA;
+            if (!bucket_op(sys, b, al, Aw, AdA)) continue;
+            for (std::size_t k = 0; k < D; ++k) S[k] += AdA[k];
+            Aws.push_back(Aw);
+            AdAs.push_back(AdA);
+            als.push_back(al);
+        }
+        if (als.empty()) continue;
+        std::vector<cd> Hh(D);
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < n; ++c) Hh[r + n * c] = 0.5 * (S[r + n * c] + std::conj(S[c + n * r]));
+        const std::vector<cd> GHh = unitary_grad(GU, n, Hh);
+        std::vector<cd> GS(D);
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < n; ++c) GS[r + n * c] = 0.5 * (GHh[r + n * c] + std::conj(GHh[c + n * r]));
+        for (std::size_t a = 0; a < als.size(); ++a) {
+            const std::vector<cd>& Aw = Aws[a];
+            const std::vector<cd>& AdA = AdAs[a];
+            std::vector<cd> Ac(D), AdAT(D);
+            for (int r = 0; r < n; ++r)
+                for (int c = 0; c < n; ++c) {
+                    Ac[r + n * c] = std::conj(Aw[r + n * c]);
+                    AdAT[r + n * c] = AdA[c + n * r];
+                }
+            std::vector<cd> GAc(D, cd(0.0, 0.0)), GAw(D, cd(0.0, 0.0)), GAdA(GS), GAdAT(D, cd(0.0, 0.0));
+            kron_add_grad(GD, n, Ac, Aw, 1.0, &GAc, &GAw);
+            kron_add_grad(GD, n, I, AdA, -0.5, nullptr, &GAdA);
+            kron_add_grad(GD, n, AdAT, I, -0.5, &GAdAT, nullptr);
+            for (int r = 0; r < n; ++r)
+                for (int c = 0; c < n; ++c) GAdA[c + n * r] += GAdAT[r + n * c];
+            // AdA = Aw^H Aw: G(Aw) += Aw (G + G^H)
+            for (int r = 0; r < n; ++r)
+                for (int c = 0; c < n; ++c) {
+                    cd acc(0.0, 0.0);
+                    for (int k = 0; k < n; ++k) acc += Aw[r + n * k] * (GAdA[k + n * c] + std::conj(GAdA[c + n * k]));
+                    GAw[r + n * c] += acc + std::conj(GAc[r + n * c]);
+                }
+            for (std::size_t k = 0; k < D; ++k)
+                if (sys.p2f[k] == b) G[static_cast<std::size_t>(als[a]) * D + k] += GAw[k];
+        }
+    }
+}
+
+void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2* gamma, std::size_t Nt,
+                        const std::vector<uint32_t>& tidx, double2* out, cudaStream_t st) {
+    const int nf = sys.nf;
+    const std::size_t E = static_cast<std::size_t>(sys.N) * sys.N * sys.N * sys.N;
+    std::vector<double2> L0, Db, Ub;
+    tcl2_maps(sys, eps, L0, Db, Ub);
     // device staging of the (small) maps: allocated for the call, released after it
     const std::size_t bytes = (E + 2 * nf * E) * sizeof(double2) + tidx.size() * sizeof(uint32_t);
     void* d = nullptr;
@@ -247,7 +374,7 @@ void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2*
             const unsigned gy = static_cast<unsigned>(std::min<std::size_t>(65535, tidx.size() - o0));
             k_tcl2_series<<<dim3(gx, gy), 128, 0, st>>>(gamma, Nt, nf, dt + o0, gy, dL0, dD, dU,
                                                          static_cast<uint32_t>(E), out + o0 * E);
-            cuda_check(cudaGetLastError(), "k_tcl2_series");
+            launched("k_tcl2_series");
         }
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl2)");
     } catch (...) {
@@ -272,10 +399,10 @@ void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::v
         cuda_check(cudaMemcpyAsync(dom, omegas.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st), "omegas");
         k_gamma_reduce<<<dim3(static_cast<unsigned>(nchunks), static_cast<unsigned>(nb)), GT_THREADS, 0, st>>>(
             C, N, dt, dom, part, nchunks);
-        cuda_check(cudaGetLastError(), "k_gamma_reduce");
+        launched("k_gamma_reduce");
         k_gamma_scan<<<dim3(static_cast<unsigned>(nchunks), static_cast<unsigned>(nb)), GT_THREADS, 0, st>>>(
             C, N, dt, dom, part, nchunks, G);
-        cuda_check(cudaGetLastError(), "k_gamma_scan");
+        launched("k_gamma_scan");
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(gamma)");
     } catch (...) {
         cudaStreamSynchronize(st);

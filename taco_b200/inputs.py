@@ -43,6 +43,8 @@ class System:
                     reps.append(x)
                     pairs.append([(m, n)])
         order = np.argsort(np.array(reps), kind="stable")
+        # first-seen (m, n) pair of each bucket: omega_b = eps_m - eps_n (the representative)
+        self.rep_pairs = [pairs[ob][0] for ob in order]
         self.N = d
         self.eps = w
         self.U = U
