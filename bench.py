@@ -51,6 +51,13 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--grad-instances", type=int, default=64, help="differentiation form (0: skip)")
+    p.add_argument("--grad-N", type=int, default=1 << 16)
+    p.add_argument("--grad-dt", type=float, default=1e-3)
+    p.add_argument("--grad-steps", type=int, default=4096)
+    p.add_argument("--c3-dims", default="4,6", help="precision form on random systems (empty: skip)")
+    p.add_argument("--c3-N", type=int, default=1 << 18)
+    p.add_argument("--c3-stride", type=int, default=4)
     return p.parse_args()
 
 
@@ -196,6 +203,131 @@ def timed(torch, fn, reps, warmup=1):
     e1.record()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def gue_system(d, rng):
+    """Seeded GUE Hamiltonian (H_ii ~ N(0, 1/d), off-diagonal real and imaginary parts
+    N(0, 1/(2d))) and a random Hermitian coupling of unit spectral norm."""
+    from taco_b200.inputs import System
+    X = rng.normal(0.0, np.sqrt(1.0 / (2 * d)), (d, d)) + 1j * rng.normal(0.0, np.sqrt(1.0 / (2 * d)), (d, d))
+    H = np.triu(X, 1)
+    H = H + H.conj().T + np.diag(rng.normal(0.0, np.sqrt(1.0 / d), d))
+    Y = rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
+    A = np.triu(Y, 1)
+    A = A + A.conj().T + np.diag(rng.normal(size=d))
+    A = A / np.linalg.norm(A, 2)
+    return System(H, [A]), A
+
+
+def precision_random(args, d, cpu_leg):
+    """Precision form on a random system: GUE H (dimension d), random unit-norm A, Ohmic
+    (alpha 0.1, wc 5) + Drude-Lorentz (lambda 0.05, gamma 2) bath at beta 0.5, N grid
+    points, dt 1e-3, tidx 0:stride:N-1.  L4 in FP32 and FP64 on the device; <A(t)> by RK4
+    under L2 + L4 over the sampled times; on the CPU leg, the oracle on the first 2001 steps."""
+    import torch
+    import taco_b200 as tb
+    from taco_b200 import adjoint as adj
+    rng = np.random.default_rng(args.seed + 300 + d)
+    s, A = gue_system(d, rng)
+    N, dt = args.c3_N, 1e-3
+    tidx = np.arange(0, N, args.c3_stride, dtype=np.uint32)
+    T = tidx.size
+    C = adj.bcf_device([dict(model=1, alpha=0.1, omega_c=5.0, lam=0.05, gam=2.0, beta=0.5, N=N, dt=dt)], N + 1)[0]
+    G = tb.gamma_trapz_device(C, dt, s.omegas)
+    out = {"d": d, "nf": int(s.nf), "N": N, "T": int(T), "triples": int(s.nf) ** 3}
+    res = {}
+    for prec in ("fp32", "fp64"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L4 = tb.build_TCL4_generator_batch(s, G, dt, tidx, precision=prec)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        res[prec] = L4
+        out[prec] = {"value": T / sec, "unit": "builds/s", "seconds": round(sec, 3)}
+    L64 = res["fp64"]
+    err = float(torch.linalg.vector_norm(res["fp32"].to(torch.complex128) - L64) / torch.linalg.vector_norm(L64))
+    out["l4_fp32_rel_err_vs_fp64"] = err
+    # <A(t)> under L2 + L4 on the sampled times (RK4 step stride * dt), FP64 state
+    L2 = tb.tcl2_generator_series(s, G, tidx)
+    U = s.U
+    rho0 = np.zeros((d, d), np.complex128)
+    rho0[0, 0] = 1.0
+    r0 = torch.from_numpy((U.conj().T @ rho0 @ U).reshape(-1, order="F")).cuda()
+    ob = torch.from_numpy((U.conj().T @ A @ U).T.reshape(-1, order="F")).cuda()
+    trajs = {}
+    for prec in ("fp32", "fp64"):
+        _, _, o = tb.propagate_rk4_dense(L2, r0, dt * args.c3_stride, L_add=res[prec].to(torch.complex128),
+                                         sample_every=16, obs=ob)
+        trajs[prec] = o.real.cpu().numpy()
+    out["expect_A_fp32_rel_err_vs_fp64"] = float(np.linalg.norm(trajs["fp32"] - trajs["fp64"])
+                                                 / np.linalg.norm(trajs["fp64"]))
+    if cpu_leg:
+        import oracle
+        k = int(np.searchsorted(tidx, 2001))
+        Gh = np.ascontiguousarray(G[:, :2001].cpu().numpy())
+        p2f = np.ascontiguousarray(s.pair_to_freq.T, np.int32)
+        ops = np.ascontiguousarray(np.stack([Ae.T for Ae in s.A_eig]))
+        t0 = time.perf_counter()
+        ref = oracle.tcl4_build_batch(s.N, s.nf, s.omegas, s.mirror, p2f, ops, Gh, dt, tidx=tidx[:k])
+        g64 = L64[:k].cpu().numpy()
+        g32 = res["fp32"][:k].cpu().numpy()
+        out["oracle_window"] = {"tidx": f"0:{args.c3_stride}:2000", "fp64_rel_err": float(np.linalg.norm(g64 - ref) / np.linalg.norm(ref)),
+                                "fp32_rel_err": float(np.linalg.norm(g32 - ref) / np.linalg.norm(ref)),
+                                "oracle_seconds": round(time.perf_counter() - t0, 2)}
+    del res, L64, L2
+    torch.cuda.empty_cache()
+    return out
+
+
+def differentiation(args, rank, world, cpu_leg):
+    """The differentiation form: loss = mean_t (<sz(t)> - target)^2 per spin-boson instance,
+    gradient in (eps, Delta, alpha, wc, beta) by the hand-written adjoint (FP64 and with the
+    FP32 L4 build), timed end to end; on the CPU leg, central differences (h = 1e-6) of the
+    FP64 oracle chain for one instance."""
+    import torch
+    from taco_b200 import adjoint as adj
+    B = args.grad_instances
+    rng = np.random.default_rng(args.seed + 77 + 1000 * rank)
+    params = np.stack([rng.uniform(0.5, 2.0, B), rng.uniform(0.5, 2.0, B),
+                       np.exp(rng.uniform(np.log(0.01), np.log(0.2), B)), rng.uniform(1.0, 20.0, B),
+                       np.exp(rng.uniform(np.log(0.2), np.log(5.0), B))], axis=1)
+    out = {"instances_per_gpu": B, "N": args.grad_N, "dt": args.grad_dt, "rk4_steps": args.grad_steps,
+           "loss": "mean over 4097 samples of (<sz(t)> - target(t))^2, seeded damped-cosine target"}
+    t = np.arange(args.grad_steps + 1) * args.grad_dt
+    tgt = (0.6 * np.cos(rng.uniform(0.5, 2.0, (B, 1)) * t[None, :]) * np.exp(-0.1 * t[None, :]))
+    for prec in ("fp64", "fp32"):
+        cfg = adj.SpinBosonConfig(N=args.grad_N, dt=args.grad_dt, steps=args.grad_steps, precision=prec)
+        adj.mse_loss_and_grad(params, tgt, cfg)  # warm-up (workspaces, tables)
+        ph = adj.Phases()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss, grads = adj.mse_loss_and_grad(params, tgt, cfg, phases=ph)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        out[prec] = {"value": world * B / (ms / 1e3), "unit": "loss+gradient evaluations/s", "ms_per_step": ms,
+                     "phases_ms": {k: round(v, 3) for k, v in ph.ms.items()}}
+        if prec == "fp64":
+            g64 = grads
+        else:
+            out["fp32_grad_rel_diff_vs_fp64"] = float(np.linalg.norm(grads - g64) / np.linalg.norm(g64))
+    if cpu_leg:
+        import oracle
+        h = 1e-6
+        fd = np.zeros(5)
+        t0 = time.perf_counter()
+        for k in range(5):
+            pp, pm = params[0].copy(), params[0].copy()
+            pp[k] += h
+            pm[k] -= h
+            lp = np.mean((oracle.spin_boson_trajectory(pp, args.grad_N, args.grad_dt, args.grad_steps) - tgt[0]) ** 2)
+            lm = np.mean((oracle.spin_boson_trajectory(pm, args.grad_N, args.grad_dt, args.grad_steps) - tgt[0]) ** 2)
+            fd[k] = (lp - lm) / (2 * h)
+        out["oracle_fd_check"] = {"instance": 0, "params": params[0].tolist(), "grad": g64[0].tolist(),
+                                  "fd": fd.tolist(),
+                                  "rel_err": float(np.linalg.norm(g64[0] - fd) / np.linalg.norm(fd)),
+                                  "max_component_rel_err": float(np.max(np.abs(g64[0] - fd) / np.abs(fd))),
+                                  "oracle_seconds": round(time.perf_counter() - t0, 2)}
+    return out
 
 
 def main():
@@ -364,6 +496,11 @@ def main():
         fp64_parity = {"vs_oracle_convolution": re(g64, L4o), "vs_oracle_direct": re(g64, L4d),
                        "oracle_convolution_vs_direct": re(L4o, L4d), "fp32_vs_oracle_direct": re(g32, L4d)}
 
+    grad = differentiation(args, rank, world, rank == 0 and world == 1 and not args.no_cpu_baseline) \
+        if args.grad_instances > 0 else None
+    c3 = [precision_random(args, int(d), rank == 0 and world == 1 and not args.no_cpu_baseline)
+          for d in args.c3_dims.split(",") if d.strip()]
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
@@ -389,6 +526,8 @@ def main():
             "e2e": {"value": e2e_value, "unit": "builds/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms, "max_abs_diff_vs_device_run": err_e2e},
             "roofline": roofline, "kernels": kernels,
+            "differentiation": grad,
+            "precision_random": c3,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk.summary(),

@@ -223,6 +223,10 @@ int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t*
  * two in [8, 8192]), bytes of Z/W scratch per chunk of triples (sized to stay in L2), and
  * the largest number of output rows for which the inverse column pass is a pruned direct
  * DFT.  Unset lengths use the defaults (4096, 2048, 48 MiB, 16). */
+/* Transient device memory one group of a build may use (0, the default: 45% of the free
+ * memory at the call, at most 64 GiB).  Instances that need more are built in slices of
+ * their frequency triples (same results, more passes over the output). */
+int taco_set_work_budget(size_t bytes);
 int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows);
 int taco_get_tuning(int log2_nfft, int precision, int* col_tile, int* row_tile, size_t* chunk_bytes,
                     int* inv_dft_rows);

@@ -263,3 +263,27 @@ def rk4_propagate_const(L, r0, t0, tf, dt):
     _check(lib().oracle_rk4_propagate_const(_p(_c128(L.T)), ct.c_int(L.shape[0]), ct.c_double(t0),
                                             ct.c_double(tf), ct.c_double(dt), _p(r)))
     return r
+
+
+def spin_boson_trajectory(params, N, dt, steps, rho0=None, observable=None, sample_every=1):
+    """<O(t)> (real) of the FP64 chain for one spin boson (eps, Delta, alpha, wc, beta):
+    H = eps/2 sz + Delta/2 sx, A = sz, Ohmic bath by bcf_fft, trapezoid Gamma, L4 by the
+    convolution method, L2 by tcl2_total, RK4 under L2 + L4 from rho0 (lab basis, |0><0|
+    by default), O = sz by default (examples/TCL4_spin_boson_example.cpp:196-394)."""
+    sx = np.array([[0, 1], [1, 0]], np.complex128)
+    sz = np.array([[1, 0], [0, -1]], np.complex128)
+    rho0 = np.array([[1, 0], [0, 0]], np.complex128) if rho0 is None else np.asarray(rho0, np.complex128)
+    O = sz if observable is None else np.asarray(observable, np.complex128)
+    eps, delta, alpha, wc, beta = params
+    T = steps + 1
+    osys = System(0.5 * eps * sz + 0.5 * delta * sx, [sz])
+    _, C = bcf_fft(N, dt, J_OHMIC, [alpha, wc], beta)
+    G = gamma_trapz(C[:T], dt, osys.omegas)
+    L4 = tcl4_build_batch(osys.N, osys.nf, osys.omegas, osys.mirror, osys.p2f_colmajor(), osys.ops_colmajor(),
+                          G, dt, tidx=np.arange(T))
+    L2 = np.stack([tcl2_total(osys, G[:, t])[0] for t in range(T)])
+    U = osys.U
+    r0 = (U.conj().T @ rho0 @ U).reshape(-1, order="F")
+    ov = (U.conj().T @ O @ U).T.reshape(-1, order="F")
+    _, samp = rk4_propagate(L2 + L4, r0, dt, sample_every=sample_every)
+    return np.real(samp @ ov)

@@ -40,7 +40,7 @@ __all__ = [
     "build_TCL4_generator", "build_TCL4_generator_batch", "build_correction_series", "build_instances",
     "propagate_rk4_dense", "l4_coefficients", "Tcl4Plan", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
     "version", "device_count", "kernel_launches", "profile", "tcl2_generator_series", "gamma_trapz_device",
-    "propagate_tcl", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
+    "propagate_tcl", "set_work_budget", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
 ]
 
 
@@ -87,6 +87,12 @@ class profile:
             _capi.check(L.taco_profile_get(k, ct.byref(name), ct.byref(n), ct.byref(ms), None))
             self.entries[name.value.decode()] = (int(n.value), float(ms.value))
         return False
+
+
+def set_work_budget(nbytes: int) -> None:
+    """Transient device memory of one group of a build (0: automatic).  Larger instances
+    are built in slices of their frequency triples."""
+    _capi.check(_capi.lib().taco_set_work_budget(int(nbytes)))
 
 
 def set_fcr_fft_pad_factor(factor: int) -> None:

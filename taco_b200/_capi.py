@@ -38,7 +38,7 @@ EXPORTED = [
     "taco_tcl4_build_batch_noalloc", "taco_tcl2_generator_series", "taco_gamma_trapz", "taco_propagate_tcl",
     "taco_build_mikx", "taco_assemble_liouvillian", "taco_gw_to_liouvillian",
     "taco_bcf_fft", "taco_rk4_forward_checkpointed", "taco_rk4_adjoint", "taco_tcl4_adjoint",
-    "taco_tcl2_adjoint", "taco_inner_re",
+    "taco_tcl2_adjoint", "taco_inner_re", "taco_set_work_budget",
 ]
 
 
@@ -164,6 +164,7 @@ def lib():
                                                 ct.c_int, ct.c_int, ct.c_size_t, ct.c_int, ct.c_void_p, ct.c_int,
                                                 ct.c_void_p]
         L.taco_gw_to_liouvillian.argtypes = [ct.c_void_p, ct.c_int, ct.c_size_t, ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.taco_set_work_budget.argtypes = [ct.c_size_t]
         L.taco_bcf_fft.argtypes = [ct.POINTER(BcfRequest), ct.c_size_t, ct.c_int, ct.c_void_p]
         L.taco_rk4_forward_checkpointed.argtypes = [ct.POINTER(Rk4GradJob), ct.c_size_t, ct.c_size_t, ct.c_void_p]
         L.taco_rk4_adjoint.argtypes = [ct.POINTER(Rk4GradJob), ct.c_size_t, ct.c_size_t, ct.c_void_p]

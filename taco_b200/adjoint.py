@@ -26,8 +26,10 @@ have no counterpart there.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as ct
 import math
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -260,6 +262,26 @@ class SpinBosonConfig:
         return (self.steps + self.sample_every - 1) // self.sample_every + 1
 
 
+class Phases:
+    """Host wall time per phase (each phase ends with a device synchronisation)."""
+
+    def __init__(self):
+        self.ms = {}
+
+    @contextlib.contextmanager
+    def __call__(self, name):
+        torch = _torch()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        yield
+        torch.cuda.synchronize()
+        self.ms[name] = self.ms.get(name, 0.0) + (time.perf_counter() - t0) * 1e3
+
+
+def _phase(phases, name):
+    return phases(name) if phases is not None else contextlib.nullcontext()
+
+
 def _systems(params, cfg):
     out = []
     for eps, delta, *_ in params:
@@ -268,7 +290,7 @@ def _systems(params, cfg):
     return out
 
 
-def spin_boson_forward(params, cfg: SpinBosonConfig, device="cuda"):
+def spin_boson_forward(params, cfg: SpinBosonConfig, device="cuda", phases=None):
     """<O(t)> [B, n_samples] (real, torch float64 on the device) and the saved state."""
     from . import build_instances, gamma_trapz_device, tcl2_generator_series
     torch = _torch()
@@ -277,33 +299,39 @@ def spin_boson_forward(params, cfg: SpinBosonConfig, device="cuda"):
     T = cfg.steps + 1
     if T > cfg.N + 1:
         raise ValueError("steps must not exceed the bath grid N")
-    systems = _systems(params, cfg)
+    with _phase(phases, "system"):
+        systems = _systems(params, cfg)
     nf = systems[0].nf
     if any(s.nf != nf for s in systems):
         raise ValueError("all instances must share the Bohr-bucket count")
     reqs = [dict(model=0, which=0, alpha=a, omega_c=wc, beta=be, N=cfg.N, dt=cfg.dt)
             for (_, _, a, wc, be) in params]
-    C = bcf_device(reqs, T, device)
-    gammas = [gamma_trapz_device(C[b], cfg.dt, systems[b].omegas) for b in range(B)]
+    with _phase(phases, "bcf"):
+        C = bcf_device(reqs, T, device)
+    with _phase(phases, "gamma"):
+        gammas = [gamma_trapz_device(C[b], cfg.dt, systems[b].omegas) for b in range(B)]
     N2 = systems[0].N ** 2
     E = N2 * N2
     cdt = torch.complex128 if cfg.precision == "fp64" else torch.complex64
-    outs = [torch.empty((T, E), dtype=cdt, device=device) for _ in range(B)]
-    build_instances([(systems[b], gammas[b], cfg.dt, np.arange(T)) for b in range(B)], precision=cfg.precision,
-                    outs=outs)
-    L4 = torch.stack([o.to(torch.complex128) for o in outs])
-    L2 = torch.stack([tcl2_generator_series(systems[b], gammas[b]).transpose(1, 2).reshape(T, E)
-                      for b in range(B)]).contiguous()
-    r0 = np.stack([(s.U.conj().T @ cfg.rho0 @ s.U).reshape(-1, order="F") for s in systems])
-    ov = np.stack([(s.U.conj().T @ cfg.observable @ s.U).T.reshape(-1, order="F") for s in systems])
-    r0_d = torch.from_numpy(r0).to(device)
-    ov_d = torch.from_numpy(ov).to(device)
-    obs, _, ckpt = rk4_forward_checkpointed(L2, L4, r0_d, ov_d, cfg.dt, cfg.sample_every, cfg.every)
+    with _phase(phases, "l4"):
+        outs = [torch.empty((T, E), dtype=cdt, device=device) for _ in range(B)]
+        build_instances([(systems[b], gammas[b], cfg.dt, np.arange(T)) for b in range(B)], precision=cfg.precision,
+                        outs=outs)
+        L4 = torch.stack([o.to(torch.complex128) for o in outs])
+    with _phase(phases, "l2"):
+        L2 = torch.stack([tcl2_generator_series(systems[b], gammas[b]).transpose(1, 2).reshape(T, E)
+                          for b in range(B)]).contiguous()
+    with _phase(phases, "rk4"):
+        r0 = np.stack([(s.U.conj().T @ cfg.rho0 @ s.U).reshape(-1, order="F") for s in systems])
+        ov = np.stack([(s.U.conj().T @ cfg.observable @ s.U).T.reshape(-1, order="F") for s in systems])
+        r0_d = torch.from_numpy(r0).to(device)
+        ov_d = torch.from_numpy(ov).to(device)
+        obs, _, ckpt = rk4_forward_checkpointed(L2, L4, r0_d, ov_d, cfg.dt, cfg.sample_every, cfg.every)
     state = dict(params=params, systems=systems, C=C, gammas=gammas, L2=L2, L4=L4, r0=r0_d, ov=ov_d, ckpt=ckpt)
     return obs.real.contiguous(), state
 
 
-def spin_boson_backward(state, g_obs, cfg: SpinBosonConfig):
+def spin_boson_backward(state, g_obs, cfg: SpinBosonConfig, phases=None):
     """d(loss)/d(eps, Delta, alpha, wc, beta) [B, 5] from g_obs = d(loss)/d<O(t)> [B, n_samples]."""
     from . import compute_triple_kernels, gamma_trapz_device
     torch = _torch()
@@ -313,28 +341,33 @@ def spin_boson_backward(state, g_obs, cfg: SpinBosonConfig):
     T = cfg.steps + 1
     dt = cfg.dt
     obs_bar = g_obs.to(device=dev, dtype=torch.float64).to(torch.complex128)
-    L_bar, r0_bar, ov_bar = rk4_adjoint(state["L2"], state["L4"], state["r0"], state["ov"], dt, cfg.sample_every,
-                                        cfg.every, state["ckpt"], obs_bar)
+    with _phase(phases, "rk4_adjoint"):
+        L_bar, r0_bar, ov_bar = rk4_adjoint(state["L2"], state["L4"], state["r0"], state["ov"], dt,
+                                            cfg.sample_every, cfg.every, state["ckpt"], obs_bar)
     gammas = state["gammas"]
-    sources = [compute_triple_kernels(systems[b], gammas[b], dt) for b in range(B)]
-    gbar, wbar, ops4 = tcl4_adjoint(systems, gammas, dt, L_bar, sources, want_ops=True)
-    gbar, ops2, eps_bar = tcl2_adjoint(systems, gammas, L_bar, gbar)
+    with _phase(phases, "fcr_sources"):
+        sources = [compute_triple_kernels(systems[b], gammas[b], dt) for b in range(B)]
+    with _phase(phases, "l4_adjoint"):
+        gbar, wbar, ops4 = tcl4_adjoint(systems, gammas, dt, L_bar, sources, want_ops=True)
+    with _phase(phases, "l2_adjoint"):
+        gbar, ops2, eps_bar = tcl2_adjoint(systems, gammas, L_bar, gbar)
     # tangents of Gamma: bath parameters (BCF derivative spectra) and the bucket frequency
     reqs = []
     for (_, _, a, wc, be) in params:
         for which in (1, 2, 3):
             reqs.append(dict(model=0, which=which, alpha=a, omega_c=wc, beta=be, N=cfg.N, dt=dt))
-    dC = bcf_device(reqs, T, dev).view(B, 3, T)
-    tau = torch.arange(T, dtype=torch.float64, device=dev) * dt
-    pairs = []
-    for b in range(B):
-        om = systems[b].omegas
-        for k in range(3):
-            pairs.append((gbar[b], gamma_trapz_device(dC[b, k].contiguous(), dt, om)))
-        gw = gamma_trapz_device((1j * tau * state["C"][b]).contiguous(), dt, om)
-        for j in range(len(om)):
-            pairs.append((gbar[b][j].contiguous(), gw[j].contiguous()))
-    dots = inner_re(pairs, dev)
+    with _phase(phases, "bath_tangents"):
+        dC = bcf_device(reqs, T, dev).view(B, 3, T)
+        tau = torch.arange(T, dtype=torch.float64, device=dev) * dt
+        pairs = []
+        for b in range(B):
+            om = systems[b].omegas
+            for k in range(3):
+                pairs.append((gbar[b], gamma_trapz_device(dC[b, k].contiguous(), dt, om)))
+            gw = gamma_trapz_device((1j * tau * state["C"][b]).contiguous(), dt, om)
+            for j in range(len(om)):
+                pairs.append((gbar[b][j].contiguous(), gw[j].contiguous()))
+        dots = inner_re(pairs, dev)
     grads = np.zeros((B, 5), np.float64)
     r0b = r0_bar.cpu().numpy()
     ovb = ov_bar.cpu().numpy()
@@ -390,14 +423,14 @@ class SpinBosonTCL4:
         return cls._fn.apply(params, cfg)
 
 
-def mse_loss_and_grad(params, target, cfg: SpinBosonConfig, device="cuda"):
+def mse_loss_and_grad(params, target, cfg: SpinBosonConfig, device="cuda", phases=None):
     """Per-instance loss mean_t (<sz(t)> - target)^2 and its gradient [B, 5] (numpy)."""
     torch = _torch()
-    obs, state = spin_boson_forward(params, cfg, device)
+    obs, state = spin_boson_forward(params, cfg, device, phases)
     tgt = torch.as_tensor(np.asarray(target, np.float64), device=obs.device)
     diff = obs - tgt
     ns = obs.shape[1]
     loss = (diff * diff).mean(dim=1)
     g = 2.0 * diff / ns
-    grads = spin_boson_backward(state, g, cfg)
+    grads = spin_boson_backward(state, g, cfg, phases)
     return loss.cpu().numpy(), grads

@@ -576,6 +576,10 @@ int taco_gw_to_liouvillian(const taco_c128* GW, int N, size_t T, taco_c128* L4, 
     });
 }
 
+int taco_set_work_budget(size_t bytes) {
+    return guarded([&] { taco::set_work_budget(bytes); });
+}
+
 int taco_bcf_fft(const taco_bcf_request* reqs, size_t n, int flags, void* stream) {
     return guarded([&] {
         require_device();

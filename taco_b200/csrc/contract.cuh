@@ -12,6 +12,33 @@
 
 namespace taco {
 
+// Accumulator of one L4 entry: plain in FP64; compensated (Kahan, separately for the
+// real and imaginary parts) in the FP32 form, where a sequential FP32 sum of the ~10^3
+// terms per entry of d >= 6 systems would lose ~1e-6 relative accuracy.
+template <class C>
+struct EntryAcc;
+
+template <>
+struct EntryAcc<double2> {
+    double2 s = make_double2(0.0, 0.0);
+    __device__ __forceinline__ void add(double2 x) { s = cadd(s, x); }
+    __device__ __forceinline__ double2 get() const { return s; }
+};
+
+template <>
+struct EntryAcc<float2> {
+    float2 s = make_float2(0.f, 0.f), c = make_float2(0.f, 0.f);
+    __device__ __forceinline__ void add(float2 x) {
+        const float yx = x.x - c.x, yy = x.y - c.y;
+        const float tx = s.x + yx, ty = s.y + yy;
+        c.x = (tx - s.x) - yx;
+        c.y = (ty - s.y) - yy;
+        s.x = tx;
+        s.y = ty;
+    }
+    __device__ __forceinline__ float2 get() const { return s; }
+};
+
 struct ContractJob {
     const int32_t* rowptr;  // [E + 1]
     const uint32_t* src;    // [nnz] source | conj << 31
@@ -20,6 +47,7 @@ struct ContractJob {
     const uint32_t* out_u;  // [T] unique-time position of each output
     void* out;              // [T][E] working complex type
     uint32_t T, U, E;
+    uint32_t accumulate;    // 1: add into out (later slices of a sliced instance)
 };
 
 template <class R>
@@ -38,21 +66,22 @@ __global__ void k_contract(const ContractJob* __restrict__ jobs, int OT) {
         const uint32_t ol = idx % OT, e = idx / OT;
         if (ol >= ot) continue;
         const uint32_t u = __ldg(&job.out_u[o0 + ol]);
-        C acc = C{0, 0};
+        EntryAcc<C> acc;
         const int32_t b = __ldg(&job.rowptr[e]), end = __ldg(&job.rowptr[e + 1]);
         for (int32_t k = b; k < end; ++k) {
             const uint32_t sk = __ldg(&job.src[k]);
             const C w = coef[k];
             C x = v[static_cast<size_t>(sk & 0x7fffffffu) * job.U + u];
             if (sk & 0x80000000u) x.y = -x.y;
-            acc = cadd(acc, cmul(w, x));
+            acc.add(cmul(w, x));
         }
-        res[ol * job.E + e] = acc;
+        res[ol * job.E + e] = acc.get();
     }
     __syncthreads();
     C* out = static_cast<C*>(job.out) + static_cast<size_t>(o0) * job.E;
     const uint32_t total = ot * job.E;
-    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) out[idx] = res[idx];
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x)
+        out[idx] = job.accumulate ? cadd(out[idx], res[idx]) : res[idx];
 }
 
 // Shared-memory variant: the CTA stages v[s][u(o)] for its OT outputs and the CSR table,
@@ -88,20 +117,21 @@ __global__ void k_contract_smem(const ContractJob* __restrict__ jobs, int OT, in
     const uint32_t work = job.E * OT;
     for (uint32_t idx = threadIdx.x; idx < work; idx += blockDim.x) {
         const uint32_t ol = idx % OT, e = idx / OT;
-        C acc = C{0, 0};
+        EntryAcc<C> acc;
         const int32_t b = rp[e], end = rp[e + 1];
         for (int32_t k = b; k < end; ++k) {
             const uint32_t sk = sr[k];
             C x = vs[(sk & 0x7fffffffu) * OT + ol];
             if (sk & 0x80000000u) x.y = -x.y;
-            acc = cadd(acc, cmul(cf[k], x));
+            acc.add(cmul(cf[k], x));
         }
-        res[ol * job.E + e] = acc;
+        res[ol * job.E + e] = acc.get();
     }
     __syncthreads();
     C* out = static_cast<C*>(job.out) + static_cast<size_t>(o0) * job.E;
     const uint32_t total = ot * job.E;
-    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) out[idx] = res[idx];
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x)
+        out[idx] = job.accumulate ? cadd(out[idx], res[idx]) : res[idx];
 }
 
 // Output-per-thread variant: thread o evaluates every L4 entry at output time o, walking
@@ -137,15 +167,15 @@ __global__ void __launch_bounds__(CONTRACT_ROW_THREADS) k_contract_rows(const Co
         const uint32_t u = __ldg(&job.out_u[o]);
         for (uint32_t e = 0; e < E; ++e) {
             if (l4_partner(e, N) < e) continue;
-            C acc = C{0, 0};
+            EntryAcc<C> acc;
             const int32_t b = __ldg(&job.rowptr[e]), end = __ldg(&job.rowptr[e + 1]);
             for (int32_t k = b; k < end; ++k) {
                 const uint32_t sk = __ldg(&job.src[k]);
                 C x = v[static_cast<size_t>(sk & 0x7fffffffu) * job.U + u];
                 if (sk & 0x80000000u) x.y = -x.y;
-                acc = cadd(acc, cmul(coef[k], x));
+                acc.add(cmul(coef[k], x));
             }
-            res[threadIdx.x * ld + e] = acc;
+            res[threadIdx.x * ld + e] = acc.get();
         }
         for (uint32_t e = 0; e < E; ++e) {
             const uint32_t p = l4_partner(e, N);
@@ -157,7 +187,53 @@ __global__ void __launch_bounds__(CONTRACT_ROW_THREADS) k_contract_rows(const Co
     const uint32_t total = ot * E;
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
         const uint32_t ol = idx / E, e = idx - ol * E;
-        out[idx] = res[ol * ld + e];
+        out[idx] = job.accumulate ? cadd(out[idx], res[ol * ld + e]) : res[ol * ld + e];
+    }
+}
+
+// Tiled variant for large L4 matrices: a CTA owns 32 consecutive entries x 32
+// consecutive output times; each warp walks the CSR rows of some of its entries with
+// warp-uniform (broadcast) coefficient loads while its lanes gather 32 consecutive times
+// of the same source (one coalesced line per source), and the tile is written through
+// shared memory as 32 contiguous entries per output time.
+constexpr int CONTRACT_TILE = 32;
+constexpr int CONTRACT_TILE_THREADS = 256;
+
+template <class R>
+__global__ void __launch_bounds__(CONTRACT_TILE_THREADS) k_contract_tiles(const ContractJob* __restrict__ jobs) {
+    using C = cplx_t<R>;
+    __shared__ C res[CONTRACT_TILE][CONTRACT_TILE + 1];  // [time][entry]
+    const ContractJob job = jobs[blockIdx.z];
+    const uint32_t o0 = blockIdx.x * CONTRACT_TILE, e0 = blockIdx.y * CONTRACT_TILE;
+    if (o0 >= job.T || e0 >= job.E) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t o = o0 + lane;
+    const uint32_t u = o < job.T ? __ldg(&job.out_u[o]) : 0u;
+    const C* coef = static_cast<const C*>(job.coef);
+    const C* v = static_cast<const C*>(job.v);
+    for (int r = warp; r < CONTRACT_TILE; r += CONTRACT_TILE_THREADS / 32) {
+        const uint32_t e = e0 + r;
+        EntryAcc<C> acc;
+        if (e < job.E) {
+            const int32_t b = __ldg(&job.rowptr[e]), end = __ldg(&job.rowptr[e + 1]);
+            for (int32_t k = b; k < end; ++k) {
+                const uint32_t sk = __ldg(&job.src[k]);
+                const C w = coef[k];
+                C x = v[static_cast<size_t>(sk & 0x7fffffffu) * job.U + u];
+                if (sk & 0x80000000u) x.y = -x.y;
+                acc.add(cmul(w, x));
+            }
+        }
+        res[lane][r] = acc.get();
+    }
+    __syncthreads();
+    C* out = static_cast<C*>(job.out);
+    for (int idx = threadIdx.x; idx < CONTRACT_TILE * CONTRACT_TILE; idx += CONTRACT_TILE_THREADS) {
+        const int ol = idx / CONTRACT_TILE, el = idx % CONTRACT_TILE;
+        const uint32_t oo = o0 + ol, e = e0 + el;
+        if (oo >= job.T || e >= job.E) continue;
+        C* p = out + static_cast<size_t>(oo) * job.E + e;
+        *p = job.accumulate ? cadd(*p, res[ol][el]) : res[ol][el];
     }
 }
 

@@ -101,7 +101,8 @@ struct PlanTables {
 struct Workspace {
     int device = -1;
     cudaStream_t stream = nullptr;
-    DeviceBuffer arena;
+    DeviceBuffer arena;  // metadata of the running group
+    DeviceBuffer work;   // transient arrays of the running group
     PinnedBuffer staging;
     std::map<std::pair<int, int>, std::unique_ptr<PlanTables>> plans;  // (L, fp32)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -265,9 +266,7 @@ int cluster_lm_for(int L, bool fp32, const Tuning& t) {
 
 template <class K>
 void set_smem(K kernel, std::size_t bytes) {
-    if (bytes > 48 * 1024)
-        cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
-                   "cudaFuncSetAttribute(smem)");
+    raise_smem_limit(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 struct Geometry {
@@ -395,134 +394,235 @@ void derive_meta(const Tcl4Instance& in, const BuildOptions& opt, InstMeta& m, b
 }
 
 struct TripleRef {
-    int inst;
+    int unit;
     int tri;  // (i*nf + j)*nf + k
 };
 
-// One group (instances with equal FFT length): lays out `mem`, stages the small
-// metadata and the host inputs (stream-ordered on `st`), and returns the closure that
-// enqueues the group's kernels (and the D2H copies of host outputs) on a stream.
-// `fcr_out` (non-null) writes the F/C/R series (FP64) into caller buffers instead of
-// running the contraction.
+// A slice of one instance's triples, [lo, hi) of the nf^3, processed by one group.  The
+// contraction uses the coefficients of the slice's sources only (local source index
+// kind * (hi - lo) + (tri - lo)); every slice after an instance's first adds into its
+// output, so an instance too large for one pass streams through device memory slice
+// by slice.
+struct WorkUnit {
+    Tcl4Instance* in = nullptr;
+    InstMeta* meta = nullptr;
+    int lo = 0, hi = 0;
+    bool accumulate = false;
+    const CoefTable* coef = nullptr;
+    std::shared_ptr<CoefTable> own;
+    int nsub() const { return hi - lo; }
+};
+
+// Coefficients of the sources of triples [lo, hi), re-indexed to the slice.
+std::shared_ptr<CoefTable> slice_table(const CoefTable& full, int lo, int hi) {
+    auto t = std::make_shared<CoefTable>();
+    const uint32_t nf3 = static_cast<uint32_t>(full.nf) * full.nf * full.nf;
+    const uint32_t nsub = static_cast<uint32_t>(hi - lo);
+    t->N = full.N;
+    t->nf = full.nf;
+    const std::size_t E = full.rowptr.size() - 1;
+    t->rowptr.assign(E + 1, 0);
+    for (std::size_t e = 0; e < E; ++e) {
+        for (int32_t q = full.rowptr[e]; q < full.rowptr[e + 1]; ++q) {
+            const uint32_t key = full.src[q], s = key & 0x7fffffffu;
+            const uint32_t kind = s / nf3, tri = s % nf3;
+            if (tri < static_cast<uint32_t>(lo) || tri >= static_cast<uint32_t>(hi)) continue;
+            t->src.push_back((kind * nsub + (tri - lo)) | (key & 0x80000000u));
+            t->coef.push_back(full.coef[q]);
+        }
+        t->rowptr[e + 1] = static_cast<int32_t>(t->src.size());
+    }
+    t->triple_fc_used.assign(full.triple_fc_used.begin() + lo, full.triple_fc_used.begin() + hi);
+    t->triple_r_used.assign(full.triple_r_used.begin() + lo, full.triple_r_used.begin() + hi);
+    return t;
+}
+
+// Launch geometry of one group (units with equal FFT length).
+template <class R>
+struct GroupGeom {
+    int L = 0;
+    std::size_t Nfft = 0, ntri = 0, Q = 1, nchunks = 0, max_tcount = 0;
+    Tuning tune;
+    Geometry g;
+    int clm = -1, inv_rows = 0, max_chunks = 0;
+    bool use_cluster = false, inv_dft = false;
+};
+
+template <class R>
+GroupGeom<R> group_geom(const std::vector<WorkUnit*>& units) {
+    using C = cplx_t<R>;
+    GroupGeom<R> G;
+    G.L = units[0]->meta->L;
+    G.Nfft = std::size_t(1) << G.L;
+    G.tune = tuning_for(G.L, std::is_same<R, float>::value);
+    FftPlan<C> shape{};
+    shape.L = G.L;
+    shape.L2 = (G.L + 1) / 2;
+    shape.L1 = G.L - shape.L2;
+    G.g = geometry(shape, G.tune.col_tile, G.tune.row_tile);
+    for (auto* u : units) G.ntri += static_cast<std::size_t>(u->nsub());
+    G.clm = cluster_lm_for(G.L, std::is_same<R, float>::value, G.tune);
+    G.use_cluster = G.clm > 0;
+    const std::size_t per_tri_scratch = 2 * G.Nfft * sizeof(C);
+    G.Q = std::max<std::size_t>(1, G.tune.chunk_bytes / per_tri_scratch);
+    G.Q = std::min<std::size_t>({G.Q, std::max<std::size_t>(1, G.ntri), 32767});
+    G.nchunks = (G.ntri + G.Q - 1) / G.Q;
+    for (auto* u : units) G.max_tcount = std::max(G.max_tcount, u->meta->t_count);
+    const int N2 = 1 << shape.L2;
+    G.inv_rows = static_cast<int>((G.max_tcount + N2 - 1) / N2);
+    G.inv_dft = G.inv_rows <= std::min(G.tune.inv_dft_rows, INV_DFT_MAXR);
+    G.max_chunks = static_cast<int>((G.max_tcount + SCAN_CHUNK - 1) / SCAN_CHUNK);
+    return G;
+}
+
+// Transient device arrays of a group (reused by the next group): staged host gamma,
+// spectra, convolution outputs, sources, staged host output, FFT scratch, scan partials.
+template <class C>
+struct WorkPtrs {
+    std::vector<const double2*> gamma;
+    std::vector<C*> spec, conv, v, out;
+    C* scratch = nullptr;
+    double* partial = nullptr;
+};
+
+template <class R>
+void layout_work(const std::vector<WorkUnit*>& units, const GroupGeom<R>& G, bool fcr_only, bool fcr_out_dev,
+                 Layout& lay, WorkPtrs<cplx_t<R>>& P) {
+    using C = cplx_t<R>;
+    const std::size_t ni = units.size();
+    P.gamma.assign(ni, nullptr);
+    P.spec.assign(ni, nullptr);
+    P.conv.assign(ni, nullptr);
+    P.v.assign(ni, nullptr);
+    P.out.assign(ni, nullptr);
+    for (std::size_t a = 0; a < ni; ++a) {
+        const Tcl4Instance& in = *units[a]->in;
+        const InstMeta& m = *units[a]->meta;
+        const std::size_t nf = in.sys.nf, nsub = units[a]->nsub();
+        if (!in.gamma_on_device) P.gamma[a] = lay.take<double2>(nf * m.n_in);
+        P.spec[a] = lay.take<C>(2 * nf * G.Nfft);
+        P.conv[a] = lay.take<C>(nsub * 2 * m.t_count);
+        if (!fcr_only) {
+            P.v[a] = lay.take<C>(3 * nsub * m.U);
+            if (!in.out_on_device) {
+                const std::size_t E = static_cast<std::size_t>(in.sys.N) * in.sys.N * in.sys.N * in.sys.N;
+                P.out[a] = lay.take<C>(m.T * E);
+            }
+        } else if (!fcr_out_dev) {
+            P.v[a] = lay.take<C>(3 * nsub * m.U);
+        }
+    }
+    P.scratch = lay.take<C>(G.use_cluster ? 1 : G.Q * 2 * G.Nfft);
+    P.partial = lay.take<double>(std::max<std::size_t>(1, G.ntri) * G.max_chunks * SCAN_W);
+}
+
+template <class R>
+std::size_t measure_work(const std::vector<WorkUnit*>& units, bool fcr_only, bool fcr_out_dev) {
+    const GroupGeom<R> G = group_geom<R>(units);
+    Layout meas;
+    WorkPtrs<cplx_t<R>> P;
+    layout_work<R>(units, G, fcr_only, fcr_out_dev, meas, P);
+    return meas.off + 256;
+}
+
+// One group (units with equal FFT length): lays out its metadata in `meta_mem` and its
+// transient arrays in `work_mem`, stages the small metadata and the host inputs
+// (stream-ordered on `st`), and returns the closure that enqueues the group's kernels
+// (and the D2H copies of host outputs) on a stream.  `fcr_out` (non-null) writes the
+// F/C/R series (FP64) into caller buffers instead of running the contraction.
 using Enqueue = std::function<void(cudaStream_t, ProfRecorder*, cudaEvent_t, cudaEvent_t)>;
 
 template <class R>
-Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas, const BuildOptions& opt,
-                      cudaStream_t st, Workspace& ws, DeviceBuffer& mem, double2* const* fcr_out,
-                      bool fcr_out_dev) {
+Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cudaStream_t st, Workspace& ws,
+                      DeviceBuffer& meta_mem, DeviceBuffer& work_mem, double2* const* fcr_out, bool fcr_out_dev) {
     using C = cplx_t<R>;
-    const int L = metas[0]->L;
+    (void)opt;
+    const GroupGeom<R> G = group_geom<R>(units);
+    const int L = G.L;
     const FftPlan<C> plan = get_plan<R>(ws, L, st);
-    const Tuning tune = tuning_for(L, std::is_same<R, float>::value);
-    const Geometry g = geometry(plan, tune.col_tile, tune.row_tile);
-    const std::size_t Nfft = std::size_t(1) << L;
-    const std::size_t ni = insts.size();
+    const Geometry g = G.g;
+    const std::size_t Nfft = G.Nfft;
+    const std::size_t ni = units.size();
     const bool fcr_only = (fcr_out != nullptr);
-
-    // triples running the FFT chain / scans (all nf^3 of every instance)
     std::vector<TripleRef> tris;
-    for (std::size_t a = 0; a < ni; ++a) {
-        const int nf3 = insts[a]->sys.nf * insts[a]->sys.nf * insts[a]->sys.nf;
-        for (int t = 0; t < nf3; ++t) tris.push_back({static_cast<int>(a), t});
-    }
+    for (std::size_t a = 0; a < ni; ++a)
+        for (int t = units[a]->lo; t < units[a]->hi; ++t) tris.push_back({static_cast<int>(a), t});
     const std::size_t ntri = tris.size();
-    // chunk of triples whose Z / W intermediates are meant to stay in L2 between passes
-    const int clm = cluster_lm_for(L, std::is_same<R, float>::value, tune);
-    const bool use_cluster = clm > 0;
+    const bool use_cluster = G.use_cluster;
     ClusterPlan<C> cplan{};
-    if (use_cluster) cplan = get_cluster_plan<R>(ws, L, clm, st);
-    const std::size_t per_tri_scratch = 2 * Nfft * sizeof(C);
-    std::size_t Q = std::max<std::size_t>(1, tune.chunk_bytes / per_tri_scratch);
-    Q = std::min<std::size_t>({Q, ntri, 65535});
-    const std::size_t nchunks = (ntri + Q - 1) / Q;
-    // inverse column pass: pruned direct DFT when only a few output rows are needed
-    std::size_t max_tcount = 0;
-    for (auto* m : metas) max_tcount = std::max(max_tcount, m->t_count);
+    if (use_cluster) cplan = get_cluster_plan<R>(ws, L, G.clm, st);
+    const std::size_t Q = G.Q;
+    const std::size_t nchunks = G.nchunks;
     const int N2 = 1 << plan.L2;
-    const int inv_rows = static_cast<int>((max_tcount + N2 - 1) / N2);
-    const bool inv_dft = inv_rows <= std::min(tune.inv_dft_rows, INV_DFT_MAXR);
-    const int max_chunks = static_cast<int>((max_tcount + SCAN_CHUNK - 1) / SCAN_CHUNK);
+    const int inv_rows = G.inv_rows;
+    const bool inv_dft = G.inv_dft;
+    const int max_chunks = G.max_chunks;
 
-    // ---- device layout ----
-    struct Ptrs {
-        std::vector<const double2*> gamma;
-        std::vector<C*> spec;
-        std::vector<C*> conv;     // per instance: [nf^3][2][t_count]
-        std::vector<C*> v;        // per instance: [3 nf^3][U]
+    // ---- device layout: transient arrays in work_mem, metadata in meta_mem ----
+    WorkPtrs<C> P;
+    {
+        Layout meas;
+        layout_work<R>(units, G, fcr_only, fcr_out_dev, meas, P);
+        work_mem.ensure(meas.off + 256);
+        Layout lay{static_cast<char*>(work_mem.p)};
+        layout_work<R>(units, G, fcr_only, fcr_out_dev, lay, P);
+    }
+    struct MetaPtrs {
         std::vector<int*> tmap;
         std::vector<uint32_t*> out_u;
         std::vector<int32_t*> rowptr;
         std::vector<uint32_t*> src;
         std::vector<C*> coef;
-        std::vector<C*> out;
-        C* scratch = nullptr;
-        double* partial = nullptr;
         ClusterJob* clj = nullptr;
         ColJob* colj = nullptr;
         RowJob* rowj = nullptr;
         InvJob* invj = nullptr;
         ScanJob* scanj = nullptr;
         ContractJob* conj = nullptr;
-    } P;
+    } M;
     const std::size_t n_spec_jobs = [&] {
         std::size_t s = 0;
-        for (auto* in : insts) s += 2 * in->sys.nf;
+        for (auto* u : units) s += 2 * u->in->sys.nf;
         return s;
     }();
     const std::size_t n_col_jobs = n_spec_jobs + ntri;
     const std::size_t n_row_jobs = n_spec_jobs + ntri;
-    auto layout = [&](Layout& lay) {
-        P.gamma.assign(ni, nullptr);
-        P.spec.assign(ni, nullptr);
-        P.conv.assign(ni, nullptr);
-        P.v.assign(ni, nullptr);
-        P.tmap.assign(ni, nullptr);
-        P.out_u.assign(ni, nullptr);
-        P.rowptr.assign(ni, nullptr);
-        P.src.assign(ni, nullptr);
-        P.coef.assign(ni, nullptr);
-        P.out.assign(ni, nullptr);
+    auto layout_meta = [&](Layout& lay) {
+        M.tmap.assign(ni, nullptr);
+        M.out_u.assign(ni, nullptr);
+        M.rowptr.assign(ni, nullptr);
+        M.src.assign(ni, nullptr);
+        M.coef.assign(ni, nullptr);
         for (std::size_t a = 0; a < ni; ++a) {
-            const Tcl4Instance& in = *insts[a];
-            const InstMeta& m = *metas[a];
-            const std::size_t nf = in.sys.nf, nf3 = nf * nf * nf;
-            if (!in.gamma_on_device) P.gamma[a] = lay.take<double2>(nf * m.n_in);
-            P.spec[a] = lay.take<C>(2 * nf * Nfft);
-            P.conv[a] = lay.take<C>(nf3 * 2 * m.t_count);
-            P.tmap[a] = lay.take<int>(m.t_count);
+            const InstMeta& m = *units[a]->meta;
+            M.tmap[a] = lay.take<int>(m.t_count);
             if (!fcr_only) {
-                P.v[a] = lay.take<C>(3 * nf3 * m.U);
-                P.out_u[a] = lay.take<uint32_t>(m.T);
-                P.rowptr[a] = lay.take<int32_t>(m.coef.rowptr.size());
-                P.src[a] = lay.take<uint32_t>(std::max<std::size_t>(1, m.coef.src.size()));
-                P.coef[a] = lay.take<C>(std::max<std::size_t>(1, m.coef.coef.size()));
-                if (!in.out_on_device) {
-                    const std::size_t E = static_cast<std::size_t>(in.sys.N) * in.sys.N * in.sys.N * in.sys.N;
-                    P.out[a] = lay.take<C>(m.T * E);
-                }
-            } else if (!fcr_out_dev) {
-                P.v[a] = lay.take<C>(3 * nf3 * m.U);
+                const CoefTable& ct = *units[a]->coef;
+                M.out_u[a] = lay.take<uint32_t>(m.T);
+                M.rowptr[a] = lay.take<int32_t>(ct.rowptr.size());
+                M.src[a] = lay.take<uint32_t>(std::max<std::size_t>(1, ct.src.size()));
+                M.coef[a] = lay.take<C>(std::max<std::size_t>(1, ct.coef.size()));
             }
         }
-        P.scratch = lay.take<C>(use_cluster ? 1 : Q * 2 * Nfft);
-        P.partial = lay.take<double>(ntri * max_chunks * SCAN_W);
-        P.clj = lay.take<ClusterJob>(n_spec_jobs + ntri);
-        P.colj = lay.take<ColJob>(n_col_jobs);
-        P.rowj = lay.take<RowJob>(n_row_jobs);
-        P.invj = lay.take<InvJob>(2 * ntri);
-        P.scanj = lay.take<ScanJob>(ntri);
-        P.conj = lay.take<ContractJob>(ni);
+        M.clj = lay.take<ClusterJob>(n_spec_jobs + ntri);
+        M.colj = lay.take<ColJob>(n_col_jobs);
+        M.rowj = lay.take<RowJob>(n_row_jobs);
+        M.invj = lay.take<InvJob>(2 * ntri);
+        M.scanj = lay.take<ScanJob>(ntri);
+        M.conj = lay.take<ContractJob>(ni);
     };
-    Layout meas;
-    layout(meas);
-    mem.ensure(meas.off);
-    Layout lay{static_cast<char*>(mem.p)};
-    layout(lay);
+    {
+        Layout meas;
+        layout_meta(meas);
+        meta_mem.ensure(meas.off);
+        Layout lay{static_cast<char*>(meta_mem.p)};
+        layout_meta(lay);
+    }
     // column stride of gamma on the device: Nt for caller buffers, n_in for staged host input
     std::vector<std::size_t> gs(ni);
     for (std::size_t a = 0; a < ni; ++a) {
-        if (insts[a]->gamma_on_device) P.gamma[a] = insts[a]->gamma;
-        gs[a] = insts[a]->gamma_on_device ? insts[a]->Nt : metas[a]->n_in;
+        if (units[a]->in->gamma_on_device) P.gamma[a] = units[a]->in->gamma;
+        gs[a] = units[a]->in->gamma_on_device ? units[a]->in->Nt : units[a]->meta->n_in;
     }
 
     // ---- host staging of small metadata (one pinned buffer, one copy per array) ----
@@ -533,8 +633,8 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     std::vector<ContractJob> conj(ni);
     std::size_t cj = 0;
     for (std::size_t a = 0; a < ni; ++a) {
-        const Tcl4Instance& in = *insts[a];
-        const InstMeta& m = *metas[a];
+        const Tcl4Instance& in = *units[a]->in;
+        const InstMeta& m = *units[a]->meta;
         const int nf = in.sys.nf;
         for (int half = 0; half < 2; ++half)
             for (int b = 0; b < nf; ++b) {
@@ -551,9 +651,11 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
             }
     }
     for (std::size_t q = 0; q < ntri; ++q) {
-        const int a = tris[q].inst, tri = tris[q].tri;
-        const Tcl4Instance& in = *insts[a];
-        const InstMeta& m = *metas[a];
+        const int a = tris[q].unit, tri = tris[q].tri;
+        const Tcl4Instance& in = *units[a]->in;
+        const InstMeta& m = *units[a]->meta;
+        const std::size_t lo = static_cast<std::size_t>(units[a]->lo), nsub = units[a]->nsub();
+        const std::size_t lt = tri - lo;  // triple index within the slice
         const int nf = in.sys.nf;
         const int i = tri / (nf * nf), j = (tri / nf) % nf, k = tri % nf;
         const int jm = in.sys.mirror[j] >= 0 ? in.sys.mirror[j] : j;
@@ -571,7 +673,7 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
         c.out = z;
         rowj[n_spec_jobs + q] = RowJob{z, wcb, P.spec[a] + static_cast<std::size_t>(jm) * Nfft,
                                        P.spec[a] + static_cast<std::size_t>(nf + j) * Nfft};
-        C* cf = P.conv[a] + static_cast<std::size_t>(tri) * 2 * m.t_count;
+        C* cf = P.conv[a] + lt * 2 * m.t_count;
         C* cc = cf + m.t_count;
         const double scale = in.dt / static_cast<double>(Nfft);
         invj[2 * q] = InvJob{z, cf, static_cast<uint32_t>(m.t_count), scale};
@@ -586,16 +688,15 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
         s.t_count = static_cast<uint32_t>(m.t_count);
         s.conv_f = cf;
         s.conv_c = cc;
-        s.tmap = P.tmap[a];
-        const std::size_t nf3 = static_cast<std::size_t>(nf) * nf * nf;
+        s.tmap = M.tmap[a];
         if (fcr_only && fcr_out_dev) {
             s.vf = fcr_out[0] + static_cast<std::size_t>(tri) * m.U;
             s.vc = fcr_out[1] + static_cast<std::size_t>(tri) * m.U;
             s.vr = fcr_out[2] + static_cast<std::size_t>(tri) * m.U;
         } else {
-            s.vf = P.v[a] + static_cast<std::size_t>(tri) * m.U;
-            s.vc = P.v[a] + (nf3 + tri) * m.U;
-            s.vr = P.v[a] + (2 * nf3 + tri) * m.U;
+            s.vf = P.v[a] + lt * m.U;
+            s.vc = P.v[a] + (nsub + lt) * m.U;
+            s.vr = P.v[a] + (2 * nsub + lt) * m.U;
         }
     }
     // the same jobs for the cluster path (spectra in its [K][M] order)
@@ -612,18 +713,19 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     }
     if (!fcr_only) {
         for (std::size_t a = 0; a < ni; ++a) {
-            const Tcl4Instance& in = *insts[a];
-            const InstMeta& m = *metas[a];
+            const Tcl4Instance& in = *units[a]->in;
+            const InstMeta& m = *units[a]->meta;
             ContractJob& c = conj[a];
-            c.rowptr = P.rowptr[a];
-            c.src = P.src[a];
-            c.coef = P.coef[a];
+            c.rowptr = M.rowptr[a];
+            c.src = M.src[a];
+            c.coef = M.coef[a];
             c.v = P.v[a];
-            c.out_u = P.out_u[a];
+            c.out_u = M.out_u[a];
             c.out = in.out_on_device ? in.out : P.out[a];
             c.T = static_cast<uint32_t>(m.T);
             c.U = static_cast<uint32_t>(m.U);
             c.E = static_cast<uint32_t>(in.sys.N * in.sys.N * in.sys.N * in.sys.N);
+            c.accumulate = units[a]->accumulate ? 1u : 0u;
         }
     }
     // pack everything small into the pinned staging buffer
@@ -642,20 +744,21 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     auto plan_copy = [&](void* dst, std::size_t bytes) {
         if (bytes) copies.push_back({dst, stage_size(bytes), bytes});
     };
-    plan_copy(P.colj, colj.size() * sizeof(ColJob));
-    plan_copy(P.rowj, rowj.size() * sizeof(RowJob));
-    plan_copy(P.invj, invj.size() * sizeof(InvJob));
-    plan_copy(P.scanj, scanj.size() * sizeof(ScanJob));
-    plan_copy(P.clj, clj.size() * sizeof(ClusterJob));
-    if (!fcr_only) plan_copy(P.conj, conj.size() * sizeof(ContractJob));
+    plan_copy(M.colj, colj.size() * sizeof(ColJob));
+    plan_copy(M.rowj, rowj.size() * sizeof(RowJob));
+    plan_copy(M.invj, invj.size() * sizeof(InvJob));
+    plan_copy(M.scanj, scanj.size() * sizeof(ScanJob));
+    plan_copy(M.clj, clj.size() * sizeof(ClusterJob));
+    if (!fcr_only) plan_copy(M.conj, conj.size() * sizeof(ContractJob));
     for (std::size_t a = 0; a < ni; ++a) {
-        const InstMeta& m = *metas[a];
-        plan_copy(P.tmap[a], m.tmap.size() * sizeof(int));
+        const InstMeta& m = *units[a]->meta;
+        plan_copy(M.tmap[a], m.tmap.size() * sizeof(int));
         if (!fcr_only) {
-            plan_copy(P.out_u[a], m.out_u.size() * sizeof(uint32_t));
-            plan_copy(P.rowptr[a], m.coef.rowptr.size() * sizeof(int32_t));
-            plan_copy(P.src[a], m.coef.src.size() * sizeof(uint32_t));
-            plan_copy(P.coef[a], m.coef.coef.size() * sizeof(C));
+            const CoefTable& ct = *units[a]->coef;
+            plan_copy(M.out_u[a], m.out_u.size() * sizeof(uint32_t));
+            plan_copy(M.rowptr[a], ct.rowptr.size() * sizeof(int32_t));
+            plan_copy(M.src[a], ct.src.size() * sizeof(uint32_t));
+            plan_copy(M.coef[a], ct.coef.size() * sizeof(C));
         }
     }
     ws.staging.ensure(soff);
@@ -674,17 +777,18 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
         put(clj.data(), clj.size() * sizeof(ClusterJob));
         if (!fcr_only) put(conj.data(), conj.size() * sizeof(ContractJob));
         for (std::size_t a = 0; a < ni; ++a) {
-            const InstMeta& m = *metas[a];
+            const InstMeta& m = *units[a]->meta;
             put(m.tmap.data(), m.tmap.size() * sizeof(int));
             if (!fcr_only) {
+                const CoefTable& ct = *units[a]->coef;
                 put(m.out_u.data(), m.out_u.size() * sizeof(uint32_t));
-                put(m.coef.rowptr.data(), m.coef.rowptr.size() * sizeof(int32_t));
-                put(m.coef.src.data(), m.coef.src.size() * sizeof(uint32_t));
+                put(ct.rowptr.data(), ct.rowptr.size() * sizeof(int32_t));
+                put(ct.src.data(), ct.src.size() * sizeof(uint32_t));
                 if (std::is_same<R, double>::value) {
-                    put(m.coef.coef.data(), m.coef.coef.size() * sizeof(C));
+                    put(ct.coef.data(), ct.coef.size() * sizeof(C));
                 } else {
-                    std::vector<float2> cf(m.coef.coef.size());
-                    for (std::size_t e = 0; e < cf.size(); ++e) cf[e] = to_f2(m.coef.coef[e]);
+                    std::vector<float2> cf(ct.coef.size());
+                    for (std::size_t e = 0; e < cf.size(); ++e) cf[e] = to_f2(ct.coef[e]);
                     put(cf.data(), cf.size() * sizeof(float2));
                 }
             }
@@ -694,10 +798,10 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
         cuda_check(cudaMemcpyAsync(c.dst, sb + c.off, c.bytes, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(meta)");
     // host gamma: only the n_in leading samples of each bucket are consumed
     for (std::size_t a = 0; a < ni; ++a)
-        if (!insts[a]->gamma_on_device)
-            cuda_check(cudaMemcpy2DAsync(const_cast<double2*>(P.gamma[a]), gs[a] * sizeof(double2), insts[a]->gamma,
-                                         insts[a]->Nt * sizeof(double2), metas[a]->n_in * sizeof(double2),
-                                         insts[a]->sys.nf, cudaMemcpyHostToDevice, st),
+        if (!units[a]->in->gamma_on_device)
+            cuda_check(cudaMemcpy2DAsync(const_cast<double2*>(P.gamma[a]), gs[a] * sizeof(double2), units[a]->in->gamma,
+                                         units[a]->in->Nt * sizeof(double2), units[a]->meta->n_in * sizeof(double2),
+                                         units[a]->in->sys.nf, cudaMemcpyHostToDevice, st),
                        "cudaMemcpy2DAsync(gamma)");
 
     // the pinned staging buffer is reused by the next call: wait for the copies
@@ -709,22 +813,23 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     set_smem(k_row<R>, g.row_smem);
     int maxE = 0, maxS = 0;
     std::size_t maxNnz = 1;
-    for (auto* in : insts) {
-        maxE = std::max(maxE, in->sys.N * in->sys.N * in->sys.N * in->sys.N);
-        maxS = std::max(maxS, 3 * in->sys.nf * in->sys.nf * in->sys.nf);
+    for (auto* u : units) {
+        maxE = std::max(maxE, u->in->sys.N * u->in->sys.N * u->in->sys.N * u->in->sys.N);
+        maxS = std::max(maxS, 3 * u->nsub());
+        if (!fcr_only) maxNnz = std::max(maxNnz, u->coef->src.size());
     }
-    for (auto* m : metas) maxNnz = std::max(maxNnz, m->coef.src.size());
     std::size_t maxT = 0;
-    for (auto* m : metas) maxT = std::max(maxT, m->T);
+    for (auto* u : units) maxT = std::max(maxT, u->meta->T);
     // contraction: one thread per output time while a [threads][E+1] result tile fits in
-    // shared memory (d <= 3); the shared-memory-tile kernels otherwise
+    // shared memory (d <= 3); the staged-source kernel for small tables; one warp per
+    // (32 entries x 32 times) tile otherwise
     const std::size_t rows_smem = static_cast<std::size_t>(CONTRACT_ROW_THREADS) * (maxE + 1) * sizeof(C);
     const bool contract_rows = rows_smem <= 100 * 1024;
     int maxN = 0;
-    for (auto* in : insts) maxN = std::max(maxN, in->sys.N);
+    for (auto* u : units) maxN = std::max(maxN, u->in->sys.N);
     const bool same_N = [&] {
-        for (auto* in : insts)
-            if (in->sys.N != maxN) return false;
+        for (auto* u : units)
+            if (u->in->sys.N != maxN) return false;
         return true;
     }();
     const std::size_t smem_budget = 100 * 1024;
@@ -735,15 +840,11 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     };
     while (OTs > 16 && smem_need(OTs) > smem_budget) OTs /= 2;
     const bool use_rows = contract_rows && same_N;
-    const bool contract_smem = !use_rows && smem_need(OTs) <= smem_budget;
-    const int OT = use_rows ? CONTRACT_ROW_THREADS
-                            : contract_smem ? OTs
-                                            : std::max(1, std::min(128, static_cast<int>((48 * 1024) / (maxE * sizeof(C)))));
-    const std::size_t csmem = use_rows ? rows_smem
-                                       : contract_smem ? smem_need(OT) : static_cast<std::size_t>(OT) * maxE * sizeof(C);
+    const bool contract_smem = !use_rows && maxE < 256 && smem_need(OTs) <= smem_budget;
+    const int OT = use_rows ? CONTRACT_ROW_THREADS : OTs;
+    const std::size_t csmem = use_rows ? rows_smem : contract_smem ? smem_need(OT) : 0;
     if (use_rows) set_smem(k_contract_rows<R>, csmem);
     else if (contract_smem) set_smem(k_contract_smem<R>, csmem);
-    else set_smem(k_contract<R>, csmem);
     const int nnz_cap = static_cast<int>(maxNnz);
     struct D2H {
         void* dst;
@@ -753,19 +854,21 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     std::vector<D2H> d2h;
     if (!fcr_only) {
         for (std::size_t a = 0; a < ni; ++a) {
-            if (insts[a]->out_on_device) continue;
-            const std::size_t E = static_cast<std::size_t>(insts[a]->sys.N) * insts[a]->sys.N * insts[a]->sys.N *
-                                  insts[a]->sys.N;
-            d2h.push_back({insts[a]->out, P.out[a], metas[a]->T * E * sizeof(C)});
+            if (units[a]->in->out_on_device) continue;
+            const Tcl4Instance& in = *units[a]->in;
+            const std::size_t E = static_cast<std::size_t>(in.sys.N) * in.sys.N * in.sys.N * in.sys.N;
+            d2h.push_back({in.out, P.out[a], units[a]->meta->T * E * sizeof(C)});
         }
     } else if (!fcr_out_dev) {
-        const Tcl4Instance& in = *insts[0];
+        const Tcl4Instance& in = *units[0]->in;
         const std::size_t nf3 = static_cast<std::size_t>(in.sys.nf) * in.sys.nf * in.sys.nf;
-        const std::size_t U = metas[0]->U;
+        const std::size_t U = units[0]->meta->U;
         for (int kind = 0; kind < 3; ++kind)
             d2h.push_back({fcr_out[kind], P.v[0] + kind * nf3 * U, nf3 * U * sizeof(C)});
     }
     const std::size_t n_scan = ntri;
+    const MetaPtrs Mc = M;
+    const WorkPtrs<C> Pc = P;
     return [=](cudaStream_t st, ProfRecorder* prp, cudaEvent_t ev0, cudaEvent_t ev1) {
     ProfRecorder dummy;
     ProfRecorder& pr = prp ? *prp : dummy;
@@ -773,61 +876,68 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
     if (ev0) cuda_check(cudaEventRecord(ev0, st), "cudaEventRecord");
     if (use_cluster) {
         pr.before(f32 ? "spectra_cluster_f32" : "spectra_cluster_f64");
-        launch_cluster<R>(P.clj, n_spec_jobs, cplan, st);
+        launch_cluster<R>(Mc.clj, n_spec_jobs, cplan, st);
         check_launch("k_conv_cluster(spectra)", &pr);
         pr.before(f32 ? "conv_cluster_f32" : "conv_cluster_f64");
-        launch_cluster<R>(P.clj + n_spec_jobs, ntri, cplan, st);
+        launch_cluster<R>(Mc.clj + n_spec_jobs, ntri, cplan, st);
         check_launch("k_conv_cluster", &pr);
     } else {
         pr.before(f32 ? "spectra_col_f32" : "spectra_col_f64");
         k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(n_spec_jobs)), g.col_threads, g.col_smem, st>>>(
-            P.colj, plan, g.log2c);
+            Mc.colj, plan, g.log2c);
         check_launch("k_fwd_col(spectra)", &pr);
         pr.before(f32 ? "spectra_row_f32" : "spectra_row_f64");
         k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
-            P.rowj, plan, g.log2r);
+            Mc.rowj, plan, g.log2r);
         check_launch("k_row(spectra)", &pr);
         const unsigned dft_grid = static_cast<unsigned>((N2 + INV_DFT_THREADS - 1) / INV_DFT_THREADS);
         for (std::size_t ch = 0; ch < nchunks; ++ch) {
             const std::size_t q0 = ch * Q, nq = std::min(Q, ntri - q0);
             pr.before(f32 ? "fwd_col_f32" : "fwd_col_f64");
             k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(nq)), g.col_threads, g.col_smem, st>>>(
-                P.colj + n_spec_jobs + q0, plan, g.log2c);
+                Mc.colj + n_spec_jobs + q0, plan, g.log2c);
             check_launch("k_fwd_col", &pr);
             pr.before(f32 ? "row_conv_f32" : "row_conv_f64");
             k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
-                P.rowj + n_spec_jobs + q0, plan, g.log2r);
+                Mc.rowj + n_spec_jobs + q0, plan, g.log2r);
             check_launch("k_row", &pr);
             pr.before(f32 ? "inv_col_f32" : "inv_col_f64");
             if (inv_dft) {
                 k_inv_col_dft<R><<<dim3(dft_grid, static_cast<unsigned>(2 * nq)), INV_DFT_THREADS, 0, st>>>(
-                    P.invj + 2 * q0, plan, inv_rows);
+                    Mc.invj + 2 * q0, plan, inv_rows);
                 check_launch("k_inv_col_dft", &pr);
             } else {
                 k_inv_col<R><<<dim3(g.col_grid, static_cast<unsigned>(2 * nq)), g.col_threads, g.col_smem, st>>>(
-                    P.invj + 2 * q0, plan, g.log2c);
+                    Mc.invj + 2 * q0, plan, g.log2c);
                 check_launch("k_inv_col", &pr);
             }
         }
     }
-    pr.before(f32 ? "scan_reduce_f32" : "scan_reduce_f64");
-    k_scan_reduce<R><<<dim3(static_cast<unsigned>(max_chunks), static_cast<unsigned>(n_scan)), SCAN_THREADS, 0, st>>>(
-        P.scanj, P.partial, max_chunks);
-    check_launch("k_scan_reduce", &pr);
-    pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
-    k_scan_chunks<R><<<dim3(static_cast<unsigned>(max_chunks), static_cast<unsigned>(n_scan)), SCAN_THREADS, 0, st>>>(
-        P.scanj, P.partial, max_chunks);
-    check_launch("k_scan_chunks", &pr);
+    for (std::size_t s0 = 0; s0 < n_scan; s0 += 65535) {
+        const unsigned ns = static_cast<unsigned>(std::min<std::size_t>(65535, n_scan - s0));
+        pr.before(f32 ? "scan_reduce_f32" : "scan_reduce_f64");
+        k_scan_reduce<R><<<dim3(static_cast<unsigned>(max_chunks), ns), SCAN_THREADS, 0, st>>>(
+            Mc.scanj + s0, Pc.partial + s0 * max_chunks * SCAN_W, max_chunks);
+        check_launch("k_scan_reduce", &pr);
+        pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
+        k_scan_chunks<R><<<dim3(static_cast<unsigned>(max_chunks), ns), SCAN_THREADS, 0, st>>>(
+            Mc.scanj + s0, Pc.partial + s0 * max_chunks * SCAN_W, max_chunks);
+        check_launch("k_scan_chunks", &pr);
+    }
     if (ev1) cuda_check(cudaEventRecord(ev1, st), "cudaEventRecord");
     if (!fcr_only) {
         pr.before(f32 ? "contract_f32" : "contract_f64");
-        const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
-        if (use_rows)
-            k_contract_rows<R><<<dim3(gx, static_cast<unsigned>(ni)), CONTRACT_ROW_THREADS, csmem, st>>>(P.conj, maxN);
-        else if (contract_smem)
-            k_contract_smem<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(P.conj, OT, maxS, nnz_cap);
-        else
-            k_contract<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(P.conj, OT);
+        if (use_rows) {
+            const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
+            k_contract_rows<R><<<dim3(gx, static_cast<unsigned>(ni)), CONTRACT_ROW_THREADS, csmem, st>>>(Mc.conj, maxN);
+        } else if (contract_smem) {
+            const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
+            k_contract_smem<R><<<dim3(gx, static_cast<unsigned>(ni)), 256, csmem, st>>>(Mc.conj, OT, maxS, nnz_cap);
+        } else {
+            const unsigned gx = static_cast<unsigned>((maxT + CONTRACT_TILE - 1) / CONTRACT_TILE);
+            const unsigned gy = static_cast<unsigned>((maxE + CONTRACT_TILE - 1) / CONTRACT_TILE);
+            k_contract_tiles<R><<<dim3(gx, gy, static_cast<unsigned>(ni)), CONTRACT_TILE_THREADS, 0, st>>>(Mc.conj);
+        }
         check_launch("k_contract", &pr);
     }
     for (const D2H& c : d2h)
@@ -836,9 +946,9 @@ Enqueue prepare_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>&
 }
 
 template <class R>
-void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas, const BuildOptions& opt,
-               cudaStream_t st, Workspace& ws, double2* const* fcr_out, bool fcr_out_dev) {
-    Enqueue enq = prepare_group<R>(insts, metas, opt, st, ws, ws.arena, fcr_out, fcr_out_dev);
+void run_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cudaStream_t st, Workspace& ws,
+               double2* const* fcr_out, bool fcr_out_dev) {
+    Enqueue enq = prepare_group<R>(units, opt, st, ws, ws.arena, ws.work, fcr_out, fcr_out_dev);
     ProfRecorder pr;
     pr.st = st;
     enq(st, &pr, opt.fcr_ms ? ws.ev0 : nullptr, opt.fcr_ms ? ws.ev1 : nullptr);
@@ -850,6 +960,138 @@ void run_group(std::vector<Tcl4Instance*>& insts, std::vector<InstMeta*>& metas,
         *opt.fcr_ms += ms;
     }
 }
+
+// Transient-memory budget of one group: set explicitly, or 45% of the free device memory
+// (at most 64 GiB) at the time of the call.
+std::atomic<std::size_t> g_work_budget{0};
+
+std::size_t work_budget() {
+    const std::size_t set = g_work_budget.load();
+    if (set) return set;
+    std::size_t fr = 0, tot = 0;
+    cuda_check(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+    return std::min<std::size_t>(fr / 100 * 45, std::size_t(64) << 30);
+}
+
+// Work units for a set of instances: instances with equal FFT length are packed into
+// groups while their transient arrays fit the budget; an instance that alone exceeds it
+// is cut into triple slices, each its own group, run in order (the first overwrites the
+// output, the rest accumulate).
+template <class R>
+std::vector<std::vector<WorkUnit*>> plan_units(std::vector<Tcl4Instance>& insts, std::vector<InstMeta>& metas,
+                                               std::size_t budget, std::vector<std::unique_ptr<WorkUnit>>& store) {
+    std::map<int, std::vector<std::size_t>> byL;
+    for (std::size_t a = 0; a < insts.size(); ++a)
+        if (!insts[a].tidx.empty()) byL[metas[a].L].push_back(a);
+    std::vector<std::vector<WorkUnit*>> groups;
+    for (auto& kv : byL) {
+        std::vector<WorkUnit*> cur;
+        for (std::size_t a : kv.second) {
+            const int nf3 = insts[a].sys.nf * insts[a].sys.nf * insts[a].sys.nf;
+            auto unit = std::make_unique<WorkUnit>();
+            unit->in = &insts[a];
+            unit->meta = &metas[a];
+            unit->lo = 0;
+            unit->hi = nf3;
+            unit->coef = &metas[a].coef;
+            std::vector<WorkUnit*> one{unit.get()};
+            const std::size_t need = measure_work<R>(one, false, false);
+            if (need > budget) {
+                // slices sized from the per-triple cost of a probe slice
+                WorkUnit probe = *unit;
+                probe.hi = 1;
+                std::vector<WorkUnit*> p1{&probe};
+                const std::size_t base = measure_work<R>(p1, false, false);
+                probe.hi = std::min(nf3, 2);
+                const std::size_t two = measure_work<R>(p1, false, false);
+                const std::size_t per = std::max<std::size_t>(1, two > base ? two - base : base);
+                const std::size_t nsub = budget > base ? std::max<std::size_t>(1, (budget - base) / per + 1) : 1;
+                if (!insts[a].gamma_on_device || !insts[a].out_on_device)
+                    throw Error(kRuntime, "sliced instances need device inputs and outputs");
+                for (int lo = 0; lo < nf3; lo += static_cast<int>(nsub)) {
+                    auto u = std::make_unique<WorkUnit>();
+                    u->in = &insts[a];
+                    u->meta = &metas[a];
+                    u->lo = lo;
+                    u->hi = std::min(nf3, lo + static_cast<int>(nsub));
+                    u->accumulate = lo > 0;
+                    u->own = slice_table(metas[a].coef, u->lo, u->hi);
+                    u->coef = u->own.get();
+                    groups.push_back({u.get()});
+                    store.push_back(std::move(u));
+                }
+                continue;
+            }
+            cur.push_back(unit.get());
+            store.push_back(std::move(unit));
+            if (cur.size() > 1 && measure_work<R>(cur, false, false) > budget) {
+                WorkUnit* last = cur.back();
+                cur.pop_back();
+                groups.push_back(cur);
+                cur = {last};
+            }
+        }
+        if (!cur.empty()) groups.push_back(cur);
+    }
+    return groups;
+}
+
+// Instances that will be sliced read and write device memory: host gamma and host
+// outputs go through device copies made here (and copied back by the caller).
+struct HostIoStage {
+    std::vector<void*> bufs;
+    struct Back {
+        void* host;
+        const void* dev;
+        std::size_t bytes;
+    };
+    std::vector<Back> back;
+    ~HostIoStage() {
+        for (void* p : bufs) cudaFree(p);
+    }
+};
+
+template <class R>
+void stage_sliced_io(std::vector<Tcl4Instance>& insts, std::vector<InstMeta>& metas, std::size_t budget,
+                     HostIoStage& io, cudaStream_t st) {
+    using C = cplx_t<R>;
+    for (std::size_t a = 0; a < insts.size(); ++a) {
+        Tcl4Instance& in = insts[a];
+        if (in.tidx.empty() || (in.gamma_on_device && in.out_on_device)) continue;
+        WorkUnit u;
+        u.in = &in;
+        u.meta = &metas[a];
+        u.hi = in.sys.nf * in.sys.nf * in.sys.nf;
+        u.coef = &metas[a].coef;
+        std::vector<WorkUnit*> one{&u};
+        if (measure_work<R>(one, false, false) <= budget) continue;
+        if (!in.gamma_on_device) {
+            const std::size_t bytes = static_cast<std::size_t>(in.sys.nf) * in.Nt * sizeof(double2);
+            void* d = nullptr;
+            cuda_check(cudaMalloc(&d, bytes), "cudaMalloc(sliced gamma)");
+            io.bufs.push_back(d);
+            cuda_check(cudaMemcpyAsync(d, in.gamma, bytes, cudaMemcpyHostToDevice, st), "sliced gamma");
+            in.gamma = static_cast<const double2*>(d);
+            in.gamma_on_device = true;
+        }
+        if (!in.out_on_device) {
+            const std::size_t E = static_cast<std::size_t>(in.sys.N) * in.sys.N * in.sys.N * in.sys.N;
+            const std::size_t bytes = metas[a].T * E * sizeof(C);
+            void* d = nullptr;
+            cuda_check(cudaMalloc(&d, bytes), "cudaMalloc(sliced out)");
+            io.bufs.push_back(d);
+            io.back.push_back({in.out, d, bytes});
+            in.out = d;
+            in.out_on_device = true;
+        }
+    }
+}
+
+}  // namespace
+
+void set_work_budget(std::size_t bytes) { g_work_budget.store(bytes); }
+
+namespace {
 
 void validate_system(const SystemDesc& s) {
     if (s.N <= 0) throw Error(kInvalidArgument, "system: N must be > 0");
@@ -890,6 +1132,20 @@ void clear_tuning() {
 }
 
 uint64_t kernel_launches() { return g_launches.load(); }
+
+void raise_smem_limit(const void* kernel, std::size_t bytes) {
+    if (bytes <= 48 * 1024) return;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, std::size_t> granted;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(mu);
+    std::size_t& g = granted[{dev, kernel}];
+    if (bytes <= g) return;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
+               "cudaFuncSetAttribute(smem)");
+    g = bytes;
+}
 void count_launches(uint64_t n) { g_launches.fetch_add(n); }
 void profile_enable(bool on) { g_profile.store(on); }
 void profile_reset() {
@@ -954,20 +1210,24 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
     if (opt.fcr_ms) *opt.fcr_ms = 0.0;
     std::vector<InstMeta> metas;
     validate_and_derive(insts, opt, metas);
-    // group by FFT length
-    std::map<int, std::vector<std::size_t>> groups;
-    for (std::size_t a = 0; a < insts.size(); ++a)
-        if (!insts[a].tidx.empty()) groups[metas[a].L].push_back(a);
-    for (auto& kv : groups) {
-        std::vector<Tcl4Instance*> gi;
-        std::vector<InstMeta*> gm;
-        for (std::size_t a : kv.second) {
-            gi.push_back(&insts[a]);
-            gm.push_back(&metas[a]);
-        }
-        if (opt.fp32) run_group<float>(gi, gm, opt, st, ws, nullptr, false);
-        else run_group<double>(gi, gm, opt, st, ws, nullptr, false);
+    const std::size_t budget = work_budget();
+    HostIoStage io;
+    std::vector<std::unique_ptr<WorkUnit>> store;
+    std::vector<std::vector<WorkUnit*>> groups;
+    if (opt.fp32) {
+        stage_sliced_io<float>(insts, metas, budget, io, st);
+        groups = plan_units<float>(insts, metas, budget, store);
+    } else {
+        stage_sliced_io<double>(insts, metas, budget, io, st);
+        groups = plan_units<double>(insts, metas, budget, store);
     }
+    for (auto& gu : groups) {
+        if (opt.fp32) run_group<float>(gu, opt, st, ws, nullptr, false);
+        else run_group<double>(gu, opt, st, ws, nullptr, false);
+    }
+    for (const auto& b : io.back)
+        cuda_check(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(sliced out)");
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(build)");
 }
 
 void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_device, std::size_t Nt, double dt,
@@ -998,17 +1258,23 @@ void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_d
     o.causal_truncation = false;
     InstMeta m;
     derive_meta(in, o, m, false);
-    std::vector<Tcl4Instance*> gi{&in};
-    std::vector<InstMeta*> gm{&m};
+    WorkUnit u;
+    u.in = &in;
+    u.meta = &m;
+    u.hi = s.nf * s.nf * s.nf;
+    u.coef = &m.coef;
+    std::vector<WorkUnit*> gu{&u};
     double2* outs[3] = {F, Cc, R};
     if (opt.fcr_ms) *opt.fcr_ms = 0.0;
-    run_group<double>(gi, gm, o, st, ws, outs, out_on_device);
+    run_group<double>(gu, o, st, ws, outs, out_on_device);
 }
 
 struct Tcl4Plan {
     int device = 0;
     cudaStream_t stream = nullptr;
-    std::vector<std::unique_ptr<DeviceBuffer>> mems;
+    std::vector<std::unique_ptr<DeviceBuffer>> mems;  // per-group metadata
+    DeviceBuffer work;                                 // transient arrays, shared
+    std::vector<std::unique_ptr<WorkUnit>> units;
     std::vector<Enqueue> enqs;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1049,21 +1315,21 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
     cuda_check(cudaGetDevice(&plan->device), "cudaGetDevice");
     cuda_check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate(plan)");
     Workspace& ws = workspace();
-    std::map<int, std::vector<std::size_t>> groups;
-    for (std::size_t a = 0; a < insts.size(); ++a)
-        if (!insts[a].tidx.empty()) groups[metas[a].L].push_back(a);
-    for (auto& kv : groups) {
-        std::vector<Tcl4Instance*> gi;
-        std::vector<InstMeta*> gm;
-        for (std::size_t a : kv.second) {
-            gi.push_back(&insts[a]);
-            gm.push_back(&metas[a]);
-        }
+    const std::size_t budget = work_budget();
+    std::vector<std::vector<WorkUnit*>> groups =
+        opt.fp32 ? plan_units<float>(insts, metas, budget, plan->units) : plan_units<double>(insts, metas, budget, plan->units);
+    // one transient buffer shared by the groups (they run in order on the plan's stream),
+    // sized before any group records its pointers
+    std::size_t work = 0;
+    for (auto& gu : groups)
+        work = std::max(work, opt.fp32 ? measure_work<float>(gu, false, false) : measure_work<double>(gu, false, false));
+    plan->work.ensure(work);
+    for (auto& gu : groups) {
         plan->mems.push_back(std::make_unique<DeviceBuffer>());
         if (opt.fp32)
-            plan->enqs.push_back(prepare_group<float>(gi, gm, opt, plan->stream, ws, *plan->mems.back(), nullptr, false));
+            plan->enqs.push_back(prepare_group<float>(gu, opt, plan->stream, ws, *plan->mems.back(), plan->work, nullptr, false));
         else
-            plan->enqs.push_back(prepare_group<double>(gi, gm, opt, plan->stream, ws, *plan->mems.back(), nullptr, false));
+            plan->enqs.push_back(prepare_group<double>(gu, opt, plan->stream, ws, *plan->mems.back(), plan->work, nullptr, false));
     }
     const uint64_t k0 = g_launches.load();
     cuda_check(cudaStreamBeginCapture(plan->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");

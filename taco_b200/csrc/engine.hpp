@@ -38,6 +38,9 @@ struct Tuning {
     int cluster_lm = 0;  // log2 points per CTA of the cluster path (0: multi-pass path, -1: automatic)
 };
 void set_tuning(int L, bool fp32, const Tuning& t);
+// Transient device memory one group of a build may use (0: 45% of the free memory, at
+// most 64 GiB); an instance above it is processed in slices of its frequency triples.
+void set_work_budget(std::size_t bytes);
 Tuning get_tuning(int L, bool fp32);
 void clear_tuning();
 
@@ -198,6 +201,10 @@ cudaStream_t default_stream();
 // on, each launch is bracketed by CUDA events and its device time is accumulated per
 // kernel name after the call's final synchronisation.
 uint64_t kernel_launches();
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` (per device).  The
+// limit only grows: launches prepared earlier, and replayed later from a captured graph,
+// keep the room they were prepared with.
+void raise_smem_limit(const void* kernel, std::size_t bytes);
 // Adds n to the process-wide launch counter (kernels launched outside engine.cu).
 void count_launches(uint64_t n);
 // Checks the launch just issued and counts it.

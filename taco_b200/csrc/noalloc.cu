@@ -85,9 +85,7 @@ struct Carve {
 
 template <class K>
 void smem_attr(K kernel, std::size_t bytes) {
-    if (bytes > 48 * 1024)
-        cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
-                   "cudaFuncSetAttribute(smem)");
+    raise_smem_limit(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 template <class R>

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <complex>
+#include <map>
 #include <vector>
 
 #include "common.cuh"
@@ -168,6 +169,32 @@ __global__ void k_add_c64(const float2* __restrict__ src, double2* __restrict__ 
     for (std::size_t k = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; k < n;
          k += static_cast<std::size_t>(gridDim.x) * blockDim.x)
         dst[k] = cadd(dst[k], to_d2(src[k]));
+}
+
+// Grow-only device scratch per host thread and device (the small maps and partial sums).
+struct Tcl2Scratch {
+    void* p = nullptr;
+    std::size_t cap = 0;
+    char* ensure(std::size_t bytes) {
+        if (bytes > cap) {
+            if (p) cudaFree(p);
+            p = nullptr;
+            cap = 0;
+            cuda_check(cudaMalloc(&p, bytes), "cudaMalloc(tcl2 scratch)");
+            cap = bytes;
+        }
+        return static_cast<char*>(p);
+    }
+    ~Tcl2Scratch() {
+        if (p) cudaFree(p);
+    }
+};
+
+char* tcl2_scratch(std::size_t bytes) {
+    thread_local std::map<int, Tcl2Scratch> per_dev;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    return per_dev[dev].ensure(bytes);
 }
 
 }  // namespace
@@ -358,9 +385,8 @@ void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2*
     tcl2_maps(sys, eps, L0, Db, Ub);
     // device staging of the (small) maps: allocated for the call, released after it
     const std::size_t bytes = (E + 2 * nf * E) * sizeof(double2) + tidx.size() * sizeof(uint32_t);
-    void* d = nullptr;
-    cuda_check(cudaMalloc(&d, bytes), "cudaMalloc(tcl2 maps)");
-    try {
+    void* d = tcl2_scratch(bytes);
+    {
         double2* dL0 = static_cast<double2*>(d);
         double2* dD = dL0 + E;
         double2* dU = dD + nf * E;
@@ -377,12 +403,7 @@ void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2*
             launched("k_tcl2_series");
         }
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl2)");
-    } catch (...) {
-        cudaStreamSynchronize(st);
-        cudaFree(d);
-        throw;
     }
-    cudaFree(d);
 }
 
 void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::vector<double>& omegas, double2* G,
@@ -390,10 +411,9 @@ void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::v
     const int nb = static_cast<int>(omegas.size());
     const int nchunks = static_cast<int>((N + GT_CHUNK - 1) / GT_CHUNK);
     if (nb > 65535) throw Error(kInvalidArgument, "gamma_trapz: too many frequencies");
-    void* d = nullptr;
     const std::size_t bytes = nb * sizeof(double) + static_cast<std::size_t>(nb) * nchunks * sizeof(double2) + 256;
-    cuda_check(cudaMalloc(&d, bytes), "cudaMalloc(gamma_trapz)");
-    try {
+    void* d = tcl2_scratch(bytes);
+    {
         double* dom = static_cast<double*>(d);
         double2* part = reinterpret_cast<double2*>(static_cast<char*>(d) + ((nb * sizeof(double) + 255) / 256) * 256);
         cuda_check(cudaMemcpyAsync(dom, omegas.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st), "omegas");
@@ -404,12 +424,7 @@ void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::v
             C, N, dt, dom, part, nchunks, G);
         launched("k_gamma_scan");
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(gamma)");
-    } catch (...) {
-        cudaStreamSynchronize(st);
-        cudaFree(d);
-        throw;
     }
-    cudaFree(d);
 }
 
 }  // namespace taco

@@ -202,21 +202,7 @@ def test_tcl2_adjoint_matches_fd(d, T):
 
 
 def oracle_spin_boson_obs(p, cfg):
-    """<sz(t)> of the FP64 oracle chain for one parameter vector (eps, Delta, alpha, wc, beta)."""
-    eps, delta, alpha, wc, beta = p
-    T = cfg.steps + 1
-    H = 0.5 * eps * SZ + 0.5 * delta * SX
-    osys = oracle.System(H, [SZ])
-    _, C = oracle.bcf_fft(cfg.N, cfg.dt, oracle.J_OHMIC, [alpha, wc], beta)
-    G = oracle.gamma_trapz(C[:T], cfg.dt, osys.omegas)
-    L4 = oracle.tcl4_build_batch(osys.N, osys.nf, osys.omegas, osys.mirror, osys.p2f_colmajor(),
-                                 osys.ops_colmajor(), G, cfg.dt, tidx=np.arange(T))
-    L2 = np.stack([oracle.tcl2_total(osys, G[:, t])[0] for t in range(T)])
-    U = osys.U
-    r0 = (U.conj().T @ cfg.rho0 @ U).reshape(-1, order="F")
-    ov = (U.conj().T @ cfg.observable @ U).T.reshape(-1, order="F")
-    _, samp = oracle.rk4_propagate(L2 + L4, r0, cfg.dt, sample_every=cfg.sample_every)
-    return np.real(samp @ ov)
+    return oracle.spin_boson_trajectory(p, cfg.N, cfg.dt, cfg.steps, cfg.rho0, cfg.observable, cfg.sample_every)
 
 
 def test_spin_boson_gradient_matches_oracle_fd():
