@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--c3-dims", default="4,6", help="precision form on random systems (empty: skip)")
     p.add_argument("--c3-N", type=int, default=1 << 18)
     p.add_argument("--c3-stride", type=int, default=4)
+    p.add_argument("--c4-instances", type=int, default=32, help="heterogeneous batch (0: skip; the config names 256)")
     return p.parse_args()
 
 
@@ -279,6 +280,83 @@ def precision_random(args, d, cpu_leg):
     return out
 
 
+def heterogeneous_batch(args, rank, world, cpu_leg):
+    """Batching form: seeded instances with d ~ U{2,3,4,6,8} (GUE H, random unit-norm A),
+    Ohmic bath alpha ~ logU[0.01, 0.2], wc ~ U[1, 20], beta ~ logU[0.2, 5], N ~ U{2^14..2^18},
+    dt = 10 / (N wc), every 8th time index; one plan (the FP32 form) replayed as a CUDA
+    graph.  FP64 reference: the same plan in FP64.  CPU leg: the oracle on the smallest
+    instance of each dimension, at four sampled times within its first 2049 steps."""
+    import torch
+    import taco_b200 as tb
+    from taco_b200 import adjoint as adj
+    B = args.c4_instances
+    rng = np.random.default_rng(args.seed + 400 + 1000 * rank)
+    dims = rng.choice([2, 3, 4, 6, 8], B)
+    Ns = 1 << rng.integers(14, 19, B)
+    alpha = np.exp(rng.uniform(np.log(0.01), np.log(0.2), B))
+    wc = rng.uniform(1.0, 20.0, B)
+    beta = np.exp(rng.uniform(np.log(0.2), np.log(5.0), B))
+    systems, gammas, tids, dts = [], [], [], []
+    t0 = time.perf_counter()
+    for b in range(B):
+        s, _ = gue_system(int(dims[b]), rng)
+        dt = 10.0 / (Ns[b] * wc[b])
+        C = adj.bcf_device([dict(alpha=alpha[b], omega_c=wc[b], beta=beta[b], N=int(Ns[b]), dt=dt)], int(Ns[b]) + 1)[0]
+        gammas.append(tb.gamma_trapz_device(C, dt, s.omegas))
+        systems.append(s)
+        tids.append(np.arange(0, int(Ns[b]), 8, dtype=np.uint32))
+        dts.append(dt)
+    inputs_s = time.perf_counter() - t0
+    inst = [(systems[b], gammas[b], dts[b], tids[b]) for b in range(B)]
+    builds = int(sum(t.size for t in tids))
+    out = {"instances_per_gpu": B, "dims": np.bincount(dims, minlength=9)[[2, 3, 4, 6, 8]].tolist(),
+           "builds_per_step": builds, "input_build_seconds": round(inputs_s, 2)}
+    res = {}
+    for prec in ("fp32", "fp64"):
+        t0 = time.perf_counter()
+        plan = tb.Tcl4Plan(inst, precision=prec)
+        prep = time.perf_counter() - t0
+        plan.run()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        plan.run()
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        out[prec] = {"value": world * builds / (ms / 1e3), "unit": "builds/s", "ms_per_step": ms,
+                     "plan_prepare_seconds": round(prep, 2)}
+        res[prec] = [r.to(torch.complex128) if prec == "fp32" else r for r in plan.results]
+        if prec == "fp32":
+            res[prec] = [r.clone() for r in res[prec]]
+        plan.close()
+    errs = [float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) for a, b in zip(res["fp32"], res["fp64"])]
+    out["l4_fp32_rel_err_vs_fp64_max"] = max(errs)
+    out["per_instance"] = [[int(dims[b]), int(np.log2(Ns[b])), round(float(wc[b]), 3), errs[b]] for b in range(B)]
+    if cpu_leg:
+        # the oracle on the smallest instance of each dimension: F/C/R over the first 2049
+        # steps, L4 at four of the sampled times in that window
+        import oracle
+        chk = {}
+        for d in sorted(set(dims.tolist())):
+            b = min((k for k in range(B) if dims[k] == d), key=lambda k: Ns[k])
+            s = systems[b]
+            pos = [16, 64, 128, 256]
+            Gh = np.ascontiguousarray(gammas[b][:, :2049].cpu().numpy())
+            p2f = np.ascontiguousarray(s.pair_to_freq.T, np.int32)
+            ops = np.ascontiguousarray(np.stack([Ae.T for Ae in s.A_eig]))
+            ref = oracle.tcl4_build_batch(s.N, s.nf, s.omegas, s.mirror, p2f, ops, Gh, dts[b], tidx=tids[b][pos])
+            g64 = res["fp64"][b][pos].cpu().numpy()
+            g32 = res["fp32"][b][pos].cpu().numpy()
+            chk[str(d)] = {"instance": int(b), "times": tids[b][pos].tolist(),
+                           "fp64_rel_err": float(np.linalg.norm(g64 - ref) / np.linalg.norm(ref)),
+                           "fp32_rel_err": float(np.linalg.norm(g32 - ref) / np.linalg.norm(ref))}
+        out["oracle_check"] = chk
+    del res
+    torch.cuda.empty_cache()
+    return out
+
+
 def differentiation(args, rank, world, cpu_leg):
     """The differentiation form: loss = mean_t (<sz(t)> - target)^2 per spin-boson instance,
     gradient in (eps, Delta, alpha, wc, beta) by the hand-written adjoint (FP64 and with the
@@ -496,10 +574,12 @@ def main():
         fp64_parity = {"vs_oracle_convolution": re(g64, L4o), "vs_oracle_direct": re(g64, L4d),
                        "oracle_convolution_vs_direct": re(L4o, L4d), "fp32_vs_oracle_direct": re(g32, L4d)}
 
-    grad = differentiation(args, rank, world, rank == 0 and world == 1 and not args.no_cpu_baseline) \
-        if args.grad_instances > 0 else None
-    c3 = [precision_random(args, int(d), rank == 0 and world == 1 and not args.no_cpu_baseline)
-          for d in args.c3_dims.split(",") if d.strip()]
+    # the other forms and configurations: one GPU only (the scaling runs time the headline)
+    cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+    single = world == 1
+    grad = differentiation(args, rank, world, cpu_leg) if single and args.grad_instances > 0 else None
+    c3 = [precision_random(args, int(d), cpu_leg) for d in args.c3_dims.split(",") if d.strip()] if single else None
+    c4 = heterogeneous_batch(args, rank, world, cpu_leg) if single and args.c4_instances > 0 else None
 
     if rank == 0:
         line = {
@@ -528,6 +608,7 @@ def main():
             "roofline": roofline, "kernels": kernels,
             "differentiation": grad,
             "precision_random": c3,
+            "heterogeneous_batch": c4,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk.summary(),
