@@ -238,6 +238,7 @@ def precision_random(args, d, cpu_leg):
     out = {"d": d, "nf": int(s.nf), "N": N, "T": int(T), "triples": int(s.nf) ** 3}
     res = {}
     for prec in ("fp32", "fp64"):
+        tb.build_TCL4_generator_batch(s, G, dt, tidx, precision=prec)  # warm-up (tables, workspace)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         L4 = tb.build_TCL4_generator_batch(s, G, dt, tidx, precision=prec)
@@ -419,6 +420,7 @@ def main():
 
     import torch
     import taco_b200 as tb
+    from taco_b200 import workloads
     from taco_b200.workloads import spin_boson_batch
 
     torch.cuda.set_device(local)
@@ -435,14 +437,10 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return workloads.max_over_ranks(dist, x, device)
 
     B = args.instances
-    params, systems, gammas = spin_boson_batch(torch, B, args.N, args.dt, seed=args.seed + 1000 * rank,
+    params, systems, gammas = spin_boson_batch(torch, B, args.N, args.dt, seed=workloads.rank_seed(args.seed, rank),
                                                device=device)
     T = args.tmax + 1
     tidx = np.arange(T, dtype=np.uint32)
@@ -471,7 +469,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
-    value = world * B * T / (ms / 1e3)
+    value = workloads.aggregate_rate(world, B * T, ms)
 
     # per-kernel device time of one more step (the same launches, not graph-captured)
     with tb.profile() as prof:

@@ -1,11 +1,14 @@
-"""Seeded synthetic workloads of the TCL4 path (input preparation on the device with torch).
+"""Seeded synthetic workloads of the TCL4 path, and the instance sharding across ranks.
 
 spin_boson_batch(): B spin-boson instances H = (eps sz + Delta sx)/2, A = sz with Ohmic
 baths J = alpha w exp(-w/wc); eps, Delta ~ U[0.5, 2], alpha ~ logU[0.01, 0.2],
-wc ~ U[1, 20], beta ~ logU[0.2, 5].  C(t) follows the KMS construction of
-cpp/include/taco/correlation_fft.hpp:153-214 and Gamma the trapezoid prefix integrals of
-cpp/include/taco/gamma.hpp:166-213, computed with torch on the GPU (setup only, not the
-measured path).
+wc ~ U[1, 20], beta ~ logU[0.2, 5].  C(t) (bcf_fft_fun, correlation_fft.hpp:153-214) and
+Gamma (trapezoid prefix integrals, gamma.hpp:166-213) are built by the library's own
+device kernels.
+
+Multi-GPU: the path shards over independent instances.  Rank r draws its own instances
+from seed + 1000 r (weak scaling: fixed work per rank), no data crosses ranks, and the
+step time is the maximum over ranks.
 """
 from __future__ import annotations
 
@@ -23,41 +26,45 @@ def draw_params(rng, B):
             for _ in range(B)]
 
 
-def gamma_device(torch, sysm, prm, N, dt, device):
-    """[nf, N+1] complex128 Gamma on `device` for an Ohmic bath."""
-    Nt = N + 1
-    nfft = 1 << (2 * Nt - 1).bit_length()
-    dw = 2 * math.pi / (dt * nfft)
-    wny = math.pi / dt
-    a, wc, beta = prm["alpha"], prm["wc"], prm["beta"]
-    k = torch.arange(1, nfft // 2, dtype=torch.float64, device=device)
-    w = dw * k
-    J = a * w * torch.exp(-w / wc)
-    r = math.exp(-beta * dw)
-    kms = torch.exp(-beta * dw * k)
-    sp = (math.pi / 2) * J / (1.0 - kms)
-    S = torch.zeros(nfft, dtype=torch.complex128, device=device)
-    S[1:nfft // 2] = sp.to(torch.complex128)
-    S[nfft // 2 + 1:] = torch.flip(sp * kms, [0]).to(torch.complex128)
-    S[0] = 0.5 * (math.pi / 2) * (a * dw * math.exp(-dw / wc)) * (1 + r) / (1 - r)
-    x = beta * wny  # coth(x/2) = 1 + 2/(e^x - 1); the term vanishes once e^x overflows
-    S[nfft // 2] = 0.25 * math.pi * (a * wny * math.exp(-wny / wc)) * (1 + (2 / math.expm1(x) if x < 700 else 0.0))
-    C = torch.fft.fft(S)[:Nt] * (dw / math.pi)
-    t = torch.arange(Nt, dtype=torch.float64, device=device) * dt
-    G = torch.zeros((sysm.nf, Nt), dtype=torch.complex128, device=device)
-    for b, om in enumerate(sysm.omegas):
-        y = torch.exp(1j * om * t) * C
-        G[b, 1:] = torch.cumsum(0.5 * dt * (y[:-1] + y[1:]), 0)
-    return G
+def rank_seed(seed: int, rank: int) -> int:
+    """Seed of rank `rank`'s instance set."""
+    return seed + 1000 * rank
+
+
+def max_over_ranks(dist, x: float, device) -> float:
+    """Maximum of a per-rank scalar (the step time) over all ranks; x itself on one rank."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, units_per_rank: int, ms_per_step: float) -> float:
+    """Whole-job throughput: the units all ranks processed per second of the slowest rank."""
+    return world * units_per_rank / (ms_per_step / 1e3)
+
+
+def gamma_device(sysm, prm, N, dt, device):
+    """[nf, N+1] complex128 Gamma on `device` for an Ohmic bath (device BCF + trapezoid)."""
+    from . import gamma_trapz_device
+    from .adjoint import bcf_device
+    C = bcf_device([dict(alpha=prm["alpha"], omega_c=prm["wc"], beta=prm["beta"], N=N, dt=dt)], N + 1, device)[0]
+    return gamma_trapz_device(C, dt, sysm.omegas)
+
+
+def spin_boson_systems(B, seed=0):
+    """-> (params, systems) for B seeded spin-boson instances (host only)."""
+    rng = np.random.default_rng(seed)
+    params = draw_params(rng, B)
+    systems = [System(0.5 * prm["eps"] * SZ + 0.5 * prm["delta"] * SX, [SZ]) for prm in params]
+    return params, systems
 
 
 def spin_boson_batch(torch, B, N=200000, dt=5e-4, seed=0, device="cuda"):
     """-> (params, systems, gammas) for B seeded instances."""
-    rng = np.random.default_rng(seed)
-    params = draw_params(rng, B)
-    systems, gammas = [], []
-    for prm in params:
-        s = System(0.5 * prm["eps"] * SZ + 0.5 * prm["delta"] * SX, [SZ])
-        systems.append(s)
-        gammas.append(gamma_device(torch, s, prm, N, dt, device))
+    del torch
+    params, systems = spin_boson_systems(B, seed)
+    gammas = [gamma_device(s, prm, N, dt, device) for s, prm in zip(systems, params)]
     return params, systems, gammas
