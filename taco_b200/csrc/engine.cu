@@ -269,6 +269,50 @@ void set_smem(K kernel, std::size_t bytes) {
     raise_smem_limit(reinterpret_cast<const void*>(kernel), bytes);
 }
 
+// FFT pass kernels with compile-time sizes for (log2 pass length, log2 tile count) with
+// pass length 2^7..2^10 and tiles of 2^10..2^12 elements (FFT lengths 2^14..2^20 under
+// the default and tuned schedules); the runtime-size kernels otherwise.
+template <class R>
+using ColFn = void (*)(const ColJob*, FftPlan<cplx_t<R>>, int);
+template <class R>
+using RowFn = void (*)(const RowJob*, FftPlan<cplx_t<R>>, int);
+template <class R>
+using InvFn = void (*)(const InvJob*, FftPlan<cplx_t<R>>, int);
+
+#define TACO_CT_CASES(X) \
+    X(7, 3) X(7, 4) X(7, 5) X(8, 2) X(8, 3) X(8, 4) X(9, 1) X(9, 2) X(9, 3) X(10, 0) X(10, 1) X(10, 2)
+
+template <class R>
+ColFn<R> fwd_col_fn(int l, int c) {
+    switch (l * 16 + c) {
+#define X(a, b) case a * 16 + b: return k_fwd_col_ct<R, a, b>;
+        TACO_CT_CASES(X)
+#undef X
+        default: return k_fwd_col<R>;
+    }
+}
+
+template <class R>
+InvFn<R> inv_col_fn(int l, int c) {
+    switch (l * 16 + c) {
+#define X(a, b) case a * 16 + b: return k_inv_col_ct<R, a, b>;
+        TACO_CT_CASES(X)
+#undef X
+        default: return k_inv_col<R>;
+    }
+}
+
+template <class R>
+RowFn<R> row_fn(int l, int c) {
+    switch (l * 16 + c) {
+#define X(a, b) case a * 16 + b: return k_row_ct<R, a, b>;
+        TACO_CT_CASES(X)
+#undef X
+        default: return k_row<R>;
+    }
+}
+#undef TACO_CT_CASES
+
 struct Geometry {
     int log2c, col_threads, log2r, row_threads;
     std::size_t col_smem, row_smem;
@@ -808,9 +852,12 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(meta)");
 
     // ---- launches ----
-    set_smem(k_fwd_col<R>, g.col_smem);
-    set_smem(k_inv_col<R>, g.col_smem);
-    set_smem(k_row<R>, g.row_smem);
+    const ColFn<R> fwd_col = fwd_col_fn<R>(plan.L1, g.log2c);
+    const InvFn<R> inv_col = inv_col_fn<R>(plan.L1, g.log2c);
+    const RowFn<R> row = row_fn<R>(plan.L2, g.log2r);
+    set_smem(fwd_col, g.col_smem);
+    set_smem(inv_col, g.col_smem);
+    set_smem(row, g.row_smem);
     int maxE = 0, maxS = 0;
     std::size_t maxNnz = 1;
     for (auto* u : units) {
@@ -883,22 +930,22 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         check_launch("k_conv_cluster", &pr);
     } else {
         pr.before(f32 ? "spectra_col_f32" : "spectra_col_f64");
-        k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(n_spec_jobs)), g.col_threads, g.col_smem, st>>>(
+        fwd_col<<<dim3(g.col_grid, static_cast<unsigned>(n_spec_jobs)), g.col_threads, g.col_smem, st>>>(
             Mc.colj, plan, g.log2c);
         check_launch("k_fwd_col(spectra)", &pr);
         pr.before(f32 ? "spectra_row_f32" : "spectra_row_f64");
-        k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
+        row<<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
             Mc.rowj, plan, g.log2r);
         check_launch("k_row(spectra)", &pr);
         const unsigned dft_grid = static_cast<unsigned>((N2 + INV_DFT_THREADS - 1) / INV_DFT_THREADS);
         for (std::size_t ch = 0; ch < nchunks; ++ch) {
             const std::size_t q0 = ch * Q, nq = std::min(Q, ntri - q0);
             pr.before(f32 ? "fwd_col_f32" : "fwd_col_f64");
-            k_fwd_col<R><<<dim3(g.col_grid, static_cast<unsigned>(nq)), g.col_threads, g.col_smem, st>>>(
+            fwd_col<<<dim3(g.col_grid, static_cast<unsigned>(nq)), g.col_threads, g.col_smem, st>>>(
                 Mc.colj + n_spec_jobs + q0, plan, g.log2c);
             check_launch("k_fwd_col", &pr);
             pr.before(f32 ? "row_conv_f32" : "row_conv_f64");
-            k_row<R><<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
+            row<<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
                 Mc.rowj + n_spec_jobs + q0, plan, g.log2r);
             check_launch("k_row", &pr);
             pr.before(f32 ? "inv_col_f32" : "inv_col_f64");
@@ -907,7 +954,7 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
                     Mc.invj + 2 * q0, plan, inv_rows);
                 check_launch("k_inv_col_dft", &pr);
             } else {
-                k_inv_col<R><<<dim3(g.col_grid, static_cast<unsigned>(2 * nq)), g.col_threads, g.col_smem, st>>>(
+                inv_col<<<dim3(g.col_grid, static_cast<unsigned>(2 * nq)), g.col_threads, g.col_smem, st>>>(
                     Mc.invj + 2 * q0, plan, g.log2c);
                 check_launch("k_inv_col", &pr);
             }

@@ -90,6 +90,9 @@ struct ScanJob {
     void* vr;
 };
 
+// Threads of a compile-time-size FFT tile (8 elements per thread).
+constexpr int ct_threads(int kl, int kc) { return kl >= 0 ? (1 << (kl + kc)) / 8 : 1024; }
+
 __device__ __forceinline__ double2 phase_minus(double omega, double dt, uint32_t t) {
     const double tk = static_cast<double>(t) * dt;  // t_k = k dt, then exp(-i omega t_k)
     double sn, cs;
@@ -100,29 +103,33 @@ __device__ __forceinline__ double2 phase_minus(double omega, double dt, uint32_t
 // ---------------------------------------------------------------- B1 -------
 // Column tile: 2^log2c columns n2_0 .. n2_0 + 2^log2c - 1, all N1 rows; element
 // (column c, row n1) at pad(n1 * 2^log2c + c).
-template <class R>
-__global__ void k_fwd_col(const ColJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2c) {
+// KL, KC >= 0: N1 = 2^KL and the tile width 2^KC fixed at compile time (-1: runtime).
+template <class R, int KL, int KC>
+__device__ __forceinline__ void fwd_col_body(const ColJob* __restrict__ jobs, const FftPlan<cplx_t<R>>& plan, int log2c_rt) {
     using C = cplx_t<R>;
+    constexpr bool CT = KL >= 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     const ColJob job = jobs[blockIdx.y];
+    const int L1 = CT ? KL : plan.L1;
+    const int log2c = CT ? KC : log2c_rt;
+    const int nthr = CT ? ((1 << (KL + KC)) / 8) : static_cast<int>(blockDim.x);
     const int N2 = 1 << plan.L2;
     const int ccols = 1 << log2c;
     const int n2_0 = blockIdx.x << log2c;
-    const int elems = ccols << plan.L1;
     const double2 shift = __ldg(&job.g[job.n_in - 1]);
-    // elems == 8 * blockDim.x: issue the 8 loads of a thread before using any of them
+    // (N1 << log2c) == 8 * threads: issue the 8 loads of a thread before using any of them
     double2 v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int idx = threadIdx.x + q * blockDim.x;
+        const int idx = threadIdx.x + q * nthr;
         const int n1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
         v[q] = t < job.n_in ? __ldg(&job.g[t]) : shift;
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int idx = threadIdx.x + q * blockDim.x;
+        const int idx = threadIdx.x + q * nthr;
         const int n1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
         double2 x = csub(v[q], shift);  // zero beyond n_in
@@ -131,12 +138,12 @@ __global__ void k_fwd_col(const ColJob* __restrict__ jobs, FftPlan<cplx_t<R>> pl
         s[pad_idx<C>(idx)] = from_d2<C>(x);
     }
     __syncthreads();
-    tile_fft<C, false, true>(s, plan.L1, log2c, 1, ccols, plan.tw1);
+    if constexpr (CT) tile_fft_ct<C, false, true, KL, KC>(s, plan.tw1);
+    else tile_fft<C, false, true>(s, L1, log2c, 1, ccols, plan.tw1);
     C* out = static_cast<C*>(job.out);
-    (void)elems;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int idx = threadIdx.x + q * blockDim.x;
+        const int idx = threadIdx.x + q * nthr;
         const int k1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t n2 = n2_0 + c;
         out[static_cast<size_t>(k1) * N2 + n2] =
@@ -148,21 +155,26 @@ __global__ void k_fwd_col(const ColJob* __restrict__ jobs, FftPlan<cplx_t<R>> pl
 // Row tile: 2^log2r rows of N2 elements, element (row r, i) at pad(r * N2 + i).
 // Forward row FFT; with spec_f set: two spectral products, inverse row FFTs and the
 // inverse inter-step twiddle.  Shared memory: two padded tiles.
-template <class R>
-__global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2r) {
+// KL, KC >= 0: N2 = 2^KL and 2^KC rows per tile fixed at compile time (-1: runtime).
+template <class R, int KL, int KC>
+__device__ __forceinline__ void row_body(const RowJob* __restrict__ jobs, const FftPlan<cplx_t<R>>& plan, int log2r_rt) {
     using C = cplx_t<R>;
+    constexpr bool CT = KL >= 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N2 = 1 << plan.L2;
+    const int L2 = CT ? KL : plan.L2;
+    const int log2r = CT ? KC : log2r_rt;
+    const int nthr = CT ? ((1 << (KL + KC)) / 8) : static_cast<int>(blockDim.x);
+    const int N2 = 1 << L2;
     const int elems = N2 << log2r;
     C* a = reinterpret_cast<C*>(smem_raw);
     C* p = a + padded_size<C>(elems);
     const RowJob job = jobs[blockIdx.y];
     const size_t off = static_cast<size_t>(blockIdx.x) * elems;
     C* data = static_cast<C*>(job.data) + off;
-    // elems == 8 * blockDim.x: 8 loads per thread in flight at once
+    // elems == 8 * threads: 8 loads per thread in flight at once
     C x[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) x[q] = data[threadIdx.x + q * blockDim.x];
+    for (int q = 0; q < 8; ++q) x[q] = data[threadIdx.x + q * nthr];
     const bool conv = job.spec_f != nullptr;
     // the partner spectra arrive while the forward transform runs
     C sf[8], sc[8];
@@ -171,18 +183,19 @@ __global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, 
         const C* spc = static_cast<const C*>(job.spec_c) + off;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            sf[q] = __ldg(&spf[threadIdx.x + q * blockDim.x]);
-            sc[q] = __ldg(&spc[threadIdx.x + q * blockDim.x]);
+            sf[q] = __ldg(&spf[threadIdx.x + q * nthr]);
+            sc[q] = __ldg(&spc[threadIdx.x + q * nthr]);
         }
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) a[pad_idx<C>(threadIdx.x + q * blockDim.x)] = x[q];
+    for (int q = 0; q < 8; ++q) a[pad_idx<C>(threadIdx.x + q * nthr)] = x[q];
     __syncthreads();
-    tile_fft<C, false, false>(a, plan.L2, log2r, N2, 1, plan.tw2);
+    if constexpr (CT) tile_fft_ct<C, false, false, KL, KC>(a, plan.tw2);
+    else tile_fft<C, false, false>(a, L2, log2r, N2, 1, plan.tw2);
     if (!conv) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const int idx = threadIdx.x + q * blockDim.x;
+            const int idx = threadIdx.x + q * nthr;
             data[idx] = a[pad_idx<C>(idx)];
         }
         return;
@@ -191,16 +204,17 @@ __global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, 
     for (int which = 0; which < 2; ++which) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const int idx = threadIdx.x + q * blockDim.x;
+            const int idx = threadIdx.x + q * nthr;
             p[pad_idx<C>(idx)] = cmul(a[pad_idx<C>(idx)], which == 0 ? sf[q] : sc[q]);
         }
         __syncthreads();
-        tile_fft<C, true, false>(p, plan.L2, log2r, N2, 1, plan.tw2);
+        if constexpr (CT) tile_fft_ct<C, true, false, KL, KC>(p, plan.tw2);
+        else tile_fft<C, true, false>(p, L2, log2r, N2, 1, plan.tw2);
         C* dst = (which == 0 ? data : static_cast<C*>(job.wc) + off);
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const int idx = threadIdx.x + q * blockDim.x;
-            const int r = idx >> plan.L2, n2 = idx & (N2 - 1);
+            const int idx = threadIdx.x + q * nthr;
+            const int r = idx >> L2, n2 = idx & (N2 - 1);
             const uint32_t k1 = static_cast<uint32_t>(k1_0 + r);
             dst[idx] = cmulc(p[pad_idx<C>(idx)], inter_twiddle(plan, static_cast<uint32_t>(n2) * k1));
         }
@@ -209,38 +223,71 @@ __global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, 
 }
 
 // ---------------------------------------------------------------- B3 -------
-template <class R>
-__global__ void k_inv_col(const InvJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2c) {
+template <class R, int KL, int KC>
+__device__ __forceinline__ void inv_col_body(const InvJob* __restrict__ jobs, const FftPlan<cplx_t<R>>& plan, int log2c_rt) {
     using C = cplx_t<R>;
+    constexpr bool CT = KL >= 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     const InvJob job = jobs[blockIdx.y];
+    const int L1 = CT ? KL : plan.L1;
+    const int log2c = CT ? KC : log2c_rt;
+    const int nthr = CT ? ((1 << (KL + KC)) / 8) : static_cast<int>(blockDim.x);
     const int N2 = 1 << plan.L2;
     const int ccols = 1 << log2c;
     const int n2_0 = blockIdx.x << log2c;
-    const int elems = ccols << plan.L1;
     const C* w = static_cast<const C*>(job.w);
-    (void)elems;
     C x[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int idx = threadIdx.x + q * blockDim.x;
+        const int idx = threadIdx.x + q * nthr;
         const int k1 = idx >> log2c, c = idx & (ccols - 1);
         x[q] = w[static_cast<size_t>(k1) * N2 + n2_0 + c];
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) s[pad_idx<C>(threadIdx.x + q * blockDim.x)] = x[q];
+    for (int q = 0; q < 8; ++q) s[pad_idx<C>(threadIdx.x + q * nthr)] = x[q];
     __syncthreads();
-    tile_fft<C, true, true>(s, plan.L1, log2c, 1, ccols, plan.tw1);
+    if constexpr (CT) tile_fft_ct<C, true, true, KL, KC>(s, plan.tw1);
+    else tile_fft<C, true, true>(s, L1, log2c, 1, ccols, plan.tw1);
     C* out = static_cast<C*>(job.out);
     const R scale = static_cast<R>(job.scale);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int idx = threadIdx.x + q * blockDim.x;
+        const int idx = threadIdx.x + q * nthr;
         const int n1 = idx >> log2c, c = idx & (ccols - 1);
         const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
         if (t < job.t_count) out[t] = cscale(s[pad_idx<C>(idx)], scale);
     }
+}
+
+// Kernels: runtime sizes (k_fwd_col, k_row, k_inv_col) and compile-time sizes (the _ct
+// variants, bounded to two CTAs per SM).
+template <class R>
+__global__ void k_fwd_col(const ColJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2c) {
+    fwd_col_body<R, -1, -1>(jobs, plan, log2c);
+}
+template <class R>
+__global__ void k_row(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2r) {
+    row_body<R, -1, -1>(jobs, plan, log2r);
+}
+template <class R>
+__global__ void k_inv_col(const InvJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan, int log2c) {
+    inv_col_body<R, -1, -1>(jobs, plan, log2c);
+}
+template <class R, int KL, int KC>
+__global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ? 1 : 2) k_fwd_col_ct(const ColJob* __restrict__ jobs,
+                                                                       FftPlan<cplx_t<R>> plan, int log2c) {
+    fwd_col_body<R, KL, KC>(jobs, plan, log2c);
+}
+template <class R, int KL, int KC>
+__global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ? 1 : 2) k_row_ct(const RowJob* __restrict__ jobs,
+                                                                   FftPlan<cplx_t<R>> plan, int log2r) {
+    row_body<R, KL, KC>(jobs, plan, log2r);
+}
+template <class R, int KL, int KC>
+__global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ? 1 : 2) k_inv_col_ct(const InvJob* __restrict__ jobs,
+                                                                       FftPlan<cplx_t<R>> plan, int log2c) {
+    inv_col_body<R, KL, KC>(jobs, plan, log2c);
 }
 
 // Pruned inverse column pass for t_count <= MAXR * N2: only rows n1 < nrows of the

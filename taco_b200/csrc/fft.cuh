@@ -149,4 +149,69 @@ __device__ void tile_fft(C* s, int log2n, int log2nfft, int fs, int es, const C*
     }
 }
 
+// ---- compile-time sizes -------------------------------------------------------
+// The same Stockham stages with the transform length, the tile count and the strides
+// known at compile time (fs = 1, es = 2^LOG2NFFT for column tiles; fs = 2^LOG2N, es = 1
+// for row tiles), so that the index arithmetic folds into constants and the stage loop
+// unrolls.  Used for the FFT lengths of the measured configurations.
+template <class C, int LR, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT, int P>
+__device__ __forceinline__ void stockham_stage_ct(C* s, const C* __restrict__ tw) {
+    constexpr int RAD = 1 << LR;
+    constexpr int ITEMS = 8 / RAD;
+    constexpr int n = 1 << LOG2N;
+    constexpr int lq = LOG2N - LR;
+    constexpr int fs = F_FAST ? 1 : n;
+    constexpr int es = F_FAST ? (1 << LOG2NFFT) : 1;
+    C x[8];
+    int base[ITEMS], jout[ITEMS];
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+        const int g = threadIdx.x * ITEMS + q;
+        int f, i;
+        if (F_FAST) {
+            f = g & ((1 << LOG2NFFT) - 1);
+            i = g >> LOG2NFFT;
+        } else {
+            f = g >> lq;
+            i = g & ((1 << lq) - 1);
+        }
+        const int k = i & (P - 1);
+        base[q] = f * fs;
+        jout[q] = ((i - k) << LR) + k;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) x[q * RAD + r] = s[pad_idx<C>(base[q] + (i + (r << lq)) * es)];
+        if (P > 1) {
+            constexpr int st = n / (P * RAD);
+            const int stride = st * k;
+#pragma unroll
+            for (int r = 1; r < RAD; ++r) x[q * RAD + r] = mul_w<C, INV>(x[q * RAD + r], __ldg(&tw[r * stride]));
+        }
+        if (RAD == 8) dft8<C, INV>(&x[q * RAD]);
+        else if (RAD == 4) dft4<C, INV>(x[q * RAD], x[q * RAD + 1], x[q * RAD + 2], x[q * RAD + 3]);
+        else dft2<C, INV>(x[q * RAD], x[q * RAD + 1]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) s[pad_idx<C>(base[q] + (jout[q] + r * P) * es)] = x[q * RAD + r];
+    }
+    __syncthreads();
+}
+
+template <class C, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT, int P, int REM>
+__device__ __forceinline__ void stages_ct(C* s, const C* __restrict__ tw) {
+    if constexpr (REM > 0) {
+        constexpr int LR = (P == 1 && REM % 3 == 2) ? 2 : ((P == 1 && REM % 3 == 1) ? 1 : 3);
+        stockham_stage_ct<C, LR, INV, F_FAST, LOG2N, LOG2NFFT, P>(s, tw);
+        stages_ct<C, INV, F_FAST, LOG2N, LOG2NFFT, (P << LR), REM - LR>(s, tw);
+    }
+}
+
+// tile_fft with compile-time sizes: the same stage sequence (radix 4 or 2 first, then 8).
+template <class C, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT>
+__device__ __forceinline__ void tile_fft_ct(C* s, const C* __restrict__ tw) {
+    stages_ct<C, INV, F_FAST, LOG2N, LOG2NFFT, 1, LOG2N>(s, tw);
+}
+
 }  // namespace taco
