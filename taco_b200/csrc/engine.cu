@@ -914,6 +914,9 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
             d2h.push_back({fcr_out[kind], P.v[0] + kind * nf3 * U, nf3 * U * sizeof(C)});
     }
     const std::size_t n_scan = ntri;
+    // single-pass scan (one CTA per triple) once the triples alone fill the GPU four times
+    // over; the chunked reduce-then-scan otherwise
+    const bool scan_single = n_scan >= static_cast<std::size_t>(148 * 2 * 4);
     const MetaPtrs Mc = M;
     const WorkPtrs<C> Pc = P;
     return [=](cudaStream_t st, ProfRecorder* prp, cudaEvent_t ev0, cudaEvent_t ev1) {
@@ -960,7 +963,13 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
             }
         }
     }
-    for (std::size_t s0 = 0; s0 < n_scan; s0 += 65535) {
+    if (scan_single) {
+        // enough triples to fill the GPU: one CTA per triple walks its whole time axis
+        pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
+        k_scan_assemble<R><<<static_cast<unsigned>(n_scan), SCAN_THREADS, 0, st>>>(Mc.scanj);
+        check_launch("k_scan_assemble", &pr);
+    }
+    for (std::size_t s0 = 0; !scan_single && s0 < n_scan; s0 += 65535) {
         const unsigned ns = static_cast<unsigned>(std::min<std::size_t>(65535, n_scan - s0));
         pr.before(f32 ? "scan_reduce_f32" : "scan_reduce_f64");
         k_scan_reduce<R><<<dim3(static_cast<unsigned>(max_chunks), ns), SCAN_THREADS, 0, st>>>(

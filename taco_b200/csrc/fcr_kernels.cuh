@@ -127,14 +127,30 @@ __device__ __forceinline__ void fwd_col_body(const ColJob* __restrict__ jobs, co
         const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
         v[q] = t < job.n_in ? __ldg(&job.g[t]) : shift;
     }
+    // when the tile is at most nthr columns wide, a thread's 8 samples are equally spaced
+    // in t (stride nthr / ccols rows): phases by recurrence from the first
+    const bool spaced = nthr >= ccols;
+    const uint32_t t_first = static_cast<uint32_t>(threadIdx.x >> log2c) * N2 + n2_0 + (threadIdx.x & (ccols - 1));
+    const uint32_t t_step = static_cast<uint32_t>(nthr >> log2c) * N2;
+    double2 ph = make_double2(1.0, 0.0), ph_step = ph;
+    if (job.has_phase && spaced) {
+        ph = phase_minus(job.omega, job.dt, t_first);
+        ph_step = phase_minus(job.omega, job.dt, t_step);
+    }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const int idx = threadIdx.x + q * nthr;
-        const int n1 = idx >> log2c, c = idx & (ccols - 1);
-        const uint32_t t = static_cast<uint32_t>(n1) * N2 + n2_0 + c;
         double2 x = csub(v[q], shift);  // zero beyond n_in
         if (job.conj) x.y = -x.y;
-        if (job.has_phase && t < job.n_in) x = cmul(x, phase_minus(job.omega, job.dt, t));
+        if (job.has_phase) {
+            if (spaced) {
+                x = cmul(x, ph);
+                ph = cmul(ph, ph_step);
+            } else {
+                const uint32_t t = static_cast<uint32_t>(idx >> log2c) * N2 + n2_0 + (idx & (ccols - 1));
+                x = cmul(x, phase_minus(job.omega, job.dt, t));
+            }
+        }
         s[pad_idx<C>(idx)] = from_d2<C>(x);
     }
     __syncthreads();
@@ -366,6 +382,7 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_assemble(const ScanJob
     const double2 cmj = __ldg(&job.gmj[job.n_in - 1]);
     const double2 cj = __ldg(&job.gj[job.n_in - 1]);
     const double dt = job.dt;
+    const double2 step = phase_minus(job.omega, dt, 1);  // e^{-i w dt}: phases by recurrence over a thread's samples
     const uint32_t tile = SCAN_THREADS * SCAN_ITEMS;
     __syncthreads();
     for (uint32_t t0 = 0; t0 < job.t_count; t0 += tile) {
@@ -373,14 +390,19 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_assemble(const ScanJob
         double run[SCAN_W];
 #pragma unroll
         for (int k = 0; k < SCAN_W; ++k) run[k] = 0.0;
+        const double2 pm0 = phase_minus(job.omega, dt, tb);
+        {
+            double2 pm = pm0;
 #pragma unroll
-        for (int q = 0; q < SCAN_ITEMS; ++q) {
-            const uint32_t t = tb + q;
-            if (t < job.t_count) {
-                double v[SCAN_W];
-                scan_integrands(job, t, ci, phase_minus(job.omega, dt, t), __ldg(&job.gi[t]), v);
+            for (int q = 0; q < SCAN_ITEMS; ++q) {
+                const uint32_t t = tb + q;
+                if (t < job.t_count) {
+                    double v[SCAN_W];
+                    scan_integrands(job, t, ci, pm, __ldg(&job.gi[t]), v);
 #pragma unroll
-                for (int k = 0; k < SCAN_W; ++k) run[k] += v[k];
+                    for (int k = 0; k < SCAN_W; ++k) run[k] += v[k];
+                }
+                pm = cmul(pm, step);
             }
         }
         // block-exclusive prefix of the per-thread sums
@@ -404,11 +426,11 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_assemble(const ScanJob
             for (int q = 0; q < warp; ++q) w += warp_tot[q][k];
             pre[k] = carry[k] + (w + pre[k]);
         }
+        double2 pm = pm0;
 #pragma unroll
-        for (int q = 0; q < SCAN_ITEMS; ++q) {
+        for (int q = 0; q < SCAN_ITEMS; ++q, pm = cmul(pm, step)) {
             const uint32_t t = tb + q;
             if (t >= job.t_count) break;
-            const double2 pm = phase_minus(job.omega, dt, t);
             const double2 gi = __ldg(&job.gi[t]);
             double v[SCAN_W];
             scan_integrands(job, t, ci, pm, gi, v);
@@ -468,12 +490,14 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_reduce(const ScanJob* 
 #pragma unroll
     for (int k = 0; k < SCAN_W; ++k) run[k] = 0.0;
     const uint32_t tb = t0 + threadIdx.x * SCAN_ITEMS;
+    const double2 step = phase_minus(job.omega, job.dt, 1);
+    double2 pm = phase_minus(job.omega, job.dt, tb);
 #pragma unroll
-    for (int q = 0; q < SCAN_ITEMS; ++q) {
+    for (int q = 0; q < SCAN_ITEMS; ++q, pm = cmul(pm, step)) {
         const uint32_t t = tb + q;
         if (t < job.t_count) {
             double v[SCAN_W];
-            scan_integrands(job, t, ci, phase_minus(job.omega, job.dt, t), __ldg(&job.gi[t]), v);
+            scan_integrands(job, t, ci, pm, __ldg(&job.gi[t]), v);
 #pragma unroll
             for (int k = 0; k < SCAN_W; ++k) run[k] += v[k];
         }
@@ -513,17 +537,22 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_chunks(const ScanJob* 
     const double2 cj = __ldg(&job.gj[job.n_in - 1]);
     const double dt = job.dt;
     const uint32_t tb = t0 + threadIdx.x * SCAN_ITEMS;
+    const double2 step = phase_minus(job.omega, dt, 1);  // e^{-i w dt}: phases by recurrence over a thread's samples
+    const double2 pm0 = phase_minus(job.omega, dt, tb);
     double run[SCAN_W];
 #pragma unroll
     for (int k = 0; k < SCAN_W; ++k) run[k] = 0.0;
+    {
+        double2 pm = pm0;
 #pragma unroll
-    for (int q = 0; q < SCAN_ITEMS; ++q) {
-        const uint32_t t = tb + q;
-        if (t < job.t_count) {
-            double v[SCAN_W];
-            scan_integrands(job, t, ci, phase_minus(job.omega, dt, t), __ldg(&job.gi[t]), v);
+        for (int q = 0; q < SCAN_ITEMS; ++q, pm = cmul(pm, step)) {
+            const uint32_t t = tb + q;
+            if (t < job.t_count) {
+                double v[SCAN_W];
+                scan_integrands(job, t, ci, pm, __ldg(&job.gi[t]), v);
 #pragma unroll
-            for (int k = 0; k < SCAN_W; ++k) run[k] += v[k];
+                for (int k = 0; k < SCAN_W; ++k) run[k] += v[k];
+            }
         }
     }
     double pre[SCAN_W];
@@ -546,11 +575,11 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_chunks(const ScanJob* 
         for (int q = 0; q < warp; ++q) w += warp_tot[q][k];
         pre[k] = carry[k] + (w + pre[k]);
     }
+    double2 pm = pm0;
 #pragma unroll
-    for (int q = 0; q < SCAN_ITEMS; ++q) {
+    for (int q = 0; q < SCAN_ITEMS; ++q, pm = cmul(pm, step)) {
         const uint32_t t = tb + q;
         if (t >= job.t_count) break;
-        const double2 pm = phase_minus(job.omega, dt, t);
         const double2 gi = __ldg(&job.gi[t]);
         double v[SCAN_W];
         scan_integrands(job, t, ci, pm, gi, v);
