@@ -61,31 +61,45 @@ def candidates(precision: str):
             for c, r, b, d in itertools.product(cols, rows, chunks, dft)]
 
 
-def tune(run, log2_nfft: int, precision: str, cands=None, reps: int = 3, warmup: int = 1, log=None):
-    """run(): one timed unit of work (e.g. a batched build).  Returns (best, results)."""
+def _time(log2_nfft, precision, sch, run, factory, reps, warmup, log):
+    """Device time of one unit of work under schedule `sch` (inf when the schedule fails)."""
     import torch
 
+    unit = None
+    try:
+        set_schedule(log2_nfft, precision, **sch)
+        unit = factory() if factory is not None else run
+        for _ in range(warmup):
+            unit()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            unit()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+    except _capi.TacoError as exc:  # e.g. a tile that does not fit shared memory
+        ms = float("inf")
+        if log:
+            log(f"schedule {sch} failed: {exc}")
+    finally:
+        if unit is not None and hasattr(unit, "close"):
+            unit.close()
+    if log:
+        log(f"{precision} 2^{log2_nfft} {sch} -> {ms:.3f} ms")
+    return ms
+
+
+def tune(run, log2_nfft: int, precision: str, cands=None, reps: int = 3, warmup: int = 1, log=None, factory=None):
+    """Times one unit of work under every candidate schedule and keeps the fastest.
+
+    run(): the unit (e.g. a batched build); or factory(): called after each schedule is
+    set, returns the unit (e.g. a prepared plan's replay, with a close()).  Returns
+    (best, results)."""
     results = []
     for sch in cands or candidates(precision):
-        try:
-            set_schedule(log2_nfft, precision, **sch)
-            for _ in range(warmup):
-                run()
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
-                run()
-            e1.record()
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-        except _capi.TacoError as exc:  # e.g. a tile that does not fit shared memory
-            ms = float("inf")
-            if log:
-                log(f"schedule {sch} failed: {exc}")
-        results.append((ms, sch))
-        if log:
-            log(f"{precision} 2^{log2_nfft} {sch} -> {ms:.3f} ms")
+        results.append((_time(log2_nfft, precision, sch, run, factory, reps, warmup, log), sch))
     results.sort(key=lambda x: x[0])
     best = dict(results[0][1])
     # phase 2: the thread-block-cluster path (points per CTA), with the best multi-pass tiles
@@ -94,25 +108,7 @@ def tune(run, log2_nfft: int, precision: str, cands=None, reps: int = 3, warmup:
         if lm > lm_max or log2_nfft - lm > 3 or lm > log2_nfft:
             continue
         sch = dict(best, cluster_lm=lm)
-        try:
-            set_schedule(log2_nfft, precision, **sch)
-            for _ in range(warmup):
-                run()
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
-                run()
-            e1.record()
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-        except _capi.TacoError as exc:
-            ms = float("inf")
-            if log:
-                log(f"schedule {sch} failed: {exc}")
-        results.append((ms, sch))
-        if log:
-            log(f"{precision} 2^{log2_nfft} {sch} -> {ms:.3f} ms")
+        results.append((_time(log2_nfft, precision, sch, run, factory, reps, warmup, log), sch))
     results.sort(key=lambda x: x[0])
     best = dict(results[0][1])
     best.setdefault("cluster_lm", 0)
@@ -130,6 +126,21 @@ def save(entries: dict, path: str = DEFAULT_TABLE, note: str = "") -> None:
         table["_note"] = note
     with open(path, "w") as f:
         json.dump(table, f, indent=1, sort_keys=True)
+
+
+class _Plans:
+    """Replays of prepared plans as one unit of work."""
+
+    def __init__(self, plans):
+        self.plans = plans
+
+    def __call__(self):
+        for p in self.plans:
+            p.run()
+
+    def close(self):
+        for p in self.plans:
+            p.close()
 
 
 def main():
@@ -161,15 +172,14 @@ def main():
             dtype = torch.complex64 if prec == "fp32" else torch.complex128
             outs = [torch.empty((T, 16), dtype=dtype, device="cuda") for _ in systems]
             inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
-            if prec == "fp64":  # the plain path runs one instance per call
-                def run():
-                    for k in range(min(4, len(inst))):
-                        tb.build_TCL4_generator_batch(inst[k][0], inst[k][1], args.dt, tidx, precision="fp64",
-                                                      out=outs[k], full_length=full)
-            else:
-                def run():
-                    tb.build_instances(inst, precision=prec, outs=outs, full_length=full)
-            best, res = tune(run, L, prec, log=print)
+            if prec == "fp64":  # the plain path: one instance per plan
+                def factory():
+                    return _Plans([tb.Tcl4Plan([inst[k]], precision="fp64", outs=[outs[k]], full_length=full)
+                                   for k in range(min(4, len(inst)))])
+            else:  # the batched path: one plan over every instance
+                def factory():
+                    return _Plans([tb.Tcl4Plan(inst, precision=prec, outs=outs, full_length=full)])
+            best, res = tune(None, L, prec, log=print, factory=factory)
             entries[f"{L}:{prec}"] = dict(best, ms=res[0][0])
     save(entries, args.out, note="measured on B200 by taco_b200.autotune (C2-shaped spin-boson batch)")
     print(json.dumps(entries))
