@@ -334,6 +334,18 @@ Geometry geometry(const FftPlan<C>& p, int col_tile, int row_tile) {
     g.log2r = ilog2(static_cast<std::size_t>(rr));
     g.row_threads = (N2 << g.log2r) / 8;
     g.row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << g.log2r)) * sizeof(C);
+    constexpr std::size_t kSmemMax = 227 * 1024;
+    while (g.row_smem > kSmemMax && g.log2r > 0) {  // explicit schedules too large for one CTA
+        --g.log2r;
+        g.row_threads = (N2 << g.log2r) / 8;
+        g.row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << g.log2r)) * sizeof(C);
+    }
+    while (g.col_smem > kSmemMax && g.log2c > 0) {
+        --g.log2c;
+        g.col_threads = (N1 << g.log2c) / 8;
+        g.col_smem = static_cast<std::size_t>(padded_size<C>(N1 << g.log2c)) * sizeof(C);
+    }
+    g.col_grid = static_cast<unsigned>(N2 >> g.log2c);
     g.row_grid = static_cast<unsigned>(N1 >> g.log2r);
     return g;
 }

@@ -154,15 +154,15 @@ __device__ void tile_fft(C* s, int log2n, int log2nfft, int fs, int es, const C*
 // known at compile time (fs = 1, es = 2^LOG2NFFT for column tiles; fs = 2^LOG2N, es = 1
 // for row tiles), so that the index arithmetic folds into constants and the stage loop
 // unrolls.  Used for the FFT lengths of the measured configurations.
-template <class C, int LR, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT, int P>
+template <class C, int LR, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT, int P, int EPT>
 __device__ __forceinline__ void stockham_stage_ct(C* s, const C* __restrict__ tw) {
     constexpr int RAD = 1 << LR;
-    constexpr int ITEMS = 8 / RAD;
+    constexpr int ITEMS = EPT / RAD;
     constexpr int n = 1 << LOG2N;
     constexpr int lq = LOG2N - LR;
     constexpr int fs = F_FAST ? 1 : n;
     constexpr int es = F_FAST ? (1 << LOG2NFFT) : 1;
-    C x[8];
+    C x[EPT];
     int base[ITEMS], jout[ITEMS];
 #pragma unroll
     for (int q = 0; q < ITEMS; ++q) {
@@ -199,19 +199,20 @@ __device__ __forceinline__ void stockham_stage_ct(C* s, const C* __restrict__ tw
     __syncthreads();
 }
 
-template <class C, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT, int P, int REM>
+template <class C, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT, int P, int REM, int EPT>
 __device__ __forceinline__ void stages_ct(C* s, const C* __restrict__ tw) {
     if constexpr (REM > 0) {
         constexpr int LR = (P == 1 && REM % 3 == 2) ? 2 : ((P == 1 && REM % 3 == 1) ? 1 : 3);
-        stockham_stage_ct<C, LR, INV, F_FAST, LOG2N, LOG2NFFT, P>(s, tw);
-        stages_ct<C, INV, F_FAST, LOG2N, LOG2NFFT, (P << LR), REM - LR>(s, tw);
+        stockham_stage_ct<C, LR, INV, F_FAST, LOG2N, LOG2NFFT, P, EPT>(s, tw);
+        stages_ct<C, INV, F_FAST, LOG2N, LOG2NFFT, (P << LR), REM - LR, EPT>(s, tw);
     }
 }
 
 // tile_fft with compile-time sizes: the same stage sequence (radix 4 or 2 first, then 8).
-template <class C, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT>
+// EPT elements per thread (8, or 16 for a tile of twice the transforms on the same threads).
+template <class C, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT, int EPT = 8>
 __device__ __forceinline__ void tile_fft_ct(C* s, const C* __restrict__ tw) {
-    stages_ct<C, INV, F_FAST, LOG2N, LOG2NFFT, 1, LOG2N>(s, tw);
+    stages_ct<C, INV, F_FAST, LOG2N, LOG2NFFT, 1, LOG2N, EPT>(s, tw);
 }
 
 }  // namespace taco
