@@ -291,7 +291,7 @@ __global__ void k_inv_col(const InvJob* __restrict__ jobs, FftPlan<cplx_t<R>> pl
     inv_col_body<R, -1, -1>(jobs, plan, log2c);
 }
 template <class R, int KL, int KC>
-__global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ? 1 : 2) k_fwd_col_ct(const ColJob* __restrict__ jobs,
+__global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ? 1 : 3) k_fwd_col_ct(const ColJob* __restrict__ jobs,
                                                                        FftPlan<cplx_t<R>> plan, int log2c) {
     fwd_col_body<R, KL, KC>(jobs, plan, log2c);
 }
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ?
     row_body<R, KL, KC>(jobs, plan, log2r);
 }
 template <class R, int KL, int KC>
-__global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ? 1 : 2) k_inv_col_ct(const InvJob* __restrict__ jobs,
+__global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ? 1 : 3) k_inv_col_ct(const InvJob* __restrict__ jobs,
                                                                        FftPlan<cplx_t<R>> plan, int log2c) {
     inv_col_body<R, KL, KC>(jobs, plan, log2c);
 }
@@ -366,7 +366,7 @@ __device__ __forceinline__ void scan_integrands(const ScanJob& job, uint32_t t, 
 // the integrands (cheaper than keeping them live: it doubles the occupancy) and
 // assembles F, C, R at the requested times.
 template <class R>
-__global__ void __launch_bounds__(SCAN_THREADS, 2) k_scan_assemble(const ScanJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(SCAN_THREADS, 3) k_scan_assemble(const ScanJob* __restrict__ jobs) {
     using C = cplx_t<R>;
     __shared__ double warp_tot[SCAN_THREADS / 32][SCAN_W];
     __shared__ double carry[SCAN_W];
