@@ -246,6 +246,17 @@ int taco_profile_enable(int on);
 int taco_profile_reset(void);
 int taco_profile_get(size_t index, const char** name, uint64_t* launches, double* total_ms, size_t* count);
 
+/* Batched trapezoid Gamma on device arrays: C [N], G [M][N] per request (omegas on the host). */
+typedef struct {
+    const taco_c128* C;
+    size_t N;
+    double dt;
+    const double* omegas;
+    size_t M;
+    taco_c128* G;
+} taco_gamma_request;
+int taco_gamma_trapz_batch(const taco_gamma_request* reqs, size_t n, void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Bath correlation function on the device: bcf_fft_fun (cpp/include/taco/correlation_fft.hpp:153-214)
  * for J(w) = alpha w e^{-w/omega_c} (+ 2 lambda gamma w / (w^2 + gamma^2) when model = 1), and

@@ -40,7 +40,7 @@ __all__ = [
     "build_TCL4_generator", "build_TCL4_generator_batch", "build_correction_series", "build_instances",
     "propagate_rk4_dense", "l4_coefficients", "Tcl4Plan", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
     "version", "device_count", "kernel_launches", "profile", "tcl2_generator_series", "gamma_trapz_device",
-    "propagate_tcl", "set_work_budget", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
+    "propagate_tcl", "gamma_trapz_device_batch", "set_work_budget", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
 ]
 
 
@@ -400,6 +400,26 @@ def gamma_trapz_device(C, dt: float, omegas):
     _capi.check(_capi.lib().taco_gamma_trapz(_ptr(c), c.shape[0], float(dt), _ptr(om), om.size, _ptr(out), flags,
                                              _stream_ptr(c)))
     return out
+
+
+def gamma_trapz_device_batch(Cs, dts, omegas_list):
+    """gamma_trapz_device for many correlation functions in one pair of launches: Cs are
+    complex128 CUDA tensors [N_k]; returns the list of [nb_k, N_k] tensors."""
+    torch = _torch()
+    cs = [c.to(torch.complex128).contiguous() for c in Cs]
+    oms = [np.ascontiguousarray(o, np.float64) for o in omegas_list]
+    outs = [torch.empty((o.size, c.shape[0]), dtype=torch.complex128, device=c.device) for c, o in zip(cs, oms)]
+    reqs = (_capi.GammaRequest * len(cs))()
+    for k, (c, dt, o, g) in enumerate(zip(cs, dts, oms, outs)):
+        reqs[k].C = c.data_ptr()
+        reqs[k].N = c.shape[0]
+        reqs[k].dt = float(dt)
+        reqs[k].omegas = o.ctypes.data
+        reqs[k].M = o.size
+        reqs[k].G = g.data_ptr()
+    if cs:
+        _capi.check(_capi.lib().taco_gamma_trapz_batch(reqs, len(cs), _stream_ptr(cs[0])))
+    return outs
 
 
 def propagate_tcl(system: System, gamma, dt: float, steps: int, rho0, obs=None, order: int = 4,

@@ -38,7 +38,7 @@ EXPORTED = [
     "taco_tcl4_build_batch_noalloc", "taco_tcl2_generator_series", "taco_gamma_trapz", "taco_propagate_tcl",
     "taco_build_mikx", "taco_assemble_liouvillian", "taco_gw_to_liouvillian",
     "taco_bcf_fft", "taco_rk4_forward_checkpointed", "taco_rk4_adjoint", "taco_tcl4_adjoint",
-    "taco_tcl2_adjoint", "taco_inner_re", "taco_set_work_budget",
+    "taco_tcl2_adjoint", "taco_inner_re", "taco_set_work_budget", "taco_gamma_trapz_batch",
 ]
 
 
@@ -99,6 +99,11 @@ class Tcl2AdjointJob(ct.Structure):
     _fields_ = [("sys", ct.POINTER(SystemView)), ("eps", ct.c_void_p), ("gamma", ct.c_void_p), ("T", ct.c_size_t),
                 ("L_bar", ct.c_void_p), ("gamma_bar", ct.c_void_p), ("ops_bar", ct.c_void_p),
                 ("eps_bar", ct.c_void_p)]
+
+
+class GammaRequest(ct.Structure):
+    _fields_ = [("C", ct.c_void_p), ("N", ct.c_size_t), ("dt", ct.c_double), ("omegas", ct.c_void_p),
+                ("M", ct.c_size_t), ("G", ct.c_void_p)]
 
 
 class InnerJob(ct.Structure):
@@ -165,6 +170,7 @@ def lib():
                                                 ct.c_void_p]
         L.taco_gw_to_liouvillian.argtypes = [ct.c_void_p, ct.c_int, ct.c_size_t, ct.c_void_p, ct.c_int, ct.c_void_p]
         L.taco_set_work_budget.argtypes = [ct.c_size_t]
+        L.taco_gamma_trapz_batch.argtypes = [ct.POINTER(GammaRequest), ct.c_size_t, ct.c_void_p]
         L.taco_bcf_fft.argtypes = [ct.POINTER(BcfRequest), ct.c_size_t, ct.c_int, ct.c_void_p]
         L.taco_rk4_forward_checkpointed.argtypes = [ct.POINTER(Rk4GradJob), ct.c_size_t, ct.c_size_t, ct.c_void_p]
         L.taco_rk4_adjoint.argtypes = [ct.POINTER(Rk4GradJob), ct.c_size_t, ct.c_size_t, ct.c_void_p]

@@ -292,7 +292,7 @@ def _systems(params, cfg):
 
 def spin_boson_forward(params, cfg: SpinBosonConfig, device="cuda", phases=None):
     """<O(t)> [B, n_samples] (real, torch float64 on the device) and the saved state."""
-    from . import build_instances, gamma_trapz_device, tcl2_generator_series
+    from . import build_instances, gamma_trapz_device_batch, tcl2_generator_series
     torch = _torch()
     params = np.asarray(params, np.float64).reshape(-1, 5)
     B = params.shape[0]
@@ -309,7 +309,7 @@ def spin_boson_forward(params, cfg: SpinBosonConfig, device="cuda", phases=None)
     with _phase(phases, "bcf"):
         C = bcf_device(reqs, T, device)
     with _phase(phases, "gamma"):
-        gammas = [gamma_trapz_device(C[b], cfg.dt, systems[b].omegas) for b in range(B)]
+        gammas = gamma_trapz_device_batch([C[b] for b in range(B)], [cfg.dt] * B, [s.omegas for s in systems])
     N2 = systems[0].N ** 2
     E = N2 * N2
     cdt = torch.complex128 if cfg.precision == "fp64" else torch.complex64
@@ -333,7 +333,7 @@ def spin_boson_forward(params, cfg: SpinBosonConfig, device="cuda", phases=None)
 
 def spin_boson_backward(state, g_obs, cfg: SpinBosonConfig, phases=None):
     """d(loss)/d(eps, Delta, alpha, wc, beta) [B, 5] from g_obs = d(loss)/d<O(t)> [B, n_samples]."""
-    from . import compute_triple_kernels, gamma_trapz_device
+    from . import compute_triple_kernels, gamma_trapz_device_batch
     torch = _torch()
     params, systems = state["params"], state["systems"]
     B = params.shape[0]
@@ -359,13 +359,20 @@ def spin_boson_backward(state, g_obs, cfg: SpinBosonConfig, phases=None):
     with _phase(phases, "bath_tangents"):
         dC = bcf_device(reqs, T, dev).view(B, 3, T)
         tau = torch.arange(T, dtype=torch.float64, device=dev) * dt
+        srcs, oms = [], []
+        for b in range(B):
+            for k in range(3):
+                srcs.append(dC[b, k])
+                oms.append(systems[b].omegas)
+            srcs.append(1j * tau * state["C"][b])
+            oms.append(systems[b].omegas)
+        tg = gamma_trapz_device_batch(srcs, [dt] * len(srcs), oms)
         pairs = []
         for b in range(B):
-            om = systems[b].omegas
             for k in range(3):
-                pairs.append((gbar[b], gamma_trapz_device(dC[b, k].contiguous(), dt, om)))
-            gw = gamma_trapz_device((1j * tau * state["C"][b]).contiguous(), dt, om)
-            for j in range(len(om)):
+                pairs.append((gbar[b], tg[4 * b + k]))
+            gw = tg[4 * b + 3]
+            for j in range(systems[b].nf):
                 pairs.append((gbar[b][j].contiguous(), gw[j].contiguous()))
         dots = inner_re(pairs, dev)
     grads = np.zeros((B, 5), np.float64)

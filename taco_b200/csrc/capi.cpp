@@ -403,6 +403,25 @@ int taco_gamma_trapz(const taco_c128* C, size_t N, double dt, const double* omeg
     });
 }
 
+int taco_gamma_trapz_batch(const taco_gamma_request* reqs, size_t n, void* stream) {
+    return guarded([&] {
+        require_device();
+        if (!reqs && n) throw taco::Error(taco::kInvalidArgument, "gamma_trapz: null requests");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : taco::default_stream();
+        std::vector<taco::GammaRequest> rs(n);
+        for (size_t k = 0; k < n; ++k) {
+            const taco_gamma_request& q = reqs[k];
+            if (!q.omegas && q.M) throw taco::Error(taco::kInvalidArgument, "gamma_trapz: null omegas");
+            rs[k].C = reinterpret_cast<const double2*>(q.C);
+            rs[k].N = q.N;
+            rs[k].dt = q.dt;
+            rs[k].omegas.assign(q.omegas, q.omegas + q.M);
+            rs[k].G = reinterpret_cast<double2*>(q.G);
+        }
+        taco::gamma_trapz_batch_device(rs, st);
+    });
+}
+
 int taco_propagate_tcl(const taco_system_view* sys, const double* eps, const taco_c128* gamma, size_t Nt, double dt,
                        size_t steps, int order, int precision, const taco_c128* rho0, const taco_c128* obs,
                        size_t sample_every, taco_c128* obs_out, taco_c128* rho_out, int flags, void* stream) {

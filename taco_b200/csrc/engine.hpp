@@ -72,6 +72,15 @@ void noalloc_tcl4_build(const SystemDesc& sys, const double2* gamma, std::size_t
 void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2* gamma, std::size_t Nt,
                         const std::vector<uint32_t>& tidx, double2* out, cudaStream_t st);
 // Trapezoid Gamma(w_b, t_k) for all buckets: C [N] and G [nb][N] are device pointers.
+struct GammaRequest {
+    const double2* C = nullptr;
+    std::size_t N = 0;
+    double dt = 0.0;
+    std::vector<double> omegas;
+    double2* G = nullptr;
+};
+// Many requests in one pair of launches.
+void gamma_trapz_batch_device(const std::vector<GammaRequest>& reqs, cudaStream_t st);
 void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::vector<double>& omegas, double2* G,
                         cudaStream_t st);
 

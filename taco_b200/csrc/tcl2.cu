@@ -92,17 +92,31 @@ __device__ __forceinline__ double2 trapz_inc(const double2* C, double w, double 
     return make_double2(0.5 * dt * (a.x + b.x), 0.5 * dt * (a.y + b.y));
 }
 
-__global__ void k_gamma_reduce(const double2* __restrict__ C, std::size_t N, double dt,
-                               const double* __restrict__ omegas, double2* __restrict__ partial, int nchunks) {
+// One Gamma job: C [N] (device), omegas [nb] (device), G [nb][N] (device), and its
+// per-(bucket, chunk) partial sums.
+struct GammaJob {
+    const double2* C;
+    std::size_t N;
+    double dt;
+    const double* omegas;
+    int nb, nchunks;
+    double2* G;
+    double2* partial;  // [nb][nchunks]
+};
+
+// grid (chunk, bucket, job)
+__global__ void k_gamma_reduce(const GammaJob* __restrict__ jobs) {
     __shared__ double2 wsum[GT_THREADS / 32];
+    const GammaJob j = jobs[blockIdx.z];
     const int b = blockIdx.y;
+    if (b >= j.nb || static_cast<int>(blockIdx.x) >= j.nchunks) return;
     const std::size_t k0 = static_cast<std::size_t>(blockIdx.x) * GT_CHUNK + threadIdx.x * GT_ITEMS;
-    const double w = omegas[b];
+    const double w = j.omegas[b];
     double2 s = make_double2(0.0, 0.0);
 #pragma unroll
     for (int q = 0; q < GT_ITEMS; ++q) {
         const std::size_t k = k0 + q;
-        if (k >= 1 && k < N) s = cadd(s, trapz_inc(C, w, dt, k));
+        if (k >= 1 && k < j.N) s = cadd(s, trapz_inc(j.C, w, j.dt, k));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -114,29 +128,30 @@ __global__ void k_gamma_reduce(const double2* __restrict__ C, std::size_t N, dou
     if (threadIdx.x == 0) {
         double2 t = make_double2(0.0, 0.0);
         for (int q = 0; q < GT_THREADS / 32; ++q) t = cadd(t, wsum[q]);
-        partial[static_cast<std::size_t>(b) * nchunks + blockIdx.x] = t;
+        j.partial[static_cast<std::size_t>(b) * j.nchunks + blockIdx.x] = t;
     }
 }
 
-__global__ void k_gamma_scan(const double2* __restrict__ C, std::size_t N, double dt, const double* __restrict__ omegas,
-                             const double2* __restrict__ partial, int nchunks, double2* __restrict__ G) {
+__global__ void k_gamma_scan(const GammaJob* __restrict__ jobs) {
     __shared__ double2 wsum[GT_THREADS / 32];
     __shared__ double2 carry;
+    const GammaJob j = jobs[blockIdx.z];
     const int b = blockIdx.y;
+    if (b >= j.nb || static_cast<int>(blockIdx.x) >= j.nchunks) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
         double2 t = make_double2(0.0, 0.0);
-        for (int c = 0; c < static_cast<int>(blockIdx.x); ++c) t = cadd(t, partial[static_cast<std::size_t>(b) * nchunks + c]);
+        for (int c = 0; c < static_cast<int>(blockIdx.x); ++c) t = cadd(t, j.partial[static_cast<std::size_t>(b) * j.nchunks + c]);
         carry = t;
     }
     const std::size_t k0 = static_cast<std::size_t>(blockIdx.x) * GT_CHUNK + threadIdx.x * GT_ITEMS;
-    const double w = omegas[b];
+    const double w = j.omegas[b];
     double2 v[GT_ITEMS];
     double2 run = make_double2(0.0, 0.0);
 #pragma unroll
     for (int q = 0; q < GT_ITEMS; ++q) {
         const std::size_t k = k0 + q;
-        v[q] = (k >= 1 && k < N) ? trapz_inc(C, w, dt, k) : make_double2(0.0, 0.0);
+        v[q] = (k >= 1 && k < j.N) ? trapz_inc(j.C, w, j.dt, k) : make_double2(0.0, 0.0);
         run = cadd(run, v[q]);
     }
     double2 x = run;
@@ -156,12 +171,12 @@ __global__ void k_gamma_scan(const double2* __restrict__ C, std::size_t N, doubl
     double2 pre = carry;
     for (int q = 0; q < warp; ++q) pre = cadd(pre, wsum[q]);
     pre = cadd(pre, excl);
-    double2* Gb = G + static_cast<std::size_t>(b) * N;
+    double2* Gb = j.G + static_cast<std::size_t>(b) * j.N;
 #pragma unroll
     for (int q = 0; q < GT_ITEMS; ++q) {
         const std::size_t k = k0 + q;
         pre = cadd(pre, v[q]);
-        if (k < N) Gb[k] = pre;  // G(0) = 0: the k = 0 increment is zero
+        if (k < j.N) Gb[k] = pre;  // G(0) = 0: the k = 0 increment is zero
     }
 }
 
@@ -406,25 +421,65 @@ void tcl2_series_device(const SystemDesc& sys, const double* eps, const double2*
     }
 }
 
+void gamma_trapz_batch_device(const std::vector<GammaRequest>& reqs, cudaStream_t st) {
+    if (reqs.empty()) return;
+    std::size_t bytes = 256 + reqs.size() * sizeof(GammaJob);
+    int max_nb = 0, max_chunks = 0;
+    for (const auto& r : reqs) {
+        if (!r.C || !r.G || r.N == 0 || r.omegas.empty() || !(r.dt > 0.0))
+            throw Error(kInvalidArgument, "gamma_trapz: null or empty input");
+        if (r.omegas.size() > 65535) throw Error(kInvalidArgument, "gamma_trapz: too many frequencies");
+        const int nch = static_cast<int>((r.N + GT_CHUNK - 1) / GT_CHUNK);
+        max_nb = std::max(max_nb, static_cast<int>(r.omegas.size()));
+        max_chunks = std::max(max_chunks, nch);
+        bytes += ((r.omegas.size() * sizeof(double) + 255) / 256) * 256 +
+                 ((r.omegas.size() * nch * sizeof(double2) + 255) / 256) * 256;
+    }
+    char* base = tcl2_scratch(bytes);
+    std::size_t off = 0;
+    auto take = [&](std::size_t n) {
+        char* p = base + off;
+        off += (n + 255) / 256 * 256;
+        return p;
+    };
+    std::vector<GammaJob> jobs(reqs.size());
+    GammaJob* dj = reinterpret_cast<GammaJob*>(take(reqs.size() * sizeof(GammaJob)));
+    for (std::size_t k = 0; k < reqs.size(); ++k) {
+        const GammaRequest& r = reqs[k];
+        GammaJob& j = jobs[k];
+        j.C = r.C;
+        j.N = r.N;
+        j.dt = r.dt;
+        j.nb = static_cast<int>(r.omegas.size());
+        j.nchunks = static_cast<int>((r.N + GT_CHUNK - 1) / GT_CHUNK);
+        j.G = r.G;
+        double* dom = reinterpret_cast<double*>(take(r.omegas.size() * sizeof(double)));
+        cuda_check(cudaMemcpyAsync(dom, r.omegas.data(), r.omegas.size() * sizeof(double), cudaMemcpyHostToDevice, st),
+                   "gamma omegas");
+        j.omegas = dom;
+        j.partial = reinterpret_cast<double2*>(take(static_cast<std::size_t>(j.nb) * j.nchunks * sizeof(double2)));
+    }
+    cuda_check(cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(GammaJob), cudaMemcpyHostToDevice, st), "gamma jobs");
+    for (std::size_t k0 = 0; k0 < reqs.size(); k0 += 65535) {
+        const unsigned nj = static_cast<unsigned>(std::min<std::size_t>(65535, reqs.size() - k0));
+        const dim3 grid(static_cast<unsigned>(max_chunks), static_cast<unsigned>(max_nb), nj);
+        k_gamma_reduce<<<grid, GT_THREADS, 0, st>>>(dj + k0);
+        launched("k_gamma_reduce");
+        k_gamma_scan<<<grid, GT_THREADS, 0, st>>>(dj + k0);
+        launched("k_gamma_scan");
+    }
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(gamma)");
+}
+
 void gamma_trapz_device(const double2* C, std::size_t N, double dt, const std::vector<double>& omegas, double2* G,
                         cudaStream_t st) {
-    const int nb = static_cast<int>(omegas.size());
-    const int nchunks = static_cast<int>((N + GT_CHUNK - 1) / GT_CHUNK);
-    if (nb > 65535) throw Error(kInvalidArgument, "gamma_trapz: too many frequencies");
-    const std::size_t bytes = nb * sizeof(double) + static_cast<std::size_t>(nb) * nchunks * sizeof(double2) + 256;
-    void* d = tcl2_scratch(bytes);
-    {
-        double* dom = static_cast<double*>(d);
-        double2* part = reinterpret_cast<double2*>(static_cast<char*>(d) + ((nb * sizeof(double) + 255) / 256) * 256);
-        cuda_check(cudaMemcpyAsync(dom, omegas.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st), "omegas");
-        k_gamma_reduce<<<dim3(static_cast<unsigned>(nchunks), static_cast<unsigned>(nb)), GT_THREADS, 0, st>>>(
-            C, N, dt, dom, part, nchunks);
-        launched("k_gamma_reduce");
-        k_gamma_scan<<<dim3(static_cast<unsigned>(nchunks), static_cast<unsigned>(nb)), GT_THREADS, 0, st>>>(
-            C, N, dt, dom, part, nchunks, G);
-        launched("k_gamma_scan");
-        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(gamma)");
-    }
+    GammaRequest r;
+    r.C = C;
+    r.N = N;
+    r.dt = dt;
+    r.omegas = omegas;
+    r.G = G;
+    gamma_trapz_batch_device({r}, st);
 }
 
 }  // namespace taco

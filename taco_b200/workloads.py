@@ -63,8 +63,12 @@ def spin_boson_systems(B, seed=0):
 
 
 def spin_boson_batch(torch, B, N=200000, dt=5e-4, seed=0, device="cuda"):
-    """-> (params, systems, gammas) for B seeded instances."""
+    """-> (params, systems, gammas) for B seeded instances (one batched BCF and one batched
+    trapezoid launch pair)."""
     del torch
+    from . import gamma_trapz_device_batch
+    from .adjoint import bcf_device
     params, systems = spin_boson_systems(B, seed)
-    gammas = [gamma_device(s, prm, N, dt, device) for s, prm in zip(systems, params)]
+    C = bcf_device([dict(alpha=p["alpha"], omega_c=p["wc"], beta=p["beta"], N=N, dt=dt) for p in params], N + 1, device)
+    gammas = gamma_trapz_device_batch([C[b] for b in range(B)], [dt] * B, [s.omegas for s in systems])
     return params, systems, gammas

@@ -78,3 +78,18 @@ def test_propagation_config1_shape(order):
     if order == 4:
         o32, r32 = tb.propagate_tcl(s, G, 0.005, steps, r0, obs=obs, order=4, precision="fp32")
         assert relerr(o32, o_ref) <= 1e-6
+
+
+def test_gamma_trapz_batch_matches_single_calls():
+    import torch
+    cases = [(20000, 0.005, [0.05, 10.0], 1.0, [-1.4, 0.0, 1.4]), (777, 0.01, [0.1, 3.0], 0.4, [-0.3, 0.0, 0.2, 0.5])]
+    Cs, dts, oms, refs = [], [], [], []
+    for N, dt, prm, beta, om in cases:
+        _, C = oracle.bcf_fft(N, dt, oracle.J_OHMIC, prm, beta)
+        Cs.append(torch.from_numpy(C).cuda())
+        dts.append(dt)
+        oms.append(np.array(om))
+        refs.append(oracle.gamma_trapz(C, dt, np.array(om)))
+    outs = tb.gamma_trapz_device_batch(Cs, dts, oms)
+    for o, r in zip(outs, refs):
+        assert relerr(o.cpu().numpy(), r) <= 1e-10
