@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(128) k_rk4g_fwd(const Rk4GJob* __restrict__ jo
     const Rk4GJob j = jobs[w];
     const int D = j.D;
     const int row = lane < D ? lane : 0;
-    double2 l0[DMAX], l1[DMAX];
+    double2 l0[DMAX], l1[DMAX], l2[DMAX];
     load_row<DMAX>(j, 0, row, l0);
     load_row<DMAX>(j, 1, row, l1);
     double2 r = lane < D ? j.r0[lane] : make_double2(0.0, 0.0);
@@ -203,12 +203,16 @@ __global__ void __launch_bounds__(128) k_rk4g_fwd(const Rk4GJob* __restrict__ jo
         if (lane == 0) j.obs_out[s] = v;
     };
     for (uint64_t i = 0; i < j.steps; ++i) {
+        // the row of L(t_{i+2}) arrives while step i runs
+        if (i + 2 <= j.steps) load_row<DMAX>(j, i + 2, row, l2);
         if (j.ckpt && (i % every) == 0 && lane < D) j.ckpt[(i / every) * D + lane] = r;
         if (se && (i % se) == 0) sample(i / se);
         r = rk4_step<DMAX>(r, l0, l1, j.dt, D);
 #pragma unroll
-        for (int c = 0; c < DMAX; ++c) l0[c] = l1[c];
-        if (i + 2 <= j.steps) load_row<DMAX>(j, i + 2, row, l1);
+        for (int c = 0; c < DMAX; ++c) {
+            l0[c] = l1[c];
+            l1[c] = l2[c];
+        }
     }
     if (se) sample(n_samples(j.steps, se) - 1);
     if (j.r_out && lane < D) j.r_out[lane] = r;
@@ -258,11 +262,21 @@ __global__ void __launch_bounds__(32) k_rk4g_adj(const Rk4GJob* __restrict__ job
         }
         __syncwarp();
         double2 r0w[DMAX], r1w[DMAX], c0[DMAX], c1[DMAX];  // rows / columns of L(t_n), L(t_{n+1})
+        double2 rp[DMAX], cp[DMAX];                        // L(t_{n-1}), fetched during step n
         load_row<DMAX>(j, s1, me, r1w);
         load_col<DMAX>(j, s1, me, c1);
+        load_row<DMAX>(j, s1 - 1, me, rp);
+        load_col<DMAX>(j, s1 - 1, me, cp);
         for (uint64_t n = s1; n-- > s0;) {
-            load_row<DMAX>(j, n, me, r0w);
-            load_col<DMAX>(j, n, me, c0);
+#pragma unroll
+            for (int c = 0; c < DMAX; ++c) {
+                r0w[c] = rp[c];
+                c0[c] = cp[c];
+            }
+            if (n > s0) {
+                load_row<DMAX>(j, n - 1, me, rp);
+                load_col<DMAX>(j, n - 1, me, cp);
+            }
             const double2 rn = own ? seg[(n - s0) * DMAX + lane] : make_double2(0.0, 0.0);
             double2 rh[DMAX], ch[DMAX];
 #pragma unroll
