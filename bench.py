@@ -562,7 +562,7 @@ def main():
 
     # ---- roofline of the dominant kernel ----
     peaks, peak_kind = measured_peaks()
-    nfft = 1 << (2 * T - 2).bit_length()  # next_pow2(2 (tmax+1) - 1)
+    nfft = tb.fft_length(T, "fp32")[0]  # causal rule: 2 (tmax+1) - 1 rounded up to 2^k, 3*2^k or 5*2^k
     shape = (T, nfft, T, T, 3)
     units_total = {"triple": B * 27, "spectrum": B * 6}
     tot_all = sum(v[1] for v in prof.entries.values()) or 1.0
@@ -629,7 +629,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{B} spin-boson instances per GPU (d=2, nf=3), N={args.N} (Nt={args.N + 1}), "
                                    f"dt={args.dt}, tidx 0..{args.tmax}, batched FP32 form, one CUDA-graph replay "
-                                   f"per step, FFT length 2^{nfft.bit_length() - 1} from max(tidx)+1",
+                                   f"per step, FFT length {nfft} from max(tidx)+1",
                        "instances_per_gpu": B, "builds_per_instance": T,
                        "l2": "inputs larger than L2 (Gamma 9.6 MB x instances; L4 outputs 1.3 MB x instances)",
                        "parallelism": f"instance-sharded x{world}"},

@@ -227,6 +227,10 @@ int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t*
  * memory at the call, at most 64 GiB).  Instances that need more are built in slices of
  * their frequency triples (same results, more passes over the output). */
 int taco_set_work_budget(size_t bytes);
+/* FFT length the build uses for n_in consumed samples (flags: TACO_FULL_LENGTH_FFT selects
+ * the reference's power-of-two rule), and its schedule key for taco_set_tuning: log2 of a
+ * power of two, + 64 for 3 * 2^k, + 128 for 5 * 2^k. */
+int taco_fft_length(size_t n_in, int precision, int flags, size_t* nfft, int* key);
 int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows);
 int taco_get_tuning(int log2_nfft, int precision, int* col_tile, int* row_tile, size_t* chunk_bytes,
                     int* inv_dft_rows);

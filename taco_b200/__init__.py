@@ -40,7 +40,7 @@ __all__ = [
     "build_TCL4_generator", "build_TCL4_generator_batch", "build_correction_series", "build_instances",
     "propagate_rk4_dense", "l4_coefficients", "Tcl4Plan", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
     "version", "device_count", "kernel_launches", "profile", "tcl2_generator_series", "gamma_trapz_device",
-    "propagate_tcl", "gamma_trapz_device_batch", "set_work_budget", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
+    "propagate_tcl", "gamma_trapz_device_batch", "set_work_budget", "fft_length", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
 ]
 
 
@@ -93,6 +93,16 @@ def set_work_budget(nbytes: int) -> None:
     """Transient device memory of one group of a build (0: automatic).  Larger instances
     are built in slices of their frequency triples."""
     _capi.check(_capi.lib().taco_set_work_budget(int(nbytes)))
+
+
+def fft_length(n_in: int, precision: str = "fp32", full_length: bool = False):
+    """(Nfft, schedule key) the build uses for n_in consumed Gamma samples."""
+    n = ct.c_size_t(0)
+    k = ct.c_int(0)
+    prec = {"fp64": _capi.TACO_PREC_FP64, "fp32": _capi.TACO_PREC_FP32}[precision]
+    _capi.check(_capi.lib().taco_fft_length(int(n_in), prec, _capi.TACO_FULL_LENGTH_FFT if full_length else 0,
+                                            ct.byref(n), ct.byref(k)))
+    return int(n.value), int(k.value)
 
 
 def set_fcr_fft_pad_factor(factor: int) -> None:

@@ -39,6 +39,7 @@ EXPORTED = [
     "taco_build_mikx", "taco_assemble_liouvillian", "taco_gw_to_liouvillian",
     "taco_bcf_fft", "taco_rk4_forward_checkpointed", "taco_rk4_adjoint", "taco_tcl4_adjoint",
     "taco_tcl2_adjoint", "taco_inner_re", "taco_set_work_budget", "taco_gamma_trapz_batch",
+    "taco_fft_length",
 ]
 
 
@@ -170,6 +171,7 @@ def lib():
                                                 ct.c_void_p]
         L.taco_gw_to_liouvillian.argtypes = [ct.c_void_p, ct.c_int, ct.c_size_t, ct.c_void_p, ct.c_int, ct.c_void_p]
         L.taco_set_work_budget.argtypes = [ct.c_size_t]
+        L.taco_fft_length.argtypes = [ct.c_size_t, ct.c_int, ct.c_int, ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_int)]
         L.taco_gamma_trapz_batch.argtypes = [ct.POINTER(GammaRequest), ct.c_size_t, ct.c_void_p]
         L.taco_bcf_fft.argtypes = [ct.POINTER(BcfRequest), ct.c_size_t, ct.c_int, ct.c_void_p]
         L.taco_rk4_forward_checkpointed.argtypes = [ct.POINTER(Rk4GradJob), ct.c_size_t, ct.c_size_t, ct.c_void_p]

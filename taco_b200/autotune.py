@@ -3,7 +3,9 @@
 For one FFT length and precision it times the batched build of a representative
 workload under each candidate schedule (column tile, row tile, Z/W chunk bytes, pruned
 inverse-DFT rows), with CUDA events after warm-up, and keeps the fastest.  Results are
-persisted as JSON ({"<log2_nfft>:<fp32|fp64>": {...}}) and applied with load().
+persisted as JSON ({"<key>:<fp32|fp64>": {...}}) and applied with load(); the key of an
+FFT length is log2 for powers of two, + 64 for 3 * 2^k and + 128 for 5 * 2^k
+(taco_b200.fft_length).
 
     python -m taco_b200.autotune --out taco_b200/tuning.json   (needs a GPU)
 """
@@ -61,13 +63,18 @@ def candidates(precision: str):
             for c, r, b, d in itertools.product(cols, rows, chunks, dft)]
 
 
-def _time(log2_nfft, precision, sch, run, factory, reps, warmup, log):
-    """Device time of one unit of work under schedule `sch` (inf when the schedule fails)."""
+def _time(log2_nfft, precision, sch, run, factory, reps, warmup, log, check=None):
+    """Device time of one unit of work under schedule `sch` (inf when the schedule fails, or
+    when `check` says the schedule changes the FFT length being tuned)."""
     import torch
 
     unit = None
     try:
         set_schedule(log2_nfft, precision, **sch)
+        if check is not None and not check():
+            if log:
+                log(f"{precision} key {log2_nfft} {sch} -> changes the FFT length, skipped")
+            return float("inf")
         unit = factory() if factory is not None else run
         for _ in range(warmup):
             unit()
@@ -87,11 +94,12 @@ def _time(log2_nfft, precision, sch, run, factory, reps, warmup, log):
         if unit is not None and hasattr(unit, "close"):
             unit.close()
     if log:
-        log(f"{precision} 2^{log2_nfft} {sch} -> {ms:.3f} ms")
+        log(f"{precision} key {log2_nfft} {sch} -> {ms:.3f} ms")
     return ms
 
 
-def tune(run, log2_nfft: int, precision: str, cands=None, reps: int = 3, warmup: int = 1, log=None, factory=None):
+def tune(run, log2_nfft: int, precision: str, cands=None, reps: int = 3, warmup: int = 1, log=None, factory=None,
+         check=None):
     """Times one unit of work under every candidate schedule and keeps the fastest.
 
     run(): the unit (e.g. a batched build); or factory(): called after each schedule is
@@ -99,13 +107,13 @@ def tune(run, log2_nfft: int, precision: str, cands=None, reps: int = 3, warmup:
     (best, results)."""
     results = []
     for sch in cands or candidates(precision):
-        results.append((_time(log2_nfft, precision, sch, run, factory, reps, warmup, log), sch))
+        results.append((_time(log2_nfft, precision, sch, run, factory, reps, warmup, log, check), sch))
     results.sort(key=lambda x: x[0])
     best = dict(results[0][1])
     # phase 2: the thread-block-cluster path (points per CTA), with the best multi-pass tiles
     lm_max = 13 if precision == "fp32" else 12
     for lm in (11, 12, 13):
-        if lm > lm_max or log2_nfft - lm > 3 or lm > log2_nfft:
+        if log2_nfft >= 64 or lm > lm_max or log2_nfft - lm > 3 or lm > log2_nfft:  # powers of two only
             continue
         sch = dict(best, cluster_lm=lm)
         results.append((_time(log2_nfft, precision, sch, run, factory, reps, warmup, log), sch))
@@ -167,8 +175,8 @@ def main():
     for full in (False, True):
         # FFT length: next_pow2(2 n - 1) with n = tmax + 1 (default) or Nt (full length)
         n = (args.N + 1) if full else T
-        L = (2 * n - 2).bit_length()
         for prec in args.precisions.split(","):
+            nfft, L = tb.fft_length(n, prec, full_length=full)  # L: the schedule key of this length
             dtype = torch.complex64 if prec == "fp32" else torch.complex128
             outs = [torch.empty((T, 16), dtype=dtype, device="cuda") for _ in systems]
             inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
@@ -179,7 +187,10 @@ def main():
             else:  # the batched path: one plan over every instance
                 def factory():
                     return _Plans([tb.Tcl4Plan(inst, precision=prec, outs=outs, full_length=full)])
-            best, res = tune(None, L, prec, log=print, factory=factory)
+            def same_length(n=n, prec=prec, full=full, nfft=nfft):
+                return tb.fft_length(n, prec, full_length=full)[0] == nfft
+
+            best, res = tune(None, L, prec, log=print, factory=factory, check=same_length)
             entries[f"{L}:{prec}"] = dict(best, ms=res[0][0])
     save(entries, args.out, note="measured on B200 by taco_b200.autotune (C2-shaped spin-boson batch)")
     print(json.dumps(entries))

@@ -599,6 +599,15 @@ int taco_set_work_budget(size_t bytes) {
     return guarded([&] { taco::set_work_budget(bytes); });
 }
 
+int taco_fft_length(size_t n_in, int precision, int flags, size_t* nfft, int* key) {
+    return guarded([&] {
+        if (n_in == 0) throw taco::Error(taco::kInvalidArgument, "fft_length: n_in must be > 0");
+        const bool full = (flags & TACO_FULL_LENGTH_FFT) != 0;
+        const std::size_t n = taco::fft_length_for(n_in, precision == TACO_PREC_FP32, !full, taco_get_fcr_fft_pad_factor(), key);
+        if (nfft) *nfft = n;
+    });
+}
+
 int taco_bcf_fft(const taco_bcf_request* reqs, size_t n, int flags, void* stream) {
     return guarded([&] {
         require_device();

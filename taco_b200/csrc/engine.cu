@@ -95,8 +95,25 @@ struct Layout {
 
 struct PlanTables {
     DeviceBuffer buf;
-    int L = 0, L1 = 0, L2 = 0, s = 0;
+    int L = 0, L1 = 0, L2 = 0, s = 0, R = 1;
 };
+
+// FFT lengths Nfft = R * 2^L with R in {1, 3, 5}.  The key names a length in the plan and
+// tuning tables: L for powers of two, L + 64 (R = 3), L + 128 (R = 5).
+int odd_index(int R) { return R == 3 ? 1 : (R == 5 ? 2 : 0); }
+int size_key(int L, int R) { return L + 64 * odd_index(R); }
+
+// Four-step split: N2 = 2^L2 rows of the row pass, N1 = R * 2^L1 points per column, with
+// N2 the smallest power of two >= sqrt(Nfft) for the mixed lengths (L2 = ceil(L/2) else).
+void fft_split(int L, int R, int& L1, int& L2) {
+    if (R == 1) {
+        L2 = (L + 1) / 2;
+    } else {
+        const double lg = L + std::log2(static_cast<double>(R));
+        L2 = static_cast<int>(std::ceil(lg / 2.0));
+    }
+    L1 = L - L2;
+}
 
 struct Workspace {
     int device = -1;
@@ -139,17 +156,18 @@ __global__ void k_fill_twiddle(C* out, uint32_t count, double denom) {
 }
 
 template <class R>
-FftPlan<cplx_t<R>> get_plan(Workspace& ws, int L, cudaStream_t st) {
+FftPlan<cplx_t<R>> get_plan(Workspace& ws, int L, int Rf, cudaStream_t st) {
     using C = cplx_t<R>;
     const bool fp32 = std::is_same<R, float>::value;
-    auto& slot = ws.plans[{L, fp32 ? 1 : 0}];
+    auto& slot = ws.plans[{size_key(L, Rf), fp32 ? 1 : 0}];
     if (!slot) {
         auto pt = std::make_unique<PlanTables>();
         pt->L = L;
-        pt->L2 = (L + 1) / 2;
-        pt->L1 = L - pt->L2;
+        pt->R = Rf;
+        fft_split(L, Rf, pt->L1, pt->L2);
         pt->s = (L + 1) / 2;
-        const std::size_t N = std::size_t(1) << L, N1 = std::size_t(1) << pt->L1, N2 = std::size_t(1) << pt->L2;
+        const std::size_t N = static_cast<std::size_t>(Rf) << L, N1 = static_cast<std::size_t>(Rf) << pt->L1,
+                          N2 = std::size_t(1) << pt->L2;
         const std::size_t nc = N >> pt->s, nfine = std::size_t(1) << pt->s;
         pt->buf.ensure((N1 + N2 + nc + nfine) * sizeof(C) + 4 * 256);
         Layout lay{static_cast<char*>(pt->buf.p)};
@@ -169,13 +187,15 @@ FftPlan<cplx_t<R>> get_plan(Workspace& ws, int L, cudaStream_t st) {
         slot = std::move(pt);
     }
     const PlanTables& pt = *slot;
-    const std::size_t N = std::size_t(1) << L, N1 = std::size_t(1) << pt.L1, N2 = std::size_t(1) << pt.L2;
+    const std::size_t N = static_cast<std::size_t>(Rf) << L, N1 = static_cast<std::size_t>(Rf) << pt.L1,
+                      N2 = std::size_t(1) << pt.L2;
     Layout lay{static_cast<char*>(pt.buf.p)};
     FftPlan<C> p;
     p.L = L;
     p.L1 = pt.L1;
     p.L2 = pt.L2;
     p.s = pt.s;
+    p.R = Rf;
     p.tw1 = lay.take<C>(N1);
     p.tw2 = lay.take<C>(N2);
     p.twc = lay.take<C>(N >> pt.s);
@@ -282,8 +302,30 @@ using InvFn = void (*)(const InvJob*, FftPlan<cplx_t<R>>, int);
 #define TACO_CT_CASES(X) \
     X(7, 3) X(7, 4) X(7, 5) X(8, 2) X(8, 3) X(8, 4) X(9, 1) X(9, 2) X(9, 3) X(10, 0) X(10, 1) X(10, 2)
 
+// Column kernels of the mixed lengths N1 = R * 2^l for the tile widths the default and
+// tuned schedules produce.
+#define TACO_MX_CASES(X) \
+    X(5, 4, 3) X(5, 4, 4) X(5, 4, 5) X(5, 5, 3) X(5, 5, 4) X(3, 5, 3) X(3, 5, 4) X(3, 5, 5) X(3, 4, 4) X(3, 4, 5)
+
+bool mixed_column_kernels(int r, int l, int c) {
+    switch (r * 256 + l * 16 + c) {
+#define X(a, b, d) case a * 256 + b * 16 + d: return true;
+        TACO_MX_CASES(X)
+#undef X
+        default: return false;
+    }
+}
+
 template <class R>
-ColFn<R> fwd_col_fn(int l, int c) {
+ColFn<R> fwd_col_fn(int r, int l, int c) {
+    if (r > 1) {
+        switch (r * 256 + l * 16 + c) {
+#define X(a, b, d) case a * 256 + b * 16 + d: return k_fwd_col_mx<R, a, b, d>;
+            TACO_MX_CASES(X)
+#undef X
+            default: throw Error(kRuntime, "no column kernel for this mixed FFT length");
+        }
+    }
     switch (l * 16 + c) {
 #define X(a, b) case a * 16 + b: return k_fwd_col_ct<R, a, b>;
         TACO_CT_CASES(X)
@@ -293,7 +335,15 @@ ColFn<R> fwd_col_fn(int l, int c) {
 }
 
 template <class R>
-InvFn<R> inv_col_fn(int l, int c) {
+InvFn<R> inv_col_fn(int r, int l, int c) {
+    if (r > 1) {
+        switch (r * 256 + l * 16 + c) {
+#define X(a, b, d) case a * 256 + b * 16 + d: return k_inv_col_mx<R, a, b, d>;
+            TACO_MX_CASES(X)
+#undef X
+            default: throw Error(kRuntime, "no column kernel for this mixed FFT length");
+        }
+    }
     switch (l * 16 + c) {
 #define X(a, b) case a * 16 + b: return k_inv_col_ct<R, a, b>;
         TACO_CT_CASES(X)
@@ -312,6 +362,7 @@ RowFn<R> row_fn(int l, int c) {
     }
 }
 #undef TACO_CT_CASES
+#undef TACO_MX_CASES
 
 struct Geometry {
     int log2c, col_threads, log2r, row_threads;
@@ -324,16 +375,22 @@ struct Geometry {
 template <class C>
 Geometry geometry(const FftPlan<C>& p, int col_tile, int row_tile) {
     Geometry g;
-    const int N1 = 1 << p.L1, N2 = 1 << p.L2;
+    const int N1 = p.R << p.L1, N2 = 1 << p.L2;
+    auto floor_log2 = [](int x) {
+        int l = 0;
+        while ((2 << l) <= x) ++l;
+        return l;
+    };
     const int cc = std::max(1, std::min(N2, col_tile / N1));
-    g.log2c = ilog2(static_cast<std::size_t>(cc));
+    g.log2c = floor_log2(cc);
     g.col_threads = (N1 << g.log2c) / 8;
     g.col_smem = static_cast<std::size_t>(padded_size<C>(N1 << g.log2c)) * sizeof(C);
     g.col_grid = static_cast<unsigned>(N2 >> g.log2c);
-    const int rr = std::max(1, std::min(N1, row_tile / N2));
-    g.log2r = ilog2(static_cast<std::size_t>(rr));
+    const int rr = std::max(1, std::min(1 << p.L1, row_tile / N2));  // rows of a tile divide N1
+    g.log2r = floor_log2(rr);
     g.row_threads = (N2 << g.log2r) / 8;
     g.row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << g.log2r)) * sizeof(C);
+    g.row_grid = static_cast<unsigned>(N1 >> g.log2r);
     constexpr std::size_t kSmemMax = 227 * 1024;
     while (g.row_smem > kSmemMax && g.log2r > 0) {  // explicit schedules too large for one CTA
         --g.log2r;
@@ -420,11 +477,40 @@ void check_launch(const char* what, ProfRecorder* pr = nullptr) {
 // --------------------------------------------------------------- metadata --
 struct InstMeta {
     std::size_t T = 0, U = 0, t_count = 0, n_in = 0;
-    int L = 0;
+    int L = 0, R = 1;  // FFT length R * 2^L
     std::vector<int> tmap;          // [t_count]
     std::vector<uint32_t> out_u;    // [T]
     CoefTable coef;
 };
+
+// FFT length for a linear convolution of `target` outputs: the next power of two, or (when
+// allowed: the causal rule) 3 * 2^k or 5 * 2^k if shorter and column kernels exist for
+// the resulting split under the current schedule.
+void choose_fft(std::size_t target, bool fp32, bool allow_mixed, int& L_out, int& R_out) {
+    std::size_t nfft = std::max<std::size_t>(8, next_pow2(target));
+    if (nfft > (std::size_t(1) << 22)) throw Error(kOverflow, "FFT length above 2^22 is not supported");
+    L_out = ilog2(nfft);
+    R_out = 1;
+    if (!allow_mixed) return;
+    for (int Rf : {5, 3}) {
+        const std::size_t base = (target + Rf - 1) / Rf;
+        const int L = std::max(3, ilog2(base));
+        const std::size_t n = static_cast<std::size_t>(Rf) << L;
+        if (n >= nfft || n < target) continue;
+        int L1 = 0, L2 = 0;
+        fft_split(L, Rf, L1, L2);
+        if (L1 < 3) continue;
+        const Tuning t = tuning_for(size_key(L, Rf), fp32);
+        const int log2c = fp32 ? geometry(FftPlan<float2>{L, L1, L2, 0, Rf, nullptr, nullptr, nullptr, nullptr},
+                                          t.col_tile, t.row_tile).log2c
+                               : geometry(FftPlan<double2>{L, L1, L2, 0, Rf, nullptr, nullptr, nullptr, nullptr},
+                                          t.col_tile, t.row_tile).log2c;
+        if (!mixed_column_kernels(Rf, L1, log2c)) continue;
+        nfft = n;
+        L_out = L;
+        R_out = Rf;
+    }
+}
 
 void derive_meta(const Tcl4Instance& in, const BuildOptions& opt, InstMeta& m, bool want_coef) {
     m.T = in.tidx.size();
@@ -442,9 +528,7 @@ void derive_meta(const Tcl4Instance& in, const BuildOptions& opt, InstMeta& m, b
     m.n_in = opt.causal_truncation ? m.t_count : in.Nt;
     std::size_t target = 2 * m.n_in - 1;
     if (opt.pad_factor > 0) target = std::max(target, opt.pad_factor * m.n_in);
-    std::size_t nfft = std::max<std::size_t>(8, next_pow2(target));
-    if (nfft > (std::size_t(1) << 22)) throw Error(kOverflow, "FFT length above 2^22 is not supported");
-    m.L = ilog2(nfft);
+    choose_fft(target, opt.fp32, opt.causal_truncation && opt.pad_factor == 0, m.L, m.R);
     if (want_coef)
         build_coef_table(in.sys.N, in.sys.nf, in.sys.p2f.data(), in.sys.ops.data(), in.sys.num_ops, m.coef);
 }
@@ -496,7 +580,7 @@ std::shared_ptr<CoefTable> slice_table(const CoefTable& full, int lo, int hi) {
 // Launch geometry of one group (units with equal FFT length).
 template <class R>
 struct GroupGeom {
-    int L = 0;
+    int L = 0, Rf = 1;  // FFT length Rf * 2^L
     std::size_t Nfft = 0, ntri = 0, Q = 1, nchunks = 0, max_tcount = 0;
     Tuning tune;
     Geometry g;
@@ -509,15 +593,16 @@ GroupGeom<R> group_geom(const std::vector<WorkUnit*>& units) {
     using C = cplx_t<R>;
     GroupGeom<R> G;
     G.L = units[0]->meta->L;
-    G.Nfft = std::size_t(1) << G.L;
-    G.tune = tuning_for(G.L, std::is_same<R, float>::value);
+    G.Rf = units[0]->meta->R;
+    G.Nfft = static_cast<std::size_t>(G.Rf) << G.L;
+    G.tune = tuning_for(size_key(G.L, G.Rf), std::is_same<R, float>::value);
     FftPlan<C> shape{};
     shape.L = G.L;
-    shape.L2 = (G.L + 1) / 2;
-    shape.L1 = G.L - shape.L2;
+    shape.R = G.Rf;
+    fft_split(G.L, G.Rf, shape.L1, shape.L2);
     G.g = geometry(shape, G.tune.col_tile, G.tune.row_tile);
     for (auto* u : units) G.ntri += static_cast<std::size_t>(u->nsub());
-    G.clm = cluster_lm_for(G.L, std::is_same<R, float>::value, G.tune);
+    G.clm = G.Rf == 1 ? cluster_lm_for(G.L, std::is_same<R, float>::value, G.tune) : -1;
     G.use_cluster = G.clm > 0;
     const std::size_t per_tri_scratch = 2 * G.Nfft * sizeof(C);
     G.Q = std::max<std::size_t>(1, G.tune.chunk_bytes / per_tri_scratch);
@@ -595,7 +680,7 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     (void)opt;
     const GroupGeom<R> G = group_geom<R>(units);
     const int L = G.L;
-    const FftPlan<C> plan = get_plan<R>(ws, L, st);
+    const FftPlan<C> plan = get_plan<R>(ws, L, G.Rf, st);
     const Geometry g = G.g;
     const std::size_t Nfft = G.Nfft;
     const std::size_t ni = units.size();
@@ -864,8 +949,8 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(meta)");
 
     // ---- launches ----
-    const ColFn<R> fwd_col = fwd_col_fn<R>(plan.L1, g.log2c);
-    const InvFn<R> inv_col = inv_col_fn<R>(plan.L1, g.log2c);
+    const ColFn<R> fwd_col = fwd_col_fn<R>(plan.R, plan.L1, g.log2c);
+    const InvFn<R> inv_col = inv_col_fn<R>(plan.R, plan.L1, g.log2c);
     const RowFn<R> row = row_fn<R>(plan.L2, g.log2r);
     set_smem(fwd_col, g.col_smem);
     set_smem(inv_col, g.col_smem);
@@ -1050,7 +1135,7 @@ std::vector<std::vector<WorkUnit*>> plan_units(std::vector<Tcl4Instance>& insts,
                                                std::size_t budget, std::vector<std::unique_ptr<WorkUnit>>& store) {
     std::map<int, std::vector<std::size_t>> byL;
     for (std::size_t a = 0; a < insts.size(); ++a)
-        if (!insts[a].tidx.empty()) byL[metas[a].L].push_back(a);
+        if (!insts[a].tidx.empty()) byL[size_key(metas[a].L, metas[a].R)].push_back(a);
     std::vector<std::vector<WorkUnit*>> groups;
     for (auto& kv : byL) {
         std::vector<WorkUnit*> cur;
@@ -1158,6 +1243,15 @@ void stage_sliced_io(std::vector<Tcl4Instance>& insts, std::vector<InstMeta>& me
 }  // namespace
 
 void set_work_budget(std::size_t bytes) { g_work_budget.store(bytes); }
+
+std::size_t fft_length_for(std::size_t n_in, bool fp32, bool causal, std::size_t pad_factor, int* key) {
+    std::size_t target = 2 * n_in - 1;
+    if (pad_factor > 0) target = std::max(target, pad_factor * n_in);
+    int L = 0, R = 1;
+    choose_fft(target, fp32, causal && pad_factor == 0, L, R);
+    if (key) *key = size_key(L, R);
+    return static_cast<std::size_t>(R) << L;
+}
 
 namespace {
 

@@ -41,6 +41,9 @@ void set_tuning(int L, bool fp32, const Tuning& t);
 // Transient device memory one group of a build may use (0: 45% of the free memory, at
 // most 64 GiB); an instance above it is processed in slices of its frequency triples.
 void set_work_budget(std::size_t bytes);
+// FFT length of the F/C/R convolutions for n_in consumed samples, and its schedule key
+// (the tuning-table key: log2 for powers of two, + 64 for 3 * 2^k, + 128 for 5 * 2^k).
+std::size_t fft_length_for(std::size_t n_in, bool fp32, bool causal, std::size_t pad_factor, int* key);
 Tuning get_tuning(int L, bool fp32);
 void clear_tuning();
 

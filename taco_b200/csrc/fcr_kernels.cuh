@@ -36,7 +36,8 @@ namespace taco {
 
 template <class C>
 struct FftPlan {
-    int L, L1, L2, s;  // Nfft = 2^L, N1 = 2^L1 (column length), N2 = 2^L2 (row length)
+    int L, L1, L2, s;  // Nfft = R*2^L = N1*N2, N1 = R*2^L1 (column length), N2 = 2^L2 (row length)
+    int R;             // odd factor of the length: 1, 3 or 5
     const C* tw1;      // exp(-2 pi i m / N1), m < N1
     const C* tw2;      // exp(-2 pi i m / N2), m < N2
     const C* twc;      // exp(-2 pi i m 2^s / N), m < N / 2^s
@@ -104,7 +105,7 @@ __device__ __forceinline__ double2 phase_minus(double omega, double dt, uint32_t
 // Column tile: 2^log2c columns n2_0 .. n2_0 + 2^log2c - 1, all N1 rows; element
 // (column c, row n1) at pad(n1 * 2^log2c + c).
 // KL, KC >= 0: N1 = 2^KL and the tile width 2^KC fixed at compile time (-1: runtime).
-template <class R, int KL, int KC>
+template <class R, int KL, int KC, int RADIX = 1>
 __device__ __forceinline__ void fwd_col_body(const ColJob* __restrict__ jobs, const FftPlan<cplx_t<R>>& plan, int log2c_rt) {
     using C = cplx_t<R>;
     constexpr bool CT = KL >= 0;
@@ -113,7 +114,7 @@ __device__ __forceinline__ void fwd_col_body(const ColJob* __restrict__ jobs, co
     const ColJob job = jobs[blockIdx.y];
     const int L1 = CT ? KL : plan.L1;
     const int log2c = CT ? KC : log2c_rt;
-    const int nthr = CT ? ((1 << (KL + KC)) / 8) : static_cast<int>(blockDim.x);
+    const int nthr = CT ? ((RADIX << (KL + KC)) / 8) : static_cast<int>(blockDim.x);
     const int N2 = 1 << plan.L2;
     const int ccols = 1 << log2c;
     const int n2_0 = blockIdx.x << log2c;
@@ -154,7 +155,8 @@ __device__ __forceinline__ void fwd_col_body(const ColJob* __restrict__ jobs, co
         s[pad_idx<C>(idx)] = from_d2<C>(x);
     }
     __syncthreads();
-    if constexpr (CT) tile_fft_ct<C, false, true, KL, KC>(s, plan.tw1);
+    if constexpr (CT && RADIX > 1) tile_fft_mx<C, false, true, RADIX, KL, KC>(s, plan.tw1);
+    else if constexpr (CT) tile_fft_ct<C, false, true, KL, KC>(s, plan.tw1);
     else tile_fft<C, false, true>(s, L1, log2c, 1, ccols, plan.tw1);
     C* out = static_cast<C*>(job.out);
 #pragma unroll
@@ -239,7 +241,7 @@ __device__ __forceinline__ void row_body(const RowJob* __restrict__ jobs, const 
 }
 
 // ---------------------------------------------------------------- B3 -------
-template <class R, int KL, int KC>
+template <class R, int KL, int KC, int RADIX = 1>
 __device__ __forceinline__ void inv_col_body(const InvJob* __restrict__ jobs, const FftPlan<cplx_t<R>>& plan, int log2c_rt) {
     using C = cplx_t<R>;
     constexpr bool CT = KL >= 0;
@@ -248,7 +250,7 @@ __device__ __forceinline__ void inv_col_body(const InvJob* __restrict__ jobs, co
     const InvJob job = jobs[blockIdx.y];
     const int L1 = CT ? KL : plan.L1;
     const int log2c = CT ? KC : log2c_rt;
-    const int nthr = CT ? ((1 << (KL + KC)) / 8) : static_cast<int>(blockDim.x);
+    const int nthr = CT ? ((RADIX << (KL + KC)) / 8) : static_cast<int>(blockDim.x);
     const int N2 = 1 << plan.L2;
     const int ccols = 1 << log2c;
     const int n2_0 = blockIdx.x << log2c;
@@ -263,7 +265,8 @@ __device__ __forceinline__ void inv_col_body(const InvJob* __restrict__ jobs, co
 #pragma unroll
     for (int q = 0; q < 8; ++q) s[pad_idx<C>(threadIdx.x + q * nthr)] = x[q];
     __syncthreads();
-    if constexpr (CT) tile_fft_ct<C, true, true, KL, KC>(s, plan.tw1);
+    if constexpr (CT && RADIX > 1) tile_fft_mx<C, true, true, RADIX, KL, KC>(s, plan.tw1);
+    else if constexpr (CT) tile_fft_ct<C, true, true, KL, KC>(s, plan.tw1);
     else tile_fft<C, true, true>(s, L1, log2c, 1, ccols, plan.tw1);
     C* out = static_cast<C*>(job.out);
     const R scale = static_cast<R>(job.scale);
@@ -295,6 +298,17 @@ __global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ?
                                                                        FftPlan<cplx_t<R>> plan, int log2c) {
     fwd_col_body<R, KL, KC>(jobs, plan, log2c);
 }
+// Column passes of the mixed lengths N1 = RADIX * 2^KL (RADIX 3 or 5).
+template <class R, int RADIX, int KL, int KC>
+__global__ void __launch_bounds__((RADIX << (KL + KC)) / 8) k_fwd_col_mx(const ColJob* __restrict__ jobs,
+                                                                         FftPlan<cplx_t<R>> plan, int log2c) {
+    fwd_col_body<R, KL, KC, RADIX>(jobs, plan, log2c);
+}
+template <class R, int RADIX, int KL, int KC>
+__global__ void __launch_bounds__((RADIX << (KL + KC)) / 8) k_inv_col_mx(const InvJob* __restrict__ jobs,
+                                                                         FftPlan<cplx_t<R>> plan, int log2c) {
+    inv_col_body<R, KL, KC, RADIX>(jobs, plan, log2c);
+}
 template <class R, int KL, int KC>
 __global__ void __launch_bounds__(ct_threads(KL, KC), ct_threads(KL, KC) > 256 ? 1 : 2) k_row_ct(const RowJob* __restrict__ jobs,
                                                                    FftPlan<cplx_t<R>> plan, int log2r) {
@@ -317,20 +331,25 @@ __global__ void __launch_bounds__(INV_DFT_THREADS) k_inv_col_dft(const InvJob* _
                                                                   FftPlan<cplx_t<R>> plan, int nrows) {
     using C = cplx_t<R>;
     const InvJob job = jobs[blockIdx.y];
-    const int N1 = 1 << plan.L1, N2 = 1 << plan.L2;
+    const int N1 = plan.R << plan.L1, N2 = 1 << plan.L2;
     const int n2 = blockIdx.x * INV_DFT_THREADS + threadIdx.x;
     if (n2 >= N2) return;
     const C* w = static_cast<const C*>(job.w) + n2;
     C acc[INV_DFT_MAXR];
+    int e[INV_DFT_MAXR];  // (r * k1) mod N1, advanced by r per k1
 #pragma unroll
-    for (int r = 0; r < INV_DFT_MAXR; ++r) acc[r] = C{0, 0};
-    const int mask = N1 - 1;
+    for (int r = 0; r < INV_DFT_MAXR; ++r) {
+        acc[r] = C{0, 0};
+        e[r] = 0;
+    }
 #pragma unroll 4
     for (int k1 = 0; k1 < N1; ++k1) {
         const C x = w[static_cast<size_t>(k1) * N2];
 #pragma unroll
         for (int r = 0; r < INV_DFT_MAXR; ++r) {
-            if (r < nrows) acc[r] = cadd(acc[r], cmulc(x, __ldg(&plan.tw1[(r * k1) & mask])));
+            if (r < nrows) acc[r] = cadd(acc[r], cmulc(x, __ldg(&plan.tw1[e[r]])));
+            e[r] += r;
+            if (e[r] >= N1) e[r] -= N1;
         }
     }
     C* out = static_cast<C*>(job.out);

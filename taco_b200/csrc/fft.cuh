@@ -79,6 +79,40 @@ __device__ __forceinline__ void dft8(C* x) {
     x[7] = csub(e3, t3);
 }
 
+// 3- and 5-point DFTs (radix factors of the mixed lengths 3*2^k and 5*2^k).
+// y_k = sum_r x_r w^{r k}, w = exp(-+ 2 pi i / R); rot90 supplies the -+i.
+template <class C, bool INV>
+__device__ __forceinline__ void dft3(C& x0, C& x1, C& x2) {
+    using R = decltype(x0.x);
+    const R h = static_cast<R>(0.86602540378443864676);  // sin(2 pi / 3)
+    const C t = cadd(x1, x2);
+    const C m = C{x0.x - static_cast<R>(0.5) * t.x, x0.y - static_cast<R>(0.5) * t.y};
+    const C d = rot90<C, INV>(cscale(csub(x1, x2), h));
+    x0 = cadd(x0, t);
+    x1 = cadd(m, d);
+    x2 = csub(m, d);
+}
+
+template <class C, bool INV>
+__device__ __forceinline__ void dft5(C* x) {
+    using R = decltype(x[0].x);
+    const R c1 = static_cast<R>(0.30901699437494742410);   // cos(2 pi / 5)
+    const R c2 = static_cast<R>(-0.80901699437494742410);  // cos(4 pi / 5)
+    const R s1 = static_cast<R>(0.95105651629515357212);   // sin(2 pi / 5)
+    const R s2 = static_cast<R>(0.58778525229247312917);   // sin(4 pi / 5)
+    const C t1 = cadd(x[1], x[4]), t2 = cadd(x[2], x[3]);
+    const C t3 = csub(x[1], x[4]), t4 = csub(x[2], x[3]);
+    const C a1 = C{x[0].x + c1 * t1.x + c2 * t2.x, x[0].y + c1 * t1.y + c2 * t2.y};
+    const C a2 = C{x[0].x + c2 * t1.x + c1 * t2.x, x[0].y + c2 * t1.y + c1 * t2.y};
+    const C b1 = rot90<C, INV>(C{s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y});
+    const C b2 = rot90<C, INV>(C{s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y});
+    x[0] = cadd(x[0], cadd(t1, t2));
+    x[1] = cadd(a1, b1);
+    x[4] = csub(a1, b1);
+    x[2] = cadd(a2, b2);
+    x[3] = csub(a2, b2);
+}
+
 // One Stockham stage of radix 2^LR on a shared-memory tile.
 template <class C, int LR, bool INV, bool F_FAST>
 __device__ __forceinline__ void stockham_stage(C* s, int log2n, int log2nfft, int p, int fs, int es,
@@ -213,6 +247,82 @@ __device__ __forceinline__ void stages_ct(C* s, const C* __restrict__ tw) {
 template <class C, bool INV, bool F_FAST, int LOG2N, int LOG2NFFT, int EPT = 8>
 __device__ __forceinline__ void tile_fft_ct(C* s, const C* __restrict__ tw) {
     stages_ct<C, INV, F_FAST, LOG2N, LOG2NFFT, 1, LOG2N, EPT>(s, tw);
+}
+
+// ---- mixed lengths N = R * 2^a (R = 3 or 5), compile-time sizes ------------------
+// The general Stockham stage: butterfly i of a transform reads x[i + r N/RAD], applies
+// w_{P RAD}^{r k} (k = i mod P) and writes x[(i - k) RAD + k + r P].  Radix 3 and 5 stages
+// stride their butterflies over the threads (EPT / RAD is not an integer); the others
+// keep EPT / RAD consecutive butterflies per thread.
+template <class C, int RAD, bool INV, bool F_FAST, int N, int LOG2NFFT, int P, int EPT>
+__device__ __forceinline__ void stockham_stage_mx(C* s, const C* __restrict__ tw) {
+    constexpr int NB = N / RAD;
+    constexpr int NT = 1 << LOG2NFFT;
+    constexpr int TOTAL = NT * NB;
+    constexpr int NTHR = NT * N / EPT;
+    constexpr bool STRIDED = (EPT % RAD) != 0;
+    constexpr int ITEMS = STRIDED ? (TOTAL + NTHR - 1) / NTHR : EPT / RAD;
+    constexpr int fs = F_FAST ? 1 : N;
+    constexpr int es = F_FAST ? NT : 1;
+    C x[ITEMS * RAD];
+    int base[ITEMS], jout[ITEMS];
+    bool ok[ITEMS];
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+        const int g = STRIDED ? static_cast<int>(threadIdx.x) + q * NTHR : static_cast<int>(threadIdx.x) * ITEMS + q;
+        ok[q] = g < TOTAL;
+        const int gg = ok[q] ? g : 0;
+        int f, i;
+        if (F_FAST) {
+            f = gg % NT;
+            i = gg / NT;
+        } else {
+            f = gg / NB;
+            i = gg % NB;
+        }
+        const int k = i % P;
+        base[q] = f * fs;
+        jout[q] = (i - k) * RAD + k;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) x[q * RAD + r] = s[pad_idx<C>(base[q] + (i + r * NB) * es)];
+        if (P > 1) {
+            const int stride = (N / (P * RAD)) * k;
+#pragma unroll
+            for (int r = 1; r < RAD; ++r) x[q * RAD + r] = mul_w<C, INV>(x[q * RAD + r], __ldg(&tw[r * stride]));
+        }
+        if (RAD == 8) dft8<C, INV>(&x[q * RAD]);
+        else if (RAD == 5) dft5<C, INV>(&x[q * RAD]);
+        else if (RAD == 4) dft4<C, INV>(x[q * RAD], x[q * RAD + 1], x[q * RAD + 2], x[q * RAD + 3]);
+        else if (RAD == 3) dft3<C, INV>(x[q * RAD], x[q * RAD + 1], x[q * RAD + 2]);
+        else dft2<C, INV>(x[q * RAD], x[q * RAD + 1]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+        if (!ok[q]) continue;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) s[pad_idx<C>(base[q] + (jout[q] + r * P) * es)] = x[q * RAD + r];
+    }
+    __syncthreads();
+}
+
+template <class C, bool INV, bool F_FAST, int N, int LOG2NFFT, int P, int REM, int EPT>
+__device__ __forceinline__ void stages_mx_pow2(C* s, const C* __restrict__ tw) {
+    if constexpr (REM > 0) {
+        constexpr int LR2 = (REM % 3 == 2) ? 2 : ((REM % 3 == 1) ? 1 : 3);
+        stockham_stage_mx<C, (1 << LR2), INV, F_FAST, N, LOG2NFFT, P, EPT>(s, tw);
+        stages_mx_pow2<C, INV, F_FAST, N, LOG2NFFT, P * (1 << LR2), REM - LR2, EPT>(s, tw);
+    }
+}
+
+// Transform of length N = RADIX * 2^LOG2A (RADIX 3 or 5): the radix stage first, then the
+// power-of-two stages (radix 4 or 2 first when needed, then 8).  The tile holds 2^LOG2NFFT
+// transforms; EPT * threads == 2^LOG2NFFT * N.  tw[m] = exp(-2 pi i m / N), m < N.
+template <class C, bool INV, bool F_FAST, int RADIX, int LOG2A, int LOG2NFFT, int EPT = 8>
+__device__ __forceinline__ void tile_fft_mx(C* s, const C* __restrict__ tw) {
+    constexpr int N = RADIX << LOG2A;
+    stockham_stage_mx<C, RADIX, INV, F_FAST, N, LOG2NFFT, 1, EPT>(s, tw);
+    stages_mx_pow2<C, INV, F_FAST, N, LOG2NFFT, RADIX, LOG2A, EPT>(s, tw);
 }
 
 }  // namespace taco

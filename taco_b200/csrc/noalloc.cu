@@ -181,6 +181,7 @@ void run(const SystemDesc& sys, const double2* gamma, std::size_t Nt, double dt,
     FftPlan<C> plan;
     plan.L = L;
     plan.L1 = L1;
+    plan.R = 1;
     plan.L2 = L2;
     plan.s = sfine;
     plan.tw1 = tw;

@@ -194,3 +194,25 @@ def test_rk4_vs_oracle_with_samples(D):
     assert relerr(r, r_ref) <= 1e-12
     assert samples.shape == s_ref.shape and relerr(samples, s_ref) <= 1e-12
     assert relerr(ov, s_ref @ obs) <= 1e-12
+
+
+@pytest.mark.parametrize("tmax,nfft", [(10000, 5 << 12), (12000, 3 << 13)])
+def test_mixed_radix_fft_lengths_vs_oracle(tmax, nfft):
+    """The causal rule rounds 2 (tmax + 1) - 1 up to 5 * 2^k or 3 * 2^k when shorter than the
+    next power of two; results match the oracle Direct method on the truncated series."""
+    assert tb.fft_length(tmax + 1, "fp64")[0] == nfft
+    assert tb.fft_length(tmax + 1, "fp32")[0] == nfft
+    assert tb.fft_length(tmax + 1, "fp64", full_length=True)[0] == 1 << (2 * tmax + 1).bit_length()
+    osys, s, G = spin_boson_case(tmax + 500, 0.005)
+    Gt = np.ascontiguousarray(G[:, :tmax + 1])
+    tidx = np.array([0, 1, 17, tmax // 3, tmax - 1, tmax])
+    ref = oracle.tcl4_build_batch(osys.N, osys.nf, osys.omegas, osys.mirror, osys.p2f_colmajor(),
+                                  osys.ops_colmajor(), Gt, 0.005, tidx=tidx, method=oracle.FCR_DIRECT)
+    out = tb.build_TCL4_generator_batch(s, G, 0.005, tidx)
+    assert relerr(out, ref) <= 1e-10
+    out32 = tb.build_TCL4_generator_batch(s, G, 0.005, tidx, precision="fp32")
+    assert relerr(out32, ref) <= 1e-6
+    F, C, R = tb.compute_triple_kernels(s, Gt, 0.005)
+    Fo, Co, Ro = oracle.fcr_series(Gt, osys.omegas, osys.mirror, 0.005)
+    for a, b in ((F, Fo), (C, Co), (R, Ro)):
+        assert relerr(a.reshape(osys.nf ** 3, -1), b) <= 1e-10
