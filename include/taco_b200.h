@@ -218,11 +218,6 @@ int taco_gw_to_liouvillian(const taco_c128* GW, int N, size_t T, taco_c128* L4, 
 int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t* src, taco_c128* coef,
                          size_t cap, size_t* nnz);
 
-/* Launch schedule of the F/C/R passes for FFT length 2^log2_nfft and a precision, as chosen
- * by the autotuner (taco_b200/autotune.py): column / row tile sizes in elements (powers of
- * two in [8, 8192]), bytes of Z/W scratch per chunk of triples (sized to stay in L2), and
- * the largest number of output rows for which the inverse column pass is a pruned direct
- * DFT.  Unset lengths use the defaults (4096, 2048, 48 MiB, 16). */
 /* Transient device memory one group of a build may use (0, the default: 45% of the free
  * memory at the call, at most 64 GiB).  Instances that need more are built in slices of
  * their frequency triples (same results, more passes over the output). */
@@ -231,6 +226,11 @@ int taco_set_work_budget(size_t bytes);
  * the reference's power-of-two rule), and its schedule key for taco_set_tuning: log2 of a
  * power of two, + 64 for 3 * 2^k, + 128 for 5 * 2^k. */
 int taco_fft_length(size_t n_in, int precision, int flags, size_t* nfft, int* key);
+/* Launch schedule of the F/C/R passes for the FFT length with schedule key `log2_nfft`
+ * (taco_fft_length) and a precision, as chosen by the autotuner (taco_b200/autotune.py):
+ * column / row tile sizes in elements (powers of two in [8, 8192]), bytes of Z/W scratch per
+ * chunk of triples, and the largest number of output rows for which the inverse column pass
+ * is a pruned direct DFT.  Unset lengths use the defaults (4096, 2048, 48 MiB, 16). */
 int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows);
 int taco_get_tuning(int log2_nfft, int precision, int* col_tile, int* row_tile, size_t* chunk_bytes,
                     int* inv_dft_rows);

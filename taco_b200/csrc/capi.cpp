@@ -771,7 +771,9 @@ int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t*
 
 int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows) {
     return guarded([&] {
-        if (log2_nfft < 3 || log2_nfft > 22) throw taco::Error(taco::kInvalidArgument, "tuning: log2_nfft out of range");
+        // schedule key: log2 of a power-of-two length (3..22), + 64 for 3 * 2^k, + 128 for 5 * 2^k
+        if ((log2_nfft & 63) < 3 || (log2_nfft & 63) > 22 || log2_nfft >= 192)
+            throw taco::Error(taco::kInvalidArgument, "tuning: schedule key out of range");
         taco::Tuning t = taco::get_tuning(log2_nfft, precision == TACO_PREC_FP32);
         t.col_tile = col_tile;
         t.row_tile = row_tile;
@@ -794,7 +796,9 @@ int taco_get_tuning(int log2_nfft, int precision, int* col_tile, int* row_tile, 
 
 int taco_set_cluster_points(int log2_nfft, int precision, int log2_points) {
     return guarded([&] {
-        if (log2_nfft < 3 || log2_nfft > 22) throw taco::Error(taco::kInvalidArgument, "tuning: log2_nfft out of range");
+        // schedule key: log2 of a power-of-two length (3..22), + 64 for 3 * 2^k, + 128 for 5 * 2^k
+        if ((log2_nfft & 63) < 3 || (log2_nfft & 63) > 22 || log2_nfft >= 192)
+            throw taco::Error(taco::kInvalidArgument, "tuning: schedule key out of range");
         if (log2_points < -1 || log2_points > 13)
             throw taco::Error(taco::kInvalidArgument, "tuning: log2_points must be -1 (automatic), 0 (off) or 3..13");
         taco::Tuning t = taco::get_tuning(log2_nfft, precision == TACO_PREC_FP32);
