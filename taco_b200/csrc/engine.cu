@@ -983,7 +983,10 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         return (static_cast<std::size_t>(maxS) + maxE) * ot * sizeof(C) + csr_bytes;
     };
     while (OTs > 16 && smem_need(OTs) > smem_budget) OTs /= 2;
-    const bool use_rows = contract_rows && same_N;
+    // one thread per time leaves a small group (a single instance) with too few CTAs: the
+    // staged-source kernel spreads its entries over the threads instead
+    const std::size_t row_ctas = (maxT + CONTRACT_ROW_THREADS - 1) / CONTRACT_ROW_THREADS * ni;
+    const bool use_rows = contract_rows && same_N && row_ctas >= 2 * 148;
     const bool contract_smem = !use_rows && maxE < 256 && smem_need(OTs) <= smem_budget;
     const int OT = use_rows ? CONTRACT_ROW_THREADS : OTs;
     const std::size_t csmem = use_rows ? rows_smem : contract_smem ? smem_need(OT) : 0;
