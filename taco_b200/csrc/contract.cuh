@@ -150,6 +150,97 @@ __device__ __forceinline__ uint32_t l4_partner(uint32_t e, int N) {
     return (m + N * n) + N2 * (j + N * i);
 }
 
+// Real coefficients of one term with the source conjugation folded in:
+// c * x      = (a x.x + b x.y, c x.y + d x.x) with (a, b, c, d) = ( c.x, -c.y,  c.x, c.y)
+// c * conj x                                    with (a, b, c, d) = ( c.x,  c.y, -c.x, c.y)
+template <class R>
+struct alignas(4 * sizeof(R)) Coef4 {
+    R a, b, c, d;
+};
+
+template <class C, class R>
+__device__ __forceinline__ void term_mac(C& p, const Coef4<R>& w, C x) {
+    p.x = fma(w.a, x.x, p.x);
+    p.x = fma(w.b, x.y, p.x);
+    p.y = fma(w.c, x.y, p.y);
+    p.y = fma(w.d, x.x, p.y);
+}
+
+// Shared-memory bytes of k_contract_rows_staged for `threads` times, E entries and a table
+// of nnz terms.
+template <class R>
+inline std::size_t rows_staged_smem(int threads, int E, std::size_t nnz) {
+    return static_cast<std::size_t>(threads) * (E + 1) * 2 * sizeof(R) + nnz * (sizeof(Coef4<R>) + 4) +
+           static_cast<std::size_t>(E + 1) * 4 + 64;
+}
+
+// One thread per output time, as k_contract_rows, with the CSR table preprocessed into
+// shared memory once per CTA: four real coefficients per term (conjugation folded in) and
+// the source's element offset s * U (the host guarantees 3 nf^3 U < 2^32).  Terms are
+// summed in groups of four by plain FMAs and each group is added with compensation.
+template <class R>
+__global__ void __launch_bounds__(CONTRACT_ROW_THREADS) k_contract_rows_staged(const ContractJob* __restrict__ jobs,
+                                                                               int N, int nnz_cap) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const ContractJob job = jobs[blockIdx.y];
+    const uint32_t o0 = blockIdx.x * CONTRACT_ROW_THREADS;
+    if (o0 >= job.T) return;
+    const uint32_t E = job.E, ld = E + 1;
+    Coef4<R>* cf = reinterpret_cast<Coef4<R>*>(smem_raw);                      // [nnz_cap]
+    C* res = reinterpret_cast<C*>(cf + nnz_cap);                               // [threads][E + 1]
+    uint32_t* off = reinterpret_cast<uint32_t*>(res + CONTRACT_ROW_THREADS * ld);  // [nnz_cap]
+    int32_t* rp = reinterpret_cast<int32_t*>(off + nnz_cap);                   // [E + 1]
+    const int32_t nnz = __ldg(&job.rowptr[E]);
+    const C* coef = static_cast<const C*>(job.coef);
+    for (int32_t k = threadIdx.x; k < nnz; k += blockDim.x) {
+        const uint32_t sk = __ldg(&job.src[k]);
+        const C w = coef[k];
+        const bool cj = (sk & 0x80000000u) != 0;
+        cf[k] = Coef4<R>{w.x, cj ? w.y : -w.y, cj ? -w.x : w.x, w.y};
+        off[k] = (sk & 0x7fffffffu) * job.U;
+    }
+    for (uint32_t e = threadIdx.x; e <= E; e += blockDim.x) rp[e] = __ldg(&job.rowptr[e]);
+    __syncthreads();
+    const uint32_t ot = min(static_cast<uint32_t>(CONTRACT_ROW_THREADS), job.T - o0);
+    const uint32_t o = o0 + threadIdx.x;
+    if (threadIdx.x < ot) {
+        const C* v = static_cast<const C*>(job.v) + __ldg(&job.out_u[o]);
+        for (uint32_t e = 0; e < E; ++e) {
+            if (l4_partner(e, N) < e) continue;
+            EntryAcc<C> acc;
+            int32_t k = rp[e];
+            const int32_t end = rp[e + 1];
+            for (; k + 4 <= end; k += 4) {
+                const C x0 = v[off[k]], x1 = v[off[k + 1]], x2 = v[off[k + 2]], x3 = v[off[k + 3]];
+                C p{0, 0};
+                term_mac(p, cf[k], x0);
+                term_mac(p, cf[k + 1], x1);
+                term_mac(p, cf[k + 2], x2);
+                term_mac(p, cf[k + 3], x3);
+                acc.add(p);
+            }
+            for (; k < end; ++k) {
+                C p{0, 0};
+                term_mac(p, cf[k], v[off[k]]);
+                acc.add(p);
+            }
+            res[threadIdx.x * ld + e] = acc.get();
+        }
+        for (uint32_t e = 0; e < E; ++e) {
+            const uint32_t p = l4_partner(e, N);
+            if (p < e) res[threadIdx.x * ld + e] = cconj(res[threadIdx.x * ld + p]);
+        }
+    }
+    __syncthreads();
+    C* out = static_cast<C*>(job.out) + static_cast<size_t>(o0) * E;
+    const uint32_t total = ot * E;
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const uint32_t ol = idx / E, e = idx - ol * E;
+        out[idx] = job.accumulate ? cadd(out[idx], res[ol * ld + e]) : res[ol * ld + e];
+    }
+}
+
 template <class R>
 __global__ void __launch_bounds__(CONTRACT_ROW_THREADS) k_contract_rows(const ContractJob* __restrict__ jobs, int N) {
     using C = cplx_t<R>;

@@ -987,10 +987,20 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     // staged-source kernel spreads its entries over the threads instead
     const std::size_t row_ctas = (maxT + CONTRACT_ROW_THREADS - 1) / CONTRACT_ROW_THREADS * ni;
     const bool use_rows = contract_rows && same_N && row_ctas >= 2 * 148;
+    // the rows kernel with its table preprocessed into shared memory when the table fits and
+    // every source offset s * U fits 32 bits
+    const std::size_t staged_smem = rows_staged_smem<R>(CONTRACT_ROW_THREADS, maxE, maxNnz);
+    const bool offsets_32 = [&] {
+        for (auto* u : units)
+            if (static_cast<std::size_t>(3) * u->nsub() * u->meta->U >= (std::size_t(1) << 32)) return false;
+        return true;
+    }();
+    const bool rows_staged = use_rows && offsets_32 && staged_smem <= 100 * 1024;
     const bool contract_smem = !use_rows && maxE < 256 && smem_need(OTs) <= smem_budget;
     const int OT = use_rows ? CONTRACT_ROW_THREADS : OTs;
-    const std::size_t csmem = use_rows ? rows_smem : contract_smem ? smem_need(OT) : 0;
-    if (use_rows) set_smem(k_contract_rows<R>, csmem);
+    const std::size_t csmem = rows_staged ? staged_smem : use_rows ? rows_smem : contract_smem ? smem_need(OT) : 0;
+    if (rows_staged) set_smem(k_contract_rows_staged<R>, csmem);
+    else if (use_rows) set_smem(k_contract_rows<R>, csmem);
     else if (contract_smem) set_smem(k_contract_smem<R>, csmem);
     const int nnz_cap = static_cast<int>(maxNnz);
     struct D2H {
@@ -1083,7 +1093,11 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     if (ev1) cuda_check(cudaEventRecord(ev1, st), "cudaEventRecord");
     if (!fcr_only) {
         pr.before(f32 ? "contract_f32" : "contract_f64");
-        if (use_rows) {
+        if (rows_staged) {
+            const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
+            k_contract_rows_staged<R><<<dim3(gx, static_cast<unsigned>(ni)), CONTRACT_ROW_THREADS, csmem, st>>>(
+                Mc.conj, maxN, nnz_cap);
+        } else if (use_rows) {
             const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
             k_contract_rows<R><<<dim3(gx, static_cast<unsigned>(ni)), CONTRACT_ROW_THREADS, csmem, st>>>(Mc.conj, maxN);
         } else if (contract_smem) {
