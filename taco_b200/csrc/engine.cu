@@ -1076,7 +1076,7 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     if (scan_single) {
         // enough triples to fill the GPU: one CTA per triple walks its whole time axis
         pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
-        k_scan_assemble<R><<<static_cast<unsigned>(n_scan), SCAN_THREADS, 0, st>>>(Mc.scanj);
+        k_scan_assemble<R, 2, 4><<<static_cast<unsigned>(n_scan), SCAN_THREADS, 0, st>>>(Mc.scanj);
         check_launch("k_scan_assemble", &pr);
     }
     for (std::size_t s0 = 0; !scan_single && s0 < n_scan; s0 += 65535) {

@@ -380,12 +380,12 @@ __device__ __forceinline__ void scan_integrands(const ScanJob& job, uint32_t t, 
     v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
 }
 
-// One CTA per triple, SCAN_ITEMS consecutive samples per thread, FP64 sums and carries.
+// One CTA per triple, ITEMS consecutive samples per thread, FP64 sums and carries.
 // Pass 1 of a tile sums each thread's samples; after the block scan, pass 2 recomputes
 // the integrands (cheaper than keeping them live: it doubles the occupancy) and
 // assembles F, C, R at the requested times.
-template <class R>
-__global__ void __launch_bounds__(SCAN_THREADS, 3) k_scan_assemble(const ScanJob* __restrict__ jobs) {
+template <class R, int ITEMS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(SCAN_THREADS, MIN_BLOCKS) k_scan_assemble(const ScanJob* __restrict__ jobs) {
     using C = cplx_t<R>;
     __shared__ double warp_tot[SCAN_THREADS / 32][SCAN_W];
     __shared__ double carry[SCAN_W];
@@ -402,18 +402,21 @@ __global__ void __launch_bounds__(SCAN_THREADS, 3) k_scan_assemble(const ScanJob
     const double2 cj = __ldg(&job.gj[job.n_in - 1]);
     const double dt = job.dt;
     const double2 step = phase_minus(job.omega, dt, 1);  // e^{-i w dt}: phases by recurrence over a thread's samples
-    const uint32_t tile = SCAN_THREADS * SCAN_ITEMS;
+    const uint32_t tile = SCAN_THREADS * ITEMS;
+    const double2 tile_step = phase_minus(job.omega, dt, tile);  // and from one tile to the next
+    double2 pm_next = phase_minus(job.omega, dt, threadIdx.x * ITEMS);
     __syncthreads();
     for (uint32_t t0 = 0; t0 < job.t_count; t0 += tile) {
-        const uint32_t tb = t0 + threadIdx.x * SCAN_ITEMS;
+        const uint32_t tb = t0 + threadIdx.x * ITEMS;
         double run[SCAN_W];
 #pragma unroll
         for (int k = 0; k < SCAN_W; ++k) run[k] = 0.0;
-        const double2 pm0 = phase_minus(job.omega, dt, tb);
+        const double2 pm0 = pm_next;
+        pm_next = cmul(pm_next, tile_step);
         {
             double2 pm = pm0;
 #pragma unroll
-            for (int q = 0; q < SCAN_ITEMS; ++q) {
+            for (int q = 0; q < ITEMS; ++q) {
                 const uint32_t t = tb + q;
                 if (t < job.t_count) {
                     double v[SCAN_W];
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(SCAN_THREADS, 3) k_scan_assemble(const ScanJob
         }
         double2 pm = pm0;
 #pragma unroll
-        for (int q = 0; q < SCAN_ITEMS; ++q, pm = cmul(pm, step)) {
+        for (int q = 0; q < ITEMS; ++q, pm = cmul(pm, step)) {
             const uint32_t t = tb + q;
             if (t >= job.t_count) break;
             const double2 gi = __ldg(&job.gi[t]);

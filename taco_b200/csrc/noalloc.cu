@@ -297,7 +297,7 @@ void run(const SystemDesc& sys, const double2* gamma, std::size_t Nt, double dt,
         }
         cuda_check(cudaGetLastError(), "k_inv_col");
     }
-    k_scan_assemble<R><<<static_cast<unsigned>(nf3), SCAN_THREADS, 0, st>>>(sjd);
+    k_scan_assemble<R, SCAN_ITEMS, 3><<<static_cast<unsigned>(nf3), SCAN_THREADS, 0, st>>>(sjd);
     cuda_check(cudaGetLastError(), "k_scan_assemble");
     const int OT = std::max(1, std::min(128, static_cast<int>((48 * 1024) / (E * sizeof(C)))));
     const std::size_t csmem = static_cast<std::size_t>(OT) * E * sizeof(C);
