@@ -952,6 +952,10 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     const ColFn<R> fwd_col = fwd_col_fn<R>(plan.R, plan.L1, g.log2c);
     const InvFn<R> inv_col = inv_col_fn<R>(plan.R, plan.L1, g.log2c);
     const RowFn<R> row = row_fn<R>(plan.L2, g.log2r);
+    // 256-point rows: one warp per row with the transform in registers
+    const bool row_warp = plan.L2 == 8;
+    const int n_rows = plan.R << plan.L1;  // N1
+    const unsigned wrow_grid = static_cast<unsigned>((n_rows + WROW_WARPS - 1) / WROW_WARPS);
     set_smem(fwd_col, g.col_smem);
     set_smem(inv_col, g.col_smem);
     set_smem(row, g.row_smem);
@@ -1047,8 +1051,12 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
             Mc.colj, plan, g.log2c);
         check_launch("k_fwd_col(spectra)", &pr);
         pr.before(f32 ? "spectra_row_f32" : "spectra_row_f64");
-        row<<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
-            Mc.rowj, plan, g.log2r);
+        if (row_warp)
+            k_row_warp256<R><<<dim3(wrow_grid, static_cast<unsigned>(n_spec_jobs)), WROW_THREADS, 0, st>>>(
+                Mc.rowj, plan, n_rows);
+        else
+            row<<<dim3(g.row_grid, static_cast<unsigned>(n_spec_jobs)), g.row_threads, g.row_smem, st>>>(
+                Mc.rowj, plan, g.log2r);
         check_launch("k_row(spectra)", &pr);
         const unsigned dft_grid = static_cast<unsigned>((N2 + INV_DFT_THREADS - 1) / INV_DFT_THREADS);
         for (std::size_t ch = 0; ch < nchunks; ++ch) {
@@ -1058,8 +1066,12 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
                 Mc.colj + n_spec_jobs + q0, plan, g.log2c);
             check_launch("k_fwd_col", &pr);
             pr.before(f32 ? "row_conv_f32" : "row_conv_f64");
-            row<<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
-                Mc.rowj + n_spec_jobs + q0, plan, g.log2r);
+            if (row_warp)
+                k_row_warp256<R><<<dim3(wrow_grid, static_cast<unsigned>(nq)), WROW_THREADS, 0, st>>>(
+                    Mc.rowj + n_spec_jobs + q0, plan, n_rows);
+            else
+                row<<<dim3(g.row_grid, static_cast<unsigned>(nq)), g.row_threads, g.row_smem, st>>>(
+                    Mc.rowj + n_spec_jobs + q0, plan, g.log2r);
             check_launch("k_row", &pr);
             pr.before(f32 ? "inv_col_f32" : "inv_col_f64");
             if (inv_dft) {

@@ -240,6 +240,141 @@ __device__ __forceinline__ void row_body(const RowJob* __restrict__ jobs, const 
     }
 }
 
+// ------------------------------------------------------ B2, one warp per row ----
+// 256-point row transforms held in registers, 8 elements per lane, as 256 = 8 * 8 * 4:
+//   x[l + 32 r] (lane l, r < 8) --DFT8 over r--> k1; twiddle w256^(l k1);
+//   transpose 1: lane (q, a) = (lane / 4, lane % 4) takes z_b = y_{a + 4 b}[q], b < 8;
+//   --DFT8 over b--> c; twiddle w256^(8 a c) (= w32^(a c));
+//   transpose 2: lane takes the pairs P = 2 lane + h (h < 2), each with its 4 values of a;
+//   --DFT4 over a--> d:  element 4 h + d holds X[k] with k = P / 8 + 8 (P % 8) + 64 d.
+// The inverse runs the same steps backwards with conjugate twiddles (unnormalised), so
+// a forward transform, an elementwise product in that register order and an inverse
+// give the cyclic convolution in natural order.  Both transposes go through a
+// warp-private shared buffer with padding that keeps every access conflict-free
+// (rows of 36 for the first, P * 4 + a + P / 2 for the second); the warp never waits
+// on other warps.
+constexpr int WROW_WARPS = 8;
+constexpr int WROW_THREADS = 32 * WROW_WARPS;
+constexpr int WROW_BUF = 288;
+
+__device__ __forceinline__ int wrow_k(int lane, int j) {
+    const int P = 2 * lane + (j >> 2), d = j & 3;
+    return (P >> 3) + 8 * (P & 7) + 64 * d;
+}
+
+template <class C, bool INV>
+__device__ __forceinline__ void warp_fft256(C (&x)[8], C* buf, const C* __restrict__ tw, int lane) {
+    const int q = lane >> 2, a = lane & 3;
+    if (!INV) {
+        dft8<C, false>(x);
+#pragma unroll
+        for (int k = 1; k < 8; ++k) x[k] = cmul(x[k], __ldg(&tw[(lane * k) & 255]));
+#pragma unroll
+        for (int k = 0; k < 8; ++k) buf[k * 36 + lane] = x[k];
+        __syncwarp();
+#pragma unroll
+        for (int b = 0; b < 8; ++b) x[b] = buf[q * 36 + a + 4 * b];
+        __syncwarp();
+        dft8<C, false>(x);
+#pragma unroll
+        for (int c = 1; c < 8; ++c) x[c] = cmul(x[c], __ldg(&tw[(8 * a * c) & 255]));
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int P = q * 8 + c;
+            buf[P * 4 + a + (P >> 1)] = x[c];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int P = 2 * lane + h;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) x[4 * h + e] = buf[P * 4 + e + (P >> 1)];
+        }
+        __syncwarp();
+        dft4<C, false>(x[0], x[1], x[2], x[3]);
+        dft4<C, false>(x[4], x[5], x[6], x[7]);
+    } else {
+        dft4<C, true>(x[0], x[1], x[2], x[3]);
+        dft4<C, true>(x[4], x[5], x[6], x[7]);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int P = 2 * lane + h;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) buf[P * 4 + e + (P >> 1)] = x[4 * h + e];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int P = q * 8 + c;
+            x[c] = buf[P * 4 + a + (P >> 1)];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int c = 1; c < 8; ++c) x[c] = cmulc(x[c], __ldg(&tw[(8 * a * c) & 255]));
+        dft8<C, true>(x);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) buf[q * 36 + a + 4 * b] = x[b];
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = buf[k * 36 + lane];
+        __syncwarp();
+#pragma unroll
+        for (int k = 1; k < 8; ++k) x[k] = cmulc(x[k], __ldg(&tw[(lane * k) & 255]));
+        dft8<C, true>(x);
+    }
+}
+
+// B2 for N2 = 256: one warp per row (row k1 of the job's N1 rows).  Spectra jobs
+// (spec_f == nullptr) write the forward row transform; triple jobs multiply it by both
+// partner spectra (loaded while the forward transform runs), invert each product, apply
+// the inverse inter-step twiddle and write W_F (in place) and W_C.
+template <class R>
+__global__ void __launch_bounds__(WROW_THREADS) k_row_warp256(const RowJob* __restrict__ jobs, FftPlan<cplx_t<R>> plan,
+                                                               int n_rows) {
+    using C = cplx_t<R>;
+    __shared__ C bufs[WROW_WARPS][WROW_BUF];
+    const RowJob job = jobs[blockIdx.y];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int row = blockIdx.x * WROW_WARPS + warp;
+    if (row >= n_rows) return;
+    const size_t off = static_cast<size_t>(row) * 256;
+    C* data = static_cast<C*>(job.data) + off;
+    C* buf = bufs[warp];
+    C x[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) x[r] = data[lane + 32 * r];
+    const bool conv = job.spec_f != nullptr;
+    C sf[8], sc[8];
+    if (conv) {
+        const C* spf = static_cast<const C*>(job.spec_f) + off;
+        const C* spc = static_cast<const C*>(job.spec_c) + off;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            sf[j] = __ldg(&spf[wrow_k(lane, j)]);
+            sc[j] = __ldg(&spc[wrow_k(lane, j)]);
+        }
+    }
+    warp_fft256<C, false>(x, buf, plan.tw2, lane);
+    if (!conv) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) data[wrow_k(lane, j)] = x[j];
+        return;
+    }
+#pragma unroll
+    for (int which = 0; which < 2; ++which) {
+        C y[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) y[j] = cmul(x[j], which == 0 ? sf[j] : sc[j]);
+        warp_fft256<C, true>(y, buf, plan.tw2, lane);
+        C* dst = which == 0 ? data : static_cast<C*>(job.wc) + off;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const uint32_t n2 = static_cast<uint32_t>(lane + 32 * r);
+            dst[n2] = cmulc(y[r], inter_twiddle(plan, n2 * static_cast<uint32_t>(row)));
+        }
+    }
+}
+
 // ---------------------------------------------------------------- B3 -------
 template <class R, int KL, int KC, int RADIX = 1>
 __device__ __forceinline__ void inv_col_body(const InvJob* __restrict__ jobs, const FftPlan<cplx_t<R>>& plan, int log2c_rt) {
