@@ -536,11 +536,15 @@ __global__ void __launch_bounds__(SCAN_THREADS, MIN_BLOCKS) k_scan_assemble(cons
     const double2 cmj = __ldg(&job.gmj[job.n_in - 1]);
     const double2 cj = __ldg(&job.gj[job.n_in - 1]);
     const double dt = job.dt;
-    const double2 step = phase_minus(job.omega, dt, 1);  // e^{-i w dt}: phases by recurrence over a thread's samples
+    // e^{-i w dt} and e^{-i w tile dt}: phases by recurrence over a thread's samples and
+    // from one tile to the next (computed once per CTA)
+    __shared__ double2 steps[2];
     const uint32_t tile = SCAN_THREADS * ITEMS;
-    const double2 tile_step = phase_minus(job.omega, dt, tile);  // and from one tile to the next
+    if (threadIdx.x == 0) steps[0] = phase_minus(job.omega, dt, 1);
+    if (threadIdx.x == 32) steps[1] = phase_minus(job.omega, dt, tile);
     double2 pm_next = phase_minus(job.omega, dt, threadIdx.x * ITEMS);
     __syncthreads();
+    const double2 step = steps[0], tile_step = steps[1];
     for (uint32_t t0 = 0; t0 < job.t_count; t0 += tile) {
         const uint32_t tb = t0 + threadIdx.x * ITEMS;
         double run[SCAN_W];
