@@ -581,11 +581,15 @@ __global__ void __launch_bounds__(SCAN_THREADS, MIN_BLOCKS) k_scan_assemble(cons
             pre[k] = lane == 0 ? 0.0 : excl;
         }
         __syncthreads();
+        {
+            // lane k < SCAN_W adds the carry and the preceding warps' totals of component k
+            double wk = 0.0;
+            if (lane < SCAN_W) {
+                wk = carry[lane];
+                for (int q = 0; q < warp; ++q) wk += warp_tot[q][lane];
+            }
 #pragma unroll
-        for (int k = 0; k < SCAN_W; ++k) {
-            double w = 0.0;
-            for (int q = 0; q < warp; ++q) w += warp_tot[q][k];
-            pre[k] = carry[k] + (w + pre[k]);
+            for (int k = 0; k < SCAN_W; ++k) pre[k] += __shfl_sync(0xffffffffu, wk, k);
         }
         double2 pm = pm0;
 #pragma unroll
