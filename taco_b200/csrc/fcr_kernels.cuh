@@ -522,11 +522,12 @@ __device__ __forceinline__ void scan_integrands(const ScanJob& job, uint32_t t, 
 template <class R, int ITEMS, int MIN_BLOCKS>
 __global__ void __launch_bounds__(SCAN_THREADS, MIN_BLOCKS) k_scan_assemble(const ScanJob* __restrict__ jobs) {
     using C = cplx_t<R>;
-    __shared__ double warp_tot[SCAN_THREADS / 32][SCAN_W];
-    __shared__ double carry[SCAN_W];
+    // warp totals and carries double-buffered by tile parity: one block barrier per tile
+    __shared__ double warp_tot[2][SCAN_THREADS / 32][SCAN_W];
+    __shared__ double carry[2][SCAN_W];
     const ScanJob job = jobs[blockIdx.x];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x < SCAN_W) carry[threadIdx.x] = 0.0;
+    if (threadIdx.x < SCAN_W) carry[0][threadIdx.x] = 0.0;
     const C* cf = static_cast<const C*>(job.conv_f);
     const C* cc = static_cast<const C*>(job.conv_c);
     C* vf = static_cast<C*>(job.vf);
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(SCAN_THREADS, MIN_BLOCKS) k_scan_assemble(cons
     double2 pm_next = phase_minus(job.omega, dt, threadIdx.x * ITEMS);
     __syncthreads();
     const double2 step = steps[0], tile_step = steps[1];
-    for (uint32_t t0 = 0; t0 < job.t_count; t0 += tile) {
+    for (uint32_t t0 = 0, par = 0; t0 < job.t_count; t0 += tile, par ^= 1u) {
         const uint32_t tb = t0 + threadIdx.x * ITEMS;
         double run[SCAN_W];
 #pragma unroll
@@ -576,17 +577,19 @@ __global__ void __launch_bounds__(SCAN_THREADS, MIN_BLOCKS) k_scan_assemble(cons
                 const double nb = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= o) x += nb;
             }
-            if (lane == 31) warp_tot[warp][k] = x;
+            if (lane == 31) warp_tot[par][warp][k] = x;
             double excl = __shfl_up_sync(0xffffffffu, x, 1);
             pre[k] = lane == 0 ? 0.0 : excl;
         }
         __syncthreads();
         {
             // lane k < SCAN_W adds the carry and the preceding warps' totals of component k
+            // (the last warp also leaves the next tile's carry in the other buffer)
             double wk = 0.0;
             if (lane < SCAN_W) {
-                wk = carry[lane];
-                for (int q = 0; q < warp; ++q) wk += warp_tot[q][lane];
+                wk = carry[par][lane];
+                for (int q = 0; q < warp; ++q) wk += warp_tot[par][q][lane];
+                if (warp == SCAN_THREADS / 32 - 1) carry[par ^ 1u][lane] = wk + warp_tot[par][warp][lane];
             }
 #pragma unroll
             for (int k = 0; k < SCAN_W; ++k) pre[k] += __shfl_sync(0xffffffffu, wk, k);
@@ -614,13 +617,6 @@ __global__ void __launch_bounds__(SCAN_THREADS, MIN_BLOCKS) k_scan_assemble(cons
             vc[u] = from_d2<C>(csub(cmulc(dip, PR1), convc));  // P_C = conj(P_R1)
             vr[u] = from_d2<C>(csub(cmul(gi, PR1), PR2));
         }
-        __syncthreads();
-        if (threadIdx.x < SCAN_W) {
-            double w = 0.0;
-            for (int q = 0; q < SCAN_THREADS / 32; ++q) w += warp_tot[q][threadIdx.x];
-            carry[threadIdx.x] += w;
-        }
-        __syncthreads();
     }
 }
 
