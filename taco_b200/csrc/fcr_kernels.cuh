@@ -253,7 +253,7 @@ __device__ __forceinline__ void row_body(const RowJob* __restrict__ jobs, const 
 // warp-private shared buffer with padding that keeps every access conflict-free
 // (rows of 36 for the first, P * 4 + a + P / 2 for the second); the warp never waits
 // on other warps.
-constexpr int WROW_WARPS = 8;
+constexpr int WROW_WARPS = 4;
 constexpr int WROW_THREADS = 32 * WROW_WARPS;
 constexpr int WROW_BUF = 288;
 
