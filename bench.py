@@ -178,22 +178,26 @@ def ncu_traffic():
 
 
 def kernel_model_bytes(name, inst_shape):
-    """Algorithmic bytes per unit (unit = triple, or spectrum for the spectra passes)."""
-    Nt, nfft, tcount, U, nf = inst_shape
+    """Algorithmic bytes per unit (unit = triple, or spectrum for the spectra passes): the
+    traffic the kernel cannot avoid.  Inputs shared by all triples of an instance (its nf
+    Gamma columns, its 2 nf partner spectra) count once per instance, spread over its nf^3
+    triples; per-triple arrays (Z, W_F, W_C, the convolutions, F/C/R) count in full."""
+    n_in, nfft, tcount, U, nf = inst_shape
     s = 8 if name.endswith("f32") else 16
     base = name.rsplit("_", 1)[0]
-    if base == "fwd_col":
-        return Nt * 16 + nfft * s, "triple"
-    if base == "row_conv":
-        return 5 * nfft * s, "triple"
-    if base == "inv_col":
+    per_tri = lambda per_instance: per_instance / nf ** 3
+    if base == "fwd_col":  # Gamma_i shared; Z written
+        return per_tri(nf * n_in * 16) + nfft * s, "triple"
+    if base == "row_conv":  # Z in; W_F, W_C out; partner spectra shared
+        return 3 * nfft * s + per_tri(2 * nf * nfft * s), "triple"
+    if base == "inv_col":  # W_F, W_C in; both convolutions (t <= t_max) out
         return 2 * nfft * s + 2 * tcount * s, "triple"
-    if base == "spectra_col":
-        return Nt * 16 + nfft * s, "spectrum"
+    if base == "spectra_col":  # each Gamma column feeds two spectra
+        return n_in * 16 / 2 + nfft * s, "spectrum"
     if base == "spectra_row":
         return 2 * nfft * s, "spectrum"
-    if base == "scan_assemble":
-        return 3 * tcount * 16 + 2 * tcount * s + 3 * U * s, "triple"
+    if base == "scan_assemble":  # Gamma shared; conv in; F, C, R at the requested times out
+        return per_tri(nf * tcount * 16) + 2 * tcount * s + 3 * U * s, "triple"
     return None, None
 
 
