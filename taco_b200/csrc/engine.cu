@@ -20,6 +20,8 @@
 #include <map>
 #include <memory>
 #include <unordered_map>
+#include <thread>
+#include <exception>
 
 #include "cluster_conv.cuh"
 #include "contract.cuh"
@@ -480,8 +482,41 @@ struct InstMeta {
     int L = 0, R = 1;  // FFT length R * 2^L
     std::vector<int> tmap;          // [t_count]
     std::vector<uint32_t> out_u;    // [T]
-    CoefTable coef;
+    std::shared_ptr<const CoefTable> coef;  // shared with the table cache (empty when unused)
 };
+
+// Coefficient tables by system content (N, nf, pair_to_freq, coupling operators): the
+// table depends on nothing else, so repeated builds of the same systems (parameter sweeps
+// over baths and times, repeated calls) skip the NAKZWAN walk.  Bounded by total bytes;
+// the cache is dropped when a new table would exceed the bound.
+std::shared_ptr<const CoefTable> coef_table_for(const SystemDesc& s) {
+    static std::mutex mu;
+    static std::unordered_map<std::string, std::shared_ptr<const CoefTable>> cache;
+    static std::size_t cached_bytes = 0;
+    constexpr std::size_t kMaxBytes = std::size_t(512) << 20;
+    std::string key;
+    key.reserve(12 + s.p2f.size() * sizeof(int) + s.ops.size() * sizeof(double2));
+    const int head[3] = {s.N, s.nf, s.num_ops};
+    key.append(reinterpret_cast<const char*>(head), sizeof(head));
+    key.append(reinterpret_cast<const char*>(s.p2f.data()), s.p2f.size() * sizeof(int));
+    key.append(reinterpret_cast<const char*>(s.ops.data()), s.ops.size() * sizeof(double2));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    auto t = std::make_shared<CoefTable>();
+    build_coef_table(s.N, s.nf, s.p2f.data(), s.ops.data(), s.num_ops, *t);
+    const std::size_t bytes = key.size() + t->rowptr.size() * 4 + t->src.size() * 4 + t->coef.size() * 16 +
+                              t->triple_fc_used.size() + t->triple_r_used.size();
+    std::lock_guard<std::mutex> lk(mu);
+    if (cached_bytes + bytes > kMaxBytes) {
+        cache.clear();
+        cached_bytes = 0;
+    }
+    if (bytes <= kMaxBytes && cache.emplace(key, t).second) cached_bytes += bytes;
+    return t;
+}
 
 // FFT length for a linear convolution of `target` outputs: the next power of two, or (when
 // allowed: the causal rule) 3 * 2^k or 5 * 2^k if shorter and column kernels exist for
@@ -515,22 +550,34 @@ void choose_fft(std::size_t target, bool fp32, bool allow_mixed, int& L_out, int
 void derive_meta(const Tcl4Instance& in, const BuildOptions& opt, InstMeta& m, bool want_coef) {
     m.T = in.tidx.size();
     uint32_t tmax = 0;
-    for (uint32_t t : in.tidx) tmax = std::max(tmax, t);
+    bool increasing = true;
+    for (std::size_t o = 0; o < m.T; ++o) {
+        tmax = std::max(tmax, in.tidx[o]);
+        if (o > 0 && in.tidx[o] <= in.tidx[o - 1]) increasing = false;
+    }
     m.t_count = static_cast<std::size_t>(tmax) + 1;
-    std::vector<uint32_t> uniq(in.tidx);
-    std::sort(uniq.begin(), uniq.end());
-    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-    m.U = uniq.size();
     m.tmap.assign(m.t_count, -1);
-    for (std::size_t u = 0; u < uniq.size(); ++u) m.tmap[uniq[u]] = static_cast<int>(u);
     m.out_u.resize(m.T);
-    for (std::size_t o = 0; o < m.T; ++o) m.out_u[o] = static_cast<uint32_t>(m.tmap[in.tidx[o]]);
+    if (increasing) {  // the unique times are the requested ones, in order
+        m.U = m.T;
+        for (std::size_t o = 0; o < m.T; ++o) {
+            m.tmap[in.tidx[o]] = static_cast<int>(o);
+            m.out_u[o] = static_cast<uint32_t>(o);
+        }
+    } else {
+        std::vector<uint32_t> uniq(in.tidx);
+        std::sort(uniq.begin(), uniq.end());
+        uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+        m.U = uniq.size();
+        for (std::size_t u = 0; u < uniq.size(); ++u) m.tmap[uniq[u]] = static_cast<int>(u);
+        for (std::size_t o = 0; o < m.T; ++o) m.out_u[o] = static_cast<uint32_t>(m.tmap[in.tidx[o]]);
+    }
     m.n_in = opt.causal_truncation ? m.t_count : in.Nt;
     std::size_t target = 2 * m.n_in - 1;
     if (opt.pad_factor > 0) target = std::max(target, opt.pad_factor * m.n_in);
     choose_fft(target, opt.fp32, opt.causal_truncation && opt.pad_factor == 0, m.L, m.R);
-    if (want_coef)
-        build_coef_table(in.sys.N, in.sys.nf, in.sys.p2f.data(), in.sys.ops.data(), in.sys.num_ops, m.coef);
+    static const std::shared_ptr<const CoefTable> kEmpty = std::make_shared<CoefTable>();
+    m.coef = want_coef ? coef_table_for(in.sys) : kEmpty;
 }
 
 struct TripleRef {
@@ -869,21 +916,18 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
             c.accumulate = units[a]->accumulate ? 1u : 0u;
         }
     }
-    // pack everything small into the pinned staging buffer
+    // pack everything small into the pinned staging buffer as an image of the metadata
+    // buffer's layout (offset of each array = its offset in meta_mem), copied in one piece
     struct Copy {
-        void* dst;
         std::size_t off, bytes;
     };
     std::vector<Copy> copies;
     std::size_t soff = 0;
-    auto stage_size = [&](std::size_t bytes) {
-        soff = align_up(soff, 64);
-        const std::size_t o = soff;
-        soff += bytes;
-        return o;
-    };
     auto plan_copy = [&](void* dst, std::size_t bytes) {
-        if (bytes) copies.push_back({dst, stage_size(bytes), bytes});
+        if (!bytes) return;
+        const std::size_t o = static_cast<std::size_t>(static_cast<char*>(dst) - static_cast<char*>(meta_mem.p));
+        copies.push_back({o, bytes});
+        soff = std::max(soff, o + bytes);
     };
     plan_copy(M.colj, colj.size() * sizeof(ColJob));
     plan_copy(M.rowj, rowj.size() * sizeof(RowJob));
@@ -935,8 +979,7 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
             }
         }
     }
-    for (const Copy& c : copies)
-        cuda_check(cudaMemcpyAsync(c.dst, sb + c.off, c.bytes, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(meta)");
+    if (soff) cuda_check(cudaMemcpyAsync(meta_mem.p, sb, soff, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(meta)");
     // host gamma: only the n_in leading samples of each bucket are consumed
     for (std::size_t a = 0; a < ni; ++a)
         if (!units[a]->in->gamma_on_device)
@@ -1175,7 +1218,7 @@ std::vector<std::vector<WorkUnit*>> plan_units(std::vector<Tcl4Instance>& insts,
             unit->meta = &metas[a];
             unit->lo = 0;
             unit->hi = nf3;
-            unit->coef = &metas[a].coef;
+            unit->coef = metas[a].coef.get();
             std::vector<WorkUnit*> one{unit.get()};
             const std::size_t need = measure_work<R>(one, false, false);
             if (need > budget) {
@@ -1197,7 +1240,7 @@ std::vector<std::vector<WorkUnit*>> plan_units(std::vector<Tcl4Instance>& insts,
                     u->lo = lo;
                     u->hi = std::min(nf3, lo + static_cast<int>(nsub));
                     u->accumulate = lo > 0;
-                    u->own = slice_table(metas[a].coef, u->lo, u->hi);
+                    u->own = slice_table(*metas[a].coef, u->lo, u->hi);
                     u->coef = u->own.get();
                     groups.push_back({u.get()});
                     store.push_back(std::move(u));
@@ -1244,7 +1287,7 @@ void stage_sliced_io(std::vector<Tcl4Instance>& insts, std::vector<InstMeta>& me
         u.in = &in;
         u.meta = &metas[a];
         u.hi = in.sys.nf * in.sys.nf * in.sys.nf;
-        u.coef = &metas[a].coef;
+        u.coef = metas[a].coef.get();
         std::vector<WorkUnit*> one{&u};
         if (measure_work<R>(one, false, false) <= budget) continue;
         if (!in.gamma_on_device) {
@@ -1453,7 +1496,7 @@ void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_d
     u.in = &in;
     u.meta = &m;
     u.hi = s.nf * s.nf * s.nf;
-    u.coef = &m.coef;
+    u.coef = m.coef.get();
     std::vector<WorkUnit*> gu{&u};
     double2* outs[3] = {F, Cc, R};
     if (opt.fcr_ms) *opt.fcr_ms = 0.0;
@@ -1491,8 +1534,32 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
         if (!in.out) throw Error(kInvalidArgument, "output pointer is null");
         for (uint32_t t : in.tidx)
             if (t >= in.Nt) throw Error(kOutOfRange, "time_index out of range");
-        derive_meta(in, opt, metas[a], true);
     }
+    // per-instance metadata (time maps, FFT length, coefficient table) on several host
+    // threads for large batches; the first failing instance's error is rethrown
+    const std::size_t n = insts.size();
+    const unsigned nthreads =
+        n >= 16 ? std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency())) : 1u;
+    std::vector<std::exception_ptr> errs(n);
+    auto work = [&](std::size_t a0, std::size_t step) {
+        for (std::size_t a = a0; a < n; a += step) {
+            if (insts[a].tidx.empty()) continue;
+            try {
+                derive_meta(insts[a], opt, metas[a], true);
+            } catch (...) {
+                errs[a] = std::current_exception();
+            }
+        }
+    };
+    if (nthreads <= 1) {
+        work(0, 1);
+    } else {
+        std::vector<std::thread> pool;
+        for (unsigned k = 0; k < nthreads; ++k) pool.emplace_back(work, k, nthreads);
+        for (auto& th : pool) th.join();
+    }
+    for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
 }
 }  // namespace
 
