@@ -131,6 +131,15 @@ def _ptr(x):
     return x.ctypes.data_as(ct.c_void_p)
 
 
+def _addr(x) -> int:
+    """Integer address of a numpy array's or torch tensor's data (0 for None)."""
+    if x is None:
+        return 0
+    if _is_torch(x):
+        return x.data_ptr()
+    return x.__array_interface__["data"][0]
+
+
 def _stream_ptr(x):
     if x is not None and _is_torch(x) and x.is_cuda:
         return ct.c_void_p(_torch().cuda.current_stream(x.device).cuda_stream)
@@ -163,9 +172,9 @@ class _View:
         ops = system.A_eig
         self.ops = (np.ascontiguousarray(np.stack([np.asarray(A, np.complex128).T for A in ops]))
                     if len(ops) else np.zeros((0,), np.complex128))
-        self.view = _capi.SystemView(int(system.N), int(system.nf), len(ops), _ptr(self.omegas).value,
-                                     _ptr(self.mirror).value, _ptr(self.p2f).value,
-                                     _ptr(self.ops).value if len(ops) else None, float(system.tol))
+        self.view = _capi.SystemView(int(system.N), int(system.nf), len(ops), _addr(self.omegas),
+                                     _addr(self.mirror), _addr(self.p2f),
+                                     _addr(self.ops) if len(ops) else None, float(system.tol))
 
 
 def _out_array(like_device, shape, dtype, device=None):
@@ -269,12 +278,12 @@ def _instance_array(instances, prec, outs):
         v = _View(system)
         keep += [g, tid, o, v]
         arr[k].sys = v.view
-        arr[k].gamma = _ptr(g).value
+        arr[k].gamma = _addr(g)
         arr[k].Nt = Nt
         arr[k].dt = float(dt)
-        arr[k].tidx = _ptr(tid).value if tid is not None else None
+        arr[k].tidx = _addr(tid) if tid is not None else None
         arr[k].T = 0 if tid is None else tid.size
-        arr[k].L4_out = _ptr(o).value
+        arr[k].L4_out = _addr(o)
         results.append(_l4_view(o, N2))
     return arr, keep, results, bool(dev)
 
