@@ -123,12 +123,17 @@ struct Workspace {
     DeviceBuffer arena;  // metadata of the running group
     DeviceBuffer work;   // transient arrays of the running group
     PinnedBuffer staging;
+    // second lane of pipelined direct builds: its own stream and buffers
+    cudaStream_t stream2 = nullptr;
+    DeviceBuffer arena2, work2;
+    PinnedBuffer staging2;
     std::map<std::pair<int, int>, std::unique_ptr<PlanTables>> plans;  // (L, fp32)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~Workspace() {
         plans.clear();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -722,7 +727,8 @@ using Enqueue = std::function<void(cudaStream_t, ProfRecorder*, cudaEvent_t, cud
 
 template <class R>
 Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cudaStream_t st, Workspace& ws,
-                      DeviceBuffer& meta_mem, DeviceBuffer& work_mem, double2* const* fcr_out, bool fcr_out_dev) {
+                      DeviceBuffer& meta_mem, DeviceBuffer& work_mem, double2* const* fcr_out, bool fcr_out_dev,
+                      PinnedBuffer* staging_buf = nullptr) {
     using C = cplx_t<R>;
     (void)opt;
     const GroupGeom<R> G = group_geom<R>(units);
@@ -946,8 +952,9 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
             plan_copy(M.coef[a], ct.coef.size() * sizeof(C));
         }
     }
-    ws.staging.ensure(soff);
-    char* sb = static_cast<char*>(ws.staging.p);
+    PinnedBuffer& staging = staging_buf ? *staging_buf : ws.staging;
+    staging.ensure(soff);
+    char* sb = static_cast<char*>(staging.p);
     {
         std::size_t k = 0;
         auto put = [&](const void* src, std::size_t bytes) {
@@ -1455,9 +1462,50 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
         stage_sliced_io<double>(insts, metas, budget, io, st);
         groups = plan_units<double>(insts, metas, budget, store);
     }
-    for (auto& gu : groups) {
-        if (opt.fp32) run_group<float>(gu, opt, st, ws, nullptr, false);
-        else run_group<double>(gu, opt, st, ws, nullptr, false);
+    // Large builds of whole instances run as sub-batches of about kPipeSub instances on two
+    // lanes (streams with their own buffers): the host preparation and the input upload of
+    // one sub-batch overlap the kernels and the output download of the other.  Slices
+    // (ordered accumulation), profiling and F/C/R timing keep the single-lane order.
+    constexpr std::size_t kPipeSub = 64;
+    std::size_t nunits = 0;
+    bool whole = true;
+    for (auto& gu : groups)
+        for (auto* u : gu) {
+            ++nunits;
+            whole = whole && !u->accumulate && u->lo == 0 && u->hi == u->in->sys.nf * u->in->sys.nf * u->in->sys.nf;
+        }
+    const bool pipeline = whole && io.back.empty() && !opt.fcr_ms && !g_profile.load() && nunits >= kPipeSub;
+    if (!pipeline) {
+        for (auto& gu : groups) {
+            if (opt.fp32) run_group<float>(gu, opt, st, ws, nullptr, false);
+            else run_group<double>(gu, opt, st, ws, nullptr, false);
+        }
+    } else {
+        if (!ws.stream2) cuda_check(cudaStreamCreateWithFlags(&ws.stream2, cudaStreamNonBlocking), "cudaStreamCreate");
+        // the second lane starts after the work already queued on the caller's stream
+        cuda_check(cudaEventRecord(ws.ev0, st), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(ws.stream2, ws.ev0, 0), "cudaStreamWaitEvent");
+        struct Lane {
+            cudaStream_t s;
+            DeviceBuffer* arena;
+            DeviceBuffer* work;
+            PinnedBuffer* staging;
+        };
+        const Lane lanes[2] = {{st, &ws.arena, &ws.work, &ws.staging}, {ws.stream2, &ws.arena2, &ws.work2, &ws.staging2}};
+        std::size_t k = 0;
+        for (auto& gu : groups) {
+            const std::size_t n = gu.size(), parts = (n + kPipeSub - 1) / kPipeSub;
+            for (std::size_t p = 0; p < parts; ++p) {
+                std::vector<WorkUnit*> sub(gu.begin() + p * n / parts, gu.begin() + (p + 1) * n / parts);
+                const Lane& L = lanes[k++ & 1];
+                // the lane's previous sub-batch has finished with its buffers
+                cuda_check(cudaStreamSynchronize(L.s), "cudaStreamSynchronize(lane)");
+                Enqueue enq = opt.fp32 ? prepare_group<float>(sub, opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging)
+                                       : prepare_group<double>(sub, opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging);
+                enq(L.s, nullptr, nullptr, nullptr);
+            }
+        }
+        cuda_check(cudaStreamSynchronize(ws.stream2), "cudaStreamSynchronize(lane)");
     }
     for (const auto& b : io.back)
         cuda_check(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(sliced out)");

@@ -216,3 +216,18 @@ def test_mixed_radix_fft_lengths_vs_oracle(tmax, nfft):
     Fo, Co, Ro = oracle.fcr_series(Gt, osys.omegas, osys.mirror, 0.005)
     for a, b in ((F, Fo), (C, Co), (R, Ro)):
         assert relerr(a.reshape(osys.nf ** 3, -1), b) <= 1e-10
+
+
+def test_pipelined_direct_build_matches_single_calls():
+    """72 instances with host buffers run as sub-batches on two lanes; each result equals the
+    single-instance call (same kernels; tolerance for summation order)."""
+    rng = np.random.default_rng(5)
+    cases = [spin_boson_case(600, 0.01, eps=rng.uniform(0.5, 2.0), delta=rng.uniform(0.5, 2.0),
+                             alpha=rng.uniform(0.01, 0.1)) for _ in range(72)]
+    tidx = np.arange(0, 300, 3)
+    inst = [(s, G, 0.01, tidx) for (_, s, G) in cases]
+    for precision, tol in (("fp64", 1e-12), ("fp32", 1e-6)):
+        batch = [np.asarray(x) for x in tb.build_instances(inst, precision=precision)]
+        for k in (0, 1, 35, 36, 70, 71):
+            single = np.asarray(tb.build_instances([inst[k]], precision=precision)[0])
+            assert relerr(batch[k], single) <= tol
