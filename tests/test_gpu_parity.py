@@ -231,3 +231,25 @@ def test_pipelined_direct_build_matches_single_calls():
         for k in (0, 1, 35, 36, 70, 71):
             single = np.asarray(tb.build_instances([inst[k]], precision=precision)[0])
             assert relerr(batch[k], single) <= tol
+
+
+def test_coefficient_cache_follows_the_coupling_operators():
+    """Two systems with the same H (same frequencies and pair_to_freq) and different coupling
+    operators, built in turn (and again): each result matches the oracle for its own
+    operators, so the coefficient-table cache never serves another system's table."""
+    osys, s, G = spin_boson_case(800, 0.01)
+    A2 = np.array([[0.3, 0.8 - 0.2j], [0.8 + 0.2j, -0.3]])
+    # same eigenbasis, rotated coupling: A_eig' = U^H A2 U
+    A_eig2 = osys.U.conj().T @ A2 @ osys.U
+    s2 = tb.System.from_arrays(osys.N, osys.omegas, osys.pair_to_freq, [A_eig2], mirror=osys.mirror, eps=osys.eps)
+    tidx = np.arange(0, 400, 5)
+    ref1 = oracle.tcl4_build_batch(osys.N, osys.nf, osys.omegas, osys.mirror, osys.p2f_colmajor(),
+                                   osys.ops_colmajor(), G, 0.01, tidx=tidx)
+    ops2 = np.ascontiguousarray(np.stack([A_eig2.T]))
+    ref2 = oracle.tcl4_build_batch(osys.N, osys.nf, osys.omegas, osys.mirror, osys.p2f_colmajor(),
+                                   ops2, G, 0.01, tidx=tidx)
+    assert relerr(ref1, ref2) > 1e-3  # the operators matter
+    for _ in range(2):
+        out1, out2 = tb.build_instances([(s, G, 0.01, tidx), (s2, G, 0.01, tidx)])
+        assert relerr(out1, ref1) <= 1e-10
+        assert relerr(out2, ref2) <= 1e-10
