@@ -341,6 +341,232 @@ __global__ void __launch_bounds__(32) k_rk4g_adj(const Rk4GJob* __restrict__ job
     }
 }
 
+// ------------------------------------------- RK4 sweeps with a generator ring --
+// D <= 4: each warp streams the generator matrices through a ring of GR_RING slots in
+// shared memory (L(t) and L_add(t), 16 complex each), filled by cp.async GR_RING - 1 steps
+// ahead, so that no step waits on a global load (register prefetch did: the register
+// rotation at the end of a step forced the load to complete).  The arithmetic is that of
+// k_rk4g_fwd / k_rk4g_adj, in the same order.
+constexpr int GR_RING = 8;
+constexpr int GR_SLOT = 32;
+
+__device__ __forceinline__ void gr_cp16(void* dst, const void* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void gr_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void gr_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// copy L(t) (and L_add(t)) into the slot of t: lanes < D*D, 16 bytes each
+__device__ __forceinline__ void gr_fetch(const Rk4GJob& j, uint64_t t, double2* ring, int lane) {
+    const int DD = j.D * j.D;
+    double2* slot = ring + (t % GR_RING) * GR_SLOT;
+    if (lane < DD) {
+        gr_cp16(slot + lane, j.L + t * DD + lane);
+        if (j.L_add) gr_cp16(slot + 16 + lane, j.L_add + t * DD + lane);
+    }
+}
+
+// entry (r, c) of L + L_add at the endpoint held in `slot` (gen_at from shared memory)
+__device__ __forceinline__ double2 gr_at(const Rk4GJob& j, const double2* slot, int r, int c) {
+    const int e = r + c * j.D;
+    double2 v = slot[e];
+    if (j.L_add) v = cadd(v, slot[16 + e]);
+    return v;
+}
+
+__device__ __forceinline__ void gr_row(const Rk4GJob& j, const double2* ring, uint64_t t, int row, double2* out) {
+    const double2* slot = ring + (t % GR_RING) * GR_SLOT;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out[c] = c < j.D ? gr_at(j, slot, row, c) : make_double2(0.0, 0.0);
+}
+__device__ __forceinline__ void gr_col(const Rk4GJob& j, const double2* ring, uint64_t t, int col, double2* out) {
+    const double2* slot = ring + (t % GR_RING) * GR_SLOT;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) out[r] = r < j.D ? gr_at(j, slot, r, col) : make_double2(0.0, 0.0);
+}
+
+// Forward sweep (k_rk4g_fwd for D <= 4): one warp per job, four warps per CTA.
+__global__ void __launch_bounds__(128) k_rk4g_fwd_ring(const Rk4GJob* __restrict__ jobs, int njobs, uint64_t every) {
+    __shared__ __align__(16) double2 ring_all[4][GR_RING * GR_SLOT];
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= njobs) return;
+    double2* ring = ring_all[threadIdx.x >> 5];
+    const Rk4GJob j = jobs[w];
+    const int D = j.D;
+    const int row = lane < D ? lane : 0;
+    const uint64_t steps = j.steps;
+    for (uint64_t t = 0; t + 1 < GR_RING; ++t) {
+        if (t <= steps) gr_fetch(j, t, ring, lane);
+        gr_commit();
+    }
+    double2 r = lane < D ? j.r0[lane] : make_double2(0.0, 0.0);
+    const uint64_t se = j.sample_every;
+    auto sample = [&](uint64_t s) {
+        if (!j.obs_out) return;
+        const double2 v = warp_sum2(lane < D ? cmul(j.obs[lane], r) : make_double2(0.0, 0.0));
+        if (lane == 0) j.obs_out[s] = v;
+    };
+    uint64_t ck_left = 0, s_left = 0;  // steps until the next checkpoint / sample
+    for (uint64_t i = 0; i < steps; ++i) {
+        const uint64_t tn = i + GR_RING - 1;
+        if (tn <= steps) gr_fetch(j, tn, ring, lane);
+        gr_commit();
+        gr_wait<GR_RING - 2>();  // L(t_i) and L(t_{i+1}) have arrived
+        __syncwarp();
+        if (ck_left == 0) {
+            if (j.ckpt && lane < D) j.ckpt[(i / every) * D + lane] = r;
+            ck_left = every;
+        }
+        --ck_left;
+        if (se) {
+            if (s_left == 0) {
+                sample(i / se);
+                s_left = se;
+            }
+            --s_left;
+        }
+        double2 l0[4], l1[4];
+        gr_row(j, ring, i, row, l0);
+        gr_row(j, ring, i + 1, row, l1);
+        r = rk4_step<4>(r, l0, l1, j.dt, D);
+        __syncwarp();  // slot of t_i is refilled next step
+    }
+    gr_wait<0>();
+    if (se) sample(n_samples(steps, se) - 1);
+    if (j.r_out && lane < D) j.r_out[lane] = r;
+}
+
+// Reverse sweep (k_rk4g_adj for D <= 4): one warp per block and job; shared memory holds
+// the ring, then one segment of states.
+__global__ void __launch_bounds__(32) k_rk4g_adj_ring(const Rk4GJob* __restrict__ jobs, uint64_t every) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* ring = reinterpret_cast<double2*>(smem_raw);  // [GR_RING][GR_SLOT]
+    double2* seg = ring + GR_RING * GR_SLOT;                // [every][4]
+    const Rk4GJob j = jobs[blockIdx.x];
+    const int lane = threadIdx.x;
+    const int D = j.D;
+    const int me = lane < D ? lane : 0;
+    const bool own = lane < D;
+    const uint64_t steps = j.steps, se = j.sample_every;
+    const uint64_t nck = (steps + every - 1) / every;
+    const uint64_t nsamp = n_samples(steps, se);
+    const double dt = j.dt;
+    const size_t DD = static_cast<size_t>(D) * D;
+    const double2 ob_l = (j.obs && own) ? j.obs[lane] : make_double2(0.0, 0.0);
+    double2 g = (j.r_final_bar && own) ? j.r_final_bar[lane] : make_double2(0.0, 0.0);
+    double2 ovb = make_double2(0.0, 0.0);
+    double2 pend[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) pend[c] = make_double2(0.0, 0.0);
+    for (uint64_t sg = nck; sg-- > 0;) {
+        const uint64_t s0 = sg * every, s1 = min(s0 + every, steps);
+        // recompute the segment's states from its checkpoint (t = s0 .. s1 through the ring)
+        double2 r = own ? j.ckpt[sg * D + lane] : make_double2(0.0, 0.0);
+        for (uint64_t k = 0; k + 1 < GR_RING; ++k) {
+            if (s0 + k <= s1) gr_fetch(j, s0 + k, ring, lane);
+            gr_commit();
+        }
+        for (uint64_t i = s0; i < s1; ++i) {
+            const uint64_t tn = i + GR_RING - 1;
+            if (tn <= s1) gr_fetch(j, tn, ring, lane);
+            gr_commit();
+            gr_wait<GR_RING - 2>();
+            __syncwarp();
+            if (own) seg[(i - s0) * 4 + lane] = r;
+            double2 l0[4], l1[4];
+            gr_row(j, ring, i, me, l0);
+            gr_row(j, ring, i + 1, me, l1);
+            r = rk4_step<4>(r, l0, l1, dt, D);
+            __syncwarp();
+        }
+        gr_wait<0>();
+        __syncwarp();
+        if (sg == nck - 1 && se && j.obs_bar) {  // the final sample, taken at r_steps
+            const double2 o = j.obs_bar[nsamp - 1];
+            g = cadd(g, cmulc(o, ob_l));   // conj(obs_l) o
+            ovb = cadd(ovb, cmulc(o, r));  // conj(r_l) o
+        }
+        // reverse: step n uses L(t_n) and L(t_{n+1}); the ring runs from t = s1 downwards
+        for (uint64_t k = 0; k + 1 < GR_RING; ++k) {
+            if (s1 >= s0 + k) gr_fetch(j, s1 - k, ring, lane);
+            gr_commit();
+        }
+        for (uint64_t n = s1; n-- > s0;) {
+            const uint64_t q = s1 - 1 - n;  // iteration index
+            if (s1 >= s0 + q + GR_RING - 1) gr_fetch(j, s1 - (q + GR_RING - 1), ring, lane);
+            gr_commit();
+            gr_wait<GR_RING - 2>();  // L(t_{n+1}) and L(t_n) have arrived
+            __syncwarp();
+            double2 r0w[4], r1w[4], c0[4], c1[4];
+            gr_row(j, ring, n, me, r0w);
+            gr_col(j, ring, n, me, c0);
+            gr_row(j, ring, n + 1, me, r1w);
+            gr_col(j, ring, n + 1, me, c1);
+            const double2 rn = own ? seg[(n - s0) * 4 + lane] : make_double2(0.0, 0.0);
+            double2 rh[4], ch[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                rh[c] = make_double2(0.5 * (r0w[c].x + r1w[c].x), 0.5 * (r0w[c].y + r1w[c].y));
+                ch[c] = make_double2(0.5 * (c0[c].x + c1[c].x), 0.5 * (c0[c].y + c1[c].y));
+            }
+            const double2 u1 = rn;
+            const double2 k1 = mv_row<4>(r0w, u1, D);
+            const double2 u2 = cadd(rn, cscale(k1, 0.5 * dt));
+            const double2 k2 = mv_row<4>(rh, u2, D);
+            const double2 u3 = cadd(rn, cscale(k2, 0.5 * dt));
+            const double2 k3 = mv_row<4>(rh, u3, D);
+            const double2 u4 = cadd(rn, cscale(k3, dt));
+            double2 gk1 = cscale(g, dt / 6.0), gk2 = cscale(g, dt / 3.0), gk3 = cscale(g, dt / 3.0);
+            const double2 gk4 = cscale(g, dt / 6.0);
+            double2 gr = g;
+            const double2 gu4 = mhv_col<4>(c1, gk4, D);
+            gr = cadd(gr, gu4);
+            gk3 = cadd(gk3, cscale(gu4, dt));
+            const double2 gu3 = mhv_col<4>(ch, gk3, D);
+            gr = cadd(gr, gu3);
+            gk2 = cadd(gk2, cscale(gu3, 0.5 * dt));
+            const double2 gu2 = mhv_col<4>(ch, gk2, D);
+            gr = cadd(gr, gu2);
+            gk1 = cadd(gk1, cscale(gu2, 0.5 * dt));
+            const double2 gu1 = mhv_col<4>(c0, gk1, D);
+            gr = cadd(gr, gu1);
+            double2* Lb1 = j.L_bar + static_cast<size_t>(n + 1) * DD;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (c < D) {
+                    const double2 x1 = shfl2(u1, c), x2 = shfl2(u2, c), x3 = shfl2(u3, c), x4 = shfl2(u4, c);
+                    const double2 h = cscale(cadd(cmulc(gk2, x2), cmulc(gk3, x3)), 0.5);
+                    const double2 gl0 = cadd(cmulc(gk1, x1), h);
+                    const double2 gl1 = cadd(cmulc(gk4, x4), h);
+                    if (own) Lb1[lane + static_cast<size_t>(c) * D] = cadd(pend[c], gl1);
+                    pend[c] = gl0;
+                }
+            }
+            if (se && j.obs_bar && (n % se) == 0) {
+                const double2 o = j.obs_bar[n / se];
+                gr = cadd(gr, cmulc(o, ob_l));
+                ovb = cadd(ovb, cmulc(o, rn));
+            }
+            g = own ? gr : make_double2(0.0, 0.0);
+            __syncwarp();  // the slot of t_{n+1} is refilled next step
+        }
+        gr_wait<0>();
+        __syncwarp();
+    }
+    if (own) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (c < D) j.L_bar[lane + static_cast<size_t>(c) * D] = pend[c];
+        if (j.r0_bar) j.r0_bar[lane] = g;
+        if (j.obs_vec_bar) j.obs_vec_bar[lane] = ovb;
+    }
+}
+
 // ---------------------------------------------------- L4 -> sources (CSC) --
 // src_bar[s][t] = sum over entries (e, w, cj) of column s: cj ? w conj(Lb[t][e]) : conj(w) Lb[t][e]
 __global__ void k_src_adj(const double2* __restrict__ Lb, uint32_t T, uint32_t E, const int32_t* __restrict__ colptr,
@@ -828,7 +1054,7 @@ void rk4_forward_checkpointed(const std::vector<Rk4GradJob>& jobs, std::size_t e
     for (const auto& j : jobs) dmax = std::max(dmax, j.D);
     const int n = static_cast<int>(jobs.size());
     const unsigned grid = static_cast<unsigned>((n + 3) / 4);
-    if (dmax <= 4) k_rk4g_fwd<4><<<grid, 128, 0, st>>>(dj, n, every);
+    if (dmax <= 4) k_rk4g_fwd_ring<<<grid, 128, 0, st>>>(dj, n, every);
     else k_rk4g_fwd<16><<<grid, 128, 0, st>>>(dj, n, every);
     launched("k_rk4g_fwd");
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(rk4 forward)");
@@ -846,10 +1072,10 @@ void rk4_adjoint(const std::vector<Rk4GradJob>& jobs, std::size_t every, cudaStr
     for (const auto& j : jobs) dmax = std::max(dmax, j.D);
     const unsigned n = static_cast<unsigned>(jobs.size());
     if (dmax <= 4) {
-        const std::size_t smem = every * 4 * sizeof(double2);
-        cuda_check(cudaFuncSetAttribute(k_rk4g_adj<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-                   "cudaFuncSetAttribute(k_rk4g_adj)");
-        k_rk4g_adj<4><<<n, 32, smem, st>>>(dj, every);
+        const std::size_t smem = (GR_RING * GR_SLOT + every * 4) * sizeof(double2);
+        cuda_check(cudaFuncSetAttribute(k_rk4g_adj_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                   "cudaFuncSetAttribute(k_rk4g_adj_ring)");
+        k_rk4g_adj_ring<<<n, 32, smem, st>>>(dj, every);
     } else {
         const std::size_t smem = every * 16 * sizeof(double2);
         cuda_check(cudaFuncSetAttribute(k_rk4g_adj<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
