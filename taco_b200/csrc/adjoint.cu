@@ -181,7 +181,7 @@ __device__ __forceinline__ double2 rk4_step(double2 r, const double2* l0, const 
     return cadd(r, cscale(s, dt / 6.0));
 }
 
-__device__ __forceinline__ uint64_t n_samples(uint64_t steps, uint64_t se) { return se ? (steps + se - 1) / se + 1 : 0; }
+__host__ __device__ __forceinline__ uint64_t n_samples(uint64_t steps, uint64_t se) { return se ? (steps + se - 1) / se + 1 : 0; }
 
 // Forward sweep: one warp per job, lane l < D owns component l of r.
 template <int DMAX>
@@ -341,14 +341,10 @@ __global__ void __launch_bounds__(32) k_rk4g_adj(const Rk4GJob* __restrict__ job
     }
 }
 
-// ------------------------------------------- RK4 sweeps with a generator ring --
-// D <= 4: each warp streams the generator matrices through a ring of GR_RING slots in
-// shared memory (L(t) and L_add(t), 16 complex each), filled by cp.async GR_RING - 1 steps
-// ahead, so that no step waits on a global load (register prefetch did: the register
-// rotation at the end of a step forced the load to complete).  The arithmetic is that of
-// k_rk4g_fwd / k_rk4g_adj, in the same order.
+// ------------------------------------------------ asynchronous copies (cp.async) --
+// Per-warp rings of GR_RING slots in shared memory, filled GR_RING - 1 steps ahead of
+// their use, so that a sequential sweep never waits on a global load.
 constexpr int GR_RING = 8;
-constexpr int GR_SLOT = 32;
 
 __device__ __forceinline__ void gr_cp16(void* dst, const void* src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -360,211 +356,339 @@ __device__ __forceinline__ void gr_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// copy L(t) (and L_add(t)) into the slot of t: lanes < D*D, 16 bytes each
-__device__ __forceinline__ void gr_fetch(const Rk4GJob& j, uint64_t t, double2* ring, int lane) {
+// ------------------------------------------------ RK4 by step matrices (D <= 4) --
+// For the linear system r' = L(t) r, one RK4 step is r_{n+1} = M_n r_n with
+//   K1 = L0, K2 = Lh + dt/2 Lh K1, K3 = Lh + dt/2 Lh K2, K4 = L1 + dt L1 K3,
+//   M_n = I + dt/6 (K1 + 2 K2 + 2 K3 + K4),  L0 = L(t_n), L1 = L(t_{n+1}), Lh = (L0 + L1)/2,
+// which depends on the generator only.  All M_n are built in parallel; the sequential
+// sweeps then apply one D x D matrix per step (instead of four dependent products), with
+// the matrices streamed through the shared-memory ring.  The reverse sweep applies M_n^H;
+// the generator gradients of every step, which need r_n and G(r_{n+1}) only, are formed
+// in parallel afterwards.  Matrices are column-major D x D in records of 16 entries.
+constexpr int SM_REC = 16;
+
+__device__ __forceinline__ void sm_load(const Rk4GJob& j, uint64_t t, double2* A) {
     const int DD = j.D * j.D;
-    double2* slot = ring + (t % GR_RING) * GR_SLOT;
-    if (lane < DD) {
-        gr_cp16(slot + lane, j.L + t * DD + lane);
-        if (j.L_add) gr_cp16(slot + 16 + lane, j.L_add + t * DD + lane);
+    for (int e = 0; e < DD; ++e) {
+        double2 v = j.L[t * DD + e];
+        if (j.L_add) v = cadd(v, j.L_add[t * DD + e]);
+        A[e] = v;
     }
 }
 
-// entry (r, c) of L + L_add at the endpoint held in `slot` (gen_at from shared memory)
-__device__ __forceinline__ double2 gr_at(const Rk4GJob& j, const double2* slot, int r, int c) {
-    const int e = r + c * j.D;
-    double2 v = slot[e];
-    if (j.L_add) v = cadd(v, slot[16 + e]);
-    return v;
+// C = A (I + a B): C = A + a A B (column-major, D x D)
+__device__ __forceinline__ void sm_stage(const double2* A, const double2* B, double a, int D, double2* C) {
+    for (int c = 0; c < D; ++c)
+        for (int r = 0; r < D; ++r) {
+            double2 acc = make_double2(0.0, 0.0);
+            for (int k = 0; k < D; ++k) acc = cfma2(A[r + k * D], B[k + c * D], acc);
+            C[r + c * D] = cadd(A[r + c * D], cscale(acc, a));
+        }
 }
 
-__device__ __forceinline__ void gr_row(const Rk4GJob& j, const double2* ring, uint64_t t, int row, double2* out) {
-    const double2* slot = ring + (t % GR_RING) * GR_SLOT;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) out[c] = c < j.D ? gr_at(j, slot, row, c) : make_double2(0.0, 0.0);
-}
-__device__ __forceinline__ void gr_col(const Rk4GJob& j, const double2* ring, uint64_t t, int col, double2* out) {
-    const double2* slot = ring + (t % GR_RING) * GR_SLOT;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) out[r] = r < j.D ? gr_at(j, slot, r, col) : make_double2(0.0, 0.0);
+__global__ void k_rk4g_stepmat(const Rk4GJob* __restrict__ jobs, uint64_t mstride, double2* __restrict__ M) {
+    const Rk4GJob& j = jobs[blockIdx.y];
+    const uint64_t n = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= j.steps) return;
+    const int D = j.D, DD = D * D;
+    const double dt = j.dt;
+    double2 L0[SM_REC], L1[SM_REC], Lh[SM_REC], Ka[SM_REC], Kb[SM_REC], S[SM_REC];
+    sm_load(j, n, L0);
+    sm_load(j, n + 1, L1);
+    for (int e = 0; e < DD; ++e) {
+        Lh[e] = make_double2(0.5 * (L0[e].x + L1[e].x), 0.5 * (L0[e].y + L1[e].y));
+        S[e] = L0[e];  // K1
+    }
+    sm_stage(Lh, L0, 0.5 * dt, D, Ka);  // K2
+    for (int e = 0; e < DD; ++e) S[e] = cadd(S[e], cscale(Ka[e], 2.0));
+    sm_stage(Lh, Ka, 0.5 * dt, D, Kb);  // K3
+    for (int e = 0; e < DD; ++e) S[e] = cadd(S[e], cscale(Kb[e], 2.0));
+    sm_stage(L1, Kb, dt, D, Ka);  // K4
+    double2* out = M + (static_cast<size_t>(blockIdx.y) * mstride + n) * SM_REC;
+    for (int c = 0; c < D; ++c)
+        for (int r = 0; r < D; ++r) {
+            const int e = r + c * D;
+            double2 v = cscale(cadd(S[e], Ka[e]), dt / 6.0);
+            if (r == c) v.x += 1.0;
+            out[e] = v;
+        }
 }
 
-// Forward sweep (k_rk4g_fwd for D <= 4): one warp per job, four warps per CTA.
-__global__ void __launch_bounds__(128) k_rk4g_fwd_ring(const Rk4GJob* __restrict__ jobs, int njobs, uint64_t every) {
-    __shared__ __align__(16) double2 ring_all[4][GR_RING * GR_SLOT];
+// ring of step matrices: lanes < D*D copy 16 bytes each
+__device__ __forceinline__ void sm_fetch(const double2* Mj, uint64_t n, int DD, double2* ring, int lane) {
+    if (lane < DD) gr_cp16(ring + (n % GR_RING) * SM_REC + lane, Mj + n * SM_REC + lane);
+}
+
+// Forward sweep: one warp per job (four per CTA), r_{n+1} = M_n r_n.  Every state goes
+// to R (the job's [steps + 1][4] array) and the samples are formed afterwards
+// (k_rk4g_samples), so that nothing in the loop waits on memory.
+__global__ void __launch_bounds__(128) k_rk4g_chain(const Rk4GJob* __restrict__ jobs, int njobs, uint64_t every,
+                                                    const double2* __restrict__ M, uint64_t mstride,
+                                                    double2* __restrict__ R) {
+    __shared__ __align__(16) double2 ring_all[4][GR_RING * SM_REC];
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= njobs) return;
     double2* ring = ring_all[threadIdx.x >> 5];
     const Rk4GJob j = jobs[w];
-    const int D = j.D;
+    const int D = j.D, DD = D * D;
     const int row = lane < D ? lane : 0;
     const uint64_t steps = j.steps;
+    const double2* Mj = M + static_cast<size_t>(w) * mstride * SM_REC;
+    double2* Rj = R + static_cast<size_t>(w) * (mstride + 1) * 4;
     for (uint64_t t = 0; t + 1 < GR_RING; ++t) {
-        if (t <= steps) gr_fetch(j, t, ring, lane);
+        if (t < steps) sm_fetch(Mj, t, DD, ring, lane);
         gr_commit();
     }
     double2 r = lane < D ? j.r0[lane] : make_double2(0.0, 0.0);
-    const uint64_t se = j.sample_every;
-    auto sample = [&](uint64_t s) {
-        if (!j.obs_out) return;
-        const double2 v = warp_sum2(lane < D ? cmul(j.obs[lane], r) : make_double2(0.0, 0.0));
-        if (lane == 0) j.obs_out[s] = v;
-    };
-    uint64_t ck_left = 0, s_left = 0;  // steps until the next checkpoint / sample
+    uint64_t ck_left = 0, ck = 0;
     for (uint64_t i = 0; i < steps; ++i) {
         const uint64_t tn = i + GR_RING - 1;
-        if (tn <= steps) gr_fetch(j, tn, ring, lane);
+        if (tn < steps) sm_fetch(Mj, tn, DD, ring, lane);
         gr_commit();
-        gr_wait<GR_RING - 2>();  // L(t_i) and L(t_{i+1}) have arrived
+        gr_wait<GR_RING - 2>();
         __syncwarp();
+        if (lane < D) Rj[i * 4 + lane] = r;
         if (ck_left == 0) {
-            if (j.ckpt && lane < D) j.ckpt[(i / every) * D + lane] = r;
+            if (j.ckpt && lane < D) j.ckpt[ck * D + lane] = r;
+            ++ck;
             ck_left = every;
         }
         --ck_left;
-        if (se) {
-            if (s_left == 0) {
-                sample(i / se);
-                s_left = se;
-            }
-            --s_left;
-        }
-        double2 l0[4], l1[4];
-        gr_row(j, ring, i, row, l0);
-        gr_row(j, ring, i + 1, row, l1);
-        r = rk4_step<4>(r, l0, l1, j.dt, D);
-        __syncwarp();  // slot of t_i is refilled next step
+        const double2* m = ring + (i % GR_RING) * SM_REC;
+        double2 mrow[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) mrow[c] = c < D ? m[row + c * D] : make_double2(0.0, 0.0);
+        r = mv_row<4>(mrow, r, D);
+        __syncwarp();
     }
     gr_wait<0>();
-    if (se) sample(n_samples(steps, se) - 1);
+    if (lane < D) Rj[steps * 4 + lane] = r;
     if (j.r_out && lane < D) j.r_out[lane] = r;
 }
 
-// Reverse sweep (k_rk4g_adj for D <= 4): one warp per block and job; shared memory holds
-// the ring, then one segment of states.
-__global__ void __launch_bounds__(32) k_rk4g_adj_ring(const Rk4GJob* __restrict__ jobs, uint64_t every) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2* ring = reinterpret_cast<double2*>(smem_raw);  // [GR_RING][GR_SLOT]
-    double2* seg = ring + GR_RING * GR_SLOT;                // [every][4]
-    const Rk4GJob j = jobs[blockIdx.x];
-    const int lane = threadIdx.x;
-    const int D = j.D;
-    const int me = lane < D ? lane : 0;
-    const bool own = lane < D;
-    const uint64_t steps = j.steps, se = j.sample_every;
+// obs_out[s] = obs . r(t_s), t_s = min(s * sample_every, steps): one thread per (s, job).
+__global__ void k_rk4g_samples(const Rk4GJob* __restrict__ jobs, uint64_t mstride, const double2* __restrict__ R) {
+    const Rk4GJob& j = jobs[blockIdx.y];
+    const uint64_t se = j.sample_every;
+    if (!se || !j.obs_out) return;
+    const uint64_t s = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n_samples(j.steps, se)) return;
+    const uint64_t t = min(s * se, j.steps);
+    const double2* Rt = R + (static_cast<size_t>(blockIdx.y) * (mstride + 1) + t) * 4;
+    double2 v = make_double2(0.0, 0.0);
+    for (int l = 0; l < j.D; ++l) v = cadd(v, cmul(j.obs[l], Rt[l]));
+    j.obs_out[s] = v;
+}
+
+// States of every checkpoint segment (one warp per (segment, job)): R[n] for n in [s0, s1],
+// R the job's [steps + 1][4] array.
+__global__ void __launch_bounds__(32) k_rk4g_states(const Rk4GJob* __restrict__ jobs, uint64_t every,
+                                                    const double2* __restrict__ M, uint64_t mstride,
+                                                    double2* __restrict__ R) {
+    __shared__ __align__(16) double2 ring[GR_RING * SM_REC];
+    const Rk4GJob j = jobs[blockIdx.y];
+    const uint64_t sg = blockIdx.x;
+    const uint64_t steps = j.steps;
     const uint64_t nck = (steps + every - 1) / every;
+    if (sg >= nck) return;
+    const int lane = threadIdx.x;
+    const int D = j.D, DD = D * D;
+    const int row = lane < D ? lane : 0;
+    const uint64_t s0 = sg * every, s1 = min(s0 + every, steps);
+    const double2* Mj = M + static_cast<size_t>(blockIdx.y) * mstride * SM_REC;
+    double2* Rj = R + static_cast<size_t>(blockIdx.y) * (mstride + 1) * 4;
+    for (uint64_t k = 0; k + 1 < GR_RING; ++k) {
+        if (s0 + k < s1) sm_fetch(Mj, s0 + k, DD, ring, lane);
+        gr_commit();
+    }
+    double2 r = lane < D ? j.ckpt[sg * D + lane] : make_double2(0.0, 0.0);
+    for (uint64_t i = s0; i < s1; ++i) {
+        const uint64_t tn = i + GR_RING - 1;
+        if (tn < s1) sm_fetch(Mj, tn, DD, ring, lane);
+        gr_commit();
+        gr_wait<GR_RING - 2>();
+        __syncwarp();
+        if (lane < D) Rj[i * 4 + lane] = r;
+        const double2* m = ring + (i % GR_RING) * SM_REC;
+        double2 mrow[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) mrow[c] = c < D ? m[row + c * D] : make_double2(0.0, 0.0);
+        r = mv_row<4>(mrow, r, D);
+        __syncwarp();
+    }
+    gr_wait<0>();
+    if (s1 == steps && lane < D) Rj[steps * 4 + lane] = r;
+}
+
+// Reverse sweep (one warp per job, four per CTA): G[steps] = G(r_steps),
+// G[n] = M_n^H G[n+1] + conj(obs) obs_bar[n / se] at sampled n; G(r_0) = G[0].  The sample
+// weights travel with the step matrices through the ring (entry SM_REC of a slot), and
+// G(obs) = sum over samples of conj(r(t_s)) obs_bar[s] is summed after the loop.
+constexpr int SB_SLOT = SM_REC + 2;
+
+__global__ void __launch_bounds__(128) k_rk4g_backchain(const Rk4GJob* __restrict__ jobs, int njobs,
+                                                        const double2* __restrict__ M, uint64_t mstride,
+                                                        const double2* __restrict__ R, double2* __restrict__ G) {
+    __shared__ __align__(16) double2 ring_all[4][GR_RING * SB_SLOT];
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= njobs) return;
+    double2* ring = ring_all[threadIdx.x >> 5];
+    const Rk4GJob j = jobs[w];
+    const int D = j.D, DD = D * D;
+    const bool own = lane < D;
+    const int col = own ? lane : 0;
+    const uint64_t steps = j.steps, se = j.sample_every;
+    const bool samples = se && j.obs_bar;
     const uint64_t nsamp = n_samples(steps, se);
-    const double dt = j.dt;
-    const size_t DD = static_cast<size_t>(D) * D;
+    const double2* Mj = M + static_cast<size_t>(w) * mstride * SM_REC;
+    const double2* Rj = R + static_cast<size_t>(w) * (mstride + 1) * 4;
+    double2* Gj = G + static_cast<size_t>(w) * (mstride + 1) * 4;
     const double2 ob_l = (j.obs && own) ? j.obs[lane] : make_double2(0.0, 0.0);
     double2 g = (j.r_final_bar && own) ? j.r_final_bar[lane] : make_double2(0.0, 0.0);
-    double2 ovb = make_double2(0.0, 0.0);
-    double2 pend[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) pend[c] = make_double2(0.0, 0.0);
-    for (uint64_t sg = nck; sg-- > 0;) {
-        const uint64_t s0 = sg * every, s1 = min(s0 + every, steps);
-        // recompute the segment's states from its checkpoint (t = s0 .. s1 through the ring)
-        double2 r = own ? j.ckpt[sg * D + lane] : make_double2(0.0, 0.0);
-        for (uint64_t k = 0; k + 1 < GR_RING; ++k) {
-            if (s0 + k <= s1) gr_fetch(j, s0 + k, ring, lane);
-            gr_commit();
+    if (samples) g = cadd(g, cmulc(j.obs_bar[nsamp - 1], ob_l));  // the final sample, at r_steps
+    if (own) Gj[steps * 4 + lane] = g;
+    // fetch position f (descending) with f % se and f / se kept incrementally
+    uint64_t f = steps, f_mod = 0, f_div = 0;
+    if (samples && steps > 0) {
+        f_mod = (steps - 1) % se;
+        f_div = (steps - 1) / se;
+    }
+    auto fetch_next = [&]() {  // the slot of step f - 1
+        if (f == 0) return;
+        --f;
+        double2* slot = ring + (f % GR_RING) * SB_SLOT;
+        if (lane < DD) gr_cp16(slot + lane, Mj + f * SM_REC + lane);
+        if (lane == 16) {
+            if (samples && f_mod == 0) gr_cp16(slot + SM_REC, j.obs_bar + f_div);
+            else slot[SM_REC] = make_double2(0.0, 0.0);
         }
-        for (uint64_t i = s0; i < s1; ++i) {
-            const uint64_t tn = i + GR_RING - 1;
-            if (tn <= s1) gr_fetch(j, tn, ring, lane);
-            gr_commit();
-            gr_wait<GR_RING - 2>();
-            __syncwarp();
-            if (own) seg[(i - s0) * 4 + lane] = r;
-            double2 l0[4], l1[4];
-            gr_row(j, ring, i, me, l0);
-            gr_row(j, ring, i + 1, me, l1);
-            r = rk4_step<4>(r, l0, l1, dt, D);
-            __syncwarp();
+        if (samples) {
+            if (f_mod == 0) {
+                f_mod = se - 1;
+                --f_div;
+            } else {
+                --f_mod;
+            }
         }
-        gr_wait<0>();
+    };
+    for (int k = 0; k + 1 < GR_RING; ++k) {
+        fetch_next();
+        gr_commit();
+    }
+    for (uint64_t n = steps; n-- > 0;) {
+        fetch_next();
+        gr_commit();
+        gr_wait<GR_RING - 2>();
         __syncwarp();
-        if (sg == nck - 1 && se && j.obs_bar) {  // the final sample, taken at r_steps
-            const double2 o = j.obs_bar[nsamp - 1];
-            g = cadd(g, cmulc(o, ob_l));   // conj(obs_l) o
-            ovb = cadd(ovb, cmulc(o, r));  // conj(r_l) o
-        }
-        // reverse: step n uses L(t_n) and L(t_{n+1}); the ring runs from t = s1 downwards
-        for (uint64_t k = 0; k + 1 < GR_RING; ++k) {
-            if (s1 >= s0 + k) gr_fetch(j, s1 - k, ring, lane);
-            gr_commit();
-        }
-        for (uint64_t n = s1; n-- > s0;) {
-            const uint64_t q = s1 - 1 - n;  // iteration index
-            if (s1 >= s0 + q + GR_RING - 1) gr_fetch(j, s1 - (q + GR_RING - 1), ring, lane);
-            gr_commit();
-            gr_wait<GR_RING - 2>();  // L(t_{n+1}) and L(t_n) have arrived
-            __syncwarp();
-            double2 r0w[4], r1w[4], c0[4], c1[4];
-            gr_row(j, ring, n, me, r0w);
-            gr_col(j, ring, n, me, c0);
-            gr_row(j, ring, n + 1, me, r1w);
-            gr_col(j, ring, n + 1, me, c1);
-            const double2 rn = own ? seg[(n - s0) * 4 + lane] : make_double2(0.0, 0.0);
-            double2 rh[4], ch[4];
+        const double2* m = ring + (n % GR_RING) * SB_SLOT;
+        double2 mcol[4];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                rh[c] = make_double2(0.5 * (r0w[c].x + r1w[c].x), 0.5 * (r0w[c].y + r1w[c].y));
-                ch[c] = make_double2(0.5 * (c0[c].x + c1[c].x), 0.5 * (c0[c].y + c1[c].y));
-            }
-            const double2 u1 = rn;
-            const double2 k1 = mv_row<4>(r0w, u1, D);
-            const double2 u2 = cadd(rn, cscale(k1, 0.5 * dt));
-            const double2 k2 = mv_row<4>(rh, u2, D);
-            const double2 u3 = cadd(rn, cscale(k2, 0.5 * dt));
-            const double2 k3 = mv_row<4>(rh, u3, D);
-            const double2 u4 = cadd(rn, cscale(k3, dt));
-            double2 gk1 = cscale(g, dt / 6.0), gk2 = cscale(g, dt / 3.0), gk3 = cscale(g, dt / 3.0);
-            const double2 gk4 = cscale(g, dt / 6.0);
-            double2 gr = g;
-            const double2 gu4 = mhv_col<4>(c1, gk4, D);
-            gr = cadd(gr, gu4);
-            gk3 = cadd(gk3, cscale(gu4, dt));
-            const double2 gu3 = mhv_col<4>(ch, gk3, D);
-            gr = cadd(gr, gu3);
-            gk2 = cadd(gk2, cscale(gu3, 0.5 * dt));
-            const double2 gu2 = mhv_col<4>(ch, gk2, D);
-            gr = cadd(gr, gu2);
-            gk1 = cadd(gk1, cscale(gu2, 0.5 * dt));
-            const double2 gu1 = mhv_col<4>(c0, gk1, D);
-            gr = cadd(gr, gu1);
-            double2* Lb1 = j.L_bar + static_cast<size_t>(n + 1) * DD;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                if (c < D) {
-                    const double2 x1 = shfl2(u1, c), x2 = shfl2(u2, c), x3 = shfl2(u3, c), x4 = shfl2(u4, c);
-                    const double2 h = cscale(cadd(cmulc(gk2, x2), cmulc(gk3, x3)), 0.5);
-                    const double2 gl0 = cadd(cmulc(gk1, x1), h);
-                    const double2 gl1 = cadd(cmulc(gk4, x4), h);
-                    if (own) Lb1[lane + static_cast<size_t>(c) * D] = cadd(pend[c], gl1);
-                    pend[c] = gl0;
-                }
-            }
-            if (se && j.obs_bar && (n % se) == 0) {
-                const double2 o = j.obs_bar[n / se];
-                gr = cadd(gr, cmulc(o, ob_l));
-                ovb = cadd(ovb, cmulc(o, rn));
-            }
-            g = own ? gr : make_double2(0.0, 0.0);
-            __syncwarp();  // the slot of t_{n+1} is refilled next step
-        }
-        gr_wait<0>();
+        for (int r = 0; r < 4; ++r) mcol[r] = r < D ? m[r + col * D] : make_double2(0.0, 0.0);
+        double2 gr = mhv_col<4>(mcol, g, D);
+        gr = cadd(gr, cmulc(m[SM_REC], ob_l));  // zero weight at steps without a sample
+        g = own ? gr : make_double2(0.0, 0.0);
+        if (own) Gj[n * 4 + lane] = g;
         __syncwarp();
     }
-    if (own) {
+    gr_wait<0>();
+    if (own && j.r0_bar) j.r0_bar[lane] = g;
+    // G(obs)_l = sum_s conj(r_l(t_s)) obs_bar[s]: lane = (component lane % 4, slice lane / 4)
+    if (j.obs_vec_bar) {
+        const int c = lane & 3, sl = lane >> 2;
+        double2 acc = make_double2(0.0, 0.0);
+        if (samples && c < D)
+            for (uint64_t sidx = sl; sidx < nsamp; sidx += 8) {
+                const uint64_t t = min(sidx * se, steps);
+                acc = cadd(acc, cmulc(j.obs_bar[sidx], Rj[t * 4 + c]));
+            }
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
-            if (c < D) j.L_bar[lane + static_cast<size_t>(c) * D] = pend[c];
-        if (j.r0_bar) j.r0_bar[lane] = g;
-        if (j.obs_vec_bar) j.obs_vec_bar[lane] = ovb;
+        for (int o = 4; o < 32; o <<= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        }
+        if (lane < D) j.obs_vec_bar[lane] = acc;
     }
+}
+
+// Gradient of the RK4 step n with respect to L(t_n) (as L0) and L(t_{n+1}) (as L1),
+// from r_n and g = G(r_{n+1}): the reverse-mode rules of the vector recursion
+//   u1 = r, k_i = A_i u_i (A = L0, Lh, Lh, L1), u_{i+1} = r + c_i k_i, r' = r + dt/6 (k1 + 2k2 + 2k3 + k4).
+__device__ void sm_step_grads(const double2* L0, const double2* L1, int D, double dt, const double2* rn,
+                              const double2* g, double2* gl0, double2* gl1) {
+    double2 Lh[SM_REC];
+    for (int e = 0; e < D * D; ++e) Lh[e] = make_double2(0.5 * (L0[e].x + L1[e].x), 0.5 * (L0[e].y + L1[e].y));
+    auto mv = [&](const double2* A, const double2* x, double2* y) {
+        for (int r = 0; r < D; ++r) {
+            double2 acc = make_double2(0.0, 0.0);
+            for (int c = 0; c < D; ++c) acc = cfma2(A[r + c * D], x[c], acc);
+            y[r] = acc;
+        }
+    };
+    auto mhv = [&](const double2* A, const double2* x, double2* y) {
+        for (int c = 0; c < D; ++c) {
+            double2 acc = make_double2(0.0, 0.0);
+            for (int r = 0; r < D; ++r) acc = cfma2(cconj(A[r + c * D]), x[r], acc);
+            y[c] = acc;
+        }
+    };
+    double2 u1[4], u2[4], u3[4], u4[4], k[4];
+    for (int r = 0; r < D; ++r) u1[r] = rn[r];
+    mv(L0, u1, k);
+    for (int r = 0; r < D; ++r) u2[r] = cadd(rn[r], cscale(k[r], 0.5 * dt));
+    mv(Lh, u2, k);
+    for (int r = 0; r < D; ++r) u3[r] = cadd(rn[r], cscale(k[r], 0.5 * dt));
+    mv(Lh, u3, k);
+    for (int r = 0; r < D; ++r) u4[r] = cadd(rn[r], cscale(k[r], dt));
+    double2 gk1[4], gk2[4], gk3[4], gk4[4], gu[4];
+    for (int r = 0; r < D; ++r) {
+        gk1[r] = cscale(g[r], dt / 6.0);
+        gk2[r] = cscale(g[r], dt / 3.0);
+        gk3[r] = cscale(g[r], dt / 3.0);
+        gk4[r] = cscale(g[r], dt / 6.0);
+    }
+    mhv(L1, gk4, gu);
+    for (int r = 0; r < D; ++r) gk3[r] = cadd(gk3[r], cscale(gu[r], dt));
+    mhv(Lh, gk3, gu);
+    for (int r = 0; r < D; ++r) gk2[r] = cadd(gk2[r], cscale(gu[r], 0.5 * dt));
+    mhv(Lh, gk2, gu);
+    for (int r = 0; r < D; ++r) gk1[r] = cadd(gk1[r], cscale(gu[r], 0.5 * dt));
+    for (int c = 0; c < D; ++c)
+        for (int r = 0; r < D; ++r) {
+            const double2 h = cscale(cadd(cmulc(gk2[r], u2[c]), cmulc(gk3[r], u3[c])), 0.5);
+            gl0[r + c * D] = cadd(cmulc(gk1[r], u1[c]), h);
+            gl1[r + c * D] = cadd(cmulc(gk4[r], u4[c]), h);
+        }
+}
+
+// L_bar[t] = (step t's gradient as L0) + (step t-1's gradient as L1), one thread per (t, job).
+__global__ void k_rk4g_lbar(const Rk4GJob* __restrict__ jobs, uint64_t mstride, const double2* __restrict__ R,
+                            const double2* __restrict__ G) {
+    const Rk4GJob& j = jobs[blockIdx.y];
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t steps = j.steps;
+    if (t > steps) return;
+    const int D = j.D, DD = D * D;
+    const double2* Rj = R + static_cast<size_t>(blockIdx.y) * (mstride + 1) * 4;
+    const double2* Gj = G + static_cast<size_t>(blockIdx.y) * (mstride + 1) * 4;
+    double2 acc[SM_REC];
+    for (int e = 0; e < DD; ++e) acc[e] = make_double2(0.0, 0.0);
+    double2 La[SM_REC], Lb[SM_REC], gl0[SM_REC], gl1[SM_REC];
+    if (t < steps) {  // step t: L(t) is its L0
+        sm_load(j, t, La);
+        sm_load(j, t + 1, Lb);
+        sm_step_grads(La, Lb, D, j.dt, Rj + t * 4, Gj + (t + 1) * 4, gl0, gl1);
+        for (int e = 0; e < DD; ++e) acc[e] = gl0[e];
+    }
+    if (t >= 1) {  // step t-1: L(t) is its L1
+        sm_load(j, t - 1, La);
+        sm_load(j, t, Lb);
+        sm_step_grads(La, Lb, D, j.dt, Rj + (t - 1) * 4, Gj + t * 4, gl0, gl1);
+        for (int e = 0; e < DD; ++e) acc[e] = cadd(acc[e], gl1[e]);
+    }
+    double2* out = j.L_bar + t * DD;
+    for (int e = 0; e < DD; ++e) out[e] = acc[e];
 }
 
 // ---------------------------------------------------- L4 -> sources (CSC) --
@@ -1046,17 +1170,41 @@ void rk4_forward_checkpointed(const std::vector<Rk4GradJob>& jobs, std::size_t e
     if (jobs.empty()) return;
     validate_rk4g(jobs, every, false);
     std::vector<Rk4GJob> gj = to_gjobs(jobs);
+    int dmax = 0;
+    uint64_t mstride = 1;
+    for (const auto& j : jobs) {
+        dmax = std::max(dmax, j.D);
+        mstride = std::max<uint64_t>(mstride, j.steps);
+    }
+    const int n = static_cast<int>(jobs.size());
+    const bool stepmat = dmax <= 4;  // step matrices: [jobs][mstride] records
     Carve probe{nullptr};
     probe.take<Rk4GJob>(gj.size());
+    if (stepmat) {
+        probe.take<double2>(static_cast<std::size_t>(n) * mstride * SM_REC);
+        probe.take<double2>(static_cast<std::size_t>(n) * (mstride + 1) * 4);
+    }
     Carve cv{grad_scratch().ensure(probe.off + 256)};
     Rk4GJob* dj = upload(cv, gj, st, "rk4g jobs");
-    int dmax = 0;
-    for (const auto& j : jobs) dmax = std::max(dmax, j.D);
-    const int n = static_cast<int>(jobs.size());
     const unsigned grid = static_cast<unsigned>((n + 3) / 4);
-    if (dmax <= 4) k_rk4g_fwd_ring<<<grid, 128, 0, st>>>(dj, n, every);
-    else k_rk4g_fwd<16><<<grid, 128, 0, st>>>(dj, n, every);
-    launched("k_rk4g_fwd");
+    if (stepmat) {
+        double2* M = cv.take<double2>(static_cast<std::size_t>(n) * mstride * SM_REC);
+        double2* R = cv.take<double2>(static_cast<std::size_t>(n) * (mstride + 1) * 4);
+        k_rk4g_stepmat<<<dim3(static_cast<unsigned>((mstride + 127) / 128), static_cast<unsigned>(n)), 128, 0, st>>>(
+            dj, mstride, M);
+        launched("k_rk4g_stepmat");
+        k_rk4g_chain<<<grid, 128, 0, st>>>(dj, n, every, M, mstride, R);
+        launched("k_rk4g_chain");
+        uint64_t smax = 1;
+        for (const auto& j : jobs)
+            if (j.sample_every) smax = std::max<uint64_t>(smax, n_samples(j.steps, j.sample_every));
+        k_rk4g_samples<<<dim3(static_cast<unsigned>((smax + 127) / 128), static_cast<unsigned>(n)), 128, 0, st>>>(
+            dj, mstride, R);
+        launched("k_rk4g_samples");
+    } else {
+        k_rk4g_fwd<16><<<grid, 128, 0, st>>>(dj, n, every);
+        launched("k_rk4g_fwd");
+    }
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(rk4 forward)");
 }
 
@@ -1064,25 +1212,45 @@ void rk4_adjoint(const std::vector<Rk4GradJob>& jobs, std::size_t every, cudaStr
     if (jobs.empty()) return;
     validate_rk4g(jobs, every, true);
     std::vector<Rk4GJob> gj = to_gjobs(jobs);
+    int dmax = 0;
+    uint64_t mstride = 1;
+    for (const auto& j : jobs) {
+        dmax = std::max(dmax, j.D);
+        mstride = std::max<uint64_t>(mstride, j.steps);
+    }
+    const unsigned n = static_cast<unsigned>(jobs.size());
+    const bool stepmat = dmax <= 4;  // step matrices, all states R and adjoint states G
+    const std::size_t nM = static_cast<std::size_t>(n) * mstride * SM_REC;
+    const std::size_t nR = static_cast<std::size_t>(n) * (mstride + 1) * 4;
     Carve probe{nullptr};
     probe.take<Rk4GJob>(gj.size());
+    if (stepmat) {
+        probe.take<double2>(nM);
+        probe.take<double2>(nR);
+        probe.take<double2>(nR);
+    }
     Carve cv{grad_scratch().ensure(probe.off + 256)};
     Rk4GJob* dj = upload(cv, gj, st, "rk4g jobs");
-    int dmax = 0;
-    for (const auto& j : jobs) dmax = std::max(dmax, j.D);
-    const unsigned n = static_cast<unsigned>(jobs.size());
-    if (dmax <= 4) {
-        const std::size_t smem = (GR_RING * GR_SLOT + every * 4) * sizeof(double2);
-        cuda_check(cudaFuncSetAttribute(k_rk4g_adj_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-                   "cudaFuncSetAttribute(k_rk4g_adj_ring)");
-        k_rk4g_adj_ring<<<n, 32, smem, st>>>(dj, every);
+    if (stepmat) {
+        double2* M = cv.take<double2>(nM);
+        double2* R = cv.take<double2>(nR);
+        double2* G = cv.take<double2>(nR);
+        const unsigned nck = static_cast<unsigned>((mstride + every - 1) / every);
+        k_rk4g_stepmat<<<dim3(static_cast<unsigned>((mstride + 127) / 128), n), 128, 0, st>>>(dj, mstride, M);
+        launched("k_rk4g_stepmat");
+        k_rk4g_states<<<dim3(nck, n), 32, 0, st>>>(dj, every, M, mstride, R);
+        launched("k_rk4g_states");
+        k_rk4g_backchain<<<(n + 3) / 4, 128, 0, st>>>(dj, static_cast<int>(n), M, mstride, R, G);
+        launched("k_rk4g_backchain");
+        k_rk4g_lbar<<<dim3(static_cast<unsigned>((mstride + 1 + 127) / 128), n), 128, 0, st>>>(dj, mstride, R, G);
+        launched("k_rk4g_lbar");
     } else {
         const std::size_t smem = every * 16 * sizeof(double2);
         cuda_check(cudaFuncSetAttribute(k_rk4g_adj<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                    "cudaFuncSetAttribute(k_rk4g_adj)");
         k_rk4g_adj<16><<<n, 32, smem, st>>>(dj, every);
+        launched("k_rk4g_adj");
     }
-    launched("k_rk4g_adj");
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(rk4 adjoint)");
 }
 
