@@ -346,15 +346,6 @@ __global__ void __launch_bounds__(32) k_rk4g_adj(const Rk4GJob* __restrict__ job
 // their use, so that a sequential sweep never waits on a global load.
 constexpr int GR_RING = 8;
 
-__device__ __forceinline__ void gr_cp16(void* dst, const void* src) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void gr_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void gr_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 // ------------------------------------------------ RK4 by step matrices (D <= 4) --
 // For the linear system r' = L(t) r, one RK4 step is r_{n+1} = M_n r_n with
@@ -416,7 +407,7 @@ __global__ void k_rk4g_stepmat(const Rk4GJob* __restrict__ jobs, uint64_t mstrid
 
 // ring of step matrices: lanes < D*D copy 16 bytes each
 __device__ __forceinline__ void sm_fetch(const double2* Mj, uint64_t n, int DD, double2* ring, int lane) {
-    if (lane < DD) gr_cp16(ring + (n % GR_RING) * SM_REC + lane, Mj + n * SM_REC + lane);
+    if (lane < DD) cp_async16(ring + (n % GR_RING) * SM_REC + lane, Mj + n * SM_REC + lane);
 }
 
 // Forward sweep: one warp per job (four per CTA), r_{n+1} = M_n r_n.  Every state goes
@@ -438,15 +429,15 @@ __global__ void __launch_bounds__(128) k_rk4g_chain(const Rk4GJob* __restrict__ 
     double2* Rj = R + static_cast<size_t>(w) * (mstride + 1) * 4;
     for (uint64_t t = 0; t + 1 < GR_RING; ++t) {
         if (t < steps) sm_fetch(Mj, t, DD, ring, lane);
-        gr_commit();
+        cp_async_commit();
     }
     double2 r = lane < D ? j.r0[lane] : make_double2(0.0, 0.0);
     uint64_t ck_left = 0, ck = 0;
     for (uint64_t i = 0; i < steps; ++i) {
         const uint64_t tn = i + GR_RING - 1;
         if (tn < steps) sm_fetch(Mj, tn, DD, ring, lane);
-        gr_commit();
-        gr_wait<GR_RING - 2>();
+        cp_async_commit();
+        cp_async_wait<GR_RING - 2>();
         __syncwarp();
         if (lane < D) Rj[i * 4 + lane] = r;
         if (ck_left == 0) {
@@ -462,7 +453,7 @@ __global__ void __launch_bounds__(128) k_rk4g_chain(const Rk4GJob* __restrict__ 
         r = mv_row<4>(mrow, r, D);
         __syncwarp();
     }
-    gr_wait<0>();
+    cp_async_wait<0>();
     if (lane < D) Rj[steps * 4 + lane] = r;
     if (j.r_out && lane < D) j.r_out[lane] = r;
 }
@@ -500,14 +491,14 @@ __global__ void __launch_bounds__(32) k_rk4g_states(const Rk4GJob* __restrict__ 
     double2* Rj = R + static_cast<size_t>(blockIdx.y) * (mstride + 1) * 4;
     for (uint64_t k = 0; k + 1 < GR_RING; ++k) {
         if (s0 + k < s1) sm_fetch(Mj, s0 + k, DD, ring, lane);
-        gr_commit();
+        cp_async_commit();
     }
     double2 r = lane < D ? j.ckpt[sg * D + lane] : make_double2(0.0, 0.0);
     for (uint64_t i = s0; i < s1; ++i) {
         const uint64_t tn = i + GR_RING - 1;
         if (tn < s1) sm_fetch(Mj, tn, DD, ring, lane);
-        gr_commit();
-        gr_wait<GR_RING - 2>();
+        cp_async_commit();
+        cp_async_wait<GR_RING - 2>();
         __syncwarp();
         if (lane < D) Rj[i * 4 + lane] = r;
         const double2* m = ring + (i % GR_RING) * SM_REC;
@@ -517,7 +508,7 @@ __global__ void __launch_bounds__(32) k_rk4g_states(const Rk4GJob* __restrict__ 
         r = mv_row<4>(mrow, r, D);
         __syncwarp();
     }
-    gr_wait<0>();
+    cp_async_wait<0>();
     if (s1 == steps && lane < D) Rj[steps * 4 + lane] = r;
 }
 
@@ -559,9 +550,9 @@ __global__ void __launch_bounds__(128) k_rk4g_backchain(const Rk4GJob* __restric
         if (f == 0) return;
         --f;
         double2* slot = ring + (f % GR_RING) * SB_SLOT;
-        if (lane < DD) gr_cp16(slot + lane, Mj + f * SM_REC + lane);
+        if (lane < DD) cp_async16(slot + lane, Mj + f * SM_REC + lane);
         if (lane == 16) {
-            if (samples && f_mod == 0) gr_cp16(slot + SM_REC, j.obs_bar + f_div);
+            if (samples && f_mod == 0) cp_async16(slot + SM_REC, j.obs_bar + f_div);
             else slot[SM_REC] = make_double2(0.0, 0.0);
         }
         if (samples) {
@@ -575,12 +566,12 @@ __global__ void __launch_bounds__(128) k_rk4g_backchain(const Rk4GJob* __restric
     };
     for (int k = 0; k + 1 < GR_RING; ++k) {
         fetch_next();
-        gr_commit();
+        cp_async_commit();
     }
     for (uint64_t n = steps; n-- > 0;) {
         fetch_next();
-        gr_commit();
-        gr_wait<GR_RING - 2>();
+        cp_async_commit();
+        cp_async_wait<GR_RING - 2>();
         __syncwarp();
         const double2* m = ring + (n % GR_RING) * SB_SLOT;
         double2 mcol[4];
@@ -592,7 +583,7 @@ __global__ void __launch_bounds__(128) k_rk4g_backchain(const Rk4GJob* __restric
         if (own) Gj[n * 4 + lane] = g;
         __syncwarp();
     }
-    gr_wait<0>();
+    cp_async_wait<0>();
     if (own && j.r0_bar) j.r0_bar[lane] = g;
     // G(obs)_l = sum_s conj(r_l(t_s)) obs_bar[s]: lane = (component lane % 4, slice lane / 4)
     if (j.obs_vec_bar) {

@@ -78,4 +78,18 @@ inline int ilog2(std::size_t n) {
     return l;
 }
 
+#ifdef __CUDACC__
+// Asynchronous 16-byte global -> shared copies (cp.async), their groups and waits.  Used
+// by per-warp rings of shared-memory slots filled a few steps ahead of their use.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+#endif
+
 }  // namespace taco

@@ -1722,13 +1722,35 @@ void rk4_propagate_device(const std::vector<Rk4Request>& reqs, cudaStream_t stre
             const int warps_per_block = 4;
             const unsigned grid = static_cast<unsigned>((n + warps_per_block - 1) / warps_per_block);
             if (D <= 4) {
-                if (f32) k_rk4_warp<float2, 4><<<grid, 32 * warps_per_block, 0, st>>>(base, n, D);
-                else k_rk4_warp<double2, 4><<<grid, 32 * warps_per_block, 0, st>>>(base, n, D);
+                // step matrices built in parallel, one matrix per sequential step
+                uint64_t mstride = 1, sstride = 1;
+                for (std::size_t k = 0; k < rg.second; ++k) {
+                    const Rk4Job& jk = ordered[rg.first + k];
+                    mstride = std::max<uint64_t>(mstride, jk.steps);
+                    if (jk.sample_every)
+                        sstride = std::max<uint64_t>(sstride, (jk.steps + jk.sample_every - 1) / jk.sample_every + 1);
+                }
+                const std::size_t mbytes = static_cast<std::size_t>(n) * mstride * RK_REC * sizeof(double2);
+                const std::size_t sbytes = static_cast<std::size_t>(n) * sstride * 4 * sizeof(double2);
+                ws.work.ensure(mbytes + sbytes + 512);
+                double2* M = static_cast<double2*>(ws.work.p);
+                double2* Rs = reinterpret_cast<double2*>(static_cast<char*>(ws.work.p) + align_up(mbytes, 256));
+                const dim3 mgrid(static_cast<unsigned>((mstride + 127) / 128), static_cast<unsigned>(n));
+                if (f32) k_rk4_stepmat<float2><<<mgrid, 128, 0, st>>>(base, D, mstride, M);
+                else k_rk4_stepmat<double2><<<mgrid, 128, 0, st>>>(base, D, mstride, M);
+                check_launch("k_rk4_stepmat", &pr);
+                pr.before("rk4_chain");
+                k_rk4_chain<<<grid, 32 * warps_per_block, 0, st>>>(base, n, D, M, mstride, Rs, sstride);
+                check_launch("k_rk4_chain", &pr);
+                pr.before("rk4_samples");
+                k_rk4_samples<<<dim3(static_cast<unsigned>((sstride + 127) / 128), static_cast<unsigned>(n)), 128, 0, st>>>(
+                    base, D, Rs, sstride);
+                check_launch("k_rk4_samples", &pr);
             } else {
                 if (f32) k_rk4_warp<float2, 16><<<grid, 32 * warps_per_block, 0, st>>>(base, n, D);
                 else k_rk4_warp<double2, 16><<<grid, 32 * warps_per_block, 0, st>>>(base, n, D);
+                check_launch("k_rk4_warp", &pr);
             }
-            check_launch("k_rk4_warp", &pr);
         } else {
             const std::size_t smem = 6 * static_cast<std::size_t>(D) * sizeof(double2);
             const int threads = std::min(256, ((D + 31) / 32) * 32);

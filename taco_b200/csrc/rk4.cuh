@@ -117,6 +117,133 @@ __global__ void k_rk4_warp(const Rk4Job* __restrict__ jobs, int njobs, int D) {
     if (lane < D) j.r[lane] = r;
 }
 
+// ------------------------------------------------ step matrices (D <= 4) --
+// For r' = L(t) r one RK4 step is r_{n+1} = M_n r_n, M_n = I + dt/6 (K1 + 2 K2 + 2 K3 + K4)
+// with K1 = L0, K2 = Lh + dt/2 Lh K1, K3 = Lh + dt/2 Lh K2, K4 = L1 + dt L1 K3 (Lh the given
+// midpoint, or (L0 + L1)/2).  k_rk4_stepmat builds every M_n in parallel (FP64 from the
+// storage type); k_rk4_chain applies one matrix per sequential step, the matrices streamed
+// through a per-warp shared-memory ring by cp.async, and stores the sampled states;
+// k_rk4_samples writes the samples and observables.  Records of 16 entries, column-major.
+constexpr int RK_RING = 8;
+constexpr int RK_REC = 16;
+
+template <class S>
+__device__ __forceinline__ void rk_load(const Rk4Job& j, int D, uint64_t t, double2* A) {
+    const S* L = static_cast<const S*>(j.L);
+    const S* La = static_cast<const S*>(j.L_add);
+    const size_t DD = static_cast<size_t>(D) * D;
+    for (size_t e = 0; e < DD; ++e) {
+        double2 v = to_d2(L[t * DD + e]);
+        if (La) v = cadd(v, to_d2(La[t * DD + e]));
+        A[e] = v;
+    }
+}
+
+// C = A + a A B (column-major D x D)
+__device__ __forceinline__ void rk_stage(const double2* A, const double2* B, double a, int D, double2* C) {
+    for (int c = 0; c < D; ++c)
+        for (int r = 0; r < D; ++r) {
+            double2 acc = make_double2(0.0, 0.0);
+            for (int k = 0; k < D; ++k) acc = cadd(acc, cmul(A[r + k * D], B[k + c * D]));
+            C[r + c * D] = cadd(A[r + c * D], cscale(acc, a));
+        }
+}
+
+template <class S>
+__global__ void k_rk4_stepmat(const Rk4Job* __restrict__ jobs, int D, uint64_t mstride, double2* __restrict__ M) {
+    const Rk4Job& j = jobs[blockIdx.y];
+    const uint64_t n = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= j.steps) return;
+    const int DD = D * D;
+    const double dt = j.dt;
+    double2 L0[RK_REC], L1[RK_REC], Lh[RK_REC], Ka[RK_REC], Kb[RK_REC], Sm[RK_REC];
+    rk_load<S>(j, D, n, L0);
+    rk_load<S>(j, D, n + 1, L1);
+    const S* Lhalf = static_cast<const S*>(j.L_half);
+    for (int e = 0; e < DD; ++e) {
+        Lh[e] = Lhalf ? to_d2(Lhalf[n * DD + e]) : make_double2(0.5 * (L0[e].x + L1[e].x), 0.5 * (L0[e].y + L1[e].y));
+        Sm[e] = L0[e];  // K1
+    }
+    rk_stage(Lh, L0, 0.5 * dt, D, Ka);  // K2
+    for (int e = 0; e < DD; ++e) Sm[e] = cadd(Sm[e], cscale(Ka[e], 2.0));
+    rk_stage(Lh, Ka, 0.5 * dt, D, Kb);  // K3
+    for (int e = 0; e < DD; ++e) Sm[e] = cadd(Sm[e], cscale(Kb[e], 2.0));
+    rk_stage(L1, Kb, dt, D, Ka);  // K4
+    double2* out = M + (static_cast<size_t>(blockIdx.y) * mstride + n) * RK_REC;
+    for (int c = 0; c < D; ++c)
+        for (int r = 0; r < D; ++r) {
+            double2 v = cscale(cadd(Sm[r + c * D], Ka[r + c * D]), dt / 6.0);
+            if (r == c) v.x += 1.0;
+            out[r + c * D] = v;
+        }
+}
+
+// One warp per job (four per CTA); sampled states go to Rs (the job's [sstride][4] array).
+__global__ void __launch_bounds__(128) k_rk4_chain(const Rk4Job* __restrict__ jobs, int njobs, int D,
+                                                   const double2* __restrict__ M, uint64_t mstride,
+                                                   double2* __restrict__ Rs, uint64_t sstride) {
+    __shared__ __align__(16) double2 ring_all[4][RK_RING * RK_REC];
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= njobs) return;
+    double2* ring = ring_all[threadIdx.x >> 5];
+    const Rk4Job j = jobs[w];
+    const int DD = D * D;
+    const int row = lane < D ? lane : 0;
+    const uint64_t steps = j.steps, se = j.sample_every;
+    const double2* Mj = M + static_cast<size_t>(w) * mstride * RK_REC;
+    double2* Rj = Rs + static_cast<size_t>(w) * sstride * 4;
+    auto fetch = [&](uint64_t t) {
+        if (t < steps && lane < DD) cp_async16(ring + (t % RK_RING) * RK_REC + lane, Mj + t * RK_REC + lane);
+    };
+    for (uint64_t t = 0; t + 1 < RK_RING; ++t) {
+        fetch(t);
+        cp_async_commit();
+    }
+    double2 r = lane < D ? j.r[lane] : make_double2(0.0, 0.0);
+    uint64_t s_left = 0, ns = 0;
+    for (uint64_t i = 0; i < steps; ++i) {
+        fetch(i + RK_RING - 1);
+        cp_async_commit();
+        cp_async_wait<RK_RING - 2>();
+        __syncwarp();
+        if (se) {
+            if (s_left == 0) {
+                if (lane < D) Rj[ns * 4 + lane] = r;
+                ++ns;
+                s_left = se;
+            }
+            --s_left;
+        }
+        const double2* m = ring + (i % RK_RING) * RK_REC;
+        double2 mrow[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) mrow[c] = c < D ? m[row + c * D] : make_double2(0.0, 0.0);
+        r = warp_matvec<4>(mrow, r, D);
+        __syncwarp();
+    }
+    cp_async_wait<0>();
+    if (se && lane < D) Rj[ns * 4 + lane] = r;
+    if (lane < D) j.r[lane] = r;
+}
+
+// samples[s] and obs_out[s] from the sampled states: one thread per (s, job)
+__global__ void k_rk4_samples(const Rk4Job* __restrict__ jobs, int D, const double2* __restrict__ Rs, uint64_t sstride) {
+    const Rk4Job& j = jobs[blockIdx.y];
+    const uint64_t se = j.sample_every;
+    if (!se) return;
+    const uint64_t s = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= (j.steps + se - 1) / se + 1) return;
+    const double2* r = Rs + (static_cast<size_t>(blockIdx.y) * sstride + s) * 4;
+    if (j.samples)
+        for (int l = 0; l < D; ++l) j.samples[s * D + l] = r[l];
+    if (j.obs_out) {
+        double2 v = make_double2(0.0, 0.0);
+        for (int l = 0; l < D; ++l) v = cadd(v, cmul(j.obs[l], r[l]));
+        j.obs_out[s] = v;
+    }
+}
+
 // One CTA per instance for larger D: state in shared memory, thread t owns rows
 // t, t + blockDim.x, ...; generator entries read from global (L2-resident rows).
 template <class S>
