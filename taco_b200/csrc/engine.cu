@@ -492,13 +492,13 @@ struct InstMeta {
 
 // Coefficient tables by system content (N, nf, pair_to_freq, coupling operators): the
 // table depends on nothing else, so repeated builds of the same systems (parameter sweeps
-// over baths and times, repeated calls) skip the NAKZWAN walk.  Bounded by total bytes;
+// over baths and times, repeated calls) skip the NAKZWAN walk.  Bounded by 2 GB in total;
 // the cache is dropped when a new table would exceed the bound.
 std::shared_ptr<const CoefTable> coef_table_for(const SystemDesc& s) {
     static std::mutex mu;
     static std::unordered_map<std::string, std::shared_ptr<const CoefTable>> cache;
     static std::size_t cached_bytes = 0;
-    constexpr std::size_t kMaxBytes = std::size_t(512) << 20;
+    constexpr std::size_t kMaxBytes = std::size_t(2) << 30;
     std::string key;
     key.reserve(12 + s.p2f.size() * sizeof(int) + s.ops.size() * sizeof(double2));
     const int head[3] = {s.N, s.nf, s.num_ops};
@@ -1585,19 +1585,28 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
     }
     // per-instance metadata (time maps, FFT length, coefficient table) on several host
     // threads for large batches; the first failing instance's error is rethrown
+    // Systems with large coefficient maps (nf >= 21, d >= 5) one at a time, each map built on
+    // several threads; the others spread over the threads, one map per thread.
     const std::size_t n = insts.size();
     const unsigned nthreads =
         n >= 16 ? std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency())) : 1u;
     std::vector<std::exception_ptr> errs(n);
-    auto work = [&](std::size_t a0, std::size_t step) {
-        for (std::size_t a = a0; a < n; a += step) {
-            if (insts[a].tidx.empty()) continue;
-            try {
-                derive_meta(insts[a], opt, metas[a], true);
-            } catch (...) {
-                errs[a] = std::current_exception();
-            }
+    auto large = [&](std::size_t a) { return insts[a].sys.nf >= 21; };
+    auto derive = [&](std::size_t a) {
+        if (insts[a].tidx.empty()) return;
+        try {
+            derive_meta(insts[a], opt, metas[a], true);
+        } catch (...) {
+            errs[a] = std::current_exception();
         }
+    };
+    for (std::size_t a = 0; a < n; ++a)
+        if (large(a)) derive(a);
+    auto work = [&](std::size_t a0, std::size_t step) {
+        set_coef_table_threads(nthreads > 1 ? 1 : 0);
+        for (std::size_t a = a0; a < n; a += step)
+            if (!large(a)) derive(a);
+        set_coef_table_threads(0);
     };
     if (nthreads <= 1) {
         work(0, 1);

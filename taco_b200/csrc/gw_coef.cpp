@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <array>
 #include <complex>
+#include <thread>
 #include <unordered_map>
 
 namespace taco {
@@ -95,40 +96,108 @@ struct TermWalker {
 
 }  // namespace
 
+thread_local int g_coef_threads = 0;
+
+void set_coef_table_threads(int n) { g_coef_threads = n; }
+
+// Entries are independent: each is merged on its own (terms added in walk order, sources in
+// ascending key order), on up to 16 host threads for large maps.  Per thread, a dense
+// accumulator over (source, conjugation) with a list of the keys an entry touched replaces
+// a hash map; the result is the same table.
 void build_coef_table(int N, int nf, const int* p2f, const double2* ops, int num_ops, CoefTable& out, bool structural) {
     const TermWalker tw{N, nf, num_ops, p2f, static_cast<std::size_t>(nf) * nf * nf};
     const cd* op = reinterpret_cast<const cd*>(ops);
     const std::size_t N2 = static_cast<std::size_t>(N) * N;
     const std::size_t E = N2 * N2;
+    const std::size_t S = 3 * tw.nf3;
     auto val = [&](const Factor& x) { return op[static_cast<std::size_t>(x.op) * N2 + x.r + N * x.c]; };
+    std::vector<std::vector<uint32_t>> row_src(E);
+    std::vector<std::vector<cd>> row_coef(E);
+    const bool dense = 2 * S <= (std::size_t(1) << 26);
+    const std::size_t per_thread = dense ? 2 * S * (sizeof(cd) + 1) : 0;
+    unsigned nthreads = g_coef_threads > 0 ? static_cast<unsigned>(g_coef_threads)
+                                           : std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+    if (E < 256) nthreads = 1;
+    if (per_thread) nthreads = std::max<unsigned>(1, std::min<std::size_t>(nthreads, (std::size_t(512) << 20) / per_thread));
+    auto work = [&](std::size_t e0, std::size_t step) {
+        std::vector<cd> dacc(dense ? 2 * S : 0);
+        std::vector<uint8_t> seen(dense ? 2 * S : 0, 0);
+        std::vector<uint32_t> keys;
+        std::unordered_map<uint32_t, cd> macc;  // very large maps
+        for (std::size_t e = e0; e < E; e += step) {
+            keys.clear();
+            macc.clear();
+            tw.walk_entry(e, [&](uint32_t s, bool cj, double sg, const std::array<Factor, 4>& fs) {
+                const cd w = sg * (val(fs[0]) * val(fs[1]) * val(fs[2]) * val(fs[3]));
+                if (w == cd(0.0, 0.0) && !structural) return;
+                const uint32_t key = s | (cj ? 0x80000000u : 0u);
+                const cd add = cj ? std::conj(w) : w;
+                if (dense) {
+                    const std::size_t idx = 2 * static_cast<std::size_t>(s) + (cj ? 1 : 0);
+                    if (!seen[idx]) {
+                        seen[idx] = 1;
+                        dacc[idx] = cd(0.0, 0.0);
+                        keys.push_back(key);
+                    }
+                    dacc[idx] += add;
+                } else {
+                    auto it = macc.find(key);
+                    if (it == macc.end()) {
+                        macc.emplace(key, cd(0.0, 0.0) + add);
+                        keys.push_back(key);
+                    } else {
+                        it->second += add;
+                    }
+                }
+            });
+            std::sort(keys.begin(), keys.end());
+            for (uint32_t key : keys) {
+                const uint32_t s = key & 0x7fffffffu;
+                cd v;
+                if (dense) {
+                    const std::size_t idx = 2 * static_cast<std::size_t>(s) + (key >> 31);
+                    v = dacc[idx];
+                    seen[idx] = 0;
+                } else {
+                    v = macc[key];
+                }
+                if (v == cd(0.0, 0.0) && !structural) continue;
+                row_src[e].push_back(key);
+                row_coef[e].push_back(v);
+            }
+        }
+    };
+    if (nthreads <= 1) {
+        work(0, 1);
+    } else {
+        std::vector<std::thread> pool;
+        for (unsigned k = 0; k < nthreads; ++k) pool.emplace_back(work, k, nthreads);
+        for (auto& th : pool) th.join();
+    }
     out.N = N;
     out.nf = nf;
     out.rowptr.assign(E + 1, 0);
-    out.src.clear();
-    out.coef.clear();
+    std::size_t total = 0;
+    for (std::size_t e = 0; e < E; ++e) {
+        total += row_src[e].size();
+        out.rowptr[e + 1] = static_cast<int32_t>(total);
+    }
+    out.src.resize(total);
+    out.coef.resize(total);
     out.triple_fc_used.assign(tw.nf3, 0);
     out.triple_r_used.assign(tw.nf3, 0);
-    std::unordered_map<uint32_t, cd> acc;  // key: source | conj << 31
-    std::vector<std::pair<uint32_t, cd>> row;
-    for (std::size_t e = 0; e < E; ++e) {
-        acc.clear();
-        tw.walk_entry(e, [&](uint32_t s, bool cj, double sg, const std::array<Factor, 4>& fs) {
-            const cd w = sg * (val(fs[0]) * val(fs[1]) * val(fs[2]) * val(fs[3]));
-            if (w == cd(0.0, 0.0) && !structural) return;
-            acc[s | (cj ? 0x80000000u : 0u)] += cj ? std::conj(w) : w;
-        });
-        row.assign(acc.begin(), acc.end());
-        std::sort(row.begin(), row.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
-        for (const auto& kv : row) {
-            if (kv.second == cd(0.0, 0.0) && !structural) continue;
-            out.src.push_back(kv.first);
-            out.coef.push_back(make_double2(kv.second.real(), kv.second.imag()));
-            const uint32_t s = kv.first & 0x7fffffffu;
+    for (std::size_t e = 0, k = 0; e < E; ++e) {
+        for (std::size_t q = 0; q < row_src[e].size(); ++q, ++k) {
+            const uint32_t key = row_src[e][q];
+            out.src[k] = key;
+            out.coef[k] = make_double2(row_coef[e][q].real(), row_coef[e][q].imag());
+            const uint32_t s = key & 0x7fffffffu;
             const std::size_t kind = s / tw.nf3, t = s % tw.nf3;
             if (kind < 2) out.triple_fc_used[t] = 1;
             else out.triple_r_used[t] = 1;
         }
-        out.rowptr[e + 1] = static_cast<int32_t>(out.src.size());
+        std::vector<uint32_t>().swap(row_src[e]);
+        std::vector<cd>().swap(row_coef[e]);
     }
 }
 

@@ -33,6 +33,9 @@ struct CoefTable {
 // ops: num_ops matrices, column-major N x N (eigenbasis); p2f column-major N x N.
 // structural: keep every (entry, source) pair the sums reach, zero coefficients included
 // (the sparsity pattern of the map for all operator values, as the gradient needs).
+// Host threads of build_coef_table on this thread (0: up to 16, as the map's size allows).
+void set_coef_table_threads(int n);
+
 void build_coef_table(int N, int nf, const int* p2f, const double2* ops, int num_ops, CoefTable& out,
                       bool structural = false);
 
