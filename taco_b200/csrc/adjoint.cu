@@ -684,9 +684,31 @@ __global__ void k_rk4g_lbar(const Rk4GJob* __restrict__ jobs, uint64_t mstride, 
 
 // ---------------------------------------------------- L4 -> sources (CSC) --
 // src_bar[s][t] = sum over entries (e, w, cj) of column s: cj ? w conj(Lb[t][e]) : conj(w) Lb[t][e]
-__global__ void k_src_adj(const double2* __restrict__ Lb, uint32_t T, uint32_t E, const int32_t* __restrict__ colptr,
-                          const uint32_t* __restrict__ rows, const double2* __restrict__ coef,
-                          double2* __restrict__ src_bar) {
+// The arrays of one instance for k_src_adj and k_coef_z (launched over all instances).
+struct SrcAdjJob {
+    const double2* Lb;
+    const int32_t* colptr;
+    const uint32_t* rows;
+    const double2* coef;
+    double2* src_bar;
+    const uint32_t* erow;
+    const uint32_t* keys;
+    uint32_t nnz;  // 0: no coupling-operator aggregation
+    const double2* F;
+    const double2* Cc;
+    const double2* R;
+    double2* Z;
+    uint32_t E;  // entries of L4 (N^4)
+};
+
+__global__ void k_src_adj(const SrcAdjJob* __restrict__ jobs, uint32_t T) {
+    const SrcAdjJob& jb = jobs[blockIdx.z];
+    const uint32_t E = jb.E;
+    const double2* __restrict__ Lb = jb.Lb;
+    const int32_t* __restrict__ colptr = jb.colptr;
+    const uint32_t* __restrict__ rows = jb.rows;
+    const double2* __restrict__ coef = jb.coef;
+    double2* __restrict__ src_bar = jb.src_bar;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t s = blockIdx.y;
     if (t >= T) return;
@@ -701,10 +723,17 @@ __global__ void k_src_adj(const double2* __restrict__ Lb, uint32_t T, uint32_t E
 }
 
 // Z[q] = sum_t conj(Lb[t][e_q]) v~_q(t), one warp per CSR entry.
-__global__ void k_coef_z(const double2* __restrict__ Lb, uint32_t T, uint32_t E, const uint32_t* __restrict__ entry_row,
-                         const uint32_t* __restrict__ keys, uint32_t nnz, const double2* __restrict__ F,
-                         const double2* __restrict__ Cc, const double2* __restrict__ R, uint32_t nf3,
-                         double2* __restrict__ Z) {
+__global__ void k_coef_z(const SrcAdjJob* __restrict__ jobs, uint32_t T, uint32_t nf3) {
+    const SrcAdjJob& jb = jobs[blockIdx.y];
+    const uint32_t E = jb.E;
+    const double2* __restrict__ Lb = jb.Lb;
+    const uint32_t* __restrict__ entry_row = jb.erow;
+    const uint32_t* __restrict__ keys = jb.keys;
+    const uint32_t nnz = jb.nnz;
+    const double2* __restrict__ F = jb.F;
+    const double2* __restrict__ Cc = jb.Cc;
+    const double2* __restrict__ R = jb.R;
+    double2* __restrict__ Z = jb.Z;
     const uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (q >= nnz) return;
@@ -1277,7 +1306,7 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
             std::vector<uint32_t> entry_row;
         };
         std::vector<Host> hs(idx.size());
-        std::size_t bytes = 0;
+        std::size_t bytes = 0, packed_bytes = 0;
         {
             Carve probe{nullptr};
             for (std::size_t a = 0; a < idx.size(); ++a) {
@@ -1307,19 +1336,32 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
                 probe.take<double2>(nnz);
                 probe.take<uint32_t>(nnz);
                 probe.take<uint32_t>(nnz);
-                probe.take<double2>(nnz);             // Z
-                probe.take<double2>(3 * nf3 * T);     // src_bar
-                probe.take<double2>(5 * nf3 * T);     // G1, G2F, G2C, G2R, A2
-                probe.take<double>(nf3 * (1 + ntiles));
                 probe.take<double>(nf);
                 probe.take<int>(nf);
                 probe.take<uint8_t>(nf3);
             }
             probe.take<FcrAdjJob>(idx.size());
             probe.take<double2*>(idx.size());
+            probe.take<SrcAdjJob>(idx.size());
+            packed_bytes = probe.off;  // the uploaded arrays: one host image, one copy
+            for (std::size_t a = 0; a < idx.size(); ++a) {
+                const std::size_t nnz = hs[a].tab.src.size();
+                probe.take<double2>(nnz);             // Z
+                probe.take<double2>(3 * nf3 * T);     // src_bar
+                probe.take<double2>(5 * nf3 * T);     // G1, G2F, G2C, G2R, A2
+                probe.take<double>(nf3 * (1 + ntiles));
+            }
             bytes = probe.off + 256;
         }
         Carve cv{grad_scratch().ensure(bytes)};
+        std::vector<char> image(packed_bytes);
+        // carve an array from the packed region and copy its host contents into the image
+        auto pack = [&](const auto& v) {
+            using T0 = typename std::decay_t<decltype(v)>::value_type;
+            T0* d = cv.take<T0>(v.size());
+            if (!v.empty()) std::memcpy(image.data() + (reinterpret_cast<char*>(d) - cv.base), v.data(), v.size() * sizeof(T0));
+            return d;
+        };
         std::vector<FcrAdjJob> fj(idx.size());
         std::vector<double2*> gbar(idx.size());
         struct Dev {
@@ -1333,26 +1375,43 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
             double* wpart;
         };
         std::vector<Dev> dv(idx.size());
+        std::vector<double*> dom_v(idx.size());
+        std::vector<int*> dmir_v(idx.size());
+        std::vector<uint8_t*> dused_v(idx.size());
         for (std::size_t a = 0; a < idx.size(); ++a) {
-            const auto& j = jobs[idx[a]];
-            const SystemDesc& s = *j.sys;
+            const SystemDesc& s = *jobs[idx[a]].sys;
             Host& h = hs[a];
             Dev& d = dv[a];
-            const std::size_t nnz = h.tab.src.size();
-            d.colptr = upload(cv, h.colptr, st, "adj colptr");
-            d.rows = upload(cv, h.rows, st, "adj rows");
-            d.ccoef = upload(cv, h.ccoef, st, "adj coef");
-            d.erow = upload(cv, h.entry_row, st, "adj entry rows");
-            d.keys = upload(cv, h.tab.src, st, "adj keys");
+            d.colptr = pack(h.colptr);
+            d.rows = pack(h.rows);
+            d.ccoef = pack(h.ccoef);
+            d.erow = pack(h.entry_row);
+            d.keys = pack(h.tab.src);
+            dom_v[a] = pack(s.omegas);
+            dmir_v[a] = pack(s.mirror);
+            std::vector<uint8_t> used(nf3);
+            for (std::size_t q = 0; q < nf3; ++q) used[q] = h.tab.triple_fc_used[q];
+            dused_v[a] = pack(used);
+        }
+        FcrAdjJob* dfj = cv.take<FcrAdjJob>(idx.size());
+        double2** dgbar = cv.take<double2*>(idx.size());
+        SrcAdjJob* dsj = cv.take<SrcAdjJob>(idx.size());
+        std::vector<SrcAdjJob> sj(idx.size());
+        for (std::size_t a = 0; a < idx.size(); ++a) {
+            const auto& j = jobs[idx[a]];
+            Dev& d = dv[a];
+            const std::size_t nnz = hs[a].tab.src.size();
             d.Z = cv.take<double2>(nnz);
             d.src_bar = cv.take<double2>(3 * nf3 * T);
             double2* parts = cv.take<double2>(5 * nf3 * T);
             d.wpart = cv.take<double>(nf3 * (1 + ntiles));
-            double* dom = upload(cv, s.omegas, st, "adj omegas");
-            int* dmir = upload(cv, s.mirror, st, "adj mirror");
-            std::vector<uint8_t> used(nf3);
-            for (std::size_t q = 0; q < nf3; ++q) used[q] = h.tab.triple_fc_used[q];
-            uint8_t* dused = upload(cv, used, st, "adj used");
+            double* dom = dom_v[a];
+            int* dmir = dmir_v[a];
+            uint8_t* dused = dused_v[a];
+            const bool want_ops = j.ops_bar && j.F && j.C && j.R && nnz;
+            sj[a] = SrcAdjJob{j.L_bar, d.colptr, d.rows, d.ccoef, d.src_bar, d.erow, d.keys,
+                              static_cast<uint32_t>(want_ops ? nnz : 0), j.F, j.C, j.R, d.Z,
+                              static_cast<uint32_t>(j.sys->N * j.sys->N * j.sys->N * j.sys->N)};
             FcrAdjJob& f = fj[a];
             f.gamma = j.gamma;
             f.Fb = d.src_bar;
@@ -1370,21 +1429,20 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
             f.ntiles = ntiles;
             gbar[a] = j.gamma_bar;
         }
-        FcrAdjJob* dfj = upload(cv, fj, st, "adj jobs");
-        double2** dgbar = upload(cv, gbar, st, "adj gbar");
-        // 1. sources and the coupling-operator aggregation
-        for (std::size_t a = 0; a < idx.size(); ++a) {
-            const auto& j = jobs[idx[a]];
-            const std::size_t E = static_cast<std::size_t>(j.sys->N) * j.sys->N * j.sys->N * j.sys->N;
-            k_src_adj<<<dim3(static_cast<unsigned>((T + 127) / 128), static_cast<unsigned>(3 * nf3)), 128, 0, st>>>(
-                j.L_bar, static_cast<uint32_t>(T), static_cast<uint32_t>(E), dv[a].colptr, dv[a].rows, dv[a].ccoef,
-                dv[a].src_bar);
+        std::memcpy(image.data() + (reinterpret_cast<char*>(dfj) - cv.base), fj.data(), fj.size() * sizeof(FcrAdjJob));
+        std::memcpy(image.data() + (reinterpret_cast<char*>(dgbar) - cv.base), gbar.data(), gbar.size() * sizeof(double2*));
+        std::memcpy(image.data() + (reinterpret_cast<char*>(dsj) - cv.base), sj.data(), sj.size() * sizeof(SrcAdjJob));
+        cuda_check(cudaMemcpyAsync(cv.base, image.data(), packed_bytes, cudaMemcpyHostToDevice, st), "adj arrays");
+        // 1. sources and the coupling-operator aggregation, all instances in one launch each
+        {
+            std::size_t max_nnz = 0;
+            for (const auto& x : sj) max_nnz = std::max<std::size_t>(max_nnz, x.nnz);
+            k_src_adj<<<dim3(static_cast<unsigned>((T + 127) / 128), static_cast<unsigned>(3 * nf3),
+                             static_cast<unsigned>(idx.size())), 128, 0, st>>>(dsj, static_cast<uint32_t>(T));
             launched("k_src_adj");
-            const std::size_t nnz = hs[a].tab.src.size();
-            if (j.ops_bar && j.F && j.C && j.R && nnz) {
-                k_coef_z<<<static_cast<unsigned>((nnz + 7) / 8), 256, 0, st>>>(
-                    j.L_bar, static_cast<uint32_t>(T), static_cast<uint32_t>(E), dv[a].erow, dv[a].keys,
-                    static_cast<uint32_t>(nnz), j.F, j.C, j.R, static_cast<uint32_t>(nf3), dv[a].Z);
+            if (max_nnz) {
+                k_coef_z<<<dim3(static_cast<unsigned>((max_nnz + 7) / 8), static_cast<unsigned>(idx.size())), 256, 0, st>>>(
+                    dsj, static_cast<uint32_t>(T), static_cast<uint32_t>(nf3));
                 launched("k_coef_z");
             }
         }
