@@ -35,6 +35,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <thread>
 #include <map>
 #include <memory>
 #include <vector>
@@ -1309,11 +1310,14 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
         std::size_t bytes = 0, packed_bytes = 0;
         {
             Carve probe{nullptr};
-            for (std::size_t a = 0; a < idx.size(); ++a) {
+            // structural tables and their transposes, one instance per host thread
+            auto build_host = [&](std::size_t a) {
                 const auto& j = jobs[idx[a]];
                 const SystemDesc& s = *j.sys;
                 Host& h = hs[a];
+                set_coef_table_threads(1);
                 build_coef_table(s.N, s.nf, s.p2f.data(), s.ops.data(), s.num_ops, h.tab, true);
+                set_coef_table_threads(0);
                 const std::size_t E = static_cast<std::size_t>(s.N) * s.N * s.N * s.N;
                 const std::size_t nnz = h.tab.src.size();
                 h.colptr.assign(3 * nf3 + 1, 0);
@@ -1331,6 +1335,24 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
                         h.ccoef[dst] = h.tab.coef[q];
                         h.entry_row[q] = static_cast<uint32_t>(e);
                     }
+            };
+            {
+                const std::size_t n = idx.size();
+                const unsigned nth = n >= 4 ? std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency())) : 1u;
+                if (nth <= 1) {
+                    for (std::size_t a = 0; a < n; ++a) build_host(a);
+                } else {
+                    std::vector<std::thread> pool;
+                    for (unsigned k = 0; k < nth; ++k)
+                        pool.emplace_back([&, k] {
+                            for (std::size_t a = k; a < n; a += nth) build_host(a);
+                        });
+                    for (auto& th : pool) th.join();
+                }
+            }
+            for (std::size_t a = 0; a < idx.size(); ++a) {
+                const Host& h = hs[a];
+                const std::size_t nnz = h.tab.src.size();
                 probe.take<int32_t>(h.colptr.size());
                 probe.take<uint32_t>(nnz);
                 probe.take<double2>(nnz);
@@ -1459,21 +1481,30 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
         k_fcr_adj_reduce<<<dim3(static_cast<unsigned>((T + 127) / 128), static_cast<unsigned>(nf), nj), 128, 0, st>>>(
             dfj, nf, static_cast<uint32_t>(T), dgbar);
         launched("k_fcr_adj_reduce");
-        // 3. host: Bohr-frequency and coupling-operator gradients
-        std::vector<double> wpart(nf3 * (1 + ntiles));
-        std::vector<double2> Z;
+        // 3. host: Bohr-frequency and coupling-operator gradients (all partials copied back,
+        // then one synchronisation)
+        std::vector<std::vector<double>> wparts(idx.size(), std::vector<double>(nf3 * (1 + ntiles)));
+        std::vector<std::vector<double2>> Zs(idx.size());
+        for (std::size_t a = 0; a < idx.size(); ++a) {
+            const auto& j = jobs[idx[a]];
+            cuda_check(cudaMemcpyAsync(wparts[a].data(), dv[a].wpart, wparts[a].size() * sizeof(double),
+                                       cudaMemcpyDeviceToHost, st),
+                       "adj wpart");
+            const std::size_t nnz = hs[a].tab.src.size();
+            if (j.ops_bar && j.F && j.C && j.R && nnz) {
+                Zs[a].resize(nnz);
+                cuda_check(cudaMemcpyAsync(Zs[a].data(), dv[a].Z, nnz * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                           "adj Z");
+            }
+        }
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl4 adjoint)");
         for (std::size_t a = 0; a < idx.size(); ++a) {
             const auto& j = jobs[idx[a]];
             const SystemDesc& s = *j.sys;
-            cuda_check(cudaMemcpyAsync(wpart.data(), dv[a].wpart, wpart.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
-                       "adj wpart");
+            const std::vector<double>& wpart = wparts[a];
+            const std::vector<double2>& Z = Zs[a];
             const std::size_t nnz = hs[a].tab.src.size();
             const bool want_ops = j.ops_bar && j.F && j.C && j.R && nnz;
-            if (want_ops) {
-                Z.resize(nnz);
-                cuda_check(cudaMemcpyAsync(Z.data(), dv[a].Z, nnz * sizeof(double2), cudaMemcpyDeviceToHost, st), "adj Z");
-            }
-            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl4 adjoint)");
             if (j.omega_bar) {
                 for (std::size_t q = 0; q < nf3; ++q) {
                     double wq = 0.0;
