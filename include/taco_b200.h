@@ -104,6 +104,21 @@ int taco_compute_triple_kernels(const taco_system_view* sys, const taco_c128* ga
                                 int method, taco_c128* F, taco_c128* C, taco_c128* R, int flags,
                                 void* stream);
 
+/* Batching form of compute_triple_kernels (no counterpart in the reference, which computes
+ * one system per call): the F, C, R series of n instances in as few launches as the work
+ * budget allows.  Device buffers only (gamma [nf][Nt], F/C/R [nf^3][Nt] complex128);
+ * instances with equal Nt share build groups. */
+typedef struct {
+    taco_system_view sys;
+    const taco_c128* gamma;
+    size_t Nt;
+    double dt;
+    taco_c128* F;
+    taco_c128* C;
+    taco_c128* R;
+} taco_fcr_request;
+int taco_compute_triple_kernels_batch(const taco_fcr_request* reqs, size_t n, int method, void* stream);
+
 /* build_TCL4_generator_cuda_fused_batch(system, gamma_series, dt, time_indices, method, exec,
  * cuda_fcr_ms) (cpp/include/taco/backend/cuda/tcl4_fused_cuda.hpp:25-41).  tidx == NULL or
  * T == 0 means all time indices [0, Nt).  L4_out: [T][N^2 x N^2] column-major, complex128

@@ -39,7 +39,7 @@ __all__ = [
     "System", "bcf_fft", "gamma_trapz", "spin_boson_system", "compute_triple_kernels",
     "build_TCL4_generator", "build_TCL4_generator_batch", "build_correction_series", "build_instances",
     "propagate_rk4_dense", "l4_coefficients", "Tcl4Plan", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
-    "version", "device_count", "kernel_launches", "profile", "tcl2_generator_series", "gamma_trapz_device",
+    "version", "device_count", "kernel_launches", "profile", "compute_triple_kernels_batch", "tcl2_generator_series", "gamma_trapz_device",
     "propagate_tcl", "gamma_trapz_device_batch", "set_work_budget", "fft_length", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
 ]
 
@@ -210,6 +210,35 @@ def compute_triple_kernels(system: System, gamma, dt: float, nmax: int = 2, meth
                                                         _ptr(outs[0]), _ptr(outs[1]), _ptr(outs[2]), flags,
                                                         _stream_ptr(g)))
     return tuple(outs)
+
+
+def compute_triple_kernels_batch(systems, gammas, dts, method: int = 0):
+    """compute_triple_kernels for many instances with CUDA tensors (batching form): one
+    (F, C, R) tuple of [nf, nf, nf, Nt] complex128 tensors per instance."""
+    if isinstance(dts, (int, float)):
+        dts = [float(dts)] * len(systems)
+    if not (len(systems) == len(gammas) == len(dts)):
+        raise ValueError("systems, gammas and dts must have equal lengths")
+    reqs = (_capi.FcrRequest * len(systems))()
+    keep, results = [], []
+    for k, (system, gamma, dt) in enumerate(zip(systems, gammas, dts)):
+        g, dev = _prep_gamma(gamma)
+        if not dev:
+            raise ValueError("compute_triple_kernels_batch needs CUDA tensors for gamma")
+        nf, Nt = g.shape
+        v = _View(system)
+        outs = [_out_array(True, (nf, nf, nf, Nt), np.complex128, g.device) for _ in range(3)]
+        keep += [g, v]
+        reqs[k].sys = v.view
+        reqs[k].gamma = _addr(g)
+        reqs[k].Nt = Nt
+        reqs[k].dt = float(dt)
+        reqs[k].F, reqs[k].C, reqs[k].R = _addr(outs[0]), _addr(outs[1]), _addr(outs[2])
+        results.append(tuple(outs))
+    if results:
+        _capi.check(_capi.lib().taco_compute_triple_kernels_batch(reqs, len(results), int(method),
+                                                                  _stream_ptr(keep[0])))
+    return results
 
 
 def build_TCL4_generator_batch(system: System, gamma, dt: float, time_indices=None, method: int = 0,

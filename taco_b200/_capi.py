@@ -39,7 +39,7 @@ EXPORTED = [
     "taco_build_mikx", "taco_assemble_liouvillian", "taco_gw_to_liouvillian",
     "taco_bcf_fft", "taco_rk4_forward_checkpointed", "taco_rk4_adjoint", "taco_tcl4_adjoint",
     "taco_tcl2_adjoint", "taco_inner_re", "taco_set_work_budget", "taco_gamma_trapz_batch",
-    "taco_fft_length",
+    "taco_fft_length", "taco_compute_triple_kernels_batch",
 ]
 
 
@@ -52,6 +52,11 @@ class SystemView(ct.Structure):
 class Instance(ct.Structure):
     _fields_ = [("sys", SystemView), ("gamma", ct.c_void_p), ("Nt", ct.c_size_t), ("dt", ct.c_double),
                 ("tidx", ct.c_void_p), ("T", ct.c_size_t), ("L4_out", ct.c_void_p)]
+
+
+class FcrRequest(ct.Structure):
+    _fields_ = [("sys", SystemView), ("gamma", ct.c_void_p), ("Nt", ct.c_size_t), ("dt", ct.c_double),
+                ("F", ct.c_void_p), ("C", ct.c_void_p), ("R", ct.c_void_p)]
 
 
 class TacoError(RuntimeError):
@@ -130,6 +135,7 @@ def lib():
         L.taco_compute_triple_kernels.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t, ct.c_double,
                                                   ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int,
                                                   ct.c_void_p]
+        L.taco_compute_triple_kernels_batch.argtypes = [ct.POINTER(FcrRequest), ct.c_size_t, ct.c_int, ct.c_void_p]
         L.taco_tcl4_build_batch.argtypes = [ct.POINTER(SystemView), ct.c_void_p, ct.c_size_t, ct.c_double,
                                             ct.c_void_p, ct.c_size_t, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int,
                                             ct.c_void_p, ct.POINTER(ct.c_double)]

@@ -333,7 +333,7 @@ def spin_boson_forward(params, cfg: SpinBosonConfig, device="cuda", phases=None)
 
 def spin_boson_backward(state, g_obs, cfg: SpinBosonConfig, phases=None):
     """d(loss)/d(eps, Delta, alpha, wc, beta) [B, 5] from g_obs = d(loss)/d<O(t)> [B, n_samples]."""
-    from . import compute_triple_kernels, gamma_trapz_device_batch
+    from . import compute_triple_kernels_batch, gamma_trapz_device_batch
     torch = _torch()
     params, systems = state["params"], state["systems"]
     B = params.shape[0]
@@ -346,7 +346,7 @@ def spin_boson_backward(state, g_obs, cfg: SpinBosonConfig, phases=None):
                                             cfg.sample_every, cfg.every, state["ckpt"], obs_bar)
     gammas = state["gammas"]
     with _phase(phases, "fcr_sources"):
-        sources = [compute_triple_kernels(systems[b], gammas[b], dt) for b in range(B)]
+        sources = compute_triple_kernels_batch(systems, gammas, dt)
     with _phase(phases, "l4_adjoint"):
         gbar, wbar, ops4 = tcl4_adjoint(systems, gammas, dt, L_bar, sources, want_ops=True)
     with _phase(phases, "l2_adjoint"):

@@ -154,6 +154,25 @@ int taco_compute_triple_kernels(const taco_system_view* sys, const taco_c128* ga
     });
 }
 
+int taco_compute_triple_kernels_batch(const taco_fcr_request* reqs, size_t n, int method, void* stream) {
+    return guarded([&] {
+        check_method(method);
+        require_device();
+        if (n && !reqs) throw taco::Error(taco::kInvalidArgument, "null request array");
+        std::vector<taco::FcrRequest> rs(n);
+        for (size_t k = 0; k < n; ++k) {
+            rs[k].sys = to_desc(&reqs[k].sys, false);
+            rs[k].gamma = reinterpret_cast<const double2*>(reqs[k].gamma);
+            rs[k].Nt = reqs[k].Nt;
+            rs[k].dt = reqs[k].dt;
+            rs[k].F = reinterpret_cast<double2*>(reqs[k].F);
+            rs[k].C = reinterpret_cast<double2*>(reqs[k].C);
+            rs[k].R = reinterpret_cast<double2*>(reqs[k].R);
+        }
+        taco::triple_kernels_batch(rs, options(TACO_PREC_FP64, 0, nullptr), static_cast<cudaStream_t>(stream));
+    });
+}
+
 int taco_tcl4_build_batch(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
                           const uint32_t* tidx, size_t T, int method, int precision, void* L4_out, int flags,
                           void* stream, double* fcr_ms) {

@@ -884,9 +884,9 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         s.conv_c = cc;
         s.tmap = M.tmap[a];
         if (fcr_only && fcr_out_dev) {
-            s.vf = fcr_out[0] + static_cast<std::size_t>(tri) * m.U;
-            s.vc = fcr_out[1] + static_cast<std::size_t>(tri) * m.U;
-            s.vr = fcr_out[2] + static_cast<std::size_t>(tri) * m.U;
+            s.vf = fcr_out[3 * a + 0] + static_cast<std::size_t>(tri) * m.U;  // three outputs per unit
+            s.vc = fcr_out[3 * a + 1] + static_cast<std::size_t>(tri) * m.U;
+            s.vr = fcr_out[3 * a + 2] + static_cast<std::size_t>(tri) * m.U;
         } else {
             s.vf = P.v[a] + lt * m.U;
             s.vc = P.v[a] + (nsub + lt) * m.U;
@@ -1510,6 +1510,72 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
     for (const auto& b : io.back)
         cuda_check(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(sliced out)");
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(build)");
+}
+
+// F/C/R series of many instances with device buffers: instances of equal Nt share build
+// groups (within the work budget), each unit writing its own three outputs.
+void triple_kernels_batch(const std::vector<FcrRequest>& reqs, const BuildOptions& opt, cudaStream_t stream) {
+    if (reqs.empty()) return;
+    Workspace& ws = workspace();
+    cudaStream_t st = stream ? stream : ws.stream;
+    std::vector<Tcl4Instance> insts(reqs.size());
+    std::vector<InstMeta> metas(reqs.size());
+    BuildOptions o = opt;
+    o.fp32 = false;
+    o.causal_truncation = false;
+    o.fcr_ms = nullptr;
+    for (std::size_t k = 0; k < reqs.size(); ++k) {
+        const FcrRequest& r = reqs[k];
+        SystemDesc s = r.sys;
+        if (s.num_ops <= 0) {  // F/C/R do not depend on the coupling operators
+            s.num_ops = 1;
+            s.ops.assign(static_cast<std::size_t>(s.N) * s.N, make_double2(0.0, 0.0));
+        }
+        validate_system(s);
+        if (r.Nt == 0) throw Error(kInvalidArgument, "empty gamma_series");
+        if (r.Nt >= (std::size_t(1) << 31)) throw Error(kOverflow, "Nt too large");
+        if (!(r.dt > 0.0)) throw Error(kInvalidArgument, "dt must be > 0");
+        if (!r.gamma || !r.F || !r.C || !r.R) throw Error(kInvalidArgument, "null pointer");
+        Tcl4Instance& in = insts[k];
+        in.sys = s;
+        in.gamma = r.gamma;
+        in.gamma_on_device = true;
+        in.Nt = r.Nt;
+        in.dt = r.dt;
+        in.tidx.resize(r.Nt);
+        for (std::size_t t = 0; t < r.Nt; ++t) in.tidx[t] = static_cast<uint32_t>(t);
+        derive_meta(in, o, metas[k], false);
+    }
+    std::vector<WorkUnit> units(reqs.size());
+    std::map<std::size_t, std::vector<std::size_t>> by_nt;
+    for (std::size_t k = 0; k < reqs.size(); ++k) {
+        units[k].in = &insts[k];
+        units[k].meta = &metas[k];
+        units[k].hi = insts[k].sys.nf * insts[k].sys.nf * insts[k].sys.nf;
+        units[k].coef = metas[k].coef.get();
+        by_nt[reqs[k].Nt].push_back(k);
+    }
+    const std::size_t budget = work_budget();
+    for (auto& kv : by_nt) {
+        std::vector<WorkUnit*> gu;
+        std::vector<double2*> outs;
+        auto flush = [&] {
+            if (gu.empty()) return;
+            run_group<double>(gu, o, st, ws, outs.data(), true);
+            gu.clear();
+            outs.clear();
+        };
+        for (std::size_t k : kv.second) {
+            gu.push_back(&units[k]);
+            if (gu.size() > 1 && measure_work<double>(gu, true, true) > budget) {
+                gu.pop_back();
+                flush();
+                gu.push_back(&units[k]);
+            }
+            outs.insert(outs.end(), {reqs[k].F, reqs[k].C, reqs[k].R});
+        }
+        flush();
+    }
 }
 
 void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_device, std::size_t Nt, double dt,

@@ -97,6 +97,17 @@ void gw_to_l4_device(const double2* GW, int N, std::size_t T, double2* L4, cudaS
 // dst[k] += src[k] (complex64 into complex128), n entries, device pointers.
 void add_c64_into_c128(const float2* src, double2* dst, std::size_t n, cudaStream_t st);
 
+// compute_triple_kernels for many instances (device buffers): full F/C/R series [nf^3][Nt]
+// (FP64) of each.
+struct FcrRequest {
+    SystemDesc sys;
+    const double2* gamma = nullptr;  // device [nf][Nt]
+    std::size_t Nt = 0;
+    double dt = 0.0;
+    double2 *F = nullptr, *C = nullptr, *R = nullptr;  // device [nf^3][Nt]
+};
+void triple_kernels_batch(const std::vector<FcrRequest>& reqs, const BuildOptions& opt, cudaStream_t stream);
+
 // compute_triple_kernels: full F/C/R series [nf^3][Nt] (FP64) for one instance.
 void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_device, std::size_t Nt,
                     double dt, double2* F, double2* Cc, double2* R, bool out_on_device,

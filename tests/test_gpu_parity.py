@@ -253,3 +253,17 @@ def test_coefficient_cache_follows_the_coupling_operators():
         out1, out2 = tb.build_instances([(s, G, 0.01, tidx), (s2, G, 0.01, tidx)])
         assert relerr(out1, ref1) <= 1e-10
         assert relerr(out2, ref2) <= 1e-10
+
+
+def test_triple_kernels_batch_matches_single_calls():
+    """compute_triple_kernels_batch (device buffers, instances of two lengths in separate
+    build groups) against one compute_triple_kernels call per instance."""
+    cases = [spin_boson_case(700, 0.01, eps=e, delta=dl) for e, dl in ((1.0, 1.0), (0.6, 1.4), (1.7, 0.4))]
+    cases.append(random_case(3, 1, 401, 0.01, seed=3))
+    gammas = [torch_dev(G) for (_, _, G) in cases]
+    systems = [s for (_, s, _) in cases]
+    batch = tb.compute_triple_kernels_batch(systems, gammas, 0.01)
+    for s, g, out in zip(systems, gammas, batch):
+        single = tb.compute_triple_kernels(s, g, 0.01)
+        for a, b in zip(out, single):
+            assert relerr(a.cpu().numpy(), b.cpu().numpy()) <= 1e-12
