@@ -1076,9 +1076,26 @@ __global__ void k_fcr_adj_reduce(const FcrAdjJob* __restrict__ jobs, int nf, uin
 
 // ------------------------------------------------------------ TCL2 adjoint --
 // G(Gamma_b(t)) += 2 Re sum_e conj(Lb_e) D_b,e + i Re sum_e conj(Lb_e) U_b,e
-__global__ void k_tcl2_adj_gamma(const double2* __restrict__ Lb, uint32_t T, uint32_t E, int nf,
-                                 const double2* __restrict__ Db, const double2* __restrict__ Ub,
-                                 double2* __restrict__ gbar) {
+// One instance of the TCL2 adjoint kernels (launched over all instances).
+struct Tcl2AdjJob {
+    const double2* Lb;     // [T][E]
+    const double2* Db;     // [nf][E]
+    const double2* Ub;     // [nf][E]
+    const double2* gamma;  // [nf][T]
+    double2* gbar;         // [nf][T], accumulated
+    double2* maps;         // [(1 + 2 nf)][E] or null
+    uint32_t T, E;
+    int nf;
+};
+
+__global__ void k_tcl2_adj_gamma(const Tcl2AdjJob* __restrict__ jobs) {
+    const Tcl2AdjJob& jb = jobs[blockIdx.y];
+    const double2* __restrict__ Lb = jb.Lb;
+    const double2* __restrict__ Db = jb.Db;
+    const double2* __restrict__ Ub = jb.Ub;
+    double2* __restrict__ gbar = jb.gbar;
+    const uint32_t T = jb.T, E = jb.E;
+    const int nf = jb.nf;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     const double2* l = Lb + static_cast<size_t>(t) * E;
@@ -1096,10 +1113,16 @@ __global__ void k_tcl2_adj_gamma(const double2* __restrict__ Lb, uint32_t T, uin
 }
 
 // Per entry e: GL0 = sum_t Lb, GD_b = sum_t 2 Re Gamma_b(t) Lb, GU_b = sum_t Im Gamma_b(t) Lb.
-__global__ void k_tcl2_adj_maps(const double2* __restrict__ Lb, uint32_t T, uint32_t E, int nf,
-                                const double2* __restrict__ gamma, double2* __restrict__ out /* [(1+2nf)][E] */) {
+__global__ void k_tcl2_adj_maps(const Tcl2AdjJob* __restrict__ jobs) {
     __shared__ double2 sm[8][32];
+    const Tcl2AdjJob& jb = jobs[blockIdx.y];
+    const double2* __restrict__ Lb = jb.Lb;
+    const double2* __restrict__ gamma = jb.gamma;
+    double2* __restrict__ out = jb.maps;  // [(1 + 2 nf)][E]
+    const uint32_t T = jb.T, E = jb.E;
+    const int nf = jb.nf;
     const uint32_t e = blockIdx.x;
+    if (!out || e >= E) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int v = 0; v < 1 + 2 * nf; ++v) {
         double2 acc = make_double2(0.0, 0.0);
@@ -1522,42 +1545,121 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
 }
 
 void tcl2_adjoint(const std::vector<Tcl2AdjointJob>& jobs, cudaStream_t st) {
-    for (const auto& j : jobs) {
+    if (jobs.empty()) return;
+    for (const auto& j : jobs)
         if (!j.sys || !j.eps || !j.gamma || !j.L_bar || !j.gamma_bar || j.T == 0)
             throw Error(kInvalidArgument, "tcl2 adjoint: null or empty input");
-        const SystemDesc& s = *j.sys;
-        const int nf = s.nf;
-        const std::size_t E = static_cast<std::size_t>(s.N) * s.N * s.N * s.N;
-        std::vector<double2> L0, Db, Ub;
-        tcl2_maps(s, j.eps, L0, Db, Ub);
-        Carve probe{nullptr};
-        probe.take<double2>(Db.size());
-        probe.take<double2>(Ub.size());
-        probe.take<double2>((1 + 2 * nf) * E);
-        Carve cv{grad_scratch().ensure(probe.off + 256)};
-        double2* dD = upload(cv, Db, st, "tcl2 adj D");
-        double2* dU = upload(cv, Ub, st, "tcl2 adj U");
-        double2* maps = cv.take<double2>((1 + 2 * nf) * E);
-        k_tcl2_adj_gamma<<<static_cast<unsigned>((j.T + 127) / 128), 128, 0, st>>>(
-            j.L_bar, static_cast<uint32_t>(j.T), static_cast<uint32_t>(E), nf, dD, dU, j.gamma_bar);
-        launched("k_tcl2_adj_gamma");
-        if (j.ops_bar || j.eps_bar) {
-            k_tcl2_adj_maps<<<static_cast<unsigned>(E), 256, 0, st>>>(j.L_bar, static_cast<uint32_t>(j.T),
-                                                                       static_cast<uint32_t>(E), nf, j.gamma, maps);
-            launched("k_tcl2_adj_maps");
-            std::vector<double2> h((1 + 2 * nf) * E);
-            cuda_check(cudaMemcpyAsync(h.data(), maps, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, st), "tcl2 adj maps");
-            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl2 adjoint)");
-            std::vector<double2> GL0(h.begin(), h.begin() + E), GD(nf * E), GU(nf * E);
-            for (int b = 0; b < nf; ++b)
-                for (std::size_t e = 0; e < E; ++e) {
-                    GD[b * E + e] = h[(1 + 2 * b) * E + e];
-                    GU[b * E + e] = h[(2 + 2 * b) * E + e];
-                }
-            tcl2_maps_grad(s, j.eps, GL0, GD, GU, j.ops_bar, j.eps_bar);
-        } else {
-            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl2 adjoint)");
+    const std::size_t n = jobs.size();
+    const unsigned nth = n >= 4 ? std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency())) : 1u;
+    auto parallel = [&](auto&& fn) {  // fn(k) for every job, on host threads
+        if (nth <= 1) {
+            for (std::size_t k = 0; k < n; ++k) fn(k);
+            return;
         }
+        std::vector<std::thread> pool;
+        for (unsigned w = 0; w < nth; ++w)
+            pool.emplace_back([&, w] {
+                for (std::size_t k = w; k < n; k += nth) fn(k);
+            });
+        for (auto& th : pool) th.join();
+    };
+    // 1. host maps of every job
+    std::vector<std::vector<double2>> Db(n), Ub(n);
+    parallel([&](std::size_t k) {
+        std::vector<double2> L0;
+        tcl2_maps(*jobs[k].sys, jobs[k].eps, L0, Db[k], Ub[k]);
+    });
+    auto E_of = [&](std::size_t k) {
+        const int N = jobs[k].sys->N;
+        return static_cast<std::size_t>(N) * N * N * N;
+    };
+    auto want_maps = [&](std::size_t k) { return jobs[k].ops_bar || jobs[k].eps_bar; };
+    // 2. device layout: D and U of every job and the job table (one upload), then the maps
+    Carve probe{nullptr};
+    for (std::size_t k = 0; k < n; ++k) {
+        probe.take<double2>(Db[k].size());
+        probe.take<double2>(Ub[k].size());
+    }
+    probe.take<Tcl2AdjJob>(n);
+    const std::size_t packed = probe.off;
+    for (std::size_t k = 0; k < n; ++k)
+        if (want_maps(k)) probe.take<double2>((1 + 2 * jobs[k].sys->nf) * E_of(k));
+    Carve cv{grad_scratch().ensure(probe.off + 256)};
+    std::vector<char> image(packed);
+    auto pack = [&](const std::vector<double2>& v) {
+        double2* d = cv.take<double2>(v.size());
+        if (!v.empty()) std::memcpy(image.data() + (reinterpret_cast<char*>(d) - cv.base), v.data(), v.size() * sizeof(double2));
+        return d;
+    };
+    std::vector<Tcl2AdjJob> tj(n);
+    for (std::size_t k = 0; k < n; ++k) {
+        const auto& j = jobs[k];
+        tj[k].Db = pack(Db[k]);
+        tj[k].Ub = pack(Ub[k]);
+        tj[k].Lb = j.L_bar;
+        tj[k].gamma = j.gamma;
+        tj[k].gbar = j.gamma_bar;
+        tj[k].T = static_cast<uint32_t>(j.T);
+        tj[k].E = static_cast<uint32_t>(E_of(k));
+        tj[k].nf = j.sys->nf;
+    }
+    Tcl2AdjJob* dj = cv.take<Tcl2AdjJob>(n);
+    std::vector<double2*> maps(n, nullptr);
+    for (std::size_t k = 0; k < n; ++k)
+        if (want_maps(k)) maps[k] = tj[k].maps = cv.take<double2>((1 + 2 * jobs[k].sys->nf) * E_of(k));
+    std::memcpy(image.data() + (reinterpret_cast<char*>(dj) - cv.base), tj.data(), n * sizeof(Tcl2AdjJob));
+    cuda_check(cudaMemcpyAsync(cv.base, image.data(), packed, cudaMemcpyHostToDevice, st), "tcl2 adj arrays");
+    // 3. G(Gamma) of every job; the aggregated maps where operator or energy gradients are wanted
+    std::size_t Tmax = 0, Emax = 0;
+    bool any_maps = false;
+    for (std::size_t k = 0; k < n; ++k) {
+        Tmax = std::max(Tmax, jobs[k].T);
+        Emax = std::max(Emax, E_of(k));
+        any_maps = any_maps || want_maps(k);
+    }
+    k_tcl2_adj_gamma<<<dim3(static_cast<unsigned>((Tmax + 127) / 128), static_cast<unsigned>(n)), 128, 0, st>>>(dj);
+    launched("k_tcl2_adj_gamma");
+    std::vector<std::vector<double2>> h(n);
+    if (any_maps) {
+        k_tcl2_adj_maps<<<dim3(static_cast<unsigned>(Emax), static_cast<unsigned>(n)), 256, 0, st>>>(dj);
+        launched("k_tcl2_adj_maps");
+        for (std::size_t k = 0; k < n; ++k)
+            if (maps[k]) {
+                h[k].resize((1 + 2 * jobs[k].sys->nf) * E_of(k));
+                cuda_check(cudaMemcpyAsync(h[k].data(), maps[k], h[k].size() * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                           "tcl2 adj maps");
+            }
+    }
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(tcl2 adjoint)");
+    // 4. host: reverse the construction of the maps (on threads unless jobs share a
+    // gradient buffer, whose accumulation must then stay sequential)
+    bool shared_out = false;
+    {
+        std::vector<const void*> outs;
+        for (const auto& j : jobs) {
+            if (j.ops_bar) outs.push_back(j.ops_bar);
+            if (j.eps_bar) outs.push_back(j.eps_bar);
+        }
+        std::sort(outs.begin(), outs.end());
+        shared_out = std::adjacent_find(outs.begin(), outs.end()) != outs.end();
+    }
+    auto host_grad = [&](std::size_t k) {
+        if (!maps[k]) return;
+        const auto& j = jobs[k];
+        const int nf = j.sys->nf;
+        const std::size_t E = E_of(k);
+        std::vector<double2> GL0(h[k].begin(), h[k].begin() + static_cast<std::ptrdiff_t>(E)), GD(nf * E), GU(nf * E);
+        for (int b = 0; b < nf; ++b)
+            for (std::size_t e = 0; e < E; ++e) {
+                GD[b * E + e] = h[k][(1 + 2 * b) * E + e];
+                GU[b * E + e] = h[k][(2 + 2 * b) * E + e];
+            }
+        tcl2_maps_grad(*j.sys, j.eps, GL0, GD, GU, j.ops_bar, j.eps_bar);
+    };
+    if (shared_out) {
+        for (std::size_t k = 0; k < n; ++k) host_grad(k);
+    } else {
+        parallel(host_grad);
     }
 }
 
