@@ -241,6 +241,81 @@ __global__ void __launch_bounds__(CONTRACT_ROW_THREADS) k_contract_rows_staged(c
     }
 }
 
+// d = 2 (E = 16): k_contract_rows_staged with the 16 results of a time in registers and
+// written as one 128-byte (FP32) or 256-byte (FP64) row by vector stores, so that shared
+// memory holds only the table and more CTAs stay resident.  Unique entries (partner(e) >= e)
+// are summed, the other six are conjugates.
+__host__ __device__ constexpr int d2_partner_e(int e) {
+    return (e % 4 / 2 + 2 * (e % 4 % 2)) + 4 * (e / 4 / 2 + 2 * (e / 4 % 2));
+}
+
+template <class R>
+inline std::size_t rows_d2_smem(std::size_t nnz) {
+    return nnz * (sizeof(Coef4<R>) + 4) + 17 * 4 + 64;
+}
+
+template <class R>
+__global__ void __launch_bounds__(CONTRACT_ROW_THREADS) k_contract_rows_d2(const ContractJob* __restrict__ jobs,
+                                                                           int nnz_cap) {
+    using C = cplx_t<R>;
+    constexpr int E = 16;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const ContractJob job = jobs[blockIdx.y];
+    const uint32_t o0 = blockIdx.x * CONTRACT_ROW_THREADS;
+    if (o0 >= job.T) return;
+    Coef4<R>* cf = reinterpret_cast<Coef4<R>*>(smem_raw);          // [nnz_cap]
+    uint32_t* off = reinterpret_cast<uint32_t*>(cf + nnz_cap);     // [nnz_cap]
+    int32_t* rp = reinterpret_cast<int32_t*>(off + nnz_cap);       // [E + 1]
+    const int32_t nnz = __ldg(&job.rowptr[E]);
+    const C* coef = static_cast<const C*>(job.coef);
+    for (int32_t k = threadIdx.x; k < nnz; k += blockDim.x) {
+        const uint32_t sk = __ldg(&job.src[k]);
+        const C w = coef[k];
+        const bool cj = (sk & 0x80000000u) != 0;
+        cf[k] = Coef4<R>{w.x, cj ? w.y : -w.y, cj ? -w.x : w.x, w.y};
+        off[k] = (sk & 0x7fffffffu) * job.U;
+    }
+    for (uint32_t e = threadIdx.x; e <= E; e += blockDim.x) rp[e] = __ldg(&job.rowptr[e]);
+    __syncthreads();
+    const uint32_t o = o0 + threadIdx.x;
+    if (o >= job.T) return;
+    const C* v = static_cast<const C*>(job.v) + __ldg(&job.out_u[o]);
+    C res[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        if (d2_partner_e(e) < e) continue;
+        EntryAcc<C> acc;
+        int32_t k = rp[e];
+        const int32_t end = rp[e + 1];
+        for (; k + 4 <= end; k += 4) {
+            const C x0 = v[off[k]], x1 = v[off[k + 1]], x2 = v[off[k + 2]], x3 = v[off[k + 3]];
+            C p{0, 0};
+            term_mac(p, cf[k], x0);
+            term_mac(p, cf[k + 1], x1);
+            term_mac(p, cf[k + 2], x2);
+            term_mac(p, cf[k + 3], x3);
+            acc.add(p);
+        }
+        for (; k < end; ++k) {
+            C p{0, 0};
+            term_mac(p, cf[k], v[off[k]]);
+            acc.add(p);
+        }
+        res[e] = acc.get();
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+        if (d2_partner_e(e) < e) res[e] = cconj(res[d2_partner_e(e)]);
+    C* out = static_cast<C*>(job.out) + static_cast<size_t>(o) * E;
+    if (job.accumulate) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) out[e] = cadd(out[e], res[e]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) out[e] = res[e];
+    }
+}
+
 template <class R>
 __global__ void __launch_bounds__(CONTRACT_ROW_THREADS) k_contract_rows(const ContractJob* __restrict__ jobs, int N) {
     using C = cplx_t<R>;

@@ -1050,9 +1050,12 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         return true;
     }();
     const bool rows_staged = use_rows && offsets_32 && staged_smem <= 100 * 1024;
+    const bool rows_d2 = rows_staged && maxN == 2;  // results in registers
     const bool contract_smem = !use_rows && maxE < 256 && smem_need(OTs) <= smem_budget;
     const int OT = use_rows ? CONTRACT_ROW_THREADS : OTs;
     const std::size_t csmem = rows_staged ? staged_smem : use_rows ? rows_smem : contract_smem ? smem_need(OT) : 0;
+    const std::size_t d2smem = rows_d2_smem<R>(maxNnz);
+    if (rows_d2) set_smem(k_contract_rows_d2<R>, d2smem);
     if (rows_staged) set_smem(k_contract_rows_staged<R>, csmem);
     else if (use_rows) set_smem(k_contract_rows<R>, csmem);
     else if (contract_smem) set_smem(k_contract_smem<R>, csmem);
@@ -1155,7 +1158,11 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     if (ev1) cuda_check(cudaEventRecord(ev1, st), "cudaEventRecord");
     if (!fcr_only) {
         pr.before(f32 ? "contract_f32" : "contract_f64");
-        if (rows_staged) {
+        if (rows_d2) {
+            const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
+            k_contract_rows_d2<R><<<dim3(gx, static_cast<unsigned>(ni)), CONTRACT_ROW_THREADS, d2smem, st>>>(Mc.conj,
+                                                                                                       nnz_cap);
+        } else if (rows_staged) {
             const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
             k_contract_rows_staged<R><<<dim3(gx, static_cast<unsigned>(ni)), CONTRACT_ROW_THREADS, csmem, st>>>(
                 Mc.conj, maxN, nnz_cap);
