@@ -185,6 +185,32 @@ def _out_array(like_device, shape, dtype, device=None):
     return np.empty(shape, dtype=dtype)
 
 
+def _content_key(x):
+    a = x if isinstance(x, np.ndarray) else np.asarray(x)
+    return a.dtype.str, a.shape, a.tobytes()
+
+
+def _system_view(system: System) -> _View:
+    """The _View of `system`, reused while its arrays hold the same contents.
+
+    Batched calls marshal hundreds of systems per call; the key (the bytes of the small
+    arrays a view copies) costs a fraction of building the view again.
+    """
+    ops = system.A_eig
+    key = (int(system.N), int(system.nf), float(system.tol), _content_key(system.omegas),
+           _content_key(system.mirror), _content_key(system.pair_to_freq),
+           tuple(_content_key(A) for A in ops))
+    cached = getattr(system, "_taco_view", None)
+    if cached is not None and cached[0] == key:
+        return cached[1]
+    v = _View(system)
+    try:
+        system._taco_view = (key, v)
+    except AttributeError:  # objects without a __dict__ are marshalled every call
+        pass
+    return v
+
+
 def _l4_view(buf, N2):
     """[T, N^2*N^2] column-major matrices -> [T, N^2, N^2] indexed [t, row, col]."""
     T = buf.shape[0]
@@ -293,6 +319,7 @@ def _instance_array(instances, prec, outs):
     keep = []
     results = []
     dev = None
+    tid_of = {}  # one conversion per distinct time-index object (batches often share one)
     for k, (system, gamma, dt, tidx) in enumerate(instances):
         g, d = _prep_gamma(gamma)
         if dev is None:
@@ -300,19 +327,27 @@ def _instance_array(instances, prec, outs):
         elif dev != d:
             raise ValueError("mix of host and device gamma")
         nf, Nt = g.shape
-        tid = None if tidx is None or len(tidx) == 0 else np.ascontiguousarray(tidx, np.uint32)
+        if tidx is None or len(tidx) == 0:
+            tid, tid_addr = None, None
+        else:
+            hit = tid_of.get(id(tidx))
+            if hit is None or hit[0] is not tidx:
+                t = np.ascontiguousarray(tidx, np.uint32)
+                hit = tid_of[id(tidx)] = (tidx, t, _addr(t))
+            tid, tid_addr = hit[1], hit[2]
         T = Nt if tid is None else tid.size
         N2 = int(system.N) ** 2
         o = outs[k] if outs is not None else _out_array(d, (T, N2 * N2), dtype, g.device if d else None)
-        v = _View(system)
+        v = _system_view(system)
         keep += [g, tid, o, v]
-        arr[k].sys = v.view
-        arr[k].gamma = _addr(g)
-        arr[k].Nt = Nt
-        arr[k].dt = float(dt)
-        arr[k].tidx = _addr(tid) if tid is not None else None
-        arr[k].T = 0 if tid is None else tid.size
-        arr[k].L4_out = _addr(o)
+        a = arr[k]
+        a.sys = v.view
+        a.gamma = _addr(g)
+        a.Nt = Nt
+        a.dt = float(dt)
+        a.tidx = tid_addr
+        a.T = 0 if tid is None else tid.size
+        a.L4_out = _addr(o)
         results.append(_l4_view(o, N2))
     return arr, keep, results, bool(dev)
 

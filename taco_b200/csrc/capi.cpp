@@ -1,10 +1,12 @@
 // capi.cpp -- extern "C" entry points of libtaco_b200.so (see include/taco_b200.h).
 #include "taco_b200.h"
 
+#include <chrono>
 #include <cuda_runtime.h>
 
 #include <atomic>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -87,17 +89,15 @@ taco::BuildOptions options(int precision, int flags, double* fcr_ms) {
 }
 
 void fill_tidx(taco::Tcl4Instance& in, const uint32_t* tidx, std::size_t T) {
-    if (tidx == nullptr || T == 0) {
-        in.tidx.resize(in.Nt);
-        for (std::size_t t = 0; t < in.Nt; ++t) in.tidx[t] = static_cast<uint32_t>(t);
-    } else {
-        in.tidx.assign(tidx, tidx + T);
-    }
+    if (tidx == nullptr || T == 0) in.tidx.iota(in.Nt);
+    else in.tidx.assign(tidx, tidx + T);
 }
 
 std::vector<taco::Tcl4Instance> to_instances(const taco_tcl4_instance* inst, size_t count, int flags) {
     if (count > 0 && !inst) throw taco::Error(taco::kInvalidArgument, "instances is null");
     std::vector<taco::Tcl4Instance> insts(count);
+    // instances naming the same caller array (pointer and length) share one copy of it
+    std::map<std::pair<const uint32_t*, std::size_t>, std::size_t> first_of;
     for (std::size_t k = 0; k < count; ++k) {
         taco::Tcl4Instance& in = insts[k];
         in.sys = to_desc(&inst[k].sys);
@@ -106,7 +106,16 @@ std::vector<taco::Tcl4Instance> to_instances(const taco_tcl4_instance* inst, siz
         in.Nt = inst[k].Nt;
         in.dt = inst[k].dt;
         if (in.Nt == 0) throw taco::Error(taco::kInvalidArgument, "empty gamma_series");
-        fill_tidx(in, inst[k].tidx, inst[k].T);
+        const bool listed = inst[k].tidx != nullptr && inst[k].T > 0;
+        const std::pair<const uint32_t*, std::size_t> key{listed ? inst[k].tidx : nullptr,
+                                                          listed ? inst[k].T : inst[k].Nt};
+        auto it = first_of.find(key);
+        if (it != first_of.end()) {
+            in.tidx.share_with(insts[it->second].tidx);
+        } else {
+            fill_tidx(in, inst[k].tidx, inst[k].T);
+            first_of.emplace(key, k);
+        }
         in.out = inst[k].L4_out;
         in.out_on_device = (flags & TACO_OUT_DEVICE) != 0;
     }
@@ -215,7 +224,9 @@ int taco_tcl4_build_instances(const taco_tcl4_instance* inst, size_t count, int 
     return guarded([&] {
         check_method(method);
         require_device();
+        const auto t0 = std::chrono::steady_clock::now();
         std::vector<taco::Tcl4Instance> insts = to_instances(inst, count, flags);
+        taco::host_trace_add("abi", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
         taco::tcl4_build(insts, options(precision, flags, nullptr), static_cast<cudaStream_t>(stream));
     });
 }

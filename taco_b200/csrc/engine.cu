@@ -11,6 +11,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <functional>
 #include <cmath>
 #include <mutex>
@@ -47,6 +50,32 @@ Tuning tuning_for(int L, bool fp32) {
 }
 
 std::size_t align_up(std::size_t x, std::size_t a) { return (x + a - 1) / a * a; }
+
+// Host phase accumulator of the calling thread (see host_trace_on).
+struct HostPhases {
+    std::vector<std::pair<const char*, double>> ms;
+    void add(const char* phase, double v) {
+        for (auto& e : ms)
+            if (std::strcmp(e.first, phase) == 0) {
+                e.second += v;
+                return;
+            }
+        ms.emplace_back(phase, v);
+    }
+};
+thread_local HostPhases t_phases;
+
+// Milliseconds since the previous lap, added to `phase` when tracing is on.
+struct Lap {
+    bool on = host_trace_on();
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void operator()(const char* phase) {
+        if (!on) return;
+        const auto now = std::chrono::steady_clock::now();
+        t_phases.add(phase, std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
 
 struct DeviceBuffer {
     void* p = nullptr;
@@ -482,11 +511,48 @@ void check_launch(const char* what, ProfRecorder* pr = nullptr) {
 }
 
 // --------------------------------------------------------------- metadata --
+// Maps of one list of requested times (shared by the instances of a call that name the
+// same list): the unique times in increasing order and each request's position among them.
+struct TimeMap {
+    std::size_t T = 0, U = 0, t_count = 0;
+    std::vector<int> tmap;        // [t_count] sample -> unique-time position, or -1
+    std::vector<uint32_t> out_u;  // [T] request -> unique-time position
+};
+
+std::shared_ptr<const TimeMap> make_time_map(const TimeList& list) {
+    auto m = std::make_shared<TimeMap>();
+    const uint32_t* tidx = list.begin();
+    m->T = list.size();
+    uint32_t tmax = 0;
+    bool increasing = true;
+    for (std::size_t o = 0; o < m->T; ++o) {
+        tmax = std::max(tmax, tidx[o]);
+        if (o > 0 && tidx[o] <= tidx[o - 1]) increasing = false;
+    }
+    m->t_count = static_cast<std::size_t>(tmax) + 1;
+    m->tmap.assign(m->t_count, -1);
+    m->out_u.resize(m->T);
+    if (increasing) {  // the unique times are the requested ones, in order
+        m->U = m->T;
+        for (std::size_t o = 0; o < m->T; ++o) {
+            m->tmap[tidx[o]] = static_cast<int>(o);
+            m->out_u[o] = static_cast<uint32_t>(o);
+        }
+    } else {
+        std::vector<uint32_t> uniq(list.vec());
+        std::sort(uniq.begin(), uniq.end());
+        uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+        m->U = uniq.size();
+        for (std::size_t u = 0; u < uniq.size(); ++u) m->tmap[uniq[u]] = static_cast<int>(u);
+        for (std::size_t o = 0; o < m->T; ++o) m->out_u[o] = static_cast<uint32_t>(m->tmap[tidx[o]]);
+    }
+    return m;
+}
+
 struct InstMeta {
     std::size_t T = 0, U = 0, t_count = 0, n_in = 0;
     int L = 0, R = 1;  // FFT length R * 2^L
-    std::vector<int> tmap;          // [t_count]
-    std::vector<uint32_t> out_u;    // [T]
+    std::shared_ptr<const TimeMap> times;   // tmap [t_count], out_u [T]
     std::shared_ptr<const CoefTable> coef;  // shared with the table cache (empty when unused)
 };
 
@@ -552,31 +618,12 @@ void choose_fft(std::size_t target, bool fp32, bool allow_mixed, int& L_out, int
     }
 }
 
-void derive_meta(const Tcl4Instance& in, const BuildOptions& opt, InstMeta& m, bool want_coef) {
-    m.T = in.tidx.size();
-    uint32_t tmax = 0;
-    bool increasing = true;
-    for (std::size_t o = 0; o < m.T; ++o) {
-        tmax = std::max(tmax, in.tidx[o]);
-        if (o > 0 && in.tidx[o] <= in.tidx[o - 1]) increasing = false;
-    }
-    m.t_count = static_cast<std::size_t>(tmax) + 1;
-    m.tmap.assign(m.t_count, -1);
-    m.out_u.resize(m.T);
-    if (increasing) {  // the unique times are the requested ones, in order
-        m.U = m.T;
-        for (std::size_t o = 0; o < m.T; ++o) {
-            m.tmap[in.tidx[o]] = static_cast<int>(o);
-            m.out_u[o] = static_cast<uint32_t>(o);
-        }
-    } else {
-        std::vector<uint32_t> uniq(in.tidx);
-        std::sort(uniq.begin(), uniq.end());
-        uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-        m.U = uniq.size();
-        for (std::size_t u = 0; u < uniq.size(); ++u) m.tmap[uniq[u]] = static_cast<int>(u);
-        for (std::size_t o = 0; o < m.T; ++o) m.out_u[o] = static_cast<uint32_t>(m.tmap[in.tidx[o]]);
-    }
+void derive_meta(const Tcl4Instance& in, const BuildOptions& opt, InstMeta& m, bool want_coef,
+                 std::shared_ptr<const TimeMap> times = nullptr) {
+    m.times = times ? std::move(times) : make_time_map(in.tidx);
+    m.T = m.times->T;
+    m.U = m.times->U;
+    m.t_count = m.times->t_count;
     m.n_in = opt.causal_truncation ? m.t_count : in.Nt;
     std::size_t target = 2 * m.n_in - 1;
     if (opt.pad_factor > 0) target = std::max(target, opt.pad_factor * m.n_in);
@@ -731,6 +778,7 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
                       PinnedBuffer* staging_buf = nullptr) {
     using C = cplx_t<R>;
     (void)opt;
+    const auto t_prep = std::chrono::steady_clock::now();
     const GroupGeom<R> G = group_geom<R>(units);
     const int L = G.L;
     const FftPlan<C> plan = get_plan<R>(ws, L, G.Rf, st);
@@ -781,6 +829,18 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     }();
     const std::size_t n_col_jobs = n_spec_jobs + ntri;
     const std::size_t n_row_jobs = n_spec_jobs + ntri;
+    // one device copy of each distinct time map: first_use[a] is true for the first unit
+    // naming it, and the others reuse that unit's arrays
+    std::vector<char> first_use(ni, 1);
+    std::vector<std::size_t> owner(ni);
+    {
+        std::unordered_map<const TimeMap*, std::size_t> seen;
+        for (std::size_t a = 0; a < ni; ++a) {
+            auto r = seen.emplace(units[a]->meta->times.get(), a);
+            owner[a] = r.first->second;
+            first_use[a] = r.second;
+        }
+    }
     auto layout_meta = [&](Layout& lay) {
         M.tmap.assign(ni, nullptr);
         M.out_u.assign(ni, nullptr);
@@ -789,10 +849,10 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         M.coef.assign(ni, nullptr);
         for (std::size_t a = 0; a < ni; ++a) {
             const InstMeta& m = *units[a]->meta;
-            M.tmap[a] = lay.take<int>(m.t_count);
+            M.tmap[a] = first_use[a] ? lay.take<int>(m.t_count) : M.tmap[owner[a]];
             if (!fcr_only) {
                 const CoefTable& ct = *units[a]->coef;
-                M.out_u[a] = lay.take<uint32_t>(m.T);
+                M.out_u[a] = first_use[a] ? lay.take<uint32_t>(m.T) : M.out_u[owner[a]];
                 M.rowptr[a] = lay.take<int32_t>(ct.rowptr.size());
                 M.src[a] = lay.take<uint32_t>(std::max<std::size_t>(1, ct.src.size()));
                 M.coef[a] = lay.take<C>(std::max<std::size_t>(1, ct.coef.size()));
@@ -943,10 +1003,10 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     if (!fcr_only) plan_copy(M.conj, conj.size() * sizeof(ContractJob));
     for (std::size_t a = 0; a < ni; ++a) {
         const InstMeta& m = *units[a]->meta;
-        plan_copy(M.tmap[a], m.tmap.size() * sizeof(int));
+        if (first_use[a]) plan_copy(M.tmap[a], m.times->tmap.size() * sizeof(int));
         if (!fcr_only) {
             const CoefTable& ct = *units[a]->coef;
-            plan_copy(M.out_u[a], m.out_u.size() * sizeof(uint32_t));
+            if (first_use[a]) plan_copy(M.out_u[a], m.times->out_u.size() * sizeof(uint32_t));
             plan_copy(M.rowptr[a], ct.rowptr.size() * sizeof(int32_t));
             plan_copy(M.src[a], ct.src.size() * sizeof(uint32_t));
             plan_copy(M.coef[a], ct.coef.size() * sizeof(C));
@@ -970,10 +1030,10 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         if (!fcr_only) put(conj.data(), conj.size() * sizeof(ContractJob));
         for (std::size_t a = 0; a < ni; ++a) {
             const InstMeta& m = *units[a]->meta;
-            put(m.tmap.data(), m.tmap.size() * sizeof(int));
+            if (first_use[a]) put(m.times->tmap.data(), m.times->tmap.size() * sizeof(int));
             if (!fcr_only) {
                 const CoefTable& ct = *units[a]->coef;
-                put(m.out_u.data(), m.out_u.size() * sizeof(uint32_t));
+                if (first_use[a]) put(m.times->out_u.data(), m.times->out_u.size() * sizeof(uint32_t));
                 put(ct.rowptr.data(), ct.rowptr.size() * sizeof(int32_t));
                 put(ct.src.data(), ct.src.size() * sizeof(uint32_t));
                 if (std::is_same<R, double>::value) {
@@ -995,8 +1055,10 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
                                          units[a]->in->sys.nf, cudaMemcpyHostToDevice, st),
                        "cudaMemcpy2DAsync(gamma)");
 
-    // the pinned staging buffer is reused by the next call: wait for the copies
-    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(meta)");
+    host_trace_add("prepare.host", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_prep).count());
+    // the pinned staging buffer is reused by the next call: wait for the copies (a caller
+    // that passes its own staging buffer synchronises the stream before reusing it)
+    if (!staging_buf) cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(meta)");
 
     // ---- launches ----
     const ColFn<R> fwd_col = fwd_col_fn<R>(plan.R, plan.L1, g.log2c);
@@ -1395,6 +1457,13 @@ void raise_smem_limit(const void* kernel, std::size_t bytes) {
     g = bytes;
 }
 void count_launches(uint64_t n) { g_launches.fetch_add(n); }
+bool host_trace_on() {
+    static const bool on = std::getenv("TACO_TRACE_HOST") != nullptr;
+    return on;
+}
+void host_trace_add(const char* phase, double ms) {
+    if (host_trace_on()) t_phases.add(phase, ms);
+}
 void profile_enable(bool on) { g_profile.store(on); }
 void profile_reset() {
     ProfStore& ps = prof_store();
@@ -1456,8 +1525,10 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
     Workspace& ws = workspace();
     cudaStream_t st = stream ? stream : ws.stream;
     if (opt.fcr_ms) *opt.fcr_ms = 0.0;
+    Lap lap;
     std::vector<InstMeta> metas;
     validate_and_derive(insts, opt, metas);
+    lap("derive");
     const std::size_t budget = work_budget();
     HostIoStage io;
     std::vector<std::unique_ptr<WorkUnit>> store;
@@ -1469,6 +1540,7 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
         stage_sliced_io<double>(insts, metas, budget, io, st);
         groups = plan_units<double>(insts, metas, budget, store);
     }
+    lap("plan");
     // Large builds of whole instances run as sub-batches of about kPipeSub instances on two
     // lanes (streams with their own buffers): the host preparation and the input upload of
     // one sub-batch overlap the kernels and the output download of the other.  Slices
@@ -1487,6 +1559,7 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
             if (opt.fp32) run_group<float>(gu, opt, st, ws, nullptr, false);
             else run_group<double>(gu, opt, st, ws, nullptr, false);
         }
+        lap("groups");
     } else {
         if (!ws.stream2) cuda_check(cudaStreamCreateWithFlags(&ws.stream2, cudaStreamNonBlocking), "cudaStreamCreate");
         // the second lane starts after the work already queued on the caller's stream
@@ -1507,16 +1580,27 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
                 const Lane& L = lanes[k++ & 1];
                 // the lane's previous sub-batch has finished with its buffers
                 cuda_check(cudaStreamSynchronize(L.s), "cudaStreamSynchronize(lane)");
+                lap("lane_wait");
                 Enqueue enq = opt.fp32 ? prepare_group<float>(sub, opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging)
                                        : prepare_group<double>(sub, opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging);
+                lap("prepare");
                 enq(L.s, nullptr, nullptr, nullptr);
+                lap("enqueue");
             }
         }
         cuda_check(cudaStreamSynchronize(ws.stream2), "cudaStreamSynchronize(lane)");
+        lap("lane_wait");
     }
     for (const auto& b : io.back)
         cuda_check(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(sliced out)");
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(build)");
+    lap("final_wait");
+    if (lap.on) {
+        std::string line = "taco host phases (ms, " + std::to_string(insts.size()) + " instances):";
+        for (const auto& e : t_phases.ms) line += " " + std::string(e.first) + "=" + std::to_string(e.second);
+        std::fprintf(stderr, "%s\n", line.c_str());
+        t_phases.ms.clear();
+    }
 }
 
 // F/C/R series of many instances with device buffers: instances of equal Nt share build
@@ -1549,8 +1633,7 @@ void triple_kernels_batch(const std::vector<FcrRequest>& reqs, const BuildOption
         in.gamma_on_device = true;
         in.Nt = r.Nt;
         in.dt = r.dt;
-        in.tidx.resize(r.Nt);
-        for (std::size_t t = 0; t < r.Nt; ++t) in.tidx[t] = static_cast<uint32_t>(t);
+        in.tidx.iota(r.Nt);
         derive_meta(in, o, metas[k], false);
     }
     std::vector<WorkUnit> units(reqs.size());
@@ -1606,8 +1689,7 @@ void triple_kernels(const SystemDesc& sys, const double2* gamma, bool gamma_on_d
     in.gamma_on_device = gamma_on_device;
     in.Nt = Nt;
     in.dt = dt;
-    in.tidx.resize(Nt);
-    for (std::size_t t = 0; t < Nt; ++t) in.tidx[t] = static_cast<uint32_t>(t);
+    in.tidx.iota(Nt);
     BuildOptions o = opt;
     o.fp32 = false;
     o.causal_truncation = false;
@@ -1643,8 +1725,30 @@ struct Tcl4Plan {
 
 namespace {
 void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, std::vector<InstMeta>& metas) {
-    metas.resize(insts.size());
-    for (std::size_t a = 0; a < insts.size(); ++a) {
+    const std::size_t n = insts.size();
+    metas.resize(n);
+    const unsigned nthreads =
+        n >= 16 ? std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency())) : 1u;
+    // fn(k) for k in [0, count) on the host threads (round robin)
+    auto spread = [&](std::size_t count, const std::function<void(std::size_t)>& fn) {
+        const unsigned nt = static_cast<unsigned>(std::min<std::size_t>(nthreads, count));
+        if (nt <= 1) {
+            for (std::size_t k = 0; k < count; ++k) fn(k);
+            return;
+        }
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t)
+            pool.emplace_back([&, t] {
+                for (std::size_t k = t; k < count; k += nt) fn(k);
+            });
+        for (auto& th : pool) th.join();
+    };
+    // distinct time lists (instances sharing a caller's array share one list)
+    constexpr std::size_t kNone = ~std::size_t(0);
+    std::unordered_map<const void*, std::size_t> list_index;
+    std::vector<std::size_t> first;          // first instance of each distinct list
+    std::vector<std::size_t> lid(n, kNone);  // list of each instance
+    for (std::size_t a = 0; a < n; ++a) {
         Tcl4Instance& in = insts[a];
         validate_system(in.sys);
         if (in.Nt == 0) throw Error(kInvalidArgument, "empty gamma_series");
@@ -1653,22 +1757,26 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
         if (!in.gamma) throw Error(kInvalidArgument, "gamma is null");
         if (in.tidx.empty()) continue;
         if (!in.out) throw Error(kInvalidArgument, "output pointer is null");
-        for (uint32_t t : in.tidx)
-            if (t >= in.Nt) throw Error(kOutOfRange, "time_index out of range");
+        auto r = list_index.emplace(in.tidx.identity(), first.size());
+        if (r.second) first.push_back(a);
+        lid[a] = r.first->second;
     }
-    // per-instance metadata (time maps, FFT length, coefficient table) on several host
-    // threads for large batches; the first failing instance's error is rethrown
-    // Systems with large coefficient maps (nf >= 21, d >= 5) one at a time, each map built on
-    // several threads; the others spread over the threads, one map per thread.
-    const std::size_t n = insts.size();
-    const unsigned nthreads =
-        n >= 16 ? std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency())) : 1u;
+    std::vector<std::shared_ptr<const TimeMap>> maps(first.size());
+    spread(first.size(), [&](std::size_t k) { maps[k] = make_time_map(insts[first[k]].tidx); });
+    // every requested index below the instance's Nt: t_count = largest index + 1
+    for (std::size_t a = 0; a < n; ++a)
+        if (lid[a] != kNone && maps[lid[a]]->t_count > insts[a].Nt)
+            throw Error(kOutOfRange, "time_index out of range");
+    // per-instance metadata (FFT length, coefficient table) on several host threads for
+    // large batches; the first failing instance's error is rethrown.  Systems with large
+    // coefficient maps (nf >= 21, d >= 5) one at a time, each map built on several threads;
+    // the others spread over the threads, one map per thread.
     std::vector<std::exception_ptr> errs(n);
     auto large = [&](std::size_t a) { return insts[a].sys.nf >= 21; };
     auto derive = [&](std::size_t a) {
-        if (insts[a].tidx.empty()) return;
+        if (lid[a] == kNone) return;
         try {
-            derive_meta(insts[a], opt, metas[a], true);
+            derive_meta(insts[a], opt, metas[a], true, maps[lid[a]]);
         } catch (...) {
             errs[a] = std::current_exception();
         }

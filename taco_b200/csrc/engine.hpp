@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
@@ -18,13 +19,46 @@ struct SystemDesc {
     std::vector<double2> ops;   // num_ops x (N x N) column-major
 };
 
+// Requested time indices of an instance.  Instances of one call that name the same caller
+// array share one copy (share_with), so their time maps are derived and uploaded once.
+class TimeList {
+public:
+    std::size_t size() const { return v_ ? v_->size() : 0; }
+    bool empty() const { return size() == 0; }
+    uint32_t operator[](std::size_t k) const { return (*v_)[k]; }
+    const uint32_t* begin() const { return v_ ? v_->data() : nullptr; }
+    const uint32_t* end() const { return v_ ? v_->data() + v_->size() : nullptr; }
+    const std::vector<uint32_t>& vec() const { return v_ ? *v_ : empty_vec(); }
+    const void* identity() const { return v_.get(); }
+    void assign(const uint32_t* first, const uint32_t* last) {
+        v_ = std::make_shared<std::vector<uint32_t>>(first, last);
+    }
+    void iota(std::size_t n) {  // 0, 1, ..., n-1
+        auto v = std::make_shared<std::vector<uint32_t>>(n);
+        for (std::size_t t = 0; t < n; ++t) (*v)[t] = static_cast<uint32_t>(t);
+        v_ = std::move(v);
+    }
+    TimeList& operator=(const std::vector<uint32_t>& v) {
+        v_ = std::make_shared<std::vector<uint32_t>>(v);
+        return *this;
+    }
+    void share_with(const TimeList& o) { v_ = o.v_; }
+
+private:
+    static const std::vector<uint32_t>& empty_vec() {
+        static const std::vector<uint32_t> e;
+        return e;
+    }
+    std::shared_ptr<const std::vector<uint32_t>> v_;
+};
+
 struct Tcl4Instance {
     SystemDesc sys;
     const double2* gamma = nullptr;  // [nf][Nt] (column-major Nt x nf)
     bool gamma_on_device = false;
     std::size_t Nt = 0;
     double dt = 0.0;
-    std::vector<uint32_t> tidx;      // explicit list of requested time indices
+    TimeList tidx;                   // explicit list of requested time indices
     void* out = nullptr;             // [T][N^2 x N^2] complex (FP64: double2, FP32: float2)
     bool out_on_device = false;
 };
@@ -230,6 +264,11 @@ uint64_t kernel_launches();
 void raise_smem_limit(const void* kernel, std::size_t bytes);
 // Adds n to the process-wide launch counter (kernels launched outside engine.cu).
 void count_launches(uint64_t n);
+// Host phase times of the build calls: with TACO_TRACE_HOST set in the environment each
+// tcl4_build prints, on stderr, the milliseconds its host thread spent in each phase
+// (argument conversion, metadata derivation, preparation, waits).  Diagnostic only.
+bool host_trace_on();
+void host_trace_add(const char* phase, double ms);
 // Checks the launch just issued and counts it.
 inline void launched(const char* what) {
     cuda_check(cudaGetLastError(), what);

@@ -267,3 +267,29 @@ def test_triple_kernels_batch_matches_single_calls():
         single = tb.compute_triple_kernels(s, g, 0.01)
         for a, b in zip(out, single):
             assert relerr(a.cpu().numpy(), b.cpu().numpy()) <= 1e-12
+
+
+def test_shared_time_lists_match_single_calls():
+    """Instances that share one time-index array (one derived time map and one upload per
+    build group), instances with their own unsorted lists with repeats, and one equal list
+    in a separate array: each result equals its single-instance call, in the pipelined
+    (72 instances) and the single-lane (5 instances) paths.  A shared list that exceeds a
+    shorter instance's gamma raises the reference's out-of-range error."""
+    rng = np.random.default_rng(11)
+    cases = [spin_boson_case(600, 0.01, eps=rng.uniform(0.5, 2.0), delta=rng.uniform(0.5, 2.0))
+             for _ in range(72)]
+    shared = np.arange(0, 300, 3)
+    own = rng.integers(0, 400, 90)  # unsorted, with repeats
+    equal = shared.copy()
+    lists = [shared if k % 3 == 0 else (own if k % 3 == 1 else equal) for k in range(72)]
+    inst = [(s, G, 0.01, lists[k]) for k, (_, s, G) in enumerate(cases)]
+    for sel in (list(range(72)), [0, 1, 2, 3, 4]):
+        batch = [np.asarray(x) for x in tb.build_instances([inst[k] for k in sel], precision="fp64")]
+        for pos in sorted({0, 1, 2, len(sel) - 2, len(sel) - 1}):
+            k = sel[pos]
+            single = np.asarray(tb.build_instances([inst[k]], precision="fp64")[0])
+            assert batch[pos].shape == single.shape
+            assert relerr(batch[pos], single) <= 1e-12
+    _, s_short, G_short = spin_boson_case(200, 0.01)
+    with pytest.raises(tb.TacoOutOfRange):
+        tb.build_instances([inst[0], (s_short, G_short, 0.01, shared)], precision="fp64")
