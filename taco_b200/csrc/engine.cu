@@ -152,17 +152,21 @@ struct Workspace {
     DeviceBuffer arena;  // metadata of the running group
     DeviceBuffer work;   // transient arrays of the running group
     PinnedBuffer staging;
-    // second lane of pipelined direct builds: its own stream and buffers
-    cudaStream_t stream2 = nullptr;
-    DeviceBuffer arena2, work2;
-    PinnedBuffer staging2;
+    // further lanes of pipelined direct builds: their own streams and buffers
+    struct ExtraLane {
+        cudaStream_t s = nullptr;
+        DeviceBuffer arena, work;
+        PinnedBuffer staging;
+    };
+    ExtraLane extra[2];
     std::map<std::pair<int, int>, std::unique_ptr<PlanTables>> plans;  // (L, fp32)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~Workspace() {
         plans.clear();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        if (stream2) cudaStreamDestroy(stream2);
+        for (auto& l : extra)
+            if (l.s) cudaStreamDestroy(l.s);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -1542,10 +1546,10 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
     }
     lap("plan");
     // Large builds of whole instances run as sub-batches of about kPipeSub instances on two
-    // lanes (streams with their own buffers): the host preparation and the input upload of
-    // one sub-batch overlap the kernels and the output download of the other.  Slices
-    // (ordered accumulation), profiling and F/C/R timing keep the single-lane order.
-    constexpr std::size_t kPipeSub = 64;
+    // or three lanes (streams with their own buffers): the host preparation and the input
+    // upload of one sub-batch overlap the kernels and the output download of the others.
+    // Slices (ordered accumulation), profiling and F/C/R timing keep the single-lane order.
+    constexpr std::size_t kPipeSub = 48;
     std::size_t nunits = 0;
     bool whole = true;
     for (auto& gu : groups)
@@ -1561,34 +1565,47 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
         }
         lap("groups");
     } else {
-        if (!ws.stream2) cuda_check(cudaStreamCreateWithFlags(&ws.stream2, cudaStreamNonBlocking), "cudaStreamCreate");
-        // the second lane starts after the work already queued on the caller's stream
-        cuda_check(cudaEventRecord(ws.ev0, st), "cudaEventRecord");
-        cuda_check(cudaStreamWaitEvent(ws.stream2, ws.ev0, 0), "cudaStreamWaitEvent");
+        // sub-batches of kPipeSub instances or more (rounded count per group)
+        std::vector<std::vector<WorkUnit*>> subs;
+        std::size_t max_work = 0;
+        for (auto& gu : groups) {
+            const std::size_t n = gu.size(), parts = std::max<std::size_t>(1, (n + kPipeSub / 2) / kPipeSub);
+            for (std::size_t p = 0; p < parts; ++p) {
+                subs.emplace_back(gu.begin() + p * n / parts, gu.begin() + (p + 1) * n / parts);
+                max_work = std::max(max_work, opt.fp32 ? measure_work<float>(subs.back(), false, false)
+                                                       : measure_work<double>(subs.back(), false, false));
+            }
+        }
+        // a third lane while three sub-batches' transient arrays fit twice the group budget
+        const std::size_t nlanes = subs.size() >= 3 && 3 * max_work <= 2 * budget ? 3 : 2;
         struct Lane {
             cudaStream_t s;
             DeviceBuffer* arena;
             DeviceBuffer* work;
             PinnedBuffer* staging;
         };
-        const Lane lanes[2] = {{st, &ws.arena, &ws.work, &ws.staging}, {ws.stream2, &ws.arena2, &ws.work2, &ws.staging2}};
-        std::size_t k = 0;
-        for (auto& gu : groups) {
-            const std::size_t n = gu.size(), parts = (n + kPipeSub - 1) / kPipeSub;
-            for (std::size_t p = 0; p < parts; ++p) {
-                std::vector<WorkUnit*> sub(gu.begin() + p * n / parts, gu.begin() + (p + 1) * n / parts);
-                const Lane& L = lanes[k++ & 1];
-                // the lane's previous sub-batch has finished with its buffers
-                cuda_check(cudaStreamSynchronize(L.s), "cudaStreamSynchronize(lane)");
-                lap("lane_wait");
-                Enqueue enq = opt.fp32 ? prepare_group<float>(sub, opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging)
-                                       : prepare_group<double>(sub, opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging);
-                lap("prepare");
-                enq(L.s, nullptr, nullptr, nullptr);
-                lap("enqueue");
-            }
+        std::vector<Lane> lanes{{st, &ws.arena, &ws.work, &ws.staging}};
+        // the other lanes start after the work already queued on the caller's stream
+        cuda_check(cudaEventRecord(ws.ev0, st), "cudaEventRecord");
+        for (std::size_t l = 1; l < nlanes; ++l) {
+            auto& x = ws.extra[l - 1];
+            if (!x.s) cuda_check(cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking), "cudaStreamCreate");
+            cuda_check(cudaStreamWaitEvent(x.s, ws.ev0, 0), "cudaStreamWaitEvent");
+            lanes.push_back({x.s, &x.arena, &x.work, &x.staging});
         }
-        cuda_check(cudaStreamSynchronize(ws.stream2), "cudaStreamSynchronize(lane)");
+        for (std::size_t k = 0; k < subs.size(); ++k) {
+            const Lane& L = lanes[k % nlanes];
+            // the lane's previous sub-batch has finished with its buffers
+            cuda_check(cudaStreamSynchronize(L.s), "cudaStreamSynchronize(lane)");
+            lap("lane_wait");
+            Enqueue enq = opt.fp32 ? prepare_group<float>(subs[k], opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging)
+                                   : prepare_group<double>(subs[k], opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging);
+            lap("prepare");
+            enq(L.s, nullptr, nullptr, nullptr);
+            lap("enqueue");
+        }
+        for (std::size_t l = 1; l < nlanes; ++l)
+            cuda_check(cudaStreamSynchronize(lanes[l].s), "cudaStreamSynchronize(lane)");
         lap("lane_wait");
     }
     for (const auto& b : io.back)
