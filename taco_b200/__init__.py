@@ -137,6 +137,8 @@ def _addr(x) -> int:
         return 0
     if _is_torch(x):
         return x.data_ptr()
+    if x.flags.writeable and x.flags.c_contiguous and x.size:
+        return ct.addressof(ct.c_char.from_buffer(x))  # the cheapest route for writable buffers
     return x.__array_interface__["data"][0]
 
 
@@ -185,21 +187,20 @@ def _out_array(like_device, shape, dtype, device=None):
     return np.empty(shape, dtype=dtype)
 
 
-def _content_key(x):
-    a = x if isinstance(x, np.ndarray) else np.asarray(x)
-    return a.dtype.str, a.shape, a.tobytes()
-
-
 def _system_view(system: System) -> _View:
     """The _View of `system`, reused while its arrays hold the same contents.
 
-    Batched calls marshal hundreds of systems per call; the key (the bytes of the small
-    arrays a view copies) costs a fraction of building the view again.
+    Batched calls marshal hundreds of systems per call; the key (the bytes, types and shapes
+    of the small arrays a view copies) costs a fraction of building the view again.
+    Systems whose fields are not numpy arrays are marshalled every call.
     """
-    ops = system.A_eig
-    key = (int(system.N), int(system.nf), float(system.tol), _content_key(system.omegas),
-           _content_key(system.mirror), _content_key(system.pair_to_freq),
-           tuple(_content_key(A) for A in ops))
+    om, mi, pf, ops = system.omegas, system.mirror, system.pair_to_freq, system.A_eig
+    if not (type(om) is np.ndarray and type(mi) is np.ndarray and type(pf) is np.ndarray
+            and all(type(A) is np.ndarray for A in ops)):
+        return _View(system)
+    key = (system.N, system.nf, system.tol, om.dtype.char, om.shape, om.tobytes(), mi.dtype.char, mi.shape,
+           mi.tobytes(), pf.dtype.char, pf.shape, pf.tobytes(),
+           tuple((A.dtype.char, A.shape, A.tobytes()) for A in ops))
     cached = getattr(system, "_taco_view", None)
     if cached is not None and cached[0] == key:
         return cached[1]
