@@ -159,6 +159,19 @@ struct Workspace {
         PinnedBuffer staging;
     };
     ExtraLane extra[2];
+    // per sub-batch buffers of pipelined direct builds (metadata, staged host input, pinned
+    // staging, upload event) and the stream that carries every upload of such a build
+    struct SubBuffers {
+        DeviceBuffer arena, input;
+        PinnedBuffer staging;
+        cudaEvent_t uploaded = nullptr, done = nullptr;
+        ~SubBuffers() {
+            if (uploaded) cudaEventDestroy(uploaded);
+            if (done) cudaEventDestroy(done);
+        }
+    };
+    std::vector<std::unique_ptr<SubBuffers>> sub_bufs;
+    cudaStream_t upload = nullptr;
     std::map<std::pair<int, int>, std::unique_ptr<PlanTables>> plans;  // (L, fp32)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~Workspace() {
@@ -167,6 +180,8 @@ struct Workspace {
         if (ev1) cudaEventDestroy(ev1);
         for (auto& l : extra)
             if (l.s) cudaStreamDestroy(l.s);
+        sub_bufs.clear();
+        if (upload) cudaStreamDestroy(upload);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -224,6 +239,8 @@ FftPlan<cplx_t<R>> get_plan(Workspace& ws, int L, int Rf, cudaStream_t st) {
         fill(tw2, N2, static_cast<double>(N2));
         fill(twc, nc, static_cast<double>(nc));
         fill(twf, nfine, static_cast<double>(N));
+        // kernels on other streams (pipelined lanes) read the tables: complete them first
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(twiddles)");
         slot = std::move(pt);
     }
     const PlanTables& pt = *slot;
@@ -267,6 +284,7 @@ ClusterPlan<cplx_t<R>> get_cluster_plan(Workspace& ws, int L, int LM, cudaStream
         fill(twM, M, static_cast<double>(M));
         fill(twc, nc, static_cast<double>(nc));
         fill(twf, nfine, static_cast<double>(N));
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(twiddles)");
         slot = std::move(pt);
     }
     Layout lay{static_cast<char*>(slot->buf.p)};
@@ -731,7 +749,7 @@ struct WorkPtrs {
 
 template <class R>
 void layout_work(const std::vector<WorkUnit*>& units, const GroupGeom<R>& G, bool fcr_only, bool fcr_out_dev,
-                 Layout& lay, WorkPtrs<cplx_t<R>>& P) {
+                 Layout& lay, WorkPtrs<cplx_t<R>>& P, bool gamma_elsewhere = false) {
     using C = cplx_t<R>;
     const std::size_t ni = units.size();
     P.gamma.assign(ni, nullptr);
@@ -743,7 +761,7 @@ void layout_work(const std::vector<WorkUnit*>& units, const GroupGeom<R>& G, boo
         const Tcl4Instance& in = *units[a]->in;
         const InstMeta& m = *units[a]->meta;
         const std::size_t nf = in.sys.nf, nsub = units[a]->nsub();
-        if (!in.gamma_on_device) P.gamma[a] = lay.take<double2>(nf * m.n_in);
+        if (!in.gamma_on_device && !gamma_elsewhere) P.gamma[a] = lay.take<double2>(nf * m.n_in);
         P.spec[a] = lay.take<C>(2 * nf * G.Nfft);
         P.conv[a] = lay.take<C>(nsub * 2 * m.t_count);
         if (!fcr_only) {
@@ -779,7 +797,8 @@ using Enqueue = std::function<void(cudaStream_t, ProfRecorder*, cudaEvent_t, cud
 template <class R>
 Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cudaStream_t st, Workspace& ws,
                       DeviceBuffer& meta_mem, DeviceBuffer& work_mem, double2* const* fcr_out, bool fcr_out_dev,
-                      PinnedBuffer* staging_buf = nullptr) {
+                      PinnedBuffer* staging_buf = nullptr, DeviceBuffer* input_mem = nullptr,
+                      cudaStream_t upload = nullptr, cudaEvent_t uploaded = nullptr) {
     using C = cplx_t<R>;
     (void)opt;
     const auto t_prep = std::chrono::steady_clock::now();
@@ -807,11 +826,23 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     // ---- device layout: transient arrays in work_mem, metadata in meta_mem ----
     WorkPtrs<C> P;
     {
+        // staged host gamma in `input_mem` when given (kept apart from the reused work arrays)
+        const bool apart = input_mem != nullptr;
         Layout meas;
-        layout_work<R>(units, G, fcr_only, fcr_out_dev, meas, P);
+        layout_work<R>(units, G, fcr_only, fcr_out_dev, meas, P, apart);
         work_mem.ensure(meas.off + 256);
         Layout lay{static_cast<char*>(work_mem.p)};
-        layout_work<R>(units, G, fcr_only, fcr_out_dev, lay, P);
+        layout_work<R>(units, G, fcr_only, fcr_out_dev, lay, P, apart);
+        if (apart) {
+            Layout mi;
+            for (auto* u : units)
+                if (!u->in->gamma_on_device) mi.take<double2>(static_cast<std::size_t>(u->in->sys.nf) * u->meta->n_in);
+            input_mem->ensure(mi.off + 256);
+            Layout li{static_cast<char*>(input_mem->p)};
+            for (std::size_t a = 0; a < ni; ++a)
+                if (!units[a]->in->gamma_on_device)
+                    P.gamma[a] = li.take<double2>(static_cast<std::size_t>(units[a]->in->sys.nf) * units[a]->meta->n_in);
+        }
     }
     struct MetaPtrs {
         std::vector<int*> tmap;
@@ -1050,14 +1081,18 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
             }
         }
     }
-    if (soff) cuda_check(cudaMemcpyAsync(meta_mem.p, sb, soff, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(meta)");
+    // uploads on `upload` when given, else on st
+    cudaStream_t cs = upload ? upload : st;
+    if (soff) cuda_check(cudaMemcpyAsync(meta_mem.p, sb, soff, cudaMemcpyHostToDevice, cs), "cudaMemcpyAsync(meta)");
     // host gamma: only the n_in leading samples of each bucket are consumed
     for (std::size_t a = 0; a < ni; ++a)
         if (!units[a]->in->gamma_on_device)
             cuda_check(cudaMemcpy2DAsync(const_cast<double2*>(P.gamma[a]), gs[a] * sizeof(double2), units[a]->in->gamma,
                                          units[a]->in->Nt * sizeof(double2), units[a]->meta->n_in * sizeof(double2),
-                                         units[a]->in->sys.nf, cudaMemcpyHostToDevice, st),
+                                         units[a]->in->sys.nf, cudaMemcpyHostToDevice, cs),
                        "cudaMemcpy2DAsync(gamma)");
+    // the caller makes the kernels' stream wait for `uploaded` before it enqueues them
+    if (upload) cuda_check(cudaEventRecord(uploaded, upload), "cudaEventRecord(uploaded)");
 
     host_trace_add("prepare.host", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_prep).count());
     // the pinned staging buffer is reused by the next call: wait for the copies (a caller
@@ -1567,46 +1602,105 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
     } else {
         // sub-batches of kPipeSub instances or more (rounded count per group)
         std::vector<std::vector<WorkUnit*>> subs;
-        std::size_t max_work = 0;
+        std::size_t max_work = 0, max_input = 0;
         for (auto& gu : groups) {
             const std::size_t n = gu.size(), parts = std::max<std::size_t>(1, (n + kPipeSub / 2) / kPipeSub);
             for (std::size_t p = 0; p < parts; ++p) {
                 subs.emplace_back(gu.begin() + p * n / parts, gu.begin() + (p + 1) * n / parts);
                 max_work = std::max(max_work, opt.fp32 ? measure_work<float>(subs.back(), false, false)
                                                        : measure_work<double>(subs.back(), false, false));
+                std::size_t in_bytes = 0;
+                for (auto* u : subs.back())
+                    if (!u->in->gamma_on_device)
+                        in_bytes += static_cast<std::size_t>(u->in->sys.nf) * u->meta->n_in * sizeof(double2) + 256;
+                max_input = std::max(max_input, in_bytes);
             }
         }
         // a third lane while three sub-batches' transient arrays fit twice the group budget
         const std::size_t nlanes = subs.size() >= 3 && 3 * max_work <= 2 * budget ? 3 : 2;
+        // sub-batch buffer slots (metadata, staged input): up to two per lane, while the
+        // lanes' work arrays and the slots' inputs fit twice the group budget; a slot is
+        // reused once the sub-batch that held it has finished
+        std::size_t nslots = std::min<std::size_t>(subs.size(), 2 * nlanes);
+        while (nslots > 1 && nlanes * max_work + nslots * max_input > 2 * budget) --nslots;
         struct Lane {
             cudaStream_t s;
-            DeviceBuffer* arena;
             DeviceBuffer* work;
-            PinnedBuffer* staging;
         };
-        std::vector<Lane> lanes{{st, &ws.arena, &ws.work, &ws.staging}};
-        // the other lanes start after the work already queued on the caller's stream
+        std::vector<Lane> lanes{{st, &ws.work}};
+        if (!ws.upload) cuda_check(cudaStreamCreateWithFlags(&ws.upload, cudaStreamNonBlocking), "cudaStreamCreate");
+        // the other lanes and the uploads start after the work already queued on the caller's stream
         cuda_check(cudaEventRecord(ws.ev0, st), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(ws.upload, ws.ev0, 0), "cudaStreamWaitEvent");
         for (std::size_t l = 1; l < nlanes; ++l) {
             auto& x = ws.extra[l - 1];
             if (!x.s) cuda_check(cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking), "cudaStreamCreate");
             cuda_check(cudaStreamWaitEvent(x.s, ws.ev0, 0), "cudaStreamWaitEvent");
-            lanes.push_back({x.s, &x.arena, &x.work, &x.staging});
+            lanes.push_back({x.s, &x.work});
         }
-        for (std::size_t k = 0; k < subs.size(); ++k) {
-            const Lane& L = lanes[k % nlanes];
-            // the lane's previous sub-batch has finished with its buffers
-            cuda_check(cudaStreamSynchronize(L.s), "cudaStreamSynchronize(lane)");
-            lap("lane_wait");
-            Enqueue enq = opt.fp32 ? prepare_group<float>(subs[k], opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging)
-                                   : prepare_group<double>(subs[k], opt, L.s, ws, *L.arena, *L.work, nullptr, false, L.staging);
-            lap("prepare");
-            enq(L.s, nullptr, nullptr, nullptr);
-            lap("enqueue");
+        // Every buffer a sub-batch writes from the host (metadata, staged input) is its own, so
+        // the host never waits inside the loop: all uploads queue on the upload stream ahead of
+        // the downloads, each lane's kernels wait for their sub-batch's upload event, and a
+        // lane's work arrays (sized here for the largest sub-batch) are reused in its stream order.
+        while (ws.sub_bufs.size() < nslots) {
+            ws.sub_bufs.push_back(std::make_unique<Workspace::SubBuffers>());
+            cuda_check(cudaEventCreateWithFlags(&ws.sub_bufs.back()->uploaded, cudaEventDisableTiming), "cudaEventCreate");
+            cuda_check(cudaEventCreateWithFlags(&ws.sub_bufs.back()->done, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        for (auto& L : lanes) L.work->ensure(max_work);
+        // traced calls time each sub-batch on the device: lane start, inputs uploaded,
+        // F/C/R done, outputs downloaded
+        std::vector<cudaEvent_t> evs(lap.on ? 4 * subs.size() : 0);
+        for (auto& e : evs) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        // in waves of nslots sub-batches: every upload of a wave is queued before any of its
+        // downloads (a download queued first, while it waits for its kernels, held back the
+        // uploads queued after it)
+        for (std::size_t w0 = 0; w0 < subs.size(); w0 += nslots) {
+            const std::size_t w1 = std::min(subs.size(), w0 + nslots);
+            std::vector<Enqueue> enqs;
+            for (std::size_t k = w0; k < w1; ++k) {
+                const Lane& L = lanes[k % nlanes];
+                Workspace::SubBuffers& sb = *ws.sub_bufs[k % nslots];
+                if (k >= nslots) {
+                    cuda_check(cudaEventSynchronize(sb.done), "cudaEventSynchronize(slot)");
+                    lap("slot_wait");
+                }
+                enqs.push_back(opt.fp32 ? prepare_group<float>(subs[k], opt, L.s, ws, sb.arena, *L.work, nullptr, false,
+                                                               &sb.staging, &sb.input, ws.upload, sb.uploaded)
+                                        : prepare_group<double>(subs[k], opt, L.s, ws, sb.arena, *L.work, nullptr, false,
+                                                                &sb.staging, &sb.input, ws.upload, sb.uploaded));
+                lap("prepare");
+            }
+            for (std::size_t k = w0; k < w1; ++k) {
+                const Lane& L = lanes[k % nlanes];
+                if (lap.on) cuda_check(cudaEventRecord(evs[4 * k], L.s), "cudaEventRecord");
+                cuda_check(cudaStreamWaitEvent(L.s, ws.sub_bufs[k % nslots]->uploaded, 0), "cudaStreamWaitEvent(uploaded)");
+                if (lap.on) cuda_check(cudaEventRecord(evs[4 * k + 1], L.s), "cudaEventRecord");
+                enqs[k - w0](L.s, nullptr, nullptr, lap.on ? evs[4 * k + 2] : nullptr);
+                cuda_check(cudaEventRecord(ws.sub_bufs[k % nslots]->done, L.s), "cudaEventRecord(slot)");
+                if (lap.on) cuda_check(cudaEventRecord(evs[4 * k + 3], L.s), "cudaEventRecord");
+                lap("enqueue");
+            }
         }
         for (std::size_t l = 1; l < nlanes; ++l)
             cuda_check(cudaStreamSynchronize(lanes[l].s), "cudaStreamSynchronize(lane)");
+        cuda_check(cudaStreamSynchronize(ws.upload), "cudaStreamSynchronize(upload)");
         lap("lane_wait");
+        if (lap.on) {
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(build)");
+            std::string line = "taco sub-batch device times (ms from the first lane event; queued/uploaded/fcr/done):";
+            for (std::size_t k = 0; k < subs.size(); ++k) {
+                line += " [" + std::to_string(subs[k].size()) + " inst, lane " + std::to_string(k % nlanes) + ":";
+                for (int q = 0; q < 4; ++q) {
+                    float ms = 0.f;
+                    cuda_check(cudaEventElapsedTime(&ms, evs[0], evs[4 * k + q]), "cudaEventElapsedTime");
+                    line += " " + std::to_string(ms);
+                }
+                line += "]";
+            }
+            std::fprintf(stderr, "%s\n", line.c_str());
+        }
+        for (auto& e : evs) cudaEventDestroy(e);
     }
     for (const auto& b : io.back)
         cuda_check(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(sliced out)");

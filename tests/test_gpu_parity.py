@@ -293,3 +293,36 @@ def test_shared_time_lists_match_single_calls():
     _, s_short, G_short = spin_boson_case(200, 0.01)
     with pytest.raises(tb.TacoOutOfRange):
         tb.build_instances([inst[0], (s_short, G_short, 0.01, shared)], precision="fp64")
+
+
+def test_pipelined_slots_are_reused_safely():
+    """336 host-buffer instances make seven sub-batches, more than the buffer slots of three
+    lanes: the last sub-batch reuses the first one's metadata and input buffers after it has
+    finished.  Results equal single-instance calls in the first and the last sub-batches."""
+    rng = np.random.default_rng(21)
+    cases = [spin_boson_case(400, 0.01, eps=rng.uniform(0.5, 2.0), delta=rng.uniform(0.5, 2.0))
+             for _ in range(13)]
+    tidx = np.arange(0, 200, 2)
+    inst = [(cases[k % 13][1], cases[k % 13][2], 0.01, tidx) for k in range(336)]
+    batch = [np.asarray(x) for x in tb.build_instances(inst, precision="fp32")]
+    for k in (0, 5, 47, 290, 301, 335):
+        single = np.asarray(tb.build_instances([inst[k]], precision="fp32")[0])
+        assert relerr(batch[k], single) <= 1e-6
+
+
+def test_long_host_buckets_match_device_inputs():
+    """Host gamma with buckets of 5000 consumed samples (uploaded as one plain copy per
+    bucket) gives the same result as the same gamma on the device, alone and in a
+    48-instance pipelined batch."""
+    import torch
+    osys, s, G = spin_boson_case(6000, 0.002)
+    tidx = np.arange(0, 5000, 7)
+    host = tb.build_TCL4_generator_batch(s, G, 0.002, tidx)
+    dev = tb.build_TCL4_generator_batch(s, torch_dev(G), 0.002, tidx).cpu().numpy()
+    assert np.array_equal(host, dev)
+    Gd = torch_dev(G)
+    outs_h = [np.asarray(x) for x in tb.build_instances([(s, G, 0.002, tidx)] * 48, precision="fp32")]
+    outs_d = [x.cpu().numpy() for x in tb.build_instances([(s, Gd, 0.002, tidx)] * 48, precision="fp32")]
+    torch.cuda.synchronize()
+    for k in (0, 23, 47):
+        assert np.array_equal(outs_h[k], outs_d[k])
