@@ -122,3 +122,32 @@ def test_device_entry_points_fail_loudly_without_gpu():
         tb.compute_triple_kernels(s, g["gamma"], float(g["dt"]))
     with pytest.raises(tb.TacoError):
         tb.propagate_rk4_dense(np.zeros((3, 2, 2)), np.zeros(2), 0.1)
+
+
+def test_system_views_are_reused_only_while_unchanged():
+    """The Python marshalling reuses a System's packed view while its arrays keep their
+    bytes, types and shapes, and rebuilds it after an in-place change or a replaced array;
+    marshalled instances name the same time-index array once."""
+    s = tb.spin_boson_system(1.0, 0.7)
+    v1 = tb._system_view(s)
+    assert tb._system_view(s) is v1
+    s.omegas[0] += 0.25  # in place
+    v2 = tb._system_view(s)
+    assert v2 is not v1 and v2.omegas[0] == s.omegas[0]
+    s.A_eig = [A.copy() * 2.0 for A in s.A_eig]  # replaced, new contents
+    v3 = tb._system_view(s)
+    assert v3 is not v2 and np.allclose(v3.ops[0], np.asarray(s.A_eig[0]).T)
+    s.mirror = s.mirror.astype(np.int64)  # same values, another type
+    assert tb._system_view(s) is not v3
+    # addresses: writable, read-only and empty arrays
+    for a in (np.arange(6.0), np.arange(6.0)[::2].copy(), np.zeros(0)):
+        assert tb._addr(a) == a.__array_interface__["data"][0]
+    r = np.arange(4.0)
+    r.flags.writeable = False
+    assert tb._addr(r) == r.__array_interface__["data"][0]
+    tidx = np.arange(0, 40, 4, dtype=np.uint32)
+    g = np.zeros((s.nf, 50), np.complex128)
+    outs = [np.empty((tidx.size, s.N ** 4), np.complex64) for _ in range(3)]
+    arr, keep, res, dev = tb._instance_array([(s, g, 0.1, tidx)] * 3, _capi.TACO_PREC_FP32, outs)
+    assert not dev and len({arr[k].tidx for k in range(3)}) == 1 and arr[0].T == tidx.size
+    assert [arr[k].L4_out for k in range(3)] == [tb._addr(o) for o in outs]
