@@ -1872,12 +1872,23 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
         if (r.second) first.push_back(a);
         lid[a] = r.first->second;
     }
-    std::vector<std::shared_ptr<const TimeMap>> maps(first.size());
-    spread(first.size(), [&](std::size_t k) { maps[k] = make_time_map(insts[first[k]].tidx); });
-    // every requested index below the instance's Nt: t_count = largest index + 1
+    // every requested index below the instance's Nt, checked before any map is sized by it
+    std::vector<uint32_t> tmax(first.size(), 0);
+    for (std::size_t k = 0; k < first.size(); ++k)
+        for (uint32_t t : insts[first[k]].tidx) tmax[k] = std::max(tmax[k], t);
     for (std::size_t a = 0; a < n; ++a)
-        if (lid[a] != kNone && maps[lid[a]]->t_count > insts[a].Nt)
-            throw Error(kOutOfRange, "time_index out of range");
+        if (lid[a] != kNone && tmax[lid[a]] >= insts[a].Nt) throw Error(kOutOfRange, "time_index out of range");
+    std::vector<std::shared_ptr<const TimeMap>> maps(first.size());
+    std::vector<std::exception_ptr> map_errs(first.size());
+    spread(first.size(), [&](std::size_t k) {
+        try {
+            maps[k] = make_time_map(insts[first[k]].tidx);
+        } catch (...) {
+            map_errs[k] = std::current_exception();
+        }
+    });
+    for (auto& e : map_errs)
+        if (e) std::rethrow_exception(e);
     // per-instance metadata (FFT length, coefficient table) on several host threads for
     // large batches; the first failing instance's error is rethrown.  Systems with large
     // coefficient maps (nf >= 21, d >= 5) one at a time, each map built on several threads;
