@@ -50,7 +50,9 @@ def parse():
     p.add_argument("--tmax", type=int, default=10000)
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=10)
+    p.add_argument("--err-instances", type=int, default=32, help="instances compared with FP64 per window")
+    p.add_argument("--rk4-instances", type=int, default=8, help="C2 RK4 leg: trajectories (0: skip)")
     p.add_argument("--grad-instances", type=int, default=64, help="differentiation form (0: skip)")
     p.add_argument("--grad-N", type=int, default=1 << 16)
     p.add_argument("--grad-dt", type=float, default=1e-3)
@@ -58,7 +60,9 @@ def parse():
     p.add_argument("--c3-dims", default="4,6", help="precision form on random systems (empty: skip)")
     p.add_argument("--c3-N", type=int, default=1 << 18)
     p.add_argument("--c3-stride", type=int, default=4)
-    p.add_argument("--c4-instances", type=int, default=32, help="heterogeneous batch (0: skip; the config names 256)")
+    p.add_argument("--c4-instances", type=int, default=256, help="heterogeneous batch (0: skip)")
+    p.add_argument("--c4-ref-instances", type=int, default=32,
+                   help="heterogeneous batch: instances (evenly spaced) also built in FP64 for the errors")
     return p.parse_args()
 
 
@@ -182,7 +186,7 @@ def kernel_model_bytes(name, inst_shape):
     traffic the kernel cannot avoid.  Inputs shared by all triples of an instance (its nf
     Gamma columns, its 2 nf partner spectra) count once per instance, spread over its nf^3
     triples; per-triple arrays (Z, W_F, W_C, the convolutions, F/C/R) count in full."""
-    n_in, nfft, tcount, U, nf = inst_shape
+    n_in, nfft, tcount, U, nf, E = inst_shape
     s = 8 if name.endswith("f32") else 16
     base = name.rsplit("_", 1)[0]
     per_tri = lambda per_instance: per_instance / nf ** 3
@@ -198,7 +202,47 @@ def kernel_model_bytes(name, inst_shape):
         return 2 * nfft * s, "spectrum"
     if base == "scan_assemble":  # Gamma shared; conv in; F, C, R at the requested times out
         return per_tri(nf * tcount * 16) + 2 * tcount * s + 3 * U * s, "triple"
+    if base == "contract":  # F, C, R at the unique times in; L4 at the requested times out
+        return 3 * nf ** 3 * U * s + tcount * E * s, "instance"
+    if base == "fz_spectra":  # the partner spectra by the fused transform
+        return n_in * 16 / 2 + nfft * s, "spectrum"
+    if base == "fz_conv_scan":  # the survey's per-triple figure of the FFT convolution (A-hat
+        # written and read twice, B-hat read twice) and the F, C, R writes; Gamma shared
+        return per_tri(nf * tcount * 16) + 5 * nfft * s + 3 * U * s, "triple"
     return None, None
+
+
+def causal_fft_length(tcount):
+    """FFT length of the causal rule: the smallest 2^k, 3*2^k or 5*2^k >= 2 tcount - 1."""
+    target = 2 * tcount - 1
+    best = 1 << max(3, (target - 1).bit_length())
+    for r in (3, 5):
+        k = 0
+        while r << k < target:
+            k += 1
+        best = min(best, r << k)
+    return best
+
+
+def headline_config(args, world):
+    """The workload both arms report (the reference arm times a bounded sample of it)."""
+    return {"workload": f"{args.instances} spin-boson instances per GPU (d=2, nf=3), N={args.N} (Nt={args.N + 1}), "
+                        f"dt={args.dt}, tidx 0..{args.tmax}, L4(t) builds",
+            "instances_per_gpu": args.instances, "builds_per_instance": args.tmax + 1,
+            "l2": "inputs larger than L2 (Gamma 9.6 MB x instances; L4 outputs 1.3 MB x instances)",
+            "parallelism": f"instance-sharded x{world}"}
+
+
+def window_errors(a, b, tidx):
+    """Relative Frobenius errors over the requested times in [0, 64) and [2^k, 2^(k+1)), k >= 6."""
+    out = []
+    lo, hi = 0, 64
+    while lo <= int(tidx.max()):
+        m = (tidx >= lo) & (tidx < hi)
+        if m.any():
+            out.append((lo, float(np.linalg.norm(a[m] - b[m]) / max(np.linalg.norm(b[m]), 1e-300))))
+        lo, hi = hi, 2 * hi
+    return out
 
 
 def reference_arm(args, rank, world):
@@ -229,11 +273,11 @@ def reference_arm(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"spin-boson d=2, N={args.N}, dt={args.dt}, tidx 0..{args.tmax}",
-                   "instances_per_step": 1},
+        "config": headline_config(args, world),
         "cpu_baseline": {"value": value, "unit": "builds/s", "cores": threads, "kind": "port",
-                         "sample": f"one instance per step (all 27 triples, FFT 2^19, {tidx.size} L4 builds), "
-                                   "C++/OpenMP restatement of the reference CPU path (reference needs Eigen, absent)"},
+                         "sample": f"one of the {args.instances} instances per step (all 27 triples, FFT 2^19 as the "
+                                   f"reference, {tidx.size} L4 builds, FP64), C++/OpenMP restatement of the reference "
+                                   "CPU path (the reference needs Eigen, absent here)"},
         "e2e": {"value": value, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -275,6 +319,8 @@ def precision_random(args, d, cpu_leg):
     import torch
     import taco_b200 as tb
     from taco_b200 import adjoint as adj
+    tb.release_workspace()
+    torch.cuda.empty_cache()
     rng = np.random.default_rng(args.seed + 300 + d)
     s, A = gue_system(d, rng)
     N, dt = args.c3_N, 1e-3
@@ -331,76 +377,125 @@ def precision_random(args, d, cpu_leg):
 def heterogeneous_batch(args, rank, world, cpu_leg):
     """Batching form: seeded instances with d ~ U{2,3,4,6,8} (GUE H, random unit-norm A),
     Ohmic bath alpha ~ logU[0.01, 0.2], wc ~ U[1, 20], beta ~ logU[0.2, 5], N ~ U{2^14..2^18},
-    dt = 10 / (N wc), every 8th time index; one plan (the FP32 form) replayed as a CUDA
-    graph.  FP64 reference: the same plan in FP64.  CPU leg: the oracle on the smallest
-    instance of each dimension, at four sampled times within its first 2049 steps."""
+    dt = 10 / (N wc), every 8th time index; one plan (the FP32 form with its precision guard)
+    replayed as a CUDA graph.  FP64 reference: the same plan in FP64 on an evenly spaced subset
+    of the instances (errors over the whole series and every dyadic window; <A(t)> by RK4 under
+    L2 + L4 for a few of them).  CPU leg: the oracle on the smallest instance of each dimension,
+    at four sampled times within its first 2049 steps."""
     import torch
     import taco_b200 as tb
     from taco_b200 import adjoint as adj
     B = args.c4_instances
+    tb.release_workspace()  # earlier sections' transient buffers
+    torch.cuda.empty_cache()
     rng = np.random.default_rng(args.seed + 400 + 1000 * rank)
     dims = rng.choice([2, 3, 4, 6, 8], B)
     Ns = 1 << rng.integers(14, 19, B)
     alpha = np.exp(rng.uniform(np.log(0.01), np.log(0.2), B))
     wc = rng.uniform(1.0, 20.0, B)
     beta = np.exp(rng.uniform(np.log(0.2), np.log(5.0), B))
-    systems, gammas, tids, dts = [], [], [], []
+    systems, gammas, tids, dts, As = [], [], [], [], []
     t0 = time.perf_counter()
     for b in range(B):
-        s, _ = gue_system(int(dims[b]), rng)
+        s, A = gue_system(int(dims[b]), rng)
         dt = 10.0 / (Ns[b] * wc[b])
         C = adj.bcf_device([dict(alpha=alpha[b], omega_c=wc[b], beta=beta[b], N=int(Ns[b]), dt=dt)], int(Ns[b]) + 1)[0]
         gammas.append(tb.gamma_trapz_device(C, dt, s.omegas))
         systems.append(s)
+        As.append(A)
         tids.append(np.arange(0, int(Ns[b]), 8, dtype=np.uint32))
         dts.append(dt)
     inputs_s = time.perf_counter() - t0
     inst = [(systems[b], gammas[b], dts[b], tids[b]) for b in range(B)]
     builds = int(sum(t.size for t in tids))
+    # FP64 subset: evenly spaced instances
+    nref = min(B, args.c4_ref_instances)
+    ref_ids = sorted(set(int(round(k * (B - 1) / max(1, nref - 1))) for k in range(nref)))
     out = {"instances_per_gpu": B, "dims": np.bincount(dims, minlength=9)[[2, 3, 4, 6, 8]].tolist(),
            "builds_per_step": builds, "input_build_seconds": round(inputs_s, 2)}
-    res = {}
-    for prec in ("fp32", "fp64"):
-        t0 = time.perf_counter()
-        plan = tb.Tcl4Plan(inst, precision=prec)
-        prep = time.perf_counter() - t0
-        plan.run()
-        torch.cuda.synchronize()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record()
-        plan.run()
-        ev1.record()
-        torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1)
-        out[prec] = {"value": world * builds / (ms / 1e3), "unit": "builds/s", "ms_per_step": ms,
-                     "plan_prepare_seconds": round(prep, 2)}
-        res[prec] = [r.to(torch.complex128) if prec == "fp32" else r for r in plan.results]
-        if prec == "fp32":
-            res[prec] = [r.clone() for r in res[prec]]
-        plan.close()
-    errs = [float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) for a, b in zip(res["fp32"], res["fp64"])]
-    out["l4_fp32_rel_err_vs_fp64_max"] = max(errs)
-    out["per_instance"] = [[int(dims[b]), int(np.log2(Ns[b])), round(float(wc[b]), 3), errs[b]] for b in range(B)]
+    t0 = time.perf_counter()
+    plan = tb.Tcl4Plan(inst, precision="fp32")
+    prep = time.perf_counter() - t0
+    guard = tb.fp32_guard_stats()
+    plan.run()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    plan.run()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    out["fp32"] = {"value": world * builds / (ms / 1e3), "unit": "builds/s", "ms_per_step": ms,
+                   "plan_prepare_seconds": round(prep, 2), "precision_guard": guard}
+    res32 = {b: plan.results[b].to(torch.complex128) for b in ref_ids}
+    plan.close()
+    ref_inst = [inst[b] for b in ref_ids]
+    ref_builds = int(sum(tids[b].size for b in ref_ids))
+    t0 = time.perf_counter()
+    plan64 = tb.Tcl4Plan(ref_inst, precision="fp64")
+    prep64 = time.perf_counter() - t0
+    plan64.run()
+    torch.cuda.synchronize()
+    ev0.record()
+    plan64.run()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms64 = ev0.elapsed_time(ev1)
+    out["fp64_subset"] = {"instances": len(ref_ids), "value": world * ref_builds / (ms64 / 1e3), "unit": "builds/s",
+                          "ms_per_step": ms64, "plan_prepare_seconds": round(prep64, 2)}
+    res64 = {b: r for b, r in zip(ref_ids, plan64.results)}
+    per, werr = [], []
+    for b in ref_ids:
+        a = res32[b].cpu().numpy().reshape(tids[b].size, -1)
+        r = res64[b].cpu().numpy().reshape(tids[b].size, -1)
+        g = float(np.linalg.norm(a - r) / np.linalg.norm(r))
+        w = max(e for _, e in window_errors(a, r, tids[b]))
+        per.append([b, int(dims[b]), int(np.log2(Ns[b])), round(float(wc[b]), 3), g, w])
+        werr.append(w)
+    out["l4_fp32_rel_err_vs_fp64_max"] = max(p[4] for p in per)
+    out["l4_fp32_window_rel_err_max"] = max(werr)
+    out["per_instance"] = per
+    out["per_instance_columns"] = ["instance", "d", "log2 N", "wc", "whole-series err", "max dyadic-window err"]
+    # <A(t)> under L2 + L4 (RK4 at the sampled times, stride 8 dt) for the first subset
+    # instance of each dimension
+    expect = {}
+    for d in sorted(set(int(dims[b]) for b in ref_ids)):
+        b = next(x for x in ref_ids if dims[x] == d)
+        s = systems[b]
+        L2 = tb.tcl2_generator_series(s, gammas[b], tids[b])
+        U = s.U
+        rho0 = np.zeros((d, d), np.complex128)
+        rho0[0, 0] = 1.0
+        r0 = torch.from_numpy((U.conj().T @ rho0 @ U).reshape(-1, order="F")).cuda()
+        ob = torch.from_numpy((U.conj().T @ As[b] @ U).T.reshape(-1, order="F")).cuda()
+        tr = {}
+        for name, L4 in (("fp32", res32[b]), ("fp64", res64[b])):
+            _, _, o = tb.propagate_rk4_dense(L2, r0, dts[b] * 8, L_add=L4, sample_every=16, obs=ob)
+            tr[name] = o.real.cpu().numpy()
+        expect[str(d)] = {"instance": b, "rel_err": float(np.linalg.norm(tr["fp32"] - tr["fp64"]) / np.linalg.norm(tr["fp64"]))}
+        del L2
+    out["expect_A_fp32_rel_err_vs_fp64"] = expect
     if cpu_leg:
-        # the oracle on the smallest instance of each dimension: F/C/R over the first 2049
-        # steps, L4 at four of the sampled times in that window
+        # the oracle on the smallest subset instance of each dimension: F/C/R over the first
+        # 2049 steps, L4 at four of the sampled times in that window
         import oracle
         chk = {}
-        for d in sorted(set(dims.tolist())):
-            b = min((k for k in range(B) if dims[k] == d), key=lambda k: Ns[k])
+        for d in sorted(set(int(dims[b]) for b in ref_ids)):
+            b = min((k for k in ref_ids if dims[k] == d), key=lambda k: Ns[k])
             s = systems[b]
             pos = [16, 64, 128, 256]
             Gh = np.ascontiguousarray(gammas[b][:, :2049].cpu().numpy())
             p2f = np.ascontiguousarray(s.pair_to_freq.T, np.int32)
             ops = np.ascontiguousarray(np.stack([Ae.T for Ae in s.A_eig]))
             ref = oracle.tcl4_build_batch(s.N, s.nf, s.omegas, s.mirror, p2f, ops, Gh, dts[b], tidx=tids[b][pos])
-            g64 = res["fp64"][b][pos].cpu().numpy()
-            g32 = res["fp32"][b][pos].cpu().numpy()
+            g64 = res64[b][pos].cpu().numpy()
+            g32 = res32[b][pos].cpu().numpy()
             chk[str(d)] = {"instance": int(b), "times": tids[b][pos].tolist(),
                            "fp64_rel_err": float(np.linalg.norm(g64 - ref) / np.linalg.norm(ref)),
                            "fp32_rel_err": float(np.linalg.norm(g32 - ref) / np.linalg.norm(ref))}
         out["oracle_check"] = chk
-    del res
+    plan64.close()
+    del res32, res64
     torch.cuda.empty_cache()
     return out
 
@@ -456,6 +551,54 @@ def differentiation(args, rank, world, cpu_leg):
     return out
 
 
+def c2_rk4_leg(args, systems, gammas, outs32, outs64, tidx):
+    """The config's RK4 leg: rho(t) over all tmax steps under L = L2(t) + L4(t) on the device
+    (FP64 state), one call per trajectory, with the FP32 form's and the FP64 path's L4;
+    <sz(t)> in the lab frame sampled every 10 steps."""
+    import torch
+    import taco_b200 as tb
+    P = min(args.rk4_instances, len(outs64))
+    if P <= 0:
+        return None
+    T = tidx.size
+    times, errs = [], []
+    with tb.profile() as prof:
+        for k in range(P):
+            s, g = systems[k], gammas[k]
+            L2 = tb.tcl2_generator_series(s, g, tidx)
+            U = s.U
+            rho0 = np.zeros((2, 2), np.complex128)
+            rho0[0, 0] = 1.0
+            r0 = torch.from_numpy((U.conj().T @ rho0 @ U).reshape(-1, order="F")).cuda()
+            ob = torch.from_numpy((U.conj().T @ SZ @ U).T.reshape(-1, order="F")).cuda()
+            traj = {}
+            for name, L4 in (("fp32", outs32[k]), ("fp64", outs64[k])):
+                L4v = L4.view(T, 4, 4).transpose(1, 2).to(torch.complex128)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                _, _, o = tb.propagate_rk4_dense(L2, r0, args.dt, L_add=L4v, sample_every=10, obs=ob)
+                e1.record()
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+                traj[name] = o.real.cpu().numpy()
+            errs.append(float(np.linalg.norm(traj["fp32"] - traj["fp64"]) / np.linalg.norm(traj["fp64"])))
+    steps = T - 1
+    ms = statistics.median(times)
+    rk4 = {}
+    for name, (n, tot) in prof.entries.items():
+        rk4[name] = {"launches": n, "total_ms": round(tot, 4)}
+    # bytes of the step-matrix scheme per trajectory: L2 and L4 series (FP64 after the add)
+    # read once to form the step matrices, the matrices written and read by the chain
+    D2 = 16 * 16
+    bytes_traj = (steps + 1) * D2 * 2 + 2 * steps * D2
+    return {"trajectories": P, "steps": steps, "ms_per_trajectory": ms,
+            "trajectories_per_s": 1e3 / ms, "gbs_per_trajectory_call": round(bytes_traj / (ms / 1e3) / 1e9, 2),
+            "expect_sz_fp32_rel_err_vs_fp64_max": max(errs), "kernels": rk4,
+            "note": "latency-bound (one matrix-vector product per sequential step); bytes: L2+L4 series "
+                    "read once, step matrices written and read once"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -496,8 +639,10 @@ def main():
     inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
     torch.cuda.synchronize()
 
-    # ---- headline: the batching form, prepared once and replayed as one CUDA graph ----
+    # ---- headline: the batching form (FP32 pass + precision guard), prepared once and
+    # replayed as one CUDA graph ----
     plan32 = tb.Tcl4Plan(inst, precision="fp32", outs=outs32)
+    guard = dict(tb.fp32_guard_stats(), tolerance=tb.fp32_guard())
     for _ in range(args.warmup):
         plan32.run()
     torch.cuda.synchronize()
@@ -518,35 +663,54 @@ def main():
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
     value = workloads.aggregate_rate(world, B * T, ms)
 
+    # the FP32 pass alone (guard off), for the guard's share of the step
+    tb.set_fp32_guard(0.0)
+    outs32r = [torch.empty_like(o) for o in outs32]
+    plan32r = tb.Tcl4Plan(inst, precision="fp32", outs=outs32r)
+    tb.set_fp32_guard(guard["tolerance"])
+    ms_pass = max_over_ranks(timed(torch, plan32r.run, 5))
+    plan32r.close()
+    del outs32r
+
     # per-kernel device time of one more step (the same launches, not graph-captured)
     with tb.profile() as prof:
         tb.build_instances(inst, precision="fp32", outs=outs32)
     direct32_ms = max_over_ranks(timed(torch, lambda: tb.build_instances(inst, precision="fp32", outs=outs32), 2))
+    plan32.run()
 
     # ---- plain FP64 path: one instance per call (replayed plan, and the direct call) ----
     P = min(args.plain_instances, B)
-    outs64 = [torch.empty((T, N2 * N2), dtype=torch.complex128, device=device) for _ in range(P)]
+    Pe = min(max(args.err_instances, P), B)
+    outs64 = [torch.empty((T, N2 * N2), dtype=torch.complex128, device=device) for _ in range(Pe)]
     plans64 = [tb.Tcl4Plan([inst[k]], precision="fp64", outs=[outs64[k]]) for k in range(P)]
     ms64 = max_over_ranks(timed(torch, lambda: [p.run() for p in plans64], 3) / P)
     ms64_direct = max_over_ranks(timed(torch, lambda: [tb.build_TCL4_generator_batch(
         systems[k], gammas[k], args.dt, tidx, precision="fp64", out=outs64[k]) for k in range(P)], 2) / P)
     plain_value = T / (ms64 / 1e3)
-    err32 = max(float(torch.linalg.vector_norm(outs32[k].to(torch.complex128) - outs64[k])
-                      / torch.linalg.vector_norm(outs64[k])) for k in range(P))
+    # FP32 form against FP64 on Pe instances: whole series and every dyadic window
+    tb.build_instances(inst[P:Pe], precision="fp64", outs=outs64[P:Pe])
+    torch.cuda.synchronize()
+    errs_g, errs_w = [], []
+    for k in range(Pe):
+        a = outs32[k].to(torch.complex128).cpu().numpy()
+        b = outs64[k].cpu().numpy()
+        errs_g.append(float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+        errs_w.append(max(e for _, e in window_errors(a, b, tidx)))
+    err32 = max(errs_g)
 
     # ---- the same work with the reference's FFT length (2^19 from Nt), labelled separately ----
     Bf = min(B, 64)
     outs32f = [torch.empty((T, N2 * N2), dtype=torch.complex64, device=device) for _ in range(Bf)]
     plan32f = tb.Tcl4Plan(inst[:Bf], precision="fp32", outs=outs32f, full_length=True)
     ms_full = max_over_ranks(timed(torch, plan32f.run, 2))
-    plan64f = tb.Tcl4Plan([inst[0]], precision="fp64", outs=[outs64[0]], full_length=True)
+    outs64f = torch.empty((T, N2 * N2), dtype=torch.complex128, device=device)
+    plan64f = tb.Tcl4Plan([inst[0]], precision="fp64", outs=[outs64f], full_length=True)
     ms64_full = max_over_ranks(timed(torch, plan64f.run, 3))
     torch.cuda.synchronize()
     full_err = float(torch.linalg.vector_norm(outs32f[0].to(torch.complex128) - outs64[0])
                      / torch.linalg.vector_norm(outs64[0]))
-    for p in plans64:
-        p.run()  # restore the truncated-path result in outs64 for the parity checks below
-    torch.cuda.synchronize()
+    del outs32f
+    plan32f.close()
 
     # ---- end to end through the C-ABI with pinned host buffers (H2D of Gamma, D2H of L4) ----
     host_g = [g.cpu().pin_memory() for g in gammas]
@@ -555,32 +719,38 @@ def main():
     outs_h = [o.numpy() for o in host_out]
     tb.build_instances(inst_h, precision="fp32", outs=outs_h)
     barrier()
-    t0 = time.perf_counter()
+    e2e_times = []
     for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
         tb.build_instances(inst_h, precision="fp32", outs=outs_h)
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.e2e_steps)
+        e2e_times.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(sum(e2e_times) / len(e2e_times))
     h2d = sum(g.shape[0] * T * 16 for g in gammas)  # the consumed samples t <= tmax of every bucket
     d2h = B * T * N2 * N2 * 8
     e2e_value = world * B * T / (e2e_ms / 1e3)
     err_e2e = float(np.abs(outs_h[0] - outs32[0].cpu().numpy()).max())
 
-    # ---- roofline of the dominant kernel ----
+    # ---- roofline of the dominant kernel (FP32 pass kernels: the byte model's shapes) ----
     peaks, peak_kind = measured_peaks()
     nfft = tb.fft_length(T, "fp32")[0]  # causal rule: 2 (tmax+1) - 1 rounded up to 2^k, 3*2^k or 5*2^k
-    shape = (T, nfft, T, T, 3)
-    units_total = {"triple": B * 27, "spectrum": B * 6}
+    shape = (T, nfft, T, T, 3, 16)
+    units_total = {"triple": B * 27, "spectrum": B * 6, "instance": B}
     tot_all = sum(v[1] for v in prof.entries.values()) or 1.0
     kernels = {}
     for name, (n, tot) in prof.entries.items():
-        per_unit, unit = kernel_model_bytes(name, shape)
+        per_unit, unit = kernel_model_bytes(name, shape) if name.endswith("f32") else (None, None)
         ent = {"launches": n, "total_ms": round(tot, 4), "share": round(tot / tot_all, 4)}
         if per_unit:
-            ent["gbs"] = round(per_unit * units_total[unit] / (tot / 1e3) / 1e9, 1)
+            gbs = per_unit * units_total[unit] / (tot / 1e3) / 1e9
+            ent["gbs"] = round(gbs, 1)
+            ent["frac_of_measured_hbm"] = round(gbs / peaks["hbm_gbs"], 4)
+        elif name.endswith("f64"):
+            ent["note"] = "FP64 head of the precision guard"
         kernels[name] = ent
     roofline = None
     ranked = sorted(prof.entries.items(), key=lambda kv: -kv[1][1])
     for name, (n, tot) in ranked:
-        per_unit, unit = kernel_model_bytes(name, shape)
+        per_unit, unit = kernel_model_bytes(name, shape) if name.endswith("f32") else (None, None)
         if not per_unit:
             continue
         per_launch = per_unit * units_total[unit] / n
@@ -617,40 +787,71 @@ def main():
             return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
         fp64_parity = {"vs_oracle_convolution": re(g64, L4o), "vs_oracle_direct": re(g64, L4d),
-                       "oracle_convolution_vs_direct": re(L4o, L4d), "fp32_vs_oracle_direct": re(g32, L4d)}
+                       "oracle_convolution_vs_direct": re(L4o, L4d), "fp32_vs_oracle_direct": re(g32, L4d),
+                       "fp32_vs_oracle_direct_windows_max": max(e for _, e in window_errors(
+                           g32.reshape(T, -1), L4d.reshape(T, -1), tidx))}
 
     # the other forms and configurations: one GPU only (the scaling runs time the headline)
     cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
     single = world == 1
-    grad = differentiation(args, rank, world, cpu_leg) if single and args.grad_instances > 0 else None
-    c3 = [precision_random(args, int(d), cpu_leg) for d in args.c3_dims.split(",") if d.strip()] if single else None
-    c4 = heterogeneous_batch(args, rank, world, cpu_leg) if single and args.c4_instances > 0 else None
+    def section(fn, *a):
+        # a secondary section that fails reports its error instead of losing the headline line
+        t0s = time.perf_counter()
+        try:
+            res = fn(*a)
+            if isinstance(res, dict):
+                res["section_seconds"] = round(time.perf_counter() - t0s, 1)
+            return res
+        except Exception as exc:  # noqa: BLE001
+            import traceback
+            traceback.print_exc()
+            try:
+                tb.release_workspace()
+                torch.cuda.empty_cache()
+            except Exception:  # noqa: BLE001
+                pass
+            return {"error": f"{type(exc).__name__}: {exc}"}
+
+    rk4 = section(c2_rk4_leg, args, systems, gammas, outs32, outs64, tidx) if single else None
+    grad = section(differentiation, args, rank, world, cpu_leg) if single and args.grad_instances > 0 else None
+    c3 = ([section(precision_random, args, int(d), cpu_leg) for d in args.c3_dims.split(",") if d.strip()]
+          if single else None)
+    c4 = section(heterogeneous_batch, args, rank, world, cpu_leg) if single and args.c4_instances > 0 else None
 
     if rank == 0:
+        full_plain = T / (ms64_full / 1e3)
         line = {
             "metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{B} spin-boson instances per GPU (d=2, nf=3), N={args.N} (Nt={args.N + 1}), "
-                                   f"dt={args.dt}, tidx 0..{args.tmax}, batched FP32 form, one CUDA-graph replay "
-                                   f"per step, FFT length {nfft} from max(tidx)+1",
-                       "instances_per_gpu": B, "builds_per_instance": T,
-                       "l2": "inputs larger than L2 (Gamma 9.6 MB x instances; L4 outputs 1.3 MB x instances)",
-                       "parallelism": f"instance-sharded x{world}"},
-            "plain_fp64": {"value": plain_value, "unit": "builds/s", "ms_per_instance": ms64,
-                           "ms_per_instance_direct_call": ms64_direct, "instances": P},
+            "config": headline_config(args, world),
             "speedup_vs_plain_fp64": value / (world * plain_value),
             "fp32_rel_err_vs_fp64": err32,
+            "fp32_window_rel_err_max": max(errs_w),
+            "like_for_like": {"plain_fp64_full_length_builds_per_s": full_plain,
+                              "vs_cpu_reference": (full_plain / cpu["value"]) if cpu else None,
+                              "note": "one instance, FP64, FFT 2^19 from Nt: the reference's precision and "
+                                      "algorithm length on the GPU against the CPU restatement"},
+            "step": {"fft_length": nfft, "fp32_pass_ms": ms_pass, "guard_ms": ms - ms_pass,
+                     "note": "one step = the FP32 pass over all instances, then the precision guard's "
+                             "FP64 heads and row patch (heads chosen at plan creation)"},
+            "precision_guard": guard,
+            "plain_fp64": {"value": plain_value, "unit": "builds/s", "ms_per_instance": ms64,
+                           "ms_per_instance_direct_call": ms64_direct, "instances": P},
+            "fp32_errors": {"instances": Pe, "whole_series_max": err32, "dyadic_windows_max": max(errs_w),
+                            "whole_series": [round(e, 10) for e in errs_g]},
             "fp64_parity": fp64_parity,
             "direct_call_ms_per_step": direct32_ms,
             "full_length_fft": {"note": "FFT length 2^19 from Nt as the reference; same results",
                                 "value": world * Bf * T / (ms_full / 1e3), "instances": Bf, "ms_per_step": ms_full,
-                                "plain_fp64_value": T / (ms64_full / 1e3),
-                                "speedup_vs_plain_fp64": (Bf * T / (ms_full / 1e3)) / (T / (ms64_full / 1e3)),
+                                "plain_fp64_value": full_plain,
+                                "speedup_vs_plain_fp64": (Bf * T / (ms_full / 1e3)) / full_plain,
                                 "fp32_rel_err_vs_fp64": full_err},
             "e2e": {"value": e2e_value, "unit": "builds/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_ms, "max_abs_diff_vs_device_run": err_e2e},
+                    "ms_per_step": e2e_ms, "steps": len(e2e_times), "ms_min": min(e2e_times),
+                    "max_abs_diff_vs_device_run": err_e2e},
             "roofline": roofline, "kernels": kernels,
+            "rk4_c2": rk4,
             "differentiation": grad,
             "precision_random": c3,
             "heterogeneous_batch": c4,
@@ -659,7 +860,7 @@ def main():
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
-    for p in [plan32, plan32f, plan64f, *plans64]:
+    for p in [plan32, plan64f, *plans64]:
         p.close()
     if dist is not None:
         dist.barrier()

@@ -164,13 +164,16 @@ int taco_tcl4_plan_destroy(taco_tcl4_plan* plan);
  * cudaMalloc, cudaFree or other allocating routine: all scratch comes from one fixed device
  * array of TACO_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until the
  * process exits.  gamma ([Nt x nf] column-major) and L4_out ([T][N^2 x N^2]: complex128 for
- * TACO_PREC_FP64, complex64 for TACO_PREC_FP32) are device pointers; tidx is a host array
- * (NULL/T = 0: all Nt).  The FFT length follows max(tidx)+1.  A request whose scratch would
+ * TACO_PREC_FP64, complex64 for TACO_PREC_FP32) must be device (or managed) memory of the
+ * current device, aligned for their complex type; anything else fails with
+ * TACO_ERR_INVALID_ARGUMENT before any launch.  tidx is a host array (NULL/T = 0: all Nt).
+ * The FFT length is a power of two following max(tidx)+1.  A request whose scratch would
  * exceed the fixed size fails with TACO_ERR_OVERFLOW and a message stating the need.  The
  * first call on a device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current: make it before any stream capture.  All calls share the array, so
- * calls that overlap on the GPU (other threads or streams) race; the call synchronises
- * `stream` (NULL: the legacy default stream) before returning. */
+ * that device current.  All calls share the array, so calls that overlap on the GPU (other
+ * threads or streams) race.  The call copies its metadata from pageable host memory and
+ * synchronises `stream` (NULL: the legacy default stream) before returning; on a stream
+ * that is being captured it fails with TACO_ERR_INVALID_ARGUMENT before any work. */
 #define TACO_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
 int taco_tcl4_build_batch_noalloc(const taco_system_view* sys, const taco_c128* gamma, size_t Nt, double dt,
                                   const uint32_t* tidx, size_t T, int precision, void* L4_out, void* stream);
@@ -237,6 +240,30 @@ int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t*
  * memory at the call, at most 64 GiB).  Instances that need more are built in slices of
  * their frequency triples (same results, more passes over the output). */
 int taco_set_work_budget(size_t bytes);
+/* No counterpart in the reference.  Precision guard of the FP32 form (TACO_PREC_FP32 builds
+ * and plans): after the FP32 build, a head of each instance's leading times [0, H) is built
+ * in FP64 (H = max(512, t_count/16) first, t_count = max(tidx)+1) and compared with the
+ * FP32 result on [H/2, H); within `tol` (relative Frobenius) the FP64 head replaces those
+ * FP32 rows, otherwise H grows fourfold, up to a full FP64 build of the instance.  Plans
+ * choose their heads once, at creation.  tol = 0 turns the guard off; the default is 5e-7.
+ * taco_get_fp32_guard returns the current value. */
+/* No counterpart in the reference.  The fused F/C/R path: for FFT lengths whose working
+ * array fits one CTA's shared memory (FP32 up to 24576 points, FP64 up to 12288), one CTA per
+ * (triple, half) runs the forward transform, the spectral product, the inverse transform, the
+ * prefix integrals and the assembly in shared memory.  on = 0 selects the four-step passes
+ * and the scan kernels for every length (the default is on; results agree to rounding). */
+int taco_set_fused_conv(int on);
+/* No counterpart in the reference (whose thread_local workspace is freed at thread exit,
+ * cpp/src/backend/cuda/tcl4_fused_cuda.cu:676-685).  Frees the calling thread's grow-only
+ * device and pinned transient buffers on the current device after its streams finish; the
+ * next call allocates them again.  Plans keep their own buffers. */
+int taco_release_workspace(void);
+int taco_set_fp32_guard(double tol);
+int taco_get_fp32_guard(double* tol);
+/* What the guard did in the calling thread's last FP32 build or plan creation, six counts:
+ * instances of the call, instances with an FP64 head, requested times rebuilt in FP64,
+ * requested times of those instances, instances rebuilt in FP64 entirely, growth rounds. */
+int taco_fp32_guard_stats(uint64_t* counts6);
 /* FFT length the build uses for n_in consumed samples (flags: TACO_FULL_LENGTH_FFT selects
  * the reference's power-of-two rule), and its schedule key for taco_set_tuning: log2 of a
  * power of two, + 64 for 3 * 2^k, + 128 for 5 * 2^k. */
@@ -247,6 +274,10 @@ int taco_fft_length(size_t n_in, int precision, int flags, size_t* nfft, int* ke
  * chunk of triples, and the largest number of output rows for which the inverse column pass
  * is a pruned direct DFT.  Unset lengths use the defaults (4096, 2048, 48 MiB, 16). */
 int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows);
+/* No counterpart in the reference.  Whether the causal rule may pick the mixed length of
+ * schedule key `key` (64 + k: 3 * 2^k, 128 + k: 5 * 2^k) for `precision`; the autotuner turns
+ * off a mixed length that it measured slower than the next longer one (default: enabled). */
+int taco_set_fft_length_enabled(int key, int precision, int enabled);
 int taco_get_tuning(int log2_nfft, int precision, int* col_tile, int* row_tile, size_t* chunk_bytes,
                     int* inv_dft_rows);
 /* Points per CTA of the thread-block-cluster convolution path for FFT length 2^log2_nfft:

@@ -4,11 +4,15 @@ Builds `--instances` C2-shaped spin-boson instances (N=200000, dt=5e-4, tidx 0..
 on the device and runs the batched build `--reps` times through the direct API (no CUDA
 graph, so every kernel is a separate launch a profiler can select).
 
-    python -m taco_b200.profile_case --instances 8 --precision fp32 --reps 2
+    python profile_case.py --instances 8 --precision fp32 --reps 2
+
+--guard sets the FP32 form's precision-guard tolerance (0: off, the FP32 pass alone).
 """
 from __future__ import annotations
 
 import argparse
+import os
+import sys
 import time
 
 import numpy as np
@@ -23,7 +27,9 @@ def main():
     ap.add_argument("--dt", type=float, default=5e-4)
     ap.add_argument("--tmax", type=int, default=10000)
     ap.add_argument("--full-length", action="store_true")
+    ap.add_argument("--guard", type=float, default=None)
     args = ap.parse_args()
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
     import torch
 
@@ -33,6 +39,8 @@ def main():
     _, systems, gammas = spin_boson_batch(torch, args.instances, args.N, args.dt, seed=7)
     tidx = np.arange(args.tmax + 1, dtype=np.uint32)
     inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
+    if args.guard is not None:
+        tb.set_fp32_guard(args.guard)
     torch.cuda.synchronize()
     for _ in range(args.reps):
         t0 = time.perf_counter()

@@ -95,6 +95,41 @@ def set_work_budget(nbytes: int) -> None:
     _capi.check(_capi.lib().taco_set_work_budget(int(nbytes)))
 
 
+def set_fp32_guard(tol: float) -> None:
+    """Precision guard of the FP32 form: leading times whose FP32 result differs from an FP64
+    head by more than `tol` (relative, on the head's upper half) are rebuilt in FP64, the
+    head growing fourfold up to the whole instance.  0 turns it off; default 5e-7."""
+    _capi.check(_capi.lib().taco_set_fp32_guard(float(tol)))
+
+
+def fp32_guard() -> float:
+    """The current tolerance of the FP32 form's precision guard (0: off)."""
+    v = ct.c_double(0.0)
+    _capi.check(_capi.lib().taco_get_fp32_guard(ct.byref(v)))
+    return v.value
+
+
+def set_fused_conv(on: bool) -> None:
+    """The fused F/C/R path (transforms, scans and assembly of a triple in one CTA's shared
+    memory) for the FFT lengths it fits (default on); off: the four-step passes everywhere."""
+    _capi.check(_capi.lib().taco_set_fused_conv(1 if on else 0))
+
+
+def release_workspace() -> None:
+    """Free this thread's grow-only device and pinned transient buffers (after its streams
+    finish); the next build allocates them again.  Plans keep their own."""
+    _capi.check(_capi.lib().taco_release_workspace())
+
+
+def fp32_guard_stats() -> dict:
+    """What the precision guard did in this thread's last FP32 build or plan creation."""
+    v = (ct.c_uint64 * 6)()
+    _capi.check(_capi.lib().taco_fp32_guard_stats(v))
+    keys = ("instances", "instances_with_fp64_head", "fp64_head_rows", "rows_of_those_instances",
+            "instances_fully_fp64", "rounds")
+    return dict(zip(keys, (int(x) for x in v)))
+
+
 def fft_length(n_in: int, precision: str = "fp32", full_length: bool = False):
     """(Nfft, schedule key) the build uses for n_in consumed Gamma samples."""
     n = ct.c_size_t(0)

@@ -39,7 +39,9 @@ EXPORTED = [
     "taco_build_mikx", "taco_assemble_liouvillian", "taco_gw_to_liouvillian",
     "taco_bcf_fft", "taco_rk4_forward_checkpointed", "taco_rk4_adjoint", "taco_tcl4_adjoint",
     "taco_tcl2_adjoint", "taco_inner_re", "taco_set_work_budget", "taco_gamma_trapz_batch",
-    "taco_fft_length", "taco_compute_triple_kernels_batch",
+    "taco_fft_length", "taco_compute_triple_kernels_batch", "taco_set_fp32_guard", "taco_get_fp32_guard",
+    "taco_fp32_guard_stats", "taco_set_fused_conv",
+    "taco_release_workspace", "taco_set_fft_length_enabled",
 ]
 
 
@@ -177,6 +179,12 @@ def lib():
                                                 ct.c_void_p]
         L.taco_gw_to_liouvillian.argtypes = [ct.c_void_p, ct.c_int, ct.c_size_t, ct.c_void_p, ct.c_int, ct.c_void_p]
         L.taco_set_work_budget.argtypes = [ct.c_size_t]
+        L.taco_set_fp32_guard.argtypes = [ct.c_double]
+        L.taco_get_fp32_guard.argtypes = [ct.POINTER(ct.c_double)]
+        L.taco_fp32_guard_stats.argtypes = [ct.POINTER(ct.c_uint64)]
+        L.taco_set_fused_conv.argtypes = [ct.c_int]
+        L.taco_release_workspace.argtypes = []
+        L.taco_set_fft_length_enabled.argtypes = [ct.c_int, ct.c_int, ct.c_int]
         L.taco_fft_length.argtypes = [ct.c_size_t, ct.c_int, ct.c_int, ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_int)]
         L.taco_gamma_trapz_batch.argtypes = [ct.POINTER(GammaRequest), ct.c_size_t, ct.c_void_p]
         L.taco_bcf_fft.argtypes = [ct.POINTER(BcfRequest), ct.c_size_t, ct.c_int, ct.c_void_p]

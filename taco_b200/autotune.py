@@ -1,13 +1,19 @@
-"""Autotuner for the F/C/R launch schedules.
+"""Autotuner for the F/C/R launch schedules and FFT lengths.
 
-For one FFT length and precision it times the batched build of a representative
+Tiles: for one FFT length and precision it times the batched build of a representative
 workload under each candidate schedule (column tile, row tile, Z/W chunk bytes, pruned
-inverse-DFT rows), with CUDA events after warm-up, and keeps the fastest.  Results are
-persisted as JSON ({"<key>:<fp32|fp64>": {...}}) and applied with load(); the key of an
-FFT length is log2 for powers of two, + 64 for 3 * 2^k and + 128 for 5 * 2^k
-(taco_b200.fft_length).
+inverse-DFT rows), with CUDA events after warm-up, and keeps the fastest.
+Radix: for a requested length the causal rule may use 2^k, 3 * 2^k or 5 * 2^k; the tuner
+times the workload with each admissible length and turns off ("enabled": false) the mixed
+lengths that lose to a longer one.
+Results are persisted as JSON ({"<key>:<fp32|fp64>": {...}}) and applied with load(); the key
+of an FFT length is log2 for powers of two, + 64 for 3 * 2^k and + 128 for 5 * 2^k
+(taco_b200.fft_length).  Workloads: "c2" (spin-boson batch of the headline shape: the radix
+choice for t_max = 10000 and the tiles of its lengths) and "c4" (batching-form lengths
+2^15..2^19: spin-boson instances with Nt = 2^(L-1) and every 8th time).  The FP32 form is
+tuned with its precision guard off (the guard's FP64 heads are tuned as FP64 lengths).
 
-    python -m taco_b200.autotune --out taco_b200/tuning.json   (needs a GPU)
+    python -m taco_b200.autotune --workloads c2,c4 --out taco_b200/tuning.json   (needs a GPU)
 """
 from __future__ import annotations
 
@@ -37,6 +43,15 @@ def get_schedule(log2_nfft: int, precision: str) -> dict:
     return {"col_tile": c.value, "row_tile": r.value, "chunk_bytes": b.value, "inv_dft_rows": d.value}
 
 
+def set_length_enabled(key: int, precision: str, enabled: bool) -> None:
+    prec = _capi.TACO_PREC_FP32 if precision == "fp32" else _capi.TACO_PREC_FP64
+    _capi.check(_capi.lib().taco_set_fft_length_enabled(int(key), prec, 1 if enabled else 0))
+
+
+def length_of(key: int) -> int:
+    return (3 if 64 <= key < 128 else 5 if key >= 128 else 1) << (key & 63)
+
+
 def load(path: str = DEFAULT_TABLE) -> int:
     """Apply a persisted table; returns the number of schedules applied (0 if absent)."""
     if not os.path.exists(path):
@@ -48,8 +63,11 @@ def load(path: str = DEFAULT_TABLE) -> int:
         if key.startswith("_"):
             continue
         L, prec = key.split(":")
-        set_schedule(int(L), prec, sch["col_tile"], sch["row_tile"], sch["chunk_bytes"], sch["inv_dft_rows"],
-                     sch.get("cluster_lm", 0))
+        if "col_tile" in sch:
+            set_schedule(int(L), prec, sch["col_tile"], sch["row_tile"], sch["chunk_bytes"], sch["inv_dft_rows"],
+                         sch.get("cluster_lm", 0))
+        if int(L) >= 64 and "enabled" in sch:
+            set_length_enabled(int(L), prec, bool(sch["enabled"]))
         n += 1
     return n
 
@@ -151,6 +169,26 @@ class _Plans:
             p.close()
 
 
+def mixed_keys(n: int):
+    """Schedule keys of the 3 * 2^k and 5 * 2^k lengths the causal rule could pick for n samples."""
+    target = 2 * n - 1
+    p2 = 1 << max(3, (target - 1).bit_length())
+    keys = []
+    for base, r in ((64, 3), (128, 5)):
+        k = 3
+        while (r << k) < target:
+            k += 1
+        if (r << k) < p2:
+            keys.append(base + k)
+    return keys
+
+
+def small_candidates(precision: str):
+    cols = [2048, 4096] if precision == "fp32" else [2048, 4096]
+    return [dict(col_tile=c, row_tile=r, chunk_bytes=b, inv_dft_rows=d)
+            for c, r, b, d in itertools.product(cols, [1024, 2048], [48 << 20, 1 << 30], [0, 16])]
+
+
 def main():
     import argparse
 
@@ -167,32 +205,84 @@ def main():
     ap.add_argument("--dt", type=float, default=5e-4)
     ap.add_argument("--tmax", type=int, default=10000)
     ap.add_argument("--precisions", default="fp32,fp64")
+    ap.add_argument("--workloads", default="c2,c4")
+    ap.add_argument("--c4-lengths", default="15,16,17,18,19")
     args = ap.parse_args()
-    _, systems, gammas = spin_boson_batch(torch, args.instances, args.N, args.dt, seed=123)
-    tidx = np.arange(args.tmax + 1, dtype=np.uint32)
-    T = tidx.size
+    load(args.out)
+    guard = tb.fp32_guard()
+    tb.set_fp32_guard(0.0)
     entries = {}
-    for full in (False, True):
-        # FFT length: next_pow2(2 n - 1) with n = tmax + 1 (default) or Nt (full length)
-        n = (args.N + 1) if full else T
-        for prec in args.precisions.split(","):
-            nfft, L = tb.fft_length(n, prec, full_length=full)  # L: the schedule key of this length
-            dtype = torch.complex64 if prec == "fp32" else torch.complex128
-            outs = [torch.empty((T, 16), dtype=dtype, device="cuda") for _ in systems]
-            inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
-            if prec == "fp64":  # the plain path: one instance per plan
-                def factory():
-                    return _Plans([tb.Tcl4Plan([inst[k]], precision="fp64", outs=[outs[k]], full_length=full)
-                                   for k in range(min(4, len(inst)))])
-            else:  # the batched path: one plan over every instance
-                def factory():
-                    return _Plans([tb.Tcl4Plan(inst, precision=prec, outs=outs, full_length=full)])
-            def same_length(n=n, prec=prec, full=full, nfft=nfft):
-                return tb.fft_length(n, prec, full_length=full)[0] == nfft
 
-            best, res = tune(None, L, prec, log=print, factory=factory, check=same_length)
-            entries[f"{L}:{prec}"] = dict(best, ms=res[0][0])
-    save(entries, args.out, note="measured on B200 by taco_b200.autotune (C2-shaped spin-boson batch)")
+    def unit_factory(inst, prec, outs, full=False):
+        if prec == "fp64":  # the plain path: one instance per plan
+            return lambda: _Plans([tb.Tcl4Plan([inst[k]], precision="fp64", outs=[outs[k]], full_length=full)
+                                   for k in range(min(4, len(inst)))])
+        return lambda: _Plans([tb.Tcl4Plan(inst, precision=prec, outs=outs, full_length=full)])
+
+    def time_unit(factory, reps=3):
+        unit = factory()
+        try:
+            unit()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                unit()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+        finally:
+            unit.close()
+
+    def tune_tiles(inst, tidx, n, prec, full=False, cands=None):
+        nfft, L = tb.fft_length(n, prec, full_length=full)
+        dtype = torch.complex64 if prec == "fp32" else torch.complex128
+        outs = [torch.empty((tidx.size, 16), dtype=dtype, device="cuda") for _ in inst]
+
+        def same_length(n=n, prec=prec, full=full, nfft=nfft):
+            return tb.fft_length(n, prec, full_length=full)[0] == nfft
+
+        best, res = tune(None, L, prec, cands=cands, log=print, factory=unit_factory(inst, prec, outs, full),
+                         check=same_length)
+        entries[f"{L}:{prec}"] = dict(entries.get(f"{L}:{prec}", {}), **best, ms=res[0][0])
+
+    if "c2" in args.workloads:
+        _, systems, gammas = spin_boson_batch(torch, args.instances, args.N, args.dt, seed=123)
+        tidx = np.arange(args.tmax + 1, dtype=np.uint32)
+        inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
+        n = tidx.size
+        for prec in args.precisions.split(","):
+            # radix: each admissible length alone, the fastest kept
+            keys = mixed_keys(n)
+            dtype = torch.complex64 if prec == "fp32" else torch.complex128
+            outs = [torch.empty((n, 16), dtype=dtype, device="cuda") for _ in inst]
+            times = {}
+            for choice in keys + [None]:
+                for k in keys:
+                    set_length_enabled(k, prec, k == choice)
+                times[choice] = time_unit(unit_factory(inst, prec, outs))
+                print(f"{prec} length {length_of(choice) if choice else 'pow2'}: {times[choice]:.3f} ms")
+            best = min(times, key=times.get)
+            # the rule picks the shortest enabled length: the shorter ones than the winner go
+            for k in keys:
+                on = best is not None and length_of(k) >= length_of(best)
+                set_length_enabled(k, prec, on)
+                entries[f"{k}:{prec}"] = dict(entries.get(f"{k}:{prec}", {}), enabled=on)
+            tune_tiles(inst, tidx, n, prec)
+            tune_tiles(inst, tidx, args.N + 1, prec, full=True)
+    if "c4" in args.workloads:
+        for L in [int(x) for x in args.c4_lengths.split(",") if x]:
+            Nt = 1 << (L - 1)
+            B = max(2, min(16, (1 << 22) // Nt))
+            _, systems, gammas = spin_boson_batch(torch, B, Nt - 1, 1e-3, seed=400 + L)
+            tidx = np.arange(0, Nt - 1, 8, dtype=np.uint32)
+            inst = [(s, g, 1e-3, tidx) for s, g in zip(systems, gammas)]
+            for prec in args.precisions.split(","):
+                tune_tiles(inst, tidx, int(tidx[-1]) + 1, prec, cands=small_candidates(prec))
+            del gammas
+            torch.cuda.empty_cache()
+    tb.set_fp32_guard(guard)
+    save(entries, args.out, note="measured on B200 by taco_b200.autotune (workloads: " + args.workloads + ")")
     print(json.dumps(entries))
 
 

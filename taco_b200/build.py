@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("TACO_NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = os.environ.get("TACO_HOST_CXX", "g++")
 
-LIB_SOURCES = ["engine.cu", "noalloc.cu", "tcl2.cu", "mikx_gw.cu", "bcf.cu", "adjoint.cu", "capi.cpp", "gw_coef.cpp"]
+LIB_SOURCES = ["engine.cu", "guard.cu", "noalloc.cu", "tcl2.cu", "mikx_gw.cu", "bcf.cu", "adjoint.cu", "capi.cpp", "gw_coef.cpp"]
 
 
 def _native_ext() -> str:
@@ -44,15 +44,25 @@ def _deps():
 
 
 def build_lib(force: bool = False, verbose: bool = False) -> str:
+    """Compile the sources to objects in parallel (one nvcc per source), then link."""
     if not force and not _stale(LIB, _deps()):
         return LIB
-    srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
-    cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-ccbin", HOST_CXX, "-I", INCLUDE, "-I", CSRC, "--expt-relaxed-constexpr",
-           "-o", LIB, *srcs, "-lcudart"]
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(ROOT, "_build", "lib")
+    os.makedirs(objdir, exist_ok=True)
+    common = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX,
+              "-I", INCLUDE, "-I", CSRC, "--expt-relaxed-constexpr"]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+        common.insert(1, "-Xptxas=-v")
+    objs = [os.path.join(objdir, os.path.splitext(s)[0] + ".o") for s in LIB_SOURCES]
+
+    def compile_one(k):
+        subprocess.run([*common, "-c", os.path.join(CSRC, LIB_SOURCES[k]), "-o", objs[k]], check=True)
+
+    with ThreadPoolExecutor(max_workers=min(len(LIB_SOURCES), os.cpu_count() or 1)) as pool:
+        list(pool.map(compile_one, range(len(LIB_SOURCES))))
+    subprocess.run([NVCC, *ARCH, "-shared", "-ccbin", HOST_CXX, "-o", LIB, *objs, "-lcudart"], check=True)
     return LIB
 
 

@@ -43,6 +43,7 @@
 #include "common.cuh"
 #include "engine.hpp"
 #include "gw_coef.hpp"
+#include "fused_conv.cuh"
 
 namespace taco {
 
@@ -1049,6 +1050,132 @@ __global__ void __launch_bounds__(CR_TM) k_fcr_adj_corr(const FcrAdjJob* __restr
     if (threadIdx.x == 0) jb.wpart[static_cast<size_t>(q) * (1 + jb.ntiles) + 1 + blockIdx.x] = ws;
 }
 
+// ---- FFT form of the correlations (lengths whose working array fits one CTA) ----
+// c[m] = sum_{j >= 0} a[j] b[m + j] (m + j < T) is the linear convolution of a with the
+// reversed b, read backwards: c[m] = (a * b_rev)[T - 1 - m], b_rev[n] = b[T - 1 - n].  Every
+// series is transformed once by the fused path's in-place stages (length N >= 2 T - 1, so the
+// circular convolution is the linear one); each of the five outputs (c1 = c1F + c1C summed in
+// the frequency domain, c2F, c2C, c3F, c3C) is one product and one inverse transform.
+struct AdjSpecJob {
+    const double2* src;  // [T]
+    double2* out;        // [N] spectrum (digit-reversed order)
+    uint32_t T;
+    int mode;            // 0: a[n]; 1: conj(a[n]); 2: a[T-1-n]; 3: n a[n]
+};
+
+__global__ void __launch_bounds__(FZ_THREADS, 1) k_adj_series_spectrum(const AdjSpecJob* __restrict__ jobs,
+                                                                       FzPlan<double2> p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* d = reinterpret_cast<double2*>(smem_raw);
+    const AdjSpecJob job = jobs[blockIdx.x];
+    for (int n = threadIdx.x; n < p.N; n += blockDim.x) {
+        double2 x = make_double2(0.0, 0.0);
+        if (static_cast<uint32_t>(n) < job.T) {
+            switch (job.mode) {
+                case 0: x = job.src[n]; break;
+                case 1: x = cconj(job.src[n]); break;
+                case 2: x = job.src[job.T - 1 - n]; break;
+                default: x = cscale(job.src[n], static_cast<double>(n)); break;
+            }
+        }
+        d[pad_idx<double2>(n)] = x;
+    }
+    __syncthreads();
+    fz_forward(d, p);
+    for (int i = threadIdx.x; i < p.N; i += blockDim.x) job.out[i] = d[pad_idx<double2>(i)];
+}
+
+struct AdjFftSpectra {
+    const double2* gconj;  // [nf][N] spectra of conj(Gamma_b)
+    const double2* gplain; // [nf][N] spectra of Gamma_b
+    const double2* fb;     // [nf^3][N] spectra of reversed Fb
+    const double2* cb;     // [nf^3][N] spectra of reversed Cb
+    const double2* a2;     // [nf^3][N] spectra of A2
+    const double2* a3;     // [nf^3][N] spectra of n A2[n]
+};
+
+// blockIdx = (output kind 0..4, triple, job).  kind 0: G1 -= dt Q c1 (c1 = c1F + c1C);
+// 1: G2F -= dt c2F; 2: G2C -= dt c2C; 3, 4: the Bohr-frequency terms of c3F, c3C.
+__global__ void __launch_bounds__(FZ_THREADS, 1) k_fcr_adj_corr_fft(const FcrAdjJob* __restrict__ jobs,
+                                                                    const AdjFftSpectra* __restrict__ specs, int nf,
+                                                                    uint32_t T, double dt, FzPlan<double2> p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* d = reinterpret_cast<double2*>(smem_raw);
+    __shared__ double red[FZ_THREADS / 32];
+    const int kind = blockIdx.x;
+    const uint32_t q = blockIdx.y;
+    const FcrAdjJob jb = jobs[blockIdx.z];
+    if (!jb.fc_used[q]) return;
+    const AdjFftSpectra sp = specs[blockIdx.z];
+    const int nf2 = nf * nf;
+    const int i = static_cast<int>(q / nf2), jj = static_cast<int>((q / nf) % nf), kk = static_cast<int>(q % nf);
+    const int jm = jb.mirror[jj];
+    const std::size_t N = static_cast<std::size_t>(p.N), qn = static_cast<std::size_t>(q) * N;
+    const double inv = 1.0 / static_cast<double>(p.N);
+    for (int n = threadIdx.x; n < p.N; n += blockDim.x) {
+        double2 x;
+        if (kind == 0) {
+            x = cadd(cmul(sp.gconj[static_cast<std::size_t>(jm) * N + n], sp.fb[qn + n]),
+                     cmul(sp.gplain[static_cast<std::size_t>(jj) * N + n], sp.cb[qn + n]));
+        } else {
+            const double2 a = (kind <= 2 ? sp.a2 : sp.a3)[qn + n];
+            x = cmul(a, (kind == 1 || kind == 3) ? sp.fb[qn + n] : sp.cb[qn + n]);
+        }
+        d[pad_idx<double2>(n)] = cscale(x, inv);
+    }
+    __syncthreads();
+    fz_inverse(d, p);
+    const double w = jb.omegas[i] + jb.omegas[jj] + jb.omegas[kk];
+    const double2* g2F = jb.gamma + static_cast<size_t>(jm) * T;
+    const double2* gj = jb.gamma + static_cast<size_t>(jj) * T;
+    const size_t qo = static_cast<size_t>(q) * T;
+    double wv = 0.0;
+    for (uint32_t m = threadIdx.x; m < T; m += blockDim.x) {
+        const double2 c = d[pad_idx<double2>(static_cast<int>(T - 1 - m))];
+        if (kind == 0) {
+            const double2 Q = cconj(phase_m(w, dt, m));
+            jb.G1[qo + m] = csub(jb.G1[qo + m], cscale(cmul(Q, c), dt));
+        } else if (kind == 1) {
+            jb.G2F[qo + m] = csub(jb.G2F[qo + m], cscale(c, dt));
+        } else if (kind == 2) {
+            jb.G2C[qo + m] = csub(jb.G2C[qo + m], cscale(c, dt));
+        } else if (kind == 3) {
+            wv += -dt * dt * cmulc(g2F[m], c).y;
+        } else {
+            wv += -dt * dt * cconj(cmul(gj[m], c)).y;
+        }
+    }
+    if (kind >= 3) {
+        const double ws = block_sum(wv, red);
+        if (threadIdx.x == 0) atomicAdd(&jb.wpart[static_cast<size_t>(q) * (1 + jb.ntiles) + 1], ws);
+    }
+}
+
+__global__ void k_adj_fill_roots(double2* out, uint32_t n) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    double s, c;
+    sincospi(-2.0 * static_cast<double>(m) / static_cast<double>(n), &s, &c);
+    out[m] = make_double2(c, s);
+}
+
+// FFT length of the correlations for T samples: the smallest 2^k, 3 * 2^k or 5 * 2^k >= 2 T - 1
+// whose working array fits one CTA (0: none, the direct kernel runs).
+int adj_fft_length(std::size_t T) {
+    const std::size_t target = 2 * T - 1;
+    std::size_t best = 0;
+    for (std::size_t r : {1, 3, 5}) {
+        std::size_t n = r;
+        while (n < target) n *= 2;
+        if (n < 8) continue;
+        int rad[FZ_MAX_STAGES], nst = 0;
+        if (n > (std::size_t(1) << 16) || !fz_stages(static_cast<int>(n), 8, rad, nst)) continue;
+        if (fz_smem<double2>(static_cast<int>(n)) + 256 > 227 * 1024) continue;  // + the static reduction array
+        if (!best || n < best) best = n;
+    }
+    return static_cast<int>(best);
+}
+
 // Gamma_bar[b][t] += the partials of every triple that reads column b.
 __global__ void k_fcr_adj_reduce(const FcrAdjJob* __restrict__ jobs, int nf, uint32_t T, double2* const* gbar) {
     const FcrAdjJob jb = jobs[blockIdx.z];
@@ -1321,6 +1448,10 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
         const std::size_t nf3 = static_cast<std::size_t>(nf) * nf * nf;
         const auto& idx = g.second;
         const int ntiles = static_cast<int>((T + CR_TM - 1) / CR_TM);
+        // the correlations by FFT when the length fits one CTA and the spectra fit 8 GiB
+        int fftN = adj_fft_length(T);
+        if (fftN && static_cast<double>(idx.size()) * (2 * nf + 4 * nf3) * fftN * sizeof(double2) > 8.0 * (1ull << 30))
+            fftN = 0;
         // per job: coefficient tables (structural), CSC transpose, device metadata
         struct Host {
             CoefTable tab;
@@ -1395,6 +1526,12 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
                 probe.take<double2>(3 * nf3 * T);     // src_bar
                 probe.take<double2>(5 * nf3 * T);     // G1, G2F, G2C, G2R, A2
                 probe.take<double>(nf3 * (1 + ntiles));
+            }
+            if (fftN) {  // roots, per-job spectra, their jobs
+                probe.take<double2>(fftN);
+                for (std::size_t a = 0; a < idx.size(); ++a) probe.take<double2>((2 * nf + 4 * nf3) * fftN);
+                probe.take<AdjFftSpectra>(idx.size());
+                probe.take<AdjSpecJob>(idx.size() * (2 * nf + 4 * nf3));
             }
             bytes = probe.off + 256;
         }
@@ -1474,6 +1611,51 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
             f.ntiles = ntiles;
             gbar[a] = j.gamma_bar;
         }
+        // FFT correlations: spectra of conj(Gamma_b) and Gamma_b per job, and of the reversed
+        // Fb, Cb, A2 and n A2[n] per triple (A2 is written by the scan kernel, which runs first)
+        double2* roots = nullptr;
+        AdjFftSpectra* dspec = nullptr;
+        AdjSpecJob* dsjobs = nullptr;
+        std::size_t nspec_jobs = 0;
+        if (fftN) {
+            roots = cv.take<double2>(fftN);
+            std::vector<AdjFftSpectra> spv(idx.size());
+            std::vector<AdjSpecJob> sjobs;
+            const std::size_t N = static_cast<std::size_t>(fftN);
+            for (std::size_t a = 0; a < idx.size(); ++a) {
+                double2* base = cv.take<double2>((2 * nf + 4 * nf3) * N);
+                AdjFftSpectra& sp = spv[a];
+                sp.gconj = base;
+                sp.gplain = base + nf * N;
+                sp.fb = base + 2 * nf * N;
+                sp.cb = sp.fb + nf3 * N;
+                sp.a2 = sp.cb + nf3 * N;
+                sp.a3 = sp.a2 + nf3 * N;
+                const FcrAdjJob& f = fj[a];
+                const uint32_t TT = static_cast<uint32_t>(T);
+                for (int b = 0; b < nf; ++b) {
+                    sjobs.push_back({f.gamma + static_cast<std::size_t>(b) * T, base + b * N, TT, 1});
+                    sjobs.push_back({f.gamma + static_cast<std::size_t>(b) * T, base + (nf + b) * N, TT, 0});
+                }
+                for (std::size_t q = 0; q < nf3; ++q) {
+                    sjobs.push_back({f.Fb + q * T, const_cast<double2*>(sp.fb) + q * N, TT, 2});
+                    sjobs.push_back({f.Cb + q * T, const_cast<double2*>(sp.cb) + q * N, TT, 2});
+                    sjobs.push_back({f.A2 + q * T, const_cast<double2*>(sp.a2) + q * N, TT, 0});
+                    sjobs.push_back({f.A2 + q * T, const_cast<double2*>(sp.a3) + q * N, TT, 3});
+                }
+            }
+            nspec_jobs = sjobs.size();
+            dspec = cv.take<AdjFftSpectra>(idx.size());
+            dsjobs = cv.take<AdjSpecJob>(nspec_jobs);
+            cuda_check(cudaMemcpyAsync(dspec, spv.data(), spv.size() * sizeof(AdjFftSpectra), cudaMemcpyHostToDevice, st),
+                       "adj fft spectra");
+            cuda_check(cudaMemcpyAsync(dsjobs, sjobs.data(), nspec_jobs * sizeof(AdjSpecJob), cudaMemcpyHostToDevice, st),
+                       "adj fft jobs");
+            // the host vectors above are copy sources: finish before they go out of scope
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(adj fft jobs)");
+            k_adj_fill_roots<<<static_cast<unsigned>((fftN + 255) / 256), 256, 0, st>>>(roots, static_cast<uint32_t>(fftN));
+            launched("k_adj_fill_roots");
+        }
         std::memcpy(image.data() + (reinterpret_cast<char*>(dfj) - cv.base), fj.data(), fj.size() * sizeof(FcrAdjJob));
         std::memcpy(image.data() + (reinterpret_cast<char*>(dgbar) - cv.base), gbar.data(), gbar.size() * sizeof(double2*));
         std::memcpy(image.data() + (reinterpret_cast<char*>(dsj) - cv.base), sj.data(), sj.size() * sizeof(SrcAdjJob));
@@ -1498,9 +1680,24 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
         k_fcr_adj_scan<<<dim3(static_cast<unsigned>(nf3), nj), SC_THREADS, 0, st>>>(dfj, nf, static_cast<uint32_t>(T),
                                                                                     jobs[idx[0]].dt);
         launched("k_fcr_adj_scan");
-        k_fcr_adj_corr<<<dim3(static_cast<unsigned>(ntiles), static_cast<unsigned>(nf3), nj), CR_TM, 0, st>>>(
-            dfj, nf, static_cast<uint32_t>(T), jobs[idx[0]].dt);
-        launched("k_fcr_adj_corr");
+        if (fftN) {
+            FzPlan<double2> fp{};
+            fp.N = fftN;
+            fz_stages(fftN, 8, fp.rad, fp.nst);
+            fp.tw = roots;
+            const std::size_t fsm = fz_smem<double2>(fftN);
+            raise_smem_limit(reinterpret_cast<const void*>(&k_adj_series_spectrum), fsm);
+            raise_smem_limit(reinterpret_cast<const void*>(&k_fcr_adj_corr_fft), fsm);
+            k_adj_series_spectrum<<<static_cast<unsigned>(nspec_jobs), FZ_THREADS, fsm, st>>>(dsjobs, fp);
+            launched("k_adj_series_spectrum");
+            k_fcr_adj_corr_fft<<<dim3(5, static_cast<unsigned>(nf3), nj), FZ_THREADS, fsm, st>>>(
+                dfj, dspec, nf, static_cast<uint32_t>(T), jobs[idx[0]].dt, fp);
+            launched("k_fcr_adj_corr_fft");
+        } else {
+            k_fcr_adj_corr<<<dim3(static_cast<unsigned>(ntiles), static_cast<unsigned>(nf3), nj), CR_TM, 0, st>>>(
+                dfj, nf, static_cast<uint32_t>(T), jobs[idx[0]].dt);
+            launched("k_fcr_adj_corr");
+        }
         k_fcr_adj_reduce<<<dim3(static_cast<unsigned>((T + 127) / 128), static_cast<unsigned>(nf), nj), 128, 0, st>>>(
             dfj, nf, static_cast<uint32_t>(T), dgbar);
         launched("k_fcr_adj_reduce");

@@ -629,6 +629,40 @@ int taco_set_work_budget(size_t bytes) {
     return guarded([&] { taco::set_work_budget(bytes); });
 }
 
+int taco_release_workspace(void) {
+    return guarded([&] {
+        require_device();
+        taco::release_workspace();
+    });
+}
+
+int taco_set_fused_conv(int on) {
+    return guarded([&] { taco::set_fused_conv(on != 0); });
+}
+
+int taco_set_fp32_guard(double tol) {
+    return guarded([&] {
+        if (!(tol >= 0.0)) throw taco::Error(taco::kInvalidArgument, "fp32 guard tolerance must be >= 0");
+        taco::set_fp32_guard(tol);
+    });
+}
+
+int taco_fp32_guard_stats(uint64_t* counts6) {
+    return guarded([&] {
+        if (!counts6) throw taco::Error(taco::kInvalidArgument, "counts is null");
+        const taco::GuardStats g = taco::fp32_guard_stats();
+        const uint64_t v[6] = {g.instances, g.heads, g.head_rows, g.rows, g.full, g.rounds};
+        for (int k = 0; k < 6; ++k) counts6[k] = v[k];
+    });
+}
+
+int taco_get_fp32_guard(double* tol) {
+    return guarded([&] {
+        if (!tol) throw taco::Error(taco::kInvalidArgument, "tol is null");
+        *tol = taco::fp32_guard();
+    });
+}
+
 int taco_fft_length(size_t n_in, int precision, int flags, size_t* nfft, int* key) {
     return guarded([&] {
         if (n_in == 0) throw taco::Error(taco::kInvalidArgument, "fft_length: n_in must be > 0");
@@ -810,6 +844,16 @@ int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, si
         t.chunk_bytes = chunk_bytes;
         t.inv_dft_rows = inv_dft_rows;
         taco::set_tuning(log2_nfft, precision == TACO_PREC_FP32, t);
+    });
+}
+
+int taco_set_fft_length_enabled(int key, int precision, int enabled) {
+    return guarded([&] {
+        if ((key & 63) < 3 || (key & 63) > 22 || key >= 192 || key < 64)
+            throw taco::Error(taco::kInvalidArgument, "fft length key must name a 3*2^k or 5*2^k length");
+        taco::Tuning t = taco::get_tuning(key, precision == TACO_PREC_FP32);
+        t.enabled = enabled ? 1 : 0;
+        taco::set_tuning(key, precision == TACO_PREC_FP32, t);
     });
 }
 

@@ -19,6 +19,7 @@
 #include <mutex>
 #include <string>
 #include <cstring>
+#include <cstdint>
 #include <limits>
 #include <map>
 #include <memory>
@@ -29,6 +30,7 @@
 #include "cluster_conv.cuh"
 #include "contract.cuh"
 #include "fcr_kernels.cuh"
+#include "fused_conv.cuh"
 #include "gw_coef.hpp"
 #include "rk4.cuh"
 
@@ -80,8 +82,15 @@ struct Lap {
 struct DeviceBuffer {
     void* p = nullptr;
     std::size_t cap = 0;
+    bool owned = true;  // false: a caller's buffer lent to a plan (never grown or freed here)
+    void release() {
+        if (p && owned) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
     void ensure(std::size_t bytes) {
         if (bytes <= cap) return;
+        if (!owned) throw Error(kRuntime, "shared work buffer smaller than the build needs");
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
@@ -90,13 +99,18 @@ struct DeviceBuffer {
         cap = want;
     }
     ~DeviceBuffer() {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
     }
 };
 
 struct PinnedBuffer {
     void* p = nullptr;
     std::size_t cap = 0;
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
     void ensure(std::size_t bytes) {
         if (bytes <= cap) return;
         if (p) cudaFreeHost(p);
@@ -173,9 +187,11 @@ struct Workspace {
     std::vector<std::unique_ptr<SubBuffers>> sub_bufs;
     cudaStream_t upload = nullptr;
     std::map<std::pair<int, int>, std::unique_ptr<PlanTables>> plans;  // (L, fp32)
+    std::map<std::pair<int, int>, std::unique_ptr<DeviceBuffer>> fz_tables;  // (N, fp32): fused-path roots
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~Workspace() {
         plans.clear();
+        fz_tables.clear();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (auto& l : extra)
@@ -258,6 +274,42 @@ FftPlan<cplx_t<R>> get_plan(Workspace& ws, int L, int Rf, cudaStream_t st) {
     p.twc = lay.take<C>(N >> pt.s);
     p.twf = lay.take<C>(std::size_t(1) << pt.s);
     return p;
+}
+
+// Fused-path plan of length N: its stage list and the table of N-th roots.
+std::atomic<int> g_fused{1};
+
+template <class R>
+FzPlan<cplx_t<R>> get_fz_plan(Workspace& ws, int N, cudaStream_t st) {
+    using C = cplx_t<R>;
+    const bool fp32 = std::is_same<R, float>::value;
+    FzPlan<C> p{};
+    p.N = N;
+    if (!fz_stages(N, fp32 ? 16 : 8, p.rad, p.nst)) throw Error(kRuntime, "fused path: unsupported FFT length");
+    auto& slot = ws.fz_tables[{N, fp32 ? 1 : 0}];
+    if (!slot) {
+        auto buf = std::make_unique<DeviceBuffer>();
+        buf->ensure(static_cast<std::size_t>(N) * sizeof(C));
+        k_fill_twiddle<C><<<static_cast<unsigned>((N + 255) / 256), 256, 0, st>>>(static_cast<C*>(buf->p),
+                                                                              static_cast<uint32_t>(N), static_cast<double>(N));
+        cuda_check(cudaGetLastError(), "k_fill_twiddle(fused)");
+        g_launches.fetch_add(1);
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(twiddles)");
+        slot = std::move(buf);
+    }
+    p.tw = static_cast<const C*>(slot->p);
+    return p;
+}
+
+// Whether a group of FFT length N runs the fused path: its working array and the scan
+// scratch fit one CTA's shared memory, and the stage list exists.
+template <class R>
+bool fused_fits(std::size_t N) {
+    using C = cplx_t<R>;
+    if (!g_fused.load() || N > (std::size_t(1) << 16)) return false;
+    int rad[FZ_MAX_STAGES], nst = 0;
+    if (!fz_stages(static_cast<int>(N), std::is_same<R, float>::value ? 16 : 8, rad, nst)) return false;
+    return fz_smem<C>(static_cast<int>(N)) <= 227 * 1024;
 }
 
 // Tables of the cluster path: M-point twiddles and the N-point coarse/fine tables.
@@ -422,49 +474,6 @@ RowFn<R> row_fn(int l, int c) {
 #undef TACO_CT_CASES
 #undef TACO_MX_CASES
 
-struct Geometry {
-    int log2c, col_threads, log2r, row_threads;
-    std::size_t col_smem, row_smem;
-    unsigned col_grid, row_grid;
-};
-
-// Tile shapes: column tiles of col_tile elements (N1 rows x 2^log2c columns), row tiles
-// of row_tile elements (2^log2r rows of N2), both padded in shared memory.
-template <class C>
-Geometry geometry(const FftPlan<C>& p, int col_tile, int row_tile) {
-    Geometry g;
-    const int N1 = p.R << p.L1, N2 = 1 << p.L2;
-    auto floor_log2 = [](int x) {
-        int l = 0;
-        while ((2 << l) <= x) ++l;
-        return l;
-    };
-    const int cc = std::max(1, std::min(N2, col_tile / N1));
-    g.log2c = floor_log2(cc);
-    g.col_threads = (N1 << g.log2c) / 8;
-    g.col_smem = static_cast<std::size_t>(padded_size<C>(N1 << g.log2c)) * sizeof(C);
-    g.col_grid = static_cast<unsigned>(N2 >> g.log2c);
-    const int rr = std::max(1, std::min(1 << p.L1, row_tile / N2));  // rows of a tile divide N1
-    g.log2r = floor_log2(rr);
-    g.row_threads = (N2 << g.log2r) / 8;
-    g.row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << g.log2r)) * sizeof(C);
-    g.row_grid = static_cast<unsigned>(N1 >> g.log2r);
-    constexpr std::size_t kSmemMax = 227 * 1024;
-    while (g.row_smem > kSmemMax && g.log2r > 0) {  // explicit schedules too large for one CTA
-        --g.log2r;
-        g.row_threads = (N2 << g.log2r) / 8;
-        g.row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << g.log2r)) * sizeof(C);
-    }
-    while (g.col_smem > kSmemMax && g.log2c > 0) {
-        --g.log2c;
-        g.col_threads = (N1 << g.log2c) / 8;
-        g.col_smem = static_cast<std::size_t>(padded_size<C>(N1 << g.log2c)) * sizeof(C);
-    }
-    g.col_grid = static_cast<unsigned>(N2 >> g.log2c);
-    g.row_grid = static_cast<unsigned>(N1 >> g.log2r);
-    return g;
-}
-
 struct ProfStore {
     std::mutex mu;
     std::map<std::string, std::pair<uint64_t, double>> acc;
@@ -625,10 +634,17 @@ void choose_fft(std::size_t target, bool fp32, bool allow_mixed, int& L_out, int
         const int L = std::max(3, ilog2(base));
         const std::size_t n = static_cast<std::size_t>(Rf) << L;
         if (n >= nfft || n < target) continue;
+        const Tuning t = tuning_for(size_key(L, Rf), fp32);
+        if (!t.enabled) continue;  // the autotuner measured a longer length faster
+        if (fp32 ? fused_fits<float>(n) : fused_fits<double>(n)) {  // no column kernels needed
+            nfft = n;
+            L_out = L;
+            R_out = Rf;
+            continue;
+        }
         int L1 = 0, L2 = 0;
         fft_split(L, Rf, L1, L2);
         if (L1 < 3) continue;
-        const Tuning t = tuning_for(size_key(L, Rf), fp32);
         const int log2c = fp32 ? geometry(FftPlan<float2>{L, L1, L2, 0, Rf, nullptr, nullptr, nullptr, nullptr},
                                           t.col_tile, t.row_tile).log2c
                                : geometry(FftPlan<double2>{L, L1, L2, 0, Rf, nullptr, nullptr, nullptr, nullptr},
@@ -707,6 +723,7 @@ struct GroupGeom {
     Geometry g;
     int clm = -1, inv_rows = 0, max_chunks = 0;
     bool use_cluster = false, inv_dft = false;
+    bool fused = false;  // one CTA per (triple, half): transforms, scans and assembly in shared memory
 };
 
 template <class R>
@@ -725,6 +742,7 @@ GroupGeom<R> group_geom(const std::vector<WorkUnit*>& units) {
     for (auto* u : units) G.ntri += static_cast<std::size_t>(u->nsub());
     G.clm = G.Rf == 1 ? cluster_lm_for(G.L, std::is_same<R, float>::value, G.tune) : -1;
     G.use_cluster = G.clm > 0;
+    G.fused = !G.use_cluster && fused_fits<R>(G.Nfft);
     const std::size_t per_tri_scratch = 2 * G.Nfft * sizeof(C);
     G.Q = std::max<std::size_t>(1, G.tune.chunk_bytes / per_tri_scratch);
     G.Q = std::min<std::size_t>({G.Q, std::max<std::size_t>(1, G.ntri), 32767});
@@ -763,7 +781,7 @@ void layout_work(const std::vector<WorkUnit*>& units, const GroupGeom<R>& G, boo
         const std::size_t nf = in.sys.nf, nsub = units[a]->nsub();
         if (!in.gamma_on_device && !gamma_elsewhere) P.gamma[a] = lay.take<double2>(nf * m.n_in);
         P.spec[a] = lay.take<C>(2 * nf * G.Nfft);
-        P.conv[a] = lay.take<C>(nsub * 2 * m.t_count);
+        if (!G.fused) P.conv[a] = lay.take<C>(nsub * 2 * m.t_count);
         if (!fcr_only) {
             P.v[a] = lay.take<C>(3 * nsub * m.U);
             if (!in.out_on_device) {
@@ -774,8 +792,8 @@ void layout_work(const std::vector<WorkUnit*>& units, const GroupGeom<R>& G, boo
             P.v[a] = lay.take<C>(3 * nsub * m.U);
         }
     }
-    P.scratch = lay.take<C>(G.use_cluster ? 1 : G.Q * 2 * G.Nfft);
-    P.partial = lay.take<double>(std::max<std::size_t>(1, G.ntri) * G.max_chunks * SCAN_W);
+    P.scratch = lay.take<C>(G.use_cluster || G.fused ? 1 : G.Q * 2 * G.Nfft);
+    P.partial = lay.take<double>(G.fused ? 1 : std::max<std::size_t>(1, G.ntri) * G.max_chunks * SCAN_W);
 }
 
 template <class R>
@@ -939,6 +957,10 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
                 ++cj;
             }
     }
+    auto r_spec_f = [&](std::size_t a, int jm) { return P.spec[a] + static_cast<std::size_t>(jm) * Nfft; };
+    auto r_spec_c = [&](std::size_t a, int j) {
+        return P.spec[a] + static_cast<std::size_t>(units[a]->in->sys.nf + j) * Nfft;
+    };
     for (std::size_t q = 0; q < ntri; ++q) {
         const int a = tris[q].unit, tri = tris[q].tri;
         const Tcl4Instance& in = *units[a]->in;
@@ -962,8 +984,8 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         c.out = z;
         rowj[n_spec_jobs + q] = RowJob{z, wcb, P.spec[a] + static_cast<std::size_t>(jm) * Nfft,
                                        P.spec[a] + static_cast<std::size_t>(nf + j) * Nfft};
-        C* cf = P.conv[a] + lt * 2 * m.t_count;
-        C* cc = cf + m.t_count;
+        C* cf = G.fused ? nullptr : P.conv[a] + lt * 2 * m.t_count;
+        C* cc = G.fused ? nullptr : cf + m.t_count;
         const double scale = in.dt / static_cast<double>(Nfft);
         invj[2 * q] = InvJob{z, cf, static_cast<uint32_t>(m.t_count), scale};
         invj[2 * q + 1] = InvJob{wcb, cc, static_cast<uint32_t>(m.t_count), scale};
@@ -977,6 +999,8 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         s.t_count = static_cast<uint32_t>(m.t_count);
         s.conv_f = cf;
         s.conv_c = cc;
+        s.spec_f = r_spec_f(a, jm);
+        s.spec_c = r_spec_c(a, j);
         s.tmap = M.tmap[a];
         if (fcr_only && fcr_out_dev) {
             s.vf = fcr_out[3 * a + 0] + static_cast<std::size_t>(tri) * m.U;  // three outputs per unit
@@ -1185,6 +1209,15 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     // single-pass scan (one CTA per triple) once the triples alone fill the GPU four times
     // over; the chunked reduce-then-scan otherwise
     const bool scan_single = n_scan >= static_cast<std::size_t>(148 * 2 * 4);
+    const bool fused = G.fused;
+    FzPlan<C> fzp{};
+    std::size_t fz_bytes = 0;
+    if (fused) {
+        fzp = get_fz_plan<R>(ws, static_cast<int>(Nfft), st);
+        fz_bytes = fz_smem<C>(static_cast<int>(Nfft));
+        set_smem(k_fz_spectrum<R>, fz_bytes);
+        set_smem(k_fz_conv_scan<R>, fz_bytes);
+    }
     const MetaPtrs Mc = M;
     const WorkPtrs<C> Pc = P;
     return [=](cudaStream_t st, ProfRecorder* prp, cudaEvent_t ev0, cudaEvent_t ev1) {
@@ -1192,7 +1225,14 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     ProfRecorder& pr = prp ? *prp : dummy;
     const bool f32 = std::is_same<R, float>::value;
     if (ev0) cuda_check(cudaEventRecord(ev0, st), "cudaEventRecord");
-    if (use_cluster) {
+    if (fused) {
+        pr.before(f32 ? "fz_spectra_f32" : "fz_spectra_f64");
+        k_fz_spectrum<R><<<static_cast<unsigned>(n_spec_jobs), FZ_THREADS, fz_bytes, st>>>(Mc.colj, fzp);
+        check_launch("k_fz_spectrum", &pr);
+        pr.before(f32 ? "fz_conv_scan_f32" : "fz_conv_scan_f64");
+        k_fz_conv_scan<R><<<static_cast<unsigned>(2 * ntri), FZ_THREADS, fz_bytes, st>>>(Mc.scanj, fzp);
+        check_launch("k_fz_conv_scan", &pr);
+    } else if (use_cluster) {
         pr.before(f32 ? "spectra_cluster_f32" : "spectra_cluster_f64");
         launch_cluster<R>(Mc.clj, n_spec_jobs, cplan, st);
         check_launch("k_conv_cluster(spectra)", &pr);
@@ -1239,13 +1279,15 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
             }
         }
     }
-    if (scan_single) {
+    if (fused) {
+        // the fused kernel assembled F, C, R already
+    } else if (scan_single) {
         // enough triples to fill the GPU: one CTA per triple walks its whole time axis
         pr.before(f32 ? "scan_assemble_f32" : "scan_assemble_f64");
         k_scan_assemble<R, 2, 4><<<static_cast<unsigned>(n_scan), SCAN_THREADS, 0, st>>>(Mc.scanj);
         check_launch("k_scan_assemble", &pr);
     }
-    for (std::size_t s0 = 0; !scan_single && s0 < n_scan; s0 += 65535) {
+    for (std::size_t s0 = 0; !fused && !scan_single && s0 < n_scan; s0 += 65535) {
         const unsigned ns = static_cast<unsigned>(std::min<std::size_t>(65535, n_scan - s0));
         pr.before(f32 ? "scan_reduce_f32" : "scan_reduce_f64");
         k_scan_reduce<R><<<dim3(static_cast<unsigned>(max_chunks), ns), SCAN_THREADS, 0, st>>>(
@@ -1344,6 +1386,10 @@ std::vector<std::vector<WorkUnit*>> plan_units(std::vector<Tcl4Instance>& insts,
                 const std::size_t base = measure_work<R>(p1, false, false);
                 probe.hi = std::min(nf3, 2);
                 const std::size_t two = measure_work<R>(p1, false, false);
+                if (base > budget)  // not even one frequency triple fits: the budget is a hard cap
+                    throw Error(kOverflow, "one frequency triple needs " + std::to_string(base) +
+                                               " bytes of transient device memory, above the work budget of " +
+                                               std::to_string(budget) + " bytes");
                 const std::size_t per = std::max<std::size_t>(1, two > base ? two - base : base);
                 const std::size_t nsub = budget > base ? std::max<std::size_t>(1, (budget - base) / per + 1) : 1;
                 if (!insts[a].gamma_on_device || !insts[a].out_on_device)
@@ -1430,6 +1476,29 @@ void stage_sliced_io(std::vector<Tcl4Instance>& insts, std::vector<InstMeta>& me
 }  // namespace
 
 void set_work_budget(std::size_t bytes) { g_work_budget.store(bytes); }
+void set_fused_conv(bool on) { g_fused.store(on ? 1 : 0); }
+
+void release_workspace() {
+    Workspace& ws = workspace();
+    cuda_check(cudaStreamSynchronize(ws.stream), "cudaStreamSynchronize(release)");
+    for (auto& l : ws.extra)
+        if (l.s) cuda_check(cudaStreamSynchronize(l.s), "cudaStreamSynchronize(release)");
+    if (ws.upload) cuda_check(cudaStreamSynchronize(ws.upload), "cudaStreamSynchronize(release)");
+    ws.work.release();
+    ws.arena.release();
+    ws.staging.release();
+    for (auto& l : ws.extra) {
+        l.work.release();
+        l.arena.release();
+        l.staging.release();
+    }
+    for (auto& b : ws.sub_bufs) {
+        b->arena.release();
+        b->input.release();
+        b->staging.release();
+    }
+}
+bool fused_conv() { return g_fused.load() != 0; }
 
 std::size_t fft_length_for(std::size_t n_in, bool fp32, bool causal, std::size_t pad_factor, int* key) {
     std::size_t target = 2 * n_in - 1;
@@ -1560,7 +1629,7 @@ namespace {
 void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, std::vector<InstMeta>& metas);
 }
 
-void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream) {
+void tcl4_build_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream) {
     Workspace& ws = workspace();
     cudaStream_t st = stream ? stream : ws.stream;
     if (opt.fcr_ms) *opt.fcr_ms = 0.0;
@@ -1592,7 +1661,20 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
             ++nunits;
             whole = whole && !u->accumulate && u->lo == 0 && u->hi == u->in->sys.nf * u->in->sys.nf * u->in->sys.nf;
         }
-    const bool pipeline = whole && io.back.empty() && !opt.fcr_ms && !g_profile.load() && nunits >= kPipeSub;
+    bool pipeline = whole && io.back.empty() && !opt.fcr_ms && !g_profile.load() && nunits >= kPipeSub;
+    if (pipeline) {
+        // two lanes' transient arrays must fit the group budget together (large instances,
+        // whose sub-batches each fill the budget, run on one lane)
+        std::size_t mw = 0;
+        for (auto& gu : groups) {
+            const std::size_t n = gu.size(), parts = std::max<std::size_t>(1, (n + kPipeSub / 2) / kPipeSub);
+            for (std::size_t p = 0; p < parts; ++p) {
+                std::vector<WorkUnit*> sub(gu.begin() + p * n / parts, gu.begin() + (p + 1) * n / parts);
+                mw = std::max(mw, opt.fp32 ? measure_work<float>(sub, false, false) : measure_work<double>(sub, false, false));
+            }
+        }
+        pipeline = 2 * mw <= budget;
+    }
     if (!pipeline) {
         for (auto& gu : groups) {
             if (opt.fp32) run_group<float>(gu, opt, st, ws, nullptr, false);
@@ -1616,13 +1698,13 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
                 max_input = std::max(max_input, in_bytes);
             }
         }
-        // a third lane while three sub-batches' transient arrays fit twice the group budget
-        const std::size_t nlanes = subs.size() >= 3 && 3 * max_work <= 2 * budget ? 3 : 2;
+        // a third lane while three sub-batches' transient arrays fit the group budget
+        const std::size_t nlanes = subs.size() >= 3 && 3 * max_work <= budget ? 3 : 2;
         // sub-batch buffer slots (metadata, staged input): up to two per lane, while the
-        // lanes' work arrays and the slots' inputs fit twice the group budget; a slot is
-        // reused once the sub-batch that held it has finished
+        // lanes' work arrays and the slots' inputs fit the group budget; a slot is reused
+        // once the sub-batch that held it has finished
         std::size_t nslots = std::min<std::size_t>(subs.size(), 2 * nlanes);
-        while (nslots > 1 && nlanes * max_work + nslots * max_input > 2 * budget) --nslots;
+        while (nslots > 1 && nlanes * max_work + nslots * max_input > budget) --nslots;
         struct Lane {
             cudaStream_t s;
             DeviceBuffer* work;
@@ -1827,7 +1909,12 @@ struct Tcl4Plan {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t kernels = 0;
+    // work enqueued after the graph on every execute (the FP64 heads of the FP32 form),
+    // holding the buffers and plans it uses; its kernel count
+    std::function<void(cudaStream_t)> tail;
+    uint64_t tail_kernels = 0;
     ~Tcl4Plan() {
+        tail = nullptr;  // the tail's plans and buffers go before the stream
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (stream) cudaStreamDestroy(stream);
@@ -1835,6 +1922,33 @@ struct Tcl4Plan {
 };
 
 namespace {
+// A buffer flagged as device memory must be device (or managed) memory of the current device
+// and aligned for its element type: a host address or a misaligned one handed to the kernels
+// would fault instead of failing.  The last accepted pointer is remembered per thread
+// (consecutive instances often share one buffer).
+void check_device_buffer(const void* p, std::size_t align, const char* what) {
+    if (reinterpret_cast<std::uintptr_t>(p) % align != 0)
+        throw Error(kInvalidArgument, std::string(what) + " (device) is not " + std::to_string(align) + "-byte aligned");
+    thread_local const void* last_ok = nullptr;
+    thread_local int last_dev = -1;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (p == last_ok && dev == last_dev) return;
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw Error(kInvalidArgument, std::string(what) + " is flagged as device memory but is not a CUDA allocation");
+    }
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+        throw Error(kInvalidArgument, std::string(what) + " is flagged as device memory but is host memory");
+    if (a.type == cudaMemoryTypeDevice && a.device != dev)
+        throw Error(kInvalidArgument, std::string(what) + " is on device " + std::to_string(a.device) +
+                                          ", not the current device " + std::to_string(dev));
+    last_ok = p;
+    last_dev = dev;
+}
+
 void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, std::vector<InstMeta>& metas) {
     const std::size_t n = insts.size();
     metas.resize(n);
@@ -1866,8 +1980,10 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
         if (in.Nt >= (std::size_t(1) << 31)) throw Error(kOverflow, "Nt too large");
         if (!(in.dt > 0.0)) throw Error(kInvalidArgument, "dt must be > 0");
         if (!in.gamma) throw Error(kInvalidArgument, "gamma is null");
+        if (in.gamma_on_device) check_device_buffer(in.gamma, sizeof(double2), "gamma");
         if (in.tidx.empty()) continue;
         if (!in.out) throw Error(kInvalidArgument, "output pointer is null");
+        if (in.out_on_device) check_device_buffer(in.out, opt.fp32 ? sizeof(float2) : sizeof(double2), "output");
         auto r = list_index.emplace(in.tidx.identity(), first.size());
         if (r.second) first.push_back(a);
         lid[a] = r.first->second;
@@ -1923,7 +2039,21 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
 }
 }  // namespace
 
-Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt) {
+std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions& opt) {
+    std::vector<InstMeta> metas;
+    validate_and_derive(insts, opt, metas);
+    std::vector<std::unique_ptr<WorkUnit>> store;
+    const std::size_t budget = work_budget();
+    std::vector<std::vector<WorkUnit*>> groups =
+        opt.fp32 ? plan_units<float>(insts, metas, budget, store) : plan_units<double>(insts, metas, budget, store);
+    std::size_t work = 0;
+    for (auto& gu : groups)
+        work = std::max(work, opt.fp32 ? measure_work<float>(gu, false, false) : measure_work<double>(gu, false, false));
+    return work;
+}
+
+Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, void* ext_work,
+                             std::size_t ext_cap) {
     for (const auto& in : insts)
         if (!in.gamma_on_device || !in.out_on_device)
             throw Error(kInvalidArgument, "plans take device inputs and outputs (TACO_IN_DEVICE | TACO_OUT_DEVICE)");
@@ -1941,6 +2071,11 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
     std::size_t work = 0;
     for (auto& gu : groups)
         work = std::max(work, opt.fp32 ? measure_work<float>(gu, false, false) : measure_work<double>(gu, false, false));
+    if (ext_work) {  // a caller's buffer shared by plans that run one after another
+        plan->work.p = ext_work;
+        plan->work.cap = ext_cap;
+        plan->work.owned = false;
+    }
     plan->work.ensure(work);
     for (auto& gu : groups) {
         plan->mems.push_back(std::make_unique<DeviceBuffer>());
@@ -1974,11 +2109,17 @@ void plan_execute(Tcl4Plan* plan, cudaStream_t stream) {
     // asynchronous on exactly the caller's stream (0 is the legacy default stream)
     cuda_check(cudaGraphLaunch(plan->exec, stream), "cudaGraphLaunch");
     g_launches.fetch_add(plan->kernels);
+    if (plan->tail) plan->tail(stream);
+}
+
+void plan_set_tail(Tcl4Plan* plan, std::function<void(cudaStream_t)> tail, uint64_t kernels) {
+    plan->tail = std::move(tail);
+    plan->tail_kernels = kernels;
 }
 
 void plan_destroy(Tcl4Plan* plan) { delete plan; }
 
-uint64_t plan_kernels(const Tcl4Plan* plan) { return plan ? plan->kernels : 0; }
+uint64_t plan_kernels(const Tcl4Plan* plan) { return plan ? plan->kernels + plan->tail_kernels : 0; }
 
 std::size_t rk4_num_samples(std::size_t steps, std::size_t sample_every) {
     if (sample_every == 0) return 0;

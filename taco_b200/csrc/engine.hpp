@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -70,11 +71,19 @@ struct Tuning {
     std::size_t chunk_bytes = std::size_t(48) << 20;  // Z/W scratch per chunk of triples
     int inv_dft_rows = 16;                      // pruned inverse column DFT up to this many rows
     int cluster_lm = 0;  // log2 points per CTA of the cluster path (0: multi-pass path, -1: automatic)
+    int enabled = 1;     // 3 * 2^k and 5 * 2^k lengths: 0 removes the length from the causal rule's choice
 };
 void set_tuning(int L, bool fp32, const Tuning& t);
 // Transient device memory one group of a build may use (0: 45% of the free memory, at
 // most 64 GiB); an instance above it is processed in slices of its frequency triples.
 void set_work_budget(std::size_t bytes);
+// The fused F/C/R path (one CTA per triple and half, the transforms in shared memory) for the
+// FFT lengths it fits; off: the four-step passes and the scan kernels for every length.
+void set_fused_conv(bool on);
+bool fused_conv();
+// Frees the calling thread's grow-only transient buffers on the current device (after its
+// streams finish); the next build allocates them again.
+void release_workspace();
 // FFT length of the F/C/R convolutions for n_in consumed samples, and its schedule key
 // (the tuning-table key: log2 for powers of two, + 64 for 3 * 2^k, + 128 for 5 * 2^k).
 std::size_t fft_length_for(std::size_t n_in, bool fp32, bool causal, std::size_t pad_factor, int* key);
@@ -88,19 +97,46 @@ struct BuildOptions {
     double* fcr_ms = nullptr;        // device time of the F/C/R stage
 };
 
-// Full L4 builds (build_TCL4_generator_cuda_fused[_batch]) for a set of instances.
+// Full L4 builds (build_TCL4_generator_cuda_fused[_batch]) for a set of instances.  In the
+// FP32 form the precision guard (guard.cu) recomputes in FP64 the leading times at which
+// the FP32 result misses the guard's tolerance.
 void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream);
+// The same without the guard (one pass in the requested precision).
+void tcl4_build_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream);
 
 // Prepared batched build: metadata resident on the device, launch sequence captured in a
 // CUDA graph; execute replays it (stream-ordered, no host work).
 struct Tcl4Plan;
 Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt);
+// ext_work (optional): a caller's device buffer of ext_cap bytes for the plan's transient
+// arrays, shared with plans that run one after another on the same stream.
+Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, void* ext_work = nullptr,
+                             std::size_t ext_cap = 0);
+// Transient bytes a plan of these instances would allocate.
+std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions& opt);
+// Work enqueued after the plan's graph on every execute (owns what it captures).
+void plan_set_tail(Tcl4Plan* plan, std::function<void(cudaStream_t)> tail, uint64_t kernels);
 void plan_execute(Tcl4Plan* plan, cudaStream_t stream);
 void plan_destroy(Tcl4Plan* plan);
 uint64_t plan_kernels(const Tcl4Plan* plan);
 
 // L4 build of one instance with every scratch buffer in a fixed file-scope device array
 // (noalloc.cu); gamma and out are device pointers.
+// Precision guard of the FP32 form: the largest relative FP32-vs-FP64 error accepted on the
+// checked window (0: off).
+void set_fp32_guard(double tol);
+double fp32_guard();
+// What the guard did in the calling thread's last FP32 build or plan creation.
+struct GuardStats {
+    uint64_t instances = 0;  // instances of the call
+    uint64_t heads = 0;      // instances whose leading times were rebuilt in FP64
+    uint64_t head_rows = 0;  // requested times rebuilt in FP64
+    uint64_t rows = 0;       // requested times of the instances with a head
+    uint64_t full = 0;       // instances rebuilt in FP64 entirely
+    uint64_t rounds = 0;     // head-growth rounds
+};
+GuardStats fp32_guard_stats();
+
 void noalloc_tcl4_build(const SystemDesc& sys, const double2* gamma, std::size_t Nt, double dt,
                         const std::vector<uint32_t>& tidx, bool fp32, std::size_t pad_factor, void* out,
                         cudaStream_t stream);

@@ -29,6 +29,9 @@
 // times.
 #pragma once
 
+#include <algorithm>
+#include <cstddef>
+
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -43,6 +46,50 @@ struct FftPlan {
     const C* twc;      // exp(-2 pi i m 2^s / N), m < N / 2^s
     const C* twf;      // exp(-2 pi i m / N), m < 2^s
 };
+
+// Launch geometry of the four-step passes (host side).
+struct Geometry {
+    int log2c, col_threads, log2r, row_threads;
+    std::size_t col_smem, row_smem;
+    unsigned col_grid, row_grid;
+};
+
+// Tile shapes: column tiles of col_tile elements (N1 rows x 2^log2c columns), row tiles
+// of row_tile elements (2^log2r rows of N2), both padded in shared memory.
+template <class C>
+Geometry geometry(const FftPlan<C>& p, int col_tile, int row_tile) {
+    Geometry g;
+    const int N1 = p.R << p.L1, N2 = 1 << p.L2;
+    auto floor_log2 = [](int x) {
+        int l = 0;
+        while ((2 << l) <= x) ++l;
+        return l;
+    };
+    const int cc = std::max(1, std::min(N2, col_tile / N1));
+    g.log2c = floor_log2(cc);
+    g.col_threads = (N1 << g.log2c) / 8;
+    g.col_smem = static_cast<std::size_t>(padded_size<C>(N1 << g.log2c)) * sizeof(C);
+    g.col_grid = static_cast<unsigned>(N2 >> g.log2c);
+    const int rr = std::max(1, std::min(1 << p.L1, row_tile / N2));  // rows of a tile divide N1
+    g.log2r = floor_log2(rr);
+    g.row_threads = (N2 << g.log2r) / 8;
+    g.row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << g.log2r)) * sizeof(C);
+    g.row_grid = static_cast<unsigned>(N1 >> g.log2r);
+    constexpr std::size_t kSmemMax = 227 * 1024;
+    while (g.row_smem > kSmemMax && g.log2r > 0) {  // explicit schedules too large for one CTA
+        --g.log2r;
+        g.row_threads = (N2 << g.log2r) / 8;
+        g.row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << g.log2r)) * sizeof(C);
+    }
+    while (g.col_smem > kSmemMax && g.log2c > 0) {
+        --g.log2c;
+        g.col_threads = (N1 << g.log2c) / 8;
+        g.col_smem = static_cast<std::size_t>(padded_size<C>(N1 << g.log2c)) * sizeof(C);
+    }
+    g.col_grid = static_cast<unsigned>(N2 >> g.log2c);
+    g.row_grid = static_cast<unsigned>(N1 >> g.log2r);
+    return g;
+}
 
 // w_N^a for 0 <= a < N as the product of a coarse and a fine table entry.
 template <class C>
@@ -89,6 +136,8 @@ struct ScanJob {
     void* vf;          // F series at the unique requested times [U]
     void* vc;
     void* vr;
+    const void* spec_f;  // fused path: partner spectra in the fused transform's order
+    const void* spec_c;
 };
 
 // Threads of a compile-time-size FFT tile (8 elements per thread).

@@ -30,25 +30,25 @@ template <class C>
 __host__ __device__ __forceinline__ int padded_size(int n) { return n + (n >> PadShift<C>::value) + 1; }
 
 template <class C, bool INV>
-__device__ __forceinline__ C mul_w(C a, C w) {
+__host__ __device__ __forceinline__ C mul_w(C a, C w) {
     return INV ? cmulc(a, w) : cmul(a, w);  // INV: a * conj(w)
 }
 
 // multiply by -i (forward) or +i (inverse)
 template <class C, bool INV>
-__device__ __forceinline__ C rot90(C a) {
+__host__ __device__ __forceinline__ C rot90(C a) {
     return INV ? C{-a.y, a.x} : C{a.y, -a.x};
 }
 
 template <class C, bool INV>
-__device__ __forceinline__ void dft2(C& a, C& b) {
+__host__ __device__ __forceinline__ void dft2(C& a, C& b) {
     const C t = a;
     a = cadd(t, b);
     b = csub(t, b);
 }
 
 template <class C, bool INV>
-__device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3) {
+__host__ __device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3) {
     const C a = cadd(x0, x2), b = csub(x0, x2);
     const C c = cadd(x1, x3), d = rot90<C, INV>(csub(x1, x3));
     x0 = cadd(a, c);
@@ -58,7 +58,7 @@ __device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3) {
 }
 
 template <class C, bool INV>
-__device__ __forceinline__ void dft8(C* x) {
+__host__ __device__ __forceinline__ void dft8(C* x) {
     using R = decltype(x[0].x);
     const R h = static_cast<R>(0.70710678118654752440084436210484903928);
     C e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6];
@@ -82,7 +82,7 @@ __device__ __forceinline__ void dft8(C* x) {
 // 3- and 5-point DFTs (radix factors of the mixed lengths 3*2^k and 5*2^k).
 // y_k = sum_r x_r w^{r k}, w = exp(-+ 2 pi i / R); rot90 supplies the -+i.
 template <class C, bool INV>
-__device__ __forceinline__ void dft3(C& x0, C& x1, C& x2) {
+__host__ __device__ __forceinline__ void dft3(C& x0, C& x1, C& x2) {
     using R = decltype(x0.x);
     const R h = static_cast<R>(0.86602540378443864676);  // sin(2 pi / 3)
     const C t = cadd(x1, x2);
@@ -94,7 +94,7 @@ __device__ __forceinline__ void dft3(C& x0, C& x1, C& x2) {
 }
 
 template <class C, bool INV>
-__device__ __forceinline__ void dft5(C* x) {
+__host__ __device__ __forceinline__ void dft5(C* x) {
     using R = decltype(x[0].x);
     const R c1 = static_cast<R>(0.30901699437494742410);   // cos(2 pi / 5)
     const R c2 = static_cast<R>(-0.80901699437494742410);  // cos(4 pi / 5)

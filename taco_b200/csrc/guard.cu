@@ -1,0 +1,528 @@
+// guard.cu -- precision guard of the FP32 form.
+//
+// L4(t) is a combination of the F/C/R values with heavy cancellation: at early times (before
+// about one bath correlation time) L4 is orders of magnitude smaller than the values it is
+// formed from, and for long, slowly decaying series the cancellation persists at all times.
+// The FP32 FFT's round-off is spread evenly over the time axis, so the FP32 form's relative
+// error is largest where L4 is smallest: measured FP32-vs-FP64 errors exceed 1e-3 in the
+// first few hundred steps of long series, while the same series meet 1e-7 later on.  No
+// FP32 evaluation of the F/C/R values can fix this (rounding exact values to FP32 alone
+// gives 1e-4 at early times), so the guard measures the FP32 result against FP64 and
+// recomputes in FP64 where it falls short:
+//
+//   1. the FP32 build of every instance (tcl4_build_direct / plan_create_direct);
+//   2. per instance, a head [0, H) with H = max(512, t_count / 16) (t_count = max(tidx)+1)
+//      is built in FP64 (the causal rule makes its FFT length follow H);
+//   3. the FP32 and FP64 results are compared on the head's upper half [H/2, H) (at most
+//      256 requested times of it, evenly spaced): if the relative Frobenius difference is
+//      within the tolerance (default 5e-7), the FP64 head replaces the FP32 rows and the
+//      instance is done -- the FP32 error decreases or stays flat with time after the early
+//      transient in every measured series, so the rest keeps its FP32 values;
+//   4. otherwise H grows fourfold (at most to t_count, which is a full FP64 build of the
+//      instance) and step 2 repeats.
+//
+// Direct calls run the loop on every call.  Plans run it once at creation (on the inputs
+// they are created with) and replay the FP32 graph followed by the chosen FP64 heads and the
+// row patch; a plan replayed on different inputs keeps the head lengths chosen at creation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.hpp"
+
+namespace taco {
+
+namespace {
+
+std::atomic<double> g_guard_tol{5e-7};
+thread_local GuardStats t_stats;
+
+constexpr std::size_t kMinHead = 512;        // smallest head (samples)
+constexpr std::size_t kWindowSamples = 256;  // requested times compared per check
+constexpr std::size_t kTempBytes = std::size_t(1) << 30;  // FP64 head rows per chunk
+
+struct GuardJob {
+    const double2* h64;       // head rows [n][E], FP64
+    float2* out32;            // patch destination rows (the output, or a device buffer for host outputs)
+    const uint32_t* pos;      // [n] destination row of each head row
+    const float2* cmp32;      // FP32 rows compared (the output, or the staged rows of a host output)
+    const uint32_t* cmp_row;  // [nwin] row in cmp32 of each compared head row
+    const uint32_t* win;      // [nwin] head rows compared
+    uint32_t n, nwin, E;
+};
+
+// sums[2 j] = sum |cmp32 - h64|^2, sums[2 j + 1] = sum |h64|^2 over the window rows of job j.
+__global__ void __launch_bounds__(256) k_guard_compare(const GuardJob* __restrict__ jobs, double* __restrict__ sums) {
+    const GuardJob job = jobs[blockIdx.x];
+    double num = 0.0, den = 0.0;
+    const std::size_t total = static_cast<std::size_t>(job.nwin) * job.E;
+    for (std::size_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const std::size_t q = idx / job.E, e = idx % job.E;
+        const double2 r = job.h64[static_cast<std::size_t>(job.win[q]) * job.E + e];
+        const float2 f = job.cmp32[static_cast<std::size_t>(job.cmp_row[q]) * job.E + e];
+        const double dx = static_cast<double>(f.x) - r.x, dy = static_cast<double>(f.y) - r.y;
+        num += dx * dx + dy * dy;
+        den += r.x * r.x + r.y * r.y;
+    }
+    __shared__ double sn[8], sd[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, o);
+        den += __shfl_xor_sync(0xffffffffu, den, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sn[warp] = num;
+        sd[warp] = den;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+            a += sn[w];
+            b += sd[w];
+        }
+        sums[2 * blockIdx.x] = a;
+        sums[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// out32[pos[k]][e] = h64[k][e] rounded to FP32, for every head row of job blockIdx.y.
+__global__ void __launch_bounds__(256) k_guard_patch(const GuardJob* __restrict__ jobs) {
+    const GuardJob job = jobs[blockIdx.y];
+    const std::size_t total = static_cast<std::size_t>(job.n) * job.E;
+    for (std::size_t idx = static_cast<std::size_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+        const std::size_t k = idx / job.E, e = idx % job.E;
+        const double2 r = job.h64[idx];
+        job.out32[static_cast<std::size_t>(job.pos[k]) * job.E + e] =
+            make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+    }
+}
+
+struct DevMem {
+    void* p = nullptr;
+    std::size_t cap = 0;
+    void ensure(std::size_t bytes) {
+        if (bytes <= cap) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        cuda_check(cudaMalloc(&p, bytes), "cudaMalloc(guard)");
+        cap = bytes;
+    }
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    ~DevMem() {
+        if (p) cudaFree(p);
+    }
+};
+
+std::size_t entries(const Tcl4Instance& in) {
+    const std::size_t N2 = static_cast<std::size_t>(in.sys.N) * in.sys.N;
+    return N2 * N2;
+}
+
+uint32_t t_count_of(const Tcl4Instance& in) {
+    uint32_t m = 0;
+    for (uint32_t t : in.tidx) m = std::max(m, t);
+    return m + 1;
+}
+
+// The head of one instance: its requested times below H (in request order), their output
+// rows, and the head rows compared (times in [H/2, H), at most kWindowSamples evenly spaced).
+struct Head {
+    std::size_t inst = 0;
+    uint32_t H = 0, tc = 0;
+    std::vector<uint32_t> times, pos, win;
+};
+
+Head make_head(const std::vector<Tcl4Instance>& insts, std::size_t a, uint32_t H, uint32_t tc) {
+    Head h;
+    h.inst = a;
+    h.H = H;
+    h.tc = tc;
+    const Tcl4Instance& in = insts[a];
+    std::vector<uint32_t> upper;
+    for (std::size_t o = 0; o < in.tidx.size(); ++o) {
+        const uint32_t t = in.tidx[o];
+        if (t >= H) continue;
+        if (2 * static_cast<std::size_t>(t) >= H) upper.push_back(static_cast<uint32_t>(h.times.size()));
+        h.times.push_back(t);
+        h.pos.push_back(static_cast<uint32_t>(o));
+    }
+    if (upper.empty() && !h.times.empty()) {
+        // no requested time in the upper half: compare the latest quarter of the head rows
+        std::vector<uint32_t> ord(h.times.size());
+        for (std::size_t k = 0; k < ord.size(); ++k) ord[k] = static_cast<uint32_t>(k);
+        std::sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return h.times[x] > h.times[y]; });
+        upper.assign(ord.begin(), ord.begin() + std::max<std::size_t>(1, ord.size() / 4));
+    }
+    if (upper.size() <= kWindowSamples) {
+        h.win = upper;
+    } else {
+        for (std::size_t k = 0; k < kWindowSamples; ++k) h.win.push_back(upper[k * upper.size() / kWindowSamples]);
+    }
+    return h;
+}
+
+// FP64 builds of the heads of `heads` (into one device buffer of head rows), chunked so
+// that each chunk's rows fit kTempBytes (a single head may exceed it).
+template <class Fn>
+void for_chunks(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads, Fn fn) {
+    std::size_t k0 = 0;
+    while (k0 < heads.size()) {
+        std::size_t k1 = k0, bytes = 0;
+        while (k1 < heads.size() && k1 - k0 < 32768) {  // jobs of one launch along grid y
+            const std::size_t b = heads[k1].times.size() * entries(insts[heads[k1].inst]) * sizeof(double2);
+            if (k1 > k0 && bytes + b > kTempBytes) break;
+            bytes += b;
+            ++k1;
+        }
+        fn(k0, k1, bytes);
+        k0 = k1;
+    }
+}
+
+// Head instances (FP64, device output rows at `base` + offsets) for heads [k0, k1).
+std::vector<Tcl4Instance> head_instances(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads,
+                                         std::size_t k0, std::size_t k1, double2* base, std::vector<std::size_t>& off) {
+    std::vector<Tcl4Instance> hi;
+    off.assign(k1 - k0, 0);
+    std::size_t o = 0;
+    for (std::size_t k = k0; k < k1; ++k) {
+        const Tcl4Instance& in = insts[heads[k].inst];
+        Tcl4Instance h;
+        h.sys = in.sys;
+        h.gamma = in.gamma;
+        h.gamma_on_device = in.gamma_on_device;
+        h.Nt = in.Nt;
+        h.dt = in.dt;
+        h.tidx = heads[k].times;
+        h.out = base + o;
+        h.out_on_device = true;
+        off[k - k0] = o;
+        o += heads[k].times.size() * entries(in);
+        hi.push_back(std::move(h));
+    }
+    return hi;
+}
+
+// Device jobs of heads [k0, k1) and their index arrays, as one host image of the device
+// layout at `dev` (null: measure only).  Host outputs compare against their window rows
+// staged at `stage` (row offsets `stage_off`) and patch into `hpatch` (offsets `hpatch_off`).
+struct JobImage {
+    std::vector<unsigned char> host;
+};
+
+JobImage job_image(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads, std::size_t k0,
+                   std::size_t k1, const double2* base, const std::vector<std::size_t>& off, unsigned char* dev,
+                   const float2* stage = nullptr, const std::vector<std::size_t>* stage_off = nullptr,
+                   float2* hpatch = nullptr, const std::vector<std::size_t>* hpatch_off = nullptr) {
+    const std::size_t n = k1 - k0;
+    std::size_t bytes = n * sizeof(GuardJob);
+    std::vector<std::size_t> pos_off(n), cmp_off(n), win_off(n);
+    for (std::size_t k = 0; k < n; ++k) {
+        pos_off[k] = bytes;
+        bytes += heads[k0 + k].pos.size() * sizeof(uint32_t);
+        cmp_off[k] = bytes;
+        bytes += heads[k0 + k].win.size() * sizeof(uint32_t);
+        win_off[k] = bytes;
+        bytes += heads[k0 + k].win.size() * sizeof(uint32_t);
+    }
+    JobImage img;
+    img.host.assign(bytes, 0);
+    auto at = [&](std::size_t o) { return reinterpret_cast<const uint32_t*>(reinterpret_cast<std::uintptr_t>(dev) + o); };
+    for (std::size_t k = 0; k < n; ++k) {
+        const Head& h = heads[k0 + k];
+        const Tcl4Instance& in = insts[h.inst];
+        const bool host_out = !in.out_on_device;
+        GuardJob j;
+        j.h64 = base + off[k];
+        j.pos = at(pos_off[k]);
+        j.cmp_row = at(cmp_off[k]);
+        j.win = at(win_off[k]);
+        j.n = static_cast<uint32_t>(h.pos.size());
+        j.nwin = static_cast<uint32_t>(h.win.size());
+        j.E = static_cast<uint32_t>(entries(in));
+        std::vector<uint32_t> pos(h.pos), cmp(h.win.size());
+        if (host_out) {
+            j.out32 = hpatch ? hpatch + (*hpatch_off)[k] : nullptr;
+            j.cmp32 = stage ? stage + (*stage_off)[k] : nullptr;
+            for (std::size_t q = 0; q < pos.size(); ++q) pos[q] = static_cast<uint32_t>(q);
+            for (std::size_t q = 0; q < cmp.size(); ++q) cmp[q] = static_cast<uint32_t>(q);
+        } else {
+            j.out32 = static_cast<float2*>(in.out);
+            j.cmp32 = static_cast<const float2*>(in.out);
+            for (std::size_t q = 0; q < cmp.size(); ++q) cmp[q] = h.pos[h.win[q]];
+        }
+        std::memcpy(img.host.data() + k * sizeof(GuardJob), &j, sizeof(GuardJob));
+        if (!pos.empty()) std::memcpy(img.host.data() + pos_off[k], pos.data(), pos.size() * sizeof(uint32_t));
+        if (!cmp.empty()) std::memcpy(img.host.data() + cmp_off[k], cmp.data(), cmp.size() * sizeof(uint32_t));
+        if (!h.win.empty()) std::memcpy(img.host.data() + win_off[k], h.win.data(), h.win.size() * sizeof(uint32_t));
+    }
+    return img;
+}
+
+unsigned patch_blocks(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads, std::size_t k0,
+                      std::size_t k1) {
+    std::size_t most = 1;
+    for (std::size_t k = k0; k < k1; ++k) most = std::max(most, heads[k].pos.size() * entries(insts[heads[k].inst]));
+    return static_cast<unsigned>(std::min<std::size_t>((most + 255) / 256, 592));
+}
+
+struct Decision {
+    std::vector<Head> heads;  // final heads of the instances that need one
+};
+
+// Runs the guard loop: FP64 heads, comparison, growth.  With `patch`, accepted heads are
+// written into the outputs right away (direct calls); otherwise only the final heads are
+// returned (plans).  The FP32 results must already be in the outputs.  Comparison and
+// rounding run on the device; a host output stages its compared rows up and its patched
+// rows down (one copy per run of consecutive output rows).
+Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t st, bool patch) {
+    const double tol = g_guard_tol.load();
+    BuildOptions o64 = opt;
+    o64.fp32 = false;
+    o64.fcr_ms = nullptr;
+    std::vector<Head> pending;
+    for (std::size_t a = 0; a < insts.size(); ++a) {
+        if (insts[a].tidx.empty()) continue;
+        const uint32_t tc = t_count_of(insts[a]);
+        const uint32_t H = static_cast<uint32_t>(std::min<std::size_t>(tc, std::max<std::size_t>(kMinHead, (tc + 15) / 16)));
+        Head h = make_head(insts, a, H, tc);
+        if (!h.times.empty()) pending.push_back(std::move(h));
+    }
+    Decision dec;
+    DevMem temp, meta, sums, stage, hpatch;
+    std::vector<float2> stage_host;
+    t_stats = GuardStats{};
+    t_stats.instances = insts.size();
+    while (!pending.empty()) {
+        ++t_stats.rounds;
+        std::vector<Head> next;
+        for_chunks(insts, pending, [&](std::size_t k0, std::size_t k1, std::size_t bytes) {
+            const std::size_t n = k1 - k0;
+            temp.ensure(std::max<std::size_t>(bytes, 256));
+            std::vector<std::size_t> off;
+            double2* base = static_cast<double2*>(temp.p);
+            std::vector<Tcl4Instance> hi = head_instances(insts, pending, k0, k1, base, off);
+            tcl4_build_direct(hi, o64, st);  // synchronous
+            // host outputs: their window rows staged up, their patched rows in a device buffer
+            std::vector<std::size_t> soff(n, 0), poff(n, 0);
+            std::size_t srows = 0, prows = 0;
+            for (std::size_t k = k0; k < k1; ++k) {
+                const Head& h = pending[k];
+                const Tcl4Instance& in = insts[h.inst];
+                if (in.out_on_device) continue;
+                const std::size_t E = entries(in);
+                soff[k - k0] = srows;
+                poff[k - k0] = prows;
+                srows += h.win.size() * E;
+                prows += h.pos.size() * E;
+            }
+            if (srows) {
+                stage_host.resize(srows);
+                for (std::size_t k = k0; k < k1; ++k) {
+                    const Head& h = pending[k];
+                    const Tcl4Instance& in = insts[h.inst];
+                    if (in.out_on_device) continue;
+                    const std::size_t E = entries(in);
+                    const float2* f = static_cast<const float2*>(in.out);
+                    for (std::size_t q = 0; q < h.win.size(); ++q)
+                        std::memcpy(stage_host.data() + soff[k - k0] + q * E,
+                                    f + static_cast<std::size_t>(h.pos[h.win[q]]) * E, E * sizeof(float2));
+                }
+                stage.ensure(srows * sizeof(float2));
+                cuda_check(cudaMemcpyAsync(stage.p, stage_host.data(), srows * sizeof(float2), cudaMemcpyHostToDevice, st),
+                           "cudaMemcpyAsync(guard stage)");
+            }
+            if (prows) hpatch.ensure(prows * sizeof(float2));
+            const float2* stage_p = static_cast<const float2*>(stage.p);
+            float2* hpatch_p = static_cast<float2*>(hpatch.p);
+            meta.ensure(job_image(insts, pending, k0, k1, base, off, nullptr).host.size() + 256);
+            JobImage img = job_image(insts, pending, k0, k1, base, off, static_cast<unsigned char*>(meta.p), stage_p, &soff,
+                                     hpatch_p, &poff);
+            sums.ensure(2 * n * sizeof(double));
+            cuda_check(cudaMemcpyAsync(meta.p, img.host.data(), img.host.size(), cudaMemcpyHostToDevice, st),
+                       "cudaMemcpyAsync(guard jobs)");
+            k_guard_compare<<<static_cast<unsigned>(n), 256, 0, st>>>(static_cast<const GuardJob*>(meta.p),
+                                                                    static_cast<double*>(sums.p));
+            cuda_check(cudaGetLastError(), "k_guard_compare");
+            count_launches(1);
+            std::vector<double> s(2 * n, 0.0);
+            cuda_check(cudaMemcpyAsync(s.data(), sums.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, st),
+                       "cudaMemcpyAsync(guard sums)");
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(guard)");
+            // decide
+            std::vector<char> accept(n, 0);
+            for (std::size_t k = k0; k < k1; ++k) {
+                const double num = s[2 * (k - k0)], den = s[2 * (k - k0) + 1];
+                const bool ok = den > 0.0 ? std::sqrt(num / den) <= tol : num == 0.0;
+                const Head& h = pending[k];
+                if (ok || h.H >= h.tc) {
+                    accept[k - k0] = 1;
+                } else {
+                    const uint32_t H = static_cast<uint32_t>(std::min<std::size_t>(h.tc, 4 * static_cast<std::size_t>(h.H)));
+                    next.push_back(make_head(insts, h.inst, H, h.tc));
+                }
+            }
+            if (patch) {
+                // rejected heads patch nothing
+                for (std::size_t k = 0; k < n; ++k)
+                    if (!accept[k]) {
+                        GuardJob j;
+                        std::memcpy(&j, img.host.data() + k * sizeof(GuardJob), sizeof(GuardJob));
+                        j.n = 0;
+                        std::memcpy(img.host.data() + k * sizeof(GuardJob), &j, sizeof(GuardJob));
+                    }
+                cuda_check(cudaMemcpyAsync(meta.p, img.host.data(), n * sizeof(GuardJob), cudaMemcpyHostToDevice, st),
+                           "cudaMemcpyAsync(guard jobs)");
+                const dim3 grid(patch_blocks(insts, pending, k0, k1), static_cast<unsigned>(n));
+                k_guard_patch<<<grid, 256, 0, st>>>(static_cast<const GuardJob*>(meta.p));
+                cuda_check(cudaGetLastError(), "k_guard_patch");
+                count_launches(1);
+                // host outputs: one copy per run of consecutive output rows
+                for (std::size_t k = k0; k < k1; ++k) {
+                    const Head& h = pending[k];
+                    const Tcl4Instance& in = insts[h.inst];
+                    if (!accept[k - k0] || in.out_on_device) continue;
+                    const std::size_t E = entries(in);
+                    float2* f = static_cast<float2*>(in.out);
+                    const float2* src = hpatch_p + poff[k - k0];
+                    std::size_t q = 0;
+                    while (q < h.pos.size()) {
+                        std::size_t r = q + 1;
+                        while (r < h.pos.size() && h.pos[r] == h.pos[r - 1] + 1) ++r;
+                        cuda_check(cudaMemcpyAsync(f + static_cast<std::size_t>(h.pos[q]) * E, src + q * E,
+                                                   (r - q) * E * sizeof(float2), cudaMemcpyDeviceToHost, st),
+                                   "cudaMemcpyAsync(guard rows)");
+                        q = r;
+                    }
+                }
+                cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(guard patch)");
+            }
+            for (std::size_t k = k0; k < k1; ++k)
+                if (accept[k - k0]) {
+                    const Head& h = pending[k];
+                    ++t_stats.heads;
+                    t_stats.head_rows += h.times.size();
+                    t_stats.rows += insts[h.inst].tidx.size();
+                    if (h.H >= h.tc) ++t_stats.full;
+                    dec.heads.push_back(h);
+                }
+        });
+        pending.swap(next);
+    }
+    return dec;
+}
+
+}  // namespace
+
+void set_fp32_guard(double tol) { g_guard_tol.store(tol > 0.0 ? tol : 0.0); }
+GuardStats fp32_guard_stats() { return t_stats; }
+double fp32_guard() { return g_guard_tol.load(); }
+
+void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream) {
+    tcl4_build_direct(insts, opt, stream);
+    t_stats = GuardStats{};
+    if (!opt.fp32 || g_guard_tol.load() <= 0.0) return;
+    run_guard(insts, opt, stream ? stream : default_stream(), true);
+}
+
+Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt) {
+    Tcl4Plan* plan = plan_create_direct(insts, opt);
+    t_stats = GuardStats{};
+    if (!opt.fp32 || g_guard_tol.load() <= 0.0) return plan;
+    try {
+        // the FP32 results of the plan's inputs (written by the caller's streams: wait for the
+        // device first), then the guard loop on them
+        cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize(plan guard)");
+        cudaStream_t st = default_stream();
+        plan_execute(plan, st);
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(plan guard)");
+        Decision dec = run_guard(insts, opt, st, false);
+        // the guard's direct builds grew this thread's transient buffers; the plans below
+        // size theirs from the free memory
+        release_workspace();
+        if (dec.heads.empty()) return plan;
+        // the heads as FP64 plans over one shared buffer of head rows, each followed by its patch
+        BuildOptions o64 = opt;
+        o64.fp32 = false;
+        o64.fcr_ms = nullptr;
+        struct Part {
+            Tcl4Plan* plan = nullptr;
+            std::size_t jobs = 0;
+            unsigned blocks = 0;
+            std::size_t meta_off = 0;
+        };
+        struct TailState {
+            DevMem rows, meta, work;
+            std::vector<Part> parts;
+            ~TailState() {
+                for (auto& p : parts) plan_destroy(p.plan);
+            }
+        };
+        auto tail = std::make_shared<TailState>();
+        std::size_t most = 256, meta_total = 0;
+        std::vector<JobImage> imgs;
+        std::vector<std::pair<std::size_t, std::size_t>> ranges;
+        for_chunks(insts, dec.heads, [&](std::size_t k0, std::size_t k1, std::size_t bytes) {
+            most = std::max(most, bytes);
+            ranges.emplace_back(k0, k1);
+        });
+        tail->rows.ensure(most);
+        double2* base = static_cast<double2*>(tail->rows.p);
+        // job images: measured first, then placed in one metadata buffer
+        std::vector<std::vector<std::size_t>> offs(ranges.size());
+        std::vector<std::vector<Tcl4Instance>> his(ranges.size());
+        for (std::size_t c = 0; c < ranges.size(); ++c) {
+            his[c] = head_instances(insts, dec.heads, ranges[c].first, ranges[c].second, base, offs[c]);
+            JobImage im = job_image(insts, dec.heads, ranges[c].first, ranges[c].second, base, offs[c], nullptr);
+            meta_total += (im.host.size() + 255) / 256 * 256;
+        }
+        tail->meta.ensure(meta_total + 256);
+        // one transient buffer for every head plan (they run one after another)
+        std::size_t work_need = 256;
+        for (std::size_t c = 0; c < ranges.size(); ++c) work_need = std::max(work_need, plan_work_bytes(his[c], o64));
+        tail->work.ensure(work_need);
+        uint64_t kernels = 0;
+        std::size_t moff = 0;
+        for (std::size_t c = 0; c < ranges.size(); ++c) {
+            unsigned char* dev = static_cast<unsigned char*>(tail->meta.p) + moff;
+            JobImage im = job_image(insts, dec.heads, ranges[c].first, ranges[c].second, base, offs[c], dev);
+            cuda_check(cudaMemcpy(dev, im.host.data(), im.host.size(), cudaMemcpyHostToDevice), "cudaMemcpy(guard jobs)");
+            Part p;
+            p.plan = plan_create_direct(his[c], o64, tail->work.p, tail->work.cap);
+            p.jobs = ranges[c].second - ranges[c].first;
+            p.blocks = patch_blocks(insts, dec.heads, ranges[c].first, ranges[c].second);
+            p.meta_off = moff;
+            tail->parts.push_back(p);
+            kernels += plan_kernels(p.plan) + 1;
+            moff += (im.host.size() + 255) / 256 * 256;
+        }
+        plan_set_tail(plan, [tail](cudaStream_t s) {
+            for (const Part& p : tail->parts) {
+                plan_execute(p.plan, s);
+                const GuardJob* jobs = reinterpret_cast<const GuardJob*>(static_cast<unsigned char*>(tail->meta.p) + p.meta_off);
+                k_guard_patch<<<dim3(p.blocks, static_cast<unsigned>(p.jobs)), 256, 0, s>>>(jobs);
+                cuda_check(cudaGetLastError(), "k_guard_patch");
+                count_launches(1);
+            }
+        }, kernels);
+        return plan;
+    } catch (...) {
+        plan_destroy(plan);
+        throw;
+    }
+}
+
+}  // namespace taco

@@ -12,15 +12,20 @@
 // The array exists once per GPU that loads the library and is held until the process
 // exits.  Its host-side name is not a device address: host code only ever uses the
 // address returned by cudaGetSymbolAddress, looked up once per device (with that device
-// current) on the first call made on that device -- make that first call before any
-// stream capture.  All calls share the array: calls whose work overlaps on the GPU (two
-// host threads, or two streams) race on it.  Nothing in the array needs to start at zero:
-// every buffer is written before it is read within a call.  Host-side metadata lives in
+// current) on the first call made on that device.  All calls share the array: calls whose
+// work overlaps on the GPU (two host threads, or two streams) race on it.  Nothing in the
+// array needs to start at zero: every buffer is written before it is read within a call.  Host-side metadata lives in
 // ordinary heap vectors for the duration of the call and is copied with cudaMemcpyAsync
-// from pageable memory.
+// from pageable memory, and the call synchronises its stream before it returns; a call on a
+// stream that is being captured is rejected before any work.  gamma and the output must
+// be device (or managed) memory of the current device, aligned for their complex type;
+// anything else is rejected before any launch.  The FFT length is the power of two
+// next_pow2(max(2 t_count - 1, pad * t_count)) (the allocating path also uses 3*2^k and
+// 5*2^k lengths; the results agree to rounding).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -121,16 +126,17 @@ void run(const SystemDesc& sys, const double2* gamma, std::size_t Nt, double dt,
     CoefTable coef;
     build_coef_table(sys.N, nf, sys.p2f.data(), sys.ops.data(), sys.num_ops, coef);
     const std::size_t nnz = coef.src.size();
-    // schedule (same tables the tuned paths use)
+    // schedule: the tuned tile sizes, shrunk like the allocating path's to fit shared memory
     const Tuning tune = get_tuning(L, std::is_same<R, float>::value);
-    const int log2c = ilog2(static_cast<std::size_t>(std::max(1, std::min(N2, tune.col_tile / N1))));
-    const int col_threads = (N1 << log2c) / 8;
-    const std::size_t col_smem = static_cast<std::size_t>(padded_size<C>(N1 << log2c)) * sizeof(C);
-    const unsigned col_grid = static_cast<unsigned>(N2 >> log2c);
-    const int log2r = ilog2(static_cast<std::size_t>(std::max(1, std::min(N1, tune.row_tile / N2))));
-    const int row_threads = (N2 << log2r) / 8;
-    const std::size_t row_smem = 2 * static_cast<std::size_t>(padded_size<C>(N2 << log2r)) * sizeof(C);
-    const unsigned row_grid = static_cast<unsigned>(N1 >> log2r);
+    FftPlan<C> shape{};
+    shape.L = L;
+    shape.L1 = L1;
+    shape.L2 = L2;
+    shape.R = 1;
+    const Geometry geo = geometry(shape, tune.col_tile, tune.row_tile);
+    const int log2c = geo.log2c, col_threads = geo.col_threads, log2r = geo.log2r, row_threads = geo.row_threads;
+    const std::size_t col_smem = geo.col_smem, row_smem = geo.row_smem;
+    const unsigned col_grid = geo.col_grid, row_grid = geo.row_grid;
     const int inv_rows = static_cast<int>((t_count + N2 - 1) / N2);
     const bool inv_dft = inv_rows <= std::min(tune.inv_dft_rows, INV_DFT_MAXR);
 
@@ -173,7 +179,8 @@ void run(const SystemDesc& sys, const double2* gamma, std::size_t Nt, double dt,
                                    " bytes of scratch, above the fixed TACO_NOALLOC_SCRATCH_BYTES = " +
                                    std::to_string(static_cast<std::size_t>(TACO_NOALLOC_SCRATCH_BYTES)) +
                                    " (reduce max(tidx) or the number of requested times)");
-    const std::size_t Q = std::min<std::size_t>({(TACO_NOALLOC_SCRATCH_BYTES - fixed) / per_tri, nf3, 65535});
+    // the inverse pass launches 2 Q CTAs along y: Q <= 32767 keeps that within 65535
+    const std::size_t Q = std::min<std::size_t>({(TACO_NOALLOC_SCRATCH_BYTES - fixed) / per_tri, nf3, 32767});
     Carve cv{scratch_address()};
     place(cv, Q, &tw, &spec, &scratch, &conv, &v, &dtm, &dou, &drp, &dsrc, &dcoef, &cjd, &rjd, &ijd, &sjd, &kjd);
 
@@ -299,13 +306,43 @@ void run(const SystemDesc& sys, const double2* gamma, std::size_t Nt, double dt,
     }
     k_scan_assemble<R, SCAN_ITEMS, 3><<<static_cast<unsigned>(nf3), SCAN_THREADS, 0, st>>>(sjd);
     cuda_check(cudaGetLastError(), "k_scan_assemble");
-    const int OT = std::max(1, std::min(128, static_cast<int>((48 * 1024) / (E * sizeof(C)))));
-    const std::size_t csmem = static_cast<std::size_t>(OT) * E * sizeof(C);
-    smem_attr(k_contract<R>, csmem);
-    k_contract<R><<<dim3(static_cast<unsigned>((T + OT - 1) / OT), 1), 256, csmem, st>>>(kjd, OT);
-    cuda_check(cudaGetLastError(), "k_contract");
+    if (E * sizeof(C) <= 48 * 1024) {
+        // several output times per CTA, their L4 matrices staged in shared memory
+        const int OT = std::max(1, std::min(128, static_cast<int>((48 * 1024) / (E * sizeof(C)))));
+        const std::size_t csmem = static_cast<std::size_t>(OT) * E * sizeof(C);
+        k_contract<R><<<dim3(static_cast<unsigned>((T + OT - 1) / OT), 1), 256, csmem, st>>>(kjd, OT);
+        cuda_check(cudaGetLastError(), "k_contract");
+    } else {
+        // large L4 matrices: 32 x 32 (time, entry) tiles in static shared memory
+        const dim3 grid(static_cast<unsigned>((T + CONTRACT_TILE - 1) / CONTRACT_TILE),
+                        static_cast<unsigned>((E + CONTRACT_TILE - 1) / CONTRACT_TILE), 1);
+        k_contract_tiles<R><<<grid, CONTRACT_TILE_THREADS, 0, st>>>(kjd);
+        cuda_check(cudaGetLastError(), "k_contract_tiles");
+    }
     // the host vectors above are sources of the pending copies: finish before returning
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(no-alloc)");
+}
+
+// A caller's buffer must be device (or managed) memory of the current device, aligned for
+// its complex type: a host address handed to the kernels would fault instead of failing.
+void require_device_buffer(const void* p, std::size_t align, const char* what) {
+    if (reinterpret_cast<std::uintptr_t>(p) % align != 0)
+        throw Error(kInvalidArgument, std::string("no-alloc build: ") + what + " is not " + std::to_string(align) +
+                                          "-byte aligned");
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();  // clear the sticky-free error state of the query
+        throw Error(kInvalidArgument, std::string("no-alloc build: ") + what + " is not a CUDA allocation (" +
+                                          cudaGetErrorString(e) + ")");
+    }
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+        throw Error(kInvalidArgument, std::string("no-alloc build: ") + what + " must be device memory");
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (a.type == cudaMemoryTypeDevice && a.device != dev)
+        throw Error(kInvalidArgument, std::string("no-alloc build: ") + what + " is on device " +
+                                          std::to_string(a.device) + ", not the current device " + std::to_string(dev));
 }
 
 }  // namespace
@@ -314,6 +351,13 @@ void noalloc_tcl4_build(const SystemDesc& sys, const double2* gamma, std::size_t
                         const std::vector<uint32_t>& tidx, bool fp32, std::size_t pad_factor, void* out,
                         cudaStream_t stream) {
     if (!gamma || !out) throw Error(kInvalidArgument, "no-alloc build: null gamma or output");
+    // metadata is copied from pageable host memory and the stream is synchronised before
+    // the call returns, neither of which a capturing stream accepts: checked before any
+    // other CUDA call
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cuda_check(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing");
+    if (cap != cudaStreamCaptureStatusNone)
+        throw Error(kInvalidArgument, "no-alloc build: the stream is being captured; call it outside stream capture");
     if (Nt == 0) throw Error(kInvalidArgument, "empty gamma_series");
     if (Nt >= (std::size_t(1) << 31)) throw Error(kOverflow, "Nt too large");
     if (!(dt > 0.0)) throw Error(kInvalidArgument, "dt must be > 0");
@@ -331,6 +375,8 @@ void noalloc_tcl4_build(const SystemDesc& sys, const double2* gamma, std::size_t
     if (tidx.empty()) throw Error(kInvalidArgument, "no-alloc build: no time indices");
     for (uint32_t t : tidx)
         if (t >= Nt) throw Error(kOutOfRange, "time_index out of range");
+    require_device_buffer(gamma, sizeof(double2), "gamma");
+    require_device_buffer(out, fp32 ? sizeof(float2) : sizeof(double2), "L4_out");
     if (fp32) run<float>(sys, gamma, Nt, dt, tidx, pad_factor, out, stream);
     else run<double>(sys, gamma, Nt, dt, tidx, pad_factor, out, stream);
 }

@@ -32,6 +32,21 @@ def test_pad_factor_roundtrip():
     assert tb.get_fcr_fft_pad_factor() == 0
 
 
+def test_fp32_guard_setting_roundtrip():
+    old = tb.fp32_guard()
+    assert old == pytest.approx(5e-7)
+    tb.set_fp32_guard(1e-6)
+    assert tb.fp32_guard() == pytest.approx(1e-6)
+    tb.set_fp32_guard(0.0)  # off
+    assert tb.fp32_guard() == 0.0
+    with pytest.raises(ValueError):
+        tb.set_fp32_guard(-1.0)
+    with pytest.raises(ValueError):
+        tb.set_fp32_guard(float("nan"))
+    tb.set_fp32_guard(old)
+    assert tb.fp32_guard() == old
+
+
 def _synthetic_system():
     g = np.load(os.path.join(GOLD, "synthetic_gamma.npz"))
     s = tb.System.from_arrays(int(g["N"]), g["omegas"], g["p2f"], list(g["ops"]), mirror=g["mirror"])

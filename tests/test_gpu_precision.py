@@ -1,0 +1,144 @@
+"""The FP32 form on long series: the precision guard against FP64 and the oracle.
+
+L4 cancels heavily among the F/C/R values it is formed from (most at early times, and at all
+times for slowly decaying long series), so an all-FP32 build misses 1e-6 there; the guard
+rebuilds the leading times in FP64 where the FP32 result falls short.  Tolerance: 1e-6
+relative (Frobenius) over the whole series and over every dyadic window of requested times.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import taco_b200 as tb
+from cases import relerr
+
+pytestmark = pytest.mark.gpu
+
+# The batching form's worst instance in the round-to-round comparisons: d = 2 (GUE H with a
+# Bohr frequency of 0.21), N = 2^18 (FFT 2^19), Ohmic alpha 0.090, wc 12.71, beta 0.706.
+H_SLOW = np.array([[-0.6222598195398994, 0.04722114315967549 - 0.09390165050543907j],
+                   [0.04722114315967548 + 0.09390165050543912j, -0.5034041147598882]])
+A_SLOW = np.array([[0.3728503648055045, 0.8568328150495468 - 0.2491112173205089j],
+                   [0.8568328150495468 + 0.2491112173205089j, -0.2695835680327047]])
+
+
+def c4_case(H, A, logN, alpha, wc, beta):
+    """A batching-form instance: dt = 10 / (N wc), every 8th time index."""
+    osys = oracle.System(H, [A])
+    N = 1 << logN
+    dt = 10.0 / (N * wc)
+    _, C = oracle.bcf_fft(N, dt, oracle.J_OHMIC, [alpha, wc], beta)
+    G = oracle.gamma_trapz(C, dt, osys.omegas)
+    s = tb.System.from_arrays(osys.N, osys.omegas, osys.pair_to_freq, osys.A_eig, mirror=osys.mirror)
+    return osys, s, G, dt, np.arange(0, N, 8)
+
+
+def gue(d, rng):
+    X = rng.normal(0, np.sqrt(1 / (2 * d)), (d, d)) + 1j * rng.normal(0, np.sqrt(1 / (2 * d)), (d, d))
+    H = np.triu(X, 1)
+    H = H + H.conj().T + np.diag(rng.normal(0, np.sqrt(1 / d), d))
+    Y = rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
+    A = np.triu(Y, 1)
+    A = A + A.conj().T + np.diag(rng.normal(size=d))
+    return H, A / np.linalg.norm(A, 2)
+
+
+def window_errors(a, b, tidx):
+    """Relative Frobenius error over the requested times in [0, 64) and [2^k, 2^(k+1)), k >= 6."""
+    out = []
+    lo = 0
+    hi = 64
+    while lo <= tidx.max():
+        m = (tidx >= lo) & (tidx < hi)
+        if m.any():
+            out.append((lo, relerr(a[m], b[m])))
+        lo, hi = hi, 2 * hi
+    return out
+
+
+def build(s, g, dt, tidx, precision, guard=None):
+    import torch
+    old = tb.fp32_guard()
+    if guard is not None:
+        tb.set_fp32_guard(guard)
+    try:
+        out = tb.build_TCL4_generator_batch(s, g, dt, tidx, precision=precision)
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+    finally:
+        tb.set_fp32_guard(old)
+
+
+def test_guard_long_d2_series_meets_1e6_everywhere():
+    import torch
+    osys, s, G, dt, tidx = c4_case(H_SLOW, A_SLOW, 18, 0.0903971416575698, 12.713639017035707, 0.7059676185188037)
+    g = torch.from_numpy(G).cuda()
+    L64 = build(s, g, dt, tidx, "fp64")
+    raw = build(s, g, dt, tidx, "fp32", guard=0.0)
+    assert relerr(raw, L64) > 1e-6  # the unguarded FP32 build misses the tolerance here
+    L32 = build(s, g, dt, tidx, "fp32")
+    assert L32.dtype == np.complex64
+    assert relerr(L32, L64) <= 1e-6
+    for lo, e in window_errors(L32, L64, tidx):
+        assert e <= 1e-6, (lo, e)
+    # the first 2049 samples against the oracle's Direct method
+    k = tidx <= 2048
+    ref = oracle.tcl4_build_batch(osys.N, osys.nf, osys.omegas, osys.mirror, osys.p2f_colmajor(), osys.ops_colmajor(),
+                                  np.ascontiguousarray(G[:, :2049]), dt, tidx=tidx[k], method=oracle.FCR_DIRECT)
+    assert relerr(L32[k], ref) <= 1e-6
+    assert relerr(L64[k], ref) <= 1e-10
+
+
+def test_guard_d8_series_meets_1e6_everywhere():
+    import torch
+    H, A = gue(8, np.random.default_rng(808))
+    osys, s, G, dt, tidx = c4_case(H, A, 16, 0.0591096182596629, 1.0906887749364023, 4.20150566069442)
+    g = torch.from_numpy(G).cuda()
+    L64 = build(s, g, dt, tidx, "fp64")
+    L32 = build(s, g, dt, tidx, "fp32")
+    assert relerr(L32, L64) <= 1e-6
+    for lo, e in window_errors(L32, L64, tidx):
+        assert e <= 1e-6, (lo, e)
+
+
+def test_guard_plan_and_host_outputs_match_direct_device_call():
+    """Plans choose their FP64 heads at creation and replay them; host outputs are patched on
+    the host.  All three give the same FP32 rows."""
+    import torch
+    cases = [c4_case(H_SLOW, A_SLOW, 15, 0.09, wc, 0.7) for wc in (1.5, 12.7)]
+    H, A = gue(3, np.random.default_rng(33))
+    cases.append(c4_case(H, A, 14, 0.05, 4.0, 2.0))
+    inst_dev = [(s, torch.from_numpy(G).cuda(), dt, tidx) for _, s, G, dt, tidx in cases]
+    direct = [x.cpu().numpy() for x in tb.build_instances(inst_dev, precision="fp32")]
+    host = tb.build_instances([(s, G, dt, tidx) for _, s, G, dt, tidx in cases], precision="fp32")
+    plan = tb.Tcl4Plan(inst_dev, precision="fp32")
+    for _ in range(2):
+        res = plan.run()
+    torch.cuda.synchronize()
+    for a, b, c in zip(direct, host, res):
+        assert np.array_equal(a, b)
+        assert np.array_equal(a, c.cpu().numpy())
+    plan.close()
+    for (osys, s, G, dt, tidx), a, x in zip(cases, direct, inst_dev):
+        ref = build(s, x[1], dt, tidx, "fp64")
+        for lo, e in window_errors(a, ref, tidx):
+            assert e <= 1e-6, (lo, e)
+
+
+def test_guard_setting_and_unsorted_times():
+    import torch
+    old = tb.fp32_guard()
+    assert old == pytest.approx(5e-7)
+    with pytest.raises(ValueError):
+        tb.set_fp32_guard(-1.0)
+    osys, s, G, dt, tidx = c4_case(H_SLOW, A_SLOW, 14, 0.09, 3.0, 0.7)
+    rng = np.random.default_rng(1)
+    tid = rng.permutation(tidx)[: tidx.size // 2]
+    tid[:3] = tid[3]  # repeated times
+    g = torch.from_numpy(G).cuda()
+    L64 = build(s, g, dt, tid, "fp64")
+    L32 = build(s, g, dt, tid, "fp32")
+    assert relerr(L32, L64) <= 1e-6
+    for lo, e in window_errors(L32, L64, tid):
+        assert e <= 1e-6, (lo, e)
+    assert tb.fp32_guard() == old
