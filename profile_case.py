@@ -28,6 +28,7 @@ def main():
     ap.add_argument("--tmax", type=int, default=10000)
     ap.add_argument("--full-length", action="store_true")
     ap.add_argument("--guard", type=float, default=None)
+    ap.add_argument("--fused", action="store_true", help="the fused single-CTA F/C/R path where it fits")
     args = ap.parse_args()
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
@@ -41,6 +42,8 @@ def main():
     inst = [(s, g, args.dt, tidx) for s, g in zip(systems, gammas)]
     if args.guard is not None:
         tb.set_fp32_guard(args.guard)
+    if args.fused:
+        tb.set_fused_conv(True)
     torch.cuda.synchronize()
     for _ in range(args.reps):
         t0 = time.perf_counter()

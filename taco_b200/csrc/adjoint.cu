@@ -1151,14 +1151,6 @@ __global__ void __launch_bounds__(FZ_THREADS, 1) k_fcr_adj_corr_fft(const FcrAdj
     }
 }
 
-__global__ void k_adj_fill_roots(double2* out, uint32_t n) {
-    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= n) return;
-    double s, c;
-    sincospi(-2.0 * static_cast<double>(m) / static_cast<double>(n), &s, &c);
-    out[m] = make_double2(c, s);
-}
-
 // FFT length of the correlations for T samples: the smallest 2^k, 3 * 2^k or 5 * 2^k >= 2 T - 1
 // whose working array fits one CTA (0: none, the direct kernel runs).
 int adj_fft_length(std::size_t T) {
@@ -1527,8 +1519,11 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
                 probe.take<double2>(5 * nf3 * T);     // G1, G2F, G2C, G2R, A2
                 probe.take<double>(nf3 * (1 + ntiles));
             }
-            if (fftN) {  // roots, per-job spectra, their jobs
-                probe.take<double2>(fftN);
+            if (fftN) {  // twiddle tables, per-job spectra, their jobs
+                FzPlan<double2> fp{};
+                fp.N = fftN;
+                fz_stages(fftN, 8, fp.rad, fp.nst);
+                probe.take<double2>(std::max<std::size_t>(1, fz_table_layout(fp)));
                 for (std::size_t a = 0; a < idx.size(); ++a) probe.take<double2>((2 * nf + 4 * nf3) * fftN);
                 probe.take<AdjFftSpectra>(idx.size());
                 probe.take<AdjSpecJob>(idx.size() * (2 * nf + 4 * nf3));
@@ -1617,8 +1612,13 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
         AdjFftSpectra* dspec = nullptr;
         AdjSpecJob* dsjobs = nullptr;
         std::size_t nspec_jobs = 0;
+        FzPlan<double2> fplan{};
+        std::size_t ftab = 0;
         if (fftN) {
-            roots = cv.take<double2>(fftN);
+            fplan.N = fftN;
+            fz_stages(fftN, 8, fplan.rad, fplan.nst);
+            ftab = std::max<std::size_t>(1, fz_table_layout(fplan));
+            roots = cv.take<double2>(ftab);
             std::vector<AdjFftSpectra> spv(idx.size());
             std::vector<AdjSpecJob> sjobs;
             const std::size_t N = static_cast<std::size_t>(fftN);
@@ -1653,8 +1653,10 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
                        "adj fft jobs");
             // the host vectors above are copy sources: finish before they go out of scope
             cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(adj fft jobs)");
-            k_adj_fill_roots<<<static_cast<unsigned>((fftN + 255) / 256), 256, 0, st>>>(roots, static_cast<uint32_t>(fftN));
-            launched("k_adj_fill_roots");
+            fplan.tw = roots;
+            k_fz_fill_tables<double2><<<static_cast<unsigned>((ftab + 255) / 256), 256, 0, st>>>(
+                roots, fplan, static_cast<uint32_t>(ftab));
+            launched("k_fz_fill_tables");
         }
         std::memcpy(image.data() + (reinterpret_cast<char*>(dfj) - cv.base), fj.data(), fj.size() * sizeof(FcrAdjJob));
         std::memcpy(image.data() + (reinterpret_cast<char*>(dgbar) - cv.base), gbar.data(), gbar.size() * sizeof(double2*));
@@ -1681,10 +1683,7 @@ void tcl4_adjoint(const std::vector<Tcl4AdjointJob>& jobs, cudaStream_t st) {
                                                                                     jobs[idx[0]].dt);
         launched("k_fcr_adj_scan");
         if (fftN) {
-            FzPlan<double2> fp{};
-            fp.N = fftN;
-            fz_stages(fftN, 8, fp.rad, fp.nst);
-            fp.tw = roots;
+            const FzPlan<double2> fp = fplan;
             const std::size_t fsm = fz_smem<double2>(fftN);
             raise_smem_limit(reinterpret_cast<const void*>(&k_adj_series_spectrum), fsm);
             raise_smem_limit(reinterpret_cast<const void*>(&k_fcr_adj_corr_fft), fsm);

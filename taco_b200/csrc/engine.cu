@@ -277,7 +277,7 @@ FftPlan<cplx_t<R>> get_plan(Workspace& ws, int L, int Rf, cudaStream_t st) {
 }
 
 // Fused-path plan of length N: its stage list and the table of N-th roots.
-std::atomic<int> g_fused{1};
+std::atomic<int> g_fused{0};
 
 template <class R>
 FzPlan<cplx_t<R>> get_fz_plan(Workspace& ws, int N, cudaStream_t st) {
@@ -286,13 +286,14 @@ FzPlan<cplx_t<R>> get_fz_plan(Workspace& ws, int N, cudaStream_t st) {
     FzPlan<C> p{};
     p.N = N;
     if (!fz_stages(N, fp32 ? 16 : 8, p.rad, p.nst)) throw Error(kRuntime, "fused path: unsupported FFT length");
+    const std::size_t entries = fz_table_layout(p);
     auto& slot = ws.fz_tables[{N, fp32 ? 1 : 0}];
     if (!slot) {
         auto buf = std::make_unique<DeviceBuffer>();
-        buf->ensure(static_cast<std::size_t>(N) * sizeof(C));
-        k_fill_twiddle<C><<<static_cast<unsigned>((N + 255) / 256), 256, 0, st>>>(static_cast<C*>(buf->p),
-                                                                              static_cast<uint32_t>(N), static_cast<double>(N));
-        cuda_check(cudaGetLastError(), "k_fill_twiddle(fused)");
+        buf->ensure(std::max<std::size_t>(1, entries) * sizeof(C));
+        k_fz_fill_tables<C><<<static_cast<unsigned>((entries + 255) / 256 + 1), 256, 0, st>>>(
+            static_cast<C*>(buf->p), p, static_cast<uint32_t>(entries));
+        cuda_check(cudaGetLastError(), "k_fz_fill_tables");
         g_launches.fetch_add(1);
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(twiddles)");
         slot = std::move(buf);
@@ -1124,16 +1125,20 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     if (!staging_buf) cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(meta)");
 
     // ---- launches ----
-    const ColFn<R> fwd_col = fwd_col_fn<R>(plan.R, plan.L1, g.log2c);
-    const InvFn<R> inv_col = inv_col_fn<R>(plan.R, plan.L1, g.log2c);
-    const RowFn<R> row = row_fn<R>(plan.L2, g.log2r);
+    // the four-step kernels (none on the fused path, whose mixed lengths may have no
+    // column kernel)
+    const ColFn<R> fwd_col = G.fused ? nullptr : fwd_col_fn<R>(plan.R, plan.L1, g.log2c);
+    const InvFn<R> inv_col = G.fused ? nullptr : inv_col_fn<R>(plan.R, plan.L1, g.log2c);
+    const RowFn<R> row = G.fused ? nullptr : row_fn<R>(plan.L2, g.log2r);
     // 256-point rows: one warp per row with the transform in registers
     const bool row_warp = plan.L2 == 8;
     const int n_rows = plan.R << plan.L1;  // N1
     const unsigned wrow_grid = static_cast<unsigned>((n_rows + WROW_WARPS - 1) / WROW_WARPS);
-    set_smem(fwd_col, g.col_smem);
-    set_smem(inv_col, g.col_smem);
-    set_smem(row, g.row_smem);
+    if (!G.fused) {
+        set_smem(fwd_col, g.col_smem);
+        set_smem(inv_col, g.col_smem);
+        set_smem(row, g.row_smem);
+    }
     int maxE = 0, maxS = 0;
     std::size_t maxNnz = 1;
     for (auto* u : units) {
@@ -2063,7 +2068,9 @@ Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOption
     cuda_check(cudaGetDevice(&plan->device), "cudaGetDevice");
     cuda_check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate(plan)");
     Workspace& ws = workspace();
-    const std::size_t budget = work_budget();
+    // a lent buffer is the budget (the caller sized it for these instances); else the
+    // share of the free memory
+    const std::size_t budget = ext_work ? ext_cap : work_budget();
     std::vector<std::vector<WorkUnit*>> groups =
         opt.fp32 ? plan_units<float>(insts, metas, budget, plan->units) : plan_units<double>(insts, metas, budget, plan->units);
     // one transient buffer shared by the groups (they run in order on the plan's stream),

@@ -18,8 +18,8 @@
 // of length m = M / RAD: y_p = sum_q x[j + q m] w_RAD^{pq}, times w_M^{pj}, written back
 // to j + p m (every butterfly reads and writes the same slots, so a stage needs no second
 // buffer).  The odd radix (3 or 5) comes first, so every later m is a power of two.
-// Twiddles come from one table of N-th roots; radix-16 stages load six of its entries and
-// form the other nine as single products.  The two halves of a triple repeat the forward
+// Twiddles come from per-stage tables laid out [p - 1][j], so that for one p consecutive
+// butterflies read consecutive entries (coalesced), each entry evaluated directly in FP64.  The two halves of a triple repeat the forward
 // transform (one more transform per triple than the four-step path) so that one
 // 20480-point FP32 array is all a CTA holds.
 #pragma once
@@ -37,9 +37,11 @@ constexpr int FZ_ITEMS = 2;  // samples per thread per scan tile
 template <class C>
 struct FzPlan {
     int N;
-    int nst;                   // stages of the forward transform
-    int rad[FZ_MAX_STAGES];    // radix of each stage (odd radix first)
-    const C* tw;               // exp(-2 pi i m / N), m < N
+    int nst;                    // stages of the forward transform
+    int rad[FZ_MAX_STAGES];     // radix of each stage (odd radix first)
+    int twoff[FZ_MAX_STAGES];   // offset of each stage's twiddles in tw
+    const C* tw;                // per stage s (block length M, sub-block m): w_M^(p j) at
+                                // twoff[s] + (p - 1) m + j, p = 1..rad-1, j < m
 };
 
 // Shared memory of the fused kernels: the padded working array and the scan scratch.
@@ -74,6 +76,42 @@ inline bool fz_stages(int N, int max_radix, int* rad, int& nst) {
     }
     if (p > 1) rad[nst++] = p;
     return nst <= FZ_MAX_STAGES;
+}
+
+// Offsets of the per-stage twiddle tables; returns the number of entries.  A stage's table
+// is [p - 1][j]: for one p, consecutive butterflies j read consecutive entries.
+template <class C>
+inline std::size_t fz_table_layout(FzPlan<C>& p) {
+    std::size_t off = 0;
+    int M = p.N;
+    for (int s = 0; s < p.nst; ++s) {
+        const int m = M / p.rad[s];
+        p.twoff[s] = static_cast<int>(off);
+        off += static_cast<std::size_t>(p.rad[s] - 1) * m;
+        M = m;
+    }
+    return off;
+}
+
+// (stage block length M, p, j) of table entry e, for filling the tables.
+template <class C>
+__host__ __device__ inline void fz_table_entry(const FzPlan<C>& p, std::size_t e, int& M, int& pp, int& j) {
+    M = p.N;
+    for (int s = 0; s < p.nst; ++s) {
+        const int m = M / p.rad[s];
+        const std::size_t end = (s + 1 < p.nst) ? static_cast<std::size_t>(p.twoff[s + 1])
+                                                : static_cast<std::size_t>(p.twoff[s]) + static_cast<std::size_t>(p.rad[s] - 1) * m;
+        if (e < end) {
+            const std::size_t k = e - p.twoff[s];
+            pp = static_cast<int>(k / m) + 1;
+            j = static_cast<int>(k % m);
+            return;
+        }
+        M = m;
+    }
+    M = 1;
+    pp = 0;
+    j = 0;
 }
 
 // w16^e constants (forward sign), e = n2 * k1 in {0, 1, 2, 3, 4, 6, 9}
@@ -130,48 +168,31 @@ __host__ __device__ __forceinline__ void fz_dft(C* x) {
     else dft16<C, INV>(x);
 }
 
-// The RAD - 1 twiddles w_N^(p e), p = 1..RAD-1, of one butterfly (e = j * N / M).
+// The RAD - 1 twiddles w_M^(p j), p = 1..RAD-1, of one butterfly, from its stage's table
+// ([p - 1][j], m entries per p).
 template <class C, int RAD>
-__host__ __device__ __forceinline__ void fz_twiddles(const C* __restrict__ tw, int e, C* w) {
-    if constexpr (RAD == 16) {
-        const C w1 = tw[e], w2 = tw[2 * e], w3 = tw[3 * e], w4 = tw[4 * e], w8 = tw[8 * e], w12 = tw[12 * e];
-        w[1] = w1;
-        w[2] = w2;
-        w[3] = w3;
-        w[4] = w4;
-        w[5] = cmul(w4, w1);
-        w[6] = cmul(w4, w2);
-        w[7] = cmul(w4, w3);
-        w[8] = w8;
-        w[9] = cmul(w8, w1);
-        w[10] = cmul(w8, w2);
-        w[11] = cmul(w8, w3);
-        w[12] = w12;
-        w[13] = cmul(w12, w1);
-        w[14] = cmul(w12, w2);
-        w[15] = cmul(w12, w3);
-    } else {
+__host__ __device__ __forceinline__ void fz_twiddles(const C* __restrict__ tw, int j, int m, C* w) {
 #pragma unroll
-        for (int p = 1; p < RAD; ++p) w[p] = tw[p * e];
-    }
+    for (int p = 1; p < RAD; ++p) w[p] = tw[(p - 1) * m + j];
 }
 
 // One stage on blocks of length M (m = M / RAD a power of two, log2 lm), butterflies
-// tid, tid + nthr, ...  Forward: DFT then twiddles; inverse: conjugate twiddles then DFT.
+// tid, tid + nthr, ...; tw is the stage's table.  Forward: DFT then twiddles; inverse:
+// conjugate twiddles then DFT.
 template <class C, int RAD, bool INV>
 __host__ __device__ __forceinline__ void fz_stage(C* d, int N, int M, int lm, const C* __restrict__ tw, int tid,
                                                   int nthr) {
     const int m = 1 << lm;
-    const int s = N / M;
     const int nbf = N / RAD;
+    (void)M;
     for (int bf = tid; bf < nbf; bf += nthr) {
         const int blk = bf >> lm, j = bf & (m - 1);
-        const int base = blk * M + j;
+        const int base = blk * (RAD << lm) + j;
         C x[RAD];
 #pragma unroll
         for (int q = 0; q < RAD; ++q) x[q] = d[pad_idx<C>(base + q * m)];
         C w[RAD];
-        if (j) fz_twiddles<C, RAD>(tw, j * s, w);
+        if (j) fz_twiddles<C, RAD>(tw, j, m, w);
         if (INV && j) {
 #pragma unroll
             for (int q = 1; q < RAD; ++q) x[q] = cmulc(x[q], w[q]);
@@ -213,12 +234,24 @@ __host__ __device__ __forceinline__ void fz_shape(const FzPlan<C>& p, int s, int
 }
 
 #ifdef __CUDACC__
+// Fills the per-stage twiddle tables of p (n entries): w_M^(p j) evaluated in FP64.
+template <class C>
+__global__ void k_fz_fill_tables(C* out, FzPlan<C> p, uint32_t n) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    int M, pp, j;
+    fz_table_entry(p, e, M, pp, j);
+    double sn, cs;
+    sincospi(-2.0 * static_cast<double>(pp) * static_cast<double>(j) / static_cast<double>(M), &sn, &cs);
+    out[e] = from_d2<C>(make_double2(cs, sn));
+}
+
 template <class C>
 __device__ __forceinline__ void fz_forward(C* d, const FzPlan<C>& p) {
     for (int s = 0; s < p.nst; ++s) {
         int M, lm;
         fz_shape(p, s, M, lm);
-        fz_stage_any<C, false>(d, p.N, M, p.rad[s], lm, p.tw, threadIdx.x, blockDim.x);
+        fz_stage_any<C, false>(d, p.N, M, p.rad[s], lm, p.tw + p.twoff[s], threadIdx.x, blockDim.x);
         __syncthreads();
     }
 }
@@ -228,7 +261,7 @@ __device__ __forceinline__ void fz_inverse(C* d, const FzPlan<C>& p) {
     for (int s = p.nst - 1; s >= 0; --s) {
         int M, lm;
         fz_shape(p, s, M, lm);
-        fz_stage_any<C, true>(d, p.N, M, p.rad[s], lm, p.tw, threadIdx.x, blockDim.x);
+        fz_stage_any<C, true>(d, p.N, M, p.rad[s], lm, p.tw + p.twoff[s], threadIdx.x, blockDim.x);
         __syncthreads();
     }
 }
@@ -273,13 +306,22 @@ __global__ void __launch_bounds__(FZ_THREADS, 1) k_fz_conv_scan(const ScanJob* _
     // 1. x[t] = (g_i[t] - c_i) e^{-i w t dt}; phases by recurrence over the thread's samples
     const double2 ci = __ldg(&job.gi[job.n_in - 1]);
     {
+        // eight samples per thread per round: their loads are issued before any is used
         const double2 step = phase_minus(job.omega, dt, blockDim.x);
         double2 ph = phase_minus(job.omega, dt, threadIdx.x);
-        for (int t = threadIdx.x; t < p.N; t += blockDim.x) {
-            double2 x = make_double2(0.0, 0.0);
-            if (static_cast<uint32_t>(t) < job.n_in) x = cmul(csub(__ldg(&job.gi[t]), ci), ph);
-            d[pad_idx<C>(t)] = from_d2<C>(x);
-            ph = cmul(ph, step);
+        for (int t0 = threadIdx.x; t0 < p.N; t0 += 8 * blockDim.x) {
+            double2 g[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int t = t0 + k * static_cast<int>(blockDim.x);
+                g[k] = static_cast<uint32_t>(t) < job.n_in ? __ldg(&job.gi[t]) : ci;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int t = t0 + k * static_cast<int>(blockDim.x);
+                if (t < p.N) d[pad_idx<C>(t)] = from_d2<C>(cmul(csub(g[k], ci), ph));  // zero beyond n_in
+                ph = cmul(ph, step);
+            }
         }
     }
     __syncthreads();
@@ -288,9 +330,21 @@ __global__ void __launch_bounds__(FZ_THREADS, 1) k_fz_conv_scan(const ScanJob* _
     {
         const C* spec = static_cast<const C*>(half ? job.spec_c : job.spec_f);
         const R scale = static_cast<R>(dt / static_cast<double>(p.N));
-        for (int i = threadIdx.x; i < p.N; i += blockDim.x) {
-            const int k = pad_idx<C>(i);
-            d[k] = cscale(cmul(d[k], spec[i]), scale);
+        for (int i0 = threadIdx.x; i0 < p.N; i0 += 8 * blockDim.x) {
+            C sv[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int i = i0 + k * static_cast<int>(blockDim.x);
+                sv[k] = i < p.N ? __ldg(&spec[i]) : C{0, 0};
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int i = i0 + k * static_cast<int>(blockDim.x);
+                if (i < p.N) {
+                    const int q = pad_idx<C>(i);
+                    d[q] = cscale(cmul(d[q], sv[k]), scale);
+                }
+            }
         }
     }
     __syncthreads();

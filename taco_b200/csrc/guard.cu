@@ -11,26 +11,37 @@
 // recomputes in FP64 where it falls short:
 //
 //   1. the FP32 build of every instance (tcl4_build_direct / plan_create_direct);
-//   2. per instance, a head [0, H) with H = max(512, t_count / 16) (t_count = max(tidx)+1)
-//      is built in FP64 (the causal rule makes its FFT length follow H);
-//   3. the FP32 and FP64 results are compared on the head's upper half [H/2, H) (at most
-//      256 requested times of it, evenly spaced): if the relative Frobenius difference is
-//      within the tolerance (default 5e-7), the FP64 head replaces the FP32 rows and the
-//      instance is done -- the FP32 error decreases or stays flat with time after the early
-//      transient in every measured series, so the rest keeps its FP32 values;
+//   2. per instance, a head [0, H) is built in FP64 (the causal rule makes its FFT length
+//      follow H): H = max(512, t_count / 16) for direct calls, t_count / 4 for plans
+//      (t_count = max(tidx)+1);
+//   3. the FP32 and FP64 results are compared on the head's upper half [H/2, H) (direct
+//      calls: at most 256 requested times of it, evenly spaced): if the relative Frobenius
+//      difference is within the tolerance (default 5e-7), the instance is done -- the FP32
+//      error decreases or stays flat with time after the early transient in every measured
+//      series, so the rest keeps its FP32 values;
 //   4. otherwise H grows fourfold (at most to t_count, which is a full FP64 build of the
 //      instance) and step 2 repeats.
-//
-// Direct calls run the loop on every call.  Plans run it once at creation (on the inputs
-// they are created with) and replay the FP32 graph followed by the chosen FP64 heads and the
-// row patch; a plan replayed on different inputs keeps the head lengths chosen at creation.
+// A direct call replaces the FP32 rows of the accepted head with its FP64 rows, and starts
+// the next call on the same gamma buffer from the head it accepted (still checked).  A plan
+// compares every row of the head and keeps, for its replays, only the head up to the end
+// of the latest dyadic window of times ([0, 64), [64, 128), [128, 256), ...) whose FP32
+// error misses the tolerance (none: no head); it replays the FP32 graph followed by those
+// FP64 heads and the row patch.  A plan replayed on different inputs keeps the head lengths
+// chosen at creation.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <functional>
+#include <future>
+#include <map>
+#include <mutex>
+#include <thread>
 #include <memory>
 #include <vector>
 
@@ -43,6 +54,9 @@ namespace {
 
 std::atomic<double> g_guard_tol{5e-7};
 thread_local GuardStats t_stats;
+// Head length a direct call accepted, by (gamma buffer, t_count): the first guess of the next
+// call on the same buffer (it is still checked, so a changed buffer only costs more rounds).
+thread_local std::map<std::pair<const void*, uint32_t>, uint32_t> t_head_memory;
 
 constexpr std::size_t kMinHead = 512;        // smallest head (samples)
 constexpr std::size_t kWindowSamples = 256;  // requested times compared per check
@@ -55,43 +69,33 @@ struct GuardJob {
     const float2* cmp32;      // FP32 rows compared (the output, or the staged rows of a host output)
     const uint32_t* cmp_row;  // [nwin] row in cmp32 of each compared head row
     const uint32_t* win;      // [nwin] head rows compared
+    double2* rowsum;          // [nwin] per compared row: (sum |cmp32 - h64|^2, sum |h64|^2)
     uint32_t n, nwin, E;
 };
 
-// sums[2 j] = sum |cmp32 - h64|^2, sums[2 j + 1] = sum |h64|^2 over the window rows of job j.
-__global__ void __launch_bounds__(256) k_guard_compare(const GuardJob* __restrict__ jobs, double* __restrict__ sums) {
-    const GuardJob job = jobs[blockIdx.x];
+// Per compared row of job blockIdx.y (one warp per row): rowsum[q] = (sum |cmp32 - h64|^2,
+// sum |h64|^2) over the row's entries.
+__global__ void __launch_bounds__(256) k_guard_rows(const GuardJob* __restrict__ jobs) {
+    const GuardJob job = jobs[blockIdx.y];
+    const uint32_t q = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (q >= job.nwin) return;
+    const double2* r = job.h64 + static_cast<std::size_t>(job.win[q]) * job.E;
+    const float2* f = job.cmp32 + static_cast<std::size_t>(job.cmp_row[q]) * job.E;
     double num = 0.0, den = 0.0;
-    const std::size_t total = static_cast<std::size_t>(job.nwin) * job.E;
-    for (std::size_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const std::size_t q = idx / job.E, e = idx % job.E;
-        const double2 r = job.h64[static_cast<std::size_t>(job.win[q]) * job.E + e];
-        const float2 f = job.cmp32[static_cast<std::size_t>(job.cmp_row[q]) * job.E + e];
-        const double dx = static_cast<double>(f.x) - r.x, dy = static_cast<double>(f.y) - r.y;
+    for (uint32_t e = lane; e < job.E; e += 32) {
+        const double2 x = r[e];
+        const float2 y = f[e];
+        const double dx = static_cast<double>(y.x) - x.x, dy = static_cast<double>(y.y) - x.y;
         num += dx * dx + dy * dy;
-        den += r.x * r.x + r.y * r.y;
+        den += x.x * x.x + x.y * x.y;
     }
-    __shared__ double sn[8], sd[8];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         num += __shfl_xor_sync(0xffffffffu, num, o);
         den += __shfl_xor_sync(0xffffffffu, den, o);
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) {
-        sn[warp] = num;
-        sd[warp] = den;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0.0, b = 0.0;
-        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
-            a += sn[w];
-            b += sd[w];
-        }
-        sums[2 * blockIdx.x] = a;
-        sums[2 * blockIdx.x + 1] = b;
-    }
+    if (lane == 0) job.rowsum[q] = make_double2(num, den);
 }
 
 // out32[pos[k]][e] = h64[k][e] rounded to FP32, for every head row of job blockIdx.y.
@@ -138,14 +142,15 @@ uint32_t t_count_of(const Tcl4Instance& in) {
 }
 
 // The head of one instance: its requested times below H (in request order), their output
-// rows, and the head rows compared (times in [H/2, H), at most kWindowSamples evenly spaced).
+// rows, and the head rows compared (times in [H/2, H), at most kWindowSamples evenly spaced;
+// or every head row).
 struct Head {
     std::size_t inst = 0;
     uint32_t H = 0, tc = 0;
     std::vector<uint32_t> times, pos, win;
 };
 
-Head make_head(const std::vector<Tcl4Instance>& insts, std::size_t a, uint32_t H, uint32_t tc) {
+Head make_head(const std::vector<Tcl4Instance>& insts, std::size_t a, uint32_t H, uint32_t tc, bool all_rows = false) {
     Head h;
     h.inst = a;
     h.H = H;
@@ -166,7 +171,10 @@ Head make_head(const std::vector<Tcl4Instance>& insts, std::size_t a, uint32_t H
         std::sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return h.times[x] > h.times[y]; });
         upper.assign(ord.begin(), ord.begin() + std::max<std::size_t>(1, ord.size() / 4));
     }
-    if (upper.size() <= kWindowSamples) {
+    if (all_rows) {  // every head row (the row profile that sets a plan's final head)
+        h.win.resize(h.times.size());
+        for (std::size_t k = 0; k < h.win.size(); ++k) h.win[k] = static_cast<uint32_t>(k);
+    } else if (upper.size() <= kWindowSamples) {
         h.win = upper;
     } else {
         for (std::size_t k = 0; k < kWindowSamples; ++k) h.win.push_back(upper[k * upper.size() / kWindowSamples]);
@@ -226,7 +234,8 @@ struct JobImage {
 JobImage job_image(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads, std::size_t k0,
                    std::size_t k1, const double2* base, const std::vector<std::size_t>& off, unsigned char* dev,
                    const float2* stage = nullptr, const std::vector<std::size_t>* stage_off = nullptr,
-                   float2* hpatch = nullptr, const std::vector<std::size_t>* hpatch_off = nullptr) {
+                   float2* hpatch = nullptr, const std::vector<std::size_t>* hpatch_off = nullptr,
+                   double2* rowsum = nullptr, const std::vector<std::size_t>* rowsum_off = nullptr) {
     const std::size_t n = k1 - k0;
     std::size_t bytes = n * sizeof(GuardJob);
     std::vector<std::size_t> pos_off(n), cmp_off(n), win_off(n);
@@ -250,6 +259,7 @@ JobImage job_image(const std::vector<Tcl4Instance>& insts, const std::vector<Hea
         j.pos = at(pos_off[k]);
         j.cmp_row = at(cmp_off[k]);
         j.win = at(win_off[k]);
+        j.rowsum = rowsum ? rowsum + (*rowsum_off)[k] : nullptr;
         j.n = static_cast<uint32_t>(h.pos.size());
         j.nwin = static_cast<uint32_t>(h.win.size());
         j.E = static_cast<uint32_t>(entries(in));
@@ -283,39 +293,104 @@ struct Decision {
     std::vector<Head> heads;  // final heads of the instances that need one
 };
 
+// Heads built before the guard loop starts (concurrently with the FP32 pass).
+struct PreHeads {
+    std::vector<Head> heads;
+    DevMem temp;
+    std::vector<std::size_t> off;
+};
+
+// A persistent helper thread (its own thread-local workspace and stream) on which a direct
+// call builds its remembered FP64 heads while the calling thread runs the FP32 pass.  It is
+// created on first use and lives until the process exits.
+class HeadWorker {
+public:
+    static HeadWorker& get() {
+        static HeadWorker* w = new HeadWorker();  // never destroyed: no CUDA calls at exit
+        return *w;
+    }
+    std::future<void> run(std::function<void()> fn) {
+        std::packaged_task<void()> task(std::move(fn));
+        std::future<void> f = task.get_future();
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.push_back(std::move(task));
+        }
+        cv_.notify_one();
+        return f;
+    }
+
+private:
+    HeadWorker() {
+        std::thread([this] {
+            for (;;) {
+                std::packaged_task<void()> task;
+                {
+                    std::unique_lock<std::mutex> lk(mu_);
+                    cv_.wait(lk, [this] { return !q_.empty(); });
+                    task = std::move(q_.front());
+                    q_.pop_front();
+                }
+                task();
+            }
+        }).detach();
+    }
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::packaged_task<void()>> q_;
+};
+
 // Runs the guard loop: FP64 heads, comparison, growth.  With `patch`, accepted heads are
 // written into the outputs right away (direct calls); otherwise only the final heads are
 // returned (plans).  The FP32 results must already be in the outputs.  Comparison and
 // rounding run on the device; a host output stages its compared rows up and its patched
 // rows down (one copy per run of consecutive output rows).
-Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t st, bool patch) {
+Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t st, bool patch,
+                   PreHeads* pre = nullptr) {
     const double tol = g_guard_tol.load();
     BuildOptions o64 = opt;
     o64.fp32 = false;
     o64.fcr_ms = nullptr;
+    // plans (patch == false) compare every head row of device outputs: the row profile sets
+    // the head they replay; their first head is a quarter of the series, a direct call's a
+    // sixteenth (its heads are recomputed every call)
+    auto profile = [&](std::size_t a) { return !patch && insts[a].out_on_device; };
     std::vector<Head> pending;
     for (std::size_t a = 0; a < insts.size(); ++a) {
         if (insts[a].tidx.empty()) continue;
         const uint32_t tc = t_count_of(insts[a]);
-        const uint32_t H = static_cast<uint32_t>(std::min<std::size_t>(tc, std::max<std::size_t>(kMinHead, (tc + 15) / 16)));
-        Head h = make_head(insts, a, H, tc);
+        const std::size_t frac = patch ? 16 : 4;
+        uint32_t H = static_cast<uint32_t>(std::min<std::size_t>(tc, std::max<std::size_t>(kMinHead, (tc + frac - 1) / frac)));
+        if (patch) {
+            auto it = t_head_memory.find({insts[a].gamma, tc});
+            if (it != t_head_memory.end()) H = it->second;
+        }
+        Head h = make_head(insts, a, H, tc, profile(a));
         if (!h.times.empty()) pending.push_back(std::move(h));
     }
+    if (pre) pending = pre->heads;  // built already: the first round only evaluates them
     Decision dec;
-    DevMem temp, meta, sums, stage, hpatch;
+    DevMem temp, meta, rowsums, stage, hpatch;
     std::vector<float2> stage_host;
     t_stats = GuardStats{};
     t_stats.instances = insts.size();
     while (!pending.empty()) {
         ++t_stats.rounds;
         std::vector<Head> next;
-        for_chunks(insts, pending, [&](std::size_t k0, std::size_t k1, std::size_t bytes) {
+        const bool prebuilt = pre && t_stats.rounds == 1;
+        auto chunk = [&](std::size_t k0, std::size_t k1, std::size_t bytes) {
             const std::size_t n = k1 - k0;
-            temp.ensure(std::max<std::size_t>(bytes, 256));
             std::vector<std::size_t> off;
-            double2* base = static_cast<double2*>(temp.p);
-            std::vector<Tcl4Instance> hi = head_instances(insts, pending, k0, k1, base, off);
-            tcl4_build_direct(hi, o64, st);  // synchronous
+            double2* base = nullptr;
+            if (prebuilt) {
+                base = static_cast<double2*>(pre->temp.p);
+                off = pre->off;
+            } else {
+                temp.ensure(std::max<std::size_t>(bytes, 256));
+                base = static_cast<double2*>(temp.p);
+                std::vector<Tcl4Instance> hi = head_instances(insts, pending, k0, k1, base, off);
+                tcl4_build_direct(hi, o64, st);  // synchronous
+            }
             // host outputs: their window rows staged up, their patched rows in a device buffer
             std::vector<std::size_t> soff(n, 0), poff(n, 0);
             std::size_t srows = 0, prows = 0;
@@ -348,31 +423,70 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
             if (prows) hpatch.ensure(prows * sizeof(float2));
             const float2* stage_p = static_cast<const float2*>(stage.p);
             float2* hpatch_p = static_cast<float2*>(hpatch.p);
+            // per compared row: (squared difference, squared FP64 norm)
+            std::vector<std::size_t> roff(n, 0);
+            std::size_t nrows = 0, most_win = 1;
+            for (std::size_t k = k0; k < k1; ++k) {
+                roff[k - k0] = nrows;
+                nrows += pending[k].win.size();
+                most_win = std::max(most_win, pending[k].win.size());
+            }
+            rowsums.ensure(std::max<std::size_t>(1, nrows) * sizeof(double2));
+            double2* rowsum_p = static_cast<double2*>(rowsums.p);
             meta.ensure(job_image(insts, pending, k0, k1, base, off, nullptr).host.size() + 256);
             JobImage img = job_image(insts, pending, k0, k1, base, off, static_cast<unsigned char*>(meta.p), stage_p, &soff,
-                                     hpatch_p, &poff);
-            sums.ensure(2 * n * sizeof(double));
+                                     hpatch_p, &poff, rowsum_p, &roff);
             cuda_check(cudaMemcpyAsync(meta.p, img.host.data(), img.host.size(), cudaMemcpyHostToDevice, st),
                        "cudaMemcpyAsync(guard jobs)");
-            k_guard_compare<<<static_cast<unsigned>(n), 256, 0, st>>>(static_cast<const GuardJob*>(meta.p),
-                                                                    static_cast<double*>(sums.p));
-            cuda_check(cudaGetLastError(), "k_guard_compare");
+            k_guard_rows<<<dim3(static_cast<unsigned>((most_win + 7) / 8), static_cast<unsigned>(n)), 256, 0, st>>>(
+                static_cast<const GuardJob*>(meta.p));
+            cuda_check(cudaGetLastError(), "k_guard_rows");
             count_launches(1);
-            std::vector<double> s(2 * n, 0.0);
-            cuda_check(cudaMemcpyAsync(s.data(), sums.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, st),
-                       "cudaMemcpyAsync(guard sums)");
+            std::vector<double2> rs(std::max<std::size_t>(1, nrows));
+            if (nrows)
+                cuda_check(cudaMemcpyAsync(rs.data(), rowsum_p, nrows * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                           "cudaMemcpyAsync(guard rows)");
             cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(guard)");
-            // decide
+            // decide: the window [H/2, H) within the tolerance, or the whole series in FP64
+            auto ok_of = [&](double num, double den) { return den > 0.0 ? std::sqrt(num / den) <= tol : num == 0.0; };
             std::vector<char> accept(n, 0);
+            std::vector<uint32_t> final_h(n, 0);
             for (std::size_t k = k0; k < k1; ++k) {
-                const double num = s[2 * (k - k0)], den = s[2 * (k - k0) + 1];
-                const bool ok = den > 0.0 ? std::sqrt(num / den) <= tol : num == 0.0;
                 const Head& h = pending[k];
-                if (ok || h.H >= h.tc) {
+                const double2* r = rs.data() + roff[k - k0];
+                double wn = 0.0, wd = 0.0;
+                for (std::size_t q = 0; q < h.win.size(); ++q)
+                    if (2 * static_cast<std::size_t>(h.times[h.win[q]]) >= h.H || !profile(h.inst)) {
+                        wn += r[q].x;
+                        wd += r[q].y;
+                    }
+                if (ok_of(wn, wd) || h.H >= h.tc) {
                     accept[k - k0] = 1;
+                    final_h[k - k0] = h.H;
+                    if (profile(h.inst)) {
+                        // the head a plan replays: up to the end of the latest dyadic window
+                        // ([0, 64), [64, 128), [128, 256), ...) that misses the tolerance
+                        std::vector<double> num(40, 0.0), den(40, 0.0);
+                        for (std::size_t q = 0; q < h.win.size(); ++q) {
+                            const uint32_t t = h.times[h.win[q]];
+                            int w = 0;
+                            while (w < 39 && (std::size_t(64) << w) <= t) ++w;
+                            num[w] += r[q].x;
+                            den[w] += r[q].y;
+                        }
+                        uint32_t hf = 0;
+                        for (int w = 39; w >= 0; --w)
+                            if (den[w] > 0.0 || num[w] > 0.0) {
+                                if (!ok_of(num[w], den[w])) {
+                                    hf = static_cast<uint32_t>(std::min<std::size_t>(h.H, std::size_t(64) << w));
+                                    break;
+                                }
+                            }
+                        final_h[k - k0] = hf;
+                    }
                 } else {
                     const uint32_t H = static_cast<uint32_t>(std::min<std::size_t>(h.tc, 4 * static_cast<std::size_t>(h.H)));
-                    next.push_back(make_head(insts, h.inst, H, h.tc));
+                    next.push_back(make_head(insts, h.inst, H, h.tc, profile(h.inst)));
                 }
             }
             if (patch) {
@@ -410,16 +524,26 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
                 }
                 cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(guard patch)");
             }
+            if (patch) {
+                if (t_head_memory.size() > 65536) t_head_memory.clear();
+                for (std::size_t k = k0; k < k1; ++k)
+                    if (accept[k - k0]) t_head_memory[{insts[pending[k].inst].gamma, pending[k].tc}] = pending[k].H;
+            }
             for (std::size_t k = k0; k < k1; ++k)
                 if (accept[k - k0]) {
-                    const Head& h = pending[k];
+                    const Head& h0 = pending[k];
+                    if (final_h[k - k0] == 0) continue;  // FP32 within the tolerance everywhere
+                    Head h = final_h[k - k0] == h0.H ? h0 : make_head(insts, h0.inst, final_h[k - k0], h0.tc);
+                    if (h.times.empty()) continue;
                     ++t_stats.heads;
                     t_stats.head_rows += h.times.size();
                     t_stats.rows += insts[h.inst].tidx.size();
                     if (h.H >= h.tc) ++t_stats.full;
-                    dec.heads.push_back(h);
+                    dec.heads.push_back(std::move(h));
                 }
-        });
+        };
+        if (prebuilt) chunk(0, pending.size(), 0);
+        else for_chunks(insts, pending, chunk);
         pending.swap(next);
     }
     return dec;
@@ -432,9 +556,56 @@ GuardStats fp32_guard_stats() { return t_stats; }
 double fp32_guard() { return g_guard_tol.load(); }
 
 void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t stream) {
-    tcl4_build_direct(insts, opt, stream);
     t_stats = GuardStats{};
-    if (!opt.fp32 || g_guard_tol.load() <= 0.0) return;
+    if (!opt.fp32 || g_guard_tol.load() <= 0.0) {
+        tcl4_build_direct(insts, opt, stream);
+        return;
+    }
+    // the FP32 pass on a copy: a direct build may point an instance at device copies of its
+    // host input and output that it frees before returning; the guard needs the caller's
+    std::vector<Tcl4Instance> pass(insts);
+    // every instance's head remembered from an earlier call on its gamma buffer: build those
+    // heads on the helper thread while this thread runs the FP32 pass
+    PreHeads pre;
+    bool have_pre = true;
+    std::size_t pre_bytes = 0;
+    for (std::size_t a = 0; a < insts.size() && have_pre; ++a) {
+        if (insts[a].tidx.empty()) continue;
+        const uint32_t tc = t_count_of(insts[a]);
+        auto it = t_head_memory.find({insts[a].gamma, tc});
+        if (it == t_head_memory.end()) {
+            have_pre = false;
+            break;
+        }
+        Head h = make_head(insts, a, it->second, tc);
+        pre_bytes += h.times.size() * entries(insts[a]) * sizeof(double2);
+        if (!h.times.empty()) pre.heads.push_back(std::move(h));
+    }
+    have_pre = have_pre && !pre.heads.empty() && pre_bytes <= kTempBytes;
+    if (have_pre) {
+        BuildOptions o64 = opt;
+        o64.fp32 = false;
+        o64.fcr_ms = nullptr;
+        pre.temp.ensure(std::max<std::size_t>(pre_bytes, 256));
+        std::vector<Tcl4Instance> hi =
+            head_instances(insts, pre.heads, 0, pre.heads.size(), static_cast<double2*>(pre.temp.p), pre.off);
+        int dev = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        std::future<void> heads = HeadWorker::get().run([&hi, &o64, dev] {
+            cuda_check(cudaSetDevice(dev), "cudaSetDevice(guard worker)");
+            tcl4_build_direct(hi, o64, nullptr);
+        });
+        try {
+            tcl4_build_direct(pass, opt, stream);
+        } catch (...) {
+            heads.wait();
+            throw;
+        }
+        heads.get();  // rethrows the helper's error
+        run_guard(insts, opt, stream ? stream : default_stream(), true, &pre);
+        return;
+    }
+    tcl4_build_direct(pass, opt, stream);
     run_guard(insts, opt, stream ? stream : default_stream(), true);
 }
 

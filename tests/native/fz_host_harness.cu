@@ -14,10 +14,12 @@ static int convolve(int N, int max_radix, const double* a, const double* b, doub
     FzPlan<C> p{};
     p.N = N;
     if (!fz_stages(N, max_radix, p.rad, p.nst)) return 1;
-    std::vector<C> tw(N);
-    for (int m = 0; m < N; ++m) {
-        const double ang = -2.0 * M_PI * static_cast<double>(m) / N;
-        tw[m] = C{static_cast<R>(std::cos(ang)), static_cast<R>(std::sin(ang))};
+    std::vector<C> tw(std::max<std::size_t>(1, fz_table_layout(p)));
+    for (std::size_t e = 0; e < tw.size(); ++e) {
+        int M, pp, j;
+        fz_table_entry(p, e, M, pp, j);
+        const double ang = -2.0 * M_PI * static_cast<double>(pp) * static_cast<double>(j) / M;
+        tw[e] = C{static_cast<R>(std::cos(ang)), static_cast<R>(std::sin(ang))};
     }
     p.tw = tw.data();
     std::vector<C> x(padded_size<C>(N)), y(padded_size<C>(N));
@@ -29,13 +31,13 @@ static int convolve(int N, int max_radix, const double* a, const double* b, doub
         for (int s = 0; s < p.nst; ++s) {
             int M, lm;
             fz_shape(p, s, M, lm);
-            fz_stage_any<C, false>(d->data(), N, M, p.rad[s], lm, p.tw, 0, 1);
+            fz_stage_any<C, false>(d->data(), N, M, p.rad[s], lm, p.tw + p.twoff[s], 0, 1);
         }
     for (int i = 0; i < N; ++i) x[pad_idx<C>(i)] = cmul(x[pad_idx<C>(i)], y[pad_idx<C>(i)]);
     for (int s = p.nst - 1; s >= 0; --s) {
         int M, lm;
         fz_shape(p, s, M, lm);
-        fz_stage_any<C, true>(x.data(), N, M, p.rad[s], lm, p.tw, 0, 1);
+        fz_stage_any<C, true>(x.data(), N, M, p.rad[s], lm, p.tw + p.twoff[s], 0, 1);
     }
     for (int t = 0; t < N; ++t) {
         out[2 * t] = static_cast<double>(x[pad_idx<C>(t)].x) / N;
