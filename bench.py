@@ -445,15 +445,16 @@ def heterogeneous_batch(args, rank, world, cpu_leg):
     out["fp64_subset"] = {"instances": len(ref_ids), "value": world * ref_builds / (ms64 / 1e3), "unit": "builds/s",
                           "ms_per_step": ms64, "plan_prepare_seconds": round(prep64, 2)}
     res64 = {b: r for b, r in zip(ref_ids, plan64.results)}
-    # the times below 2048 from an FP64 build of those times alone (short causal FFT): the
-    # full-length FP64 transform's round-off exceeds the FP32 form's guard at the first,
-    # tiny L4 values of long series
+    # the times below 2048 and below 256 from FP64 builds of those times alone (short causal
+    # FFTs): the full-length FP64 transform's round-off exceeds the FP32 form's guard at the
+    # first, tiny L4 values of long series
     for b in ref_ids:
-        early = np.nonzero(tids[b] < 2048)[0]
-        if early.size:
-            r = res64[b].clone()
-            r[early] = tb.build_TCL4_generator_batch(systems[b], gammas[b], dts[b], tids[b][early], precision="fp64")
-            res64[b] = r
+        r = res64[b].clone()
+        for bound in (2048, 256):
+            early = np.nonzero(tids[b] < bound)[0]
+            if early.size:
+                r[early] = tb.build_TCL4_generator_batch(systems[b], gammas[b], dts[b], tids[b][early], precision="fp64")
+        res64[b] = r
     per, werr = [], []
     for b in ref_ids:
         a = res32[b].cpu().numpy().reshape(tids[b].size, -1)
@@ -699,16 +700,17 @@ def main():
         systems[k], gammas[k], args.dt, tidx, precision="fp64", out=outs64[k]) for k in range(P)], 2) / P)
     plain_value = T / (ms64 / 1e3)
     # FP32 form against FP64 on Pe instances: whole series and every dyadic window (FP64 for
-    # the times below 2048 from a build of those times alone: a short causal FFT)
+    # the times below 2048 and below 256 from builds of those times alone: short causal FFTs)
     tb.build_instances(inst[P:Pe], precision="fp64", outs=outs64[P:Pe])
     torch.cuda.synchronize()
-    early = tidx[tidx < 2048]
     errs_g, errs_w = [], []
     for k in range(Pe):
         a = outs32[k].to(torch.complex128).cpu().numpy()
         b = outs64[k].cpu().numpy().copy()
-        b[: early.size] = tb.build_TCL4_generator_batch(systems[k], gammas[k], args.dt, early,
-                                                        precision="fp64").transpose(1, 2).reshape(early.size, -1).cpu().numpy()
+        for bound in (2048, 256):
+            early = tidx[tidx < bound]
+            b[: early.size] = tb.build_TCL4_generator_batch(systems[k], gammas[k], args.dt, early, precision="fp64"
+                                                            ).transpose(1, 2).reshape(early.size, -1).cpu().numpy()
         errs_g.append(float(np.linalg.norm(a - b) / np.linalg.norm(b)))
         errs_w.append(max(e for _, e in window_errors(a, b, tidx)))
     err32 = max(errs_g)

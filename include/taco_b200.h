@@ -242,17 +242,25 @@ int taco_l4_coefficients(const taco_system_view* sys, int32_t* rowptr, uint32_t*
 int taco_set_work_budget(size_t bytes);
 /* No counterpart in the reference.  Precision guard of the FP32 form (TACO_PREC_FP32 builds
  * and plans): after the FP32 build, a head of each instance's leading times [0, H) is built
- * in FP64 (H = max(512, t_count/16) first, t_count = max(tidx)+1) and compared with the
- * FP32 result on [H/2, H); within `tol` (relative Frobenius) the FP64 head replaces those
- * FP32 rows, otherwise H grows fourfold, up to a full FP64 build of the instance.  Plans
- * choose their heads once, at creation.  tol = 0 turns the guard off; the default is 5e-7.
- * taco_get_fp32_guard returns the current value. */
+ * in FP64 (t_count = max(tidx)+1; H = t_count/4 for plans, t_count/16 for direct calls, at
+ * least 512) and compared with the FP32 result row by row; the FP32 rows up to the last
+ * dyadic window [2^k, 2^(k+1)) that misses `tol` (relative Frobenius) are replaced by FP64
+ * rows, the head growing fourfold while the misses reach its end, up to a full FP64 build of
+ * the instance.  The FP64 rows below 2048 and 256 come from builds of those times alone
+ * (short FFTs, whose round-off at the first, tiny L4 values is far below the full-length
+ * transform's).  Plans choose their heads once, at creation, and replay them; direct calls
+ * remember, per gamma buffer and a fingerprint of its contents, the heads a call needed and
+ * build only those on a helper thread during the next call's FP32 pass.  tol = 0 turns the
+ * guard off; the default is 5e-7.  taco_get_fp32_guard returns the current value. */
 /* No counterpart in the reference.  The fused F/C/R path: for FFT lengths whose working
  * array fits one CTA's shared memory (FP32 up to 24576 points, FP64 up to 12288), one CTA per
  * (triple, half) runs the forward transform, the spectral product, the inverse transform, the
- * prefix integrals and the assembly in shared memory.  on = 0 selects the four-step passes
- * and the scan kernels for every length (the default is on; results agree to rounding). */
+ * prefix integrals and the assembly in shared memory.  on = 0 (the default) selects the
+ * four-step passes and the scan kernels for every length; results agree to rounding.  On
+ * B200 the fused path is the slower one at the lengths it fits (one CTA per SM, latency
+ * bound), so it stays off unless selected.  taco_get_fused_conv returns the setting. */
 int taco_set_fused_conv(int on);
+int taco_get_fused_conv(int* on);
 /* No counterpart in the reference (whose thread_local workspace is freed at thread exit,
  * cpp/src/backend/cuda/tcl4_fused_cuda.cu:676-685).  Frees the calling thread's grow-only
  * device and pinned transient buffers on the current device after its streams finish; the

@@ -41,6 +41,7 @@ __all__ = [
     "propagate_rk4_dense", "l4_coefficients", "Tcl4Plan", "set_fcr_fft_pad_factor", "get_fcr_fft_pad_factor",
     "version", "device_count", "kernel_launches", "profile", "compute_triple_kernels_batch", "tcl2_generator_series", "gamma_trapz_device",
     "propagate_tcl", "gamma_trapz_device_batch", "set_work_budget", "fft_length", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
+    "set_fp32_guard", "fp32_guard", "fp32_guard_stats", "set_fused_conv", "fused_conv", "release_workspace",
 ]
 
 
@@ -111,8 +112,15 @@ def fp32_guard() -> float:
 
 def set_fused_conv(on: bool) -> None:
     """The fused F/C/R path (transforms, scans and assembly of a triple in one CTA's shared
-    memory) for the FFT lengths it fits (default on); off: the four-step passes everywhere."""
+    memory) for the FFT lengths it fits; off (the default): the four-step passes everywhere."""
     _capi.check(_capi.lib().taco_set_fused_conv(1 if on else 0))
+
+
+def fused_conv() -> bool:
+    """Whether the fused F/C/R path is selected."""
+    v = ct.c_int(0)
+    _capi.check(_capi.lib().taco_get_fused_conv(ct.byref(v)))
+    return bool(v.value)
 
 
 def release_workspace() -> None:

@@ -633,11 +633,19 @@ int taco_release_workspace(void) {
     return guarded([&] {
         require_device();
         taco::release_workspace();
+        taco::release_guard_scratch();
     });
 }
 
 int taco_set_fused_conv(int on) {
     return guarded([&] { taco::set_fused_conv(on != 0); });
+}
+
+int taco_get_fused_conv(int* on) {
+    return guarded([&] {
+        if (!on) throw taco::Error(taco::kInvalidArgument, "on is null");
+        *on = taco::fused_conv() ? 1 : 0;
+    });
 }
 
 int taco_set_fp32_guard(double tol) {

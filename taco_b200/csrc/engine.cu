@@ -1988,7 +1988,8 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
         if (in.gamma_on_device) check_device_buffer(in.gamma, sizeof(double2), "gamma");
         if (in.tidx.empty()) continue;
         if (!in.out) throw Error(kInvalidArgument, "output pointer is null");
-        if (in.out_on_device) check_device_buffer(in.out, opt.fp32 ? sizeof(float2) : sizeof(double2), "output");
+        if (in.out_on_device && !in.internal)
+            check_device_buffer(in.out, opt.fp32 ? sizeof(float2) : sizeof(double2), "output");
         auto r = list_index.emplace(in.tidx.identity(), first.size());
         if (r.second) first.push_back(a);
         lid[a] = r.first->second;
@@ -2044,11 +2045,12 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
 }
 }  // namespace
 
-std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions& opt) {
+std::size_t work_budget_now() { return work_budget(); }
+
+std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, std::size_t budget) {
     std::vector<InstMeta> metas;
     validate_and_derive(insts, opt, metas);
     std::vector<std::unique_ptr<WorkUnit>> store;
-    const std::size_t budget = work_budget();
     std::vector<std::vector<WorkUnit*>> groups =
         opt.fp32 ? plan_units<float>(insts, metas, budget, store) : plan_units<double>(insts, metas, budget, store);
     std::size_t work = 0;
@@ -2058,7 +2060,7 @@ std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions
 }
 
 Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, void* ext_work,
-                             std::size_t ext_cap) {
+                             std::size_t ext_cap, std::size_t budget_in) {
     for (const auto& in : insts)
         if (!in.gamma_on_device || !in.out_on_device)
             throw Error(kInvalidArgument, "plans take device inputs and outputs (TACO_IN_DEVICE | TACO_OUT_DEVICE)");
@@ -2070,7 +2072,7 @@ Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOption
     Workspace& ws = workspace();
     // a lent buffer is the budget (the caller sized it for these instances); else the
     // share of the free memory
-    const std::size_t budget = ext_work ? ext_cap : work_budget();
+    const std::size_t budget = ext_work ? (budget_in ? budget_in : ext_cap) : work_budget();
     std::vector<std::vector<WorkUnit*>> groups =
         opt.fp32 ? plan_units<float>(insts, metas, budget, plan->units) : plan_units<double>(insts, metas, budget, plan->units);
     // one transient buffer shared by the groups (they run in order on the plan's stream),

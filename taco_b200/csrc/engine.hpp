@@ -62,6 +62,7 @@ struct Tcl4Instance {
     TimeList tidx;                   // explicit list of requested time indices
     void* out = nullptr;             // [T][N^2 x N^2] complex (FP64: double2, FP32: float2)
     bool out_on_device = false;
+    bool internal = false;           // buffers allocated by the library itself (not re-checked)
 };
 
 // Launch schedule of the F/C/R passes for one FFT length and precision.
@@ -110,10 +111,15 @@ struct Tcl4Plan;
 Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt);
 // ext_work (optional): a caller's device buffer of ext_cap bytes for the plan's transient
 // arrays, shared with plans that run one after another on the same stream.
+// budget (optional, with ext_work): the group budget the plan's units are packed by.
 Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, void* ext_work = nullptr,
-                             std::size_t ext_cap = 0);
-// Transient bytes a plan of these instances would allocate.
-std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions& opt);
+                             std::size_t ext_cap = 0, std::size_t budget = 0);
+// Transient bytes a plan of these instances would allocate under the group budget.
+std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, std::size_t budget);
+// The group budget of a build started now (set, or the share of the free memory).
+std::size_t work_budget_now();
+// Frees the calling thread's precision-guard buffers on the current device.
+void release_guard_scratch();
 // Work enqueued after the plan's graph on every execute (owns what it captures).
 void plan_set_tail(Tcl4Plan* plan, std::function<void(cudaStream_t)> tail, uint64_t kernels);
 void plan_execute(Tcl4Plan* plan, cudaStream_t stream);

@@ -13,25 +13,31 @@
 //   1. the FP32 build of every instance (tcl4_build_direct / plan_create_direct);
 //   2. per instance, a head [0, H) is built in FP64 (the causal rule makes its FFT length
 //      follow H): H = max(512, t_count / 16) for direct calls, t_count / 4 for plans
-//      (t_count = max(tidx)+1);
-//   3. the FP32 and FP64 results are compared on the head's upper half [H/2, H) (direct
-//      calls: at most 256 requested times of it, evenly spaced): if the relative Frobenius
-//      difference is within the tolerance (default 5e-7), the instance is done -- the FP32
-//      error decreases or stays flat with time after the early transient in every measured
-//      series, so the rest keeps its FP32 values;
+//      (t_count = max(tidx)+1); its times below 2048 and below 256 are rebuilt by FP64 builds
+//      of those times alone (FFTs of about 4096 and 512 points): at the earliest times L4 is
+//      so small that the round-off of a long transform dominates it even in FP64 (the
+//      reference's own FP64 convolution at FFT 2^19 misses the exact direct sums by a factor
+//      of 100 at t < 64 on the batching form's longest series);
+//   3. every head row is compared with the FP32 result; if the relative Frobenius difference
+//      over the head's upper half [H/2, H) is within the tolerance (default 5e-7), the
+//      instance is done -- the FP32 error decreases or stays flat with time after the early
+//      transient in every measured series, so the rest keeps its FP32 values;
 //   4. otherwise H grows fourfold (at most to t_count, which is a full FP64 build of the
 //      instance) and step 2 repeats.
-// A direct call replaces the FP32 rows of the accepted head with its FP64 rows, and starts
-// the next call on the same gamma buffer from the head it accepted (still checked).  A plan
-// compares every row of the head and keeps, for its replays, only the head up to the end
-// of the latest dyadic window of times ([0, 64), [64, 128), [128, 256), ...) whose FP32
-// error misses the tolerance (none: no head); it replays the FP32 graph followed by those
-// FP64 heads and the row patch.  A plan replayed on different inputs keeps the head lengths
-// chosen at creation.
+// The head an instance needs is the end of the latest dyadic window of times ([0, 64),
+// [64, 128), [128, 256), ...) whose FP32 error misses the tolerance (none: no head).  A plan
+// replays the FP32 graph followed by those FP64 heads and the row patch; a plan replayed on
+// different inputs keeps the heads chosen at creation.  A direct call patches its whole
+// accepted head and remembers, per gamma buffer, the accepted and the needed head and a
+// fingerprint of the buffer's contents; a later call with the same fingerprint builds only
+// the needed heads, on a helper thread during the FP32 pass, and patches them without a
+// comparison, while a changed fingerprint is checked again from the accepted head.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstdint>
 #include <condition_variable>
@@ -54,9 +60,16 @@ namespace {
 
 std::atomic<double> g_guard_tol{5e-7};
 thread_local GuardStats t_stats;
-// Head length a direct call accepted, by (gamma buffer, t_count): the first guess of the next
-// call on the same buffer (it is still checked, so a changed buffer only costs more rounds).
-thread_local std::map<std::pair<const void*, uint32_t>, uint32_t> t_head_memory;
+// What a direct call decided for a (gamma buffer, t_count): the head it accepted, the head
+// the row profile requires, and a fingerprint of the buffer's contents.  A later call whose
+// fingerprint matches builds the required head alone (no comparison round); one whose
+// fingerprint differs starts from the accepted head and is checked as usual.
+struct HeadMemory {
+    uint32_t accepted = 0, required = 0;
+    uint64_t fingerprint = 0;
+};
+thread_local std::map<std::pair<const void*, uint32_t>, HeadMemory> t_head_memory;
+
 
 constexpr std::size_t kMinHead = 512;        // smallest head (samples)
 constexpr std::size_t kWindowSamples = 256;  // requested times compared per check
@@ -129,6 +142,85 @@ struct DevMem {
         if (p) cudaFree(p);
     }
 };
+
+// FNV-1a over bytes.
+uint64_t fnv1a(uint64_t h, const void* p, std::size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (std::size_t k = 0; k < n; ++k) {
+        h ^= b[k];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+constexpr int kPrintSamples = 64;  // gamma samples per bucket in a fingerprint
+
+__global__ void k_guard_gather(const double2* const* __restrict__ src, double2* __restrict__ out, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = *src[k];
+}
+
+// Fingerprints of the instances' gamma (the consumed samples of every bucket at 64 evenly
+// spaced times, with the sizes and dt); device inputs are gathered by one launch.
+std::vector<uint64_t> fingerprints(const std::vector<Tcl4Instance>& insts, cudaStream_t st) {
+    const std::size_t n = insts.size();
+    std::vector<uint64_t> fp(n, 0);
+    std::vector<const double2*> addr;
+    std::vector<std::size_t> first(n, 0);
+    std::vector<std::size_t> count(n, 0);
+    for (std::size_t a = 0; a < n; ++a) {
+        const Tcl4Instance& in = insts[a];
+        if (in.tidx.empty()) continue;
+        uint32_t tc = 0;
+        for (uint32_t t : in.tidx) tc = std::max(tc, t + 1);
+        const std::size_t n_in = std::min<std::size_t>(in.Nt, tc);
+        first[a] = addr.size();
+        for (int b = 0; b < in.sys.nf; ++b)
+            for (int k = 0; k < kPrintSamples; ++k)
+                addr.push_back(in.gamma + static_cast<std::size_t>(b) * in.Nt + (n_in - 1) * k / (kPrintSamples - 1));
+        count[a] = addr.size() - first[a];
+    }
+    std::vector<double2> vals(addr.size());
+    std::vector<const double2*> dev_addr;
+    std::vector<std::size_t> dev_pos;
+    for (std::size_t a = 0; a < n; ++a) {
+        if (!count[a]) continue;
+        if (insts[a].gamma_on_device) {
+            for (std::size_t k = 0; k < count[a]; ++k) {
+                dev_addr.push_back(addr[first[a] + k]);
+                dev_pos.push_back(first[a] + k);
+            }
+        } else {
+            for (std::size_t k = 0; k < count[a]; ++k) vals[first[a] + k] = *addr[first[a] + k];
+        }
+    }
+    if (!dev_addr.empty()) {
+        DevMem da, dv;
+        da.ensure(dev_addr.size() * sizeof(double2*));
+        dv.ensure(dev_addr.size() * sizeof(double2));
+        std::vector<double2> got(dev_addr.size());
+        cuda_check(cudaMemcpyAsync(da.p, dev_addr.data(), dev_addr.size() * sizeof(double2*), cudaMemcpyHostToDevice, st),
+                   "cudaMemcpyAsync(fingerprint addresses)");
+        k_guard_gather<<<static_cast<unsigned>((dev_addr.size() + 255) / 256), 256, 0, st>>>(
+            static_cast<const double2* const*>(da.p), static_cast<double2*>(dv.p), static_cast<uint32_t>(dev_addr.size()));
+        cuda_check(cudaGetLastError(), "k_guard_gather");
+        count_launches(1);
+        cuda_check(cudaMemcpyAsync(got.data(), dv.p, got.size() * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                   "cudaMemcpyAsync(fingerprint samples)");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(fingerprint)");
+        for (std::size_t k = 0; k < dev_pos.size(); ++k) vals[dev_pos[k]] = got[k];
+    }
+    for (std::size_t a = 0; a < n; ++a) {
+        if (!count[a]) continue;
+        uint64_t h = 1469598103934665603ull;
+        const uint64_t sizes[3] = {insts[a].Nt, static_cast<uint64_t>(insts[a].sys.nf), insts[a].tidx.size()};
+        h = fnv1a(h, sizes, sizeof(sizes));
+        h = fnv1a(h, &insts[a].dt, sizeof(double));
+        h = fnv1a(h, vals.data() + first[a], count[a] * sizeof(double2));
+        fp[a] = h;
+    }
+    return fp;
+}
 
 std::size_t entries(const Tcl4Instance& in) {
     const std::size_t N2 = static_cast<std::size_t>(in.sys.N) * in.sys.N;
@@ -217,11 +309,55 @@ std::vector<Tcl4Instance> head_instances(const std::vector<Tcl4Instance>& insts,
         h.tidx = heads[k].times;
         h.out = base + o;
         h.out_on_device = true;
+        h.internal = true;
         off[k - k0] = o;
         o += heads[k].times.size() * entries(in);
         hi.push_back(std::move(h));
     }
     return hi;
+}
+
+// Short-FFT levels of the heads [k0, k1): for a head longer than `bound` whose times are
+// sorted, an FP64 build of its times below `bound` alone, written over the head's first rows.
+// The causal rule gives such a build an FFT of about 2 bound points, whose round-off at the
+// earliest, tiny L4 values is orders of magnitude below that of the head's own transform.
+constexpr uint32_t kLevels[] = {2048, 256};
+
+std::vector<Tcl4Instance> level_instances(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads,
+                                          std::size_t k0, std::size_t k1, double2* base,
+                                          const std::vector<std::size_t>& off, uint32_t bound) {
+    std::vector<Tcl4Instance> li;
+    for (std::size_t k = k0; k < k1; ++k) {
+        const Head& h = heads[k];
+        if (h.H <= bound || !std::is_sorted(h.times.begin(), h.times.end())) continue;
+        const std::size_t n = static_cast<std::size_t>(std::lower_bound(h.times.begin(), h.times.end(), bound) - h.times.begin());
+        if (n == 0) continue;
+        const Tcl4Instance& in = insts[h.inst];
+        Tcl4Instance l;
+        l.sys = in.sys;
+        l.gamma = in.gamma;
+        l.gamma_on_device = in.gamma_on_device;
+        l.Nt = in.Nt;
+        l.dt = in.dt;
+        l.tidx = std::vector<uint32_t>(h.times.begin(), h.times.begin() + n);
+        l.out = base + off[k - k0];
+        l.out_on_device = true;
+        l.internal = true;
+        li.push_back(std::move(l));
+    }
+    return li;
+}
+
+// The FP64 heads [k0, k1) into their rows at base + off: the head builds, then the short-FFT
+// levels coarse to fine (each overwriting the rows below its bound).
+void build_heads(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads, std::size_t k0, std::size_t k1,
+                 double2* base, std::vector<std::size_t>& off, const BuildOptions& o64, cudaStream_t st) {
+    std::vector<Tcl4Instance> hi = head_instances(insts, heads, k0, k1, base, off);
+    tcl4_build_direct(hi, o64, st);  // synchronous
+    for (uint32_t bound : kLevels) {
+        std::vector<Tcl4Instance> li = level_instances(insts, heads, k0, k1, base, off, bound);
+        if (!li.empty()) tcl4_build_direct(li, o64, st);
+    }
 }
 
 // Device jobs of heads [k0, k1) and their index arrays, as one host image of the device
@@ -296,9 +432,27 @@ struct Decision {
 // Heads built before the guard loop starts (concurrently with the FP32 pass).
 struct PreHeads {
     std::vector<Head> heads;
-    DevMem temp;
+    DevMem* temp = nullptr;  // the calling thread's guard scratch
     std::vector<std::size_t> off;
 };
+
+// The guard's device buffers of the calling thread and device: grow-only and kept across calls
+// (allocating and freeing them every call synchronised the device and cost milliseconds).
+struct GuardScratch {
+    DevMem temp, meta, rowsums, stage, hpatch, pre;
+    std::vector<float2> stage_host;
+};
+std::map<int, std::unique_ptr<GuardScratch>>& guard_scratch_map() {
+    thread_local std::map<int, std::unique_ptr<GuardScratch>> m;
+    return m;
+}
+GuardScratch& guard_scratch() {
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    auto& p = guard_scratch_map()[dev];
+    if (!p) p = std::make_unique<GuardScratch>();
+    return *p;
+}
 
 // A persistent helper thread (its own thread-local workspace and stream) on which a direct
 // call builds its remembered FP64 heads while the calling thread runs the FP32 pass.  It is
@@ -346,15 +500,15 @@ private:
 // rounding run on the device; a host output stages its compared rows up and its patched
 // rows down (one copy per run of consecutive output rows).
 Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t st, bool patch,
-                   PreHeads* pre = nullptr) {
+                   PreHeads* pre = nullptr, bool trusted = false, const std::vector<uint64_t>* fps = nullptr) {
     const double tol = g_guard_tol.load();
     BuildOptions o64 = opt;
     o64.fp32 = false;
     o64.fcr_ms = nullptr;
-    // plans (patch == false) compare every head row of device outputs: the row profile sets
-    // the head they replay; their first head is a quarter of the series, a direct call's a
-    // sixteenth (its heads are recomputed every call)
-    auto profile = [&](std::size_t a) { return !patch && insts[a].out_on_device; };
+    // every head row is compared: the row profile sets the head a plan replays, and the head
+    // a direct call remembers for its next call on the same inputs; a plan's first head is a
+    // quarter of the series, a direct call's a sixteenth
+    auto profile = [&](std::size_t) { return true; };
     std::vector<Head> pending;
     for (std::size_t a = 0; a < insts.size(); ++a) {
         if (insts[a].tidx.empty()) continue;
@@ -363,15 +517,16 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
         uint32_t H = static_cast<uint32_t>(std::min<std::size_t>(tc, std::max<std::size_t>(kMinHead, (tc + frac - 1) / frac)));
         if (patch) {
             auto it = t_head_memory.find({insts[a].gamma, tc});
-            if (it != t_head_memory.end()) H = it->second;
+            if (it != t_head_memory.end() && it->second.accepted) H = it->second.accepted;
         }
         Head h = make_head(insts, a, H, tc, profile(a));
         if (!h.times.empty()) pending.push_back(std::move(h));
     }
     if (pre) pending = pre->heads;  // built already: the first round only evaluates them
     Decision dec;
-    DevMem temp, meta, rowsums, stage, hpatch;
-    std::vector<float2> stage_host;
+    GuardScratch& gs = guard_scratch();
+    DevMem &temp = gs.temp, &meta = gs.meta, &rowsums = gs.rowsums, &stage = gs.stage, &hpatch = gs.hpatch;
+    std::vector<float2>& stage_host = gs.stage_host;
     t_stats = GuardStats{};
     t_stats.instances = insts.size();
     while (!pending.empty()) {
@@ -383,13 +538,12 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
             std::vector<std::size_t> off;
             double2* base = nullptr;
             if (prebuilt) {
-                base = static_cast<double2*>(pre->temp.p);
+                base = static_cast<double2*>(pre->temp->p);
                 off = pre->off;
             } else {
                 temp.ensure(std::max<std::size_t>(bytes, 256));
                 base = static_cast<double2*>(temp.p);
-                std::vector<Tcl4Instance> hi = head_instances(insts, pending, k0, k1, base, off);
-                tcl4_build_direct(hi, o64, st);  // synchronous
+                build_heads(insts, pending, k0, k1, base, off, o64, st);
             }
             // host outputs: their window rows staged up, their patched rows in a device buffer
             std::vector<std::size_t> soff(n, 0), poff(n, 0);
@@ -401,7 +555,7 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
                 const std::size_t E = entries(in);
                 soff[k - k0] = srows;
                 poff[k - k0] = prows;
-                srows += h.win.size() * E;
+                if (!(prebuilt && trusted)) srows += h.win.size() * E;  // trusted heads compare nothing
                 prows += h.pos.size() * E;
             }
             if (srows) {
@@ -423,6 +577,42 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
             if (prows) hpatch.ensure(prows * sizeof(float2));
             const float2* stage_p = static_cast<const float2*>(stage.p);
             float2* hpatch_p = static_cast<float2*>(hpatch.p);
+            if (prebuilt && trusted) {
+                // heads that a matching fingerprint says suffice: patch them, no comparison
+                std::vector<std::size_t> roff0(n, 0);
+                meta.ensure(job_image(insts, pending, k0, k1, base, off, nullptr).host.size() + 256);
+                JobImage img = job_image(insts, pending, k0, k1, base, off, static_cast<unsigned char*>(meta.p), stage_p,
+                                         &soff, hpatch_p, &poff, nullptr, &roff0);
+                cuda_check(cudaMemcpyAsync(meta.p, img.host.data(), img.host.size(), cudaMemcpyHostToDevice, st),
+                           "cudaMemcpyAsync(guard jobs)");
+                const dim3 grid(patch_blocks(insts, pending, k0, k1), static_cast<unsigned>(n));
+                k_guard_patch<<<grid, 256, 0, st>>>(static_cast<const GuardJob*>(meta.p));
+                cuda_check(cudaGetLastError(), "k_guard_patch");
+                count_launches(1);
+                for (std::size_t k = k0; k < k1; ++k) {
+                    const Head& h = pending[k];
+                    const Tcl4Instance& in = insts[h.inst];
+                    ++t_stats.heads;
+                    t_stats.head_rows += h.times.size();
+                    t_stats.rows += in.tidx.size();
+                    if (h.H >= h.tc) ++t_stats.full;
+                    if (in.out_on_device) continue;
+                    const std::size_t E = entries(in);
+                    float2* f = static_cast<float2*>(in.out);
+                    const float2* src = hpatch_p + poff[k - k0];
+                    std::size_t q = 0;
+                    while (q < h.pos.size()) {
+                        std::size_t r = q + 1;
+                        while (r < h.pos.size() && h.pos[r] == h.pos[r - 1] + 1) ++r;
+                        cuda_check(cudaMemcpyAsync(f + static_cast<std::size_t>(h.pos[q]) * E, src + q * E,
+                                                   (r - q) * E * sizeof(float2), cudaMemcpyDeviceToHost, st),
+                                   "cudaMemcpyAsync(guard rows)");
+                        q = r;
+                    }
+                }
+                cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(guard patch)");
+                return;
+            }
             // per compared row: (squared difference, squared FP64 norm)
             std::vector<std::size_t> roff(n, 0);
             std::size_t nrows = 0, most_win = 1;
@@ -527,13 +717,21 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
             if (patch) {
                 if (t_head_memory.size() > 65536) t_head_memory.clear();
                 for (std::size_t k = k0; k < k1; ++k)
-                    if (accept[k - k0]) t_head_memory[{insts[pending[k].inst].gamma, pending[k].tc}] = pending[k].H;
+                    if (accept[k - k0]) {
+                        HeadMemory& m = t_head_memory[{insts[pending[k].inst].gamma, pending[k].tc}];
+                        m.accepted = pending[k].H;
+                        m.required = final_h[k - k0];
+                        m.fingerprint = fps ? (*fps)[pending[k].inst] : 0;
+                    }
             }
             for (std::size_t k = k0; k < k1; ++k)
                 if (accept[k - k0]) {
                     const Head& h0 = pending[k];
-                    if (final_h[k - k0] == 0) continue;  // FP32 within the tolerance everywhere
-                    Head h = final_h[k - k0] == h0.H ? h0 : make_head(insts, h0.inst, final_h[k - k0], h0.tc);
+                    // a direct call has patched its whole accepted head; a plan replays the
+                    // head the profile requires
+                    const uint32_t keep = patch ? h0.H : final_h[k - k0];
+                    if (keep == 0) continue;  // FP32 within the tolerance everywhere
+                    Head h = keep == h0.H ? h0 : make_head(insts, h0.inst, keep, h0.tc);
                     if (h.times.empty()) continue;
                     ++t_stats.heads;
                     t_stats.head_rows += h.times.size();
@@ -552,6 +750,11 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
 }  // namespace
 
 void set_fp32_guard(double tol) { g_guard_tol.store(tol > 0.0 ? tol : 0.0); }
+void release_guard_scratch() {
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    guard_scratch_map().erase(dev);
+}
 GuardStats fp32_guard_stats() { return t_stats; }
 double fp32_guard() { return g_guard_tol.load(); }
 
@@ -561,52 +764,75 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
         tcl4_build_direct(insts, opt, stream);
         return;
     }
+    cudaStream_t st = stream ? stream : default_stream();
     // the FP32 pass on a copy: a direct build may point an instance at device copies of its
     // host input and output that it frees before returning; the guard needs the caller's
     std::vector<Tcl4Instance> pass(insts);
-    // every instance's head remembered from an earlier call on its gamma buffer: build those
-    // heads on the helper thread while this thread runs the FP32 pass
+    const std::vector<uint64_t> fps = fingerprints(insts, st);
+    // every instance decided before on the same gamma contents: build the heads it requires
+    // on the helper thread while this thread runs the FP32 pass, then patch them
     PreHeads pre;
-    bool have_pre = true;
+    bool trusted = true;
     std::size_t pre_bytes = 0;
-    for (std::size_t a = 0; a < insts.size() && have_pre; ++a) {
+    for (std::size_t a = 0; a < insts.size() && trusted; ++a) {
         if (insts[a].tidx.empty()) continue;
         const uint32_t tc = t_count_of(insts[a]);
         auto it = t_head_memory.find({insts[a].gamma, tc});
-        if (it == t_head_memory.end()) {
-            have_pre = false;
+        if (it == t_head_memory.end() || it->second.fingerprint != fps[a] || it->second.accepted == 0) {
+            trusted = false;
             break;
         }
-        Head h = make_head(insts, a, it->second, tc);
+        if (it->second.required == 0) continue;  // FP32 suffices everywhere
+        Head h = make_head(insts, a, it->second.required, tc);
         pre_bytes += h.times.size() * entries(insts[a]) * sizeof(double2);
         if (!h.times.empty()) pre.heads.push_back(std::move(h));
     }
-    have_pre = have_pre && !pre.heads.empty() && pre_bytes <= kTempBytes;
-    if (have_pre) {
-        BuildOptions o64 = opt;
-        o64.fp32 = false;
-        o64.fcr_ms = nullptr;
-        pre.temp.ensure(std::max<std::size_t>(pre_bytes, 256));
-        std::vector<Tcl4Instance> hi =
-            head_instances(insts, pre.heads, 0, pre.heads.size(), static_cast<double2*>(pre.temp.p), pre.off);
-        int dev = 0;
-        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-        std::future<void> heads = HeadWorker::get().run([&hi, &o64, dev] {
-            cuda_check(cudaSetDevice(dev), "cudaSetDevice(guard worker)");
-            tcl4_build_direct(hi, o64, nullptr);
-        });
+    trusted = trusted && pre_bytes <= kTempBytes;
+    if (trusted) {
+        const auto t0 = std::chrono::steady_clock::now();
+        std::future<void> heads;
+        if (!pre.heads.empty()) {
+            BuildOptions o64 = opt;
+            o64.fp32 = false;
+            o64.fcr_ms = nullptr;
+            pre.temp = &guard_scratch().pre;
+            pre.temp->ensure(std::max<std::size_t>(pre_bytes, 256));
+            int dev = 0;
+            cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+            heads = HeadWorker::get().run([&insts, &pre, o64, dev] {
+                cuda_check(cudaSetDevice(dev), "cudaSetDevice(guard worker)");
+                std::vector<std::size_t> off;
+                build_heads(insts, pre.heads, 0, pre.heads.size(), static_cast<double2*>(pre.temp->p), off, o64, nullptr);
+                pre.off = off;
+            });
+        }
         try {
             tcl4_build_direct(pass, opt, stream);
         } catch (...) {
-            heads.wait();
+            if (heads.valid()) heads.wait();
             throw;
         }
-        heads.get();  // rethrows the helper's error
-        run_guard(insts, opt, stream ? stream : default_stream(), true, &pre);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (heads.valid()) heads.get();  // rethrows the helper's error
+        const auto t2 = std::chrono::steady_clock::now();
+        t_stats = GuardStats{};
+        t_stats.instances = insts.size();
+        if (!pre.heads.empty()) run_guard(insts, opt, st, true, &pre, true, &fps);
+        if (host_trace_on())
+            std::fprintf(stderr, "taco guard (ms, heads from memory): fp32 pass %.3f, heads wait %.3f, patch %.3f\n",
+                         std::chrono::duration<double, std::milli>(t1 - t0).count(),
+                         std::chrono::duration<double, std::milli>(t2 - t1).count(),
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t2).count());
         return;
     }
+    const auto t0 = std::chrono::steady_clock::now();
     tcl4_build_direct(pass, opt, stream);
-    run_guard(insts, opt, stream ? stream : default_stream(), true);
+    const auto t1 = std::chrono::steady_clock::now();
+    run_guard(insts, opt, st, true, nullptr, false, &fps);
+    if (host_trace_on())
+        std::fprintf(stderr, "taco guard (ms): fp32 pass %.3f, guard rounds %.3f\n",
+                     std::chrono::duration<double, std::milli>(t1 - t0).count(),
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count());
 }
 
 Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt) {
@@ -624,6 +850,7 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
         // the guard's direct builds grew this thread's transient buffers; the plans below
         // size theirs from the free memory
         release_workspace();
+        release_guard_scratch();
         if (dec.heads.empty()) return plan;
         // the heads as FP64 plans over one shared buffer of head rows, each followed by its patch
         BuildOptions o64 = opt;
@@ -631,6 +858,7 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
         o64.fcr_ms = nullptr;
         struct Part {
             Tcl4Plan* plan = nullptr;
+            std::vector<Tcl4Plan*> levels;  // short-FFT levels, replayed after the head
             std::size_t jobs = 0;
             unsigned blocks = 0;
             std::size_t meta_off = 0;
@@ -639,7 +867,10 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
             DevMem rows, meta, work;
             std::vector<Part> parts;
             ~TailState() {
-                for (auto& p : parts) plan_destroy(p.plan);
+                for (auto& p : parts) {
+                    plan_destroy(p.plan);
+                    for (Tcl4Plan* l : p.levels) plan_destroy(l);
+                }
             }
         };
         auto tail = std::make_shared<TailState>();
@@ -662,9 +893,20 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
         }
         tail->meta.ensure(meta_total + 256);
         // one transient buffer for every head plan (they run one after another)
+        std::vector<std::vector<std::vector<Tcl4Instance>>> lis(ranges.size());
+        for (std::size_t c = 0; c < ranges.size(); ++c)
+            for (uint32_t bound : kLevels)
+                lis[c].push_back(level_instances(insts, dec.heads, ranges[c].first, ranges[c].second, base, offs[c], bound));
+        // measured under the current budget; the plans group by that same budget, and the
+        // buffer has slack for the rounding of the slice sizes
+        const std::size_t budget = work_budget_now();
         std::size_t work_need = 256;
-        for (std::size_t c = 0; c < ranges.size(); ++c) work_need = std::max(work_need, plan_work_bytes(his[c], o64));
-        tail->work.ensure(work_need);
+        for (std::size_t c = 0; c < ranges.size(); ++c) {
+            work_need = std::max(work_need, plan_work_bytes(his[c], o64, budget));
+            for (auto& li : lis[c])
+                if (!li.empty()) work_need = std::max(work_need, plan_work_bytes(li, o64, budget));
+        }
+        tail->work.ensure(work_need + work_need / 8 + (std::size_t(1) << 20));
         uint64_t kernels = 0;
         std::size_t moff = 0;
         for (std::size_t c = 0; c < ranges.size(); ++c) {
@@ -672,7 +914,12 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
             JobImage im = job_image(insts, dec.heads, ranges[c].first, ranges[c].second, base, offs[c], dev);
             cuda_check(cudaMemcpy(dev, im.host.data(), im.host.size(), cudaMemcpyHostToDevice), "cudaMemcpy(guard jobs)");
             Part p;
-            p.plan = plan_create_direct(his[c], o64, tail->work.p, tail->work.cap);
+            p.plan = plan_create_direct(his[c], o64, tail->work.p, tail->work.cap, budget);
+            for (auto& li : lis[c])
+                if (!li.empty()) {
+                    p.levels.push_back(plan_create_direct(li, o64, tail->work.p, tail->work.cap, budget));
+                    kernels += plan_kernels(p.levels.back());
+                }
             p.jobs = ranges[c].second - ranges[c].first;
             p.blocks = patch_blocks(insts, dec.heads, ranges[c].first, ranges[c].second);
             p.meta_off = moff;
@@ -683,6 +930,7 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
         plan_set_tail(plan, [tail](cudaStream_t s) {
             for (const Part& p : tail->parts) {
                 plan_execute(p.plan, s);
+                for (Tcl4Plan* l : p.levels) plan_execute(l, s);
                 const GuardJob* jobs = reinterpret_cast<const GuardJob*>(static_cast<unsigned char*>(tail->meta.p) + p.meta_off);
                 k_guard_patch<<<dim3(p.blocks, static_cast<unsigned>(p.jobs)), 256, 0, s>>>(jobs);
                 cuda_check(cudaGetLastError(), "k_guard_patch");

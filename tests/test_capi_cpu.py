@@ -47,6 +47,14 @@ def test_fp32_guard_setting_roundtrip():
     assert tb.fp32_guard() == old
 
 
+def test_fused_conv_setting_roundtrip():
+    assert tb.fused_conv() is False  # the four-step passes are the default
+    tb.set_fused_conv(True)
+    assert tb.fused_conv() is True
+    tb.set_fused_conv(False)
+    assert tb.fused_conv() is False
+
+
 def _synthetic_system():
     g = np.load(os.path.join(GOLD, "synthetic_gamma.npz"))
     s = tb.System.from_arrays(int(g["N"]), g["omegas"], g["p2f"], list(g["ops"]), mirror=g["mirror"])

@@ -17,13 +17,14 @@ pytestmark = pytest.mark.gpu
 def build_both(inst, precision, **kw):
     """(fused, four-step) results of one batched build."""
     import torch
+    old = tb.fused_conv()
     try:
         tb.set_fused_conv(True)
         a = [x.cpu().numpy() for x in tb.build_instances(inst, precision=precision, **kw)]
         tb.set_fused_conv(False)
         b = [x.cpu().numpy() for x in tb.build_instances(inst, precision=precision, **kw)]
     finally:
-        tb.set_fused_conv(True)
+        tb.set_fused_conv(old)
     torch.cuda.synchronize()
     return a, b
 
@@ -84,12 +85,13 @@ def test_fused_batched_instances_match_four_step():
 def test_fused_fcr_series_match_four_step():
     """The F/C/R series entry point (FP64 sources) through both paths."""
     osys, s, G = spin_boson_case(2500, 0.005)
-    tb.set_fused_conv(True)
-    F1, C1, R1 = tb.compute_triple_kernels(s, G, 0.005)
-    tb.set_fused_conv(False)
+    old = tb.fused_conv()
     try:
+        tb.set_fused_conv(True)
+        F1, C1, R1 = tb.compute_triple_kernels(s, G, 0.005)
+        tb.set_fused_conv(False)
         F2, C2, R2 = tb.compute_triple_kernels(s, G, 0.005)
     finally:
-        tb.set_fused_conv(True)
+        tb.set_fused_conv(old)
     for a, b in ((F1, F2), (C1, C2), (R1, R2)):
         assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b)))
