@@ -734,7 +734,8 @@ def main():
     host_out = [torch.empty((T, N2 * N2), dtype=torch.complex64).pin_memory() for _ in range(B)]
     inst_h = [(s, hg.numpy(), args.dt, tidx) for s, hg in zip(systems, host_g)]
     outs_h = [o.numpy() for o in host_out]
-    tb.build_instances(inst_h, precision="fp32", outs=outs_h)
+    for _ in range(max(3, args.warmup)):  # the first call checks the heads, the second prepares them
+        tb.build_instances(inst_h, precision="fp32", outs=outs_h)
     barrier()
     e2e_times = []
     for _ in range(args.e2e_steps):

@@ -186,6 +186,20 @@ struct Workspace {
     };
     std::vector<std::unique_ptr<SubBuffers>> sub_bufs;
     cudaStream_t upload = nullptr;
+    // the download side of each lane of pipelined direct builds: staged host outputs (reused
+    // by the lane's next sub-batch once `done`), and the stream that carries their copies, so
+    // that the lane's next kernels do not queue behind them
+    struct Download {
+        DeviceBuffer out;
+        cudaStream_t s = nullptr;
+        cudaEvent_t contracted = nullptr, done = nullptr;
+        ~Download() {
+            if (contracted) cudaEventDestroy(contracted);
+            if (done) cudaEventDestroy(done);
+            if (s) cudaStreamDestroy(s);
+        }
+    };
+    Download down[3];
     std::map<std::pair<int, int>, std::unique_ptr<PlanTables>> plans;  // (L, fp32)
     std::map<std::pair<int, int>, std::unique_ptr<DeviceBuffer>> fz_tables;  // (N, fp32): fused-path roots
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -768,7 +782,7 @@ struct WorkPtrs {
 
 template <class R>
 void layout_work(const std::vector<WorkUnit*>& units, const GroupGeom<R>& G, bool fcr_only, bool fcr_out_dev,
-                 Layout& lay, WorkPtrs<cplx_t<R>>& P, bool gamma_elsewhere = false) {
+                 Layout& lay, WorkPtrs<cplx_t<R>>& P, bool gamma_elsewhere = false, bool out_elsewhere = false) {
     using C = cplx_t<R>;
     const std::size_t ni = units.size();
     P.gamma.assign(ni, nullptr);
@@ -785,7 +799,7 @@ void layout_work(const std::vector<WorkUnit*>& units, const GroupGeom<R>& G, boo
         if (!G.fused) P.conv[a] = lay.take<C>(nsub * 2 * m.t_count);
         if (!fcr_only) {
             P.v[a] = lay.take<C>(3 * nsub * m.U);
-            if (!in.out_on_device) {
+            if (!in.out_on_device && !out_elsewhere) {
                 const std::size_t E = static_cast<std::size_t>(in.sys.N) * in.sys.N * in.sys.N * in.sys.N;
                 P.out[a] = lay.take<C>(m.T * E);
             }
@@ -817,9 +831,9 @@ template <class R>
 Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cudaStream_t st, Workspace& ws,
                       DeviceBuffer& meta_mem, DeviceBuffer& work_mem, double2* const* fcr_out, bool fcr_out_dev,
                       PinnedBuffer* staging_buf = nullptr, DeviceBuffer* input_mem = nullptr,
-                      cudaStream_t upload = nullptr, cudaEvent_t uploaded = nullptr) {
+                      cudaStream_t upload = nullptr, cudaEvent_t uploaded = nullptr,
+                      Workspace::Download* down = nullptr) {
     using C = cplx_t<R>;
-    (void)opt;
     const auto t_prep = std::chrono::steady_clock::now();
     const GroupGeom<R> G = group_geom<R>(units);
     const int L = G.L;
@@ -847,11 +861,25 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     {
         // staged host gamma in `input_mem` when given (kept apart from the reused work arrays)
         const bool apart = input_mem != nullptr;
+        const bool out_apart = down != nullptr && !fcr_only;
         Layout meas;
-        layout_work<R>(units, G, fcr_only, fcr_out_dev, meas, P, apart);
+        layout_work<R>(units, G, fcr_only, fcr_out_dev, meas, P, apart, out_apart);
         work_mem.ensure(meas.off + 256);
         Layout lay{static_cast<char*>(work_mem.p)};
-        layout_work<R>(units, G, fcr_only, fcr_out_dev, lay, P, apart);
+        layout_work<R>(units, G, fcr_only, fcr_out_dev, lay, P, apart, out_apart);
+        if (out_apart) {
+            // staged host outputs in the lane's download buffer
+            Layout mo;
+            for (auto* u : units)
+                if (!u->in->out_on_device)
+                    mo.take<C>(u->meta->T * static_cast<std::size_t>(u->in->sys.N) * u->in->sys.N * u->in->sys.N * u->in->sys.N);
+            down->out.ensure(mo.off + 256);
+            Layout lo{static_cast<char*>(down->out.p)};
+            for (std::size_t a = 0; a < ni; ++a)
+                if (!units[a]->in->out_on_device)
+                    P.out[a] = lo.take<C>(units[a]->meta->T * static_cast<std::size_t>(units[a]->in->sys.N) *
+                                          units[a]->in->sys.N * units[a]->in->sys.N * units[a]->in->sys.N);
+        }
         if (apart) {
             Layout mi;
             for (auto* u : units)
@@ -1210,6 +1238,15 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         for (int kind = 0; kind < 3; ++kind)
             d2h.push_back({fcr_out[kind], P.v[0] + kind * nf3 * U, nf3 * U * sizeof(C)});
     }
+    // whole instances of the group with the device address of their rows, for opt.out_hook
+    std::vector<std::pair<const Tcl4Instance*, void*>> hooked;
+    if (!fcr_only && opt.out_hook)
+        for (std::size_t a = 0; a < ni; ++a) {
+            const WorkUnit& u = *units[a];
+            if (u.accumulate || u.lo != 0 || u.hi != u.in->sys.nf * u.in->sys.nf * u.in->sys.nf) continue;
+            hooked.emplace_back(u.in, u.in->out_on_device ? u.in->out : static_cast<void*>(P.out[a]));
+        }
+    const auto out_hook = opt.out_hook;
     const std::size_t n_scan = ntri;
     // single-pass scan (one CTA per triple) once the triples alone fill the GPU four times
     // over; the chunked reduce-then-scan otherwise
@@ -1305,6 +1342,8 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
     }
     if (ev1) cuda_check(cudaEventRecord(ev1, st), "cudaEventRecord");
     if (!fcr_only) {
+        // the lane's previous sub-batch has left the output staging
+        if (down && !d2h.empty()) cuda_check(cudaStreamWaitEvent(st, down->done, 0), "cudaStreamWaitEvent(download)");
         pr.before(f32 ? "contract_f32" : "contract_f64");
         if (rows_d2) {
             const unsigned gx = static_cast<unsigned>((maxT + OT - 1) / OT);
@@ -1327,8 +1366,17 @@ Enqueue prepare_group(std::vector<WorkUnit*>& units, const BuildOptions& opt, cu
         }
         check_launch("k_contract", &pr);
     }
+    cudaStream_t ds = st;
+    if (down && !d2h.empty()) {
+        cuda_check(cudaEventRecord(down->contracted, st), "cudaEventRecord(contracted)");
+        cuda_check(cudaStreamWaitEvent(down->s, down->contracted, 0), "cudaStreamWaitEvent(contracted)");
+        ds = down->s;
+    }
+    // the hook's work goes where the downloads go: it does not hold up the lane's next kernels
+    if (!hooked.empty()) out_hook(hooked, ds);
     for (const D2H& c : d2h)
-        cuda_check(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(out)");
+        cuda_check(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, ds), "cudaMemcpyAsync(out)");
+    if (ds != st) cuda_check(cudaEventRecord(down->done, ds), "cudaEventRecord(download)");
     };
 }
 
@@ -1501,6 +1549,10 @@ void release_workspace() {
         b->arena.release();
         b->input.release();
         b->staging.release();
+    }
+    for (auto& d : ws.down) {
+        if (d.s) cuda_check(cudaStreamSynchronize(d.s), "cudaStreamSynchronize(release)");
+        d.out.release();
     }
 }
 bool fused_conv() { return g_fused.load() != 0; }
@@ -1688,12 +1740,20 @@ void tcl4_build_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt
         lap("groups");
     } else {
         // sub-batches of kPipeSub instances or more (rounded count per group)
+        // (the first group starts with a third of that: its outputs start downloading early)
         std::vector<std::vector<WorkUnit*>> subs;
         std::size_t max_work = 0, max_input = 0;
+        bool first = true;
         for (auto& gu : groups) {
-            const std::size_t n = gu.size(), parts = std::max<std::size_t>(1, (n + kPipeSub / 2) / kPipeSub);
-            for (std::size_t p = 0; p < parts; ++p) {
-                subs.emplace_back(gu.begin() + p * n / parts, gu.begin() + (p + 1) * n / parts);
+            const std::size_t b0 = first && gu.size() > kPipeSub ? kPipeSub / 3 : 0;
+            first = false;
+            const std::size_t n = gu.size() - b0, parts = std::max<std::size_t>(1, (n + kPipeSub / 2) / kPipeSub);
+            for (std::size_t p = 0; p < parts + (b0 ? 1 : 0); ++p) {
+                if (b0 && p == 0) subs.emplace_back(gu.begin(), gu.begin() + b0);
+                else {
+                    const std::size_t q = b0 ? p - 1 : p;
+                    subs.emplace_back(gu.begin() + b0 + q * n / parts, gu.begin() + b0 + (q + 1) * n / parts);
+                }
                 max_work = std::max(max_work, opt.fp32 ? measure_work<float>(subs.back(), false, false)
                                                        : measure_work<double>(subs.back(), false, false));
                 std::size_t in_bytes = 0;
@@ -1735,43 +1795,51 @@ void tcl4_build_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt
             cuda_check(cudaEventCreateWithFlags(&ws.sub_bufs.back()->done, cudaEventDisableTiming), "cudaEventCreate");
         }
         for (auto& L : lanes) L.work->ensure(max_work);
+        // each lane downloads on its own stream (created once)
+        for (std::size_t l = 0; l < nlanes; ++l) {
+            auto& d = ws.down[l];
+            if (!d.s) {
+                cuda_check(cudaStreamCreateWithFlags(&d.s, cudaStreamNonBlocking), "cudaStreamCreate");
+                cuda_check(cudaEventCreateWithFlags(&d.contracted, cudaEventDisableTiming), "cudaEventCreate");
+                cuda_check(cudaEventCreateWithFlags(&d.done, cudaEventDisableTiming), "cudaEventCreate");
+            }
+            // the previous build's downloads are complete (the build ended with them); a
+            // fresh event makes the first wait of this build a no-op
+            cuda_check(cudaEventRecord(d.done, d.s), "cudaEventRecord");
+        }
         // traced calls time each sub-batch on the device: lane start, inputs uploaded,
         // F/C/R done, outputs downloaded
         std::vector<cudaEvent_t> evs(lap.on ? 4 * subs.size() : 0);
         for (auto& e : evs) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
-        // in waves of nslots sub-batches: every upload of a wave is queued before any of its
-        // downloads (a download queued first, while it waits for its kernels, held back the
-        // uploads queued after it)
-        for (std::size_t w0 = 0; w0 < subs.size(); w0 += nslots) {
-            const std::size_t w1 = std::min(subs.size(), w0 + nslots);
-            std::vector<Enqueue> enqs;
-            for (std::size_t k = w0; k < w1; ++k) {
-                const Lane& L = lanes[k % nlanes];
-                Workspace::SubBuffers& sb = *ws.sub_bufs[k % nslots];
-                if (k >= nslots) {
-                    cuda_check(cudaEventSynchronize(sb.done), "cudaEventSynchronize(slot)");
-                    lap("slot_wait");
-                }
-                enqs.push_back(opt.fp32 ? prepare_group<float>(subs[k], opt, L.s, ws, sb.arena, *L.work, nullptr, false,
-                                                               &sb.staging, &sb.input, ws.upload, sb.uploaded)
-                                        : prepare_group<double>(subs[k], opt, L.s, ws, sb.arena, *L.work, nullptr, false,
-                                                                &sb.staging, &sb.input, ws.upload, sb.uploaded));
-                lap("prepare");
+        // each sub-batch is enqueued as soon as it is prepared: its upload on the upload stream,
+        // its kernels on its lane (after the upload), its download on the lane's download
+        // stream (the lane's next kernels do not wait for it)
+        for (std::size_t k = 0; k < subs.size(); ++k) {
+            const Lane& L = lanes[k % nlanes];
+            Workspace::SubBuffers& sb = *ws.sub_bufs[k % nslots];
+            if (k >= nslots) {
+                cuda_check(cudaEventSynchronize(sb.done), "cudaEventSynchronize(slot)");
+                lap("slot_wait");
             }
-            for (std::size_t k = w0; k < w1; ++k) {
-                const Lane& L = lanes[k % nlanes];
-                if (lap.on) cuda_check(cudaEventRecord(evs[4 * k], L.s), "cudaEventRecord");
-                cuda_check(cudaStreamWaitEvent(L.s, ws.sub_bufs[k % nslots]->uploaded, 0), "cudaStreamWaitEvent(uploaded)");
-                if (lap.on) cuda_check(cudaEventRecord(evs[4 * k + 1], L.s), "cudaEventRecord");
-                enqs[k - w0](L.s, nullptr, nullptr, lap.on ? evs[4 * k + 2] : nullptr);
-                cuda_check(cudaEventRecord(ws.sub_bufs[k % nslots]->done, L.s), "cudaEventRecord(slot)");
-                if (lap.on) cuda_check(cudaEventRecord(evs[4 * k + 3], L.s), "cudaEventRecord");
-                lap("enqueue");
-            }
+            Workspace::Download* dl = &ws.down[k % nlanes];
+            Enqueue enq = opt.fp32 ? prepare_group<float>(subs[k], opt, L.s, ws, sb.arena, *L.work, nullptr, false,
+                                                          &sb.staging, &sb.input, ws.upload, sb.uploaded, dl)
+                                   : prepare_group<double>(subs[k], opt, L.s, ws, sb.arena, *L.work, nullptr, false,
+                                                           &sb.staging, &sb.input, ws.upload, sb.uploaded, dl);
+            lap("prepare");
+            if (lap.on) cuda_check(cudaEventRecord(evs[4 * k], L.s), "cudaEventRecord");
+            cuda_check(cudaStreamWaitEvent(L.s, sb.uploaded, 0), "cudaStreamWaitEvent(uploaded)");
+            if (lap.on) cuda_check(cudaEventRecord(evs[4 * k + 1], L.s), "cudaEventRecord");
+            enq(L.s, nullptr, nullptr, lap.on ? evs[4 * k + 2] : nullptr);
+            cuda_check(cudaEventRecord(sb.done, L.s), "cudaEventRecord(slot)");
+            if (lap.on) cuda_check(cudaEventRecord(evs[4 * k + 3], dl->s), "cudaEventRecord");
+            lap("enqueue");
         }
         for (std::size_t l = 1; l < nlanes; ++l)
             cuda_check(cudaStreamSynchronize(lanes[l].s), "cudaStreamSynchronize(lane)");
         cuda_check(cudaStreamSynchronize(ws.upload), "cudaStreamSynchronize(upload)");
+        for (std::size_t l = 0; l < nlanes; ++l)
+            cuda_check(cudaStreamSynchronize(ws.down[l].s), "cudaStreamSynchronize(download)");
         lap("lane_wait");
         if (lap.on) {
             cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(build)");
@@ -1916,10 +1984,11 @@ struct Tcl4Plan {
     uint64_t kernels = 0;
     // work enqueued after the graph on every execute (the FP64 heads of the FP32 form),
     // holding the buffers and plans it uses; its kernel count
-    std::function<void(cudaStream_t)> tail;
+    std::function<void(cudaStream_t)> pre, tail;
     uint64_t tail_kernels = 0;
     ~Tcl4Plan() {
-        tail = nullptr;  // the tail's plans and buffers go before the stream
+        pre = nullptr;  // the pre and tail work's plans and buffers go before the stream
+        tail = nullptr;
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (stream) cudaStreamDestroy(stream);
@@ -2047,16 +2116,40 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
 
 std::size_t work_budget_now() { return work_budget(); }
 
+// Transient arrays of a plan's groups.  Groups of whole instances run concurrently (branches
+// of the plan's graph, each group in its own region of the buffer) when their sum fits `cap`;
+// otherwise, or when an instance is built in slices (its slices accumulate into one output
+// in order), one after another in one shared region.
+struct PlanWork {
+    std::vector<std::size_t> each;  // bytes of each group
+    std::size_t total = 0;
+    bool concurrent = false;
+};
+PlanWork plan_work(const std::vector<std::vector<WorkUnit*>>& groups, bool fp32, std::size_t cap) {
+    PlanWork w;
+    std::size_t most = 0, sum = 0;
+    bool whole = true;
+    for (auto& gu : groups) {
+        std::vector<WorkUnit*> g(gu);
+        const std::size_t b = fp32 ? measure_work<float>(g, false, false) : measure_work<double>(g, false, false);
+        w.each.push_back(b);
+        most = std::max(most, b);
+        sum += align_up(b, std::size_t(256));
+        for (auto* u : gu)
+            whole = whole && !u->accumulate && u->lo == 0 && u->hi == u->in->sys.nf * u->in->sys.nf * u->in->sys.nf;
+    }
+    w.concurrent = groups.size() > 1 && whole && sum <= cap;
+    w.total = w.concurrent ? sum : most;
+    return w;
+}
+
 std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, std::size_t budget) {
     std::vector<InstMeta> metas;
     validate_and_derive(insts, opt, metas);
     std::vector<std::unique_ptr<WorkUnit>> store;
     std::vector<std::vector<WorkUnit*>> groups =
         opt.fp32 ? plan_units<float>(insts, metas, budget, store) : plan_units<double>(insts, metas, budget, store);
-    std::size_t work = 0;
-    for (auto& gu : groups)
-        work = std::max(work, opt.fp32 ? measure_work<float>(gu, false, false) : measure_work<double>(gu, false, false));
-    return work;
+    return plan_work(groups, opt.fp32, budget).total;
 }
 
 Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, void* ext_work,
@@ -2066,6 +2159,8 @@ Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOption
             throw Error(kInvalidArgument, "plans take device inputs and outputs (TACO_IN_DEVICE | TACO_OUT_DEVICE)");
     std::vector<InstMeta> metas;
     validate_and_derive(insts, opt, metas);
+    BuildOptions popt = opt;
+    popt.out_hook = nullptr;  // a replayed graph calls no host code
     auto plan = std::make_unique<Tcl4Plan>();
     cuda_check(cudaGetDevice(&plan->device), "cudaGetDevice");
     cuda_check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate(plan)");
@@ -2075,28 +2170,59 @@ Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOption
     const std::size_t budget = ext_work ? (budget_in ? budget_in : ext_cap) : work_budget();
     std::vector<std::vector<WorkUnit*>> groups =
         opt.fp32 ? plan_units<float>(insts, metas, budget, plan->units) : plan_units<double>(insts, metas, budget, plan->units);
-    // one transient buffer shared by the groups (they run in order on the plan's stream),
-    // sized before any group records its pointers
-    std::size_t work = 0;
-    for (auto& gu : groups)
-        work = std::max(work, opt.fp32 ? measure_work<float>(gu, false, false) : measure_work<double>(gu, false, false));
+    // one transient buffer, sized before any group records its pointers: a region per group
+    // when the groups run concurrently, else one region they share in order
+    const PlanWork pw = plan_work(groups, opt.fp32, ext_work ? ext_cap : budget);
     if (ext_work) {  // a caller's buffer shared by plans that run one after another
         plan->work.p = ext_work;
         plan->work.cap = ext_cap;
         plan->work.owned = false;
     }
-    plan->work.ensure(work);
-    for (auto& gu : groups) {
+    plan->work.ensure(pw.total);
+    std::size_t region = 0;
+    for (std::size_t gi = 0; gi < groups.size(); ++gi) {
+        auto& gu = groups[gi];
+        DeviceBuffer view;  // the group's region (prepare_group records pointers into it)
+        view.owned = false;
+        view.p = static_cast<char*>(plan->work.p) + region;
+        view.cap = pw.concurrent ? pw.each[gi] : plan->work.cap;
+        if (pw.concurrent) region += align_up(pw.each[gi], std::size_t(256));
         plan->mems.push_back(std::make_unique<DeviceBuffer>());
         if (opt.fp32)
-            plan->enqs.push_back(prepare_group<float>(gu, opt, plan->stream, ws, *plan->mems.back(), plan->work, nullptr, false));
+            plan->enqs.push_back(prepare_group<float>(gu, popt, plan->stream, ws, *plan->mems.back(), view, nullptr, false));
         else
-            plan->enqs.push_back(prepare_group<double>(gu, opt, plan->stream, ws, *plan->mems.back(), plan->work, nullptr, false));
+            plan->enqs.push_back(prepare_group<double>(gu, popt, plan->stream, ws, *plan->mems.back(), view, nullptr, false));
+    }
+    // concurrent groups: captured as branches forked from and joined into the plan's stream
+    struct Branches {
+        std::vector<cudaStream_t> s;
+        std::vector<cudaEvent_t> e;
+        ~Branches() {
+            for (auto x : s) cudaStreamDestroy(x);
+            for (auto x : e) cudaEventDestroy(x);
+        }
+    } br;
+    if (pw.concurrent) {
+        br.s.assign(groups.size() - 1, nullptr);
+        br.e.assign(groups.size(), nullptr);
+        for (auto& x : br.s) cuda_check(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking), "cudaStreamCreate(branch)");
+        for (auto& x : br.e) cuda_check(cudaEventCreateWithFlags(&x, cudaEventDisableTiming), "cudaEventCreate(branch)");
     }
     const uint64_t k0 = g_launches.load();
     cuda_check(cudaStreamBeginCapture(plan->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     try {
-        for (auto& e : plan->enqs) e(plan->stream, nullptr, nullptr, nullptr);
+        if (pw.concurrent) {
+            cuda_check(cudaEventRecord(br.e[0], plan->stream), "cudaEventRecord(fork)");
+            for (auto x : br.s) cuda_check(cudaStreamWaitEvent(x, br.e[0], 0), "cudaStreamWaitEvent(fork)");
+            plan->enqs[0](plan->stream, nullptr, nullptr, nullptr);
+            for (std::size_t gi = 1; gi < groups.size(); ++gi) {
+                plan->enqs[gi](br.s[gi - 1], nullptr, nullptr, nullptr);
+                cuda_check(cudaEventRecord(br.e[gi], br.s[gi - 1]), "cudaEventRecord(join)");
+                cuda_check(cudaStreamWaitEvent(plan->stream, br.e[gi], 0), "cudaStreamWaitEvent(join)");
+            }
+        } else {
+            for (auto& e : plan->enqs) e(plan->stream, nullptr, nullptr, nullptr);
+        }
     } catch (...) {
         cudaGraph_t g = nullptr;
         cudaStreamEndCapture(plan->stream, &g);
@@ -2116,12 +2242,15 @@ void plan_execute(Tcl4Plan* plan, cudaStream_t stream) {
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev != plan->device) throw Error(kInvalidArgument, "plan belongs to another device");
     // asynchronous on exactly the caller's stream (0 is the legacy default stream)
+    if (plan->pre) plan->pre(stream);
     cuda_check(cudaGraphLaunch(plan->exec, stream), "cudaGraphLaunch");
     g_launches.fetch_add(plan->kernels);
     if (plan->tail) plan->tail(stream);
 }
 
-void plan_set_tail(Tcl4Plan* plan, std::function<void(cudaStream_t)> tail, uint64_t kernels) {
+void plan_set_tail(Tcl4Plan* plan, std::function<void(cudaStream_t)> pre, std::function<void(cudaStream_t)> tail,
+                   uint64_t kernels) {
+    plan->pre = std::move(pre);
     plan->tail = std::move(tail);
     plan->tail_kernels = kernels;
 }

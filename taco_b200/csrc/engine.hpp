@@ -96,6 +96,12 @@ struct BuildOptions {
     bool causal_truncation = false;  // FFT length from max(tidx)+1 instead of Nt
     std::size_t pad_factor = 0;      // Nfft = next_pow2(max(2 n - 1, pad * n))
     double* fcr_ms = nullptr;        // device time of the F/C/R stage
+    // Called with a stream ordered after a group's contraction, which has written the rows
+    // [T][E] of the whole (unsliced) instances it lists -- each with the device address of its
+    // rows, the output itself or its staging for a host output -- and before any of those rows
+    // is downloaded (the downloads follow on that stream).  A build lists every instance at
+    // most once and has finished the hook's work when it returns.  Plans ignore it.
+    std::function<void(const std::vector<std::pair<const Tcl4Instance*, void*>>&, cudaStream_t)> out_hook;
 };
 
 // Full L4 builds (build_TCL4_generator_cuda_fused[_batch]) for a set of instances.  In the
@@ -120,8 +126,10 @@ std::size_t plan_work_bytes(std::vector<Tcl4Instance>& insts, const BuildOptions
 std::size_t work_budget_now();
 // Frees the calling thread's precision-guard buffers on the current device.
 void release_guard_scratch();
-// Work enqueued after the plan's graph on every execute (owns what it captures).
-void plan_set_tail(Tcl4Plan* plan, std::function<void(cudaStream_t)> tail, uint64_t kernels);
+// Work enqueued on every execute before the plan's graph (`pre`, may be empty) and after it
+// (`tail`), on the execute's stream; each owns what it captures.
+void plan_set_tail(Tcl4Plan* plan, std::function<void(cudaStream_t)> pre, std::function<void(cudaStream_t)> tail,
+                   uint64_t kernels);
 void plan_execute(Tcl4Plan* plan, cudaStream_t stream);
 void plan_destroy(Tcl4Plan* plan);
 uint64_t plan_kernels(const Tcl4Plan* plan);

@@ -29,9 +29,11 @@
 // replays the FP32 graph followed by those FP64 heads and the row patch; a plan replayed on
 // different inputs keeps the heads chosen at creation.  A direct call patches its whole
 // accepted head and remembers, per gamma buffer, the accepted and the needed head and a
-// fingerprint of the buffer's contents; a later call with the same fingerprint builds only
-// the needed heads, on a helper thread during the FP32 pass, and patches them without a
-// comparison, while a changed fingerprint is checked again from the accepted head.
+// fingerprint of the buffer's contents; a later call with the same fingerprint replays only
+// the needed heads -- prepared FP64 plans, kept while consecutive calls have the same heads --
+// on a side stream beside the FP32 pass, whose groups patch them on the device before their
+// outputs are downloaded (no comparison), while a changed fingerprint is checked again from
+// the accepted head.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,14 +42,11 @@
 #include <cstdio>
 #include <cmath>
 #include <cstdint>
-#include <condition_variable>
 #include <cstring>
-#include <deque>
 #include <functional>
-#include <future>
 #include <map>
-#include <mutex>
-#include <thread>
+#include <string>
+#include <tuple>
 #include <memory>
 #include <vector>
 
@@ -153,7 +152,7 @@ uint64_t fnv1a(uint64_t h, const void* p, std::size_t n) {
     return h;
 }
 
-constexpr int kPrintSamples = 64;  // gamma samples per bucket in a fingerprint
+constexpr int kPrintSamples = 16;  // gamma samples per bucket in a fingerprint (first and last included)
 
 __global__ void k_guard_gather(const double2* const* __restrict__ src, double2* __restrict__ out, uint32_t n) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -162,7 +161,8 @@ __global__ void k_guard_gather(const double2* const* __restrict__ src, double2* 
 
 // Fingerprints of the instances' gamma (the consumed samples of every bucket at 64 evenly
 // spaced times, with the sizes and dt); device inputs are gathered by one launch.
-std::vector<uint64_t> fingerprints(const std::vector<Tcl4Instance>& insts, cudaStream_t st) {
+std::vector<uint64_t> fingerprints(const std::vector<Tcl4Instance>& insts, const std::vector<uint32_t>& tcs,
+                                   cudaStream_t st) {
     const std::size_t n = insts.size();
     std::vector<uint64_t> fp(n, 0);
     std::vector<const double2*> addr;
@@ -171,8 +171,7 @@ std::vector<uint64_t> fingerprints(const std::vector<Tcl4Instance>& insts, cudaS
     for (std::size_t a = 0; a < n; ++a) {
         const Tcl4Instance& in = insts[a];
         if (in.tidx.empty()) continue;
-        uint32_t tc = 0;
-        for (uint32_t t : in.tidx) tc = std::max(tc, t + 1);
+        const uint32_t tc = tcs[a];
         const std::size_t n_in = std::min<std::size_t>(in.Nt, tc);
         first[a] = addr.size();
         for (int b = 0; b < in.sys.nf; ++b)
@@ -240,6 +239,7 @@ struct Head {
     std::size_t inst = 0;
     uint32_t H = 0, tc = 0;
     std::vector<uint32_t> times, pos, win;
+    uint64_t rows_hash = 0;  // of times and pos
 };
 
 Head make_head(const std::vector<Tcl4Instance>& insts, std::size_t a, uint32_t H, uint32_t tc, bool all_rows = false) {
@@ -263,6 +263,8 @@ Head make_head(const std::vector<Tcl4Instance>& insts, std::size_t a, uint32_t H
         std::sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return h.times[x] > h.times[y]; });
         upper.assign(ord.begin(), ord.begin() + std::max<std::size_t>(1, ord.size() / 4));
     }
+    h.rows_hash = fnv1a(fnv1a(1469598103934665603ull, h.times.data(), h.times.size() * sizeof(uint32_t)), h.pos.data(),
+                        h.pos.size() * sizeof(uint32_t));
     if (all_rows) {  // every head row (the row profile that sets a plan's final head)
         h.win.resize(h.times.size());
         for (std::size_t k = 0; k < h.win.size(); ++k) h.win[k] = static_cast<uint32_t>(k);
@@ -273,6 +275,30 @@ Head make_head(const std::vector<Tcl4Instance>& insts, std::size_t a, uint32_t H
     }
     return h;
 }
+
+// Per call: the t_count and the head templates of each distinct time list (the instances of
+// a call that name one caller array share one list, so each is scanned once).
+class TimeCache {
+public:
+    uint32_t t_count(const Tcl4Instance& in) {
+        if (in.tidx.empty()) return 0;
+        auto it = tc_.find(in.tidx.identity());
+        if (it == tc_.end()) it = tc_.emplace(in.tidx.identity(), t_count_of(in)).first;
+        return it->second;
+    }
+    Head head(const std::vector<Tcl4Instance>& insts, std::size_t a, uint32_t H, uint32_t tc, bool all_rows = false) {
+        const auto key = std::make_tuple(insts[a].tidx.identity(), H, all_rows);
+        auto it = heads_.find(key);
+        if (it == heads_.end()) it = heads_.emplace(key, make_head(insts, a, H, tc, all_rows)).first;
+        Head h = it->second;
+        h.inst = a;
+        return h;
+    }
+
+private:
+    std::map<const void*, uint32_t> tc_;
+    std::map<std::tuple<const void*, uint32_t, bool>, Head> heads_;
+};
 
 // FP64 builds of the heads of `heads` (into one device buffer of head rows), chunked so
 // that each chunk's rows fit kTempBytes (a single head may exceed it).
@@ -436,10 +462,31 @@ struct PreHeads {
     std::vector<std::size_t> off;
 };
 
+// Grow-only pinned host memory (asynchronous uploads from it do not wait for the device).
+struct PinnedMem {
+    void* p = nullptr;
+    std::size_t cap = 0;
+    void ensure(std::size_t bytes) {
+        if (bytes <= cap) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        cuda_check(cudaHostAlloc(&p, bytes, cudaHostAllocDefault), "cudaHostAlloc(guard)");
+        cap = bytes;
+    }
+    PinnedMem() = default;
+    PinnedMem(const PinnedMem&) = delete;
+    PinnedMem& operator=(const PinnedMem&) = delete;
+    ~PinnedMem() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
 // The guard's device buffers of the calling thread and device: grow-only and kept across calls
 // (allocating and freeing them every call synchronised the device and cost milliseconds).
 struct GuardScratch {
-    DevMem temp, meta, rowsums, stage, hpatch, pre;
+    DevMem temp, meta, rowsums, stage, hpatch, jobs;
+    PinnedMem jobs_host;
     std::vector<float2> stage_host;
 };
 std::map<int, std::unique_ptr<GuardScratch>>& guard_scratch_map() {
@@ -454,46 +501,6 @@ GuardScratch& guard_scratch() {
     return *p;
 }
 
-// A persistent helper thread (its own thread-local workspace and stream) on which a direct
-// call builds its remembered FP64 heads while the calling thread runs the FP32 pass.  It is
-// created on first use and lives until the process exits.
-class HeadWorker {
-public:
-    static HeadWorker& get() {
-        static HeadWorker* w = new HeadWorker();  // never destroyed: no CUDA calls at exit
-        return *w;
-    }
-    std::future<void> run(std::function<void()> fn) {
-        std::packaged_task<void()> task(std::move(fn));
-        std::future<void> f = task.get_future();
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            q_.push_back(std::move(task));
-        }
-        cv_.notify_one();
-        return f;
-    }
-
-private:
-    HeadWorker() {
-        std::thread([this] {
-            for (;;) {
-                std::packaged_task<void()> task;
-                {
-                    std::unique_lock<std::mutex> lk(mu_);
-                    cv_.wait(lk, [this] { return !q_.empty(); });
-                    task = std::move(q_.front());
-                    q_.pop_front();
-                }
-                task();
-            }
-        }).detach();
-    }
-    std::mutex mu_;
-    std::condition_variable cv_;
-    std::deque<std::packaged_task<void()>> q_;
-};
-
 // Runs the guard loop: FP64 heads, comparison, growth.  With `patch`, accepted heads are
 // written into the outputs right away (direct calls); otherwise only the final heads are
 // returned (plans).  The FP32 results must already be in the outputs.  Comparison and
@@ -505,6 +512,7 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
     BuildOptions o64 = opt;
     o64.fp32 = false;
     o64.fcr_ms = nullptr;
+    o64.out_hook = nullptr;
     // every head row is compared: the row profile sets the head a plan replays, and the head
     // a direct call remembers for its next call on the same inputs; a plan's first head is a
     // quarter of the series, a direct call's a sixteenth
@@ -747,6 +755,241 @@ Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cu
     return dec;
 }
 
+// A direct call's remembered heads as prepared FP64 plans -- the heads, then each short-FFT
+// level over the heads' first rows -- replayed on a side stream while the FP32 pass runs; the
+// pass's groups wait for them on the device and patch.  Host gamma is copied each call (from
+// the caller's buffers, on the side stream) into a device buffer of the samples the heads
+// consume.  One set per thread and device, kept while
+// consecutive calls have the same heads (instances, systems, buffers, times, head lengths).
+struct HeadPlans {
+    uint64_t key = 0;
+    std::vector<std::size_t> off;      // first element of each head's rows in `rows`
+    std::vector<std::size_t> pos_off;  // first entry of each head's output positions in `pos`
+    DevMem rows, work, gam, pos;
+    struct Upload {
+        const double2* src;
+        std::size_t nf, stride, n, dst;  // buckets, source stride, samples per bucket, first element in gam
+        uint32_t chunk;
+    };
+    std::vector<Upload> uploads;
+    std::size_t gam_elems = 0;
+    // The heads in chunks of the call's instance order (the FP32 pass downloads its first
+    // instances first): each chunk's head and level plans, and the event after them.
+    struct Chunk {
+        std::vector<Tcl4Plan*> plans;
+        cudaEvent_t ready = nullptr;
+    };
+    std::vector<Chunk> chunks;
+    std::vector<uint32_t> chunk_of;  // per head
+    cudaStream_t s = nullptr;
+    cudaEvent_t start = nullptr;
+    bool launched = false;
+    bool empty() const { return chunks.empty(); }
+    cudaEvent_t ready() const { return chunks.back().ready; }
+    void drop() {
+        for (auto& c : chunks) {
+            for (Tcl4Plan* p : c.plans) plan_destroy(p);
+            if (c.ready) cudaEventDestroy(c.ready);
+        }
+        chunks.clear();
+        launched = false;
+        key = 0;
+    }
+    HeadPlans() = default;
+    HeadPlans(const HeadPlans&) = delete;
+    HeadPlans& operator=(const HeadPlans&) = delete;
+    ~HeadPlans() {
+        drop();
+        if (start) cudaEventDestroy(start);
+        if (s) cudaStreamDestroy(s);
+    }
+};
+// Instance-index bounds of the head chunks: the first 16 instances (the pass's short first
+// sub-batch), the next 48, the rest.
+constexpr std::size_t kChunkBounds[] = {16, 64};
+std::map<int, std::unique_ptr<HeadPlans>>& head_plans_map() {
+    thread_local std::map<int, std::unique_ptr<HeadPlans>> m;
+    return m;
+}
+HeadPlans& head_plans() {
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    auto& p = head_plans_map()[dev];
+    if (!p) p = std::make_unique<HeadPlans>();
+    return *p;
+}
+
+uint64_t system_hash(uint64_t h, const SystemDesc& s) {
+    const int head[3] = {s.N, s.nf, s.num_ops};
+    h = fnv1a(h, head, sizeof(head));
+    h = fnv1a(h, s.omegas.data(), s.omegas.size() * sizeof(double));
+    h = fnv1a(h, s.mirror.data(), s.mirror.size() * sizeof(int));
+    h = fnv1a(h, s.p2f.data(), s.p2f.size() * sizeof(int));
+    return fnv1a(h, s.ops.data(), s.ops.size() * sizeof(double2));
+}
+
+// Identity of a call's heads: options, and per head its instance (position in the call,
+// system, gamma buffer, sizes, dt) and its rows.
+uint64_t heads_key(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads, const BuildOptions& opt) {
+    uint64_t h = 1469598103934665603ull;
+    const uint64_t o[3] = {opt.causal_truncation ? 1u : 0u, opt.pad_factor, heads.size()};
+    h = fnv1a(h, o, sizeof(o));
+    for (const Head& hd : heads) {
+        const Tcl4Instance& in = insts[hd.inst];
+        const uint64_t v[8] = {hd.inst, static_cast<uint64_t>(reinterpret_cast<std::uintptr_t>(in.gamma)),
+                               in.gamma_on_device ? 1u : 0u, in.Nt, hd.H, hd.tc, hd.rows_hash, in.tidx.size()};
+        h = fnv1a(h, v, sizeof(v));
+        h = fnv1a(h, &in.dt, sizeof(double));
+        h = system_hash(h, in.sys);
+    }
+    return h;
+}
+
+// Prepares the plans of `heads` (their rows, positions and gamma copies) in `hp`.
+void build_head_plans(HeadPlans& hp, const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads,
+                      const BuildOptions& o64) {
+    hp.drop();
+    const std::size_t nh = heads.size();
+    hp.off.assign(nh, 0);
+    hp.pos_off.assign(nh, 0);
+    std::size_t rows = 0, npos = 0;
+    for (std::size_t k = 0; k < nh; ++k) {
+        hp.off[k] = rows;
+        rows += heads[k].times.size() * entries(insts[heads[k].inst]);
+        hp.pos_off[k] = npos;
+        npos += heads[k].pos.size();
+    }
+    hp.rows.ensure(std::max<std::size_t>(rows, 1) * sizeof(double2));
+    hp.pos.ensure(std::max<std::size_t>(npos, 1) * sizeof(uint32_t));
+    {
+        std::vector<uint32_t> pos_h(std::max<std::size_t>(npos, 1));
+        for (std::size_t k = 0; k < nh; ++k) std::copy(heads[k].pos.begin(), heads[k].pos.end(), pos_h.begin() + hp.pos_off[k]);
+        cuda_check(cudaMemcpy(hp.pos.p, pos_h.data(), npos * sizeof(uint32_t), cudaMemcpyHostToDevice),
+                   "cudaMemcpy(guard positions)");
+    }
+    // host gamma: the samples each head consumes (the causal rule reads up to its last time)
+    hp.uploads.clear();
+    hp.gam_elems = 0;
+    std::vector<std::size_t> g_at(nh, 0), g_n(nh, 0);
+    for (std::size_t k = 0; k < nh; ++k) {
+        const Tcl4Instance& in = insts[heads[k].inst];
+        if (in.gamma_on_device) continue;
+        const std::size_t n =
+            o64.causal_truncation ? static_cast<std::size_t>(*std::max_element(heads[k].times.begin(), heads[k].times.end())) + 1
+                                  : in.Nt;
+        g_at[k] = hp.gam_elems;
+        g_n[k] = n;
+        hp.uploads.push_back({in.gamma, static_cast<std::size_t>(in.sys.nf), in.Nt, n, hp.gam_elems, 0});
+        hp.gam_elems += static_cast<std::size_t>(in.sys.nf) * n;
+    }
+    hp.gam.ensure(std::max<std::size_t>(hp.gam_elems, 1) * sizeof(double2));
+    // the plans' instances; heads of one time list and length share one list of times
+    std::map<std::tuple<const void*, uint32_t, uint32_t>, TimeList> lists;
+    auto list_of = [&](const Head& h, uint32_t n) -> const TimeList& {
+        const auto key = std::make_tuple(insts[h.inst].tidx.identity(), h.H, n);
+        auto it = lists.find(key);
+        if (it == lists.end()) {
+            TimeList t;
+            t.assign(h.times.data(), h.times.data() + n);
+            it = lists.emplace(key, std::move(t)).first;
+        }
+        return it->second;
+    };
+    double2* rows_p = static_cast<double2*>(hp.rows.p);
+    std::vector<Tcl4Instance> hi(nh);
+    for (std::size_t k = 0; k < nh; ++k) {
+        const Head& h = heads[k];
+        const Tcl4Instance& in = insts[h.inst];
+        Tcl4Instance& x = hi[k];
+        x.sys = in.sys;
+        x.gamma = in.gamma_on_device ? in.gamma : static_cast<const double2*>(hp.gam.p) + g_at[k];
+        x.Nt = in.gamma_on_device ? in.Nt : g_n[k];
+        x.gamma_on_device = true;
+        x.dt = in.dt;
+        x.tidx.share_with(list_of(h, static_cast<uint32_t>(h.times.size())));
+        x.out = rows_p + hp.off[k];
+        x.out_on_device = true;
+        x.internal = true;
+    }
+    // chunks: per chunk the heads, then each level (instance lists; empty ones dropped)
+    hp.chunk_of.assign(nh, 0);
+    std::vector<std::vector<std::vector<Tcl4Instance>>> lists_of;
+    for (std::size_t k = 0; k < nh; ++k) {
+        uint32_t c = 0;
+        while (c < 2 && heads[k].inst >= kChunkBounds[c]) ++c;
+        hp.chunk_of[k] = c;
+    }
+    for (uint32_t c = 0; c < 3; ++c) {
+        std::vector<std::vector<Tcl4Instance>> parts(1);
+        for (std::size_t k = 0; k < nh; ++k)
+            if (hp.chunk_of[k] == c) parts[0].push_back(hi[k]);
+        if (parts[0].empty()) continue;
+        for (uint32_t bound : kLevels) {
+            std::vector<Tcl4Instance> li;
+            for (std::size_t k = 0; k < nh; ++k) {
+                const Head& h = heads[k];
+                if (hp.chunk_of[k] != c || h.H <= bound || !std::is_sorted(h.times.begin(), h.times.end())) continue;
+                const std::size_t n =
+                    static_cast<std::size_t>(std::lower_bound(h.times.begin(), h.times.end(), bound) - h.times.begin());
+                if (n == 0) continue;
+                Tcl4Instance l = hi[k];
+                l.tidx.share_with(list_of(h, static_cast<uint32_t>(n)));
+                li.push_back(std::move(l));
+            }
+            if (!li.empty()) parts.push_back(std::move(li));
+        }
+        lists_of.push_back(std::move(parts));
+    }
+    // chunks renumbered without the empty ones
+    {
+        std::vector<uint32_t> used;
+        for (uint32_t c : hp.chunk_of)
+            if (std::find(used.begin(), used.end(), c) == used.end()) used.push_back(c);
+        std::sort(used.begin(), used.end());
+        for (uint32_t& c : hp.chunk_of) c = static_cast<uint32_t>(std::find(used.begin(), used.end(), c) - used.begin());
+        std::size_t u = 0;
+        for (std::size_t k = 0; k < nh; ++k)
+            if (!insts[heads[k].inst].gamma_on_device) hp.uploads[u++].chunk = hp.chunk_of[k];
+    }
+    const std::size_t budget = work_budget_now();
+    std::size_t need = 256;
+    for (auto& parts : lists_of)
+        for (auto& li : parts) need = std::max(need, plan_work_bytes(li, o64, budget));
+    hp.work.ensure(need + need / 8 + (std::size_t(1) << 20));
+    for (auto& parts : lists_of) {
+        hp.chunks.emplace_back();
+        HeadPlans::Chunk& ch = hp.chunks.back();
+        cuda_check(cudaEventCreateWithFlags(&ch.ready, cudaEventDisableTiming), "cudaEventCreate");
+        for (auto& li : parts) ch.plans.push_back(plan_create_direct(li, o64, hp.work.p, hp.work.cap, budget));
+    }
+}
+
+// Replays the head plans on their stream after the work queued on `st`; `ready` marks the end.
+void launch_head_plans(HeadPlans& hp, cudaStream_t st) {
+    if (!hp.s) {
+        // high priority: the heads gate the downloads of the pass's groups, which are the
+        // slowest part of a call with host outputs
+        int lo = 0, hi = 0;
+        cuda_check(cudaDeviceGetStreamPriorityRange(&lo, &hi), "cudaDeviceGetStreamPriorityRange");
+        cuda_check(cudaStreamCreateWithPriority(&hp.s, cudaStreamNonBlocking, hi), "cudaStreamCreate(guard heads)");
+    }
+    if (!hp.start) cuda_check(cudaEventCreateWithFlags(&hp.start, cudaEventDisableTiming), "cudaEventCreate");
+    if (hp.launched) cuda_check(cudaEventSynchronize(hp.ready()), "cudaEventSynchronize(guard heads)");
+    cuda_check(cudaEventRecord(hp.start, st), "cudaEventRecord");
+    cuda_check(cudaStreamWaitEvent(hp.s, hp.start, 0), "cudaStreamWaitEvent");
+    for (uint32_t c = 0; c < hp.chunks.size(); ++c) {
+        for (const auto& u : hp.uploads)
+            if (u.chunk == c)
+                cuda_check(cudaMemcpy2DAsync(static_cast<double2*>(hp.gam.p) + u.dst, u.n * sizeof(double2), u.src,
+                                             u.stride * sizeof(double2), u.n * sizeof(double2), u.nf,
+                                             cudaMemcpyHostToDevice, hp.s),
+                           "cudaMemcpy2DAsync(guard gamma)");
+        for (Tcl4Plan* p : hp.chunks[c].plans) plan_execute(p, hp.s);
+        cuda_check(cudaEventRecord(hp.chunks[c].ready, hp.s), "cudaEventRecord");
+    }
+    hp.launched = true;
+}
+
 }  // namespace
 
 void set_fp32_guard(double tol) { g_guard_tol.store(tol > 0.0 ? tol : 0.0); }
@@ -754,6 +997,7 @@ void release_guard_scratch() {
     int dev = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     guard_scratch_map().erase(dev);
+    head_plans_map().erase(dev);
 }
 GuardStats fp32_guard_stats() { return t_stats; }
 double fp32_guard() { return g_guard_tol.load(); }
@@ -765,74 +1009,156 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
         return;
     }
     cudaStream_t st = stream ? stream : default_stream();
+    const auto t00 = std::chrono::steady_clock::now();
     // the FP32 pass on a copy: a direct build may point an instance at device copies of its
     // host input and output that it frees before returning; the guard needs the caller's
     std::vector<Tcl4Instance> pass(insts);
-    const std::vector<uint64_t> fps = fingerprints(insts, st);
-    // every instance decided before on the same gamma contents: build the heads it requires
-    // on the helper thread while this thread runs the FP32 pass, then patch them
-    PreHeads pre;
+    TimeCache tcache;
+    std::vector<uint32_t> tcs(insts.size(), 0);
+    for (std::size_t a = 0; a < insts.size(); ++a) tcs[a] = tcache.t_count(insts[a]);
+    const std::vector<uint64_t> fps = fingerprints(insts, tcs, st);
+    const auto t01 = std::chrono::steady_clock::now();
+    // every instance decided before on the same gamma contents: replay the FP64 heads it
+    // requires (prepared plans) beside the FP32 pass, whose groups patch them on the device
+    std::vector<Head> heads;
     bool trusted = true;
-    std::size_t pre_bytes = 0;
     for (std::size_t a = 0; a < insts.size() && trusted; ++a) {
         if (insts[a].tidx.empty()) continue;
-        const uint32_t tc = t_count_of(insts[a]);
-        auto it = t_head_memory.find({insts[a].gamma, tc});
+        auto it = t_head_memory.find({insts[a].gamma, tcs[a]});
         if (it == t_head_memory.end() || it->second.fingerprint != fps[a] || it->second.accepted == 0) {
             trusted = false;
             break;
         }
         if (it->second.required == 0) continue;  // FP32 suffices everywhere
-        Head h = make_head(insts, a, it->second.required, tc);
-        pre_bytes += h.times.size() * entries(insts[a]) * sizeof(double2);
-        if (!h.times.empty()) pre.heads.push_back(std::move(h));
+        Head h = tcache.head(insts, a, it->second.required, tcs[a]);
+        if (!h.times.empty()) heads.push_back(std::move(h));
     }
-    trusted = trusted && pre_bytes <= kTempBytes;
-    if (trusted) {
-        const auto t0 = std::chrono::steady_clock::now();
-        std::future<void> heads;
-        if (!pre.heads.empty()) {
+    const auto t0 = std::chrono::steady_clock::now();
+    auto t_key = t0;
+    HeadPlans* hp = nullptr;
+    bool rebuilt = false;
+    if (trusted && !heads.empty()) {
+        hp = &head_plans();
+        const uint64_t key = heads_key(insts, heads, opt);
+        t_key = std::chrono::steady_clock::now();
+        if (key != hp->key || hp->empty()) {
             BuildOptions o64 = opt;
             o64.fp32 = false;
             o64.fcr_ms = nullptr;
-            pre.temp = &guard_scratch().pre;
-            pre.temp->ensure(std::max<std::size_t>(pre_bytes, 256));
-            int dev = 0;
-            cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-            heads = HeadWorker::get().run([&insts, &pre, o64, dev] {
-                cuda_check(cudaSetDevice(dev), "cudaSetDevice(guard worker)");
-                std::vector<std::size_t> off;
-                build_heads(insts, pre.heads, 0, pre.heads.size(), static_cast<double2*>(pre.temp->p), off, o64, nullptr);
-                pre.off = off;
-            });
+            o64.out_hook = nullptr;
+            try {
+                build_head_plans(*hp, insts, heads, o64);
+                hp->key = key;
+                rebuilt = true;
+            } catch (const Error&) {
+                // no room for the prepared heads (or no plan for them): check this call as usual
+                hp->drop();
+                trusted = false;
+            }
         }
-        try {
-            tcl4_build_direct(pass, opt, stream);
-        } catch (...) {
-            if (heads.valid()) heads.wait();
-            throw;
-        }
+    }
+    if (trusted) {
+        const std::size_t nh = heads.size();
+        if (nh) launch_head_plans(*hp, st);
         const auto t1 = std::chrono::steady_clock::now();
-        if (heads.valid()) heads.get();  // rethrows the helper's error
+        // Each group of the FP32 pass patches the heads of its whole instances on the device,
+        // after its contraction and the head plans, before its download (host outputs download
+        // once, already patched).  One pinned job slot per head.
+        GuardScratch& gs = guard_scratch();
+        std::vector<int> head_of(insts.size(), -1);
+        for (std::size_t k = 0; k < nh; ++k) head_of[heads[k].inst] = static_cast<int>(k);
+        std::vector<char> patched(nh, 0);
+        std::size_t used = 0;
+        if (nh) {
+            gs.jobs_host.ensure(nh * sizeof(GuardJob));
+            gs.jobs.ensure(nh * sizeof(GuardJob));
+        }
+        const Tcl4Instance* pass0 = pass.data();
+        BuildOptions po = opt;
+        if (nh)
+            po.out_hook = [&](const std::vector<std::pair<const Tcl4Instance*, void*>>& rows, cudaStream_t s) {
+                GuardJob* jh = static_cast<GuardJob*>(gs.jobs_host.p) + used;
+                std::size_t n = 0, most = 1;
+                uint32_t last_chunk = 0;
+                for (const auto& r : rows) {
+                    const std::size_t a = static_cast<std::size_t>(r.first - pass0);
+                    if (a >= head_of.size() || head_of[a] < 0 || patched[head_of[a]]) continue;
+                    const std::size_t k = static_cast<std::size_t>(head_of[a]);
+                    const Head& h = heads[k];
+                    GuardJob j{};
+                    j.h64 = static_cast<const double2*>(hp->rows.p) + hp->off[k];
+                    j.out32 = static_cast<float2*>(r.second);
+                    j.pos = static_cast<const uint32_t*>(hp->pos.p) + hp->pos_off[k];
+                    j.n = static_cast<uint32_t>(h.pos.size());
+                    j.E = static_cast<uint32_t>(entries(insts[a]));
+                    jh[n++] = j;
+                    patched[k] = 1;
+                    last_chunk = std::max(last_chunk, hp->chunk_of[k]);
+                    most = std::max(most, h.pos.size() * entries(insts[a]));
+                }
+                if (!n) return;
+                GuardJob* jd = static_cast<GuardJob*>(gs.jobs.p) + used;
+                used += n;
+                // the chunks run in order: the last one these heads belong to covers them all
+                cuda_check(cudaStreamWaitEvent(s, hp->chunks[last_chunk].ready, 0), "cudaStreamWaitEvent(guard heads)");
+                cuda_check(cudaMemcpyAsync(jd, jh, n * sizeof(GuardJob), cudaMemcpyHostToDevice, s),
+                           "cudaMemcpyAsync(guard jobs)");
+                const unsigned bx = static_cast<unsigned>(std::min<std::size_t>((most + 255) / 256, 592));
+                k_guard_patch<<<dim3(bx, static_cast<unsigned>(n)), 256, 0, s>>>(jd);
+                cuda_check(cudaGetLastError(), "k_guard_patch");
+                count_launches(1);
+            };
+        tcl4_build_direct(pass, po, stream);
         const auto t2 = std::chrono::steady_clock::now();
         t_stats = GuardStats{};
         t_stats.instances = insts.size();
-        if (!pre.heads.empty()) run_guard(insts, opt, st, true, &pre, true, &fps);
+        // heads of instances the pass built in slices: patched after it, as a separate step
+        PreHeads rest;
+        if (hp) rest.temp = &hp->rows;
+        for (std::size_t k = 0; k < nh; ++k) {
+            const Head& h = heads[k];
+            if (!patched[k]) {
+                rest.heads.push_back(h);
+                rest.off.push_back(hp->off[k]);
+                continue;
+            }
+            ++t_stats.heads;
+            t_stats.head_rows += h.times.size();
+            t_stats.rows += insts[h.inst].tidx.size();
+            if (h.H >= h.tc) ++t_stats.full;
+        }
+        if (!rest.heads.empty()) {
+            cuda_check(cudaEventSynchronize(hp->ready()), "cudaEventSynchronize(guard heads)");
+            const GuardStats before = t_stats;
+            run_guard(insts, opt, st, true, &rest, true, &fps);
+            t_stats.heads += before.heads;
+            t_stats.head_rows += before.head_rows;
+            t_stats.rows += before.rows;
+            t_stats.full += before.full;
+        }
+        t_stats.rounds = 1;
         if (host_trace_on())
-            std::fprintf(stderr, "taco guard (ms, heads from memory): fp32 pass %.3f, heads wait %.3f, patch %.3f\n",
-                         std::chrono::duration<double, std::milli>(t1 - t0).count(),
+            std::fprintf(stderr,
+                         "taco guard (ms, heads from memory): setup %.3f (fingerprints %.3f), key %.3f, head plans %s "
+                         "%.3f, fp32 pass with patches %.3f, rest %.3f (%zu of %zu heads patched in the pass)\n",
+                         std::chrono::duration<double, std::milli>(t0 - t00).count(),
+                         std::chrono::duration<double, std::milli>(t01 - t00).count(),
+                         std::chrono::duration<double, std::milli>(t_key - t0).count(), rebuilt ? "built+launched" : "launched",
+                         std::chrono::duration<double, std::milli>(t1 - t_key).count(),
                          std::chrono::duration<double, std::milli>(t2 - t1).count(),
-                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t2).count());
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t2).count(),
+                         nh - rest.heads.size(), nh);
         return;
     }
-    const auto t0 = std::chrono::steady_clock::now();
+    const auto t3 = std::chrono::steady_clock::now();
     tcl4_build_direct(pass, opt, stream);
-    const auto t1 = std::chrono::steady_clock::now();
+    const auto t4 = std::chrono::steady_clock::now();
     run_guard(insts, opt, st, true, nullptr, false, &fps);
     if (host_trace_on())
-        std::fprintf(stderr, "taco guard (ms): fp32 pass %.3f, guard rounds %.3f\n",
-                     std::chrono::duration<double, std::milli>(t1 - t0).count(),
-                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count());
+        std::fprintf(stderr, "taco guard (ms): setup %.3f, fp32 pass %.3f, guard rounds %.3f\n",
+                     std::chrono::duration<double, std::milli>(t3 - t00).count(),
+                     std::chrono::duration<double, std::milli>(t4 - t3).count(),
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t4).count());
 }
 
 Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt) {
@@ -856,6 +1182,8 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
         BuildOptions o64 = opt;
         o64.fp32 = false;
         o64.fcr_ms = nullptr;
+        o64.out_hook = nullptr;
+    o64.out_hook = nullptr;
         struct Part {
             Tcl4Plan* plan = nullptr;
             std::vector<Tcl4Plan*> levels;  // short-FFT levels, replayed after the head
@@ -866,14 +1194,22 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
         struct TailState {
             DevMem rows, meta, work;
             std::vector<Part> parts;
+            cudaStream_t side = nullptr;  // the heads run here, beside the FP32 graph
+            cudaEvent_t start = nullptr, done = nullptr;
             ~TailState() {
                 for (auto& p : parts) {
                     plan_destroy(p.plan);
                     for (Tcl4Plan* l : p.levels) plan_destroy(l);
                 }
+                if (start) cudaEventDestroy(start);
+                if (done) cudaEventDestroy(done);
+                if (side) cudaStreamDestroy(side);
             }
         };
         auto tail = std::make_shared<TailState>();
+        cuda_check(cudaStreamCreateWithFlags(&tail->side, cudaStreamNonBlocking), "cudaStreamCreate(guard heads)");
+        cuda_check(cudaEventCreateWithFlags(&tail->start, cudaEventDisableTiming), "cudaEventCreate");
+        cuda_check(cudaEventCreateWithFlags(&tail->done, cudaEventDisableTiming), "cudaEventCreate");
         std::size_t most = 256, meta_total = 0;
         std::vector<JobImage> imgs;
         std::vector<std::pair<std::size_t, std::size_t>> ranges;
@@ -927,16 +1263,41 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
             kernels += plan_kernels(p.plan) + 1;
             moff += (im.host.size() + 255) / 256 * 256;
         }
-        plan_set_tail(plan, [tail](cudaStream_t s) {
-            for (const Part& p : tail->parts) {
-                plan_execute(p.plan, s);
-                for (Tcl4Plan* l : p.levels) plan_execute(l, s);
-                const GuardJob* jobs = reinterpret_cast<const GuardJob*>(static_cast<unsigned char*>(tail->meta.p) + p.meta_off);
-                k_guard_patch<<<dim3(p.blocks, static_cast<unsigned>(p.jobs)), 256, 0, s>>>(jobs);
-                cuda_check(cudaGetLastError(), "k_guard_patch");
-                count_launches(1);
-            }
-        }, kernels);
+        if (host_trace_on()) {
+            std::map<uint32_t, std::size_t> hist;
+            for (const Head& h : dec.heads) ++hist[h.H];
+            std::string line = "taco guard plan: heads by length (H: count)";
+            for (const auto& e : hist) line += " " + std::to_string(e.first) + ":" + std::to_string(e.second);
+            std::size_t nl[2] = {0, 0};
+            for (std::size_t c = 0; c < ranges.size(); ++c)
+                for (std::size_t q = 0; q < lis[c].size() && q < 2; ++q) nl[q] += lis[c][q].size();
+            std::fprintf(stderr, "%s; levels %zu (<%u) %zu (<%u); tail kernels %llu\n", line.c_str(), nl[0], kLevels[0], nl[1],
+                         kLevels[1], static_cast<unsigned long long>(kernels));
+        }
+        // the FP64 heads (and their levels, in order) on the side stream, after the work queued
+        // before the execute and beside the FP32 graph; the patches after both
+        plan_set_tail(
+            plan,
+            [tail](cudaStream_t s) {
+                cuda_check(cudaEventRecord(tail->start, s), "cudaEventRecord");
+                cuda_check(cudaStreamWaitEvent(tail->side, tail->start, 0), "cudaStreamWaitEvent");
+                for (const Part& p : tail->parts) {
+                    plan_execute(p.plan, tail->side);
+                    for (Tcl4Plan* l : p.levels) plan_execute(l, tail->side);
+                }
+                cuda_check(cudaEventRecord(tail->done, tail->side), "cudaEventRecord");
+            },
+            [tail](cudaStream_t s) {
+                cuda_check(cudaStreamWaitEvent(s, tail->done, 0), "cudaStreamWaitEvent");
+                for (const Part& p : tail->parts) {
+                    const GuardJob* jobs =
+                        reinterpret_cast<const GuardJob*>(static_cast<unsigned char*>(tail->meta.p) + p.meta_off);
+                    k_guard_patch<<<dim3(p.blocks, static_cast<unsigned>(p.jobs)), 256, 0, s>>>(jobs);
+                    cuda_check(cudaGetLastError(), "k_guard_patch");
+                    count_launches(1);
+                }
+            },
+            kernels);
         return plan;
     } catch (...) {
         plan_destroy(plan);

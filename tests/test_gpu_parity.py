@@ -141,6 +141,27 @@ def test_plan_replay_matches_direct_call():
         tb.Tcl4Plan([(s, G, 0.005, None) for _, s, G in cases])
 
 
+def test_plan_groups_of_several_lengths_run_as_branches():
+    """Instances of four FFT lengths (and two system sizes) in one plan: the groups run as
+    concurrent branches of the plan's graph, each in its own region of the work buffer.
+    Every result equals the direct call's (same kernels) and matches the oracle."""
+    import torch
+    cases = [spin_boson_case(n, 0.005, eps=e) for n, e in ((400, 0.8), (900, 1.0), (1700, 1.7), (900, 1.3))]
+    cases.append(random_case(3, 1, 700, 0.01, seed=17))
+    inst = [(s, torch_dev(G), 0.005 if k < 4 else 0.01, np.arange(0, G.shape[1], 3))
+            for k, (_, s, G) in enumerate(cases)]
+    assert len({tb.fft_length(int(x[3].max()) + 1, "fp64")[0] for x in inst}) >= 3
+    direct = [x.cpu().numpy() for x in tb.build_instances(inst, precision="fp64")]
+    plan = tb.Tcl4Plan(inst, precision="fp64")
+    for _ in range(2):
+        res = plan.run()
+    torch.cuda.synchronize()
+    for (osys, _, G), x, a, b in zip(cases, inst, res, direct):
+        assert np.array_equal(a.cpu().numpy(), b)
+        assert relerr(b, oracle_l4(osys, G, x[2], x[3])) <= 1e-10
+    plan.close()
+
+
 def test_batched_instances_match_single_calls():
     cases = [spin_boson_case(1500, 0.005, eps=e, delta=dl, alpha=a) for e, dl, a in
              ((1.0, 1.0, 0.05), (0.7, 1.3, 0.1), (1.5, 0.6, 0.02))]
@@ -303,7 +324,9 @@ def test_shared_time_lists_match_single_calls():
 def test_pipelined_slots_are_reused_safely():
     """336 host-buffer instances make seven sub-batches, more than the buffer slots of three
     lanes: the last sub-batch reuses the first one's metadata and input buffers after it has
-    finished.  Results equal single-instance calls in the first and the last sub-batches."""
+    finished, and each lane's output staging serves its next sub-batch once the download
+    has left it.  Results equal single-instance calls in the first and the last sub-batches,
+    and every instance equals the others of its case."""
     rng = np.random.default_rng(21)
     cases = [spin_boson_case(400, 0.01, eps=rng.uniform(0.5, 2.0), delta=rng.uniform(0.5, 2.0))
              for _ in range(13)]
@@ -313,6 +336,10 @@ def test_pipelined_slots_are_reused_safely():
     for k in (0, 5, 47, 290, 301, 335):
         single = np.asarray(tb.build_instances([inst[k]], precision="fp32")[0])
         assert relerr(batch[k], single) <= 1e-6
+    # every instance (a lane's output staging is reused by its next sub-batch once the
+    # previous download has left it) equals the first instance of its case
+    for k in range(13, 336):
+        assert relerr(batch[k], batch[k % 13]) <= 1e-6, k
 
 
 def test_long_host_buckets_match_device_inputs():

@@ -188,9 +188,9 @@ def test_guard_setting_and_unsorted_times():
 
 def test_guard_remembers_heads_across_direct_calls():
     """A second direct call on the same gamma contents (same fingerprint) builds only the
-    heads the first call's row profile required, on the helper thread during the FP32 pass,
-    and patches them without a comparison round; both calls meet 1e-6 in every window, and
-    host outputs equal device outputs call for call."""
+    heads the first call's row profile required (prepared FP64 plans, replayed by later calls
+    beside the FP32 pass) and patches them without a comparison round; every call meets 1e-6
+    in every window, and host outputs equal device outputs call for call."""
     import torch
     cases = [c4_case(H_SLOW, A_SLOW, 15, 0.09, wc, 0.7) for wc in (1.5, 12.7, 6.0)]
     inst = [(s, torch.from_numpy(G).cuda(), dt, tidx) for _, s, G, dt, tidx in cases]
@@ -199,11 +199,15 @@ def test_guard_remembers_heads_across_direct_calls():
     second = [x.cpu().numpy() for x in tb.build_instances(inst, precision="fp32")]
     s2 = tb.fp32_guard_stats()
     assert s2["rounds"] == 1 and s2["fp64_head_rows"] <= s1["fp64_head_rows"], (s1, s2)
+    # the third call replays the FP64 heads the second one prepared: the same results
+    third = [x.cpu().numpy() for x in tb.build_instances(inst, precision="fp32")]
+    assert tb.fp32_guard_stats() == s2
     host = [(s, G, dt, tidx) for _, s, G, dt, tidx in cases]
     h1 = tb.build_instances(host, precision="fp32")
     h2 = tb.build_instances(host, precision="fp32")
-    for (osys, s, G, dt, tidx), a, b, c, d, x in zip(cases, first, second, h1, h2, inst):
-        assert np.array_equal(a, c) and np.array_equal(b, d)
+    h3 = tb.build_instances(host, precision="fp32")
+    for (osys, s, G, dt, tidx), a, b, c, d, e, f, x in zip(cases, first, second, h1, h2, third, h3, inst):
+        assert np.array_equal(a, c) and np.array_equal(b, d) and np.array_equal(b, e) and np.array_equal(b, f)
         ref = fp64_reference(s, x[1], dt, tidx)
         for got in (a, b):
             for lo, e in window_errors(got, ref, tidx):
