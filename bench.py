@@ -299,17 +299,9 @@ def timed(torch, fn, reps, warmup=1):
 
 
 def gue_system(d, rng):
-    """Seeded GUE Hamiltonian (H_ii ~ N(0, 1/d), off-diagonal real and imaginary parts
-    N(0, 1/(2d))) and a random Hermitian coupling of unit spectral norm."""
-    from taco_b200.inputs import System
-    X = rng.normal(0.0, np.sqrt(1.0 / (2 * d)), (d, d)) + 1j * rng.normal(0.0, np.sqrt(1.0 / (2 * d)), (d, d))
-    H = np.triu(X, 1)
-    H = H + H.conj().T + np.diag(rng.normal(0.0, np.sqrt(1.0 / d), d))
-    Y = rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
-    A = np.triu(Y, 1)
-    A = A + A.conj().T + np.diag(rng.normal(size=d))
-    A = A / np.linalg.norm(A, 2)
-    return System(H, [A]), A
+    """Seeded GUE system of dimension d (taco_b200.workloads.gue_system)."""
+    from taco_b200.workloads import gue_system as g
+    return g(d, rng)
 
 
 def precision_random(args, d, cpu_leg):

@@ -216,10 +216,13 @@ def _apply_tuning_table(L):
             continue
         L2, prec = key.split(":")
         pr = TACO_PREC_FP32 if prec == "fp32" else TACO_PREC_FP64
-        L.taco_set_tuning(int(L2), pr, int(sch["col_tile"]), int(sch["row_tile"]), int(sch["chunk_bytes"]),
-                          int(sch["inv_dft_rows"]))
-        if "cluster_lm" in sch:
-            L.taco_set_cluster_points(int(L2), pr, int(sch["cluster_lm"]))
+        if "col_tile" in sch:  # a tile schedule (entries may carry only the radix choice)
+            L.taco_set_tuning(int(L2), pr, int(sch["col_tile"]), int(sch["row_tile"]), int(sch["chunk_bytes"]),
+                              int(sch["inv_dft_rows"]))
+            if "cluster_lm" in sch:
+                L.taco_set_cluster_points(int(L2), pr, int(sch["cluster_lm"]))
+        if int(L2) >= 64 and "enabled" in sch:  # 3 * 2^k and 5 * 2^k lengths the tuner measured slower
+            L.taco_set_fft_length_enabled(int(L2), pr, 1 if sch["enabled"] else 0)
 
 
 def check(rc: int) -> None:

@@ -10,7 +10,8 @@ Results are persisted as JSON ({"<key>:<fp32|fp64>": {...}}) and applied with lo
 of an FFT length is log2 for powers of two, + 64 for 3 * 2^k and + 128 for 5 * 2^k
 (taco_b200.fft_length).  Workloads: "c2" (spin-boson batch of the headline shape: the radix
 choice for t_max = 10000 and the tiles of its lengths) and "c4" (batching-form lengths
-2^15..2^19: spin-boson instances with Nt = 2^(L-1) and every 8th time).  The FP32 form is
+2^15..2^19: one GUE instance of dimension 6 -- 31^3 frequency triples -- with N = 2^(L-1) and
+every 8th time).  The FP32 form is
 tuned with its precision guard off (the guard's FP64 heads are tuned as FP64 lengths).
 
     python -m taco_b200.autotune --workloads c2,c4 --out taco_b200/tuning.json   (needs a GPU)
@@ -207,6 +208,7 @@ def main():
     ap.add_argument("--precisions", default="fp32,fp64")
     ap.add_argument("--workloads", default="c2,c4")
     ap.add_argument("--c4-lengths", default="15,16,17,18,19")
+    ap.add_argument("--c4-dim", type=int, default=6)
     args = ap.parse_args()
     load(args.out)
     guard = tb.fp32_guard()
@@ -237,7 +239,7 @@ def main():
     def tune_tiles(inst, tidx, n, prec, full=False, cands=None):
         nfft, L = tb.fft_length(n, prec, full_length=full)
         dtype = torch.complex64 if prec == "fp32" else torch.complex128
-        outs = [torch.empty((tidx.size, 16), dtype=dtype, device="cuda") for _ in inst]
+        outs = [torch.empty((tidx.size, x[0].N ** 4), dtype=dtype, device="cuda") for x in inst]
 
         def same_length(n=n, prec=prec, full=full, nfft=nfft):
             return tb.fft_length(n, prec, full_length=full)[0] == nfft
@@ -271,15 +273,22 @@ def main():
             tune_tiles(inst, tidx, n, prec)
             tune_tiles(inst, tidx, args.N + 1, prec, full=True)
     if "c4" in args.workloads:
+        # one seeded GUE instance of dimension --c4-dim per length (its nf^3 triples dominate
+        # the batching form's time): Ohmic bath, N = 2^(L-1), dt = 10 / (N wc), every 8th time
+        from . import adjoint as adj
+        from .workloads import gue_system
+        s, _ = gue_system(args.c4_dim, np.random.default_rng(404))
         for L in [int(x) for x in args.c4_lengths.split(",") if x]:
             Nt = 1 << (L - 1)
-            B = max(2, min(16, (1 << 22) // Nt))
-            _, systems, gammas = spin_boson_batch(torch, B, Nt - 1, 1e-3, seed=400 + L)
-            tidx = np.arange(0, Nt - 1, 8, dtype=np.uint32)
-            inst = [(s, g, 1e-3, tidx) for s, g in zip(systems, gammas)]
+            dt = 10.0 / (Nt * 5.0)
+            C = adj.bcf_device([dict(alpha=0.05, omega_c=5.0, beta=1.0, N=Nt, dt=dt)], Nt + 1)[0]
+            g = tb.gamma_trapz_device(C, dt, s.omegas)
+            tidx = np.arange(0, Nt, 8, dtype=np.uint32)
+            inst = [(s, g, dt, tidx)]
             for prec in args.precisions.split(","):
                 tune_tiles(inst, tidx, int(tidx[-1]) + 1, prec, cands=small_candidates(prec))
-            del gammas
+            del g, C
+            tb.release_workspace()
             torch.cuda.empty_cache()
     tb.set_fp32_guard(guard)
     save(entries, args.out, note="measured on B200 by taco_b200.autotune (workloads: " + args.workloads + ")")

@@ -72,3 +72,17 @@ def spin_boson_batch(torch, B, N=200000, dt=5e-4, seed=0, device="cuda"):
     C = bcf_device([dict(alpha=p["alpha"], omega_c=p["wc"], beta=p["beta"], N=N, dt=dt) for p in params], N + 1, device)
     gammas = gamma_trapz_device_batch([C[b] for b in range(B)], [dt] * B, [s.omegas for s in systems])
     return params, systems, gammas
+
+
+def gue_system(d, rng):
+    """Seeded GUE Hamiltonian (H_ii ~ N(0, 1/d), off-diagonal real and imaginary parts
+    N(0, 1/(2d))) and a random Hermitian coupling of unit spectral norm."""
+    from .inputs import System
+    X = rng.normal(0.0, np.sqrt(1.0 / (2 * d)), (d, d)) + 1j * rng.normal(0.0, np.sqrt(1.0 / (2 * d)), (d, d))
+    H = np.triu(X, 1)
+    H = H + H.conj().T + np.diag(rng.normal(0.0, np.sqrt(1.0 / d), d))
+    Y = rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
+    A = np.triu(Y, 1)
+    A = A + A.conj().T + np.diag(rng.normal(size=d))
+    A = A / np.linalg.norm(A, 2)
+    return System(H, [A]), A

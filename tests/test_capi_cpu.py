@@ -174,3 +174,25 @@ def test_system_views_are_reused_only_while_unchanged():
     arr, keep, res, dev = tb._instance_array([(s, g, 0.1, tidx)] * 3, _capi.TACO_PREC_FP32, outs)
     assert not dev and len({arr[k].tidx for k in range(3)}) == 1 and arr[0].T == tidx.size
     assert [arr[k].L4_out for k in range(3)] == [tb._addr(o) for o in outs]
+
+
+def test_committed_tuning_table_is_applied():
+    """Every tile schedule of taco_b200/tuning.json is in effect after import (entries that
+    carry only the radix choice leave the tiles alone)."""
+    import json
+    import os
+    from taco_b200 import autotune
+    path = os.path.join(os.path.dirname(tb.__file__), "tuning.json")
+    with open(path) as f:
+        table = json.load(f)
+    tb.version()  # loads the library and applies the table
+    n = 0
+    for key, sch in table.items():
+        if key.startswith("_") or "col_tile" not in sch:
+            continue
+        L, prec = key.split(":")
+        got = autotune.get_schedule(int(L), prec)
+        for k in ("col_tile", "row_tile", "chunk_bytes", "inv_dft_rows"):
+            assert got[k] == sch[k], (key, k)
+        n += 1
+    assert n >= 10  # the batching form's lengths 2^15..2^19 and the headline's, in both precisions
