@@ -589,13 +589,21 @@ def c2_rk4_leg(args, systems, gammas, outs32, outs64, tidx):
             errs.append(float(np.linalg.norm(traj["fp32"] - traj["fp64"]) / np.linalg.norm(traj["fp64"])))
     steps = T - 1
     ms = statistics.median(times)
+    # bytes of the step-matrix scheme per trajectory (D = 4, 16-byte entries): the L2 and L4
+    # series read once to form the step matrices ("rk4_warp": the matrix kernel), the
+    # matrices written there and read once by the sequential chain ("rk4_chain")
+    D2 = 16 * 16
+    kernel_bytes = {"rk4_warp": (steps + 1) * D2 * 2 + steps * D2, "rk4_chain": steps * D2}
+    bytes_traj = sum(kernel_bytes.values())
+    peaks, _ = measured_peaks()
     rk4 = {}
     for name, (n, tot) in prof.entries.items():
-        rk4[name] = {"launches": n, "total_ms": round(tot, 4)}
-    # bytes of the step-matrix scheme per trajectory: L2 and L4 series (FP64 after the add)
-    # read once to form the step matrices, the matrices written and read by the chain
-    D2 = 16 * 16
-    bytes_traj = (steps + 1) * D2 * 2 + 2 * steps * D2
+        ent = {"launches": n, "total_ms": round(tot, 4)}
+        if name in kernel_bytes and n and tot > 0:
+            gbs = kernel_bytes[name] / (tot / n / 1e3) / 1e9
+            ent["gbs"] = round(gbs, 1)
+            ent["frac_of_measured_hbm"] = round(gbs / peaks["hbm_gbs"], 4)
+        rk4[name] = ent
     return {"trajectories": P, "steps": steps, "ms_per_trajectory": ms,
             "trajectories_per_s": 1e3 / ms, "gbs_per_trajectory_call": round(bytes_traj / (ms / 1e3) / 1e9, 2),
             "expect_sz_fp32_rel_err_vs_fp64_max": max(errs), "kernels": rk4,
@@ -655,12 +663,14 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     launches0 = tb.kernel_launches()
+    torch.cuda.profiler.start()  # a profiler started with profiling off sees the timed steps alone
     with ClockSampler(local) as clk:
         ev0.record()
         for _ in range(args.steps):
             plan32.run()
         ev1.record()
         torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     launches = tb.kernel_launches() - launches0
     barrier()
     torch.cuda.synchronize()

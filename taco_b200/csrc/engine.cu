@@ -2117,15 +2117,18 @@ void validate_and_derive(std::vector<Tcl4Instance>& insts, const BuildOptions& o
 std::size_t work_budget_now() { return work_budget(); }
 
 // Transient arrays of a plan's groups.  Groups of whole instances run concurrently (branches
-// of the plan's graph, each group in its own region of the buffer) when their sum fits `cap`;
-// otherwise, or when an instance is built in slices (its slices accumulate into one output
-// in order), one after another in one shared region.
+// of the plan's graph, each group in its own region of the buffer) when their sum fits a
+// quarter of the group budget `cap` (the plan keeps its buffer: large batches of long series
+// would otherwise hold several groups' worth of memory for the plan's lifetime) and the
+// buffer the plan is lent (`avail`); otherwise, or when an instance is built in slices (its
+// slices accumulate into one output in order), one after another in one shared region.
 struct PlanWork {
     std::vector<std::size_t> each;  // bytes of each group
     std::size_t total = 0;
     bool concurrent = false;
 };
-PlanWork plan_work(const std::vector<std::vector<WorkUnit*>>& groups, bool fp32, std::size_t cap) {
+PlanWork plan_work(const std::vector<std::vector<WorkUnit*>>& groups, bool fp32, std::size_t cap,
+                   std::size_t avail = ~std::size_t(0)) {
     PlanWork w;
     std::size_t most = 0, sum = 0;
     bool whole = true;
@@ -2138,7 +2141,7 @@ PlanWork plan_work(const std::vector<std::vector<WorkUnit*>>& groups, bool fp32,
         for (auto* u : gu)
             whole = whole && !u->accumulate && u->lo == 0 && u->hi == u->in->sys.nf * u->in->sys.nf * u->in->sys.nf;
     }
-    w.concurrent = groups.size() > 1 && whole && sum <= cap;
+    w.concurrent = groups.size() > 1 && whole && sum <= cap / 4 && sum <= avail;
     w.total = w.concurrent ? sum : most;
     return w;
 }
@@ -2172,7 +2175,7 @@ Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOption
         opt.fp32 ? plan_units<float>(insts, metas, budget, plan->units) : plan_units<double>(insts, metas, budget, plan->units);
     // one transient buffer, sized before any group records its pointers: a region per group
     // when the groups run concurrently, else one region they share in order
-    const PlanWork pw = plan_work(groups, opt.fp32, ext_work ? ext_cap : budget);
+    const PlanWork pw = plan_work(groups, opt.fp32, budget, ext_work ? ext_cap : ~std::size_t(0));
     if (ext_work) {  // a caller's buffer shared by plans that run one after another
         plan->work.p = ext_work;
         plan->work.cap = ext_cap;
