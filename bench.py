@@ -62,6 +62,8 @@ def parse():
     p.add_argument("--c3-stride", type=int, default=4)
     p.add_argument("--c4-instances", type=int, default=64,
                    help="heterogeneous batch instances (0: skip; the config names 256, which takes about 15 min)")
+    p.add_argument("--c4-budget-gib", type=float, default=0.0,
+                   help="work budget of the heterogeneous batch's builds in GiB (0: automatic)")
     p.add_argument("--c4-ref-instances", type=int, default=32,
                    help="heterogeneous batch: instances (evenly spaced) also built in FP64 for the errors")
     return p.parse_args()
@@ -381,6 +383,18 @@ def heterogeneous_batch(args, rank, world, cpu_leg):
     B = args.c4_instances
     tb.release_workspace()  # earlier sections' transient buffers
     torch.cuda.empty_cache()
+    if args.c4_budget_gib > 0:
+        tb.set_work_budget(int(args.c4_budget_gib * (1 << 30)))
+    try:
+        return _heterogeneous_batch(args, rank, world, cpu_leg, B)
+    finally:
+        tb.set_work_budget(0)
+
+
+def _heterogeneous_batch(args, rank, world, cpu_leg, B):
+    import torch
+    import taco_b200 as tb
+    from taco_b200 import adjoint as adj
     rng = np.random.default_rng(args.seed + 400 + 1000 * rank)
     dims = rng.choice([2, 3, 4, 6, 8], B)
     Ns = 1 << rng.integers(14, 19, B)
@@ -404,7 +418,8 @@ def heterogeneous_batch(args, rank, world, cpu_leg):
     # FP64 subset: evenly spaced instances
     nref = min(B, args.c4_ref_instances)
     ref_ids = sorted(set(int(round(k * (B - 1) / max(1, nref - 1))) for k in range(nref)))
-    out = {"instances_per_gpu": B, "dims": np.bincount(dims, minlength=9)[[2, 3, 4, 6, 8]].tolist(),
+    out = {"instances_per_gpu": B, "work_budget_gib": args.c4_budget_gib or "automatic",
+           "dims": np.bincount(dims, minlength=9)[[2, 3, 4, 6, 8]].tolist(),
            "builds_per_step": builds, "input_build_seconds": round(inputs_s, 2)}
     t0 = time.perf_counter()
     plan = tb.Tcl4Plan(inst, precision="fp32")

@@ -263,8 +263,9 @@ int taco_set_fused_conv(int on);
 int taco_get_fused_conv(int* on);
 /* No counterpart in the reference (whose thread_local workspace is freed at thread exit,
  * cpp/src/backend/cuda/tcl4_fused_cuda.cu:676-685).  Frees the calling thread's grow-only
- * device and pinned transient buffers on the current device after its streams finish; the
- * next call allocates them again.  Plans keep their own buffers. */
+ * device and pinned transient buffers on the current device after its streams finish, with
+ * the precision guard's buffers and the FP64 heads it prepared for repeated direct calls;
+ * the next call allocates them again.  Plans keep their own buffers. */
 int taco_release_workspace(void);
 int taco_set_fp32_guard(double tol);
 int taco_get_fp32_guard(double* tol);

@@ -88,14 +88,25 @@ struct DeviceBuffer {
         p = nullptr;
         cap = 0;
     }
-    void ensure(std::size_t bytes) {
+    // grow-only with 1/8 slack (transient buffers reused by later calls); exact: a plan's
+    // buffer, sized once
+    void ensure(std::size_t bytes, bool exact = false) {
         if (bytes <= cap) return;
         if (!owned) throw Error(kRuntime, "shared work buffer smaller than the build needs");
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
-        const std::size_t want = align_up(bytes + bytes / 8, std::size_t(1) << 20);
-        cuda_check(cudaMalloc(&p, want), "cudaMalloc(workspace)");
+        const std::size_t want = align_up(exact ? bytes : bytes + bytes / 8, std::size_t(1) << 20);
+        const cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            std::size_t fr = 0, tot = 0;
+            (void)cudaGetLastError();
+            cudaMemGetInfo(&fr, &tot);
+            throw Error(kCuda, "cudaMalloc(workspace): " + std::string(cudaGetErrorString(e)) + " (" +
+                                   std::to_string(want >> 20) + " MiB requested, " + std::to_string(fr >> 20) +
+                                   " MiB free)");
+        }
         cap = want;
     }
     ~DeviceBuffer() {
@@ -2181,7 +2192,7 @@ Tcl4Plan* plan_create_direct(std::vector<Tcl4Instance>& insts, const BuildOption
         plan->work.cap = ext_cap;
         plan->work.owned = false;
     }
-    plan->work.ensure(pw.total);
+    plan->work.ensure(pw.total, true);
     std::size_t region = 0;
     for (std::size_t gi = 0; gi < groups.size(); ++gi) {
         auto& gu = groups[gi];

@@ -131,7 +131,16 @@ struct DevMem {
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
-        cuda_check(cudaMalloc(&p, bytes), "cudaMalloc(guard)");
+        const cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            std::size_t fr = 0, tot = 0;
+            (void)cudaGetLastError();
+            cudaMemGetInfo(&fr, &tot);
+            throw Error(kCuda, "cudaMalloc(guard): " + std::string(cudaGetErrorString(e)) + " (" +
+                                   std::to_string(bytes >> 20) + " MiB requested, " + std::to_string(fr >> 20) +
+                                   " MiB free)");
+        }
         cap = bytes;
     }
     DevMem() = default;
