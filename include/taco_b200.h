@@ -273,6 +273,11 @@ int taco_get_fp32_guard(double* tol);
  * instances of the call, instances with an FP64 head, requested times rebuilt in FP64,
  * requested times of those instances, instances rebuilt in FP64 entirely, growth rounds. */
 int taco_fp32_guard_stats(uint64_t* counts6);
+/* No counterpart in the reference.  Bytes of FP64 head rows the precision guard builds and
+ * patches at a time (0: the default, 1 GiB): heads beyond it are built in further chunks
+ * (plans then replay their heads after the FP32 graph instead of beside it; direct calls
+ * check them instead of replaying remembered ones).  For memory-tight batches and tests. */
+int taco_set_guard_chunk_bytes(size_t bytes);
 /* FFT length the build uses for n_in consumed samples (flags: TACO_FULL_LENGTH_FFT selects
  * the reference's power-of-two rule), and its schedule key for taco_set_tuning: log2 of a
  * power of two, + 64 for 3 * 2^k, + 128 for 5 * 2^k. */
@@ -281,7 +286,7 @@ int taco_fft_length(size_t n_in, int precision, int flags, size_t* nfft, int* ke
  * (taco_fft_length) and a precision, as chosen by the autotuner (taco_b200/autotune.py):
  * column / row tile sizes in elements (powers of two in [8, 8192]), bytes of Z/W scratch per
  * chunk of triples, and the largest number of output rows for which the inverse column pass
- * is a pruned direct DFT.  Unset lengths use the defaults (4096, 2048, 48 MiB, 16). */
+ * is a pruned direct DFT.  Unset lengths use the defaults (4096, 2048, 48 MiB, 0). */
 int taco_set_tuning(int log2_nfft, int precision, int col_tile, int row_tile, size_t chunk_bytes, int inv_dft_rows);
 /* No counterpart in the reference.  Whether the causal rule may pick the mixed length of
  * schedule key `key` (64 + k: 3 * 2^k, 128 + k: 5 * 2^k) for `precision`; the autotuner turns

@@ -42,6 +42,7 @@ __all__ = [
     "version", "device_count", "kernel_launches", "profile", "compute_triple_kernels_batch", "tcl2_generator_series", "gamma_trapz_device",
     "propagate_tcl", "gamma_trapz_device_batch", "set_work_budget", "fft_length", "build_mikx", "assemble_liouvillian", "gw_to_liouvillian",
     "set_fp32_guard", "fp32_guard", "fp32_guard_stats", "set_fused_conv", "fused_conv", "release_workspace",
+    "set_guard_chunk_bytes",
 ]
 
 
@@ -108,6 +109,12 @@ def fp32_guard() -> float:
     v = ct.c_double(0.0)
     _capi.check(_capi.lib().taco_get_fp32_guard(ct.byref(v)))
     return v.value
+
+
+def set_guard_chunk_bytes(nbytes: int) -> None:
+    """Bytes of FP64 head rows the precision guard builds and patches at a time (0: default,
+    1 GiB); heads beyond it go in further chunks."""
+    _capi.check(_capi.lib().taco_set_guard_chunk_bytes(int(nbytes)))
 
 
 def set_fused_conv(on: bool) -> None:

@@ -40,7 +40,7 @@ EXPORTED = [
     "taco_bcf_fft", "taco_rk4_forward_checkpointed", "taco_rk4_adjoint", "taco_tcl4_adjoint",
     "taco_tcl2_adjoint", "taco_inner_re", "taco_set_work_budget", "taco_gamma_trapz_batch",
     "taco_fft_length", "taco_compute_triple_kernels_batch", "taco_set_fp32_guard", "taco_get_fp32_guard",
-    "taco_fp32_guard_stats", "taco_set_fused_conv", "taco_get_fused_conv",
+    "taco_fp32_guard_stats", "taco_set_fused_conv", "taco_get_fused_conv", "taco_set_guard_chunk_bytes",
     "taco_release_workspace", "taco_set_fft_length_enabled",
 ]
 
@@ -184,6 +184,7 @@ def lib():
         L.taco_fp32_guard_stats.argtypes = [ct.POINTER(ct.c_uint64)]
         L.taco_set_fused_conv.argtypes = [ct.c_int]
         L.taco_get_fused_conv.argtypes = [ct.POINTER(ct.c_int)]
+        L.taco_set_guard_chunk_bytes.argtypes = [ct.c_size_t]
         L.taco_release_workspace.argtypes = []
         L.taco_set_fft_length_enabled.argtypes = [ct.c_int, ct.c_int, ct.c_int]
         L.taco_fft_length.argtypes = [ct.c_size_t, ct.c_int, ct.c_int, ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_int)]

@@ -286,7 +286,12 @@ def main():
             tidx = np.arange(0, Nt, 8, dtype=np.uint32)
             inst = [(s, g, dt, tidx)]
             for prec in args.precisions.split(","):
-                tune_tiles(inst, tidx, int(tidx[-1]) + 1, prec, cands=small_candidates(prec))
+                # every output row is kept here, so the pruned inverse DFT never runs: keep the
+                # choice an earlier workload measured for this length (0 if none)
+                key = f"{tb.fft_length(int(tidx[-1]) + 1, prec)[1]}:{prec}"
+                keep = entries.get(key, {}).get("inv_dft_rows", 0)
+                cands = [c for c in small_candidates(prec) if c["inv_dft_rows"] == keep]
+                tune_tiles(inst, tidx, int(tidx[-1]) + 1, prec, cands=cands)
             del g, C
             tb.release_workspace()
             torch.cuda.empty_cache()

@@ -655,6 +655,10 @@ int taco_set_fp32_guard(double tol) {
     });
 }
 
+int taco_set_guard_chunk_bytes(size_t bytes) {
+    return guarded([&] { taco::set_guard_chunk_bytes(bytes); });
+}
+
 int taco_fp32_guard_stats(uint64_t* counts6) {
     return guarded([&] {
         if (!counts6) throw taco::Error(taco::kInvalidArgument, "counts is null");

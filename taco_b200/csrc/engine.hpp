@@ -70,7 +70,8 @@ struct Tuning {
     int col_tile = 4096;                        // elements per column-pass tile
     int row_tile = 2048;                        // elements per row-pass tile
     std::size_t chunk_bytes = std::size_t(48) << 20;  // Z/W scratch per chunk of triples
-    int inv_dft_rows = 16;                      // pruned inverse column DFT up to this many rows
+    int inv_dft_rows = 0;  // pruned inverse column DFT up to this many rows (0: the column FFT always;
+                           // measured slower than the FFT at 10 and 16 rows, in both precisions)
     int cluster_lm = 0;  // log2 points per CTA of the cluster path (0: multi-pass path, -1: automatic)
     int enabled = 1;     // 3 * 2^k and 5 * 2^k lengths: 0 removes the length from the causal rule's choice
 };
@@ -140,6 +141,8 @@ uint64_t plan_kernels(const Tcl4Plan* plan);
 // checked window (0: off).
 void set_fp32_guard(double tol);
 double fp32_guard();
+// Bytes of FP64 head rows the guard builds and patches at a time (0: the default, 1 GiB).
+void set_guard_chunk_bytes(std::size_t bytes);
 // What the guard did in the calling thread's last FP32 build or plan creation.
 struct GuardStats {
     uint64_t instances = 0;  // instances of the call

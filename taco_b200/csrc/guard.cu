@@ -72,7 +72,9 @@ thread_local std::map<std::pair<const void*, uint32_t>, HeadMemory> t_head_memor
 
 constexpr std::size_t kMinHead = 512;        // smallest head (samples)
 constexpr std::size_t kWindowSamples = 256;  // requested times compared per check
-constexpr std::size_t kTempBytes = std::size_t(1) << 30;  // FP64 head rows per chunk
+// FP64 head rows per chunk of heads (a chunk's heads are built into one buffer and patched
+// before the next chunk reuses it); settable for tests and tight memory
+std::atomic<std::size_t> g_head_chunk_bytes{std::size_t(1) << 30};
 
 struct GuardJob {
     const double2* h64;       // head rows [n][E], FP64
@@ -310,7 +312,7 @@ private:
 };
 
 // FP64 builds of the heads of `heads` (into one device buffer of head rows), chunked so
-// that each chunk's rows fit kTempBytes (a single head may exceed it).
+// that each chunk's rows fit the chunk size (a single head may exceed it).
 template <class Fn>
 void for_chunks(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads, Fn fn) {
     std::size_t k0 = 0;
@@ -318,7 +320,7 @@ void for_chunks(const std::vector<Tcl4Instance>& insts, const std::vector<Head>&
         std::size_t k1 = k0, bytes = 0;
         while (k1 < heads.size() && k1 - k0 < 32768) {  // jobs of one launch along grid y
             const std::size_t b = heads[k1].times.size() * entries(insts[heads[k1].inst]) * sizeof(double2);
-            if (k1 > k0 && bytes + b > kTempBytes) break;
+            if (k1 > k0 && bytes + b > g_head_chunk_bytes.load()) break;
             bytes += b;
             ++k1;
         }
@@ -510,6 +512,18 @@ GuardScratch& guard_scratch() {
     return *p;
 }
 
+// Options of the FP64 head builds: the causal FFT length of each head (short transforms are
+// both cheaper and more accurate at the first times) whatever length the FP32 pass uses.
+BuildOptions head_options(const BuildOptions& opt) {
+    BuildOptions o = opt;
+    o.fp32 = false;
+    o.fcr_ms = nullptr;
+    o.out_hook = nullptr;
+    o.causal_truncation = true;
+    o.pad_factor = 0;
+    return o;
+}
+
 // Runs the guard loop: FP64 heads, comparison, growth.  With `patch`, accepted heads are
 // written into the outputs right away (direct calls); otherwise only the final heads are
 // returned (plans).  The FP32 results must already be in the outputs.  Comparison and
@@ -518,10 +532,7 @@ GuardScratch& guard_scratch() {
 Decision run_guard(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaStream_t st, bool patch,
                    PreHeads* pre = nullptr, bool trusted = false, const std::vector<uint64_t>* fps = nullptr) {
     const double tol = g_guard_tol.load();
-    BuildOptions o64 = opt;
-    o64.fp32 = false;
-    o64.fcr_ms = nullptr;
-    o64.out_hook = nullptr;
+    const BuildOptions o64 = head_options(opt);
     // every head row is compared: the row profile sets the head a plan replays, and the head
     // a direct call remembers for its next call on the same inputs; a plan's first head is a
     // quarter of the series, a direct call's a sixteenth
@@ -1002,6 +1013,7 @@ void launch_head_plans(HeadPlans& hp, cudaStream_t st) {
 }  // namespace
 
 void set_fp32_guard(double tol) { g_guard_tol.store(tol > 0.0 ? tol : 0.0); }
+void set_guard_chunk_bytes(std::size_t bytes) { g_head_chunk_bytes.store(bytes ? bytes : std::size_t(1) << 30); }
 void release_guard_scratch() {
     int dev = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
@@ -1042,6 +1054,13 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
         Head h = tcache.head(insts, a, it->second.required, tcs[a]);
         if (!h.times.empty()) heads.push_back(std::move(h));
     }
+    {
+        // the prepared heads keep all their rows at once: within one chunk of head rows,
+        // else the call is checked as usual (in chunks)
+        std::size_t bytes = 0;
+        for (const Head& h : heads) bytes += h.times.size() * entries(insts[h.inst]) * sizeof(double2);
+        trusted = trusted && bytes <= g_head_chunk_bytes.load();
+    }
     const auto t0 = std::chrono::steady_clock::now();
     auto t_key = t0;
     HeadPlans* hp = nullptr;
@@ -1051,10 +1070,7 @@ void tcl4_build(std::vector<Tcl4Instance>& insts, const BuildOptions& opt, cudaS
         const uint64_t key = heads_key(insts, heads, opt);
         t_key = std::chrono::steady_clock::now();
         if (key != hp->key || hp->empty()) {
-            BuildOptions o64 = opt;
-            o64.fp32 = false;
-            o64.fcr_ms = nullptr;
-            o64.out_hook = nullptr;
+            const BuildOptions o64 = head_options(opt);
             try {
                 build_head_plans(*hp, insts, heads, o64);
                 hp->key = key;
@@ -1188,11 +1204,7 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
         release_guard_scratch();
         if (dec.heads.empty()) return plan;
         // the heads as FP64 plans over one shared buffer of head rows, each followed by its patch
-        BuildOptions o64 = opt;
-        o64.fp32 = false;
-        o64.fcr_ms = nullptr;
-        o64.out_hook = nullptr;
-    o64.out_hook = nullptr;
+        const BuildOptions o64 = head_options(opt);
         struct Part {
             Tcl4Plan* plan = nullptr;
             std::vector<Tcl4Plan*> levels;  // short-FFT levels, replayed after the head
@@ -1283,8 +1295,27 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
             std::fprintf(stderr, "%s; levels %zu (<%u) %zu (<%u); tail kernels %llu\n", line.c_str(), nl[0], kLevels[0], nl[1],
                          kLevels[1], static_cast<unsigned long long>(kernels));
         }
-        // the FP64 heads (and their levels, in order) on the side stream, after the work queued
-        // before the execute and beside the FP32 graph; the patches after both
+        // One chunk of heads: the FP64 heads (and their levels, in order) on the side stream,
+        // after the work queued before the execute and beside the FP32 graph, the patch after
+        // both.  Several chunks share one buffer of head rows: each chunk's heads, levels and
+        // patch in turn after the graph.
+        if (tail->parts.size() > 1) {
+            plan_set_tail(
+                plan, nullptr,
+                [tail](cudaStream_t s) {
+                    for (const Part& p : tail->parts) {
+                        plan_execute(p.plan, s);
+                        for (Tcl4Plan* l : p.levels) plan_execute(l, s);
+                        const GuardJob* jobs =
+                            reinterpret_cast<const GuardJob*>(static_cast<unsigned char*>(tail->meta.p) + p.meta_off);
+                        k_guard_patch<<<dim3(p.blocks, static_cast<unsigned>(p.jobs)), 256, 0, s>>>(jobs);
+                        cuda_check(cudaGetLastError(), "k_guard_patch");
+                        count_launches(1);
+                    }
+                },
+                kernels);
+            return plan;
+        }
         plan_set_tail(
             plan,
             [tail](cudaStream_t s) {

@@ -221,3 +221,27 @@ def test_guard_remembers_heads_across_direct_calls():
     ref = fp64_reference(cases[0][1], g0, cases[0][3], cases[0][4])
     for lo, e in window_errors(third, ref, cases[0][4]):
         assert e <= 1e-6, (lo, e)
+
+
+def test_guard_heads_in_several_chunks():
+    """Heads whose rows exceed one chunk of the guard's head buffer are built and patched
+    chunk by chunk: a plan (its heads after the FP32 graph, chunk after chunk) and direct
+    calls (checked, not replayed) still meet 1e-6 in every window."""
+    import torch
+    cases = [c4_case(H_SLOW, A_SLOW, 14, 0.09, wc, 0.7) for wc in (1.5, 3.0, 6.0, 12.7)]
+    inst = [(s, torch.from_numpy(G).cuda(), dt, tidx) for _, s, G, dt, tidx in cases]
+    tb.set_guard_chunk_bytes(64 << 10)  # a few hundred head rows per chunk
+    try:
+        plan = tb.Tcl4Plan(inst, precision="fp32")
+        stats = tb.fp32_guard_stats()
+        planned = [r.cpu().numpy() for r in plan.run()]
+        plan.close()
+        direct = [[x.cpu().numpy() for x in tb.build_instances(inst, precision="fp32")] for _ in range(2)]
+    finally:
+        tb.set_guard_chunk_bytes(0)
+    assert stats["instances_with_fp64_head"] >= 2, stats
+    for (osys, s, G, dt, tidx), x, p, d0, d1 in zip(cases, inst, planned, direct[0], direct[1]):
+        ref = fp64_reference(s, x[1], dt, tidx)
+        for name, got in (("plan", p), ("direct", d0), ("direct again", d1)):
+            for lo, e in window_errors(got, ref, tidx):
+                assert e <= 1e-6, (name, lo, e, stats)
