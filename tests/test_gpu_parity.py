@@ -358,3 +358,23 @@ def test_long_host_buckets_match_device_inputs():
     torch.cuda.synchronize()
     for k in (0, 23, 47):
         assert np.array_equal(outs_h[k], outs_d[k])
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 2e-6)])
+def test_pruned_inverse_dft_schedule_matches_column_fft(precision, tol):
+    """A schedule with the pruned inverse column DFT (few output rows) gives the column FFT's
+    results; the default schedule uses the FFT."""
+    from taco_b200 import autotune
+    osys, s, G = spin_boson_case(600, 0.005)
+    tidx = np.arange(0, 101)
+    nfft, key = tb.fft_length(int(tidx[-1]) + 1, precision)
+    old = autotune.get_schedule(key, precision)
+    assert old["inv_dft_rows"] == 0
+    try:
+        base = tb.build_TCL4_generator_batch(s, G, 0.005, tidx, precision=precision)
+        autotune.set_schedule(key, precision, old["col_tile"], old["row_tile"], old["chunk_bytes"], 16)
+        dft = tb.build_TCL4_generator_batch(s, G, 0.005, tidx, precision=precision)
+    finally:
+        autotune.set_schedule(key, precision, old["col_tile"], old["row_tile"], old["chunk_bytes"], old["inv_dft_rows"])
+    assert relerr(dft, base) <= tol
+    assert relerr(dft, oracle_l4(osys, G, 0.005, tidx)) <= (1e-10 if precision == "fp64" else 1e-6)
