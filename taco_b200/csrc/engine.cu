@@ -436,6 +436,7 @@ template <class R>
 using InvFn = void (*)(const InvJob*, FftPlan<cplx_t<R>>, int);
 
 #define TACO_CT_CASES(X) \
+    X(4, 5) X(5, 4) X(5, 5) X(5, 6) X(6, 5) X(6, 6) \
     X(7, 3) X(7, 4) X(7, 5) X(8, 2) X(8, 3) X(8, 4) X(9, 1) X(9, 2) X(9, 3) X(10, 0) X(10, 1) X(10, 2)
 
 // Column kernels of the mixed lengths N1 = R * 2^l for the tile widths the default and
