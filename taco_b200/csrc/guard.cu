@@ -44,6 +44,7 @@
 #include <cstdint>
 #include <cstring>
 #include <functional>
+#include <iterator>
 #include <map>
 #include <string>
 #include <tuple>
@@ -360,14 +361,22 @@ std::vector<Tcl4Instance> head_instances(const std::vector<Tcl4Instance>& insts,
 // earliest, tiny L4 values is orders of magnitude below that of the head's own transform.
 constexpr uint32_t kLevels[] = {2048, 256};
 
+// Rows of head h that the level of `bound` rebuilds (0: the level does not apply).
+std::size_t level_rows(const Head& h, uint32_t bound) {
+    if (h.H <= bound || !std::is_sorted(h.times.begin(), h.times.end())) return 0;
+    return static_cast<std::size_t>(std::lower_bound(h.times.begin(), h.times.end(), bound) - h.times.begin());
+}
+
+// keep (optional): per head of [k0, k1), whether this level is built at all.
 std::vector<Tcl4Instance> level_instances(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads,
                                           std::size_t k0, std::size_t k1, double2* base,
-                                          const std::vector<std::size_t>& off, uint32_t bound) {
+                                          const std::vector<std::size_t>& off, uint32_t bound,
+                                          const std::vector<char>* keep = nullptr) {
     std::vector<Tcl4Instance> li;
     for (std::size_t k = k0; k < k1; ++k) {
         const Head& h = heads[k];
-        if (h.H <= bound || !std::is_sorted(h.times.begin(), h.times.end())) continue;
-        const std::size_t n = static_cast<std::size_t>(std::lower_bound(h.times.begin(), h.times.end(), bound) - h.times.begin());
+        if (keep && !(*keep)[k - k0]) continue;
+        const std::size_t n = level_rows(h, bound);
         if (n == 0) continue;
         const Tcl4Instance& in = insts[h.inst];
         Tcl4Instance l;
@@ -395,6 +404,70 @@ void build_heads(const std::vector<Tcl4Instance>& insts, const std::vector<Head>
         std::vector<Tcl4Instance> li = level_instances(insts, heads, k0, k1, base, off, bound);
         if (!li.empty()) tcl4_build_direct(li, o64, st);
     }
+}
+
+// Which short-FFT levels of the heads [k0, k1) change their rows.  The heads and then each
+// level (coarse to fine) are built once in FP64; a level is kept for a head when, in some
+// window of times below its bound ([0, 64), [64, 128), ...), its rows differ from the rows it
+// would overwrite (the head's, or a kept coarser level's) by more than tol / 8 (relative
+// Frobenius); the others are left out of the replays.  keep[q][k - k0] for level q.
+std::vector<std::vector<char>> needed_levels(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads,
+                                             std::size_t k0, std::size_t k1, const BuildOptions& o64, double tol,
+                                             cudaStream_t st) {
+    const std::size_t n = k1 - k0;
+    std::vector<std::vector<char>> keep(std::size(kLevels), std::vector<char>(n, 0));
+    bool any = false;
+    for (uint32_t bound : kLevels)
+        for (std::size_t k = k0; k < k1; ++k) any = any || level_rows(heads[k], bound) > 0;
+    if (!any) return keep;
+    std::size_t bytes = 256;
+    for (std::size_t k = k0; k < k1; ++k) bytes += heads[k].times.size() * entries(insts[heads[k].inst]) * sizeof(double2);
+    DevMem hrows, lrows;
+    hrows.ensure(bytes);
+    lrows.ensure(bytes);
+    std::vector<std::size_t> off;
+    std::vector<Tcl4Instance> hi = head_instances(insts, heads, k0, k1, static_cast<double2*>(hrows.p), off);
+    tcl4_build_direct(hi, o64, st);  // synchronous
+    std::vector<double2> h_host, l_host;
+    for (std::size_t q = 0; q < std::size(kLevels); ++q) {
+        const uint32_t bound = kLevels[q];
+        std::vector<char> all(n, 1);
+        std::vector<Tcl4Instance> li =
+            level_instances(insts, heads, k0, k1, static_cast<double2*>(lrows.p), off, bound, &all);
+        if (li.empty()) continue;
+        tcl4_build_direct(li, o64, st);
+        for (std::size_t k = k0; k < k1; ++k) {
+            const Head& h = heads[k];
+            const std::size_t rows = level_rows(h, bound);
+            if (!rows) continue;
+            const std::size_t E = entries(insts[h.inst]);
+            h_host.resize(rows * E);
+            l_host.resize(rows * E);
+            const double2* hp = static_cast<const double2*>(hrows.p) + off[k - k0];
+            const double2* lp = static_cast<const double2*>(lrows.p) + off[k - k0];
+            cuda_check(cudaMemcpy(h_host.data(), hp, rows * E * sizeof(double2), cudaMemcpyDeviceToHost), "cudaMemcpy(levels)");
+            cuda_check(cudaMemcpy(l_host.data(), lp, rows * E * sizeof(double2), cudaMemcpyDeviceToHost), "cudaMemcpy(levels)");
+            std::vector<double> num(40, 0.0), den(40, 0.0);
+            for (std::size_t r = 0; r < rows; ++r) {
+                int w = 0;
+                while (w < 39 && (std::size_t(64) << w) <= h.times[r]) ++w;
+                for (std::size_t e = 0; e < E; ++e) {
+                    const double2 a = l_host[r * E + e], b = h_host[r * E + e];
+                    num[w] += (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y);
+                    den[w] += a.x * a.x + a.y * a.y;
+                }
+            }
+            bool need = false;
+            for (int w = 0; w < 40 && !need; ++w)
+                need = den[w] > 0.0 ? std::sqrt(num[w] / den[w]) > tol / 8 : num[w] > 0.0;
+            keep[q][k - k0] = need ? 1 : 0;
+            // a kept level's rows are what the next, finer level would overwrite
+            if (need)
+                cuda_check(cudaMemcpy(const_cast<double2*>(hp), lp, rows * E * sizeof(double2), cudaMemcpyDeviceToDevice),
+                           "cudaMemcpy(levels)");
+        }
+    }
+    return keep;
 }
 
 // Device jobs of heads [k0, k1) and their index arrays, as one host image of the device
@@ -939,18 +1012,19 @@ void build_head_plans(HeadPlans& hp, const std::vector<Tcl4Instance>& insts, con
         while (c < 2 && heads[k].inst >= kChunkBounds[c]) ++c;
         hp.chunk_of[k] = c;
     }
+    // the levels that change their heads' rows (measured once, for the kept set of heads)
+    const std::vector<std::vector<char>> keep = needed_levels(insts, heads, 0, nh, o64, g_guard_tol.load(), nullptr);
     for (uint32_t c = 0; c < 3; ++c) {
         std::vector<std::vector<Tcl4Instance>> parts(1);
         for (std::size_t k = 0; k < nh; ++k)
             if (hp.chunk_of[k] == c) parts[0].push_back(hi[k]);
         if (parts[0].empty()) continue;
-        for (uint32_t bound : kLevels) {
+        for (std::size_t q = 0; q < std::size(kLevels); ++q) {
             std::vector<Tcl4Instance> li;
             for (std::size_t k = 0; k < nh; ++k) {
                 const Head& h = heads[k];
-                if (hp.chunk_of[k] != c || h.H <= bound || !std::is_sorted(h.times.begin(), h.times.end())) continue;
-                const std::size_t n =
-                    static_cast<std::size_t>(std::lower_bound(h.times.begin(), h.times.end(), bound) - h.times.begin());
+                if (hp.chunk_of[k] != c || !keep[q][k]) continue;
+                const std::size_t n = level_rows(h, kLevels[q]);
                 if (n == 0) continue;
                 Tcl4Instance l = hi[k];
                 l.tidx.share_with(list_of(h, static_cast<uint32_t>(n)));
@@ -1251,9 +1325,13 @@ Tcl4Plan* plan_create(std::vector<Tcl4Instance>& insts, const BuildOptions& opt)
         tail->meta.ensure(meta_total + 256);
         // one transient buffer for every head plan (they run one after another)
         std::vector<std::vector<std::vector<Tcl4Instance>>> lis(ranges.size());
-        for (std::size_t c = 0; c < ranges.size(); ++c)
-            for (uint32_t bound : kLevels)
-                lis[c].push_back(level_instances(insts, dec.heads, ranges[c].first, ranges[c].second, base, offs[c], bound));
+        for (std::size_t c = 0; c < ranges.size(); ++c) {
+            const std::vector<std::vector<char>> keep =
+                needed_levels(insts, dec.heads, ranges[c].first, ranges[c].second, o64, g_guard_tol.load(), st);
+            for (std::size_t q = 0; q < std::size(kLevels); ++q)
+                lis[c].push_back(level_instances(insts, dec.heads, ranges[c].first, ranges[c].second, base, offs[c],
+                                                 kLevels[q], &keep[q]));
+        }
         // measured under the current budget; the plans group by that same budget, and the
         // buffer has slack for the rounding of the slice sizes
         const std::size_t budget = work_budget_now();
