@@ -126,6 +126,30 @@ __global__ void __launch_bounds__(256) k_guard_patch(const GuardJob* __restrict_
     }
 }
 
+// Per row r < rows of a level and the head rows it would overwrite (E entries each; one warp
+// per row): out[r] = (sum |l - h|^2, sum |l|^2).
+__global__ void __launch_bounds__(256) k_level_rowsums(const double2* __restrict__ l, const double2* __restrict__ h,
+                                                       uint32_t rows, uint32_t E, double2* __restrict__ out) {
+    const uint32_t r = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    const double2* a = l + static_cast<std::size_t>(r) * E;
+    const double2* b = h + static_cast<std::size_t>(r) * E;
+    double num = 0.0, den = 0.0;
+    for (uint32_t e = lane; e < E; e += 32) {
+        const double2 x = a[e], y = b[e];
+        const double dx = x.x - y.x, dy = x.y - y.y;
+        num += dx * dx + dy * dy;
+        den += x.x * x.x + x.y * x.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, o);
+        den += __shfl_xor_sync(0xffffffffu, den, o);
+    }
+    if (lane == 0) out[r] = make_double2(num, den);
+}
+
 struct DevMem {
     void* p = nullptr;
     std::size_t cap = 0;
@@ -414,6 +438,7 @@ void build_heads(const std::vector<Tcl4Instance>& insts, const std::vector<Head>
 std::vector<std::vector<char>> needed_levels(const std::vector<Tcl4Instance>& insts, const std::vector<Head>& heads,
                                              std::size_t k0, std::size_t k1, const BuildOptions& o64, double tol,
                                              cudaStream_t st) {
+    if (!st) st = default_stream();  // builds, comparisons and copies in one stream's order
     const std::size_t n = k1 - k0;
     std::vector<std::vector<char>> keep(std::size(kLevels), std::vector<char>(n, 0));
     bool any = false;
@@ -428,7 +453,8 @@ std::vector<std::vector<char>> needed_levels(const std::vector<Tcl4Instance>& in
     std::vector<std::size_t> off;
     std::vector<Tcl4Instance> hi = head_instances(insts, heads, k0, k1, static_cast<double2*>(hrows.p), off);
     tcl4_build_direct(hi, o64, st);  // synchronous
-    std::vector<double2> h_host, l_host;
+    DevMem sums;
+    std::vector<double2> rs;
     for (std::size_t q = 0; q < std::size(kLevels); ++q) {
         const uint32_t bound = kLevels[q];
         std::vector<char> all(n, 1);
@@ -441,21 +467,24 @@ std::vector<std::vector<char>> needed_levels(const std::vector<Tcl4Instance>& in
             const std::size_t rows = level_rows(h, bound);
             if (!rows) continue;
             const std::size_t E = entries(insts[h.inst]);
-            h_host.resize(rows * E);
-            l_host.resize(rows * E);
             const double2* hp = static_cast<const double2*>(hrows.p) + off[k - k0];
             const double2* lp = static_cast<const double2*>(lrows.p) + off[k - k0];
-            cuda_check(cudaMemcpy(h_host.data(), hp, rows * E * sizeof(double2), cudaMemcpyDeviceToHost), "cudaMemcpy(levels)");
-            cuda_check(cudaMemcpy(l_host.data(), lp, rows * E * sizeof(double2), cudaMemcpyDeviceToHost), "cudaMemcpy(levels)");
+            // per row on the device: (sum |level - head|^2, sum |level|^2) over the entries
+            sums.ensure(rows * sizeof(double2));
+            k_level_rowsums<<<static_cast<unsigned>((rows + 7) / 8), 256, 0, st>>>(
+                lp, hp, static_cast<uint32_t>(rows), static_cast<uint32_t>(E), static_cast<double2*>(sums.p));
+            cuda_check(cudaGetLastError(), "k_level_rowsums");
+            count_launches(1);
+            rs.resize(rows);
+            cuda_check(cudaMemcpyAsync(rs.data(), sums.p, rows * sizeof(double2), cudaMemcpyDeviceToHost, st),
+                       "cudaMemcpyAsync(levels)");
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(levels)");
             std::vector<double> num(40, 0.0), den(40, 0.0);
             for (std::size_t r = 0; r < rows; ++r) {
                 int w = 0;
                 while (w < 39 && (std::size_t(64) << w) <= h.times[r]) ++w;
-                for (std::size_t e = 0; e < E; ++e) {
-                    const double2 a = l_host[r * E + e], b = h_host[r * E + e];
-                    num[w] += (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y);
-                    den[w] += a.x * a.x + a.y * a.y;
-                }
+                num[w] += rs[r].x;
+                den[w] += rs[r].y;
             }
             bool need = false;
             for (int w = 0; w < 40 && !need; ++w)
@@ -463,10 +492,12 @@ std::vector<std::vector<char>> needed_levels(const std::vector<Tcl4Instance>& in
             keep[q][k - k0] = need ? 1 : 0;
             // a kept level's rows are what the next, finer level would overwrite
             if (need)
-                cuda_check(cudaMemcpy(const_cast<double2*>(hp), lp, rows * E * sizeof(double2), cudaMemcpyDeviceToDevice),
-                           "cudaMemcpy(levels)");
+                cuda_check(cudaMemcpyAsync(const_cast<double2*>(hp), lp, rows * E * sizeof(double2),
+                                           cudaMemcpyDeviceToDevice, st),
+                           "cudaMemcpyAsync(levels)");
         }
     }
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(levels)");
     return keep;
 }
 
