@@ -248,10 +248,12 @@ int taco_set_work_budget(size_t bytes);
  * rows, the head growing fourfold while the misses reach its end, up to a full FP64 build of
  * the instance.  The FP64 rows below 2048 and 256 come from builds of those times alone
  * (short FFTs, whose round-off at the first, tiny L4 values is far below the full-length
- * transform's).  Plans choose their heads once, at creation, and replay them; direct calls
- * remember, per gamma buffer and a fingerprint of its contents, the heads a call needed and
- * build only those on a helper thread during the next call's FP32 pass.  tol = 0 turns the
- * guard off; the default is 5e-7.  taco_get_fp32_guard returns the current value. */
+ * transform's) wherever those builds change the head's rows by more than tol/8.  Plans
+ * choose their heads once, at creation, and replay them beside the FP32 graph; direct calls
+ * remember, per gamma buffer and a fingerprint of its contents, the heads a call needed,
+ * prepare them once as FP64 plans and replay them beside the next calls' FP32 passes.
+ * tol = 0 turns the guard off; the default is 5e-7.  taco_get_fp32_guard returns the
+ * current value. */
 /* No counterpart in the reference.  The fused F/C/R path: for FFT lengths whose working
  * array fits one CTA's shared memory (FP32 up to 24576 points, FP64 up to 12288), one CTA per
  * (triple, half) runs the forward transform, the spectral product, the inverse transform, the

@@ -195,7 +195,7 @@ __global__ void k_guard_gather(const double2* const* __restrict__ src, double2* 
     if (k < n) out[k] = *src[k];
 }
 
-// Fingerprints of the instances' gamma (the consumed samples of every bucket at 64 evenly
+// Fingerprints of the instances' gamma (the consumed samples of every bucket at 16 evenly
 // spaced times, with the sizes and dt); device inputs are gathered by one launch.
 std::vector<uint64_t> fingerprints(const std::vector<Tcl4Instance>& insts, const std::vector<uint32_t>& tcs,
                                    cudaStream_t st) {
